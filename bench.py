@@ -1,0 +1,331 @@
+#!/usr/bin/env python
+"""H-matvec throughput on one B200 (or N replicas under torchrun).
+
+Workload (the batching configuration): N = 2^20 points i.i.d. uniform in [0,1]^3
+(SplitMix64 seed 1), Matern-3/2 kernel (1 + sqrt3 r/0.2) exp(-sqrt3 r/0.2), leaf
+size 128, eta 1.5 (min-diameter admissibility), adaptive ACA eps = 1e-8 with ranks
+up to 96, FP32 near-field blocks and FP32 low-rank factors, FP32 products summed in
+FP64.  One step = one H-matvec y = H x with x ~ U[-1,1] (seed 1001).
+
+  value  H-matvecs/s with x and y resident in HBM (device-timed with CUDA events);
+  e2e    the same through the host-buffer C-ABI call hmg_matvec_host: x copied
+         in from pinned memory and y copied out, every step, inside the timing.
+The stored H-matrix (~150 GB) is far larger than L2, so no L2 flush is needed
+between steps.  --impl reference times the FP64 direct product (the reference's
+apply_full_mvp, restated by the CPU oracle) on the host cores on a row sample.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOAD = {"workload": "hmatvec_uniform3d_matern32", "n": 1 << 20, "dim": 3, "seed": 1,
+            "kernel": "matern32", "rho": 0.2, "leaf": 128, "eta": 1.5, "admissibility": "min",
+            "aca_eps": 1e-8, "max_rank": 96}
+METRIC = "H-matvecs/s at N=2^20 (err<=1e-6 vs FP64)"
+
+
+def _peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons while the timed region runs."""
+
+    def __init__(self, index=0):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self, min_samples=1):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 7:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                mx = float(parts[1])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[3:7]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def cpu_direct_rate(p, x, kind, param, target_s=10.0, threads=None):
+    """FP64 direct-sum rows/s on the host cores (the oracle's apply_full_mvp)."""
+    from oracle import oracle as O
+    threads = threads or os.cpu_count() or 1
+    s, o, z = O.order_points(p, 20 if p.shape[0] == 3 else 32)
+    xs = np.ascontiguousarray(x[o])
+    n = p.shape[1]
+    rng = np.random.default_rng(0)
+    rows = np.ascontiguousarray(rng.choice(n, size=min(n, 8 * threads), replace=False).astype(np.int32))
+    t0 = time.perf_counter()
+    O.direct(kind, param, 0.0, z, z, xs, rows=rows, nthreads=threads)
+    dt = time.perf_counter() - t0
+    nrows = int(min(n, max(len(rows), len(rows) * target_s / max(dt, 1e-6))))
+    rows = np.ascontiguousarray(rng.choice(n, size=nrows, replace=False).astype(np.int32))
+    t0 = time.perf_counter()
+    O.direct(kind, param, 0.0, z, z, xs, rows=rows, nthreads=threads)
+    dt = time.perf_counter() - t0
+    return nrows / dt, nrows, dt, threads
+
+
+def run_reference(a, rank, world):
+    """The reference arm: FP64 direct product on host cores, bounded row sample per step."""
+    from hmglib_b200 import synth
+    from oracle import oracle as O
+    if rank != 0:
+        return 0
+    W = WORKLOAD
+    n = a.n or W["n"]
+    p = synth.uniform_points(n, W["dim"], W["seed"])
+    x = synth.rhs_vector(n, W["seed"])
+    kind = O.KERNEL_MATERN32
+    par = O.kernel_param(kind, W["rho"])
+    per_step = max(2.0, 20.0 / max(1, a.steps + a.warmup))
+    for _ in range(a.warmup):
+        cpu_direct_rate(p, x, kind, par, target_s=per_step / 4)
+    rates = []
+    for _ in range(a.steps):
+        r, nrows, dt, thr = cpu_direct_rate(p, x, kind, par, target_s=per_step)
+        rates.append(r)
+    rows_per_s = float(np.median(rates))
+    value = rows_per_s / n
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "matvec/s", "n_gpus": world,
+            "steps": a.steps, "warmup": a.warmup, "ms_per_step": 1000.0 / value, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": dict(W, n=n, parallelism="host cores"),
+            "cpu_baseline": {"value": value, "unit": "matvec/s", "cores": thr, "kind": "port",
+                             "sample": f"{nrows} random rows of the FP64 direct sum per step, scaled to N={n} rows"},
+            "e2e": {"value": value, "unit": "matvec/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_engine(a, rank, world):
+    import torch
+    import torch.distributed as dist
+
+    import hmglib_b200 as hmg
+    from hmglib_b200 import synth
+    from oracle import oracle as O
+
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    W = WORKLOAD
+    n = a.n or W["n"]
+    prec = hmg.PREC_FP32 if a.prec == "fp32" else hmg.PREC_FP64
+    esz = 4 if prec == hmg.PREC_FP32 else 8
+    p = synth.uniform_points(n, W["dim"], W["seed"])
+    x = synth.rhs_vector(n, W["seed"])
+
+    t0 = time.perf_counter()
+    H = hmg.HMatrix(n, n, W["dim"])
+    H.set_points(0, p)
+    H.set_points(1, p)
+    H.setup(W["eta"], W["leaf"], rule=hmg.ADMISSIBLE_MIN)
+    t_setup = time.perf_counter() - t0
+    H.set_kernel(hmg.KERNEL_MATERN32, W["rho"], 0.0)
+    t1 = time.perf_counter()
+    H.precompute_aca(W["max_rank"], W["aca_eps"], prec)
+    t_aca = time.perf_counter() - t1
+    near = a.near
+    t2 = time.perf_counter()
+    if near == "stored":
+        try:
+            H.precompute_dense(prec)
+        except hmg.HmgError as e:
+            if e.status != 3:
+                raise
+            near = "onthefly"
+    if near == "onthefly":
+        H.set_near_mode(hmg.NEAR_ONTHEFLY)
+    t_dense = time.perf_counter() - t2
+    info = H.info()
+
+    dx = torch.from_numpy(x).cuda()
+    dy = torch.empty(n, dtype=torch.float64, device="cuda")
+    stream = torch.cuda.default_stream()
+    for _ in range(max(3, a.warmup)):
+        H.matvec(dx, dy)
+    H.synchronize()
+    # per-kernel device times (events between the product's kernels)
+    H.set_profiling(True)
+    prof = []
+    for _ in range(3):
+        H.matvec(dx, dy)
+        prof.append(H.profile())
+    H.set_profiling(False)
+    k2_ms = float(np.median([q["tiles_ms"] for q in prof]))
+    k1_ms = float(np.median([q["vtx_ms"] for q in prof]))
+
+    # accuracy vs the FP64 direct sum on a row sample (on the GPU)
+    rng = np.random.default_rng(7)
+    rows = torch.from_numpy(rng.choice(n, size=min(n, 4096), replace=False).astype(np.int32)).cuda()
+    yd = torch.empty(rows.shape[0], dtype=torch.float64, device="cuda")
+    H.matvec(dx, dy)
+    H.full_matvec_rows(dx, rows, yd)
+    H.synchronize()
+    err = float(torch.linalg.norm(dy[rows.long()] - yd) / torch.linalg.norm(yd))
+
+    if world > 1:
+        dist.barrier()
+    with ClockSampler(local) as clk:
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        ev0 = torch.cuda.Event(enable_timing=True)
+        ev1 = torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
+        for _ in range(a.steps):
+            H.matvec(dx, dy)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        ms = ev0.elapsed_time(ev1)
+        # end-to-end through the host-buffer C-ABI call
+        xh = np.ascontiguousarray(x)
+        yh = np.empty(n)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        H.matvec(xh, yh)
+        e0.record(stream)
+        for _ in range(a.steps):
+            H.matvec(xh, yh)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms_e2e = e0.elapsed_time(e1)
+    if world > 1:
+        t = torch.tensor([ms, ms_e2e], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms, ms_e2e = float(t[0]), float(t[1])
+    ms_step = ms / a.steps
+    value = world * 1000.0 / ms_step
+    e2e_value = world * 1000.0 * a.steps / ms_e2e
+
+    peak, peak_kind = _peaks()
+    # algorithmic bytes of the tile kernel per launch: near entries and U factors
+    # streamed once, y written once (plus the permutation read)
+    near_b = info["near_entries"] * esz if near == "stored" else 0
+    ranks = H.ranks()
+    s1l, s1u, s2l, s2u, typ = H.blocks()
+    m1 = (s1u - s1l + 1).astype(np.int64)
+    m2 = (s2u - s2l + 1).astype(np.int64)
+    far = typ == 1
+    u_b = int((m1[far] * ranks[far]).sum()) * esz
+    v_b = int((m2[far] * ranks[far]).sum()) * esz
+    k2_bytes = near_b + u_b + 12 * n
+    achieved = k2_bytes / (k2_ms * 1e-3) / 1e9
+    whole_bytes = near_b + u_b + v_b + 8 * 2 * n
+    line = {
+        "metric": METRIC, "value": value, "unit": "matvec/s", "n_gpus": world, "steps": a.steps,
+        "warmup": a.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32" if prec == hmg.PREC_FP32 else "f64", "data": "synthetic",
+        "config": dict(W, n=n, near=near, storage=a.prec, parallelism=f"replicas{world}",
+                       l2="inputs larger than L2 (no flush)"),
+        "err_vs_fp64": err,
+        "e2e": {"value": e2e_value, "unit": "matvec/s", "h2d_bytes_per_step": 8 * n, "d2h_bytes_per_step": 8 * n},
+        "gpu_launches": 3 * a.steps,
+        "roofline": {"bound": "hbm", "kernel": "k_tile_matvec", "achieved": achieved, "peak": peak,
+                     "unit": "GB/s", "frac": achieved / peak, "traffic": None, "peak_kind": peak_kind,
+                     "bytes_per_launch": k2_bytes, "ms_per_launch": k2_ms},
+        "whole_matvec": {"bytes": whole_bytes, "GBps": whole_bytes / (ms_step * 1e-3) / 1e9,
+                         "frac": whole_bytes / (ms_step * 1e-3) / 1e9 / peak, "vtx_ms": k1_ms,
+                         "tiles_ms": k2_ms},
+        "build_s": {"setup": t_setup, "aca": t_aca, "dense": t_dense},
+        "hmatrix": {k: info[k] for k in ("block_count", "dense_count", "aca_count", "levels", "tile_count",
+                                         "max_rank", "near_entries", "far_entries", "near_bytes", "far_bytes")},
+        "clocks": clk.summary(),
+    }
+    if rank == 0 and world == 1 and not a.no_cpu:
+        kind = O.KERNEL_MATERN32
+        rate, nrows, dt, thr = cpu_direct_rate(p, x, kind, O.kernel_param(kind, W["rho"]), target_s=a.cpu_seconds)
+        line["cpu_baseline"] = {"value": rate / n, "unit": "matvec/s", "cores": thr, "kind": "port",
+                                "sample": f"FP64 direct sum over {nrows} random rows ({dt:.1f} s), scaled to N={n}"}
+    H.close()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    return 0
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
+    ap.add_argument("--n", type=int, default=0, help="override the point count (default 2^20)")
+    ap.add_argument("--prec", default="fp32", choices=["fp32", "fp64"])
+    ap.add_argument("--near", default="stored", choices=["stored", "onthefly"])
+    ap.add_argument("--cpu-seconds", type=float, default=10.0)
+    ap.add_argument("--no-cpu", action="store_true")
+    a = ap.parse_args(argv)
+    a.warmup = max(3, a.warmup)
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    if a.impl == "reference":
+        return run_reference(a, rank, world)
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    try:
+        return run_engine(a, rank, world)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,491 @@
+// aca.cu -- batched ACA of all admissible blocks, one CTA per block, FP64.
+//
+// The reference (linear_algebra.cu:3684-4012) advances all blocks in lock step:
+// every rank step is ~10 kernel launches, Thrust reduce_by_key calls and a host
+// synchronisation, over "batched" vectors that concatenate all blocks.  Here one
+// CTA owns one block for its whole ACA: the residual row / column, the pivot
+// searches and the norms are CTA reductions, and the only traffic is the block's
+// own U/V panels (L2-resident for all but the largest blocks).
+//
+// Two modes:
+//   * fixed (eps <= 0): the reference's semantics -- rank k_b = min(k,m1,m2)
+//     (:769-787), row pivots taken in index order skipping residual rows of norm
+//     < 1e-13 (:2009-2024, :2091, :1213-1230), column pivot = LAST index of the
+//     largest |v| (tuple_absolute_maximum, :991-1018), v scaled by the pivot
+//     (:963-986), residual updates with fused multiply-adds (:918-959, :1091-1147).
+//     The reference's scaling kernel reads the pivot entry while other threads
+//     overwrite it (:983); here the pivot is read once before any write.
+//   * adaptive (eps > 0): standard partial pivoting -- next row = largest |u_r| over
+//     unused rows, column = FIRST index of the largest |v| -- stopping when
+//     |u_r| |v_r| <= eps ||S_r||_F with the Frobenius norm of the approximant
+//     updated exactly (the criterion the reference keeps dormant at
+//     :1595-1755, without its (1-eta) factor, which is negative for eta > 1).
+//
+// Factors are computed into FP64 scratch per batch of blocks and then compacted
+// (converted to the storage precision, laid out as tile slices for U and as
+// padded rows of V^T) into one allocation per batch.
+#include <algorithm>
+#include <vector>
+
+#include "hmg_matrix.cuh"
+
+namespace hmg {
+
+static constexpr int ACA_THREADS = 256;
+static constexpr int ACA_WARPS = ACA_THREADS / 32;
+static constexpr int ACA_KMAX = 512;
+
+struct AcaBatch {
+    const int* blocks;       // block indices of this batch
+    const long long* uoff;   // FP64 scratch offsets
+    const long long* voff;
+    double* U;
+    double* V;
+    int* rank_out;           // per batch entry
+};
+
+struct BlockGeom {
+    const int *r0, *m1, *c0, *m2;
+};
+
+__device__ __forceinline__ double block_sum(double v, double* red)
+{
+    int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    __syncthreads();
+    if (lane == 0) red[warp] = v;
+    __syncthreads();
+    double s = 0.0;
+#pragma unroll
+    for (int w = 0; w < ACA_WARPS; w++) s += red[w];
+    return s;
+}
+
+// (value, index) argmax; last = true: ties go to the larger index, else the smaller.
+__device__ __forceinline__ bool better(double a, int i, double b, int j, bool last)
+{
+    if (a != b) return a > b;
+    return last ? i > j : i < j;
+}
+
+__device__ __forceinline__ void block_argmax(double& a, int& i, bool last, double* reda,
+                                             int* redi)
+{
+    int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        double b = __shfl_xor_sync(0xffffffffu, a, o);
+        int j = __shfl_xor_sync(0xffffffffu, i, o);
+        if (better(b, j, a, i, last)) { a = b; i = j; }
+    }
+    __syncthreads();
+    if (lane == 0) { reda[warp] = a; redi[warp] = i; }
+    __syncthreads();
+    a = reda[0];
+    i = redi[0];
+#pragma unroll
+    for (int w = 1; w < ACA_WARPS; w++)
+        if (better(reda[w], redi[w], a, i, last)) { a = reda[w]; i = redi[w]; }
+}
+
+__global__ void __launch_bounds__(ACA_THREADS)
+k_aca(BlockGeom g, KernelSpec K, PointsView P, AcaBatch B, int k, double eps)
+{
+    __shared__ double coef[ACA_KMAX];
+    __shared__ double red[ACA_WARPS];
+    __shared__ double reda[ACA_WARPS];
+    __shared__ int redi[ACA_WARPS];
+    __shared__ double dots[2][32];
+    extern __shared__ unsigned used[];  // adaptive mode: one bit per row
+
+    const int e = blockIdx.x;
+    const int b = B.blocks[e];
+    const int r0 = g.r0[b], m1 = g.m1[b], c0 = g.c0[b], m2 = g.m2[b];
+    int kb = k < m1 ? k : m1;
+    kb = kb < m2 ? kb : m2;
+    double* U = B.U + B.uoff[e];
+    double* V = B.V + B.voff[e];
+    const int tid = threadIdx.x;
+    const bool adaptive = eps > 0.0;
+    int rank = 0;
+
+    if (!adaptive) {
+        int ir = -1;
+        for (int r = 0; r < kb; r++) {
+            bool found = false;
+            for (;;) {
+                if (ir >= m1 - 1) break;
+                ir += 1;
+                for (int l = tid; l < r; l += ACA_THREADS) coef[l] = U[ir + (size_t)l * m1];
+                __syncthreads();
+                double ss = 0.0;
+                for (int j = tid; j < m2; j += ACA_THREADS) {
+                    double val = kernel_entry(K, P, r0 + ir, c0 + j);
+                    for (int l = 0; l < r; l++)
+                        val = __fma_rn(-coef[l], V[j + (size_t)l * m2], val);
+                    V[j + (size_t)r * m2] = val;
+                    ss += val * val;
+                }
+                double n2 = block_sum(ss, red);
+                if (sqrt(n2) >= 1.0e-13) { found = true; break; }
+                __syncthreads();
+            }
+            if (!found) break;
+            double best = -1.0;
+            int jr = 0;
+            for (int j = tid; j < m2; j += ACA_THREADS) {
+                double a = fabs(V[j + (size_t)r * m2]);
+                if (better(a, j, best, jr, true)) { best = a; jr = j; }
+            }
+            block_argmax(best, jr, true, reda, redi);
+            const double piv = V[jr + (size_t)r * m2];
+            __syncthreads();
+            for (int j = tid; j < m2; j += ACA_THREADS)
+                V[j + (size_t)r * m2] = V[j + (size_t)r * m2] / piv;
+            for (int l = tid; l < r; l += ACA_THREADS) coef[l] = V[jr + (size_t)l * m2];
+            __syncthreads();
+            for (int i = tid; i < m1; i += ACA_THREADS) {
+                double val = kernel_entry(K, P, r0 + i, c0 + jr);
+                for (int l = 0; l < r; l++) val = __fma_rn(-coef[l], U[i + (size_t)l * m1], val);
+                U[i + (size_t)r * m1] = val;
+            }
+            rank = r + 1;
+            __syncthreads();
+        }
+    } else {
+        const int nwords = (m1 + 31) >> 5;
+        for (int w = tid; w < nwords; w += ACA_THREADS) used[w] = 0u;
+        __syncthreads();
+        double S2 = 0.0;
+        int ir = 0, nused = 0;
+        for (int r = 0; r < kb; r++) {
+            int jr = -1;
+            double piv = 0.0;
+            bool have = false;
+            for (;;) {
+                if (tid == 0) used[ir >> 5] |= 1u << (ir & 31);
+                nused++;
+                for (int l = tid; l < r; l += ACA_THREADS) coef[l] = U[ir + (size_t)l * m1];
+                __syncthreads();
+                double best = -1.0;
+                int bj = 0x7fffffff;
+                for (int j = tid; j < m2; j += ACA_THREADS) {
+                    double val = kernel_entry(K, P, r0 + ir, c0 + j);
+                    for (int l = 0; l < r; l++)
+                        val = __fma_rn(-coef[l], V[j + (size_t)l * m2], val);
+                    V[j + (size_t)r * m2] = val;
+                    double a = fabs(val);
+                    if (better(a, j, best, bj, false)) { best = a; bj = j; }
+                }
+                block_argmax(best, bj, false, reda, redi);
+                if (best > 0.0) {
+                    jr = bj;
+                    have = true;
+                    break;
+                }
+                // zero residual row: the next unused row in index order
+                int cand = 0x7fffffff;
+                for (int i = tid; i < m1; i += ACA_THREADS)
+                    if (!((used[i >> 5] >> (i & 31)) & 1u)) { cand = i; break; }
+                double dummy = 0.0;
+                block_argmax(dummy, cand, false, reda, redi);
+                if (cand == 0x7fffffff) break;
+                ir = cand;
+                __syncthreads();
+            }
+            if (!have) break;
+            piv = V[jr + (size_t)r * m2];
+            __syncthreads();
+            double pv = 0.0;
+            for (int j = tid; j < m2; j += ACA_THREADS) {
+                double v = V[j + (size_t)r * m2] / piv;
+                V[j + (size_t)r * m2] = v;
+                pv += v * v;
+            }
+            for (int l = tid; l < r; l += ACA_THREADS) coef[l] = V[jr + (size_t)l * m2];
+            __syncthreads();
+            double pu = 0.0, bu = -1.0;
+            int bi = 0x7fffffff;
+            for (int i = tid; i < m1; i += ACA_THREADS) {
+                double val = kernel_entry(K, P, r0 + i, c0 + jr);
+                for (int l = 0; l < r; l++) val = __fma_rn(-coef[l], U[i + (size_t)l * m1], val);
+                U[i + (size_t)r * m1] = val;
+                pu += val * val;
+                if (!((used[i >> 5] >> (i & 31)) & 1u)) {
+                    double a = fabs(val);
+                    if (better(a, i, bu, bi, false)) { bu = a; bi = i; }
+                }
+            }
+            double nv2 = block_sum(pv, red);
+            double nu2 = block_sum(pu, red);
+            block_argmax(bu, bi, false, reda, redi);
+            // cross terms sum_l (u_r . U_l)(v_r . V_l), 32 columns at a time
+            double cross = 0.0;
+            for (int l0 = 0; l0 < r; l0 += 32) {
+                int nc = r - l0 < 32 ? r - l0 : 32;
+                double au[32], av[32];
+#pragma unroll
+                for (int c = 0; c < 32; c++) { au[c] = 0.0; av[c] = 0.0; }
+                for (int i = tid; i < m1; i += ACA_THREADS) {
+                    double u = U[i + (size_t)r * m1];
+#pragma unroll
+                    for (int c = 0; c < 32; c++)
+                        if (c < nc) au[c] = __fma_rn(u, U[i + (size_t)(l0 + c) * m1], au[c]);
+                }
+                for (int j = tid; j < m2; j += ACA_THREADS) {
+                    double v = V[j + (size_t)r * m2];
+#pragma unroll
+                    for (int c = 0; c < 32; c++)
+                        if (c < nc) av[c] = __fma_rn(v, V[j + (size_t)(l0 + c) * m2], av[c]);
+                }
+                __syncthreads();
+#pragma unroll
+                for (int c = 0; c < 32; c++) {
+                    double x = au[c], y = av[c];
+#pragma unroll
+                    for (int o = 16; o > 0; o >>= 1) {
+                        x += __shfl_xor_sync(0xffffffffu, x, o);
+                        y += __shfl_xor_sync(0xffffffffu, y, o);
+                    }
+                    au[c] = x;
+                    av[c] = y;
+                }
+                // lane c of each warp holds column c; accumulate warps in order
+                double mu = 0.0, mv = 0.0;
+#pragma unroll
+                for (int c = 0; c < 32; c++)
+                    if ((tid & 31) == c) { mu = au[c]; mv = av[c]; }
+                for (int w = 0; w < ACA_WARPS; w++) {
+                    if ((tid >> 5) == w && (tid & 31) < nc) {
+                        if (w == 0) { dots[0][tid & 31] = mu; dots[1][tid & 31] = mv; }
+                        else { dots[0][tid & 31] += mu; dots[1][tid & 31] += mv; }
+                    }
+                    __syncthreads();
+                }
+                for (int c = 0; c < nc; c++) cross += dots[0][c] * dots[1][c];
+                __syncthreads();
+            }
+            S2 = S2 + 2.0 * cross + nu2 * nv2;
+            rank = r + 1;
+            if (sqrt(nu2 * nv2) <= eps * sqrt(fabs(S2))) break;
+            if (nused >= m1) break;
+            if (bi == 0x7fffffff) break;
+            ir = bi;
+            __syncthreads();
+        }
+    }
+    if (tid == 0) B.rank_out[e] = rank;
+}
+
+// Write the FP64 scratch factors of one block into its final storage:
+// U as tile slices (s_pad x r column-major, padding rows zero) and V^T as r rows
+// of m2p entries (padding zero).
+template <typename T>
+__global__ void k_aca_compact(BlockGeom g, AcaBatch B, const int* tile_r0, const int* tile_s,
+                              const int* tile_pstart, const int* tfirst, const int* tlast,
+                              T* const* ptrU, T* const* ptrV)
+{
+    const int e = blockIdx.x;
+    const int b = B.blocks[e];
+    const int r0 = g.r0[b], m1 = g.m1[b], m2 = g.m2[b];
+    const int r = B.rank_out[e];
+    if (r == 0) return;
+    const double* U = B.U + B.uoff[e];
+    const double* V = B.V + B.voff[e];
+    T* dU = ptrU[b];
+    T* dV = ptrV[b];
+    const int m2p = (m2 + 3) & ~3;
+    for (long long idx = threadIdx.x; idx < (long long)r * m2p; idx += blockDim.x) {
+        int l = (int)(idx / m2p), j = (int)(idx % m2p);
+        dV[idx] = j < m2 ? (T)V[j + (size_t)l * m2] : (T)0;
+    }
+    const int p0 = tile_pstart[tfirst[b]];
+    for (int t = tfirst[b]; t <= tlast[b]; t++) {
+        int s = tile_s[t], sp = (s + 3) & ~3, tr = tile_r0[t] - r0;
+        T* dst = dU + (size_t)(tile_pstart[t] - p0) * r;
+        for (int idx = threadIdx.x; idx < sp * r; idx += blockDim.x) {
+            int l = idx / sp, i = idx % sp;
+            dst[idx] = i < s ? (T)U[(size_t)l * m1 + tr + i] : (T)0;
+        }
+    }
+}
+
+void free_far(hmg_matrix* h)
+{
+    cudaStream_t s = h->stream;
+    for (void* p : h->far_chunks) cudaFree(p);
+    h->far_chunks.clear();
+    dfree(h->rank, s);
+    dfree(h->rank_off, s);
+    dfree(h->ptrU, s);
+    dfree(h->ptrV, s);
+    dfree(h->tbuf, s);
+    h->far_prec = -1;
+    h->desc_near_mode = -1;
+    h->rank_total = h->far_entries = h->far_rows = h->far_stored = 0;
+    h->max_rank = 0;
+    h->h_rank.clear();
+}
+
+hmg_status run_aca(hmg_matrix* h, int k, double eps, int precision)
+{
+    cudaStream_t s = h->stream;
+    hmg_status st = HMG_OK;
+    if (k < 1) { set_error("ACA rank bound k must be >= 1 (got %d)", k); return HMG_ERR_INVALID; }
+    if (k > ACA_KMAX) {
+        set_error("ACA rank bound k=%d exceeds the engine's limit %d", k, ACA_KMAX);
+        return HMG_ERR_UNSUPPORTED;
+    }
+    free_far(h);
+    const int nb = h->nblocks;
+    const size_t esz = precision == HMG_PREC_FP64 ? 8 : 4;
+    std::vector<int> rank(nb, 0);
+    std::vector<void*> pU(nb, nullptr), pV(nb, nullptr);
+    if ((st = dalloc((int**)&h->rank, (size_t)nb, s)) ||
+        (st = dalloc((long long**)&h->rank_off, (size_t)nb + 1, s)) ||
+        (st = dalloc((void***)&h->ptrU, (size_t)nb, s)) ||
+        (st = dalloc((void***)&h->ptrV, (size_t)nb, s)))
+        return st;
+
+    // batches of admissible blocks whose FP64 scratch fits the budget
+    size_t free_b = 0, total_b = 0;
+    HMG_CUDA_TRY(cudaMemGetInfo(&free_b, &total_b));
+    size_t budget = free_b / 4;
+    if (budget > ((size_t)8 << 30)) budget = (size_t)8 << 30;
+    if (budget < ((size_t)64 << 20)) budget = (size_t)64 << 20;
+
+    BlockGeom g{h->blk_r0, h->blk_m1, h->blk_c0, h->blk_m2};
+    PointsView P{};
+    for (int d = 0; d < h->dim; d++) {
+        P.c1[d] = h->zpts[0] + (size_t)d * h->n[0];
+        P.c2[d] = h->zpts[1] + (size_t)d * h->n[1];
+    }
+    P.n1 = h->n[0];
+    P.n2 = h->n[1];
+
+    int bstart = h->ndense;
+    while (bstart < nb) {
+        std::vector<int> idx;
+        std::vector<long long> uo, vo;
+        long long us = 0, vs = 0;
+        int maxm1 = 1;
+        int b = bstart;
+        for (; b < nb; b++) {
+            int m1 = h->h_m1[b], m2 = h->h_m2[b];
+            int kb = std::min(k, std::min(m1, m2));
+            long long need = ((long long)m1 + m2) * kb * 8;
+            if (!idx.empty() && (us + vs) * 8 + need > (long long)budget) break;
+            idx.push_back(b);
+            uo.push_back(us);
+            vo.push_back(vs);
+            us += (long long)m1 * kb;
+            vs += (long long)m2 * kb;
+            maxm1 = std::max(maxm1, m1);
+        }
+        bstart = b;
+        int ne = (int)idx.size();
+        int* d_idx = nullptr;
+        long long *d_uo = nullptr, *d_vo = nullptr;
+        double *dU = nullptr, *dV = nullptr;
+        int* d_rank = nullptr;
+        if ((st = dalloc(&d_idx, ne, s)) || (st = dalloc(&d_uo, ne, s)) || (st = dalloc(&d_vo, ne, s)) ||
+            (st = dalloc(&dU, (size_t)us, s)) || (st = dalloc(&dV, (size_t)vs, s)) ||
+            (st = dalloc(&d_rank, ne, s))) {
+            dfree(d_idx, s); dfree(d_uo, s); dfree(d_vo, s); dfree(dU, s); dfree(dV, s);
+            dfree(d_rank, s);
+            return st;
+        }
+        HMG_CUDA_TRY(cudaMemcpyAsync(d_idx, idx.data(), sizeof(int) * ne, cudaMemcpyHostToDevice, s));
+        HMG_CUDA_TRY(cudaMemcpyAsync(d_uo, uo.data(), sizeof(long long) * ne, cudaMemcpyHostToDevice, s));
+        HMG_CUDA_TRY(cudaMemcpyAsync(d_vo, vo.data(), sizeof(long long) * ne, cudaMemcpyHostToDevice, s));
+        AcaBatch B{d_idx, d_uo, d_vo, dU, dV, d_rank};
+        size_t dyn = eps > 0.0 ? (size_t)((maxm1 + 31) / 32) * 4 : 0;
+        if (dyn > 200 * 1024) {
+            set_error("block with %d rows exceeds the adaptive ACA's row-mask capacity", maxm1);
+            return HMG_ERR_UNSUPPORTED;
+        }
+        if (dyn > 48 * 1024)
+            HMG_CUDA_TRY(cudaFuncSetAttribute(k_aca, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                              (int)dyn));
+        k_aca<<<ne, ACA_THREADS, dyn, s>>>(g, h->kspec, P, B, k, eps);
+        HMG_LAUNCH_CHECK();
+        std::vector<int> br(ne);
+        HMG_CUDA_TRY(cudaMemcpyAsync(br.data(), d_rank, sizeof(int) * ne, cudaMemcpyDeviceToHost, s));
+        HMG_CUDA_TRY(cudaStreamSynchronize(s));
+        // final storage of this batch
+        long long bytes = 0;
+        std::vector<long long> ofsU(ne), ofsV(ne);
+        for (int e = 0; e < ne; e++) {
+            int bb = idx[e], r = br[e];
+            rank[bb] = r;
+            long long rows_p = h->h_tile_pstart[h->h_blk_tlast[bb] + 1] -
+                               h->h_tile_pstart[h->h_blk_tfirst[bb]];
+            ofsU[e] = bytes;
+            bytes += rows_p * r * (long long)esz;
+            bytes = (bytes + 255) & ~255ll;
+            ofsV[e] = bytes;
+            bytes += (long long)r * ((h->h_m2[bb] + 3) & ~3) * (long long)esz;
+            bytes = (bytes + 255) & ~255ll;
+        }
+        char* chunk = nullptr;
+        if (bytes > 0) {
+            cudaError_t ce = cudaMalloc((void**)&chunk, (size_t)bytes);
+            if (ce != cudaSuccess) {
+                cudaGetLastError();
+                set_error("allocating %lld bytes of low-rank factors failed: %s", bytes,
+                          cudaGetErrorString(ce));
+                return ce == cudaErrorMemoryAllocation ? HMG_ERR_NOMEM : HMG_ERR_CUDA;
+            }
+            h->far_chunks.push_back(chunk);
+            h->far_stored += bytes;
+            for (int e = 0; e < ne; e++) {
+                pU[idx[e]] = chunk + ofsU[e];
+                pV[idx[e]] = chunk + ofsV[e];
+            }
+            // the batch is a contiguous block range
+            HMG_CUDA_TRY(cudaMemcpyAsync(h->ptrU + idx[0], pU.data() + idx[0], sizeof(void*) * ne,
+                                         cudaMemcpyHostToDevice, s));
+            HMG_CUDA_TRY(cudaMemcpyAsync(h->ptrV + idx[0], pV.data() + idx[0], sizeof(void*) * ne,
+                                         cudaMemcpyHostToDevice, s));
+            if (precision == HMG_PREC_FP64)
+                k_aca_compact<double><<<ne, 256, 0, s>>>(g, B, h->tile_r0, h->tile_s, h->tile_pstart,
+                                                         h->blk_tfirst, h->blk_tlast,
+                                                         (double* const*)h->ptrU, (double* const*)h->ptrV);
+            else
+                k_aca_compact<float><<<ne, 256, 0, s>>>(g, B, h->tile_r0, h->tile_s, h->tile_pstart,
+                                                        h->blk_tfirst, h->blk_tlast,
+                                                        (float* const*)h->ptrU, (float* const*)h->ptrV);
+            HMG_LAUNCH_CHECK();
+        }
+        HMG_CUDA_TRY(cudaStreamSynchronize(s));
+        dfree(d_idx, s); dfree(d_uo, s); dfree(d_vo, s); dfree(dU, s); dfree(dV, s);
+        dfree(d_rank, s);
+    }
+
+    // ranks and their offsets
+    std::vector<long long> roff(nb + 1, 0);
+    h->far_entries = h->far_rows = 0;
+    h->max_rank = 0;
+    for (int b = 0; b < nb; b++) {
+        roff[b + 1] = roff[b] + rank[b];
+        if (h->h_type[b] == HMG_WT_ACA) {
+            h->far_entries += (long long)(h->h_m1[b] + h->h_m2[b]) * rank[b];
+            h->far_rows += h->h_m1[b] + h->h_m2[b];
+            h->max_rank = std::max(h->max_rank, rank[b]);
+        }
+    }
+    h->rank_total = roff[nb];
+    HMG_CUDA_TRY(cudaMemcpyAsync(h->rank, rank.data(), sizeof(int) * nb, cudaMemcpyHostToDevice, s));
+    HMG_CUDA_TRY(cudaMemcpyAsync(h->rank_off, roff.data(), sizeof(long long) * (nb + 1), cudaMemcpyHostToDevice, s));
+    if ((st = dalloc((char**)&h->tbuf, (size_t)(h->rank_total > 0 ? h->rank_total : 1) * 8, s)))
+        return st;
+    HMG_CUDA_TRY(cudaStreamSynchronize(s));
+    h->h_rank = rank;
+    h->far_prec = precision;
+    h->aca_k = k;
+    h->aca_eps = eps;
+    return HMG_OK;
+}
+
+}  // namespace hmg

@@ -1,0 +1,760 @@
+// api.cu -- the C ABI (include/hmg.h) and the reference's entry points
+// (include/hmglib.h, include/kernel_system_assembler.h) on top of it.
+#include <cmath>
+#include <cstdlib>
+#include <cstring>
+#include <new>
+
+#include "../../include/hmglib.h"
+#include "../../include/kernel_system_assembler.h"
+#include "hmg_matrix.cuh"
+
+using namespace hmg;
+
+#define HMG_REQUIRE(cond, code, ...)      \
+    do {                                  \
+        if (!(cond)) {                    \
+            set_error(__VA_ARGS__);       \
+            return code;                  \
+        }                                 \
+    } while (0)
+
+extern "C" {
+
+const char* hmg_last_error(void) { return hmg::last_error(); }
+
+int hmg_version(void) { return 100; }
+
+static void free_matrix_buffers(hmg_matrix* h)
+{
+    cudaStream_t s = h->stream;
+    free_far(h);
+    free_near(h);
+    free_tree(h);
+    for (int i = 0; i < 2; i++) {
+        dfree(h->pts[i], s); dfree(h->zpts[i], s); dfree(h->codes[i], s);
+        dfree(h->perm[i], s); dfree(h->iperm[i], s);
+    }
+    dfree(h->xs64, s); dfree(h->xs32, s);
+    dfree(h->pair_desc, s);
+    dfree(h->k1_units, s);
+    dfree(h->dev_x, s); dfree(h->dev_y, s);
+    if (h->host_x) cudaFreeHost(h->host_x);
+    if (h->host_y) cudaFreeHost(h->host_y);
+    h->host_x = h->host_y = nullptr;
+}
+
+hmg_status hmg_create(hmg_matrix** out, int n1, int n2, int dim, int bits, void* stream)
+{
+    HMG_REQUIRE(out, HMG_ERR_INVALID, "hmg_create: out is NULL");
+    *out = nullptr;
+    HMG_REQUIRE(n1 >= 1 && n2 >= 1, HMG_ERR_INVALID, "hmg_create: point counts must be >= 1 (got %d, %d)", n1, n2);
+    HMG_REQUIRE(dim == 2 || dim == 3, HMG_ERR_UNSUPPORTED,
+                "hmg_create: dim must be 2 or 3 (got %d)", dim);
+    if (bits == 0) bits = dim == 2 ? 32 : 20;
+    HMG_REQUIRE(bits >= 1 && bits * dim <= 64, HMG_ERR_INVALID, "hmg_create: bits*dim must be <= 64");
+    hmg_matrix* h = new (std::nothrow) hmg_matrix();
+    HMG_REQUIRE(h, HMG_ERR_NOMEM, "hmg_create: out of host memory");
+    h->n[0] = n1;
+    h->n[1] = n2;
+    h->dim = dim;
+    h->bits = bits;
+    h->stream = (cudaStream_t)stream;
+    cudaError_t e = cudaGetDevice(&h->device);
+    if (e != cudaSuccess) {
+        set_error("hmg_create: no CUDA device: %s", cudaGetErrorString(e));
+        delete h;
+        return HMG_ERR_CUDA;
+    }
+    hmg_status st = HMG_OK;
+    for (int i = 0; i < 2 && !st; i++) {
+        size_t n = (size_t)h->n[i];
+        if ((st = dalloc(&h->pts[i], n * dim, h->stream)) || (st = dalloc(&h->zpts[i], n * dim, h->stream)) ||
+            (st = dalloc(&h->codes[i], n, h->stream)) || (st = dalloc(&h->perm[i], n, h->stream)) ||
+            (st = dalloc(&h->iperm[i], n, h->stream)))
+            break;
+    }
+    if (!st && cudaStreamSynchronize(h->stream) != cudaSuccess) {
+        set_error("hmg_create: stream synchronisation failed");
+        st = HMG_ERR_CUDA;
+    }
+    if (st) {
+        free_matrix_buffers(h);
+        delete h;
+        return st;
+    }
+    *out = h;
+    return HMG_OK;
+}
+
+static void invalidate_setup(hmg_matrix* h)
+{
+    free_far(h);
+    free_near(h);
+    free_tree(h);
+}
+
+hmg_status hmg_set_points(hmg_matrix* h, int set, const double* coords, int on_device)
+{
+    HMG_REQUIRE(h && coords, HMG_ERR_INVALID, "hmg_set_points: NULL argument");
+    HMG_REQUIRE(set == 0 || set == 1, HMG_ERR_INVALID, "hmg_set_points: set must be 0 or 1");
+    invalidate_setup(h);
+    size_t bytes = sizeof(double) * (size_t)h->n[set] * h->dim;
+    HMG_CUDA_TRY(cudaMemcpyAsync(h->pts[set], coords, bytes,
+                                 on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, h->stream));
+    HMG_CUDA_TRY(cudaStreamSynchronize(h->stream));
+    h->points_set[set] = true;
+    return HMG_OK;
+}
+
+hmg_status hmg_setup(hmg_matrix* h, double eta, int c_leaf, int max_level, int root_level1,
+                     int root_level2, int rule)
+{
+    HMG_REQUIRE(h, HMG_ERR_INVALID, "hmg_setup: NULL handle");
+    HMG_REQUIRE(h->points_set[0] && h->points_set[1], HMG_ERR_STATE, "hmg_setup: points not set");
+    HMG_REQUIRE(eta >= 0.0 && std::isfinite(eta), HMG_ERR_INVALID, "hmg_setup: eta must be finite and >= 0");
+    HMG_REQUIRE(c_leaf >= 1, HMG_ERR_INVALID, "hmg_setup: c_leaf must be >= 1 (got %d)", c_leaf);
+    HMG_REQUIRE(max_level >= 1, HMG_ERR_INVALID, "hmg_setup: max_level must be >= 1");
+    HMG_REQUIRE(rule == HMG_ADMISSIBLE_MAX || rule == HMG_ADMISSIBLE_MIN, HMG_ERR_INVALID,
+                "hmg_setup: unknown admissibility rule %d", rule);
+    HMG_REQUIRE(root_level1 == root_level2, HMG_ERR_UNSUPPORTED,
+                "hmg_setup: root levels must be equal (got %d, %d)", root_level1, root_level2);
+    invalidate_setup(h);
+    h->eta = eta;
+    h->c_leaf = c_leaf;
+    h->max_level = max_level;
+    h->rule = rule;
+    hmg_status st = setup_tree(h);
+    if (!st) st = build_tiles(h);
+    if (st) {
+        invalidate_setup(h);
+        return st;
+    }
+    h->setup_done = true;
+    return HMG_OK;
+}
+
+hmg_status hmg_set_kernel(hmg_matrix* h, int kind, double param, double regularization)
+{
+    HMG_REQUIRE(h, HMG_ERR_INVALID, "hmg_set_kernel: NULL handle");
+    HMG_REQUIRE(kind >= HMG_KERNEL_GAUSSIAN_REF && kind <= HMG_KERNEL_MATERN32, HMG_ERR_INVALID,
+                "hmg_set_kernel: unknown kernel kind %d", kind);
+    HMG_REQUIRE(std::isfinite(regularization), HMG_ERR_INVALID, "hmg_set_kernel: regularization not finite");
+    KernelSpec k{};
+    k.kind = kind;
+    k.dim = h->dim;
+    k.reg = regularization;
+    if (kind == HMG_KERNEL_GAUSSIAN || kind == HMG_KERNEL_MATERN32) {
+        HMG_REQUIRE(param > 0.0 && std::isfinite(param), HMG_ERR_INVALID,
+                    "hmg_set_kernel: parameter must be > 0 (got %g)", param);
+        k.param = kind == HMG_KERNEL_GAUSSIAN ? 1.0 / param : std::sqrt(3.0) / param;
+    }
+    k.matern_ref_denom = std::pow(2.0, (double)h->dim / 2.0) * std::tgamma(1.0 + (double)h->dim / 2.0);
+    bool same = h->kernel_set && memcmp(&k, &h->kspec, sizeof(k)) == 0;
+    if (!same) {
+        free_far(h);
+        free_near(h);
+    }
+    h->kspec = k;
+    h->kernel_set = true;
+    return HMG_OK;
+}
+
+hmg_status hmg_precompute_aca(hmg_matrix* h, int k, double eps, int precision)
+{
+    HMG_REQUIRE(h, HMG_ERR_INVALID, "hmg_precompute_aca: NULL handle");
+    HMG_REQUIRE(h->setup_done, HMG_ERR_STATE, "hmg_precompute_aca: call hmg_setup first");
+    HMG_REQUIRE(h->kernel_set, HMG_ERR_STATE, "hmg_precompute_aca: call hmg_set_kernel first");
+    HMG_REQUIRE(precision == HMG_PREC_FP64 || precision == HMG_PREC_FP32, HMG_ERR_INVALID,
+                "hmg_precompute_aca: unknown precision %d", precision);
+    HMG_REQUIRE(std::isfinite(eps), HMG_ERR_INVALID, "hmg_precompute_aca: eps not finite");
+    hmg_status st = run_aca(h, k, eps, precision);
+    if (st) free_far(h);
+    return st;
+}
+
+hmg_status hmg_precompute_dense(hmg_matrix* h, int precision)
+{
+    HMG_REQUIRE(h, HMG_ERR_INVALID, "hmg_precompute_dense: NULL handle");
+    HMG_REQUIRE(h->setup_done, HMG_ERR_STATE, "hmg_precompute_dense: call hmg_setup first");
+    HMG_REQUIRE(h->kernel_set, HMG_ERR_STATE, "hmg_precompute_dense: call hmg_set_kernel first");
+    HMG_REQUIRE(precision == HMG_PREC_FP64 || precision == HMG_PREC_FP32, HMG_ERR_INVALID,
+                "hmg_precompute_dense: unknown precision %d", precision);
+    hmg_status st = fill_near(h, precision);
+    if (st) free_near(h);
+    return st;
+}
+
+hmg_status hmg_set_near_mode(hmg_matrix* h, int mode)
+{
+    HMG_REQUIRE(h, HMG_ERR_INVALID, "hmg_set_near_mode: NULL handle");
+    HMG_REQUIRE(mode == HMG_NEAR_STORED || mode == HMG_NEAR_ONTHEFLY, HMG_ERR_INVALID,
+                "hmg_set_near_mode: unknown mode %d", mode);
+    HMG_REQUIRE(mode != HMG_NEAR_STORED || h->near_prec >= 0, HMG_ERR_STATE,
+                "hmg_set_near_mode: near field not stored (call hmg_precompute_dense)");
+    h->near_mode = mode;
+    return HMG_OK;
+}
+
+static hmg_status check_ready(hmg_matrix* h, const char* who)
+{
+    HMG_REQUIRE(h->setup_done, HMG_ERR_STATE, "%s: call hmg_setup first", who);
+    HMG_REQUIRE(h->kernel_set, HMG_ERR_STATE, "%s: call hmg_set_kernel first", who);
+    HMG_REQUIRE(h->naca == 0 || h->far_prec >= 0, HMG_ERR_STATE, "%s: call hmg_precompute_aca first", who);
+    return HMG_OK;
+}
+
+hmg_status hmg_matvec(hmg_matrix* h, const double* x, double* y)
+{
+    HMG_REQUIRE(h && x && y, HMG_ERR_INVALID, "hmg_matvec: NULL argument");
+    hmg_status st = check_ready(h, "hmg_matvec");
+    if (st) return st;
+    return matvec_device(h, x, y);
+}
+
+hmg_status hmg_matvec_host(hmg_matrix* h, const double* x_host, double* y_host)
+{
+    HMG_REQUIRE(h && x_host && y_host, HMG_ERR_INVALID, "hmg_matvec_host: NULL argument");
+    hmg_status st = check_ready(h, "hmg_matvec_host");
+    if (st) return st;
+    cudaStream_t s = h->stream;
+    if (!h->host_x) {
+        HMG_CUDA_TRY(cudaMallocHost((void**)&h->host_x, sizeof(double) * h->n[1]));
+        HMG_CUDA_TRY(cudaMallocHost((void**)&h->host_y, sizeof(double) * h->n[0]));
+        if ((st = dalloc(&h->dev_x, (size_t)h->n[1], s)) || (st = dalloc(&h->dev_y, (size_t)h->n[0], s)))
+            return st;
+    }
+    memcpy(h->host_x, x_host, sizeof(double) * h->n[1]);
+    HMG_CUDA_TRY(cudaMemcpyAsync(h->dev_x, h->host_x, sizeof(double) * h->n[1], cudaMemcpyHostToDevice, s));
+    if ((st = matvec_device(h, h->dev_x, h->dev_y))) return st;
+    HMG_CUDA_TRY(cudaMemcpyAsync(h->host_y, h->dev_y, sizeof(double) * h->n[0], cudaMemcpyDeviceToHost, s));
+    HMG_CUDA_TRY(cudaStreamSynchronize(s));
+    memcpy(y_host, h->host_y, sizeof(double) * h->n[0]);
+    return HMG_OK;
+}
+
+hmg_status hmg_full_matvec(hmg_matrix* h, const double* x, double* y)
+{
+    HMG_REQUIRE(h && x && y, HMG_ERR_INVALID, "hmg_full_matvec: NULL argument");
+    HMG_REQUIRE(h->setup_done, HMG_ERR_STATE, "hmg_full_matvec: call hmg_setup first");
+    HMG_REQUIRE(h->kernel_set, HMG_ERR_STATE, "hmg_full_matvec: call hmg_set_kernel first");
+    return direct_matvec(h, x, nullptr, 0, y);
+}
+
+hmg_status hmg_full_matvec_rows(hmg_matrix* h, const double* x, const int* rows, int nrows, double* y)
+{
+    HMG_REQUIRE(h && x && rows && y, HMG_ERR_INVALID, "hmg_full_matvec_rows: NULL argument");
+    HMG_REQUIRE(nrows >= 0, HMG_ERR_INVALID, "hmg_full_matvec_rows: nrows < 0");
+    HMG_REQUIRE(h->setup_done, HMG_ERR_STATE, "hmg_full_matvec_rows: call hmg_setup first");
+    HMG_REQUIRE(h->kernel_set, HMG_ERR_STATE, "hmg_full_matvec_rows: call hmg_set_kernel first");
+    return direct_matvec(h, x, rows, nrows, y);
+}
+
+hmg_status hmg_gaussian_rhs(hmg_matrix* h, double* b)
+{
+    HMG_REQUIRE(h && b, HMG_ERR_INVALID, "hmg_gaussian_rhs: NULL argument");
+    HMG_REQUIRE(h->points_set[0], HMG_ERR_STATE, "hmg_gaussian_rhs: points not set");
+    return gaussian_rhs(h, b);
+}
+
+hmg_status hmg_synchronize(hmg_matrix* h)
+{
+    HMG_REQUIRE(h, HMG_ERR_INVALID, "hmg_synchronize: NULL handle");
+    HMG_CUDA_TRY(cudaStreamSynchronize(h->stream));
+    return HMG_OK;
+}
+
+hmg_status hmg_set_profiling(hmg_matrix* h, int on)
+{
+    HMG_REQUIRE(h, HMG_ERR_INVALID, "hmg_set_profiling: NULL handle");
+    if (on && !h->ev[0])
+        for (int i = 0; i < 4; i++) HMG_CUDA_TRY(cudaEventCreate(&h->ev[i]));
+    h->profiling = on != 0;
+    return HMG_OK;
+}
+
+hmg_status hmg_get_profile(hmg_matrix* h, double* ms4)
+{
+    HMG_REQUIRE(h && ms4, HMG_ERR_INVALID, "hmg_get_profile: NULL argument");
+    HMG_REQUIRE(h->ev[0], HMG_ERR_STATE, "hmg_get_profile: profiling was never enabled");
+    HMG_CUDA_TRY(cudaEventSynchronize(h->ev[3]));
+    float a = 0.f, b = 0.f, c = 0.f, t = 0.f;
+    HMG_CUDA_TRY(cudaEventElapsedTime(&a, h->ev[0], h->ev[1]));
+    HMG_CUDA_TRY(cudaEventElapsedTime(&b, h->ev[1], h->ev[2]));
+    HMG_CUDA_TRY(cudaEventElapsedTime(&c, h->ev[2], h->ev[3]));
+    HMG_CUDA_TRY(cudaEventElapsedTime(&t, h->ev[0], h->ev[3]));
+    ms4[0] = a; ms4[1] = b; ms4[2] = c; ms4[3] = t;
+    return HMG_OK;
+}
+
+hmg_status hmg_destroy(hmg_matrix* h)
+{
+    if (!h) return HMG_OK;
+    cudaStreamSynchronize(h->stream);
+    for (int i = 0; i < 4; i++)
+        if (h->ev[i]) cudaEventDestroy(h->ev[i]);
+    free_matrix_buffers(h);
+    cudaStreamSynchronize(h->stream);
+    delete h;
+    return HMG_OK;
+}
+
+hmg_status hmg_get_info(hmg_matrix* h, hmg_info* info)
+{
+    HMG_REQUIRE(h && info, HMG_ERR_INVALID, "hmg_get_info: NULL argument");
+    memset(info, 0, sizeof(*info));
+    info->n1 = h->n[0];
+    info->n2 = h->n[1];
+    info->dim = h->dim;
+    info->bits = h->bits;
+    info->block_count = h->nblocks;
+    info->dense_count = h->ndense;
+    info->aca_count = h->naca;
+    info->levels = h->levels;
+    info->tile_count = h->ntiles;
+    info->max_rank = h->max_rank;
+    long long ne = 0;
+    for (int b = 0; b < h->ndense; b++) ne += (long long)h->h_m1[b] * h->h_m2[b];
+    info->near_entries = ne;
+    info->far_entries = h->far_entries;
+    long long fr = 0;
+    for (int b = h->ndense; b < h->nblocks; b++) fr += h->h_m1[b] + h->h_m2[b];
+    info->far_rows = fr;
+    int nes = h->near_prec == HMG_PREC_FP64 ? 8 : 4;
+    int fes = h->far_prec == HMG_PREC_FP64 ? 8 : 4;
+    info->near_bytes = h->near_prec >= 0 ? h->near_stored * nes : 0;
+    info->far_bytes = h->far_stored;
+    long long mb = h->far_prec >= 0 ? h->far_entries * fes : 0;
+    if (h->near_mode == HMG_NEAR_STORED && h->near_prec >= 0) mb += ne * nes;
+    mb += 8ll * (h->n[0] + h->n[1]);
+    info->matvec_bytes = mb;
+    info->near_precision = h->near_prec;
+    info->far_precision = h->far_prec;
+    info->near_mode = h->near_mode;
+    return HMG_OK;
+}
+
+hmg_status hmg_get_codes(hmg_matrix* h, int set, uint64_t* codes)
+{
+    HMG_REQUIRE(h && codes && (set == 0 || set == 1), HMG_ERR_INVALID, "hmg_get_codes: bad argument");
+    HMG_REQUIRE(h->setup_done, HMG_ERR_STATE, "hmg_get_codes: call hmg_setup first");
+    HMG_CUDA_TRY(cudaMemcpyAsync(codes, h->codes[set], sizeof(uint64_t) * h->n[set], cudaMemcpyDeviceToHost, h->stream));
+    HMG_CUDA_TRY(cudaStreamSynchronize(h->stream));
+    return HMG_OK;
+}
+
+hmg_status hmg_get_order(hmg_matrix* h, int set, int64_t* order)
+{
+    HMG_REQUIRE(h && order && (set == 0 || set == 1), HMG_ERR_INVALID, "hmg_get_order: bad argument");
+    HMG_REQUIRE(h->setup_done, HMG_ERR_STATE, "hmg_get_order: call hmg_setup first");
+    std::vector<int> p(h->n[set]);
+    HMG_CUDA_TRY(cudaMemcpyAsync(p.data(), h->perm[set], sizeof(int) * h->n[set], cudaMemcpyDeviceToHost, h->stream));
+    HMG_CUDA_TRY(cudaStreamSynchronize(h->stream));
+    for (int i = 0; i < h->n[set]; i++) order[i] = p[i];
+    return HMG_OK;
+}
+
+hmg_status hmg_get_points(hmg_matrix* h, int set, double* coords)
+{
+    HMG_REQUIRE(h && coords && (set == 0 || set == 1), HMG_ERR_INVALID, "hmg_get_points: bad argument");
+    HMG_REQUIRE(h->setup_done, HMG_ERR_STATE, "hmg_get_points: call hmg_setup first");
+    HMG_CUDA_TRY(cudaMemcpyAsync(coords, h->zpts[set], sizeof(double) * h->n[set] * h->dim,
+                                 cudaMemcpyDeviceToHost, h->stream));
+    HMG_CUDA_TRY(cudaStreamSynchronize(h->stream));
+    return HMG_OK;
+}
+
+hmg_status hmg_get_blocks(hmg_matrix* h, int* s1l, int* s1u, int* s2l, int* s2u, int* type)
+{
+    HMG_REQUIRE(h, HMG_ERR_INVALID, "hmg_get_blocks: NULL handle");
+    HMG_REQUIRE(h->setup_done, HMG_ERR_STATE, "hmg_get_blocks: call hmg_setup first");
+    for (int b = 0; b < h->nblocks; b++) {
+        if (s1l) s1l[b] = h->h_r0[b];
+        if (s1u) s1u[b] = h->h_r0[b] + h->h_m1[b] - 1;
+        if (s2l) s2l[b] = h->h_c0[b];
+        if (s2u) s2u[b] = h->h_c0[b] + h->h_m2[b] - 1;
+        if (type) type[b] = h->h_type[b];
+    }
+    return HMG_OK;
+}
+
+hmg_status hmg_get_ranks(hmg_matrix* h, int* ranks)
+{
+    HMG_REQUIRE(h && ranks, HMG_ERR_INVALID, "hmg_get_ranks: NULL argument");
+    HMG_REQUIRE(h->far_prec >= 0 || h->naca == 0, HMG_ERR_STATE, "hmg_get_ranks: no factors");
+    for (int b = 0; b < h->nblocks; b++) ranks[b] = h->h_rank.empty() ? 0 : h->h_rank[b];
+    return HMG_OK;
+}
+
+hmg_status hmg_get_factors(hmg_matrix* h, int block, double* U, double* V)
+{
+    HMG_REQUIRE(h && U && V, HMG_ERR_INVALID, "hmg_get_factors: NULL argument");
+    HMG_REQUIRE(h->far_prec >= 0, HMG_ERR_STATE, "hmg_get_factors: no factors");
+    HMG_REQUIRE(block >= h->ndense && block < h->nblocks, HMG_ERR_INVALID,
+                "hmg_get_factors: block %d is not an admissible block", block);
+    const int r = h->h_rank[block], m1 = h->h_m1[block], m2 = h->h_m2[block];
+    if (r == 0) return HMG_OK;
+    const int m2p = (m2 + 3) & ~3;
+    const int esz = h->far_prec == HMG_PREC_FP64 ? 8 : 4;
+    void* pu = nullptr;
+    void* pv = nullptr;
+    HMG_CUDA_TRY(cudaMemcpy(&pu, h->ptrU + block, sizeof(void*), cudaMemcpyDeviceToHost));
+    HMG_CUDA_TRY(cudaMemcpy(&pv, h->ptrV + block, sizeof(void*), cudaMemcpyDeviceToHost));
+    const int tf = h->h_blk_tfirst[block], tl = h->h_blk_tlast[block];
+    const int rows_p = h->h_tile_pstart[tl + 1] - h->h_tile_pstart[tf];
+    std::vector<char> hu((size_t)rows_p * r * esz), hv((size_t)r * m2p * esz);
+    HMG_CUDA_TRY(cudaMemcpy(hu.data(), pu, hu.size(), cudaMemcpyDeviceToHost));
+    HMG_CUDA_TRY(cudaMemcpy(hv.data(), pv, hv.size(), cudaMemcpyDeviceToHost));
+    auto val = [&](const std::vector<char>& buf, size_t idx) -> double {
+        return esz == 8 ? ((const double*)buf.data())[idx] : (double)((const float*)buf.data())[idx];
+    };
+    for (int l = 0; l < r; l++)
+        for (int j = 0; j < m2; j++) V[(size_t)l * m2 + j] = val(hv, (size_t)l * m2p + j);
+    // tile slices: rows of tile t at pstart[t]-pstart[tf], column-major with s_pad rows
+    std::vector<int> tr0(h->ntiles), ts(h->ntiles);
+    HMG_CUDA_TRY(cudaMemcpy(tr0.data() + tf, h->tile_r0 + tf, sizeof(int) * (tl - tf + 1), cudaMemcpyDeviceToHost));
+    HMG_CUDA_TRY(cudaMemcpy(ts.data() + tf, h->tile_s + tf, sizeof(int) * (tl - tf + 1), cudaMemcpyDeviceToHost));
+    const int r0 = h->h_r0[block];
+    for (int t = tf; t <= tl; t++) {
+        const int sp = (ts[t] + 3) & ~3;
+        const size_t base = (size_t)(h->h_tile_pstart[t] - h->h_tile_pstart[tf]) * r;
+        for (int l = 0; l < r; l++)
+            for (int i = 0; i < ts[t]; i++)
+                U[(size_t)l * m1 + (tr0[t] - r0) + i] = val(hu, base + (size_t)l * sp + i);
+    }
+    return HMG_OK;
+}
+
+hmg_status hmg_radix_sort_u64(uint64_t* keys, uint32_t* values, int n, int key_bits, void* stream)
+{
+    HMG_REQUIRE(n >= 0, HMG_ERR_INVALID, "hmg_radix_sort_u64: n < 0");
+    HMG_REQUIRE(n == 0 || (keys && values), HMG_ERR_INVALID, "hmg_radix_sort_u64: NULL argument");
+    return radix_sort_pairs(keys, values, n, key_bits, (cudaStream_t)stream);
+}
+
+hmg_status hmg_morton_codes(const double* coords, int n, int dim, int bits, uint64_t* codes, void* stream)
+{
+    HMG_REQUIRE(n >= 0 && dim >= 1, HMG_ERR_INVALID, "hmg_morton_codes: bad size");
+    HMG_REQUIRE(n == 0 || (coords && codes), HMG_ERR_INVALID, "hmg_morton_codes: NULL argument");
+    return morton_codes(coords, n, dim, bits, codes, (cudaStream_t)stream);
+}
+
+// ===========================================================================
+// The reference's entry points (include/hmglib.h)
+// ===========================================================================
+static void legacy_fail(const char* who, hmg_status st)
+{
+    fprintf(stderr, "hmglib: %s failed (status %d): %s\n", who, (int)st, hmg::last_error());
+}
+
+static hmg_matrix* legacy_handle(struct h_matrix_data* data) { return (hmg_matrix*)data->magma_queue; }
+
+__global__ void k_fill_work_items(const int* r0, const int* m1, const int* c0, const int* m2,
+                                  const int* type, int nb, const double* z1, int n1, const double* z2,
+                                  int n2, int dim, struct work_item* out)
+{
+    int b = blockIdx.x;
+    if (b >= nb) return;
+    __shared__ double red[4][3][4];
+    int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    double vals[4][3];
+    for (int d = 0; d < dim; d++) {
+        double lo1 = 1e308, hi1 = -1e308, lo2 = 1e308, hi2 = -1e308;
+        for (int i = threadIdx.x; i < m1[b]; i += blockDim.x) {
+            double v = z1[(size_t)d * n1 + r0[b] + i];
+            lo1 = fmin(lo1, v); hi1 = fmax(hi1, v);
+        }
+        for (int i = threadIdx.x; i < m2[b]; i += blockDim.x) {
+            double v = z2[(size_t)d * n2 + c0[b] + i];
+            lo2 = fmin(lo2, v); hi2 = fmax(hi2, v);
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+            lo1 = fmin(lo1, __shfl_xor_sync(0xffffffffu, lo1, o));
+            hi1 = fmax(hi1, __shfl_xor_sync(0xffffffffu, hi1, o));
+            lo2 = fmin(lo2, __shfl_xor_sync(0xffffffffu, lo2, o));
+            hi2 = fmax(hi2, __shfl_xor_sync(0xffffffffu, hi2, o));
+        }
+        vals[0][d] = lo1; vals[1][d] = hi1; vals[2][d] = lo2; vals[3][d] = hi2;
+        if (lane == 0) { red[0][d][warp] = lo1; red[1][d][warp] = hi1; red[2][d][warp] = lo2; red[3][d][warp] = hi2; }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        struct work_item w;
+        memset(&w, 0, sizeof(w));
+        w.set1_l = r0[b]; w.set1_u = r0[b] + m1[b] - 1;
+        w.set2_l = c0[b]; w.set2_u = c0[b] + m2[b] - 1;
+        w.work_type = type[b];
+        w.dim = dim;
+        for (int d = 0; d < dim; d++) {
+            double a = red[0][d][0], bb = red[1][d][0], c = red[2][d][0], e = red[3][d][0];
+            for (int k = 1; k < 4; k++) {
+                a = fmin(a, red[0][d][k]); bb = fmax(bb, red[1][d][k]);
+                c = fmin(c, red[2][d][k]); e = fmax(e, red[3][d][k]);
+            }
+            w.min1[d] = a; w.max1[d] = bb; w.min2[d] = c; w.max2[d] = e;
+        }
+        out[b] = w;
+    }
+    (void)vals;
+}
+
+__global__ void k_perm_to_u64(const int* perm, int n, uint64_t* order, unsigned int* ids)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    order[i] = (uint64_t)perm[i];
+    ids[i] = (unsigned int)perm[i];
+}
+
+void init_h_matrix_data(struct h_matrix_data* data, int point_count[2], int dim, int bits)
+{
+    memset(data, 0, sizeof(*data));
+    hmg_matrix* h = nullptr;
+    hmg_status st = hmg_create(&h, point_count[0], point_count[1], dim, bits, nullptr);
+    if (st) { legacy_fail("init_h_matrix_data", st); return; }
+    data->dim = dim;
+    data->bits = h->bits;
+    data->magma_queue = h;
+    data->max_level = 50;
+    for (int i = 0; i < 2; i++) {
+        int n = point_count[i];
+        data->point_count[i] = n;
+        data->coords_d[i] = new double*[dim];
+        for (int d = 0; d < dim; d++) data->coords_d[i][d] = h->pts[i] + (size_t)d * n;
+        cudaMalloc((void**)&data->point_ids_d[i], sizeof(unsigned int) * n);
+        cudaMalloc((void**)&data->max_per_dim_d[i], sizeof(double) * dim);
+        cudaMalloc((void**)&data->min_per_dim_d[i], sizeof(double) * dim);
+        cudaMalloc((void**)&data->coords_device[i], sizeof(double*) * dim);
+        cudaMemcpy(data->coords_device[i], data->coords_d[i], sizeof(double*) * dim, cudaMemcpyHostToDevice);
+        data->code_d[i] = h->codes[i];
+        struct point_set ps;
+        ps.coords = data->coords_device[i];
+        ps.dim = dim;
+        ps.size = n;
+        ps.max_per_dim = data->max_per_dim_d[i];
+        ps.min_per_dim = data->min_per_dim_d[i];
+        ps.point_ids = data->point_ids_d[i];
+        cudaMalloc((void**)&data->points_d[i], sizeof(ps));
+        cudaMemcpy(data->points_d[i], &ps, sizeof(ps), cudaMemcpyHostToDevice);
+        struct morton_code mc;
+        mc.code = data->code_d[i];
+        mc.size = n;
+        mc.dim = dim;
+        mc.bits = h->bits;
+        mc.max_values = nullptr;
+        mc.min_values = nullptr;
+        cudaMalloc((void**)&data->morton_d[i], sizeof(mc));
+        cudaMemcpy(data->morton_d[i], &mc, sizeof(mc), cudaMemcpyHostToDevice);
+    }
+}
+
+void setup_h_matrix(struct h_matrix_data* data)
+{
+    hmg_matrix* h = legacy_handle(data);
+    if (!h) { fprintf(stderr, "hmglib: setup_h_matrix on an uninitialised structure\n"); return; }
+    // the caller wrote the coordinates straight into the handle's point buffers
+    h->points_set[0] = h->points_set[1] = true;
+    hmg_status st = hmg_setup(h, data->eta, data->c_leaf, data->max_level, data->root_level_set_1,
+                              data->root_level_set_2, HMG_ADMISSIBLE_MAX);
+    if (st) { legacy_fail("setup_h_matrix", st); return; }
+    for (int i = 0; i < 2; i++) {
+        int n = h->n[i];
+        // the reference permutes coords_d in place (helper.cu:293-328)
+        cudaMemcpy(h->pts[i], h->zpts[i], sizeof(double) * n * h->dim, cudaMemcpyDeviceToDevice);
+        if (!data->order[i]) cudaMalloc((void**)&data->order[i], sizeof(uint64_t) * n);
+        k_perm_to_u64<<<ceil_div(n, 256), 256>>>(h->perm[i], n, data->order[i], data->point_ids_d[i]);
+        // per-dimension extremes
+        std::vector<double> z((size_t)n * h->dim), mn(h->dim), mx(h->dim);
+        cudaMemcpy(z.data(), h->zpts[i], sizeof(double) * z.size(), cudaMemcpyDeviceToHost);
+        for (int d = 0; d < h->dim; d++) {
+            double a = z[(size_t)d * n], b = a;
+            for (int k = 1; k < n; k++) { a = std::fmin(a, z[(size_t)d * n + k]); b = std::fmax(b, z[(size_t)d * n + k]); }
+            mn[d] = a; mx[d] = b;
+        }
+        cudaMemcpy(data->min_per_dim_d[i], mn.data(), sizeof(double) * h->dim, cudaMemcpyHostToDevice);
+        cudaMemcpy(data->max_per_dim_d[i], mx.data(), sizeof(double) * h->dim, cudaMemcpyHostToDevice);
+    }
+    data->mat_vec_data_count = h->nblocks;
+    data->mat_vec_info.dense_count = h->ndense;
+    data->mat_vec_info.aca_count = h->naca;
+    data->mat_vec_info.total_count = h->nblocks;
+    if (data->mat_vec_data) {
+        cudaFree(*data->mat_vec_data);
+        delete data->mat_vec_data;
+    }
+    data->mat_vec_data = new struct work_item*[1];
+    data->mat_vec_data_array_size = h->nblocks;
+    cudaMalloc((void**)data->mat_vec_data, sizeof(struct work_item) * (h->nblocks > 0 ? h->nblocks : 1));
+    if (h->nblocks > 0)
+        k_fill_work_items<<<h->nblocks, 128>>>(h->blk_r0, h->blk_m1, h->blk_c0, h->blk_m2, h->blk_type,
+                                                h->nblocks, h->zpts[0], h->n[0], h->zpts[1], h->n[1], h->dim,
+                                                *data->mat_vec_data);
+    // one batch for everything (linear_algebra.cu:4176-4288 plan batches for memory caps)
+    long long need = 0;
+    for (int b = 0; b < h->ndense; b++) need += (long long)h->h_m1[b] * h->h_m2[b];
+    long long pred = (long long)((double)need * 1.05);
+    data->max_batched_dense_size = pred > 2147483647ll ? 2147483647 : (int)pred;
+    delete[] data->dense_work_size;
+    delete[] data->aca_work_size;
+    data->dense_work_size = new int[2]{h->ndense, 0};
+    data->aca_work_size = new int[2]{h->naca, 0};
+    data->dense_batch_count = 2;
+    data->aca_batch_count = 2;
+    cudaDeviceSynchronize();
+}
+
+static hmg_status legacy_kernel(struct h_matrix_data* data, hmg_matrix* h)
+{
+    if (!data->assem) {
+        set_error("no kernel assembler set (data.assem is NULL)");
+        return HMG_ERR_STATE;
+    }
+    struct system_assembler a;
+    HMG_CUDA_TRY(cudaMemcpy(&a, data->assem, sizeof(a), cudaMemcpyDeviceToHost));
+    return hmg_set_kernel(h, a.kind, a.param, a.regularization);
+}
+
+void precompute_aca(struct h_matrix_data* data)
+{
+    hmg_matrix* h = legacy_handle(data);
+    if (!h) return;
+    hmg_status st = legacy_kernel(data, h);
+    if (!st) st = hmg_precompute_aca(h, data->k, 0.0, HMG_PREC_FP64);
+    if (st) { legacy_fail("precompute_aca", st); return; }
+    data->U = h->far_chunks.empty() ? nullptr : (double*)h->far_chunks[0];
+    data->V = data->U;
+}
+
+void precompute_dense(struct h_matrix_data* data)
+{
+    hmg_matrix* h = legacy_handle(data);
+    if (!h) return;
+    hmg_status st = legacy_kernel(data, h);
+    if (!st) st = hmg_precompute_dense(h, HMG_PREC_FP64);
+    if (st) { legacy_fail("precompute_dense", st); return; }
+    data->dA = (double*)h->near_data;
+}
+
+void apply_h_matrix_mvp(double* x, double* y, struct h_matrix_data* data)
+{
+    hmg_matrix* h = legacy_handle(data);
+    if (!h) return;
+    hmg_status st = legacy_kernel(data, h);
+    // without precompute_aca the reference recomputes the ACA in every call
+    // (linear_algebra.cu:4357-4371); here it is computed once and kept
+    if (!st && h->naca > 0 && h->far_prec < 0) st = hmg_precompute_aca(h, data->k, 0.0, HMG_PREC_FP64);
+    if (!st) st = hmg_set_near_mode(h, h->near_prec >= 0 ? HMG_NEAR_STORED : HMG_NEAR_ONTHEFLY);
+    if (!st) st = hmg_matvec(h, x, y);
+    if (!st) st = hmg_synchronize(h);
+    if (st) legacy_fail("apply_h_matrix_mvp", st);
+}
+
+void apply_h_matrix_mvp_without_batching(double* x, double* y, struct h_matrix_data* data)
+{
+    apply_h_matrix_mvp(x, y, data);
+}
+
+void apply_full_mvp(double* x, double* y, struct h_matrix_data* data)
+{
+    hmg_matrix* h = legacy_handle(data);
+    if (!h) return;
+    hmg_status st = legacy_kernel(data, h);
+    if (!st) st = hmg_full_matvec(h, x, y);
+    if (!st) st = hmg_synchronize(h);
+    if (st) legacy_fail("apply_full_mvp", st);
+}
+
+void set_gaussian_kernel_rhs(double* b, struct h_matrix_data* data)
+{
+    hmg_matrix* h = legacy_handle(data);
+    if (!h) return;
+    hmg_status st = hmg_gaussian_rhs(h, b);
+    if (!st) st = hmg_synchronize(h);
+    if (st) legacy_fail("set_gaussian_kernel_rhs", st);
+}
+
+void destroy_h_matrix_data(struct h_matrix_data* data)
+{
+    hmg_matrix* h = legacy_handle(data);
+    for (int i = 0; i < 2; i++) {
+        delete[] data->coords_d[i];
+        data->coords_d[i] = nullptr;
+        cudaFree(data->point_ids_d[i]);
+        cudaFree(data->max_per_dim_d[i]);
+        cudaFree(data->min_per_dim_d[i]);
+        cudaFree(data->coords_device[i]);
+        cudaFree(data->points_d[i]);
+        cudaFree(data->morton_d[i]);
+        cudaFree(data->order[i]);
+        data->code_d[i] = nullptr;
+    }
+    if (data->mat_vec_data) {
+        cudaFree(*data->mat_vec_data);
+        delete data->mat_vec_data;
+        data->mat_vec_data = nullptr;
+    }
+    delete[] data->dense_work_size;
+    delete[] data->aca_work_size;
+    data->dense_work_size = data->aca_work_size = nullptr;
+    data->U = data->V = data->dA = nullptr;
+    hmg_destroy(h);
+    data->magma_queue = nullptr;
+}
+
+// ---- assemblers (kernel_system_assembler.h) -------------------------------------
+static void create_assembler(void* slot, int kind, double param, double reg)
+{
+    struct system_assembler a;
+    a.kind = kind;
+    a.param = param;
+    a.regularization = reg;
+    struct system_assembler* d = nullptr;
+    if (cudaMalloc((void**)&d, sizeof(a)) != cudaSuccess) {
+        fprintf(stderr, "hmglib: cannot allocate a kernel assembler\n");
+        return;
+    }
+    cudaMemcpy(d, &a, sizeof(a), cudaMemcpyHostToDevice);
+    cudaMemcpy(slot, &d, sizeof(d), cudaMemcpyHostToDevice);
+}
+
+static void destroy_assembler(void* slot)
+{
+    struct system_assembler* d = nullptr;
+    if (cudaMemcpy(&d, slot, sizeof(d), cudaMemcpyDeviceToHost) == cudaSuccess && d) cudaFree(d);
+}
+
+void create_gaussian_kernel_system_assembler_object(struct gaussian_kernel_system_assembler** assem,
+                                                    double regularization)
+{
+    create_assembler(assem, HMG_KERNEL_GAUSSIAN_REF, 0.0, regularization);
+}
+
+void destroy_gaussian_kernel_system_assembler_object(struct gaussian_kernel_system_assembler** assem)
+{
+    destroy_assembler(assem);
+}
+
+void create_matern_kernel_system_assembler_object(struct matern_kernel_system_assembler** assem,
+                                                  double regularization)
+{
+    create_assembler(assem, HMG_KERNEL_MATERN_REF, 0.0, regularization);
+}
+
+void destroy_matern_kernel_system_assembler_object(struct matern_kernel_system_assembler** assem)
+{
+    destroy_assembler(assem);
+}
+
+void create_gaussian_lengthscale_kernel_system_assembler_object(
+    struct gaussian_lengthscale_kernel_system_assembler** assem, double length2, double regularization)
+{
+    create_assembler(assem, HMG_KERNEL_GAUSSIAN, length2, regularization);
+}
+
+void create_matern32_kernel_system_assembler_object(struct matern32_kernel_system_assembler** assem,
+                                                    double rho, double regularization)
+{
+    create_assembler(assem, HMG_KERNEL_MATERN32, rho, regularization);
+}
+
+}  // extern "C"

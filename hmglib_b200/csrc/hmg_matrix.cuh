@@ -1,0 +1,105 @@
+// hmg_matrix.cuh -- the engine's handle (opaque `hmg_matrix` of include/hmg.h).
+#pragma once
+
+#include <vector>
+
+#include "hmg_internal.cuh"
+#include "util.cuh"
+
+struct hmg_matrix {
+    int n[2] = {0, 0};
+    int dim = 0, bits = 0;
+    int device = 0;
+    cudaStream_t stream = nullptr;
+
+    // ---- points -------------------------------------------------------------
+    bool points_set[2] = {false, false};
+    double* pts[2] = {nullptr, nullptr};   // caller order, SoA dim x n
+    double* zpts[2] = {nullptr, nullptr};  // Z order, SoA dim x n
+    uint64_t* codes[2] = {nullptr, nullptr};  // Z-ordered (sorted) Morton codes
+    int* perm[2] = {nullptr, nullptr};        // perm[i] = caller index of Z point i
+    int* iperm[2] = {nullptr, nullptr};       // inverse: Z index of caller point i
+
+    // ---- tree ---------------------------------------------------------------
+    bool setup_done = false;
+    double eta = 0.0;
+    int c_leaf = 0, max_level = 0, rule = 0;
+    int nblocks = 0, ndense = 0, naca = 0, levels = 0;
+    int* blk_r0 = nullptr;  // device SoA, reference mat_vec_data order
+    int* blk_m1 = nullptr;
+    int* blk_c0 = nullptr;
+    int* blk_m2 = nullptr;
+    int* blk_type = nullptr;
+    std::vector<int> h_r0, h_m1, h_c0, h_m2, h_type;
+
+    // ---- row tiles ----------------------------------------------------------
+    int ntiles = 0;
+    int* tile_r0 = nullptr;     // first Z row of each tile
+    int* tile_s = nullptr;      // rows in tile (<= HMG_TILE_ROWS)
+    int* tile_pstart = nullptr; // padded row start (sum of round_up4(s) of earlier tiles)
+    int* blk_tfirst = nullptr;  // first tile of each block's rows
+    int* blk_tlast = nullptr;
+    int npairs = 0;
+    int* tile_pair_start = nullptr;  // CSR over tiles (ntiles+1)
+    int* pair_block = nullptr;       // block index of each (tile, block) pair
+    std::vector<int> h_tile_pstart, h_blk_tfirst, h_blk_tlast;
+
+    // ---- kernel function ------------------------------------------------------
+    bool kernel_set = false;
+    hmg::KernelSpec kspec{};
+
+    // ---- near field -----------------------------------------------------------
+    int near_mode = HMG_NEAR_ONTHEFLY;
+    int near_prec = -1;               // -1: not stored
+    void* near_data = nullptr;
+    long long* near_off = nullptr;    // element offset of each block (dense blocks)
+    long long near_entries = 0;       // sum m1*m2
+    long long near_stored = 0;        // stored elements incl. padding
+
+    // ---- far field ------------------------------------------------------------
+    int far_prec = -1;                // -1: not computed
+    int aca_k = 0;
+    double aca_eps = 0.0;
+    int* rank = nullptr;              // per block (0 for dense)
+    long long* rank_off = nullptr;    // exclusive scan of ranks over blocks
+    long long rank_total = 0;
+    void** ptrU = nullptr;            // per block device pointer (ACA blocks)
+    void** ptrV = nullptr;
+    std::vector<void*> far_chunks;    // allocations holding the factors
+    std::vector<int> h_rank;
+    long long far_entries = 0, far_rows = 0, far_stored = 0;
+    int max_rank = 0;
+
+    // ---- matvec workspace -------------------------------------------------------
+    double* xs64 = nullptr;   // Z-ordered x
+    float* xs32 = nullptr;
+    void* tbuf = nullptr;     // V^T x per block (rank_total entries)
+    void* pair_desc = nullptr;     // per (tile, block) pair: slice pointer, vector, columns
+    int desc_near_mode = -1, desc_near_prec = -2, desc_far_prec = -2;
+    void* k1_units = nullptr;      // (block, first row, end row) pieces of V^T
+    int nk1 = 0;
+    double* host_x = nullptr; // pinned staging
+    double* host_y = nullptr;
+    double* dev_x = nullptr;
+    double* dev_y = nullptr;
+    int k1_grid = 0, k2_grid = 0;
+    bool profiling = false;
+    cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+};
+
+namespace hmg {
+hmg_status setup_tree(hmg_matrix* h);
+hmg_status build_tiles(hmg_matrix* h);
+hmg_status run_aca(hmg_matrix* h, int k, double eps, int precision);
+hmg_status fill_near(hmg_matrix* h, int precision);
+hmg_status matvec_device(hmg_matrix* h, const double* x, double* y);
+hmg_status direct_matvec(hmg_matrix* h, const double* x, const int* rows, int nrows,
+                         double* y);
+hmg_status gaussian_rhs(hmg_matrix* h, double* b);
+hmg_status morton_codes(const double* coords, int n, int dim, int bits, uint64_t* codes,
+                        cudaStream_t s);
+void free_far(hmg_matrix* h);
+void free_near(hmg_matrix* h);
+void free_tree(hmg_matrix* h);
+const char* last_error();
+}  // namespace hmg

@@ -1,0 +1,519 @@
+// matvec.cu -- near-field storage and the H-matvec.
+//
+// The reference multiplies per "batch": it rebuilds index maps with Thrust on every
+// call, gathers x per block, runs MAGMA dgemv_vbatched for dense blocks and twice
+// for U (V^T x), and adds every block's result into y with double-CAS atomics
+// (linear_algebra.cu:1152-1181, 1429-1591, 2817-3137, 4292-4379).
+//
+// Here one product is three kernels and no host work:
+//   K0  x in Z order (and an FP32 copy);
+//   K1  t_b = V_b^T x_b for all admissible blocks, a warp per row of V_b^T, work
+//       split into pieces of at most ~64 KB so large blocks spread over many warps;
+//   K2  one CTA per row tile: every dense block slice and every U_b slice touching
+//       the tile is multiplied with x (dense) or t_b (low rank), FP32 products
+//       summed per slice and accumulated in FP64 across slices, the CTA's warp
+//       partials summed in a fixed order, and y written once, in the caller's
+//       order.  No atomics: y is deterministic.
+// Each stored byte is read exactly once per product (the HBM roofline's minimum).
+#include <algorithm>
+#include <vector>
+
+#include "hmg_matrix.cuh"
+
+namespace hmg {
+
+enum { PAIR_STORED = 0, PAIR_FAR = 1, PAIR_ONTHEFLY = 2 };
+
+struct PairDesc {
+    const void* data;  // tile slice (column-major, s_pad rows) or nullptr (on the fly)
+    const void* w;     // vector multiplied: x_b (dense) or t_b (low rank), storage type
+    int ncol;          // m2 (dense) or rank (low rank)
+    int kind;          // PAIR_*
+    int c0;            // first column (on the fly)
+    int pad;
+};
+
+struct K1Unit {
+    int b, l0, l1, pad;
+};
+
+// ---------------------------------------------------------------------------
+// near-field fill (precompute_batched_dense_magma, linear_algebra.cu:3140-3342):
+// one CTA per dense block, entries written tile slice by tile slice.
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void k_fill_near(const int* blocks_r0, const int* blocks_c0, const int* blocks_m2,
+                            const long long* near_off, const int* tfirst, const int* tlast,
+                            const int* tile_r0, const int* tile_s, const int* tile_pstart,
+                            KernelSpec K, PointsView P, T* out)
+{
+    const int b = blockIdx.x;
+    const int c0 = blocks_c0[b], m2 = blocks_m2[b];
+    (void)blocks_r0;
+    T* base = out + near_off[b];
+    const int p0 = tile_pstart[tfirst[b]];
+    for (int t = tfirst[b]; t <= tlast[b]; t++) {
+        const int s = tile_s[t], sp = (s + 3) & ~3, tr = tile_r0[t];
+        T* dst = base + (size_t)(tile_pstart[t] - p0) * m2;
+        for (int idx = threadIdx.x; idx < sp * m2; idx += blockDim.x) {
+            int i = idx % sp, j = idx / sp;
+            dst[idx] = i < s ? (T)kernel_entry(K, P, tr + i, c0 + j) : (T)0;
+        }
+    }
+}
+
+void free_near(hmg_matrix* h)
+{
+    if (h->near_data) cudaFree(h->near_data);
+    h->near_data = nullptr;
+    dfree(h->near_off, h->stream);
+    h->near_prec = -1;
+    h->near_stored = 0;
+    h->desc_near_mode = -1;
+    if (h->near_mode == HMG_NEAR_STORED) h->near_mode = HMG_NEAR_ONTHEFLY;
+}
+
+static PointsView points_view(hmg_matrix* h)
+{
+    PointsView P{};
+    for (int d = 0; d < h->dim; d++) {
+        P.c1[d] = h->zpts[0] + (size_t)d * h->n[0];
+        P.c2[d] = h->zpts[1] + (size_t)d * h->n[1];
+    }
+    P.n1 = h->n[0];
+    P.n2 = h->n[1];
+    return P;
+}
+
+hmg_status fill_near(hmg_matrix* h, int precision)
+{
+    cudaStream_t s = h->stream;
+    free_near(h);
+    const int nd = h->ndense;
+    const size_t esz = precision == HMG_PREC_FP64 ? 8 : 4;
+    std::vector<long long> off(nd > 0 ? nd : 1, 0);
+    long long tot = 0, entries = 0;
+    for (int b = 0; b < nd; b++) {
+        off[b] = tot;
+        long long rows_p = h->h_tile_pstart[h->h_blk_tlast[b] + 1] - h->h_tile_pstart[h->h_blk_tfirst[b]];
+        tot += rows_p * h->h_m2[b];
+        entries += (long long)h->h_m1[b] * h->h_m2[b];
+    }
+    h->near_entries = entries;
+    hmg_status st = dalloc(&h->near_off, (size_t)(nd > 0 ? nd : 1), s);
+    if (st) return st;
+    if (nd > 0) {
+        cudaError_t ce = cudaMalloc(&h->near_data, (size_t)tot * esz);
+        if (ce != cudaSuccess) {
+            cudaGetLastError();
+            h->near_data = nullptr;
+            set_error("allocating %lld bytes of near-field blocks failed: %s", tot * (long long)esz,
+                      cudaGetErrorString(ce));
+            return ce == cudaErrorMemoryAllocation ? HMG_ERR_NOMEM : HMG_ERR_CUDA;
+        }
+        HMG_CUDA_TRY(cudaMemcpyAsync(h->near_off, off.data(), sizeof(long long) * nd, cudaMemcpyHostToDevice, s));
+        PointsView P = points_view(h);
+        if (precision == HMG_PREC_FP64)
+            k_fill_near<double><<<nd, 256, 0, s>>>(h->blk_r0, h->blk_c0, h->blk_m2, h->near_off,
+                                                   h->blk_tfirst, h->blk_tlast, h->tile_r0, h->tile_s,
+                                                   h->tile_pstart, h->kspec, P, (double*)h->near_data);
+        else
+            k_fill_near<float><<<nd, 256, 0, s>>>(h->blk_r0, h->blk_c0, h->blk_m2, h->near_off,
+                                                  h->blk_tfirst, h->blk_tlast, h->tile_r0, h->tile_s,
+                                                  h->tile_pstart, h->kspec, P, (float*)h->near_data);
+        HMG_LAUNCH_CHECK();
+    }
+    HMG_CUDA_TRY(cudaStreamSynchronize(s));
+    h->near_stored = tot;
+    h->near_prec = precision;
+    h->near_mode = HMG_NEAR_STORED;
+    return HMG_OK;
+}
+
+// ---------------------------------------------------------------------------
+// descriptors of the product (rebuilt when storage or modes change)
+// ---------------------------------------------------------------------------
+__global__ void k_build_desc(const int* tile_pair_start, int ntiles, const int* pair_block,
+                             const int* tile_pstart, const int* blk_type, const int* blk_c0,
+                             const int* blk_m2, const int* tfirst, const long long* near_off,
+                             const void* near_data, int near_esz, int near_mode,
+                             const int* rank, const long long* rank_off, void* const* ptrU,
+                             const void* tbuf, int far_esz, const void* xs, int x_esz,
+                             PairDesc* desc)
+{
+    int t = blockIdx.x;
+    if (t >= ntiles) return;
+    int pt = tile_pstart[t];
+    for (int p = tile_pair_start[t] + threadIdx.x; p < tile_pair_start[t + 1]; p += blockDim.x) {
+        int b = pair_block[p];
+        PairDesc d;
+        int slice_row = pt - tile_pstart[tfirst[b]];
+        d.c0 = blk_c0[b];
+        d.pad = 0;
+        if (blk_type[b] == HMG_WT_DENSE) {
+            d.ncol = blk_m2[b];
+            d.w = (const char*)xs + (size_t)blk_c0[b] * x_esz;
+            if (near_mode == HMG_NEAR_STORED) {
+                d.kind = PAIR_STORED;
+                d.data = (const char*)near_data +
+                         (size_t)(near_off[b] + (long long)slice_row * d.ncol) * near_esz;
+            } else {
+                d.kind = PAIR_ONTHEFLY;
+                d.data = nullptr;
+            }
+        } else {
+            d.kind = PAIR_FAR;
+            d.ncol = rank[b];
+            d.w = (const char*)tbuf + (size_t)rank_off[b] * far_esz;
+            d.data = (const char*)ptrU[b] + (size_t)slice_row * d.ncol * far_esz;
+        }
+        desc[p] = d;
+    }
+}
+
+static hmg_status ensure_desc(hmg_matrix* h, int elem)
+{
+    cudaStream_t s = h->stream;
+    hmg_status st;
+    if (!h->pair_desc) {
+        PairDesc* d = nullptr;
+        if ((st = dalloc(&d, (size_t)(h->npairs > 0 ? h->npairs : 1), s))) return st;
+        h->pair_desc = d;
+        h->desc_near_mode = -1;
+    }
+    if (h->desc_near_mode == h->near_mode && h->desc_near_prec == h->near_prec &&
+        h->desc_far_prec == h->far_prec)
+        return HMG_OK;
+    const void* xs = elem == 8 ? (const void*)h->xs64 : (const void*)h->xs32;
+    int near_esz = h->near_prec == HMG_PREC_FP64 ? 8 : 4;
+    int far_esz = h->far_prec == HMG_PREC_FP64 ? 8 : 4;
+    if (h->ntiles > 0) {
+        k_build_desc<<<h->ntiles, 128, 0, s>>>(
+            h->tile_pair_start, h->ntiles, h->pair_block, h->tile_pstart, h->blk_type, h->blk_c0,
+            h->blk_m2, h->blk_tfirst, h->near_off, h->near_data, near_esz, h->near_mode, h->rank,
+            h->rank_off, h->ptrU, h->tbuf, far_esz, xs, elem, (PairDesc*)h->pair_desc);
+        HMG_LAUNCH_CHECK();
+    }
+    // K1 pieces: rows of V_b^T in runs of at most ~64 KB
+    dfree(h->k1_units, s);
+    std::vector<K1Unit> units;
+    for (int b = h->ndense; b < h->nblocks; b++) {
+        int r = h->h_rank[b];
+        if (r == 0) continue;
+        long long row_bytes = (long long)((h->h_m2[b] + 3) & ~3) * far_esz;
+        int per = (int)std::max(1ll, (65536ll) / row_bytes);
+        for (int l = 0; l < r; l += per) units.push_back({b, l, std::min(r, l + per), 0});
+    }
+    h->nk1 = (int)units.size();
+    K1Unit* du = nullptr;
+    if ((st = dalloc(&du, units.size() > 0 ? units.size() : 1, s))) return st;
+    if (!units.empty())
+        HMG_CUDA_TRY(cudaMemcpyAsync(du, units.data(), sizeof(K1Unit) * units.size(), cudaMemcpyHostToDevice, s));
+    h->k1_units = du;
+    HMG_CUDA_TRY(cudaStreamSynchronize(s));
+    h->desc_near_mode = h->near_mode;
+    h->desc_near_prec = h->near_prec;
+    h->desc_far_prec = h->far_prec;
+    return HMG_OK;
+}
+
+// ---------------------------------------------------------------------------
+// the product kernels
+// ---------------------------------------------------------------------------
+__global__ void k_gather_x(const double* x, const int* perm2, int n, double* xs64, float* xs32)
+{
+    int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= n) return;
+    double v = x[perm2[j]];
+    xs64[j] = v;
+    xs32[j] = (float)v;
+}
+
+template <typename T> struct Vec;
+template <> struct Vec<float> { typedef float4 type; static constexpr int N = 4; };
+template <> struct Vec<double> { typedef double2 type; static constexpr int N = 2; };
+
+__device__ __forceinline__ void vec_get(const float4& v, float* o) { o[0] = v.x; o[1] = v.y; o[2] = v.z; o[3] = v.w; }
+__device__ __forceinline__ void vec_get(const double2& v, double* o) { o[0] = v.x; o[1] = v.y; }
+
+// K1: t_b[l] = sum_j V_b^T[l][j] x[c0_b + j]; one warp per row, rows of a piece in turn.
+template <typename T>
+__global__ void __launch_bounds__(256) k_vtx(const K1Unit* units, int nunits, const int* blk_c0,
+                                             const int* blk_m2, const long long* rank_off,
+                                             T* const* ptrV, const T* xs, int n2, T* tbuf)
+{
+    typedef typename Vec<T>::type V4;
+    constexpr int NV = Vec<T>::N;
+    const int lane = threadIdx.x & 31;
+    const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int nw = (gridDim.x * blockDim.x) >> 5;
+    for (int u = gw; u < nunits; u += nw) {
+        K1Unit un = units[u];
+        const int b = un.b, c0 = blk_c0[b], m2 = blk_m2[b], m2p = (m2 + 3) & ~3;
+        const T* V = ptrV[b];
+        const long long ro = rank_off[b];
+        for (int l = un.l0; l < un.l1; l++) {
+            const T* row = V + (size_t)l * m2p;
+            T acc = 0;
+            for (int j = lane * NV; j < m2p; j += 32 * NV) {
+                V4 v = *reinterpret_cast<const V4*>(row + j);
+                T vv[NV];
+                vec_get(v, vv);
+#pragma unroll
+                for (int q = 0; q < NV; q++) {
+                    int jj = j + q;
+                    T xv = (jj < m2 && c0 + jj < n2) ? xs[c0 + jj] : (T)0;
+                    acc = fma(vv[q], xv, acc);
+                }
+            }
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+            if (lane == 0) tbuf[ro + l] = acc;
+        }
+    }
+}
+
+// K2: one CTA (8 warps) per row tile.  A group of RW warps covers the tile's padded
+// rows with 16-byte loads (4 FP32 or 2 FP64 rows per lane); the 8/RW groups take
+// the tile's pairs round robin.
+template <typename T>
+__global__ void __launch_bounds__(256) k_tile_matvec(const PairDesc* desc, const int* tile_pair_start,
+                                                     const int* tile_r0, const int* tile_s,
+                                                     const int* perm1, KernelSpec K, PointsView P,
+                                                     const double* xs64, double* y)
+{
+    typedef typename Vec<T>::type V4;
+    constexpr int NV = Vec<T>::N;
+    __shared__ double red[8][HMG_TILE_ROWS];
+    const int t = blockIdx.x;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int s = tile_s[t], sp = (s + 3) & ~3, tr0 = tile_r0[t];
+    const int lanes_needed = sp / NV;
+    const int RW = lanes_needed > 32 ? 2 : 1;  // sp <= 128 rows
+    const int G = 8 / RW;
+    const int g = warp / RW, rw = warp % RW;
+    const int row0 = (rw * 32 + lane) * NV;
+    const bool active = row0 < sp;
+    double acc64[NV];
+#pragma unroll
+    for (int q = 0; q < NV; q++) acc64[q] = 0.0;
+
+    const int pbeg = tile_pair_start[t], pend = tile_pair_start[t + 1];
+    for (int p = pbeg + g; p < pend; p += G) {
+        const PairDesc d = desc[p];
+        T acc[NV];
+#pragma unroll
+        for (int q = 0; q < NV; q++) acc[q] = 0;
+        if (d.kind != PAIR_ONTHEFLY) {
+            const T* base = (const T*)d.data + row0;
+            const T* w = (const T*)d.w;
+            if (active) {
+                int j = 0;
+                for (; j + 4 <= d.ncol; j += 4) {
+                    V4 v0 = *reinterpret_cast<const V4*>(base + (size_t)(j + 0) * sp);
+                    V4 v1 = *reinterpret_cast<const V4*>(base + (size_t)(j + 1) * sp);
+                    V4 v2 = *reinterpret_cast<const V4*>(base + (size_t)(j + 2) * sp);
+                    V4 v3 = *reinterpret_cast<const V4*>(base + (size_t)(j + 3) * sp);
+                    T w0 = w[j], w1 = w[j + 1], w2 = w[j + 2], w3 = w[j + 3];
+                    T a[NV];
+                    vec_get(v0, a);
+#pragma unroll
+                    for (int q = 0; q < NV; q++) acc[q] = fma(a[q], w0, acc[q]);
+                    vec_get(v1, a);
+#pragma unroll
+                    for (int q = 0; q < NV; q++) acc[q] = fma(a[q], w1, acc[q]);
+                    vec_get(v2, a);
+#pragma unroll
+                    for (int q = 0; q < NV; q++) acc[q] = fma(a[q], w2, acc[q]);
+                    vec_get(v3, a);
+#pragma unroll
+                    for (int q = 0; q < NV; q++) acc[q] = fma(a[q], w3, acc[q]);
+                }
+                for (; j < d.ncol; j++) {
+                    V4 v0 = *reinterpret_cast<const V4*>(base + (size_t)j * sp);
+                    T a[NV];
+                    vec_get(v0, a);
+                    T w0 = w[j];
+#pragma unroll
+                    for (int q = 0; q < NV; q++) acc[q] = fma(a[q], w0, acc[q]);
+                }
+            }
+#pragma unroll
+            for (int q = 0; q < NV; q++) acc64[q] += (double)acc[q];
+        } else if (active) {
+            // dense block regenerated from the points, FP64
+            double a64[NV];
+#pragma unroll
+            for (int q = 0; q < NV; q++) a64[q] = 0.0;
+            for (int j = 0; j < d.ncol; j++) {
+                double xv = xs64[d.c0 + j];
+#pragma unroll
+                for (int q = 0; q < NV; q++)
+                    if (row0 + q < s) a64[q] = fma(kernel_entry(K, P, tr0 + row0 + q, d.c0 + j), xv, a64[q]);
+            }
+#pragma unroll
+            for (int q = 0; q < NV; q++) acc64[q] += a64[q];
+        }
+    }
+    // fixed-order reduction of the groups' partial rows
+    if (active) {
+#pragma unroll
+        for (int q = 0; q < NV; q++) red[g][row0 + q] = acc64[q];
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < s; i += blockDim.x) {
+        double v = 0.0;
+        for (int gg = 0; gg < G; gg++) v += red[gg][i];
+        y[perm1[tr0 + i]] = v;
+    }
+}
+
+hmg_status matvec_device(hmg_matrix* h, const double* x, double* y)
+{
+    cudaStream_t s = h->stream;
+    hmg_status st;
+    if (!h->xs64) {
+        if ((st = dalloc(&h->xs64, (size_t)h->n[1], s)) || (st = dalloc(&h->xs32, (size_t)h->n[1], s)))
+            return st;
+    }
+    const bool fp64 = h->far_prec == HMG_PREC_FP64 ||
+                      (h->naca == 0 && h->near_prec != HMG_PREC_FP32);
+    if (h->near_mode == HMG_NEAR_STORED && h->naca > 0 && h->near_prec != h->far_prec) {
+        set_error("stored near field (precision %d) and factors (precision %d) differ", h->near_prec,
+                  h->far_prec);
+        return HMG_ERR_UNSUPPORTED;
+    }
+    int elem = fp64 ? 8 : 4;
+    if ((st = ensure_desc(h, elem))) return st;
+    PointsView P = points_view(h);
+    if (h->profiling) HMG_CUDA_TRY(cudaEventRecord(h->ev[0], s));
+    k_gather_x<<<ceil_div(h->n[1], 256), 256, 0, s>>>(x, h->perm[1], h->n[1], h->xs64, h->xs32);
+    HMG_LAUNCH_CHECK();
+    if (h->profiling) HMG_CUDA_TRY(cudaEventRecord(h->ev[1], s));
+    if (h->nk1 > 0) {
+        int grid = std::min(ceil_div(h->nk1, 8), 148 * 8);
+        if (fp64)
+            k_vtx<double><<<grid, 256, 0, s>>>((const K1Unit*)h->k1_units, h->nk1, h->blk_c0, h->blk_m2,
+                                               h->rank_off, (double* const*)h->ptrV, h->xs64, h->n[1],
+                                               (double*)h->tbuf);
+        else
+            k_vtx<float><<<grid, 256, 0, s>>>((const K1Unit*)h->k1_units, h->nk1, h->blk_c0, h->blk_m2,
+                                              h->rank_off, (float* const*)h->ptrV, h->xs32, h->n[1],
+                                              (float*)h->tbuf);
+        HMG_LAUNCH_CHECK();
+    }
+    if (h->profiling) HMG_CUDA_TRY(cudaEventRecord(h->ev[2], s));
+    if (h->ntiles > 0) {
+        if (fp64)
+            k_tile_matvec<double><<<h->ntiles, 256, 0, s>>>((const PairDesc*)h->pair_desc, h->tile_pair_start,
+                                                            h->tile_r0, h->tile_s, h->perm[0], h->kspec, P,
+                                                            h->xs64, y);
+        else
+            k_tile_matvec<float><<<h->ntiles, 256, 0, s>>>((const PairDesc*)h->pair_desc, h->tile_pair_start,
+                                                           h->tile_r0, h->tile_s, h->perm[0], h->kspec, P,
+                                                           h->xs64, y);
+        HMG_LAUNCH_CHECK();
+    }
+    if (h->profiling) HMG_CUDA_TRY(cudaEventRecord(h->ev[3], s));
+    return HMG_OK;
+}
+
+// ---------------------------------------------------------------------------
+// FP64 direct summation (apply_full_mvp, hmglib.cu:351-401, without the N^2 matrix)
+// ---------------------------------------------------------------------------
+static constexpr int DS_THREADS = 256;
+static constexpr int DS_CHUNK = 512;
+
+__global__ void __launch_bounds__(DS_THREADS)
+k_direct(KernelSpec K, PointsView P, const double* xs, const int* zrows, int nrows, const int* out_perm,
+         double* y)
+{
+    __shared__ double cx[3][DS_CHUNK];
+    __shared__ double xv[DS_CHUNK];
+    const int t = blockIdx.x * DS_THREADS + threadIdx.x;
+    const bool valid = t < nrows;
+    const int i = valid ? (zrows ? zrows[t] : t) : 0;
+    double pi[3] = {0.0, 0.0, 0.0};
+    for (int d = 0; d < K.dim; d++) pi[d] = P.c1[d][i];
+    double acc = 0.0;
+    for (int j0 = 0; j0 < P.n2; j0 += DS_CHUNK) {
+        int nc = P.n2 - j0 < DS_CHUNK ? P.n2 - j0 : DS_CHUNK;
+        __syncthreads();
+        for (int c = threadIdx.x; c < nc; c += DS_THREADS) {
+            for (int d = 0; d < K.dim; d++) cx[d][c] = P.c2[d][j0 + c];
+            xv[c] = xs[j0 + c];
+        }
+        __syncthreads();
+        if (valid) {
+            for (int c = 0; c < nc; c++) {
+                double sq = 0.0;
+                for (int d = 0; d < K.dim; d++) {
+                    double q = pi[d] - cx[d][c];
+                    sq = __fma_rn(q, q, sq);
+                }
+                double k = kernel_from_sq(K, sq);
+                if (i == j0 + c) k += K.reg;
+                acc = fma(k, xv[c], acc);
+            }
+        }
+    }
+    if (valid) y[out_perm ? out_perm[i] : t] = acc;
+}
+
+__global__ void k_rows_to_z(const int* rows, int n, const int* iperm, int* z)
+{
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < n) z[t] = iperm[rows[t]];
+}
+
+hmg_status direct_matvec(hmg_matrix* h, const double* x, const int* rows, int nrows, double* y)
+{
+    cudaStream_t s = h->stream;
+    hmg_status st;
+    if (!h->xs64) {
+        if ((st = dalloc(&h->xs64, (size_t)h->n[1], s)) || (st = dalloc(&h->xs32, (size_t)h->n[1], s)))
+            return st;
+    }
+    k_gather_x<<<ceil_div(h->n[1], 256), 256, 0, s>>>(x, h->perm[1], h->n[1], h->xs64, h->xs32);
+    HMG_LAUNCH_CHECK();
+    PointsView P = points_view(h);
+    if (!rows) {
+        k_direct<<<ceil_div(h->n[0], DS_THREADS), DS_THREADS, 0, s>>>(h->kspec, P, h->xs64, nullptr, h->n[0],
+                                                                      h->perm[0], y);
+        HMG_LAUNCH_CHECK();
+        return HMG_OK;
+    }
+    int* z = nullptr;
+    if ((st = dalloc(&z, (size_t)(nrows > 0 ? nrows : 1), s))) return st;
+    if (nrows > 0) {
+        k_rows_to_z<<<ceil_div(nrows, 256), 256, 0, s>>>(rows, nrows, h->iperm[0], z);
+        HMG_LAUNCH_CHECK();
+        k_direct<<<ceil_div(nrows, DS_THREADS), DS_THREADS, 0, s>>>(h->kspec, P, h->xs64, z, nrows, nullptr, y);
+        HMG_LAUNCH_CHECK();
+    }
+    dfree(z, s);
+    return HMG_OK;
+}
+
+// set_gaussian_kernel_rhs (hmglib.cu:403-439), evaluated in the caller's order
+__global__ void k_gaussian_rhs(const double* pts, int n, int dim, double* b)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double pi = 3.14159265358979323846;
+    double r = 1.0;
+    for (int d = 0; d < dim; d++) {
+        double x = pts[(size_t)d * n + i];
+        r = r * sqrt(pi) * (erf(1.0 - x) - erf(0.0 - x)) / 2.0;
+    }
+    b[i] = r;
+}
+
+hmg_status gaussian_rhs(hmg_matrix* h, double* b)
+{
+    k_gaussian_rhs<<<ceil_div(h->n[0], 256), 256, 0, h->stream>>>(h->pts[0], h->n[0], h->dim, b);
+    HMG_LAUNCH_CHECK();
+    return HMG_OK;
+}
+
+}  // namespace hmg

@@ -1,0 +1,180 @@
+"""Host-side mirror of the reference's H-matrix interface (src/hmglib.h:29-121).
+
+``HMatrix`` keeps the reference's life cycle -- init, setup, precompute_aca,
+precompute_dense, apply, apply_full, destroy -- and argument meaning, on top of
+the C ABI in include/hmg.h.  Vectors may be NumPy arrays (host; copied in and out
+inside the call) or CUDA tensors / any object exposing ``data_ptr()`` (device;
+stream-ordered on the handle's stream, which is the legacy default stream unless
+``stream`` is given).
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _lib as L
+
+
+def _ptr(a):
+    if hasattr(a, "data_ptr"):
+        return C.c_void_p(a.data_ptr())
+    return a.ctypes.data_as(C.c_void_p)
+
+
+class HMatrix:
+    """An H-matrix between point sets 1 (rows) and 2 (columns)."""
+
+    def __init__(self, n1: int, n2: int, dim: int, bits: int = 0, stream: int | None = None):
+        self._lib = L.lib()
+        h = C.c_void_p()
+        L.check(self._lib.hmg_create(C.byref(h), int(n1), int(n2), int(dim), int(bits),
+                                     C.c_void_p(stream or 0)), "hmg_create")
+        self._h = h
+        self.n1, self.n2, self.dim = int(n1), int(n2), int(dim)
+
+    # -- life cycle ------------------------------------------------------------
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.hmg_destroy(self._h)
+            self._h = None
+
+    destroy = close
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def _call(self, name, *args):
+        L.check(getattr(self._lib, name)(self._h, *args), name)
+
+    # -- construction ----------------------------------------------------------
+    def set_points(self, which: int, coords):
+        """coords: (dim, n) float64, host array or device tensor (SoA)."""
+        if hasattr(coords, "data_ptr"):
+            assert tuple(coords.shape) == (self.dim, (self.n1, self.n2)[which])
+            self._call("hmg_set_points", int(which), _ptr(coords), 1)
+        else:
+            c = np.ascontiguousarray(coords, dtype=np.float64)
+            assert c.shape == (self.dim, (self.n1, self.n2)[which]), c.shape
+            self._call("hmg_set_points", int(which), _ptr(c), 0)
+
+    def setup(self, eta: float, c_leaf: int, max_level: int = 50, root_levels=(0, 0),
+              rule: int = L.ADMISSIBLE_MAX):
+        self._call("hmg_setup", float(eta), int(c_leaf), int(max_level), int(root_levels[0]),
+                   int(root_levels[1]), int(rule))
+
+    def set_kernel(self, kind: int, param: float = 0.0, regularization: float = 0.0):
+        self._call("hmg_set_kernel", int(kind), float(param), float(regularization))
+
+    def precompute_aca(self, k: int, eps: float = 0.0, precision: int = L.PREC_FP64):
+        self._call("hmg_precompute_aca", int(k), float(eps), int(precision))
+
+    def precompute_dense(self, precision: int = L.PREC_FP64):
+        self._call("hmg_precompute_dense", int(precision))
+
+    def set_near_mode(self, mode: int):
+        self._call("hmg_set_near_mode", int(mode))
+
+    # -- products --------------------------------------------------------------
+    def matvec(self, x, y=None):
+        """y = H x.  Host arrays: synchronous.  Device tensors: asynchronous."""
+        if hasattr(x, "data_ptr"):
+            assert y is not None, "pass a device output tensor"
+            self._call("hmg_matvec", _ptr(x), _ptr(y))
+            return y
+        xh = np.ascontiguousarray(x, dtype=np.float64)
+        yh = np.empty(self.n1) if y is None else y
+        self._call("hmg_matvec_host", _ptr(xh), _ptr(yh))
+        return yh
+
+    apply = matvec
+
+    def matvec_device(self, x_ptr: int, y_ptr: int):
+        self._call("hmg_matvec", C.c_void_p(x_ptr), C.c_void_p(y_ptr))
+
+    def full_matvec(self, x, y):
+        """FP64 direct product on device tensors (apply_full_mvp)."""
+        self._call("hmg_full_matvec", _ptr(x), _ptr(y))
+        return y
+
+    def full_matvec_rows(self, x, rows, y):
+        self._call("hmg_full_matvec_rows", _ptr(x), _ptr(rows), int(rows.shape[0]), _ptr(y))
+        return y
+
+    def gaussian_rhs(self, b):
+        self._call("hmg_gaussian_rhs", _ptr(b))
+        return b
+
+    def synchronize(self):
+        self._call("hmg_synchronize")
+
+    def set_profiling(self, on: bool = True):
+        self._call("hmg_set_profiling", 1 if on else 0)
+
+    def profile(self) -> dict:
+        """Device milliseconds of the last product's phases."""
+        out = np.zeros(4)
+        self._call("hmg_get_profile", _ptr(out))
+        return {"gather_ms": out[0], "vtx_ms": out[1], "tiles_ms": out[2], "total_ms": out[3]}
+
+    # -- inspection --------------------------------------------------------------
+    def info(self) -> dict:
+        i = L.Info()
+        self._call("hmg_get_info", C.byref(i))
+        return i.as_dict()
+
+    def codes(self, which: int) -> np.ndarray:
+        n = (self.n1, self.n2)[which]
+        out = np.empty(n, dtype=np.uint64)
+        self._call("hmg_get_codes", int(which), _ptr(out))
+        return out
+
+    def order(self, which: int) -> np.ndarray:
+        n = (self.n1, self.n2)[which]
+        out = np.empty(n, dtype=np.int64)
+        self._call("hmg_get_order", int(which), _ptr(out))
+        return out
+
+    def points(self, which: int) -> np.ndarray:
+        n = (self.n1, self.n2)[which]
+        out = np.empty((self.dim, n), dtype=np.float64)
+        self._call("hmg_get_points", int(which), _ptr(out))
+        return out
+
+    def blocks(self):
+        """(s1l, s1u, s2l, s2u, type): the leaf list in the reference's order."""
+        nb = self.info()["block_count"]
+        arrs = [np.empty(nb, dtype=np.int32) for _ in range(5)]
+        self._call("hmg_get_blocks", *[_ptr(a) for a in arrs])
+        return tuple(arrs)
+
+    def ranks(self) -> np.ndarray:
+        nb = self.info()["block_count"]
+        out = np.empty(nb, dtype=np.int32)
+        self._call("hmg_get_ranks", _ptr(out))
+        return out
+
+    def factors(self, block: int, m1: int, m2: int, rank: int):
+        U = np.zeros((max(rank, 1), m1))
+        V = np.zeros((max(rank, 1), m2))
+        self._call("hmg_get_factors", int(block), _ptr(U), _ptr(V))
+        return U[:rank], V[:rank]
+
+
+def radix_sort_u64(keys_ptr: int, vals_ptr: int, n: int, key_bits: int = 64, stream: int = 0):
+    L.check(L.lib().hmg_radix_sort_u64(C.c_void_p(keys_ptr), C.c_void_p(vals_ptr), int(n),
+                                       int(key_bits), C.c_void_p(stream)), "hmg_radix_sort_u64")
+
+
+def morton_codes(coords_ptr: int, n: int, dim: int, bits: int, codes_ptr: int, stream: int = 0):
+    L.check(L.lib().hmg_morton_codes(C.c_void_p(coords_ptr), int(n), int(dim), int(bits),
+                                     C.c_void_p(codes_ptr), C.c_void_p(stream)), "hmg_morton_codes")

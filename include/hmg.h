@@ -1,0 +1,171 @@
+/*
+ * hmg.h -- C ABI of the B200 H-matrix engine (libhmg.so).
+ *
+ * Plain C types only: an opaque handle, int/double/pointer arguments and a status
+ * code.  Every function returns HMG_OK or an error status and never exits the
+ * process; hmg_last_error() gives the message of the last failure on the calling
+ * thread.  Device pointers are CUDA device (or managed) addresses on the device
+ * that was current when the handle was created; work is ordered on the handle's
+ * stream (hmg_create's `stream`, NULL = the legacy default stream) and the
+ * functions documented as synchronous return after it finished.
+ *
+ * Each entry point names the kadircs/hmglib interface it replaces (path:line in
+ * that project).  include/hmglib.h keeps the reference's own entry points on top
+ * of these.
+ */
+#ifndef HMG_H
+#define HMG_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct hmg_matrix hmg_matrix;
+
+typedef enum {
+    HMG_OK = 0,
+    HMG_ERR_INVALID = 1,     /* bad argument */
+    HMG_ERR_CUDA = 2,        /* a CUDA call failed (message in hmg_last_error) */
+    HMG_ERR_NOMEM = 3,       /* device memory exhausted or over the handle's budget */
+    HMG_ERR_STATE = 4,       /* call out of order (e.g. matvec before setup) */
+    HMG_ERR_UNSUPPORTED = 5  /* configuration the engine does not implement */
+} hmg_status;
+
+/* kernel functions k(x, y) = f(r), r = |x - y| (kernel_system_assembler.h:26-102) */
+#define HMG_KERNEL_GAUSSIAN_REF 1 /* exp(-r^2), the reference's gaussian assembler      */
+#define HMG_KERNEL_MATERN_REF   2 /* Y1(r+1e-15) r / (2^{d/2} Gamma(1+d/2)), the ref's   */
+#define HMG_KERNEL_GAUSSIAN     3 /* exp(-r^2 / param), param = length^2                 */
+#define HMG_KERNEL_MATERN32     4 /* (1 + sqrt3 r/param) exp(-sqrt3 r/param), param=rho  */
+
+/* admissibility rules (tree.cu:121-160) */
+#define HMG_ADMISSIBLE_MAX 0 /* max(diam1, diam2) <= eta * dist  (the reference's rule) */
+#define HMG_ADMISSIBLE_MIN 1 /* min(diam1, diam2) <= eta * dist                          */
+
+/* storage precision of the near-field blocks and the low-rank factors */
+#define HMG_PREC_FP64 0
+#define HMG_PREC_FP32 1
+
+/* near-field mode for hmg_matvec */
+#define HMG_NEAR_STORED 0   /* read the blocks stored by hmg_precompute_dense          */
+#define HMG_NEAR_ONTHEFLY 1 /* regenerate dense entries from the points in every call  */
+
+typedef struct {
+    int n1, n2, dim, bits;
+    int block_count, dense_count, aca_count, levels;
+    int tile_count;           /* row tiles of the matvec */
+    int max_rank;             /* largest rank over admissible blocks (after ACA) */
+    int64_t near_entries;     /* sum over dense blocks of m1*m2 */
+    int64_t far_entries;      /* sum over admissible blocks of (m1+m2)*rank */
+    int64_t far_rows;         /* sum over admissible blocks of m1+m2 */
+    int64_t near_bytes;       /* bytes of stored near-field data (0 if not stored) */
+    int64_t far_bytes;        /* bytes of stored factors */
+    int64_t matvec_bytes;     /* bytes one hmg_matvec streams from HBM (algorithmic) */
+    int near_precision, far_precision, near_mode;
+} hmg_info;
+
+/* message of the last failed call on this thread ("" if none) */
+const char* hmg_last_error(void);
+int hmg_version(void);
+
+/* Allocate a handle for two point sets of n1 and n2 points in `dim` (2 or 3)
+ * dimensions; `bits` is the Morton resolution per dimension (0 picks 32 for 2D,
+ * 20 for 3D, the only pairs the reference supports, morton.cu:21-67).
+ * `stream` is a cudaStream_t (NULL = default stream).
+ * Replaces init_h_matrix_data (hmglib.cu:68-123). */
+hmg_status hmg_create(hmg_matrix** out, int n1, int n2, int dim, int bits, void* stream);
+
+/* Copy the coordinates of set 0 or 1: SoA, coords[d*n + i], n = n1 or n2.
+ * on_device != 0: `coords` is a device pointer.  Replaces the caller writing
+ * data.coords_d[set][d] (hmglib_test.cu:68-75).  Synchronous. */
+hmg_status hmg_set_points(hmg_matrix* h, int set, const double* coords, int on_device);
+
+/* Morton codes, Z-order permutation and block-cluster tree.  Replaces
+ * setup_h_matrix (hmglib.cu:125-225).  root levels must be equal (the reference's
+ * drivers set both to 0, paper_benchmark.cu:106-107).  Synchronous. */
+hmg_status hmg_setup(hmg_matrix* h, double eta, int c_leaf, int max_level, int root_level1,
+                     int root_level2, int rule);
+
+/* Select the kernel function.  Replaces create_gaussian_kernel_system_assembler_object
+ * / create_matern_kernel_system_assembler_object (kernel_system_assembler.cu:25-77). */
+hmg_status hmg_set_kernel(hmg_matrix* h, int kind, double param, double regularization);
+
+/* Batched ACA of all admissible blocks.  eps <= 0: the reference's fixed-rank ACA
+ * (rank min(k,m1,m2), sequential row pivots; linear_algebra.cu:3684-4012);
+ * eps > 0: adaptive ACA to relative accuracy eps with rank at most k.  Factors are
+ * stored in `precision`.  Replaces precompute_aca (hmglib.cu:228-236).  Synchronous. */
+hmg_status hmg_precompute_aca(hmg_matrix* h, int k, double eps, int precision);
+
+/* Fill and store all dense blocks in `precision`.  Replaces precompute_dense
+ * (hmglib.cu:239-268).  Synchronous. */
+hmg_status hmg_precompute_dense(hmg_matrix* h, int precision);
+
+/* near field source of hmg_matvec (HMG_NEAR_STORED needs hmg_precompute_dense) */
+hmg_status hmg_set_near_mode(hmg_matrix* h, int mode);
+
+/* y = H x on device vectors in the caller's point order; x is not modified.
+ * Asynchronous on the handle's stream.  Replaces apply_h_matrix_mvp
+ * (hmglib.cu:271-286) and apply_h_matrix_mvp_without_batching (:288-301). */
+hmg_status hmg_matvec(hmg_matrix* h, const double* x, double* y);
+
+/* Same product with host vectors: copies x in, multiplies, copies y out, returns
+ * when y is written.  The copies use a pinned staging buffer of the handle. */
+hmg_status hmg_matvec_host(hmg_matrix* h, const double* x_host, double* y_host);
+
+/* y = K x in FP64 by direct summation on the GPU (no N^2 storage).  Replaces
+ * apply_full_mvp (hmglib.cu:351-401).  Asynchronous on the handle's stream. */
+hmg_status hmg_full_matvec(hmg_matrix* h, const double* x, double* y);
+
+/* FP64 direct sum for a list of rows (caller order indices): y[t] = (K x)[rows[t]].
+ * rows, x, y are device pointers.  Asynchronous. */
+hmg_status hmg_full_matvec_rows(hmg_matrix* h, const double* x, const int* rows, int nrows,
+                                double* y);
+
+/* b_i = prod_d sqrt(pi)/2 (erf(1 - x_id) - erf(-x_id)) for set 0, caller order, device b.
+ * Replaces set_gaussian_kernel_rhs (hmglib.cu:403-439). */
+hmg_status hmg_gaussian_rhs(hmg_matrix* h, double* b);
+
+hmg_status hmg_synchronize(hmg_matrix* h);
+
+/* Per-phase device timing of hmg_matvec (no reference counterpart: the reference's
+ * TIME_* macros are commented out, hmglib.cu:31-34).  on != 0 records CUDA events
+ * between the product's kernels; hmg_get_profile returns the last product's
+ * [gather x, V^T x, tile products, total] in milliseconds (synchronises). */
+hmg_status hmg_set_profiling(hmg_matrix* h, int on);
+hmg_status hmg_get_profile(hmg_matrix* h, double* ms4);
+
+/* Free the handle and all device memory it owns.  Replaces destroy_h_matrix_data
+ * (hmglib.cu:305-348). */
+hmg_status hmg_destroy(hmg_matrix* h);
+
+/* ---- inspection (host copies, synchronous) ---------------------------------- */
+hmg_status hmg_get_info(hmg_matrix* h, hmg_info* info);
+/* Z-ordered (sorted) Morton codes of set 0/1 (the reference's code_d after setup) */
+hmg_status hmg_get_codes(hmg_matrix* h, int set, uint64_t* codes);
+/* order[i] = caller index of Z-ordered point i (the reference's order[set]) */
+hmg_status hmg_get_order(hmg_matrix* h, int set, int64_t* order);
+/* Z-ordered coordinates, SoA coords[d*n+i] (the reference permutes coords_d in place) */
+hmg_status hmg_get_points(hmg_matrix* h, int set, double* coords);
+/* the leaf list in the reference's mat_vec_data order (bounds inclusive, work_item
+ * set1_l/set1_u/set2_l/set2_u/work_type, tree.h:38-55); arrays of block_count */
+hmg_status hmg_get_blocks(hmg_matrix* h, int* s1l, int* s1u, int* s2l, int* s2u, int* type);
+/* per block rank (0 for dense blocks) */
+hmg_status hmg_get_ranks(hmg_matrix* h, int* ranks);
+/* factors of block b as FP64 column-major U (m1 x r) and V (m2 x r) */
+hmg_status hmg_get_factors(hmg_matrix* h, int block, double* U, double* V);
+
+/* ---- primitives (device pointers, asynchronous on `stream`) ----------------- */
+/* stable LSD radix sort of 64-bit keys carrying 32-bit values, in place;
+ * `key_bits` = number of low key bits that can be nonzero (64 if unknown) */
+hmg_status hmg_radix_sort_u64(uint64_t* keys, uint32_t* values, int n, int key_bits,
+                              void* stream);
+/* Morton codes of n points (SoA coords[d*n+i]) with per-dimension min/max
+ * computed on the device (helper.cu:108-138, morton.cu:79-112) */
+hmg_status hmg_morton_codes(const double* coords, int n, int dim, int bits, uint64_t* codes,
+                            void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
