@@ -10,7 +10,7 @@
 //   order1[n1], order2[n2]; int32 blocks[count][5] (set1_l, set1_u, set2_l, set2_u,
 //   work_type); float64 y_h[n1] (apply_h_matrix_mvp), y_full[n1] (apply_full_mvp);
 //   float64 timings_ms[5]: setup, precompute_aca, precompute_dense, apply (median),
-//   apply_full.
+//   apply_full; float64 y_h2[n1]: the product after a second precompute_aca.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -132,6 +132,17 @@ int main(int argc, char** argv)
     cudaEventRecord(e1);
     t[4] = elapsed(e0, e1);
     cudaMemcpy(yf.data(), dyf, sizeof(double) * n1, cudaMemcpyDeviceToHost);
+    // a second, independent ACA of the same H-matrix and product: shows the
+    // run-to-run variation of the reference's own result
+    cudaFree(data.U);
+    cudaFree(data.V);
+    data.U = data.V = 0;
+    precompute_aca(&data);
+    cudaMemcpy(dx, x.data(), sizeof(double) * n2, cudaMemcpyHostToDevice);
+    cudaMemset(dy, 0, sizeof(double) * n1);
+    apply_h_matrix_mvp(dx, dy, &data);
+    std::vector<double> yh2(n1);
+    cudaMemcpy(yh2.data(), dy, sizeof(double) * n1, cudaMemcpyDeviceToHost);
     cudaError_t err = cudaGetLastError();
 
     FILE* o = fopen(argv[2], "wb");
@@ -149,6 +160,7 @@ int main(int argc, char** argv)
     fwrite(yh.data(), 8, n1, o);
     fwrite(yf.data(), 8, n1, o);
     fwrite(t, 8, 5, o);
+    fwrite(yh2.data(), 8, n1, o);
     fclose(o);
     printf("{\"n1\": %d, \"n2\": %d, \"blocks\": %d, \"dense\": %d, \"aca\": %d, \"setup_ms\": %.3f, "
            "\"precompute_aca_ms\": %.3f, \"precompute_dense_ms\": %.3f, \"apply_ms\": %.3f, "

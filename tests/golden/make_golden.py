@@ -48,8 +48,12 @@ CASES = {
                            c_leaf=64, eta=1.5, k=64, pre_dense=1, n_apply=5),
     "uniform3d_matern": dict(n1=8192, dim=3, gen="uniform", seed=5, scale=1.0, kernel=2,
                              c_leaf=64, eta=1.5, k=16, pre_dense=1, n_apply=3),
+    # The reference's own build fails on this clustered set: setup_h_matrix exits with
+    # "cudaMemcpy12ja: invalid argument" -- single-point clusters (levels 6 and 8 here)
+    # collide in its bounding-box lookup keys (tree.cu:1004-1022, 1061-1063).  Kept
+    # so the failure can be reproduced; no fixture is packed for it.
     "gmm2d": dict(n1=4096, dim=2, gen="gmm", seed=2, scale=0.05 ** -0.5, kernel=1,
-                  c_leaf=32, eta=1.0, k=16, pre_dense=0, n_apply=3),
+                  c_leaf=32, eta=1.0, k=16, pre_dense=0, n_apply=3, reference_fails=True),
     "rect2d": dict(n1=1000, n2=700, dim=2, gen="uniform", seed=11, seed2=12, scale=3.0, kernel=1,
                    c_leaf=16, eta=0.8, k=8, pre_dense=1, n_apply=3),
     "lattice_dups": dict(n1=2048, dim=2, gen="lattice", nx=32, dup=2, scale=1.0 / 8.0, kernel=1,
@@ -112,9 +116,12 @@ def read_output(path):
     blocks = take(np.int32, nb * 5).reshape(nb, 5)
     yh = take(np.float64, n1); yf = take(np.float64, n1)
     t = take(np.float64, 5)
-    return dict(codes1=codes1, codes2=codes2, order1=order1.astype(np.int64),
-                order2=order2.astype(np.int64), blocks=blocks, dense_count=np.int32(nd),
-                y_h=yh, y_full=yf, timings_ms=t)
+    d = dict(codes1=codes1, codes2=codes2, order1=order1.astype(np.int64),
+             order2=order2.astype(np.int64), blocks=blocks, dense_count=np.int32(nd),
+             y_h=yh, y_full=yf, timings_ms=t)
+    if len(raw) - o >= 8 * n1:
+        d["y_h2"] = take(np.float64, n1)  # a second precompute_aca + product
+    return d
 
 
 def cmd_run(a):

@@ -53,7 +53,7 @@ def test_setup_bit_exact_vs_oracle(hmg, oracle, cuda, case):
     _check_against_oracle(hmg, oracle, *case)
 
 
-GOLDEN = ["config1_parity", "uniform3d_matern", "gmm2d", "rect2d", "lattice_dups",
+GOLDEN = ["config1_parity", "uniform3d_matern", "rect2d", "lattice_dups",
           "kat_lattice2d", "kat_lattice3d"]
 
 
