@@ -66,6 +66,7 @@ _PROTOS = {
     "hmg_synchronize": (C.c_int, [_vp]),
     "hmg_set_profiling": (C.c_int, [_vp, C.c_int]),
     "hmg_get_profile": (C.c_int, [_vp, _vp]),
+    "hmg_set_matvec_variant": (C.c_int, [_vp, C.c_int]),
     "hmg_destroy": (C.c_int, [_vp]),
     "hmg_get_info": (C.c_int, [_vp, C.POINTER(Info)]),
     "hmg_get_codes": (C.c_int, [_vp, C.c_int, _vp]),

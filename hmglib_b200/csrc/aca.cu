@@ -321,6 +321,8 @@ void free_far(hmg_matrix* h)
     dfree(h->ptrU, s);
     dfree(h->ptrV, s);
     dfree(h->tbuf, s);
+    dfree(h->far_list, s);
+    h->nfar_list = 0;
     h->far_prec = -1;
     h->desc_near_mode = -1;
     h->rank_total = h->far_entries = h->far_rows = h->far_stored = 0;
@@ -478,8 +480,9 @@ hmg_status run_aca(hmg_matrix* h, int k, double eps, int precision)
     h->rank_total = roff[nb];
     HMG_CUDA_TRY(cudaMemcpyAsync(h->rank, rank.data(), sizeof(int) * nb, cudaMemcpyHostToDevice, s));
     HMG_CUDA_TRY(cudaMemcpyAsync(h->rank_off, roff.data(), sizeof(long long) * (nb + 1), cudaMemcpyHostToDevice, s));
-    if ((st = dalloc((char**)&h->tbuf, (size_t)(h->rank_total > 0 ? h->rank_total : 1) * 8, s)))
-        return st;
+    // padded and zeroed: the streaming product copies 16-byte-aligned supersets of t_b
+    if ((st = dalloc((char**)&h->tbuf, (size_t)(h->rank_total + 32) * 8, s))) return st;
+    HMG_CUDA_TRY(cudaMemsetAsync(h->tbuf, 0, (size_t)(h->rank_total + 32) * 8, s));
     HMG_CUDA_TRY(cudaStreamSynchronize(s));
     h->h_rank = rank;
     h->far_prec = precision;

@@ -38,6 +38,8 @@ static void free_matrix_buffers(hmg_matrix* h)
     dfree(h->xs64, s); dfree(h->xs32, s);
     dfree(h->pair_desc, s);
     dfree(h->k1_units, s);
+    dfree(h->far_list, s);
+    dfree(h->dev_err, s);
     dfree(h->dev_x, s); dfree(h->dev_y, s);
     if (h->host_x) cudaFreeHost(h->host_x);
     if (h->host_y) cudaFreeHost(h->host_y);
@@ -66,7 +68,8 @@ hmg_status hmg_create(hmg_matrix** out, int n1, int n2, int dim, int bits, void*
         delete h;
         return HMG_ERR_CUDA;
     }
-    hmg_status st = HMG_OK;
+    hmg_status st = dalloc(&h->dev_err, 4, h->stream);  // [0] error flag, [1],[2] work counters
+    if (!st && cudaMemsetAsync(h->dev_err, 0, 4 * sizeof(int), h->stream) != cudaSuccess) st = HMG_ERR_CUDA;
     for (int i = 0; i < 2 && !st; i++) {
         size_t n = (size_t)h->n[i];
         if ((st = dalloc(&h->pts[i], n * dim, h->stream)) || (st = dalloc(&h->zpts[i], n * dim, h->stream)) ||
@@ -212,6 +215,8 @@ hmg_status hmg_matvec(hmg_matrix* h, const double* x, double* y)
     return matvec_device(h, x, y);
 }
 
+static hmg_status check_pipeline(hmg_matrix* h);
+
 hmg_status hmg_matvec_host(hmg_matrix* h, const double* x_host, double* y_host)
 {
     HMG_REQUIRE(h && x_host && y_host, HMG_ERR_INVALID, "hmg_matvec_host: NULL argument");
@@ -228,7 +233,7 @@ hmg_status hmg_matvec_host(hmg_matrix* h, const double* x_host, double* y_host)
     HMG_CUDA_TRY(cudaMemcpyAsync(h->dev_x, h->host_x, sizeof(double) * h->n[1], cudaMemcpyHostToDevice, s));
     if ((st = matvec_device(h, h->dev_x, h->dev_y))) return st;
     HMG_CUDA_TRY(cudaMemcpyAsync(h->host_y, h->dev_y, sizeof(double) * h->n[0], cudaMemcpyDeviceToHost, s));
-    HMG_CUDA_TRY(cudaStreamSynchronize(s));
+    if ((st = check_pipeline(h))) return st;
     memcpy(y_host, h->host_y, sizeof(double) * h->n[0]);
     return HMG_OK;
 }
@@ -257,10 +262,33 @@ hmg_status hmg_gaussian_rhs(hmg_matrix* h, double* b)
     return gaussian_rhs(h, b);
 }
 
+// A streaming kernel whose shared-memory pipeline waited longer than its budget
+// records a code in the handle's device flag instead of spinning; report it once.
+static hmg_status check_pipeline(hmg_matrix* h)
+{
+    int e = 0;
+    HMG_CUDA_TRY(cudaMemcpyAsync(&e, h->dev_err, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+    HMG_CUDA_TRY(cudaStreamSynchronize(h->stream));
+    if (e) {
+        HMG_CUDA_TRY(cudaMemsetAsync(h->dev_err, 0, sizeof(int), h->stream));
+        set_error("a product kernel's shared-memory pipeline timed out (code %d); result invalid", e);
+        return HMG_ERR_CUDA;
+    }
+    return HMG_OK;
+}
+
 hmg_status hmg_synchronize(hmg_matrix* h)
 {
     HMG_REQUIRE(h, HMG_ERR_INVALID, "hmg_synchronize: NULL handle");
     HMG_CUDA_TRY(cudaStreamSynchronize(h->stream));
+    return check_pipeline(h);
+}
+
+hmg_status hmg_set_matvec_variant(hmg_matrix* h, int variant)
+{
+    HMG_REQUIRE(h, HMG_ERR_INVALID, "hmg_set_matvec_variant: NULL handle");
+    HMG_REQUIRE(variant == 0 || variant == 1, HMG_ERR_INVALID, "hmg_set_matvec_variant: variant must be 0 or 1");
+    h->matvec_variant = variant;
     return HMG_OK;
 }
 

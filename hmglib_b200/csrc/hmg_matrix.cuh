@@ -78,6 +78,11 @@ struct hmg_matrix {
     int desc_near_mode = -1, desc_near_prec = -2, desc_far_prec = -2;
     void* k1_units = nullptr;      // (block, first row, end row) pieces of V^T
     int nk1 = 0;
+    int* far_list = nullptr;       // admissible blocks with rank > 0 (streaming V^T x)
+    int nfar_list = 0;
+    int* dev_err = nullptr;        // pipeline wait time-out flag (0 = fine)
+    int matvec_variant = 0;        // 0: streaming kernels where applicable, 1: simple kernels
+    int last_variant_k1 = -1, last_variant_k2 = -1;
     double* host_x = nullptr; // pinned staging
     double* host_y = nullptr;
     double* dev_x = nullptr;

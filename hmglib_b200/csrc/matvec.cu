@@ -19,19 +19,9 @@
 #include <vector>
 
 #include "hmg_matrix.cuh"
+#include "stream.cuh"
 
 namespace hmg {
-
-enum { PAIR_STORED = 0, PAIR_FAR = 1, PAIR_ONTHEFLY = 2 };
-
-struct PairDesc {
-    const void* data;  // tile slice (column-major, s_pad rows) or nullptr (on the fly)
-    const void* w;     // vector multiplied: x_b (dense) or t_b (low rank), storage type
-    int ncol;          // m2 (dense) or rank (low rank)
-    int kind;          // PAIR_*
-    int c0;            // first column (on the fly)
-    int pad;
-};
 
 struct K1Unit {
     int b, l0, l1, pad;
@@ -210,6 +200,15 @@ static hmg_status ensure_desc(hmg_matrix* h, int elem)
     if (!units.empty())
         HMG_CUDA_TRY(cudaMemcpyAsync(du, units.data(), sizeof(K1Unit) * units.size(), cudaMemcpyHostToDevice, s));
     h->k1_units = du;
+    // the streaming V^T x kernel works on whole blocks
+    dfree(h->far_list, s);
+    std::vector<int> fl;
+    for (int b = h->ndense; b < h->nblocks; b++)
+        if (h->h_rank[b] > 0) fl.push_back(b);
+    h->nfar_list = (int)fl.size();
+    if ((st = dalloc(&h->far_list, fl.size() > 0 ? fl.size() : 1, s))) return st;
+    if (!fl.empty())
+        HMG_CUDA_TRY(cudaMemcpyAsync(h->far_list, fl.data(), sizeof(int) * fl.size(), cudaMemcpyHostToDevice, s));
     HMG_CUDA_TRY(cudaStreamSynchronize(s));
     h->desc_near_mode = h->near_mode;
     h->desc_near_prec = h->near_prec;
@@ -368,14 +367,25 @@ __global__ void __launch_bounds__(256) k_tile_matvec(const PairDesc* desc, const
     }
 }
 
+// Z-ordered x in FP64 and FP32, padded and zeroed: the streaming kernels copy
+// 16-byte-aligned supersets of x pieces.
+static hmg_status ensure_xs(hmg_matrix* h)
+{
+    if (h->xs64) return HMG_OK;
+    cudaStream_t s = h->stream;
+    hmg_status st;
+    const size_t n = (size_t)h->n[1] + 32;
+    if ((st = dalloc(&h->xs64, n, s)) || (st = dalloc(&h->xs32, n, s))) return st;
+    HMG_CUDA_TRY(cudaMemsetAsync(h->xs64, 0, sizeof(double) * n, s));
+    HMG_CUDA_TRY(cudaMemsetAsync(h->xs32, 0, sizeof(float) * n, s));
+    return HMG_OK;
+}
+
 hmg_status matvec_device(hmg_matrix* h, const double* x, double* y)
 {
     cudaStream_t s = h->stream;
     hmg_status st;
-    if (!h->xs64) {
-        if ((st = dalloc(&h->xs64, (size_t)h->n[1], s)) || (st = dalloc(&h->xs32, (size_t)h->n[1], s)))
-            return st;
-    }
+    if ((st = ensure_xs(h))) return st;
     const bool fp64 = h->far_prec == HMG_PREC_FP64 ||
                       (h->naca == 0 && h->near_prec != HMG_PREC_FP32);
     if (h->near_mode == HMG_NEAR_STORED && h->naca > 0 && h->near_prec != h->far_prec) {
@@ -390,7 +400,13 @@ hmg_status matvec_device(hmg_matrix* h, const double* x, double* y)
     k_gather_x<<<ceil_div(h->n[1], 256), 256, 0, s>>>(x, h->perm[1], h->n[1], h->xs64, h->xs32);
     HMG_LAUNCH_CHECK();
     if (h->profiling) HMG_CUDA_TRY(cudaEventRecord(h->ev[1], s));
-    if (h->nk1 > 0) {
+    const bool bulk_k1 = h->matvec_variant == 0 && h->max_rank <= K1_MAXRANK;
+    const bool bulk_k2 = h->matvec_variant == 0 && (h->near_mode == HMG_NEAR_STORED || h->ndense == 0);
+    h->last_variant_k1 = bulk_k1 ? 0 : 1;
+    h->last_variant_k2 = bulk_k2 ? 0 : 1;
+    if (bulk_k1 && h->nfar_list > 0) {
+        if ((st = launch_vtx_bulk(h, fp64))) return st;
+    } else if (h->nk1 > 0) {
         int grid = std::min(ceil_div(h->nk1, 8), 148 * 8);
         if (fp64)
             k_vtx<double><<<grid, 256, 0, s>>>((const K1Unit*)h->k1_units, h->nk1, h->blk_c0, h->blk_m2,
@@ -403,7 +419,9 @@ hmg_status matvec_device(hmg_matrix* h, const double* x, double* y)
         HMG_LAUNCH_CHECK();
     }
     if (h->profiling) HMG_CUDA_TRY(cudaEventRecord(h->ev[2], s));
-    if (h->ntiles > 0) {
+    if (h->ntiles > 0 && bulk_k2) {
+        if ((st = launch_tiles_bulk(h, fp64, y))) return st;
+    } else if (h->ntiles > 0) {
         if (fp64)
             k_tile_matvec<double><<<h->ntiles, 256, 0, s>>>((const PairDesc*)h->pair_desc, h->tile_pair_start,
                                                             h->tile_r0, h->tile_s, h->perm[0], h->kspec, P,
@@ -470,10 +488,7 @@ hmg_status direct_matvec(hmg_matrix* h, const double* x, const int* rows, int nr
 {
     cudaStream_t s = h->stream;
     hmg_status st;
-    if (!h->xs64) {
-        if ((st = dalloc(&h->xs64, (size_t)h->n[1], s)) || (st = dalloc(&h->xs32, (size_t)h->n[1], s)))
-            return st;
-    }
+    if ((st = ensure_xs(h))) return st;
     k_gather_x<<<ceil_div(h->n[1], 256), 256, 0, s>>>(x, h->perm[1], h->n[1], h->xs64, h->xs32);
     HMG_LAUNCH_CHECK();
     PointsView P = points_view(h);

@@ -75,7 +75,9 @@ __global__ void k_morton(const double* coords, int n, int dim, int bits,
         double hi = order_key_inv(mx_key[d]);
         double range = hi - lo;
         double t = (coords[(size_t)d * n + i] - lo) / range;
-        uint64_t q = (uint64_t)floor(t * scale);  // NaN -> 0, like the reference's device code
+        // same conversion as the reference's device code: a NaN quotient (max == min)
+        // converts to the top of the range and is capped below
+        uint64_t q = (uint64_t)floor(t * scale);
         q = q < cap ? q : cap;
         for (int b = 0; b < bits; b++) code |= ((q >> b) & 1ull) << (b * dim + d);
     }

@@ -117,6 +117,10 @@ class HMatrix:
     def synchronize(self):
         self._call("hmg_synchronize")
 
+    def set_matvec_variant(self, variant: int):
+        """0: streaming (bulk-copy) product kernels, 1: plain-load kernels."""
+        self._call("hmg_set_matvec_variant", int(variant))
+
     def set_profiling(self, on: bool = True):
         self._call("hmg_set_profiling", 1 if on else 0)
 

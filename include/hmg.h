@@ -135,6 +135,12 @@ hmg_status hmg_synchronize(hmg_matrix* h);
 hmg_status hmg_set_profiling(hmg_matrix* h, int on);
 hmg_status hmg_get_profile(hmg_matrix* h, double* ms4);
 
+/* Product kernels (no reference counterpart): 0 (default) streams stored slices
+ * through shared memory with bulk asynchronous copies; 1 uses plain vector loads
+ * (also used automatically for on-the-fly near fields and ranks above 128).  Both
+ * give the same result to FP64 rounding. */
+hmg_status hmg_set_matvec_variant(hmg_matrix* h, int variant);
+
 /* Free the handle and all device memory it owns.  Replaces destroy_h_matrix_data
  * (hmglib.cu:305-348). */
 hmg_status hmg_destroy(hmg_matrix* h);

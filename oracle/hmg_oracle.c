@@ -35,14 +35,17 @@ void orc_minmax(const double* coords, int n, int dim, double* mn, double* mx)
     }
 }
 
-/* morton.cu:71-75 (coord_to_fp).  A NaN quotient (max==min) converts to 0, which
- * is what the device conversion cvt.rzi.u64.f64 yields for NaN. */
+/* morton.cu:71-75 (coord_to_fp).  A NaN quotient (a dimension with max == min)
+ * converts to the largest fixed-point value, as the device conversion of the
+ * reference's `(uint64_t)floor(NaN)` does on sm_100 (observed on a B200). */
 static uint64_t coord_to_fixed(double c, double lo, double range, int bits)
 {
     double t = (c - lo) / range;
     double f = floor(t * (double)(1ull << bits));
     uint64_t q;
-    if (f != f || f <= 0.0)
+    if (f != f)
+        q = ~0ull;
+    else if (f <= 0.0)
         q = 0;
     else if (f >= 18446744073709551616.0)
         q = ~0ull;

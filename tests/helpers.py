@@ -12,6 +12,10 @@ def make_points(gen, n, dim, seed, scale=1.0):
         p = synth.uniform_points(n, dim, seed)
     elif gen == "gmm":
         p = synth.gmm_points(n, dim, seed)
+    elif gen == "line":
+        # all points share every coordinate but the first (max == min in those dimensions)
+        p = np.full((dim, n), 0.5)
+        p[0] = synth.uniform01(seed, n)
     elif gen == "lattice":
         nx = int(round(n ** (1.0 / dim)))
         g = np.stack(np.meshgrid(*[np.arange(nx, dtype=np.float64)] * dim, indexing="ij"), 0)

@@ -20,6 +20,7 @@ CASES = [
     ("lattice", 4096, 4096, 2, 0, 1.0, 8, 0),
     ("lattice", 3375, 3375, 3, 0, 1.5, 10, 0),
     ("uniform", 50, 50, 3, 3, 1.5, 64, 0),     # a single dense block
+    ("line", 5000, 5000, 3, 5, 1.5, 16, 0),    # degenerate dimensions (max == min)
     ("uniform", 1, 1, 2, 4, 1.5, 1, 0),        # one point
 ]
 
