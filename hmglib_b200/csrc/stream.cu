@@ -43,7 +43,21 @@ struct StageMeta {
     int last;   // last stage of a pair (K2) / last column piece of these rows (K1)
     int s;      // tile rows (K2) / first row (K1)
     int r0;     // first Z row of the tile (K2) / rows in the stage (K1)
+    long long ro;  // (K1) offset of the block's t_b
 };
+
+__device__ __forceinline__ PairDesc shfl_desc(const PairDesc& d, int k)
+{
+    PairDesc o;
+    o.data = reinterpret_cast<const void*>(
+        __shfl_sync(0xffffffffu, reinterpret_cast<unsigned long long>(d.data), k));
+    o.w = reinterpret_cast<const void*>(__shfl_sync(0xffffffffu, reinterpret_cast<unsigned long long>(d.w), k));
+    o.ncol = __shfl_sync(0xffffffffu, d.ncol, k);
+    o.kind = __shfl_sync(0xffffffffu, d.kind, k);
+    o.c0 = 0;
+    o.pad = 0;
+    return o;
+}
 
 template <typename T>
 __device__ __forceinline__ void load4(const T* p, double* v);
@@ -111,54 +125,91 @@ k_tiles_bulk(const PairDesc* __restrict__ desc, const int* __restrict__ tile_pai
     __syncthreads();
 
     if (warp == NCW) {
-        if (lane != 0) return;
+        // The whole producer warp fetches descriptors (32 at a time, the next batch
+        // while the current one is issued) and the next tile index; lane 0 alone
+        // arms the barriers and issues the copies.
         Ring ring;
-        // tiles are handed out dynamically (err[1] counts them; zeroed before launch)
-        for (int t = atomicAdd(err + 1, 1); t < ntiles; t = atomicAdd(err + 1, 1)) {
+        int t = lane == 0 ? atomicAdd(err + 1, 1) : 0;
+        t = __shfl_sync(0xffffffffu, t, 0);
+        while (t < ntiles) {
+            int tn = lane == 0 ? atomicAdd(err + 1, 1) : 0;  // tiles are handed out dynamically
             const int s_rows = tile_s[t], sp = (s_rows + 3) & ~3, tr0 = tile_r0[t];
             const int colbytes = sp * (int)sizeof(T);
             const int cpc = min(K2_MAXCOLS, STAGE_BYTES / colbytes);
-            const int pe = tile_pair_start[t + 1];
-            for (int p = tile_pair_start[t]; p < pe; p++) {
-                const PairDesc d = desc[p];
-                for (int c0 = 0; c0 < d.ncol; c0 += cpc) {
-                    const int nc = min(cpc, d.ncol - c0);
-                    const int s = ring.acquire(empty, err);
-                    if (s < 0) { drain(full, ring.it, err); return; }
-                    const uintptr_t a = reinterpret_cast<uintptr_t>(static_cast<const T*>(d.w) + c0);
-                    const uintptr_t a16 = a & ~(uintptr_t)15;
-                    const unsigned woffb = (unsigned)(a - a16);
-                    const unsigned wbytes = (woffb + nc * (unsigned)sizeof(T) + 15u) & ~15u;
+            const int pb = tile_pair_start[t], pe = tile_pair_start[t + 1];
+            PairDesc cur = pb + lane < pe ? desc[pb + lane] : PairDesc{};
+            for (int p0 = pb; p0 < pe; p0 += 32) {
+                PairDesc nxt = p0 + 32 + lane < pe ? desc[p0 + 32 + lane] : PairDesc{};
+                const int n = min(32, pe - p0);
+                for (int k = 0; k < n; k++) {
+                    const PairDesc d = shfl_desc(cur, k);
+                    for (int c0 = 0; c0 < d.ncol; c0 += cpc) {
+                        const int nc = min(cpc, d.ncol - c0);
+                        int ok = 1;
+                        if (lane == 0) {
+                            const int s = ring.acquire(empty, err);
+                            if (s < 0) {
+                                ok = 0;
+                            } else {
+                                const uintptr_t a = reinterpret_cast<uintptr_t>(static_cast<const T*>(d.w) + c0);
+                                const uintptr_t a16 = a & ~(uintptr_t)15;
+                                const unsigned woffb = (unsigned)(a - a16);
+                                const unsigned wbytes = (woffb + nc * (unsigned)sizeof(T) + 15u) & ~15u;
+                                StageMeta m;
+                                m.kind = ST_DATA; m.unit = t; m.nc = nc; m.sp = sp;
+                                m.woff = (int)(woffb / sizeof(T)); m.last = (c0 + nc >= d.ncol);
+                                m.s = s_rows; m.r0 = tr0; m.ro = 0;
+                                meta[s] = m;
+                                const unsigned dbytes = (unsigned)(nc * colbytes);
+                                mbar_arrive_expect_tx(&full[s], dbytes + wbytes);
+                                bulk_g2s(data + (size_t)s * STAGE_BYTES,
+                                         static_cast<const char*>(d.data) + (size_t)c0 * colbytes, dbytes, &full[s]);
+                                bulk_g2s(wbuf + (size_t)s * K2_WBYTES, reinterpret_cast<const void*>(a16), wbytes,
+                                         &full[s]);
+                            }
+                        }
+                        ok = __shfl_sync(0xffffffffu, ok, 0);
+                        if (!ok) {
+                            if (lane == 0) drain(full, ring.it, err);
+                            return;
+                        }
+                        ring.it++;
+                    }
+                }
+                cur = nxt;
+            }
+            int ok = 1;
+            if (lane == 0) {
+                const int s = ring.acquire(empty, err);
+                if (s < 0) {
+                    ok = 0;
+                } else {
                     StageMeta m;
-                    m.kind = ST_DATA; m.unit = t; m.nc = nc; m.sp = sp;
-                    m.woff = (int)(woffb / sizeof(T)); m.last = (c0 + nc >= d.ncol);
-                    m.s = s_rows; m.r0 = tr0;
+                    m.kind = ST_END; m.unit = t; m.nc = 0; m.sp = sp; m.woff = 0; m.last = 0;
+                    m.s = s_rows; m.r0 = tr0; m.ro = 0;
                     meta[s] = m;
-                    const unsigned dbytes = (unsigned)(nc * colbytes);
-                    mbar_arrive_expect_tx(&full[s], dbytes + wbytes);
-                    bulk_g2s(data + (size_t)s * STAGE_BYTES,
-                             static_cast<const char*>(d.data) + (size_t)c0 * colbytes, dbytes, &full[s]);
-                    bulk_g2s(wbuf + (size_t)s * K2_WBYTES, reinterpret_cast<const void*>(a16), wbytes, &full[s]);
-                    ring.it++;
+                    mbar_arrive(&full[s]);
                 }
             }
+            ok = __shfl_sync(0xffffffffu, ok, 0);
+            if (!ok) {
+                if (lane == 0) drain(full, ring.it, err);
+                return;
+            }
+            ring.it++;
+            t = __shfl_sync(0xffffffffu, tn, 0);
+        }
+        if (lane == 0) {
             const int s = ring.acquire(empty, err);
             if (s < 0) { drain(full, ring.it, err); return; }
-            StageMeta m;
-            m.kind = ST_END; m.unit = t; m.nc = 0; m.sp = sp; m.woff = 0; m.last = 0;
-            m.s = s_rows; m.r0 = tr0;
-            meta[s] = m;
+            meta[s].kind = ST_DONE;
             mbar_arrive(&full[s]);
-            ring.it++;
         }
-        const int s = ring.acquire(empty, err);
-        if (s < 0) { drain(full, ring.it, err); return; }
-        meta[s].kind = ST_DONE;
-        mbar_arrive(&full[s]);
         return;
     }
 
-    // consumers: lane owns padded rows 4*lane .. 4*lane+3 of the tile
+    // consumers: lane owns padded rows 4*lane .. 4*lane+3 of the tile; a warp takes
+    // columns warp, warp+8, ... of each stage, two at a time (independent chains)
     const int row0 = lane * 4;
     double acc[4] = {0.0, 0.0, 0.0, 0.0};
     double part[4] = {0.0, 0.0, 0.0, 0.0};
@@ -185,13 +236,28 @@ k_tiles_bulk(const PairDesc* __restrict__ desc, const int* __restrict__ tile_pai
             const T* buf = reinterpret_cast<const T*>(data + (size_t)s * STAGE_BYTES);
             const T* w = reinterpret_cast<const T*>(wbuf + (size_t)s * K2_WBYTES) + m.woff;
             if (row0 < m.sp) {
-                for (int j = warp; j < m.nc; j += NCW) {
+                double p2[4] = {0.0, 0.0, 0.0, 0.0};
+                int j = warp;
+                for (; j + NCW < m.nc; j += 2 * NCW) {
+                    double v[4], u[4];
+                    load4<T>(buf + (size_t)j * m.sp + row0, v);
+                    load4<T>(buf + (size_t)(j + NCW) * m.sp + row0, u);
+                    const double wj = (double)w[j], wk = (double)w[j + NCW];
+#pragma unroll
+                    for (int q = 0; q < 4; q++) {
+                        part[q] = fma(v[q], wj, part[q]);
+                        p2[q] = fma(u[q], wk, p2[q]);
+                    }
+                }
+                if (j < m.nc) {
                     double v[4];
                     load4<T>(buf + (size_t)j * m.sp + row0, v);
                     const double wj = (double)w[j];
 #pragma unroll
                     for (int q = 0; q < 4; q++) part[q] = fma(v[q], wj, part[q]);
                 }
+#pragma unroll
+                for (int q = 0; q < 4; q++) part[q] += p2[q];
             }
             if (m.last) {
 #pragma unroll
@@ -237,54 +303,94 @@ k_vtx_bulk(const int* __restrict__ blocks, int nblocks, const int* __restrict__ 
     __syncthreads();
 
     if (warp == NCW) {
-        if (lane != 0) return;
+        // Blocks are handed out 32 at a time (err[2], zeroed before launch; coarse
+        // levels come first in the list).  The producer warp loads the 32 blocks'
+        // geometry in one go and the next chunk index ahead of time; lane 0 issues.
         Ring ring;
-        // blocks are handed out dynamically, largest levels first (err[2]; zeroed before launch)
-        for (int u = atomicAdd(err + 2, 1); u < nblocks; u = atomicAdd(err + 2, 1)) {
-            const int b = blocks[u];
-            const int r = rank[b], m2 = blk_m2[b], m2p = (m2 + 3) & ~3, c0 = blk_c0[b];
-            const T* V = ptrV[b];
-            const bool whole = m2p <= CW;
-            const int cw = whole ? m2p : CW;
-            // rows per stage: whole rows when they are short, else 8 pieces of CW
-            const int rps = whole ? max(1, min(r, STAGE_BYTES / (m2p * (int)sizeof(T)))) : 8;
-            for (int l0 = 0; l0 < r; l0 += rps) {
-                const int nr = min(rps, r - l0);
-                for (int j0 = 0; j0 < m2p; j0 += cw) {
-                    const int nc = min(cw, m2p - j0);
-                    const int s = ring.acquire(empty, err);
-                    if (s < 0) { drain(full, ring.it, err); return; }
-                    const uintptr_t a = reinterpret_cast<uintptr_t>(xs + c0 + j0);
-                    const uintptr_t a16 = a & ~(uintptr_t)15;
-                    const unsigned woffb = (unsigned)(a - a16);
-                    const unsigned wbytes = (woffb + nc * (unsigned)sizeof(T) + 15u) & ~15u;
-                    StageMeta m;
-                    m.kind = ST_DATA; m.unit = b; m.nc = nc; m.sp = whole ? m2p : nc;
-                    m.woff = (int)(woffb / sizeof(T)); m.last = (j0 + nc >= m2p);
-                    m.s = l0; m.r0 = nr;
-                    meta[s] = m;
-                    const unsigned rowbytes = (unsigned)(nc * sizeof(T));
-                    mbar_arrive_expect_tx(&full[s], rowbytes * nr + wbytes);
-                    unsigned char* dst = data + (size_t)s * STAGE_BYTES;
-                    if (whole) {
-                        bulk_g2s(dst, V + (size_t)l0 * m2p, rowbytes * nr, &full[s]);
-                    } else {
-                        for (int i = 0; i < nr; i++)
-                            bulk_g2s(dst + (size_t)i * rowbytes, V + (size_t)(l0 + i) * m2p + j0, rowbytes, &full[s]);
+        int base = lane == 0 ? atomicAdd(err + 2, 32) : 0;
+        base = __shfl_sync(0xffffffffu, base, 0);
+        while (base < nblocks) {
+            int nbase = lane == 0 ? atomicAdd(err + 2, 32) : 0;
+            int mb = -1, mr = 0, mm2 = 0, mc0 = 0;
+            long long mro = 0;
+            unsigned long long mV = 0;
+            if (base + lane < nblocks) {
+                mb = blocks[base + lane];
+                mr = rank[mb];
+                mm2 = blk_m2[mb];
+                mc0 = blk_c0[mb];
+                mro = rank_off[mb];
+                mV = reinterpret_cast<unsigned long long>(ptrV[mb]);
+            }
+            const int n = min(32, nblocks - base);
+            for (int k = 0; k < n; k++) {
+                const int b = __shfl_sync(0xffffffffu, mb, k);
+                const int r = __shfl_sync(0xffffffffu, mr, k);
+                const int m2 = __shfl_sync(0xffffffffu, mm2, k);
+                const int c0 = __shfl_sync(0xffffffffu, mc0, k);
+                const long long ro = __shfl_sync(0xffffffffu, mro, k);
+                const T* V = reinterpret_cast<const T*>(__shfl_sync(0xffffffffu, mV, k));
+                const int m2p = (m2 + 3) & ~3;
+                const bool whole = m2p <= CW;
+                const int cw = whole ? m2p : CW;
+                // rows per stage: whole rows when they are short, else 8 pieces of CW
+                const int rps = whole ? max(1, min(r, STAGE_BYTES / (m2p * (int)sizeof(T)))) : 8;
+                for (int l0 = 0; l0 < r; l0 += rps) {
+                    const int nr = min(rps, r - l0);
+                    for (int j0 = 0; j0 < m2p; j0 += cw) {
+                        const int nc = min(cw, m2p - j0);
+                        int ok = 1;
+                        if (lane == 0) {
+                            const int s = ring.acquire(empty, err);
+                            if (s < 0) {
+                                ok = 0;
+                            } else {
+                                const uintptr_t a = reinterpret_cast<uintptr_t>(xs + c0 + j0);
+                                const uintptr_t a16 = a & ~(uintptr_t)15;
+                                const unsigned woffb = (unsigned)(a - a16);
+                                const unsigned wbytes = (woffb + nc * (unsigned)sizeof(T) + 15u) & ~15u;
+                                StageMeta m;
+                                m.kind = ST_DATA; m.unit = b; m.nc = nc; m.sp = whole ? m2p : nc;
+                                m.woff = (int)(woffb / sizeof(T)); m.last = (j0 + nc >= m2p);
+                                m.s = l0; m.r0 = nr; m.ro = ro;
+                                meta[s] = m;
+                                const unsigned rowbytes = (unsigned)(nc * sizeof(T));
+                                mbar_arrive_expect_tx(&full[s], rowbytes * nr + wbytes);
+                                unsigned char* dst = data + (size_t)s * STAGE_BYTES;
+                                if (whole) {
+                                    bulk_g2s(dst, V + (size_t)l0 * m2p, rowbytes * nr, &full[s]);
+                                } else {
+                                    for (int i = 0; i < nr; i++)
+                                        bulk_g2s(dst + (size_t)i * rowbytes, V + (size_t)(l0 + i) * m2p + j0, rowbytes,
+                                                 &full[s]);
+                                }
+                                bulk_g2s(wbuf + (size_t)s * K1_WBYTES, reinterpret_cast<const void*>(a16), wbytes,
+                                         &full[s]);
+                            }
+                        }
+                        ok = __shfl_sync(0xffffffffu, ok, 0);
+                        if (!ok) {
+                            if (lane == 0) drain(full, ring.it, err);
+                            return;
+                        }
+                        ring.it++;
                     }
-                    bulk_g2s(wbuf + (size_t)s * K1_WBYTES, reinterpret_cast<const void*>(a16), wbytes, &full[s]);
-                    ring.it++;
                 }
             }
+            base = __shfl_sync(0xffffffffu, nbase, 0);
         }
-        const int s = ring.acquire(empty, err);
-        if (s < 0) { drain(full, ring.it, err); return; }
-        meta[s].kind = ST_DONE;
-        mbar_arrive(&full[s]);
+        if (lane == 0) {
+            const int s = ring.acquire(empty, err);
+            if (s < 0) { drain(full, ring.it, err); return; }
+            meta[s].kind = ST_DONE;
+            mbar_arrive(&full[s]);
+        }
         return;
     }
 
-    // consumers: row l of a block belongs to warp l % NCW (fixed order of accumulation)
+    // consumers: row l of a block belongs to warp l % NCW (fixed order of
+    // accumulation); lanes take elements lane, lane+32, ... (conflict-free) in four
+    // independent FP64 chains
     for (long long it = 0;; it++) {
         const int s = (int)(it % STAGES);
         if (!mbar_wait(&full[s], (unsigned)((it / STAGES) & 1), err, 2)) break;
@@ -292,31 +398,31 @@ k_vtx_bulk(const int* __restrict__ blocks, int nblocks, const int* __restrict__ 
         if (m.kind == ST_DONE) break;
         const T* buf = reinterpret_cast<const T*>(data + (size_t)s * STAGE_BYTES);
         const T* w = reinterpret_cast<const T*>(wbuf + (size_t)s * K1_WBYTES) + m.woff;
-        const int m2 = blk_m2[m.unit];
-        for (int i = 0; i < m.r0; i++) {
+        for (int i = (warp - m.s % NCW + NCW) % NCW; i < m.r0; i += NCW) {
             const int l = m.s + i;
-            if (l % NCW != warp) continue;
             const T* row = buf + (size_t)i * m.sp;
-            double part = 0.0;
-            for (int j = lane * 4; j < m.nc; j += 128) {
-                double v[4];
-                load4<T>(row + j, v);
-#pragma unroll
-                for (int q = 0; q < 4; q++) part = fma(v[q], (double)w[j + q], part);
+            double p0 = 0.0, p1 = 0.0, p2 = 0.0, p3 = 0.0;
+            int j = lane;
+            for (; j + 96 < m.nc; j += 128) {
+                p0 = fma((double)row[j], (double)w[j], p0);
+                p1 = fma((double)row[j + 32], (double)w[j + 32], p1);
+                p2 = fma((double)row[j + 64], (double)w[j + 64], p2);
+                p3 = fma((double)row[j + 96], (double)w[j + 96], p3);
             }
+            for (; j < m.nc; j += 32) p0 = fma((double)row[j], (double)w[j], p0);
+            double part = (p0 + p1) + (p2 + p3);
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1) part += __shfl_xor_sync(0xffffffffu, part, o);
             if (lane == 0) {
                 double tot = rowacc[l] + part;
                 if (m.last) {
-                    tbuf[rank_off[m.unit] + l] = (T)tot;
+                    tbuf[m.ro + l] = (T)tot;
                     rowacc[l] = 0.0;
                 } else {
                     rowacc[l] = tot;
                 }
             }
         }
-        (void)m2;
         __syncwarp();
         if (lane == 0) mbar_arrive(&empty[s]);
     }
