@@ -166,6 +166,17 @@ hmg_status hmg_get_factors(hmg_matrix* h, int block, double* U, double* V);
  * `key_bits` = number of low key bits that can be nonzero (64 if unknown) */
 hmg_status hmg_radix_sort_u64(uint64_t* keys, uint32_t* values, int n, int key_bits,
                               void* stream);
+/* The same sort without any device allocation, for callers that must not have the
+ * library call cudaMalloc (a program that owns all device memory through its own
+ * pool, or a loop where an allocation's implicit synchronisation is not allowed).
+ * No counterpart in the reference.  Scratch is a fixed array compiled into the
+ * library (held on every GPU that loads it): n above 2^20 keys is rejected with
+ * HMG_ERR_INVALID.  The first call on a device looks the array up (make it before
+ * any stream capture); calls share the array, so calls that overlap on the GPU race
+ * -- keep them on one stream.  Result identical to hmg_radix_sort_u64. */
+hmg_status hmg_radix_sort_u64_noalloc(uint64_t* keys, uint32_t* values, int n, int key_bits,
+                                      void* stream);
+
 /* Morton codes of n points (SoA coords[d*n+i]) with per-dimension min/max
  * computed on the device (helper.cu:108-138, morton.cu:79-112) */
 hmg_status hmg_morton_codes(const double* coords, int n, int dim, int bits, uint64_t* codes,
