@@ -307,8 +307,8 @@ def main(argv=None):
     ap.add_argument("--n", type=int, default=0, help="override the point count (default 2^20)")
     ap.add_argument("--prec", default="fp32", choices=["fp32", "fp64"])
     ap.add_argument("--near", default="stored", choices=["stored", "onthefly"])
-    ap.add_argument("--variant", type=int, default=0, choices=[0, 1],
-                    help="product kernels: 0 bulk-copy streaming, 1 plain loads")
+    ap.add_argument("--variant", type=int, default=1, choices=[0, 1],
+                    help="product kernels: 1 plain 16-byte loads (default), 0 bulk-copy streaming")
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--no-cpu", action="store_true")
     a = ap.parse_args(argv)

@@ -63,6 +63,8 @@ _PROTOS = {
     "hmg_full_matvec": (C.c_int, [_vp, _vp, _vp]),
     "hmg_full_matvec_rows": (C.c_int, [_vp, _vp, _vp, C.c_int, _vp]),
     "hmg_gaussian_rhs": (C.c_int, [_vp, _vp]),
+    "hmg_cg_solve": (C.c_int, [_vp, C.c_double, _vp, _vp, C.c_double, C.c_int, C.c_int,
+                               C.POINTER(C.c_int), C.POINTER(C.c_double)]),
     "hmg_synchronize": (C.c_int, [_vp]),
     "hmg_set_profiling": (C.c_int, [_vp, C.c_int]),
     "hmg_get_profile": (C.c_int, [_vp, _vp]),

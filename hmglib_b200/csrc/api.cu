@@ -255,6 +255,20 @@ hmg_status hmg_full_matvec_rows(hmg_matrix* h, const double* x, const int* rows,
     return direct_matvec(h, x, rows, nrows, y);
 }
 
+hmg_status hmg_cg_solve(hmg_matrix* h, double shift, const double* b, double* x, double tol, int maxit,
+                        int refine, int* iters, double* relres)
+{
+    HMG_REQUIRE(h && b && x, HMG_ERR_INVALID, "hmg_cg_solve: NULL argument");
+    HMG_REQUIRE(h->n[0] == h->n[1], HMG_ERR_INVALID, "hmg_cg_solve: the matrix must be square (n1 == n2)");
+    HMG_REQUIRE(std::isfinite(shift) && std::isfinite(tol) && tol > 0.0 && maxit >= 0, HMG_ERR_INVALID,
+                "hmg_cg_solve: bad shift / tol / maxit");
+    hmg_status st = check_ready(h, "hmg_cg_solve");
+    if (st) return st;
+    st = cg_solve(h, shift, b, x, tol, maxit, refine, iters, relres);
+    if (st) return st;
+    return check_pipeline(h);
+}
+
 hmg_status hmg_gaussian_rhs(hmg_matrix* h, double* b)
 {
     HMG_REQUIRE(h && b, HMG_ERR_INVALID, "hmg_gaussian_rhs: NULL argument");

@@ -81,7 +81,7 @@ struct hmg_matrix {
     int* far_list = nullptr;       // admissible blocks with rank > 0 (streaming V^T x)
     int nfar_list = 0;
     int* dev_err = nullptr;        // pipeline wait time-out flag (0 = fine)
-    int matvec_variant = 0;        // 0: streaming kernels where applicable, 1: simple kernels
+    int matvec_variant = 1;        // 0: streaming kernels where applicable, 1: plain-load kernels
     int last_variant_k1 = -1, last_variant_k2 = -1;
     double* host_x = nullptr; // pinned staging
     double* host_y = nullptr;
@@ -101,6 +101,8 @@ hmg_status matvec_device(hmg_matrix* h, const double* x, double* y);
 hmg_status direct_matvec(hmg_matrix* h, const double* x, const int* rows, int nrows,
                          double* y);
 hmg_status gaussian_rhs(hmg_matrix* h, double* b);
+hmg_status cg_solve(hmg_matrix* h, double shift, const double* b, double* x, double tol, int maxit, int refine,
+                    int* iters_out, double* relres_out);
 hmg_status morton_codes(const double* coords, int n, int dim, int bits, uint64_t* codes,
                         cudaStream_t s);
 void free_far(hmg_matrix* h);

@@ -251,23 +251,43 @@ __global__ void __launch_bounds__(256) k_vtx(const K1Unit* units, int nunits, co
         const int b = un.b, c0 = blk_c0[b], m2 = blk_m2[b], m2p = (m2 + 3) & ~3;
         const T* V = ptrV[b];
         const long long ro = rank_off[b];
-        for (int l = un.l0; l < un.l1; l++) {
-            const T* row = V + (size_t)l * m2p;
-            T acc = 0;
+        // four rows at a time: their loads are in flight together and share the x loads
+        for (int l = un.l0; l < un.l1; l += 4) {
+            const int nr = min(4, un.l1 - l);
+            T acc[4] = {0, 0, 0, 0};
             for (int j = lane * NV; j < m2p; j += 32 * NV) {
-                V4 v = *reinterpret_cast<const V4*>(row + j);
-                T vv[NV];
-                vec_get(v, vv);
+                V4 v[4];
+#pragma unroll
+                for (int rr = 0; rr < 4; rr++)
+                    if (rr < nr) v[rr] = *reinterpret_cast<const V4*>(V + (size_t)(l + rr) * m2p + j);
+                T xv[NV];
 #pragma unroll
                 for (int q = 0; q < NV; q++) {
-                    int jj = j + q;
-                    T xv = (jj < m2 && c0 + jj < n2) ? xs[c0 + jj] : (T)0;
-                    acc = fma(vv[q], xv, acc);
+                    const int jj = j + q;
+                    xv[q] = (jj < m2 && c0 + jj < n2) ? xs[c0 + jj] : (T)0;
+                }
+#pragma unroll
+                for (int rr = 0; rr < 4; rr++) {
+                    if (rr < nr) {
+                        T vv[NV];
+                        vec_get(v[rr], vv);
+#pragma unroll
+                        for (int q = 0; q < NV; q++) acc[rr] = fma(vv[q], xv[q], acc[rr]);
+                    }
                 }
             }
 #pragma unroll
-            for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-            if (lane == 0) tbuf[ro + l] = acc;
+            for (int o = 16; o > 0; o >>= 1) {
+#pragma unroll
+                for (int rr = 0; rr < 4; rr++) acc[rr] += __shfl_xor_sync(0xffffffffu, acc[rr], o);
+            }
+            if (lane < nr) {
+                T a = acc[0];
+#pragma unroll
+                for (int rr = 1; rr < 4; rr++)
+                    if (lane == rr) a = acc[rr];
+                tbuf[ro + l + lane] = a;
+            }
         }
     }
 }

@@ -1,0 +1,207 @@
+// solve.cu -- kernel-ridge solves (H + shift I) x = b with conjugate gradients.
+//
+// No reference counterpart: hmglib stops at the product.  Its only hooks for a
+// solve are the diagonal `regularization` of the kernel assemblers
+// (kernel_system_assembler.h:47-48) and the right-hand side of
+// set_gaussian_kernel_rhs (hmglib.cu:403-439).
+//
+// The operator is the engine's H-matvec (whatever storage precision the handle
+// holds) plus shift*x; vectors, inner products and the stopping test are FP64.
+// With refinement enabled, an outer loop recomputes the true residual
+// r = b - (H + shift I) x in FP64 and runs CG on the correction to a looser
+// relative tolerance, so rounding in the inner recurrences cannot stall the
+// final accuracy.  Reductions are two-pass with a fixed order: results are
+// deterministic.
+#include <cmath>
+#include <vector>
+
+#include "hmg_matrix.cuh"
+
+namespace hmg {
+
+static constexpr int RED_THREADS = 256;
+static constexpr int RED_BLOCKS = 296;
+
+__global__ void k_dot_partial(const double* a, const double* b, long long n, double* part)
+{
+    __shared__ double sh[RED_THREADS / 32];
+    double acc = 0.0;
+    for (long long i = (long long)blockIdx.x * RED_THREADS + threadIdx.x; i < n; i += (long long)gridDim.x * RED_THREADS)
+        acc = fma(a[i], b[i], acc);
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double s = 0.0;
+        for (int w = 0; w < RED_THREADS / 32; w++) s += sh[w];
+        part[blockIdx.x] = s;
+    }
+}
+
+__global__ void k_sum_partials(const double* part, int np, double* out)
+{
+    if (threadIdx.x == 0 && blockIdx.x == 0) {
+        double s = 0.0;
+        for (int i = 0; i < np; i++) s += part[i];
+        *out = s;
+    }
+}
+
+// y = a*x + y
+__global__ void k_axpy(double a, const double* x, double* y, long long n)
+{
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        y[i] = fma(a, x[i], y[i]);
+}
+
+// p = r + beta*p
+__global__ void k_xpby(const double* r, double beta, double* p, long long n)
+{
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        p[i] = fma(beta, p[i], r[i]);
+}
+
+// y += shift*x  (the ridge term of the operator)
+__global__ void k_add_shift(double shift, const double* x, double* y, long long n)
+{
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        y[i] = fma(shift, x[i], y[i]);
+}
+
+// r = b - y
+__global__ void k_sub(const double* b, const double* y, double* r, long long n)
+{
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        r[i] = b[i] - y[i];
+}
+
+struct SolveWork {
+    double *r = nullptr, *p = nullptr, *q = nullptr, *d = nullptr, *part = nullptr, *scal = nullptr;
+};
+
+static hmg_status dot(hmg_matrix* h, const double* a, const double* b, SolveWork& w, double* out)
+{
+    const long long n = h->n[0];
+    k_dot_partial<<<RED_BLOCKS, RED_THREADS, 0, h->stream>>>(a, b, n, w.part);
+    HMG_LAUNCH_CHECK();
+    k_sum_partials<<<1, 32, 0, h->stream>>>(w.part, RED_BLOCKS, w.scal);
+    HMG_LAUNCH_CHECK();
+    HMG_CUDA_TRY(cudaMemcpyAsync(out, w.scal, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    HMG_CUDA_TRY(cudaStreamSynchronize(h->stream));
+    return HMG_OK;
+}
+
+// y = (H + shift I) x
+static hmg_status apply_op(hmg_matrix* h, double shift, const double* x, double* y)
+{
+    hmg_status st = matvec_device(h, x, y);
+    if (st) return st;
+    if (shift != 0.0) {
+        k_add_shift<<<RED_BLOCKS, RED_THREADS, 0, h->stream>>>(shift, x, y, h->n[0]);
+        HMG_LAUNCH_CHECK();
+    }
+    return HMG_OK;
+}
+
+// CG on (H + shift I) z = r0 from z = 0 until |r| <= tol |r0| or maxit; z += solution.
+static hmg_status cg(hmg_matrix* h, double shift, const double* r0, double* z, double tol, int maxit,
+                     SolveWork& w, int* iters, double* relres)
+{
+    const long long n = h->n[0];
+    cudaStream_t s = h->stream;
+    hmg_status st;
+    HMG_CUDA_TRY(cudaMemcpyAsync(w.r, r0, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
+    HMG_CUDA_TRY(cudaMemcpyAsync(w.p, r0, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
+    HMG_CUDA_TRY(cudaMemsetAsync(w.d, 0, sizeof(double) * n, s));
+    double rr = 0.0;
+    if ((st = dot(h, w.r, w.r, w, &rr))) return st;
+    const double rr0 = rr;
+    int k = 0;
+    if (rr0 == 0.0) {
+        *iters = 0;
+        *relres = 0.0;
+        return HMG_OK;
+    }
+    while (k < maxit && rr > tol * tol * rr0) {
+        if ((st = apply_op(h, shift, w.p, w.q))) return st;
+        double pq = 0.0;
+        if ((st = dot(h, w.p, w.q, w, &pq))) return st;
+        if (!(pq > 0.0)) {
+            set_error("CG: operator not positive definite along a search direction (p.Ap = %g)", pq);
+            return HMG_ERR_INVALID;
+        }
+        const double alpha = rr / pq;
+        k_axpy<<<RED_BLOCKS, RED_THREADS, 0, s>>>(alpha, w.p, w.d, n);
+        k_axpy<<<RED_BLOCKS, RED_THREADS, 0, s>>>(-alpha, w.q, w.r, n);
+        HMG_LAUNCH_CHECK();
+        double rr_new = 0.0;
+        if ((st = dot(h, w.r, w.r, w, &rr_new))) return st;
+        const double beta = rr_new / rr;
+        rr = rr_new;
+        k_xpby<<<RED_BLOCKS, RED_THREADS, 0, s>>>(w.r, beta, w.p, n);
+        HMG_LAUNCH_CHECK();
+        k++;
+    }
+    k_axpy<<<RED_BLOCKS, RED_THREADS, 0, s>>>(1.0, w.d, z, n);
+    HMG_LAUNCH_CHECK();
+    *iters = k;
+    *relres = std::sqrt(rr / rr0);
+    return HMG_OK;
+}
+
+hmg_status cg_solve(hmg_matrix* h, double shift, const double* b, double* x, double tol, int maxit, int refine,
+                    int* iters_out, double* relres_out)
+{
+    cudaStream_t s = h->stream;
+    const long long n = h->n[0];
+    SolveWork w;
+    hmg_status st;
+    double* y = nullptr;
+    double* res = nullptr;
+    if ((st = dalloc(&w.r, n, s)) || (st = dalloc(&w.p, n, s)) || (st = dalloc(&w.q, n, s)) ||
+        (st = dalloc(&w.d, n, s)) || (st = dalloc(&w.part, RED_BLOCKS, s)) || (st = dalloc(&w.scal, 1, s)) ||
+        (st = dalloc(&y, n, s)) || (st = dalloc(&res, n, s)))
+        goto done;
+    {
+        double bb = 0.0;
+        if ((st = dot(h, b, b, w, &bb))) goto done;
+        int total = 0;
+        double rel = 1.0;
+        const int outer_max = refine ? 20 : 1;
+        for (int outer = 0; outer < outer_max; outer++) {
+            // true residual in FP64: res = b - (H + shift I) x
+            if ((st = apply_op(h, shift, x, y))) goto done;
+            k_sub<<<RED_BLOCKS, RED_THREADS, 0, s>>>(b, y, res, n);
+            HMG_LAUNCH_CHECK();
+            double rr = 0.0;
+            if ((st = dot(h, res, res, w, &rr))) goto done;
+            rel = bb > 0.0 ? std::sqrt(rr / bb) : 0.0;
+            if (rel <= tol || total >= maxit) break;
+            // inner solve of the correction: to tol (plain CG) or a looser 1e-4
+            // relative reduction per refinement step
+            const double inner_tol = refine ? std::fmax(tol * std::sqrt(bb / rr), 1e-4) : tol * std::sqrt(bb / rr);
+            int it = 0;
+            double rr_rel = 0.0;
+            if ((st = cg(h, shift, res, x, std::fmin(inner_tol, 0.5), maxit - total, w, &it, &rr_rel))) goto done;
+            total += it;
+            if (it == 0) break;
+        }
+        {
+            // reported residual: recomputed from x, not taken from the recurrence
+            if ((st = apply_op(h, shift, x, y))) goto done;
+            k_sub<<<RED_BLOCKS, RED_THREADS, 0, s>>>(b, y, res, n);
+            HMG_LAUNCH_CHECK();
+            double rr = 0.0;
+            if ((st = dot(h, res, res, w, &rr))) goto done;
+            rel = bb > 0.0 ? std::sqrt(rr / bb) : 0.0;
+        }
+        if (iters_out) *iters_out = total;
+        if (relres_out) *relres_out = rel;
+    }
+done:
+    dfree(w.r, s); dfree(w.p, s); dfree(w.q, s); dfree(w.d, s); dfree(w.part, s); dfree(w.scal, s);
+    dfree(y, s); dfree(res, s);
+    return st;
+}
+
+}  // namespace hmg

@@ -110,6 +110,15 @@ class HMatrix:
         self._call("hmg_full_matvec_rows", _ptr(x), _ptr(rows), int(rows.shape[0]), _ptr(y))
         return y
 
+    def cg_solve(self, b, x, shift: float, tol: float = 1e-8, maxit: int = 1000, refine: bool = True):
+        """Solve (H + shift I) x = b on device tensors; x is the initial guess.
+        Returns (iterations, final relative residual)."""
+        it = C.c_int(0)
+        rel = C.c_double(0.0)
+        self._call("hmg_cg_solve", float(shift), _ptr(b), _ptr(x), float(tol), int(maxit),
+                   1 if refine else 0, C.byref(it), C.byref(rel))
+        return it.value, rel.value
+
     def gaussian_rhs(self, b):
         self._call("hmg_gaussian_rhs", _ptr(b))
         return b

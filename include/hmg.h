@@ -122,6 +122,18 @@ hmg_status hmg_full_matvec(hmg_matrix* h, const double* x, double* y);
 hmg_status hmg_full_matvec_rows(hmg_matrix* h, const double* x, const int* rows, int nrows,
                                 double* y);
 
+/* Kernel-ridge solve (H + shift I) x = b by conjugate gradients with the handle's
+ * H-matvec as operator (n1 == n2 and a symmetric positive definite kernel).  b and
+ * x are device vectors in the caller's order; x holds the initial guess and
+ * receives the solution.  FP64 vectors, inner products and stopping test; refine
+ * != 0 wraps CG in iterative refinement with the residual recomputed in FP64.
+ * Stops when |b - (H + shift I) x| <= tol |b| or after maxit products.  iters and
+ * relres (may be NULL) receive the CG iterations and the final relative residual,
+ * recomputed from x.  Synchronous.  No reference counterpart (hmglib has no solver;
+ * its assemblers' `regularization` is the diagonal shift, kernel_system_assembler.h:47-48). */
+hmg_status hmg_cg_solve(hmg_matrix* h, double shift, const double* b, double* x, double tol, int maxit,
+                        int refine, int* iters, double* relres);
+
 /* b_i = prod_d sqrt(pi)/2 (erf(1 - x_id) - erf(-x_id)) for set 0, caller order, device b.
  * Replaces set_gaussian_kernel_rhs (hmglib.cu:403-439). */
 hmg_status hmg_gaussian_rhs(hmg_matrix* h, double* b);
@@ -135,10 +147,11 @@ hmg_status hmg_synchronize(hmg_matrix* h);
 hmg_status hmg_set_profiling(hmg_matrix* h, int on);
 hmg_status hmg_get_profile(hmg_matrix* h, double* ms4);
 
-/* Product kernels (no reference counterpart): 0 (default) streams stored slices
- * through shared memory with bulk asynchronous copies; 1 uses plain vector loads
- * (also used automatically for on-the-fly near fields and ranks above 128).  Both
- * give the same result to FP64 rounding. */
+/* Product kernels (no reference counterpart): 1 (default) reads stored slices with
+ * coalesced 16-byte loads straight into registers; 0 streams them through shared
+ * memory with bulk asynchronous copies (not used for on-the-fly near fields or ranks
+ * above 128).  Both give the same product to rounding (variant 0 sums in FP64,
+ * variant 1 sums each slice in FP32 and the slices in FP64). */
 hmg_status hmg_set_matvec_variant(hmg_matrix* h, int variant);
 
 /* Free the handle and all device memory it owns.  Replaces destroy_h_matrix_data

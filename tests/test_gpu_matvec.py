@@ -143,6 +143,7 @@ def test_streaming_kernels_match_simple_kernels(hmg, cuda, prec):
     H.precompute_aca(96, 1e-7, prec)
     H.precompute_dense(prec)
     x = np.random.default_rng(3).uniform(-1, 1, n)
+    H.set_matvec_variant(0)
     y0 = H.matvec(x)
     np.testing.assert_array_equal(H.matvec(x), y0)
     H.set_matvec_variant(1)
@@ -151,7 +152,6 @@ def test_streaming_kernels_match_simple_kernels(hmg, cuda, prec):
     # FP64 storage: both sum FP64 products (order differs); FP32 storage: the simple
     # kernels sum each slice in FP32 first
     assert rel_err(y0, y1) < (1e-13 if prec == 0 else 2e-7)
-    H.set_matvec_variant(0)
     H.close()
 
 
