@@ -162,8 +162,8 @@ def run_engine(a, rank, world):
     torch.cuda.set_device(local)
     W = WORKLOAD
     n = a.n or W["n"]
-    prec = hmg.PREC_FP32 if a.prec == "fp32" else hmg.PREC_FP64
-    esz = 4 if prec == hmg.PREC_FP32 else 8
+    prec = {"fp32": hmg.PREC_FP32, "fp64": hmg.PREC_FP64, "mixed": hmg.PREC_MIXED}[a.prec]
+    near_esz = 8 if prec == hmg.PREC_FP64 else 4  # the mixed format stores FP32 near blocks
     p = synth.uniform_points(n, W["dim"], W["seed"])
     x = synth.rhs_vector(n, W["seed"])
 
@@ -256,21 +256,17 @@ def run_engine(a, rank, world):
     peak, peak_kind = _peaks()
     # algorithmic bytes of the tile kernel per launch: near entries and U factors
     # streamed once, y written once (plus the permutation read)
-    near_b = info["near_entries"] * esz if near == "stored" else 0
-    ranks = H.ranks()
-    s1l, s1u, s2l, s2u, typ = H.blocks()
-    m1 = (s1u - s1l + 1).astype(np.int64)
-    m2 = (s2u - s2l + 1).astype(np.int64)
-    far = typ == 1
-    u_b = int((m1[far] * ranks[far]).sum()) * esz
-    v_b = int((m2[far] * ranks[far]).sum()) * esz
+    near_b = info["near_entries"] * near_esz if near == "stored" else 0
+    u_b = int(info["far_u_bytes"])
+    v_b = int(info["far_v_bytes"])
     k2_bytes = near_b + u_b + 12 * n
     achieved = k2_bytes / (k2_ms * 1e-3) / 1e9
     whole_bytes = near_b + u_b + v_b + 8 * 2 * n
     line = {
         "metric": METRIC, "value": value, "unit": "matvec/s", "n_gpus": world, "steps": a.steps,
         "warmup": a.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f32" if prec == hmg.PREC_FP32 else "f64", "data": "synthetic",
+        "vs_baseline": None, "dtype": {"fp32": "f32", "fp64": "f64", "mixed": "f32/f16/e4m3 storage, f64 sums"}[a.prec],
+        "data": "synthetic",
         "config": dict(W, n=n, near=near, storage=a.prec, parallelism=f"replicas{world}",
                        l2="inputs larger than L2 (no flush)"),
         "err_vs_fp64": err,
@@ -305,7 +301,7 @@ def main(argv=None):
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
     ap.add_argument("--n", type=int, default=0, help="override the point count (default 2^20)")
-    ap.add_argument("--prec", default="fp32", choices=["fp32", "fp64"])
+    ap.add_argument("--prec", default="fp32", choices=["fp32", "fp64", "mixed"])
     ap.add_argument("--near", default="stored", choices=["stored", "onthefly"])
     ap.add_argument("--variant", type=int, default=1, choices=[0, 1],
                     help="product kernels: 1 plain 16-byte loads (default), 0 bulk-copy streaming")

@@ -23,6 +23,7 @@ ADMISSIBLE_MAX = 0
 ADMISSIBLE_MIN = 1
 PREC_FP64 = 0
 PREC_FP32 = 1
+PREC_MIXED = 2
 NEAR_STORED = 0
 NEAR_ONTHEFLY = 1
 
@@ -39,7 +40,8 @@ class Info(C.Structure):
                 ("levels", C.c_int), ("tile_count", C.c_int), ("max_rank", C.c_int),
                 ("near_entries", C.c_int64), ("far_entries", C.c_int64), ("far_rows", C.c_int64),
                 ("near_bytes", C.c_int64), ("far_bytes", C.c_int64), ("matvec_bytes", C.c_int64),
-                ("near_precision", C.c_int), ("far_precision", C.c_int), ("near_mode", C.c_int)]
+                ("near_precision", C.c_int), ("far_precision", C.c_int), ("near_mode", C.c_int),
+                ("far_u_bytes", C.c_int64), ("far_v_bytes", C.c_int64)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}

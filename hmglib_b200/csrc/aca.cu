@@ -24,6 +24,9 @@
 // Factors are computed into FP64 scratch per batch of blocks and then compacted
 // (converted to the storage precision, laid out as tile slices for U and as
 // padded rows of V^T) into one allocation per batch.
+#include <cuda_fp16.h>
+#include <cuda_fp8.h>
+
 #include <algorithm>
 #include <vector>
 
@@ -42,6 +45,7 @@ struct AcaBatch {
     double* U;
     double* V;
     int* rank_out;           // per batch entry
+    double* s2_out;          // per batch entry: |U V^T|_F^2 (adaptive mode), may be null
 };
 
 struct BlockGeom {
@@ -109,6 +113,7 @@ k_aca(BlockGeom g, KernelSpec K, PointsView P, AcaBatch B, int k, double eps)
     const int tid = threadIdx.x;
     const bool adaptive = eps > 0.0;
     int rank = 0;
+    double S2 = 0.0;  // adaptive mode: squared Frobenius norm of the approximant
 
     if (!adaptive) {
         int ir = -1;
@@ -157,7 +162,6 @@ k_aca(BlockGeom g, KernelSpec K, PointsView P, AcaBatch B, int k, double eps)
         const int nwords = (m1 + 31) >> 5;
         for (int w = tid; w < nwords; w += ACA_THREADS) used[w] = 0u;
         __syncthreads();
-        double S2 = 0.0;
         int ir = 0, nused = 0;
         for (int r = 0; r < kb; r++) {
             int jr = -1;
@@ -275,7 +279,10 @@ k_aca(BlockGeom g, KernelSpec K, PointsView P, AcaBatch B, int k, double eps)
             __syncthreads();
         }
     }
-    if (tid == 0) B.rank_out[e] = rank;
+    if (tid == 0) {
+        B.rank_out[e] = rank;
+        if (B.s2_out) B.s2_out[e] = S2;
+    }
 }
 
 // Write the FP64 scratch factors of one block into its final storage:
@@ -311,6 +318,165 @@ __global__ void k_aca_compact(BlockGeom g, AcaBatch B, const int* tile_r0, const
     }
 }
 
+// ---------------------------------------------------------------------------
+// Mixed-precision storage of the low-rank terms.
+//
+// The ACA terms u_l v_l^T of a block decay roughly geometrically.  A term whose
+// rounding to a short format adds an error far below the ACA accuracy does not need
+// FP32: with sigma_l = |u_l| |v_l| and S = |U V^T|_F, the terms l with
+// sum_{l' >= l} sigma_l' <= TAU16 * S are stored in FP16 (unit roundoff 4.9e-4,
+// error <~ 1e-3 TAU16 S) and those with a tail below TAU8 * S in FP8 e4m3 (error
+// <~ 0.07 TAU8 S).  Each short term is scaled (u by su, v by sv: to [-1, 1] in
+// FP16, to [-448, 448] in FP8) and su*sv is folded into t_l = v_l^T x.
+// ---------------------------------------------------------------------------
+static constexpr double TAU16 = 1e-4;
+static constexpr double TAU8 = 1.5e-6;
+
+struct TierOut {
+    int* r32;          // per batch entry: terms kept in FP32
+    int* r16;          // terms in FP16 (the rest, up to the rank, in FP8)
+    const long long* soff;  // per batch entry: offset into the scale arrays
+    float* su;         // per term: scale of u_l
+    float* sv;         // per term: scale of v_l
+};
+
+__global__ void __launch_bounds__(256) k_aca_tiers(BlockGeom g, AcaBatch B, TierOut T)
+{
+    __shared__ double sig[ACA_KMAX];
+    __shared__ double mu[ACA_KMAX];
+    __shared__ double mv[ACA_KMAX];
+    const int e = blockIdx.x;
+    const int b = B.blocks[e];
+    const int m1 = g.m1[b], m2 = g.m2[b];
+    const int r = B.rank_out[e];
+    const double* U = B.U + B.uoff[e];
+    const double* V = B.V + B.voff[e];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int l = warp; l < r; l += 8) {
+        double su = 0.0, mx_u = 0.0, sv = 0.0, mx_v = 0.0;
+        for (int i = lane; i < m1; i += 32) {
+            double u = U[(size_t)l * m1 + i];
+            su = fma(u, u, su);
+            mx_u = fmax(mx_u, fabs(u));
+        }
+        for (int j = lane; j < m2; j += 32) {
+            double v = V[(size_t)l * m2 + j];
+            sv = fma(v, v, sv);
+            mx_v = fmax(mx_v, fabs(v));
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+            su += __shfl_xor_sync(0xffffffffu, su, o);
+            sv += __shfl_xor_sync(0xffffffffu, sv, o);
+            mx_u = fmax(mx_u, __shfl_xor_sync(0xffffffffu, mx_u, o));
+            mx_v = fmax(mx_v, __shfl_xor_sync(0xffffffffu, mx_v, o));
+        }
+        if (lane == 0) {
+            sig[l] = sqrt(su) * sqrt(sv);
+            mu[l] = mx_u;
+            mv[l] = mx_v;
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const double S = sqrt(fmax(B.s2_out[e], 0.0));
+        int s16 = r, s8 = r;
+        double tail = 0.0;
+        for (int l = r - 1; l >= 0; l--) {
+            tail += sig[l];
+            if (tail <= TAU16 * S) s16 = l;
+            if (tail <= TAU8 * S) s8 = l;
+        }
+        if (s8 < s16) s8 = s16;
+        T.r32[e] = s16;
+        T.r16[e] = s8 - s16;
+        const long long so = T.soff[e];
+        for (int l = 0; l < r; l++) {
+            float a = 1.0f, c = 1.0f;
+            if (l >= s8) {
+                a = (float)(mu[l] / 448.0);
+                c = (float)(mv[l] / 448.0);
+            } else if (l >= s16) {
+                a = (float)mu[l];
+                c = (float)mv[l];
+            }
+            if (!(a > 0.0f)) a = 1.0f;
+            if (!(c > 0.0f)) c = 1.0f;
+            T.su[so + l] = a;
+            T.sv[so + l] = c;
+        }
+    }
+}
+
+// Mixed storage of one block.  U tile slices: [s_pad x r32 FP32][s_pad x r16 FP16]
+// [s_pad x r8 FP8], each column-major; a slice takes s_pad * bpr bytes with
+// bpr = 4 r32 + 2 r16 + r8 rounded up to 4.  V^T: r32 rows of m2p FP32, r16 rows of
+// m2p8 (m2 rounded up to 8) FP16, r8 rows of m2p16 (m2 rounded up to 16) FP8, then
+// r FP32 factors su_l sv_l (1 for FP32 terms).
+__global__ void __launch_bounds__(256)
+k_aca_compact_mixed(BlockGeom g, AcaBatch B, TierOut T, const int* tile_r0, const int* tile_s,
+                    const int* tile_pstart, const int* tfirst, const int* tlast, void* const* ptrU,
+                    void* const* ptrV)
+{
+    const int e = blockIdx.x;
+    const int b = B.blocks[e];
+    const int r0 = g.r0[b], m1 = g.m1[b], m2 = g.m2[b];
+    const int r = B.rank_out[e];
+    if (r == 0) return;
+    const int r32 = T.r32[e], r16 = T.r16[e], r8 = r - r32 - r16;
+    const long long so = T.soff[e];
+    const double* U = B.U + B.uoff[e];
+    const double* V = B.V + B.voff[e];
+    const int m2p = (m2 + 3) & ~3, m2p8 = (m2 + 7) & ~7, m2p16 = (m2 + 15) & ~15;
+    // V^T
+    float* v32 = static_cast<float*>(ptrV[b]);
+    __half* v16 = reinterpret_cast<__half*>(v32 + (size_t)r32 * m2p);
+    __nv_fp8_storage_t* v8 = reinterpret_cast<__nv_fp8_storage_t*>(v16 + (size_t)r16 * m2p8);
+    float* scal = reinterpret_cast<float*>(v8 + (size_t)r8 * m2p16);
+    for (long long idx = threadIdx.x; idx < (long long)r32 * m2p; idx += blockDim.x) {
+        int l = (int)(idx / m2p), j = (int)(idx % m2p);
+        v32[idx] = j < m2 ? (float)V[j + (size_t)l * m2] : 0.0f;
+    }
+    for (long long idx = threadIdx.x; idx < (long long)r16 * m2p8; idx += blockDim.x) {
+        int l = r32 + (int)(idx / m2p8), j = (int)(idx % m2p8);
+        float v = j < m2 ? (float)(V[j + (size_t)l * m2] / (double)T.sv[so + l]) : 0.0f;
+        v16[idx] = __float2half_rn(v);
+    }
+    for (long long idx = threadIdx.x; idx < (long long)r8 * m2p16; idx += blockDim.x) {
+        int l = r32 + r16 + (int)(idx / m2p16), j = (int)(idx % m2p16);
+        float v = j < m2 ? (float)(V[j + (size_t)l * m2] / (double)T.sv[so + l]) : 0.0f;
+        v8[idx] = __nv_cvt_float_to_fp8(v, __NV_SATFINITE, __NV_E4M3);
+    }
+    for (int l = threadIdx.x; l < r; l += blockDim.x) scal[l] = T.su[so + l] * T.sv[so + l];
+    // U tile slices
+    const int bpr = (4 * r32 + 2 * r16 + r8 + 3) & ~3;
+    const int p0 = tile_pstart[tfirst[b]];
+    char* ubase = static_cast<char*>(ptrU[b]);
+    for (int t = tfirst[b]; t <= tlast[b]; t++) {
+        const int s = tile_s[t], sp = (s + 3) & ~3, tr = tile_r0[t] - r0;
+        char* slice = ubase + (size_t)(tile_pstart[t] - p0) * bpr;
+        float* u32 = reinterpret_cast<float*>(slice);
+        __half* u16 = reinterpret_cast<__half*>(slice + (size_t)sp * 4 * r32);
+        __nv_fp8_storage_t* u8 = reinterpret_cast<__nv_fp8_storage_t*>(slice + (size_t)sp * (4 * r32 + 2 * r16));
+        for (int idx = threadIdx.x; idx < sp * r32; idx += blockDim.x) {
+            int l = idx / sp, i = idx % sp;
+            u32[idx] = i < s ? (float)U[(size_t)l * m1 + tr + i] : 0.0f;
+        }
+        for (int idx = threadIdx.x; idx < sp * r16; idx += blockDim.x) {
+            int l = r32 + idx / sp, i = idx % sp;
+            float u = i < s ? (float)(U[(size_t)l * m1 + tr + i] / (double)T.su[so + l]) : 0.0f;
+            u16[idx] = __float2half_rn(u);
+        }
+        for (int idx = threadIdx.x; idx < sp * r8; idx += blockDim.x) {
+            int l = r32 + r16 + idx / sp, i = idx % sp;
+            float u = i < s ? (float)(U[(size_t)l * m1 + tr + i] / (double)T.su[so + l]) : 0.0f;
+            u8[idx] = __nv_cvt_float_to_fp8(u, __NV_SATFINITE, __NV_E4M3);
+        }
+        // zero the slice's tail padding (bpr rounding)
+        const int used = sp * (4 * r32 + 2 * r16 + r8);
+        for (int idx = used + threadIdx.x; idx < sp * bpr; idx += blockDim.x) slice[idx] = 0;
+    }
+}
+
 void free_far(hmg_matrix* h)
 {
     cudaStream_t s = h->stream;
@@ -322,6 +488,11 @@ void free_far(hmg_matrix* h)
     dfree(h->ptrV, s);
     dfree(h->tbuf, s);
     dfree(h->far_list, s);
+    dfree(h->tier32, s);
+    dfree(h->tier16, s);
+    h->h_r32.clear();
+    h->h_r16.clear();
+    h->far_alg_u = h->far_alg_v = 0;
     h->nfar_list = 0;
     h->far_prec = -1;
     h->desc_near_mode = -1;
@@ -339,15 +510,22 @@ hmg_status run_aca(hmg_matrix* h, int k, double eps, int precision)
         set_error("ACA rank bound k=%d exceeds the engine's limit %d", k, ACA_KMAX);
         return HMG_ERR_UNSUPPORTED;
     }
+    const bool mixed = precision == HMG_PREC_MIXED;
+    if (mixed && !(eps > 0.0)) {
+        set_error("mixed-precision factors need the adaptive ACA (eps > 0)");
+        return HMG_ERR_INVALID;
+    }
     free_far(h);
     const int nb = h->nblocks;
     const size_t esz = precision == HMG_PREC_FP64 ? 8 : 4;
-    std::vector<int> rank(nb, 0);
+    std::vector<int> rank(nb, 0), r32v(nb, 0), r16v(nb, 0);
     std::vector<void*> pU(nb, nullptr), pV(nb, nullptr);
+    long long alg_u = 0, alg_v = 0;
     if ((st = dalloc((int**)&h->rank, (size_t)nb, s)) ||
         (st = dalloc((long long**)&h->rank_off, (size_t)nb + 1, s)) ||
         (st = dalloc((void***)&h->ptrU, (size_t)nb, s)) ||
-        (st = dalloc((void***)&h->ptrV, (size_t)nb, s)))
+        (st = dalloc((void***)&h->ptrV, (size_t)nb, s)) ||
+        (st = dalloc(&h->tier32, (size_t)nb, s)) || (st = dalloc(&h->tier16, (size_t)nb, s)))
         return st;
 
     // batches of admissible blocks whose FP64 scratch fits the budget
@@ -388,20 +566,35 @@ hmg_status run_aca(hmg_matrix* h, int k, double eps, int precision)
         bstart = b;
         int ne = (int)idx.size();
         int* d_idx = nullptr;
-        long long *d_uo = nullptr, *d_vo = nullptr;
-        double *dU = nullptr, *dV = nullptr;
-        int* d_rank = nullptr;
+        long long *d_uo = nullptr, *d_vo = nullptr, *d_so = nullptr;
+        double *dU = nullptr, *dV = nullptr, *d_s2 = nullptr;
+        int *d_rank = nullptr, *d_r32 = nullptr, *d_r16 = nullptr;
+        float *d_su = nullptr, *d_sv = nullptr;
+        std::vector<long long> so(ne);
+        long long nscale = 0;
+        for (int e = 0; e < ne; e++) {
+            so[e] = nscale;
+            nscale += std::min(k, std::min(h->h_m1[idx[e]], h->h_m2[idx[e]]));
+        }
+        auto free_batch = [&]() {
+            dfree(d_idx, s); dfree(d_uo, s); dfree(d_vo, s); dfree(dU, s); dfree(dV, s);
+            dfree(d_rank, s); dfree(d_s2, s); dfree(d_so, s); dfree(d_r32, s); dfree(d_r16, s);
+            dfree(d_su, s); dfree(d_sv, s);
+        };
         if ((st = dalloc(&d_idx, ne, s)) || (st = dalloc(&d_uo, ne, s)) || (st = dalloc(&d_vo, ne, s)) ||
             (st = dalloc(&dU, (size_t)us, s)) || (st = dalloc(&dV, (size_t)vs, s)) ||
-            (st = dalloc(&d_rank, ne, s))) {
-            dfree(d_idx, s); dfree(d_uo, s); dfree(d_vo, s); dfree(dU, s); dfree(dV, s);
-            dfree(d_rank, s);
+            (st = dalloc(&d_rank, ne, s)) || (st = dalloc(&d_s2, ne, s)) ||
+            (mixed && ((st = dalloc(&d_so, ne, s)) || (st = dalloc(&d_r32, ne, s)) || (st = dalloc(&d_r16, ne, s)) ||
+                       (st = dalloc(&d_su, (size_t)nscale, s)) || (st = dalloc(&d_sv, (size_t)nscale, s))))) {
+            free_batch();
             return st;
         }
         HMG_CUDA_TRY(cudaMemcpyAsync(d_idx, idx.data(), sizeof(int) * ne, cudaMemcpyHostToDevice, s));
         HMG_CUDA_TRY(cudaMemcpyAsync(d_uo, uo.data(), sizeof(long long) * ne, cudaMemcpyHostToDevice, s));
         HMG_CUDA_TRY(cudaMemcpyAsync(d_vo, vo.data(), sizeof(long long) * ne, cudaMemcpyHostToDevice, s));
-        AcaBatch B{d_idx, d_uo, d_vo, dU, dV, d_rank};
+        if (mixed) HMG_CUDA_TRY(cudaMemcpyAsync(d_so, so.data(), sizeof(long long) * ne, cudaMemcpyHostToDevice, s));
+        AcaBatch B{d_idx, d_uo, d_vo, dU, dV, d_rank, d_s2};
+        TierOut T{d_r32, d_r16, d_so, d_su, d_sv};
         size_t dyn = eps > 0.0 ? (size_t)((maxm1 + 31) / 32) * 4 : 0;
         if (dyn > 200 * 1024) {
             set_error("block with %d rows exceeds the adaptive ACA's row-mask capacity", maxm1);
@@ -412,8 +605,16 @@ hmg_status run_aca(hmg_matrix* h, int k, double eps, int precision)
                                               (int)dyn));
         k_aca<<<ne, ACA_THREADS, dyn, s>>>(g, h->kspec, P, B, k, eps);
         HMG_LAUNCH_CHECK();
-        std::vector<int> br(ne);
+        if (mixed) {
+            k_aca_tiers<<<ne, 256, 0, s>>>(g, B, T);
+            HMG_LAUNCH_CHECK();
+        }
+        std::vector<int> br(ne), b32(ne, 0), b16(ne, 0);
         HMG_CUDA_TRY(cudaMemcpyAsync(br.data(), d_rank, sizeof(int) * ne, cudaMemcpyDeviceToHost, s));
+        if (mixed) {
+            HMG_CUDA_TRY(cudaMemcpyAsync(b32.data(), d_r32, sizeof(int) * ne, cudaMemcpyDeviceToHost, s));
+            HMG_CUDA_TRY(cudaMemcpyAsync(b16.data(), d_r16, sizeof(int) * ne, cudaMemcpyDeviceToHost, s));
+        }
         HMG_CUDA_TRY(cudaStreamSynchronize(s));
         // final storage of this batch
         long long bytes = 0;
@@ -421,13 +622,31 @@ hmg_status run_aca(hmg_matrix* h, int k, double eps, int precision)
         for (int e = 0; e < ne; e++) {
             int bb = idx[e], r = br[e];
             rank[bb] = r;
-            long long rows_p = h->h_tile_pstart[h->h_blk_tlast[bb] + 1] -
-                               h->h_tile_pstart[h->h_blk_tfirst[bb]];
+            const long long rows_p = h->h_tile_pstart[h->h_blk_tlast[bb] + 1] -
+                                     h->h_tile_pstart[h->h_blk_tfirst[bb]];
+            const long long m1 = h->h_m1[bb], m2 = h->h_m2[bb];
             ofsU[e] = bytes;
-            bytes += rows_p * r * (long long)esz;
-            bytes = (bytes + 255) & ~255ll;
-            ofsV[e] = bytes;
-            bytes += (long long)r * ((h->h_m2[bb] + 3) & ~3) * (long long)esz;
+            if (mixed) {
+                const int r32 = b32[e], r16 = b16[e], r8 = r - r32 - r16;
+                r32v[bb] = r32;
+                r16v[bb] = r16;
+                const long long bpr = (4 * r32 + 2 * r16 + r8 + 3) & ~3;
+                bytes += rows_p * bpr;
+                bytes = (bytes + 255) & ~255ll;
+                ofsV[e] = bytes;
+                bytes += (long long)r32 * ((m2 + 3) & ~3) * 4 + (long long)r16 * ((m2 + 7) & ~7) * 2 +
+                         (long long)r8 * ((m2 + 15) & ~15) + 4ll * r;
+                alg_u += m1 * (4ll * r32 + 2ll * r16 + r8);
+                alg_v += m2 * (4ll * r32 + 2ll * r16 + r8);
+            } else {
+                r32v[bb] = r;
+                bytes += rows_p * r * (long long)esz;
+                bytes = (bytes + 255) & ~255ll;
+                ofsV[e] = bytes;
+                bytes += (long long)r * ((m2 + 3) & ~3) * (long long)esz;
+                alg_u += m1 * r * (long long)esz;
+                alg_v += m2 * r * (long long)esz;
+            }
             bytes = (bytes + 255) & ~255ll;
         }
         char* chunk = nullptr;
@@ -450,7 +669,10 @@ hmg_status run_aca(hmg_matrix* h, int k, double eps, int precision)
                                          cudaMemcpyHostToDevice, s));
             HMG_CUDA_TRY(cudaMemcpyAsync(h->ptrV + idx[0], pV.data() + idx[0], sizeof(void*) * ne,
                                          cudaMemcpyHostToDevice, s));
-            if (precision == HMG_PREC_FP64)
+            if (mixed)
+                k_aca_compact_mixed<<<ne, 256, 0, s>>>(g, B, T, h->tile_r0, h->tile_s, h->tile_pstart,
+                                                       h->blk_tfirst, h->blk_tlast, h->ptrU, h->ptrV);
+            else if (precision == HMG_PREC_FP64)
                 k_aca_compact<double><<<ne, 256, 0, s>>>(g, B, h->tile_r0, h->tile_s, h->tile_pstart,
                                                          h->blk_tfirst, h->blk_tlast,
                                                          (double* const*)h->ptrU, (double* const*)h->ptrV);
@@ -461,8 +683,7 @@ hmg_status run_aca(hmg_matrix* h, int k, double eps, int precision)
             HMG_LAUNCH_CHECK();
         }
         HMG_CUDA_TRY(cudaStreamSynchronize(s));
-        dfree(d_idx, s); dfree(d_uo, s); dfree(d_vo, s); dfree(dU, s); dfree(dV, s);
-        dfree(d_rank, s);
+        free_batch();
     }
 
     // ranks and their offsets
@@ -479,6 +700,12 @@ hmg_status run_aca(hmg_matrix* h, int k, double eps, int precision)
     }
     h->rank_total = roff[nb];
     HMG_CUDA_TRY(cudaMemcpyAsync(h->rank, rank.data(), sizeof(int) * nb, cudaMemcpyHostToDevice, s));
+    HMG_CUDA_TRY(cudaMemcpyAsync(h->tier32, r32v.data(), sizeof(int) * nb, cudaMemcpyHostToDevice, s));
+    HMG_CUDA_TRY(cudaMemcpyAsync(h->tier16, r16v.data(), sizeof(int) * nb, cudaMemcpyHostToDevice, s));
+    h->h_r32 = r32v;
+    h->h_r16 = r16v;
+    h->far_alg_u = alg_u;
+    h->far_alg_v = alg_v;
     HMG_CUDA_TRY(cudaMemcpyAsync(h->rank_off, roff.data(), sizeof(long long) * (nb + 1), cudaMemcpyHostToDevice, s));
     // padded and zeroed: the streaming product copies 16-byte-aligned supersets of t_b
     if ((st = dalloc((char**)&h->tbuf, (size_t)(h->rank_total + 32) * 8, s))) return st;

@@ -5,6 +5,9 @@
 #include <cstring>
 #include <new>
 
+#include <cuda_fp16.h>
+#include <cuda_fp8.h>
+
 #include "../../include/hmglib.h"
 #include "../../include/kernel_system_assembler.h"
 #include "hmg_matrix.cuh"
@@ -168,8 +171,8 @@ hmg_status hmg_precompute_aca(hmg_matrix* h, int k, double eps, int precision)
     HMG_REQUIRE(h, HMG_ERR_INVALID, "hmg_precompute_aca: NULL handle");
     HMG_REQUIRE(h->setup_done, HMG_ERR_STATE, "hmg_precompute_aca: call hmg_setup first");
     HMG_REQUIRE(h->kernel_set, HMG_ERR_STATE, "hmg_precompute_aca: call hmg_set_kernel first");
-    HMG_REQUIRE(precision == HMG_PREC_FP64 || precision == HMG_PREC_FP32, HMG_ERR_INVALID,
-                "hmg_precompute_aca: unknown precision %d", precision);
+    HMG_REQUIRE(precision == HMG_PREC_FP64 || precision == HMG_PREC_FP32 || precision == HMG_PREC_MIXED,
+                HMG_ERR_INVALID, "hmg_precompute_aca: unknown precision %d", precision);
     HMG_REQUIRE(std::isfinite(eps), HMG_ERR_INVALID, "hmg_precompute_aca: eps not finite");
     hmg_status st = run_aca(h, k, eps, precision);
     if (st) free_far(h);
@@ -181,9 +184,10 @@ hmg_status hmg_precompute_dense(hmg_matrix* h, int precision)
     HMG_REQUIRE(h, HMG_ERR_INVALID, "hmg_precompute_dense: NULL handle");
     HMG_REQUIRE(h->setup_done, HMG_ERR_STATE, "hmg_precompute_dense: call hmg_setup first");
     HMG_REQUIRE(h->kernel_set, HMG_ERR_STATE, "hmg_precompute_dense: call hmg_set_kernel first");
-    HMG_REQUIRE(precision == HMG_PREC_FP64 || precision == HMG_PREC_FP32, HMG_ERR_INVALID,
-                "hmg_precompute_dense: unknown precision %d", precision);
-    hmg_status st = fill_near(h, precision);
+    HMG_REQUIRE(precision == HMG_PREC_FP64 || precision == HMG_PREC_FP32 || precision == HMG_PREC_MIXED,
+                HMG_ERR_INVALID, "hmg_precompute_dense: unknown precision %d", precision);
+    // the mixed format concerns the low-rank terms; its near field is FP32
+    hmg_status st = fill_near(h, precision == HMG_PREC_MIXED ? HMG_PREC_FP32 : precision);
     if (st) free_near(h);
     return st;
 }
@@ -366,7 +370,10 @@ hmg_status hmg_get_info(hmg_matrix* h, hmg_info* info)
     int fes = h->far_prec == HMG_PREC_FP64 ? 8 : 4;
     info->near_bytes = h->near_prec >= 0 ? h->near_stored * nes : 0;
     info->far_bytes = h->far_stored;
-    long long mb = h->far_prec >= 0 ? h->far_entries * fes : 0;
+    long long mb = h->far_prec >= 0 ? h->far_alg_u + h->far_alg_v : 0;
+    (void)fes;
+    info->far_u_bytes = h->far_alg_u;
+    info->far_v_bytes = h->far_alg_v;
     if (h->near_mode == HMG_NEAR_STORED && h->near_prec >= 0) mb += ne * nes;
     mb += 8ll * (h->n[0] + h->n[1]);
     info->matvec_bytes = mb;
@@ -428,6 +435,61 @@ hmg_status hmg_get_ranks(hmg_matrix* h, int* ranks)
     return HMG_OK;
 }
 
+// Decodes one block of the mixed format: per tile slice [s_pad x r32 FP32 | s_pad x r16
+// FP16 | s_pad x r8 FP8-e4m3] column-major, V^T as r32 FP32 rows (stride m2 rounded to 4),
+// r16 FP16 rows (stride rounded to 8), r8 FP8 rows (stride rounded to 16), then r FP32 term
+// scales.  The scale of each term is folded into the returned U column.
+static hmg_status get_factors_mixed(hmg_matrix* h, int block, void* pu, void* pv, double* U, double* V)
+{
+    const int r = h->h_rank[block], m1 = h->h_m1[block], m2 = h->h_m2[block];
+    const int r32 = h->h_r32[block], r16 = h->h_r16[block], r8 = r - r32 - r16;
+    const int m2p = (m2 + 3) & ~3, m2p8 = (m2 + 7) & ~7, m2p16 = (m2 + 15) & ~15;
+    const size_t vbytes = (size_t)r32 * m2p * 4 + (size_t)r16 * m2p8 * 2 + (size_t)r8 * m2p16 + (size_t)r * 4;
+    std::vector<char> hv(vbytes);
+    HMG_CUDA_TRY(cudaMemcpy(hv.data(), pv, vbytes, cudaMemcpyDeviceToHost));
+    const float* v32 = (const float*)hv.data();
+    const __half* v16 = (const __half*)(v32 + (size_t)r32 * m2p);
+    const __nv_fp8_storage_t* v8 = (const __nv_fp8_storage_t*)(v16 + (size_t)r16 * m2p8);
+    std::vector<float> scal(r);
+    std::memcpy(scal.data(), v8 + (size_t)r8 * m2p16, sizeof(float) * r);
+    auto fp8 = [](__nv_fp8_storage_t q) -> double {
+        return (double)__half2float(__half(__nv_cvt_fp8_to_halfraw(q, __NV_E4M3)));
+    };
+    for (int l = 0; l < r; l++)
+        for (int j = 0; j < m2; j++) {
+            double v;
+            if (l < r32) v = v32[(size_t)l * m2p + j];
+            else if (l < r32 + r16) v = __half2float(v16[(size_t)(l - r32) * m2p8 + j]);
+            else v = fp8(v8[(size_t)(l - r32 - r16) * m2p16 + j]);
+            V[(size_t)l * m2 + j] = v;
+        }
+    const int tf = h->h_blk_tfirst[block], tl = h->h_blk_tlast[block];
+    const int bpr = (4 * r32 + 2 * r16 + r8 + 3) & ~3;
+    const int rows_p = h->h_tile_pstart[tl + 1] - h->h_tile_pstart[tf];
+    std::vector<char> hu((size_t)rows_p * bpr);
+    HMG_CUDA_TRY(cudaMemcpy(hu.data(), pu, hu.size(), cudaMemcpyDeviceToHost));
+    std::vector<int> tr0(tl - tf + 1), ts(tl - tf + 1);
+    HMG_CUDA_TRY(cudaMemcpy(tr0.data(), h->tile_r0 + tf, sizeof(int) * (tl - tf + 1), cudaMemcpyDeviceToHost));
+    HMG_CUDA_TRY(cudaMemcpy(ts.data(), h->tile_s + tf, sizeof(int) * (tl - tf + 1), cudaMemcpyDeviceToHost));
+    const int r0 = h->h_r0[block];
+    for (int t = tf; t <= tl; t++) {
+        const int s = ts[t - tf], sp = (s + 3) & ~3;
+        const char* slice = hu.data() + (size_t)(h->h_tile_pstart[t] - h->h_tile_pstart[tf]) * bpr;
+        const float* u32 = (const float*)slice;
+        const __half* u16 = (const __half*)(slice + (size_t)sp * 4 * r32);
+        const __nv_fp8_storage_t* u8 = (const __nv_fp8_storage_t*)(slice + (size_t)sp * (4 * r32 + 2 * r16));
+        for (int l = 0; l < r; l++)
+            for (int i = 0; i < s; i++) {
+                double u;
+                if (l < r32) u = u32[(size_t)l * sp + i];
+                else if (l < r32 + r16) u = (double)__half2float(u16[(size_t)(l - r32) * sp + i]) * scal[l];
+                else u = fp8(u8[(size_t)(l - r32 - r16) * sp + i]) * scal[l];
+                U[(size_t)l * m1 + (tr0[t - tf] - r0) + i] = u;
+            }
+    }
+    return HMG_OK;
+}
+
 hmg_status hmg_get_factors(hmg_matrix* h, int block, double* U, double* V)
 {
     HMG_REQUIRE(h && U && V, HMG_ERR_INVALID, "hmg_get_factors: NULL argument");
@@ -444,6 +506,7 @@ hmg_status hmg_get_factors(hmg_matrix* h, int block, double* U, double* V)
     HMG_CUDA_TRY(cudaMemcpy(&pv, h->ptrV + block, sizeof(void*), cudaMemcpyDeviceToHost));
     const int tf = h->h_blk_tfirst[block], tl = h->h_blk_tlast[block];
     const int rows_p = h->h_tile_pstart[tl + 1] - h->h_tile_pstart[tf];
+    if (h->far_prec == HMG_PREC_MIXED) return get_factors_mixed(h, block, pu, pv, U, V);
     std::vector<char> hu((size_t)rows_p * r * esz), hv((size_t)r * m2p * esz);
     HMG_CUDA_TRY(cudaMemcpy(hu.data(), pu, hu.size(), cudaMemcpyDeviceToHost));
     HMG_CUDA_TRY(cudaMemcpy(hv.data(), pv, hv.size(), cudaMemcpyDeviceToHost));

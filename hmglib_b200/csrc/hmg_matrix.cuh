@@ -67,7 +67,12 @@ struct hmg_matrix {
     void** ptrV = nullptr;
     std::vector<void*> far_chunks;    // allocations holding the factors
     std::vector<int> h_rank;
+    int* tier32 = nullptr;            // mixed storage: per block terms in FP32
+    int* tier16 = nullptr;            // ... in FP16 (the rest of the rank in FP8)
+    std::vector<int> h_r32, h_r16;
     long long far_entries = 0, far_rows = 0, far_stored = 0;
+    long long far_alg_u = 0;          // bytes of the stored U terms (without padding)
+    long long far_alg_v = 0;          // bytes of the stored V terms
     int max_rank = 0;
 
     // ---- matvec workspace -------------------------------------------------------

@@ -15,6 +15,9 @@
 //       partials summed in a fixed order, and y written once, in the caller's
 //       order.  No atomics: y is deterministic.
 // Each stored byte is read exactly once per product (the HBM roofline's minimum).
+#include <cuda_fp16.h>
+#include <cuda_fp8.h>
+
 #include <algorithm>
 #include <vector>
 
@@ -24,7 +27,7 @@
 namespace hmg {
 
 struct K1Unit {
-    int b, l0, l1, pad;
+    int b, l0, l1, tier;  // tier: 0 storage type (FP32/FP64), 1 FP16, 2 FP8 (mixed)
 };
 
 // ---------------------------------------------------------------------------
@@ -129,7 +132,7 @@ __global__ void k_build_desc(const int* tile_pair_start, int ntiles, const int* 
                              const void* near_data, int near_esz, int near_mode,
                              const int* rank, const long long* rank_off, void* const* ptrU,
                              const void* tbuf, int far_esz, const void* xs, int x_esz,
-                             PairDesc* desc)
+                             const int* tier32, const int* tier16, int mixed, PairDesc* desc)
 {
     int t = blockIdx.x;
     if (t >= ntiles) return;
@@ -151,6 +154,16 @@ __global__ void k_build_desc(const int* tile_pair_start, int ntiles, const int* 
                 d.kind = PAIR_ONTHEFLY;
                 d.data = nullptr;
             }
+        } else if (mixed) {
+            // FP32 / FP16 / FP8 terms; a tile slice takes s_pad * bpr bytes
+            const int r = rank[b], r32 = tier32[b], r16 = tier16[b], r8 = r - r32 - r16;
+            const int bpr = (4 * r32 + 2 * r16 + r8 + 3) & ~3;
+            d.kind = PAIR_FAR_MIXED;
+            d.ncol = r32;
+            d.c0 = r16;
+            d.pad = r8;
+            d.w = (const char*)tbuf + (size_t)rank_off[b] * 4;
+            d.data = (const char*)ptrU[b] + (size_t)slice_row * bpr;
         } else {
             d.kind = PAIR_FAR;
             d.ncol = rank[b];
@@ -181,18 +194,25 @@ static hmg_status ensure_desc(hmg_matrix* h, int elem)
         k_build_desc<<<h->ntiles, 128, 0, s>>>(
             h->tile_pair_start, h->ntiles, h->pair_block, h->tile_pstart, h->blk_type, h->blk_c0,
             h->blk_m2, h->blk_tfirst, h->near_off, h->near_data, near_esz, h->near_mode, h->rank,
-            h->rank_off, h->ptrU, h->tbuf, far_esz, xs, elem, (PairDesc*)h->pair_desc);
+            h->rank_off, h->ptrU, h->tbuf, far_esz, xs, elem, h->tier32, h->tier16,
+            h->far_prec == HMG_PREC_MIXED ? 1 : 0, (PairDesc*)h->pair_desc);
         HMG_LAUNCH_CHECK();
     }
-    // K1 pieces: rows of V_b^T in runs of at most ~64 KB
+    // K1 pieces: rows of V_b^T of one storage tier, in runs of at most ~64 KB
     dfree(h->k1_units, s);
     std::vector<K1Unit> units;
+    const bool mixed = h->far_prec == HMG_PREC_MIXED;
     for (int b = h->ndense; b < h->nblocks; b++) {
-        int r = h->h_rank[b];
+        const int r = h->h_rank[b];
         if (r == 0) continue;
-        long long row_bytes = (long long)((h->h_m2[b] + 3) & ~3) * far_esz;
-        int per = (int)std::max(1ll, (65536ll) / row_bytes);
-        for (int l = 0; l < r; l += per) units.push_back({b, l, std::min(r, l + per), 0});
+        const long long m2 = h->h_m2[b];
+        const int r32 = mixed ? h->h_r32[b] : r, r16 = mixed ? h->h_r16[b] : 0;
+        const int lo[3] = {0, r32, r32 + r16}, hi[3] = {r32, r32 + r16, r};
+        const long long rb[3] = {((m2 + 3) & ~3ll) * far_esz, ((m2 + 7) & ~7ll) * 2, (m2 + 15) & ~15ll};
+        for (int tier = 0; tier < 3; tier++) {
+            const int per = (int)std::max(1ll, 65536ll / rb[tier]);
+            for (int l = lo[tier]; l < hi[tier]; l += per) units.push_back({b, l, std::min(hi[tier], l + per), tier});
+        }
     }
     h->nk1 = (int)units.size();
     K1Unit* du = nullptr;
@@ -235,11 +255,94 @@ template <> struct Vec<double> { typedef double2 type; static constexpr int N = 
 __device__ __forceinline__ void vec_get(const float4& v, float* o) { o[0] = v.x; o[1] = v.y; o[2] = v.z; o[3] = v.w; }
 __device__ __forceinline__ void vec_get(const double2& v, double* o) { o[0] = v.x; o[1] = v.y; }
 
-// K1: t_b[l] = sum_j V_b^T[l][j] x[c0_b + j]; one warp per row, rows of a piece in turn.
+// 16 bytes of FP16 (8 values) or FP8 e4m3 (16 values) to floats
+__device__ __forceinline__ void unpack16(const uint4& u, float* o)
+{
+    const __half2* h = reinterpret_cast<const __half2*>(&u);
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        float2 f = __half22float2(h[k]);
+        o[2 * k] = f.x;
+        o[2 * k + 1] = f.y;
+    }
+}
+
+__device__ __forceinline__ float2 fp8x2_to_float2(unsigned short v)
+{
+    __half2_raw hr = __nv_cvt_fp8x2_to_halfraw2((__nv_fp8x2_storage_t)v, __NV_E4M3);
+    return __half22float2(*reinterpret_cast<const __half2*>(&hr));
+}
+
+__device__ __forceinline__ void unpack8(const uint4& u, float* o)
+{
+    const unsigned w[4] = {u.x, u.y, u.z, u.w};
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        float2 a = fp8x2_to_float2((unsigned short)(w[k] & 0xffffu));
+        float2 b = fp8x2_to_float2((unsigned short)(w[k] >> 16));
+        o[4 * k] = a.x; o[4 * k + 1] = a.y; o[4 * k + 2] = b.x; o[4 * k + 3] = b.y;
+    }
+}
+
+// K1 for the short tiers of mixed storage: rows [l0, l1) of the block's FP16 (tier 1)
+// or FP8 (tier 2) rows, four rows at a time, times the terms' scale factors.
+template <int TIER>
+__device__ void vtx_short_rows(const K1Unit& un, const float* V, int r, int r32, int r16, int m2, int c0,
+                               const float* xs, long long ro, float* tbuf, int lane)
+{
+    constexpr int NE = TIER == 1 ? 8 : 16;  // values per 16-byte load
+    const int r8 = r - r32 - r16;
+    const int m2p = (m2 + 3) & ~3, m2p8 = (m2 + 7) & ~7, m2p16 = (m2 + 15) & ~15;
+    const char* base16 = reinterpret_cast<const char*>(V) + (size_t)r32 * m2p * 4;
+    const char* base8 = base16 + (size_t)r16 * m2p8 * 2;
+    const float* scal = reinterpret_cast<const float*>(base8 + (size_t)r8 * m2p16);
+    const char* base = TIER == 1 ? base16 : base8;
+    const int first = TIER == 1 ? r32 : r32 + r16;
+    const size_t row_bytes = TIER == 1 ? (size_t)m2p8 * 2 : (size_t)m2p16;
+    const int len = TIER == 1 ? m2p8 : m2p16;
+    for (int l = un.l0; l < un.l1; l += 4) {
+        const int nr = min(4, un.l1 - l);
+        float acc[4] = {0.f, 0.f, 0.f, 0.f};
+        for (int j = lane * NE; j < len; j += 32 * NE) {
+            uint4 v[4];
+#pragma unroll
+            for (int rr = 0; rr < 4; rr++)
+                if (rr < nr) v[rr] = *reinterpret_cast<const uint4*>(base + (size_t)(l - first + rr) * row_bytes +
+                                                                     (size_t)j * (TIER == 1 ? 2 : 1));
+            float xv[NE];
+#pragma unroll
+            for (int q = 0; q < NE; q++) xv[q] = xs[c0 + j + q];  // x is padded; V is zero past m2
+#pragma unroll
+            for (int rr = 0; rr < 4; rr++) {
+                if (rr < nr) {
+                    float f[NE];
+                    if (TIER == 1) unpack16(v[rr], f); else unpack8(v[rr], f);
+#pragma unroll
+                    for (int q = 0; q < NE; q++) acc[rr] = fmaf(f[q], xv[q], acc[rr]);
+                }
+            }
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+#pragma unroll
+            for (int rr = 0; rr < 4; rr++) acc[rr] += __shfl_xor_sync(0xffffffffu, acc[rr], o);
+        }
+        if (lane < nr) {
+            float a = acc[0];
+#pragma unroll
+            for (int rr = 1; rr < 4; rr++)
+                if (lane == rr) a = acc[rr];
+            tbuf[ro + l + lane] = a * scal[l + lane];
+        }
+    }
+}
+
+// K1: t_b[l] = sum_j V_b^T[l][j] x[c0_b + j]; one warp per piece of rows, four rows at a time.
 template <typename T>
 __global__ void __launch_bounds__(256) k_vtx(const K1Unit* units, int nunits, const int* blk_c0,
                                              const int* blk_m2, const long long* rank_off,
-                                             T* const* ptrV, const T* xs, int n2, T* tbuf)
+                                             T* const* ptrV, const T* xs, int n2, T* tbuf, const int* rank,
+                                             const int* tier32, const int* tier16)
 {
     typedef typename Vec<T>::type V4;
     constexpr int NV = Vec<T>::N;
@@ -251,6 +354,15 @@ __global__ void __launch_bounds__(256) k_vtx(const K1Unit* units, int nunits, co
         const int b = un.b, c0 = blk_c0[b], m2 = blk_m2[b], m2p = (m2 + 3) & ~3;
         const T* V = ptrV[b];
         const long long ro = rank_off[b];
+        if constexpr (sizeof(T) == 4) {
+            if (un.tier != 0) {
+                if (un.tier == 1)
+                    vtx_short_rows<1>(un, V, rank[b], tier32[b], tier16[b], m2, c0, xs, ro, tbuf, lane);
+                else
+                    vtx_short_rows<2>(un, V, rank[b], tier32[b], tier16[b], m2, c0, xs, ro, tbuf, lane);
+                continue;
+            }
+        }
         // four rows at a time: their loads are in flight together and share the x loads
         for (int l = un.l0; l < un.l1; l += 4) {
             const int nr = min(4, un.l1 - l);
@@ -356,6 +468,37 @@ __global__ void __launch_bounds__(256) k_tile_matvec(const PairDesc* desc, const
 #pragma unroll
                     for (int q = 0; q < NV; q++) acc[q] = fma(a[q], w0, acc[q]);
                 }
+                if constexpr (sizeof(T) == 4) {
+                    if (d.kind == PAIR_FAR_MIXED) {
+                        // FP16 then FP8 terms of the slice: 8 resp. 4 bytes per lane per column
+                        const char* s16 = (const char*)d.data + (size_t)sp * 4 * d.ncol;
+                        const char* s8 = s16 + (size_t)sp * 2 * d.c0;
+                        const float* w16 = (const float*)d.w + d.ncol;
+                        const float* w8 = w16 + d.c0;
+#pragma unroll 4
+                        for (int jj = 0; jj < d.c0; jj++) {
+                            const uint2 raw = *reinterpret_cast<const uint2*>(s16 + ((size_t)jj * sp + row0) * 2);
+                            const __half2* h2 = reinterpret_cast<const __half2*>(&raw);
+                            const float2 f0 = __half22float2(h2[0]), f1 = __half22float2(h2[1]);
+                            const float wv = w16[jj];
+                            acc[0] = fmaf(f0.x, wv, acc[0]);
+                            acc[1] = fmaf(f0.y, wv, acc[1]);
+                            acc[2] = fmaf(f1.x, wv, acc[2]);
+                            acc[3] = fmaf(f1.y, wv, acc[3]);
+                        }
+#pragma unroll 4
+                        for (int jj = 0; jj < d.pad; jj++) {
+                            const unsigned raw = *reinterpret_cast<const unsigned*>(s8 + (size_t)jj * sp + row0);
+                            const float2 f0 = fp8x2_to_float2((unsigned short)(raw & 0xffffu));
+                            const float2 f1 = fp8x2_to_float2((unsigned short)(raw >> 16));
+                            const float wv = w8[jj];
+                            acc[0] = fmaf(f0.x, wv, acc[0]);
+                            acc[1] = fmaf(f0.y, wv, acc[1]);
+                            acc[2] = fmaf(f1.x, wv, acc[2]);
+                            acc[3] = fmaf(f1.y, wv, acc[3]);
+                        }
+                    }
+                }
             }
 #pragma unroll
             for (int q = 0; q < NV; q++) acc64[q] += (double)acc[q];
@@ -406,9 +549,12 @@ hmg_status matvec_device(hmg_matrix* h, const double* x, double* y)
     cudaStream_t s = h->stream;
     hmg_status st;
     if ((st = ensure_xs(h))) return st;
+    const bool mixed = h->far_prec == HMG_PREC_MIXED;
     const bool fp64 = h->far_prec == HMG_PREC_FP64 ||
                       (h->naca == 0 && h->near_prec != HMG_PREC_FP32);
-    if (h->near_mode == HMG_NEAR_STORED && h->naca > 0 && h->near_prec != h->far_prec) {
+    // stored near field and factors are read by one kernel instance: same element type
+    const int far_elem_prec = mixed ? HMG_PREC_FP32 : h->far_prec;
+    if (h->near_mode == HMG_NEAR_STORED && h->naca > 0 && h->near_prec != far_elem_prec) {
         set_error("stored near field (precision %d) and factors (precision %d) differ", h->near_prec,
                   h->far_prec);
         return HMG_ERR_UNSUPPORTED;
@@ -420,8 +566,9 @@ hmg_status matvec_device(hmg_matrix* h, const double* x, double* y)
     k_gather_x<<<ceil_div(h->n[1], 256), 256, 0, s>>>(x, h->perm[1], h->n[1], h->xs64, h->xs32);
     HMG_LAUNCH_CHECK();
     if (h->profiling) HMG_CUDA_TRY(cudaEventRecord(h->ev[1], s));
-    const bool bulk_k1 = h->matvec_variant == 0 && h->max_rank <= K1_MAXRANK;
-    const bool bulk_k2 = h->matvec_variant == 0 && (h->near_mode == HMG_NEAR_STORED || h->ndense == 0);
+    // the streaming kernels read FP32/FP64 storage only
+    const bool bulk_k1 = h->matvec_variant == 0 && !mixed && h->max_rank <= K1_MAXRANK;
+    const bool bulk_k2 = h->matvec_variant == 0 && !mixed && (h->near_mode == HMG_NEAR_STORED || h->ndense == 0);
     h->last_variant_k1 = bulk_k1 ? 0 : 1;
     h->last_variant_k2 = bulk_k2 ? 0 : 1;
     if (bulk_k1 && h->nfar_list > 0) {
@@ -431,11 +578,11 @@ hmg_status matvec_device(hmg_matrix* h, const double* x, double* y)
         if (fp64)
             k_vtx<double><<<grid, 256, 0, s>>>((const K1Unit*)h->k1_units, h->nk1, h->blk_c0, h->blk_m2,
                                                h->rank_off, (double* const*)h->ptrV, h->xs64, h->n[1],
-                                               (double*)h->tbuf);
+                                               (double*)h->tbuf, h->rank, h->tier32, h->tier16);
         else
             k_vtx<float><<<grid, 256, 0, s>>>((const K1Unit*)h->k1_units, h->nk1, h->blk_c0, h->blk_m2,
                                               h->rank_off, (float* const*)h->ptrV, h->xs32, h->n[1],
-                                              (float*)h->tbuf);
+                                              (float*)h->tbuf, h->rank, h->tier32, h->tier16);
         HMG_LAUNCH_CHECK();
     }
     if (h->profiling) HMG_CUDA_TRY(cudaEventRecord(h->ev[2], s));

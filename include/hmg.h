@@ -46,6 +46,11 @@ typedef enum {
 /* storage precision of the near-field blocks and the low-rank factors */
 #define HMG_PREC_FP64 0
 #define HMG_PREC_FP32 1
+/* Low-rank factors only (adaptive ACA): each block keeps its leading terms in FP32
+ * and stores the terms whose tail sum of |u_l||v_l| is below 1e-4 of the block's
+ * Frobenius norm in FP16 and below 1.5e-6 in FP8 e4m3, each scaled; the added error
+ * is ~1e-7 of the block norm.  hmg_precompute_dense with this value stores FP32. */
+#define HMG_PREC_MIXED 2
 
 /* near-field mode for hmg_matvec */
 #define HMG_NEAR_STORED 0   /* read the blocks stored by hmg_precompute_dense          */
@@ -63,6 +68,8 @@ typedef struct {
     int64_t far_bytes;        /* bytes of stored factors */
     int64_t matvec_bytes;     /* bytes one hmg_matvec streams from HBM (algorithmic) */
     int near_precision, far_precision, near_mode;
+    int64_t far_u_bytes;      /* bytes of the stored U terms (sum m1 * rank * size, no padding) */
+    int64_t far_v_bytes;      /* bytes of the stored V terms */
 } hmg_info;
 
 /* message of the last failed call on this thread ("" if none) */

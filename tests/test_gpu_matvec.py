@@ -155,6 +155,49 @@ def test_streaming_kernels_match_simple_kernels(hmg, cuda, prec):
     H.close()
 
 
+@pytest.mark.parametrize("case", [("uniform", 60000, 3, 1, 4, 0.2, 1e-8), ("gmm", 40000, 2, 2, 3, 0.05, 1e-8)],
+                         ids=["uniform3d-matern", "gmm2d-gauss"])
+def test_mixed_precision_factors(hmg, cuda, case):
+    """Mixed storage (leading terms FP32, tail terms FP16 / FP8 by their share of the
+    block norm) stays within 3e-7 of the FP64 direct product at eps = 1e-8, stores
+    fewer bytes than FP32, and agrees with the FP32 storage to ~1e-7."""
+    torch = cuda
+    gen, n, dim, seed, kind, param, eps = case
+    p = make_points(gen, n, dim, seed)
+    x = np.random.default_rng(seed).uniform(-1, 1, n)
+    dx = _torch_vec(torch, x)
+    ys, nbytes, Hs = {}, {}, {}
+    for prec in (hmg.PREC_FP32, hmg.PREC_MIXED):
+        H = Hs[prec] = engine(hmg, p, p, 1.5, 128 if dim == 3 else 64, rule=1)
+        H.set_kernel(kind, param, 0.0)
+        H.precompute_aca(96, eps, prec)
+        H.precompute_dense(prec)
+        ys[prec] = H.matvec(x)
+        nbytes[prec] = H.info()["far_bytes"]
+        np.testing.assert_array_equal(H.matvec(x), ys[prec])  # deterministic
+        if prec == hmg.PREC_MIXED:
+            dy = torch.empty(n, dtype=torch.float64, device="cuda")
+            H.full_matvec(dx, dy)
+            torch.cuda.synchronize()
+            yd = dy.cpu().numpy()
+    # decoded factors: the same low-rank terms, within the tail thresholds of the FP32 ones
+    ranks = Hs[hmg.PREC_MIXED].ranks()
+    np.testing.assert_array_equal(ranks, Hs[hmg.PREC_FP32].ranks())
+    s1l, s1u, s2l, s2u, _ = Hs[hmg.PREC_MIXED].blocks()
+    far = np.nonzero(ranks > 0)[0]
+    for b in far[np.argsort(-ranks[far], kind="stable")[:6]]:
+        shape = (int(b), int(s1u[b] - s1l[b] + 1), int(s2u[b] - s2l[b] + 1), int(ranks[b]))
+        u32, v32 = Hs[hmg.PREC_FP32].factors(*shape)
+        um, vm = Hs[hmg.PREC_MIXED].factors(*shape)
+        a, c = u32.T @ v32, um.T @ vm
+        assert np.linalg.norm(a - c) <= 1e-6 * np.linalg.norm(a), (b, np.linalg.norm(a - c) / np.linalg.norm(a))
+    for H in Hs.values():
+        H.close()
+    assert rel_err(ys[hmg.PREC_MIXED], yd) < 3e-7, rel_err(ys[hmg.PREC_MIXED], yd)
+    assert rel_err(ys[hmg.PREC_MIXED], ys[hmg.PREC_FP32]) < 3e-7
+    assert nbytes[hmg.PREC_MIXED] < 0.8 * nbytes[hmg.PREC_FP32]
+
+
 def test_adaptive_matches_oracle_adaptive(hmg, oracle, cuda):
     """Same pivot rules as the oracle's adaptive ACA: ranks agree within one and the
     products agree to the ACA tolerance."""

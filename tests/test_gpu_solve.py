@@ -32,12 +32,14 @@ def test_kernel_ridge_cg(hmg, cuda, refine, prec):
     H.synchronize()
     r_op = b - (y + shift * x)
     assert float(torch.linalg.norm(r_op) / torch.linalg.norm(b)) <= 2 * tol
-    # residual against the exact kernel matrix: bounded by the H-matrix error
+    # residual against the exact kernel matrix: the operator residual plus (H - K) x,
+    # where |x| ~ |b| / shift amplifies the H-matrix error
     yd = torch.empty_like(x)
     H.full_matvec(x, yd)
     torch.cuda.synchronize()
+    assert float(torch.linalg.norm(y - yd) / torch.linalg.norm(yd)) < 1e-7
     r_ex = b - (yd + shift * x)
-    assert float(torch.linalg.norm(r_ex) / torch.linalg.norm(b)) < 1e-5
+    assert float(torch.linalg.norm(r_ex) / torch.linalg.norm(b)) < 5e-5
     H.close()
 
 
