@@ -81,8 +81,9 @@ struct hmg_matrix {
     void* tbuf = nullptr;     // V^T x per block (rank_total entries)
     void* pair_desc = nullptr;     // per (tile, block) pair: slice pointer, vector, columns
     int desc_near_mode = -1, desc_near_prec = -2, desc_far_prec = -2;
-    void* k1_units = nullptr;      // (block, first row, end row) pieces of V^T
+    void* k1_units = nullptr;      // K1 pieces of V^T (rows of one storage tier), grouped by tier
     int nk1 = 0;
+    int k1_count[3] = {0, 0, 0};   // pieces per tier (FP32/FP64, FP16, FP8)
     int* far_list = nullptr;       // admissible blocks with rank > 0 (streaming V^T x)
     int nfar_list = 0;
     int* dev_err = nullptr;        // pipeline wait time-out flag (0 = fine)

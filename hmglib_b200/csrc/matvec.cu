@@ -30,6 +30,17 @@ struct K1Unit {
     int b, l0, l1, tier;  // tier: 0 storage type (FP32/FP64), 1 FP16, 2 FP8 (mixed)
 };
 
+// A K1 piece resolved to addresses: rows [l0, l1) of one storage tier of V_b^T.
+struct K1Desc {
+    const void* v;       // row l0 of the tier
+    const float* scal;   // the rows' term scales (FP16/FP8 tiers), else null
+    long long tout;      // tbuf index of row l0
+    int c0, m2;          // the block's x segment
+    int nrows, row_bytes;  // rows in the piece; row stride, a multiple of 16 bytes
+    int pad[2];
+};
+static_assert(sizeof(K1Desc) == 48, "K1Desc layout");
+
 // ---------------------------------------------------------------------------
 // near-field fill (precompute_batched_dense_magma, linear_algebra.cu:3140-3342):
 // one CTA per dense block, entries written tile slice by tile slice.
@@ -174,6 +185,39 @@ __global__ void k_build_desc(const int* tile_pair_start, int ntiles, const int* 
     }
 }
 
+__global__ void k_build_k1desc(const K1Unit* units, int n, const int* blk_c0, const int* blk_m2,
+                               const int* rank, const int* tier32, const int* tier16, const long long* rank_off,
+                               void* const* ptrV, int esz, int mixed, K1Desc* out)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const K1Unit un = units[i];
+    const int b = un.b, m2 = blk_m2[b], r = rank[b];
+    const int r32 = mixed ? tier32[b] : r, r16 = mixed ? tier16[b] : 0, r8 = r - r32 - r16;
+    const size_t m2p = (m2 + 3) & ~3, m2p8 = (m2 + 7) & ~7, m2p16 = (m2 + 15) & ~15;
+    const char* V = static_cast<const char*>(ptrV[b]);
+    const size_t b32 = (size_t)r32 * m2p * esz, b16 = (size_t)r16 * m2p8 * 2;
+    K1Desc d;
+    if (un.tier == 0) {
+        d.row_bytes = (int)(m2p * esz);
+        d.v = V + (size_t)un.l0 * d.row_bytes;
+    } else if (un.tier == 1) {
+        d.row_bytes = (int)(m2p8 * 2);
+        d.v = V + b32 + (size_t)(un.l0 - r32) * d.row_bytes;
+    } else {
+        d.row_bytes = (int)m2p16;
+        d.v = V + b32 + b16 + (size_t)(un.l0 - r32 - r16) * d.row_bytes;
+    }
+    d.scal = un.tier == 0 ? nullptr
+                          : reinterpret_cast<const float*>(V + b32 + b16 + (size_t)r8 * m2p16) + un.l0;
+    d.tout = rank_off[b] + un.l0;
+    d.c0 = blk_c0[b];
+    d.m2 = m2;
+    d.nrows = un.l1 - un.l0;
+    d.pad[0] = d.pad[1] = 0;
+    out[i] = d;
+}
+
 static hmg_status ensure_desc(hmg_matrix* h, int elem)
 {
     cudaStream_t s = h->stream;
@@ -198,9 +242,10 @@ static hmg_status ensure_desc(hmg_matrix* h, int elem)
             h->far_prec == HMG_PREC_MIXED ? 1 : 0, (PairDesc*)h->pair_desc);
         HMG_LAUNCH_CHECK();
     }
-    // K1 pieces: rows of V_b^T of one storage tier, in runs of at most ~64 KB
+    // K1 pieces: rows of V_b^T of one storage tier, in runs of at most ~64 KB, grouped
+    // by tier (one launch per tier)
     dfree(h->k1_units, s);
-    std::vector<K1Unit> units;
+    std::vector<K1Unit> units[3];
     const bool mixed = h->far_prec == HMG_PREC_MIXED;
     for (int b = h->ndense; b < h->nblocks; b++) {
         const int r = h->h_rank[b];
@@ -211,15 +256,29 @@ static hmg_status ensure_desc(hmg_matrix* h, int elem)
         const long long rb[3] = {((m2 + 3) & ~3ll) * far_esz, ((m2 + 7) & ~7ll) * 2, (m2 + 15) & ~15ll};
         for (int tier = 0; tier < 3; tier++) {
             const int per = (int)std::max(1ll, 65536ll / rb[tier]);
-            for (int l = lo[tier]; l < hi[tier]; l += per) units.push_back({b, l, std::min(hi[tier], l + per), tier});
+            for (int l = lo[tier]; l < hi[tier]; l += per)
+                units[tier].push_back({b, l, std::min(hi[tier], l + per), tier});
         }
     }
-    h->nk1 = (int)units.size();
+    std::vector<K1Unit> all;
+    for (int tier = 0; tier < 3; tier++) {
+        h->k1_count[tier] = (int)units[tier].size();
+        all.insert(all.end(), units[tier].begin(), units[tier].end());
+    }
+    h->nk1 = (int)all.size();
+    K1Desc* dd = nullptr;
     K1Unit* du = nullptr;
-    if ((st = dalloc(&du, units.size() > 0 ? units.size() : 1, s))) return st;
-    if (!units.empty())
-        HMG_CUDA_TRY(cudaMemcpyAsync(du, units.data(), sizeof(K1Unit) * units.size(), cudaMemcpyHostToDevice, s));
-    h->k1_units = du;
+    if ((st = dalloc(&dd, all.size() > 0 ? all.size() : 1, s))) return st;
+    h->k1_units = dd;
+    if (!all.empty()) {
+        if ((st = dalloc(&du, all.size(), s))) return st;
+        HMG_CUDA_TRY(cudaMemcpyAsync(du, all.data(), sizeof(K1Unit) * all.size(), cudaMemcpyHostToDevice, s));
+        k_build_k1desc<<<ceil_div(h->nk1, 256), 256, 0, s>>>(du, h->nk1, h->blk_c0, h->blk_m2, h->rank,
+                                                            h->tier32, h->tier16, h->rank_off, h->ptrV,
+                                                            far_esz, mixed ? 1 : 0, dd);
+        HMG_LAUNCH_CHECK();
+        dfree(du, s);
+    }
     // the streaming V^T x kernel works on whole blocks
     dfree(h->far_list, s);
     std::vector<int> fl;
@@ -284,123 +343,128 @@ __device__ __forceinline__ void unpack8(const uint4& u, float* o)
     }
 }
 
-// K1 for the short tiers of mixed storage: rows [l0, l1) of the block's FP16 (tier 1)
-// or FP8 (tier 2) rows, four rows at a time, times the terms' scale factors.
-template <int TIER>
-__device__ void vtx_short_rows(const K1Unit& un, const float* V, int r, int r32, int r16, int m2, int c0,
-                               const float* xs, long long ro, float* tbuf, int lane)
+// 16 bytes of one tier to values: FP32 (4), FP64 (2), FP16 (8), FP8 e4m3 (16)
+template <typename T, int TIER> struct Chunk;
+template <> struct Chunk<float, 0> {
+    static constexpr int N = 4;
+    __device__ static void get(const uint4& u, float* o)
+    {
+        o[0] = __uint_as_float(u.x); o[1] = __uint_as_float(u.y);
+        o[2] = __uint_as_float(u.z); o[3] = __uint_as_float(u.w);
+    }
+};
+template <> struct Chunk<double, 0> {
+    static constexpr int N = 2;
+    __device__ static void get(const uint4& u, double* o)
+    {
+        o[0] = __hiloint2double((int)u.y, (int)u.x);
+        o[1] = __hiloint2double((int)u.w, (int)u.z);
+    }
+};
+template <> struct Chunk<float, 1> {
+    static constexpr int N = 8;
+    __device__ static void get(const uint4& u, float* o) { unpack16(u, o); }
+};
+template <> struct Chunk<float, 2> {
+    static constexpr int N = 16;
+    __device__ static void get(const uint4& u, float* o) { unpack8(u, o); }
+};
+
+// K1: t_b[l] = s_l sum_j V_b^T[l][j] x[c0_b + j] over the pieces of one storage tier.
+// A warp takes a piece; its lanes split into groups of LPR = 4..32 lanes (the power of
+// two <= the row's 16-byte chunks, so short rows do not leave lanes idle), each group
+// takes four rows at a time and strides over their chunks.  The four row sums of a
+// group are reduced by a transposing butterfly (log2(LPR) + 1 shuffles for four rows)
+// in a fixed order: t is deterministic.  The next piece's descriptor is loaded while
+// the current one streams.
+template <typename T, int TIER, int LG>
+__device__ __forceinline__ void vtx_piece(const K1Desc& d, const T* __restrict__ xs, T* __restrict__ tbuf,
+                                          int lane)
 {
-    constexpr int NE = TIER == 1 ? 8 : 16;  // values per 16-byte load
-    const int r8 = r - r32 - r16;
-    const int m2p = (m2 + 3) & ~3, m2p8 = (m2 + 7) & ~7, m2p16 = (m2 + 15) & ~15;
-    const char* base16 = reinterpret_cast<const char*>(V) + (size_t)r32 * m2p * 4;
-    const char* base8 = base16 + (size_t)r16 * m2p8 * 2;
-    const float* scal = reinterpret_cast<const float*>(base8 + (size_t)r8 * m2p16);
-    const char* base = TIER == 1 ? base16 : base8;
-    const int first = TIER == 1 ? r32 : r32 + r16;
-    const size_t row_bytes = TIER == 1 ? (size_t)m2p8 * 2 : (size_t)m2p16;
-    const int len = TIER == 1 ? m2p8 : m2p16;
-    for (int l = un.l0; l < un.l1; l += 4) {
-        const int nr = min(4, un.l1 - l);
-        float acc[4] = {0.f, 0.f, 0.f, 0.f};
-        for (int j = lane * NE; j < len; j += 32 * NE) {
-            uint4 v[4];
+    typedef Chunk<T, TIER> C;
+    constexpr int EPC = C::N;
+    constexpr int R = 4;
+    constexpr int LPR = 1 << LG, G = 32 >> LG;
+    const int cpr = d.row_bytes >> 4;
+    const int grp = lane >> LG, sub = lane & (LPR - 1);
+    const char* vb = static_cast<const char*>(d.v);
+    for (int rb = 0; rb < d.nrows; rb += G * R) {
+        const int row = rb + grp * R;
+        T acc[R];
 #pragma unroll
-            for (int rr = 0; rr < 4; rr++)
-                if (rr < nr) v[rr] = *reinterpret_cast<const uint4*>(base + (size_t)(l - first + rr) * row_bytes +
-                                                                     (size_t)j * (TIER == 1 ? 2 : 1));
-            float xv[NE];
+        for (int k = 0; k < R; k++) acc[k] = (T)0;
+        // two chunks per row and iteration: eight 16-byte loads in flight per lane
+        for (int c = sub; c < cpr; c += 2 * LPR) {
+            const int c2 = c + LPR;
+            uint4 raw[2][R];
 #pragma unroll
-            for (int q = 0; q < NE; q++) xv[q] = xs[c0 + j + q];  // x is padded; V is zero past m2
+            for (int k = 0; k < R; k++) {
+                raw[0][k] = make_uint4(0u, 0u, 0u, 0u);
+                raw[1][k] = make_uint4(0u, 0u, 0u, 0u);
+                const uint4* rp = reinterpret_cast<const uint4*>(vb + (size_t)(row + k) * d.row_bytes);
+                if (row + k < d.nrows) {
+                    raw[0][k] = __ldg(rp + c);
+                    if (c2 < cpr) raw[1][k] = __ldg(rp + c2);
+                }
+            }
 #pragma unroll
-            for (int rr = 0; rr < 4; rr++) {
-                if (rr < nr) {
-                    float f[NE];
-                    if (TIER == 1) unpack16(v[rr], f); else unpack8(v[rr], f);
+            for (int h = 0; h < 2; h++) {
+                T xv[EPC];
+                const int e0 = (h ? c2 : c) * EPC;
 #pragma unroll
-                    for (int q = 0; q < NE; q++) acc[rr] = fmaf(f[q], xv[q], acc[rr]);
+                for (int q = 0; q < EPC; q++) xv[q] = e0 + q < d.m2 ? xs[d.c0 + e0 + q] : (T)0;
+#pragma unroll
+                for (int k = 0; k < R; k++) {
+                    T f[EPC];
+                    C::get(raw[h][k], f);
+#pragma unroll
+                    for (int q = 0; q < EPC; q++) acc[k] = fma(f[q], xv[q], acc[k]);
                 }
             }
         }
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-#pragma unroll
-            for (int rr = 0; rr < 4; rr++) acc[rr] += __shfl_xor_sync(0xffffffffu, acc[rr], o);
+        // transposing butterfly: after it, lane `sub` holds row sub >> (LG - 2)
+        T a0, a1;
+        {
+            constexpr int o = LPR >> 1;
+            const bool up = (sub & o) != 0;
+            const T s0 = up ? acc[0] : acc[2], s1 = up ? acc[1] : acc[3];
+            a0 = (up ? acc[2] : acc[0]) + __shfl_xor_sync(0xffffffffu, s0, o);
+            a1 = (up ? acc[3] : acc[1]) + __shfl_xor_sync(0xffffffffu, s1, o);
         }
-        if (lane < nr) {
-            float a = acc[0];
+        {
+            constexpr int o = LPR >> 2;
+            const bool up = (sub & o) != 0;
+            const T s0 = up ? a0 : a1;
+            a0 = (up ? a1 : a0) + __shfl_xor_sync(0xffffffffu, s0, o);
+        }
 #pragma unroll
-            for (int rr = 1; rr < 4; rr++)
-                if (lane == rr) a = acc[rr];
-            tbuf[ro + l + lane] = a * scal[l + lane];
+        for (int o = LPR >> 3; o >= 1; o >>= 1) a0 += __shfl_xor_sync(0xffffffffu, a0, o);
+        const int k = sub >> (LG - 2);
+        if ((sub & ((LPR >> 2) - 1)) == 0 && row + k < d.nrows) {
+            if (TIER != 0) a0 *= d.scal[row + k];
+            tbuf[d.tout + row + k] = a0;
         }
     }
 }
 
-// K1: t_b[l] = sum_j V_b^T[l][j] x[c0_b + j]; one warp per piece of rows, four rows at a time.
-template <typename T>
-__global__ void __launch_bounds__(256) k_vtx(const K1Unit* units, int nunits, const int* blk_c0,
-                                             const int* blk_m2, const long long* rank_off,
-                                             T* const* ptrV, const T* xs, int n2, T* tbuf, const int* rank,
-                                             const int* tier32, const int* tier16)
+template <typename T, int TIER>
+__global__ void __launch_bounds__(256) k_vtx(const K1Desc* __restrict__ descs, int n, const T* __restrict__ xs,
+                                             T* __restrict__ tbuf)
 {
-    typedef typename Vec<T>::type V4;
-    constexpr int NV = Vec<T>::N;
     const int lane = threadIdx.x & 31;
     const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int nw = (gridDim.x * blockDim.x) >> 5;
-    for (int u = gw; u < nunits; u += nw) {
-        K1Unit un = units[u];
-        const int b = un.b, c0 = blk_c0[b], m2 = blk_m2[b], m2p = (m2 + 3) & ~3;
-        const T* V = ptrV[b];
-        const long long ro = rank_off[b];
-        if constexpr (sizeof(T) == 4) {
-            if (un.tier != 0) {
-                if (un.tier == 1)
-                    vtx_short_rows<1>(un, V, rank[b], tier32[b], tier16[b], m2, c0, xs, ro, tbuf, lane);
-                else
-                    vtx_short_rows<2>(un, V, rank[b], tier32[b], tier16[b], m2, c0, xs, ro, tbuf, lane);
-                continue;
-            }
-        }
-        // four rows at a time: their loads are in flight together and share the x loads
-        for (int l = un.l0; l < un.l1; l += 4) {
-            const int nr = min(4, un.l1 - l);
-            T acc[4] = {0, 0, 0, 0};
-            for (int j = lane * NV; j < m2p; j += 32 * NV) {
-                V4 v[4];
-#pragma unroll
-                for (int rr = 0; rr < 4; rr++)
-                    if (rr < nr) v[rr] = *reinterpret_cast<const V4*>(V + (size_t)(l + rr) * m2p + j);
-                T xv[NV];
-#pragma unroll
-                for (int q = 0; q < NV; q++) {
-                    const int jj = j + q;
-                    xv[q] = (jj < m2 && c0 + jj < n2) ? xs[c0 + jj] : (T)0;
-                }
-#pragma unroll
-                for (int rr = 0; rr < 4; rr++) {
-                    if (rr < nr) {
-                        T vv[NV];
-                        vec_get(v[rr], vv);
-#pragma unroll
-                        for (int q = 0; q < NV; q++) acc[rr] = fma(vv[q], xv[q], acc[rr]);
-                    }
-                }
-            }
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1) {
-#pragma unroll
-                for (int rr = 0; rr < 4; rr++) acc[rr] += __shfl_xor_sync(0xffffffffu, acc[rr], o);
-            }
-            if (lane < nr) {
-                T a = acc[0];
-#pragma unroll
-                for (int rr = 1; rr < 4; rr++)
-                    if (lane == rr) a = acc[rr];
-                tbuf[ro + l + lane] = a;
-            }
-        }
+    if (gw >= n) return;
+    K1Desc d = descs[gw];
+    for (int u = gw; u < n; u += nw) {
+        // unconditional (clamped) so that nothing waits on it before the end of the piece
+        const K1Desc next = descs[min(u + nw, n - 1)];
+        const int cpr = d.row_bytes >> 4;
+        if (cpr >= 32) vtx_piece<T, TIER, 5>(d, xs, tbuf, lane);
+        else if (cpr >= 16) vtx_piece<T, TIER, 4>(d, xs, tbuf, lane);
+        else if (cpr >= 8) vtx_piece<T, TIER, 3>(d, xs, tbuf, lane);
+        else vtx_piece<T, TIER, 2>(d, xs, tbuf, lane);
+        d = next;
     }
 }
 
@@ -475,27 +539,47 @@ __global__ void __launch_bounds__(256) k_tile_matvec(const PairDesc* desc, const
                         const char* s8 = s16 + (size_t)sp * 2 * d.c0;
                         const float* w16 = (const float*)d.w + d.ncol;
                         const float* w8 = w16 + d.c0;
-#pragma unroll 4
-                        for (int jj = 0; jj < d.c0; jj++) {
-                            const uint2 raw = *reinterpret_cast<const uint2*>(s16 + ((size_t)jj * sp + row0) * 2);
-                            const __half2* h2 = reinterpret_cast<const __half2*>(&raw);
-                            const float2 f0 = __half22float2(h2[0]), f1 = __half22float2(h2[1]);
-                            const float wv = w16[jj];
-                            acc[0] = fmaf(f0.x, wv, acc[0]);
-                            acc[1] = fmaf(f0.y, wv, acc[1]);
-                            acc[2] = fmaf(f1.x, wv, acc[2]);
-                            acc[3] = fmaf(f1.y, wv, acc[3]);
+                        // loads batched 8 (FP16) and 16 (FP8) columns deep: the narrow rows
+                        // need that many in flight to keep HBM busy
+                        for (int jj = 0; jj < d.c0; jj += 8) {
+                            uint2 raw[8];
+#pragma unroll
+                            for (int k = 0; k < 8; k++)
+                                raw[k] = jj + k < d.c0
+                                             ? *reinterpret_cast<const uint2*>(s16 + ((size_t)(jj + k) * sp + row0) * 2)
+                                             : make_uint2(0u, 0u);
+#pragma unroll
+                            for (int k = 0; k < 8; k++) {
+                                if (jj + k < d.c0) {
+                                    const __half2* h2 = reinterpret_cast<const __half2*>(&raw[k]);
+                                    const float2 f0 = __half22float2(h2[0]), f1 = __half22float2(h2[1]);
+                                    const float wv = w16[jj + k];
+                                    acc[0] = fmaf(f0.x, wv, acc[0]);
+                                    acc[1] = fmaf(f0.y, wv, acc[1]);
+                                    acc[2] = fmaf(f1.x, wv, acc[2]);
+                                    acc[3] = fmaf(f1.y, wv, acc[3]);
+                                }
+                            }
                         }
-#pragma unroll 4
-                        for (int jj = 0; jj < d.pad; jj++) {
-                            const unsigned raw = *reinterpret_cast<const unsigned*>(s8 + (size_t)jj * sp + row0);
-                            const float2 f0 = fp8x2_to_float2((unsigned short)(raw & 0xffffu));
-                            const float2 f1 = fp8x2_to_float2((unsigned short)(raw >> 16));
-                            const float wv = w8[jj];
-                            acc[0] = fmaf(f0.x, wv, acc[0]);
-                            acc[1] = fmaf(f0.y, wv, acc[1]);
-                            acc[2] = fmaf(f1.x, wv, acc[2]);
-                            acc[3] = fmaf(f1.y, wv, acc[3]);
+                        for (int jj = 0; jj < d.pad; jj += 16) {
+                            unsigned raw[16];
+#pragma unroll
+                            for (int k = 0; k < 16; k++)
+                                raw[k] = jj + k < d.pad
+                                             ? *reinterpret_cast<const unsigned*>(s8 + (size_t)(jj + k) * sp + row0)
+                                             : 0u;
+#pragma unroll
+                            for (int k = 0; k < 16; k++) {
+                                if (jj + k < d.pad) {
+                                    const float2 f0 = fp8x2_to_float2((unsigned short)(raw[k] & 0xffffu));
+                                    const float2 f1 = fp8x2_to_float2((unsigned short)(raw[k] >> 16));
+                                    const float wv = w8[jj + k];
+                                    acc[0] = fmaf(f0.x, wv, acc[0]);
+                                    acc[1] = fmaf(f0.y, wv, acc[1]);
+                                    acc[2] = fmaf(f1.x, wv, acc[2]);
+                                    acc[3] = fmaf(f1.y, wv, acc[3]);
+                                }
+                            }
                         }
                     }
                 }
@@ -574,16 +658,24 @@ hmg_status matvec_device(hmg_matrix* h, const double* x, double* y)
     if (bulk_k1 && h->nfar_list > 0) {
         if ((st = launch_vtx_bulk(h, fp64))) return st;
     } else if (h->nk1 > 0) {
-        int grid = std::min(ceil_div(h->nk1, 8), 148 * 8);
-        if (fp64)
-            k_vtx<double><<<grid, 256, 0, s>>>((const K1Unit*)h->k1_units, h->nk1, h->blk_c0, h->blk_m2,
-                                               h->rank_off, (double* const*)h->ptrV, h->xs64, h->n[1],
-                                               (double*)h->tbuf, h->rank, h->tier32, h->tier16);
-        else
-            k_vtx<float><<<grid, 256, 0, s>>>((const K1Unit*)h->k1_units, h->nk1, h->blk_c0, h->blk_m2,
-                                              h->rank_off, (float* const*)h->ptrV, h->xs32, h->n[1],
-                                              (float*)h->tbuf, h->rank, h->tier32, h->tier16);
-        HMG_LAUNCH_CHECK();
+        const K1Desc* dd = static_cast<const K1Desc*>(h->k1_units);
+        const int n0 = h->k1_count[0], n1 = h->k1_count[1], n2 = h->k1_count[2];
+        auto grid = [](int n) { return std::min(ceil_div(n, 8), 148 * 8); };
+        if (n0 > 0) {
+            if (fp64)
+                k_vtx<double, 0><<<grid(n0), 256, 0, s>>>(dd, n0, h->xs64, (double*)h->tbuf);
+            else
+                k_vtx<float, 0><<<grid(n0), 256, 0, s>>>(dd, n0, h->xs32, (float*)h->tbuf);
+            HMG_LAUNCH_CHECK();
+        }
+        if (n1 > 0) {
+            k_vtx<float, 1><<<grid(n1), 256, 0, s>>>(dd + n0, n1, h->xs32, (float*)h->tbuf);
+            HMG_LAUNCH_CHECK();
+        }
+        if (n2 > 0) {
+            k_vtx<float, 2><<<grid(n2), 256, 0, s>>>(dd + n0 + n1, n2, h->xs32, (float*)h->tbuf);
+            HMG_LAUNCH_CHECK();
+        }
     }
     if (h->profiling) HMG_CUDA_TRY(cudaEventRecord(h->ev[2], s));
     if (h->ntiles > 0 && bulk_k2) {
