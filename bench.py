@@ -190,6 +190,7 @@ def run_engine(a, rank, world):
         H.set_near_mode(hmg.NEAR_ONTHEFLY)
     t_dense = time.perf_counter() - t2
     H.set_matvec_variant(a.variant)
+    H.set_product_precision(hmg.PREC_FP64 if a.arith == "fp64" else hmg.PREC_FP32)
     streaming = a.variant == 0 and near == "stored"
     tile_kernel = "k_tiles_bulk" if streaming else "k_tile_matvec"
     info = H.info()
@@ -267,11 +268,12 @@ def run_engine(a, rank, world):
         "warmup": a.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": {"fp32": "f32", "fp64": "f64", "mixed": "f32/f16/e4m3 storage, f64 sums"}[a.prec],
         "data": "synthetic",
-        "config": dict(W, n=n, near=near, storage=a.prec, parallelism=f"replicas{world}",
+        "config": dict(W, n=n, near=near, storage=a.prec, arithmetic="fp64" if a.prec == "fp64" else a.arith,
+                       parallelism=f"replicas{world}",
                        l2="inputs larger than L2 (no flush)"),
         "err_vs_fp64": err,
         "e2e": {"value": e2e_value, "unit": "matvec/s", "h2d_bytes_per_step": 8 * n, "d2h_bytes_per_step": 8 * n},
-        "gpu_launches": 3 * a.steps,
+        "gpu_launches": (3 if streaming else info["matvec_launches"]) * a.steps,
         "roofline": {"bound": "hbm", "kernel": tile_kernel, "achieved": achieved, "peak": peak,
                      "unit": "GB/s", "frac": achieved / peak, "traffic": None, "peak_kind": peak_kind,
                      "bytes_per_launch": k2_bytes, "ms_per_launch": k2_ms},
@@ -303,6 +305,8 @@ def main(argv=None):
     ap.add_argument("--n", type=int, default=0, help="override the point count (default 2^20)")
     ap.add_argument("--prec", default="fp32", choices=["fp32", "fp64", "mixed"])
     ap.add_argument("--near", default="stored", choices=["stored", "onthefly"])
+    ap.add_argument("--arith", default="fp32", choices=["fp32", "fp64"],
+                    help="arithmetic of the products over FP32/mixed storage")
     ap.add_argument("--variant", type=int, default=1, choices=[0, 1],
                     help="product kernels: 1 plain 16-byte loads (default), 0 bulk-copy streaming")
     ap.add_argument("--cpu-seconds", type=float, default=10.0)

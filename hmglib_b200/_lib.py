@@ -41,7 +41,7 @@ class Info(C.Structure):
                 ("near_entries", C.c_int64), ("far_entries", C.c_int64), ("far_rows", C.c_int64),
                 ("near_bytes", C.c_int64), ("far_bytes", C.c_int64), ("matvec_bytes", C.c_int64),
                 ("near_precision", C.c_int), ("far_precision", C.c_int), ("near_mode", C.c_int),
-                ("far_u_bytes", C.c_int64), ("far_v_bytes", C.c_int64)]
+                ("far_u_bytes", C.c_int64), ("far_v_bytes", C.c_int64), ("matvec_launches", C.c_int)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -71,6 +71,7 @@ _PROTOS = {
     "hmg_set_profiling": (C.c_int, [_vp, C.c_int]),
     "hmg_get_profile": (C.c_int, [_vp, _vp]),
     "hmg_set_matvec_variant": (C.c_int, [_vp, C.c_int]),
+    "hmg_set_product_precision": (C.c_int, [_vp, C.c_int]),
     "hmg_destroy": (C.c_int, [_vp]),
     "hmg_get_info": (C.c_int, [_vp, C.POINTER(Info)]),
     "hmg_get_codes": (C.c_int, [_vp, C.c_int, _vp]),

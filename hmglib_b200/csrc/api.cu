@@ -310,6 +310,15 @@ hmg_status hmg_set_matvec_variant(hmg_matrix* h, int variant)
     return HMG_OK;
 }
 
+hmg_status hmg_set_product_precision(hmg_matrix* h, int precision)
+{
+    HMG_REQUIRE(h, HMG_ERR_INVALID, "hmg_set_product_precision: NULL handle");
+    HMG_REQUIRE(precision == HMG_PREC_FP32 || precision == HMG_PREC_FP64, HMG_ERR_INVALID,
+                "hmg_set_product_precision: precision must be HMG_PREC_FP32 or HMG_PREC_FP64");
+    h->arith_prec = precision;
+    return HMG_OK;
+}
+
 hmg_status hmg_set_profiling(hmg_matrix* h, int on)
 {
     HMG_REQUIRE(h, HMG_ERR_INVALID, "hmg_set_profiling: NULL handle");
@@ -367,11 +376,20 @@ hmg_status hmg_get_info(hmg_matrix* h, hmg_info* info)
     for (int b = h->ndense; b < h->nblocks; b++) fr += h->h_m1[b] + h->h_m2[b];
     info->far_rows = fr;
     int nes = h->near_prec == HMG_PREC_FP64 ? 8 : 4;
-    int fes = h->far_prec == HMG_PREC_FP64 ? 8 : 4;
     info->near_bytes = h->near_prec >= 0 ? h->near_stored * nes : 0;
     info->far_bytes = h->far_stored;
     long long mb = h->far_prec >= 0 ? h->far_alg_u + h->far_alg_v : 0;
-    (void)fes;
+    // kernels per product (plain-load variant): x gather, one V^T x launch per
+    // non-empty storage tier, the tile kernel
+    bool tier[3] = {false, false, false};
+    if (h->far_prec >= 0)
+        for (int b = h->ndense; b < h->nblocks; b++) {
+            const int r = h->h_rank[b], r32 = h->h_r32[b], r16 = h->h_r16[b];
+            tier[0] |= r32 > 0;
+            tier[1] |= r16 > 0;
+            tier[2] |= r - r32 - r16 > 0;
+        }
+    info->matvec_launches = 1 + (int)tier[0] + (int)tier[1] + (int)tier[2] + (h->ntiles > 0 ? 1 : 0);
     info->far_u_bytes = h->far_alg_u;
     info->far_v_bytes = h->far_alg_v;
     if (h->near_mode == HMG_NEAR_STORED && h->near_prec >= 0) mb += ne * nes;

@@ -80,7 +80,7 @@ struct hmg_matrix {
     float* xs32 = nullptr;
     void* tbuf = nullptr;     // V^T x per block (rank_total entries)
     void* pair_desc = nullptr;     // per (tile, block) pair: slice pointer, vector, columns
-    int desc_near_mode = -1, desc_near_prec = -2, desc_far_prec = -2;
+    int desc_near_mode = -1, desc_near_prec = -2, desc_far_prec = -2, desc_elem = 0;
     void* k1_units = nullptr;      // K1 pieces of V^T (rows of one storage tier), grouped by tier
     int nk1 = 0;
     int k1_count[3] = {0, 0, 0};   // pieces per tier (FP32/FP64, FP16, FP8)
@@ -88,6 +88,7 @@ struct hmg_matrix {
     int nfar_list = 0;
     int* dev_err = nullptr;        // pipeline wait time-out flag (0 = fine)
     int matvec_variant = 1;        // 0: streaming kernels where applicable, 1: plain-load kernels
+    int arith_prec = HMG_PREC_FP32;  // products over FP32 / mixed storage: FP32 or FP64 arithmetic
     int last_variant_k1 = -1, last_variant_k2 = -1;
     double* host_x = nullptr; // pinned staging
     double* host_y = nullptr;
@@ -103,7 +104,7 @@ hmg_status setup_tree(hmg_matrix* h);
 hmg_status build_tiles(hmg_matrix* h);
 hmg_status run_aca(hmg_matrix* h, int k, double eps, int precision);
 hmg_status fill_near(hmg_matrix* h, int precision);
-hmg_status matvec_device(hmg_matrix* h, const double* x, double* y);
+hmg_status matvec_device(hmg_matrix* h, const double* x, double* y, bool fp64_arith = false);
 hmg_status direct_matvec(hmg_matrix* h, const double* x, const int* rows, int nrows,
                          double* y);
 hmg_status gaussian_rhs(hmg_matrix* h, double* b);

@@ -144,6 +144,7 @@ __global__ void k_build_desc(const int* tile_pair_start, int ntiles, const int* 
                              const int* rank, const long long* rank_off, void* const* ptrU,
                              const void* tbuf, int far_esz, const void* xs, int x_esz,
                              const int* tier32, const int* tier16, int mixed, PairDesc* desc)
+// x_esz is the arithmetic element size: x and t_b are read in that type
 {
     int t = blockIdx.x;
     if (t >= ntiles) return;
@@ -173,12 +174,12 @@ __global__ void k_build_desc(const int* tile_pair_start, int ntiles, const int* 
             d.ncol = r32;
             d.c0 = r16;
             d.pad = r8;
-            d.w = (const char*)tbuf + (size_t)rank_off[b] * 4;
+            d.w = (const char*)tbuf + (size_t)rank_off[b] * x_esz;
             d.data = (const char*)ptrU[b] + (size_t)slice_row * bpr;
         } else {
             d.kind = PAIR_FAR;
             d.ncol = rank[b];
-            d.w = (const char*)tbuf + (size_t)rank_off[b] * far_esz;
+            d.w = (const char*)tbuf + (size_t)rank_off[b] * x_esz;
             d.data = (const char*)ptrU[b] + (size_t)slice_row * d.ncol * far_esz;
         }
         desc[p] = d;
@@ -229,7 +230,7 @@ static hmg_status ensure_desc(hmg_matrix* h, int elem)
         h->desc_near_mode = -1;
     }
     if (h->desc_near_mode == h->near_mode && h->desc_near_prec == h->near_prec &&
-        h->desc_far_prec == h->far_prec)
+        h->desc_far_prec == h->far_prec && h->desc_elem == elem)
         return HMG_OK;
     const void* xs = elem == 8 ? (const void*)h->xs64 : (const void*)h->xs32;
     int near_esz = h->near_prec == HMG_PREC_FP64 ? 8 : 4;
@@ -292,6 +293,7 @@ static hmg_status ensure_desc(hmg_matrix* h, int elem)
     h->desc_near_mode = h->near_mode;
     h->desc_near_prec = h->near_prec;
     h->desc_far_prec = h->far_prec;
+    h->desc_elem = elem;
     return HMG_OK;
 }
 
@@ -373,18 +375,46 @@ template <> struct Chunk<float, 2> {
 // K1: t_b[l] = s_l sum_j V_b^T[l][j] x[c0_b + j] over the pieces of one storage tier.
 // A warp takes a piece; its lanes split into groups of LPR = 4..32 lanes (the power of
 // two <= the row's 16-byte chunks, so short rows do not leave lanes idle), each group
-// takes four rows at a time and strides over their chunks.  The four row sums of a
-// group are reduced by a transposing butterfly (log2(LPR) + 1 shuffles for four rows)
-// in a fixed order: t is deterministic.  The next piece's descriptor is loaded while
-// the current one streams.
-template <typename T, int TIER, int LG>
+// takes four rows (FP32/FP64, two chunks per row per step) or eight rows (FP16/FP8,
+// one chunk) at a time and strides over their chunks; the row width is a compile-time
+// constant of each code path.  A group's row sums are reduced by a transposing
+// butterfly in a fixed order: t is deterministic.  The next piece's descriptor is
+// loaded while the current one streams.
+// Sum of the R row partials of an LPR-lane group: a transposing butterfly (log2 R
+// halving exchanges, then plain ones).  Afterwards lane `sub` holds the total of row
+// sub / (LPR / R); the summation order is fixed.
+template <int R, int LPR, typename T>
+__device__ __forceinline__ T rows_butterfly(T (&acc)[R], int sub)
+{
+    constexpr int LOGR = R == 8 ? 3 : (R == 4 ? 2 : 1);
+#pragma unroll
+    for (int st = 0; st < LOGR; st++) {
+        const int h = (R / 2) >> st, o = (LPR / 2) >> st;
+        const bool up = (sub & o) != 0;
+#pragma unroll
+        for (int i = 0; i < h; i++) {
+            const T send = up ? acc[i] : acc[i + h];
+            const T keep = up ? acc[i + h] : acc[i];
+            acc[i] = keep + __shfl_xor_sync(0xffffffffu, send, o);
+        }
+    }
+    T a = acc[0];
+#pragma unroll
+    for (int o = LPR / (2 * R); o >= 1; o >>= 1) a += __shfl_xor_sync(0xffffffffu, a, o);
+    return a;
+}
+
+// One K1 piece: lane groups of LPR = 2^LG lanes, each taking R rows at a time and
+// NCH 16-byte chunks of each row per step (R * NCH loads in flight per lane).
+// S: the tier's decoded type; T: arithmetic type.
+template <typename S, typename T, int TIER, int LG, int R, int NCH>
 __device__ __forceinline__ void vtx_piece(const K1Desc& d, const T* __restrict__ xs, T* __restrict__ tbuf,
                                           int lane)
 {
-    typedef Chunk<T, TIER> C;
+    typedef Chunk<S, TIER> C;
     constexpr int EPC = C::N;
-    constexpr int R = 4;
     constexpr int LPR = 1 << LG, G = 32 >> LG;
+    static_assert(LPR >= R, "a group needs at least R lanes");
     const int cpr = d.row_bytes >> 4;
     const int grp = lane >> LG, sub = lane & (LPR - 1);
     const char* vb = static_cast<const char*>(d.v);
@@ -393,63 +423,46 @@ __device__ __forceinline__ void vtx_piece(const K1Desc& d, const T* __restrict__
         T acc[R];
 #pragma unroll
         for (int k = 0; k < R; k++) acc[k] = (T)0;
-        // two chunks per row and iteration: eight 16-byte loads in flight per lane
-        for (int c = sub; c < cpr; c += 2 * LPR) {
-            const int c2 = c + LPR;
-            uint4 raw[2][R];
+        for (int c = sub; c < cpr; c += NCH * LPR) {
+            uint4 raw[NCH][R];
 #pragma unroll
             for (int k = 0; k < R; k++) {
-                raw[0][k] = make_uint4(0u, 0u, 0u, 0u);
-                raw[1][k] = make_uint4(0u, 0u, 0u, 0u);
                 const uint4* rp = reinterpret_cast<const uint4*>(vb + (size_t)(row + k) * d.row_bytes);
-                if (row + k < d.nrows) {
-                    raw[0][k] = __ldg(rp + c);
-                    if (c2 < cpr) raw[1][k] = __ldg(rp + c2);
+#pragma unroll
+                for (int hh = 0; hh < NCH; hh++) {
+                    raw[hh][k] = make_uint4(0u, 0u, 0u, 0u);
+                    if (row + k < d.nrows && c + hh * LPR < cpr) raw[hh][k] = __ldg(rp + c + hh * LPR);
                 }
             }
 #pragma unroll
-            for (int h = 0; h < 2; h++) {
+            for (int hh = 0; hh < NCH; hh++) {
                 T xv[EPC];
-                const int e0 = (h ? c2 : c) * EPC;
+                const int e0 = (c + hh * LPR) * EPC;
 #pragma unroll
                 for (int q = 0; q < EPC; q++) xv[q] = e0 + q < d.m2 ? xs[d.c0 + e0 + q] : (T)0;
 #pragma unroll
                 for (int k = 0; k < R; k++) {
-                    T f[EPC];
-                    C::get(raw[h][k], f);
+                    S f[EPC];
+                    C::get(raw[hh][k], f);
 #pragma unroll
-                    for (int q = 0; q < EPC; q++) acc[k] = fma(f[q], xv[q], acc[k]);
+                    for (int q = 0; q < EPC; q++) acc[k] = fma((T)f[q], xv[q], acc[k]);
                 }
             }
         }
-        // transposing butterfly: after it, lane `sub` holds row sub >> (LG - 2)
-        T a0, a1;
-        {
-            constexpr int o = LPR >> 1;
-            const bool up = (sub & o) != 0;
-            const T s0 = up ? acc[0] : acc[2], s1 = up ? acc[1] : acc[3];
-            a0 = (up ? acc[2] : acc[0]) + __shfl_xor_sync(0xffffffffu, s0, o);
-            a1 = (up ? acc[3] : acc[1]) + __shfl_xor_sync(0xffffffffu, s1, o);
-        }
-        {
-            constexpr int o = LPR >> 2;
-            const bool up = (sub & o) != 0;
-            const T s0 = up ? a0 : a1;
-            a0 = (up ? a1 : a0) + __shfl_xor_sync(0xffffffffu, s0, o);
-        }
-#pragma unroll
-        for (int o = LPR >> 3; o >= 1; o >>= 1) a0 += __shfl_xor_sync(0xffffffffu, a0, o);
-        const int k = sub >> (LG - 2);
-        if ((sub & ((LPR >> 2) - 1)) == 0 && row + k < d.nrows) {
+        T a0 = rows_butterfly<R, LPR>(acc, sub);
+        const int k = sub / (LPR / R);
+        if (sub % (LPR / R) == 0 && row + k < d.nrows) {
             if (TIER != 0) a0 *= d.scal[row + k];
             tbuf[d.tout + row + k] = a0;
         }
     }
 }
 
-template <typename T, int TIER>
-__global__ void __launch_bounds__(256) k_vtx(const K1Desc* __restrict__ descs, int n, const T* __restrict__ xs,
-                                             T* __restrict__ tbuf)
+// S: the tier's decoded type (FP64 storage: double, else float); T: arithmetic type.
+// FP64 arithmetic over FP32 storage needs more registers: two CTAs per SM there.
+template <typename S, typename T, int TIER>
+__global__ void __launch_bounds__(256, (sizeof(T) == 8 && sizeof(S) == 4) ? 2 : 3)
+k_vtx(const K1Desc* __restrict__ descs, int n, const T* __restrict__ xs, T* __restrict__ tbuf)
 {
     const int lane = threadIdx.x & 31;
     const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -460,10 +473,12 @@ __global__ void __launch_bounds__(256) k_vtx(const K1Desc* __restrict__ descs, i
         // unconditional (clamped) so that nothing waits on it before the end of the piece
         const K1Desc next = descs[min(u + nw, n - 1)];
         const int cpr = d.row_bytes >> 4;
-        if (cpr >= 32) vtx_piece<T, TIER, 5>(d, xs, tbuf, lane);
-        else if (cpr >= 16) vtx_piece<T, TIER, 4>(d, xs, tbuf, lane);
-        else if (cpr >= 8) vtx_piece<T, TIER, 3>(d, xs, tbuf, lane);
-        else vtx_piece<T, TIER, 2>(d, xs, tbuf, lane);
+        // FP32/FP64 rows: 4 rows x 2 chunks per step; the short FP16/FP8 rows: 8 rows x 1
+        constexpr int RR = TIER == 0 ? 4 : 8, NCH = TIER == 0 ? 2 : 1;
+        if (cpr >= 32) vtx_piece<S, T, TIER, 5, RR, NCH>(d, xs, tbuf, lane);
+        else if (cpr >= 16) vtx_piece<S, T, TIER, 4, RR, NCH>(d, xs, tbuf, lane);
+        else if (cpr >= 8) vtx_piece<S, T, TIER, 3, RR, NCH>(d, xs, tbuf, lane);
+        else vtx_piece<S, T, TIER, 2, 4, NCH>(d, xs, tbuf, lane);
         d = next;
     }
 }
@@ -471,14 +486,15 @@ __global__ void __launch_bounds__(256) k_vtx(const K1Desc* __restrict__ descs, i
 // K2: one CTA (8 warps) per row tile.  A group of RW warps covers the tile's padded
 // rows with 16-byte loads (4 FP32 or 2 FP64 rows per lane); the 8/RW groups take
 // the tile's pairs round robin.
-template <typename T>
-__global__ void __launch_bounds__(256) k_tile_matvec(const PairDesc* desc, const int* tile_pair_start,
-                                                     const int* tile_r0, const int* tile_s,
-                                                     const int* perm1, KernelSpec K, PointsView P,
-                                                     const double* xs64, double* y)
+// S: storage type of the stored near field and of the FP32/FP64 terms; T: arithmetic
+// type of a pair's products (float, or double for FP64 arithmetic over FP32 storage).
+template <typename S, typename T>
+__global__ void __launch_bounds__(256, (sizeof(T) == 8 && sizeof(S) == 4) ? 2 : 3)
+k_tile_matvec(const PairDesc* desc, const int* tile_pair_start, const int* tile_r0, const int* tile_s,
+              const int* perm1, KernelSpec K, PointsView P, const double* xs64, double* y)
 {
-    typedef typename Vec<T>::type V4;
-    constexpr int NV = Vec<T>::N;
+    typedef typename Vec<S>::type V4;
+    constexpr int NV = Vec<S>::N;
     __shared__ double red[8][HMG_TILE_ROWS];
     const int t = blockIdx.x;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -500,7 +516,7 @@ __global__ void __launch_bounds__(256) k_tile_matvec(const PairDesc* desc, const
 #pragma unroll
         for (int q = 0; q < NV; q++) acc[q] = 0;
         if (d.kind != PAIR_ONTHEFLY) {
-            const T* base = (const T*)d.data + row0;
+            const S* base = (const S*)d.data + row0;
             const T* w = (const T*)d.w;
             if (active) {
                 int j = 0;
@@ -510,76 +526,56 @@ __global__ void __launch_bounds__(256) k_tile_matvec(const PairDesc* desc, const
                     V4 v2 = *reinterpret_cast<const V4*>(base + (size_t)(j + 2) * sp);
                     V4 v3 = *reinterpret_cast<const V4*>(base + (size_t)(j + 3) * sp);
                     T w0 = w[j], w1 = w[j + 1], w2 = w[j + 2], w3 = w[j + 3];
-                    T a[NV];
+                    S a[NV];
                     vec_get(v0, a);
 #pragma unroll
-                    for (int q = 0; q < NV; q++) acc[q] = fma(a[q], w0, acc[q]);
+                    for (int q = 0; q < NV; q++) acc[q] = fma((T)a[q], w0, acc[q]);
                     vec_get(v1, a);
 #pragma unroll
-                    for (int q = 0; q < NV; q++) acc[q] = fma(a[q], w1, acc[q]);
+                    for (int q = 0; q < NV; q++) acc[q] = fma((T)a[q], w1, acc[q]);
                     vec_get(v2, a);
 #pragma unroll
-                    for (int q = 0; q < NV; q++) acc[q] = fma(a[q], w2, acc[q]);
+                    for (int q = 0; q < NV; q++) acc[q] = fma((T)a[q], w2, acc[q]);
                     vec_get(v3, a);
 #pragma unroll
-                    for (int q = 0; q < NV; q++) acc[q] = fma(a[q], w3, acc[q]);
+                    for (int q = 0; q < NV; q++) acc[q] = fma((T)a[q], w3, acc[q]);
                 }
                 for (; j < d.ncol; j++) {
                     V4 v0 = *reinterpret_cast<const V4*>(base + (size_t)j * sp);
-                    T a[NV];
+                    S a[NV];
                     vec_get(v0, a);
                     T w0 = w[j];
 #pragma unroll
-                    for (int q = 0; q < NV; q++) acc[q] = fma(a[q], w0, acc[q]);
+                    for (int q = 0; q < NV; q++) acc[q] = fma((T)a[q], w0, acc[q]);
                 }
-                if constexpr (sizeof(T) == 4) {
+                if constexpr (sizeof(S) == 4) {
                     if (d.kind == PAIR_FAR_MIXED) {
                         // FP16 then FP8 terms of the slice: 8 resp. 4 bytes per lane per column
                         const char* s16 = (const char*)d.data + (size_t)sp * 4 * d.ncol;
                         const char* s8 = s16 + (size_t)sp * 2 * d.c0;
-                        const float* w16 = (const float*)d.w + d.ncol;
-                        const float* w8 = w16 + d.c0;
-                        // loads batched 8 (FP16) and 16 (FP8) columns deep: the narrow rows
-                        // need that many in flight to keep HBM busy
-                        for (int jj = 0; jj < d.c0; jj += 8) {
-                            uint2 raw[8];
-#pragma unroll
-                            for (int k = 0; k < 8; k++)
-                                raw[k] = jj + k < d.c0
-                                             ? *reinterpret_cast<const uint2*>(s16 + ((size_t)(jj + k) * sp + row0) * 2)
-                                             : make_uint2(0u, 0u);
-#pragma unroll
-                            for (int k = 0; k < 8; k++) {
-                                if (jj + k < d.c0) {
-                                    const __half2* h2 = reinterpret_cast<const __half2*>(&raw[k]);
-                                    const float2 f0 = __half22float2(h2[0]), f1 = __half22float2(h2[1]);
-                                    const float wv = w16[jj + k];
-                                    acc[0] = fmaf(f0.x, wv, acc[0]);
-                                    acc[1] = fmaf(f0.y, wv, acc[1]);
-                                    acc[2] = fmaf(f1.x, wv, acc[2]);
-                                    acc[3] = fmaf(f1.y, wv, acc[3]);
-                                }
-                            }
+                        const T* w16 = w + d.ncol;
+                        const T* w8 = w16 + d.c0;
+#pragma unroll 4
+                        for (int jj = 0; jj < d.c0; jj++) {
+                            const uint2 raw = *reinterpret_cast<const uint2*>(s16 + ((size_t)jj * sp + row0) * 2);
+                            const __half2* h2 = reinterpret_cast<const __half2*>(&raw);
+                            const float2 f0 = __half22float2(h2[0]), f1 = __half22float2(h2[1]);
+                            const T wv = w16[jj];
+                            acc[0] = fma((T)f0.x, wv, acc[0]);
+                            acc[1] = fma((T)f0.y, wv, acc[1]);
+                            acc[2] = fma((T)f1.x, wv, acc[2]);
+                            acc[3] = fma((T)f1.y, wv, acc[3]);
                         }
-                        for (int jj = 0; jj < d.pad; jj += 16) {
-                            unsigned raw[16];
-#pragma unroll
-                            for (int k = 0; k < 16; k++)
-                                raw[k] = jj + k < d.pad
-                                             ? *reinterpret_cast<const unsigned*>(s8 + (size_t)(jj + k) * sp + row0)
-                                             : 0u;
-#pragma unroll
-                            for (int k = 0; k < 16; k++) {
-                                if (jj + k < d.pad) {
-                                    const float2 f0 = fp8x2_to_float2((unsigned short)(raw[k] & 0xffffu));
-                                    const float2 f1 = fp8x2_to_float2((unsigned short)(raw[k] >> 16));
-                                    const float wv = w8[jj + k];
-                                    acc[0] = fmaf(f0.x, wv, acc[0]);
-                                    acc[1] = fmaf(f0.y, wv, acc[1]);
-                                    acc[2] = fmaf(f1.x, wv, acc[2]);
-                                    acc[3] = fmaf(f1.y, wv, acc[3]);
-                                }
-                            }
+#pragma unroll 4
+                        for (int jj = 0; jj < d.pad; jj++) {
+                            const unsigned raw = *reinterpret_cast<const unsigned*>(s8 + (size_t)jj * sp + row0);
+                            const float2 f0 = fp8x2_to_float2((unsigned short)(raw & 0xffffu));
+                            const float2 f1 = fp8x2_to_float2((unsigned short)(raw >> 16));
+                            const T wv = w8[jj];
+                            acc[0] = fma((T)f0.x, wv, acc[0]);
+                            acc[1] = fma((T)f0.y, wv, acc[1]);
+                            acc[2] = fma((T)f1.x, wv, acc[2]);
+                            acc[3] = fma((T)f1.y, wv, acc[3]);
                         }
                     }
                 }
@@ -628,14 +624,17 @@ static hmg_status ensure_xs(hmg_matrix* h)
     return HMG_OK;
 }
 
-hmg_status matvec_device(hmg_matrix* h, const double* x, double* y)
+hmg_status matvec_device(hmg_matrix* h, const double* x, double* y, bool fp64_arith)
 {
     cudaStream_t s = h->stream;
     hmg_status st;
     if ((st = ensure_xs(h))) return st;
     const bool mixed = h->far_prec == HMG_PREC_MIXED;
+    // storage element type of the stored near field and the FP32/FP64 terms
     const bool fp64 = h->far_prec == HMG_PREC_FP64 ||
                       (h->naca == 0 && h->near_prec != HMG_PREC_FP32);
+    // arithmetic type of the products
+    const bool arith64 = fp64 || fp64_arith || h->arith_prec == HMG_PREC_FP64;
     // stored near field and factors are read by one kernel instance: same element type
     const int far_elem_prec = mixed ? HMG_PREC_FP32 : h->far_prec;
     if (h->near_mode == HMG_NEAR_STORED && h->naca > 0 && h->near_prec != far_elem_prec) {
@@ -643,16 +642,18 @@ hmg_status matvec_device(hmg_matrix* h, const double* x, double* y)
                   h->far_prec);
         return HMG_ERR_UNSUPPORTED;
     }
-    int elem = fp64 ? 8 : 4;
+    const int elem = arith64 ? 8 : 4;
     if ((st = ensure_desc(h, elem))) return st;
     PointsView P = points_view(h);
     if (h->profiling) HMG_CUDA_TRY(cudaEventRecord(h->ev[0], s));
     k_gather_x<<<ceil_div(h->n[1], 256), 256, 0, s>>>(x, h->perm[1], h->n[1], h->xs64, h->xs32);
     HMG_LAUNCH_CHECK();
     if (h->profiling) HMG_CUDA_TRY(cudaEventRecord(h->ev[1], s));
-    // the streaming kernels read FP32/FP64 storage only
-    const bool bulk_k1 = h->matvec_variant == 0 && !mixed && h->max_rank <= K1_MAXRANK;
-    const bool bulk_k2 = h->matvec_variant == 0 && !mixed && (h->near_mode == HMG_NEAR_STORED || h->ndense == 0);
+    // the streaming kernels read FP32/FP64 storage in its own arithmetic only
+    const bool plain_types = !mixed && arith64 == fp64;
+    const bool bulk_k1 = h->matvec_variant == 0 && plain_types && h->max_rank <= K1_MAXRANK;
+    const bool bulk_k2 = h->matvec_variant == 0 && plain_types &&
+                         (h->near_mode == HMG_NEAR_STORED || h->ndense == 0);
     h->last_variant_k1 = bulk_k1 ? 0 : 1;
     h->last_variant_k2 = bulk_k2 ? 0 : 1;
     if (bulk_k1 && h->nfar_list > 0) {
@@ -661,19 +662,29 @@ hmg_status matvec_device(hmg_matrix* h, const double* x, double* y)
         const K1Desc* dd = static_cast<const K1Desc*>(h->k1_units);
         const int n0 = h->k1_count[0], n1 = h->k1_count[1], n2 = h->k1_count[2];
         auto grid = [](int n) { return std::min(ceil_div(n, 8), 148 * 8); };
+        double* t64 = static_cast<double*>(h->tbuf);
+        float* t32 = static_cast<float*>(h->tbuf);
         if (n0 > 0) {
             if (fp64)
-                k_vtx<double, 0><<<grid(n0), 256, 0, s>>>(dd, n0, h->xs64, (double*)h->tbuf);
+                k_vtx<double, double, 0><<<grid(n0), 256, 0, s>>>(dd, n0, h->xs64, t64);
+            else if (arith64)
+                k_vtx<float, double, 0><<<grid(n0), 256, 0, s>>>(dd, n0, h->xs64, t64);
             else
-                k_vtx<float, 0><<<grid(n0), 256, 0, s>>>(dd, n0, h->xs32, (float*)h->tbuf);
+                k_vtx<float, float, 0><<<grid(n0), 256, 0, s>>>(dd, n0, h->xs32, t32);
             HMG_LAUNCH_CHECK();
         }
         if (n1 > 0) {
-            k_vtx<float, 1><<<grid(n1), 256, 0, s>>>(dd + n0, n1, h->xs32, (float*)h->tbuf);
+            if (arith64)
+                k_vtx<float, double, 1><<<grid(n1), 256, 0, s>>>(dd + n0, n1, h->xs64, t64);
+            else
+                k_vtx<float, float, 1><<<grid(n1), 256, 0, s>>>(dd + n0, n1, h->xs32, t32);
             HMG_LAUNCH_CHECK();
         }
         if (n2 > 0) {
-            k_vtx<float, 2><<<grid(n2), 256, 0, s>>>(dd + n0 + n1, n2, h->xs32, (float*)h->tbuf);
+            if (arith64)
+                k_vtx<float, double, 2><<<grid(n2), 256, 0, s>>>(dd + n0 + n1, n2, h->xs64, t64);
+            else
+                k_vtx<float, float, 2><<<grid(n2), 256, 0, s>>>(dd + n0 + n1, n2, h->xs32, t32);
             HMG_LAUNCH_CHECK();
         }
     }
@@ -681,14 +692,16 @@ hmg_status matvec_device(hmg_matrix* h, const double* x, double* y)
     if (h->ntiles > 0 && bulk_k2) {
         if ((st = launch_tiles_bulk(h, fp64, y))) return st;
     } else if (h->ntiles > 0) {
+        const PairDesc* pd = static_cast<const PairDesc*>(h->pair_desc);
         if (fp64)
-            k_tile_matvec<double><<<h->ntiles, 256, 0, s>>>((const PairDesc*)h->pair_desc, h->tile_pair_start,
-                                                            h->tile_r0, h->tile_s, h->perm[0], h->kspec, P,
-                                                            h->xs64, y);
+            k_tile_matvec<double, double><<<h->ntiles, 256, 0, s>>>(pd, h->tile_pair_start, h->tile_r0, h->tile_s,
+                                                                    h->perm[0], h->kspec, P, h->xs64, y);
+        else if (arith64)
+            k_tile_matvec<float, double><<<h->ntiles, 256, 0, s>>>(pd, h->tile_pair_start, h->tile_r0, h->tile_s,
+                                                                   h->perm[0], h->kspec, P, h->xs64, y);
         else
-            k_tile_matvec<float><<<h->ntiles, 256, 0, s>>>((const PairDesc*)h->pair_desc, h->tile_pair_start,
-                                                           h->tile_r0, h->tile_s, h->perm[0], h->kspec, P,
-                                                           h->xs64, y);
+            k_tile_matvec<float, float><<<h->ntiles, 256, 0, s>>>(pd, h->tile_pair_start, h->tile_r0, h->tile_s,
+                                                                  h->perm[0], h->kspec, P, h->xs64, y);
         HMG_LAUNCH_CHECK();
     }
     if (h->profiling) HMG_CUDA_TRY(cudaEventRecord(h->ev[3], s));

@@ -130,6 +130,10 @@ class HMatrix:
         """0: streaming (bulk-copy) product kernels, 1: plain-load kernels."""
         self._call("hmg_set_matvec_variant", int(variant))
 
+    def set_product_precision(self, precision: int):
+        """Arithmetic of products over FP32/mixed storage: PREC_FP32 (default) or PREC_FP64."""
+        self._call("hmg_set_product_precision", int(precision))
+
     def set_profiling(self, on: bool = True):
         self._call("hmg_set_profiling", 1 if on else 0)
 

@@ -70,6 +70,7 @@ typedef struct {
     int near_precision, far_precision, near_mode;
     int64_t far_u_bytes;      /* bytes of the stored U terms (sum m1 * rank * size, no padding) */
     int64_t far_v_bytes;      /* bytes of the stored V terms */
+    int matvec_launches;      /* kernels one hmg_matvec launches (plain-load kernels) */
 } hmg_info;
 
 /* message of the last failed call on this thread ("" if none) */
@@ -132,8 +133,12 @@ hmg_status hmg_full_matvec_rows(hmg_matrix* h, const double* x, const int* rows,
 /* Kernel-ridge solve (H + shift I) x = b by conjugate gradients with the handle's
  * H-matvec as operator (n1 == n2 and a symmetric positive definite kernel).  b and
  * x are device vectors in the caller's order; x holds the initial guess and
- * receives the solution.  FP64 vectors, inner products and stopping test; refine
- * != 0 wraps CG in iterative refinement with the residual recomputed in FP64.
+ * receives the solution.  FP64 vectors, inner products and stopping test.  refine
+ * == 0: products in the handle's arithmetic (hmg_set_product_precision).  refine !=
+ * 0: the residual is that of the stored operator applied in FP64 -- true residuals
+ * use FP64-arithmetic products, CG steps use them until |r| <= 5e5 tol |b| and the
+ * handle's arithmetic after (relaxed inexact Krylov), with restarts from the true
+ * residual if the recurrence drifted.
  * Stops when |b - (H + shift I) x| <= tol |b| or after maxit products.  iters and
  * relres (may be NULL) receive the CG iterations and the final relative residual,
  * recomputed from x.  Synchronous.  No reference counterpart (hmglib has no solver;
@@ -160,6 +165,13 @@ hmg_status hmg_get_profile(hmg_matrix* h, double* ms4);
  * above 128).  Both give the same product to rounding (variant 0 sums in FP64,
  * variant 1 sums each slice in FP32 and the slices in FP64). */
 hmg_status hmg_set_matvec_variant(hmg_matrix* h, int variant);
+
+/* Arithmetic of the products over FP32 or mixed storage (no reference counterpart):
+ * HMG_PREC_FP32 (default) multiplies each slice in FP32 and sums the slices in FP64;
+ * HMG_PREC_FP64 converts every stored value and multiplies in FP64, so the stored
+ * operator is applied exactly (to FP64 rounding).  FP64 storage always uses FP64.
+ * hmg_cg_solve with refine chooses the arithmetic of its products itself. */
+hmg_status hmg_set_product_precision(hmg_matrix* h, int precision);
 
 /* Free the handle and all device memory it owns.  Replaces destroy_h_matrix_data
  * (hmglib.cu:305-348). */

@@ -269,3 +269,35 @@ def test_errors_are_statuses_not_crashes(hmg, cuda):
         H.set_near_mode(hmg.NEAR_STORED)  # nothing stored
     H.matvec(np.zeros(100))
     H.close()
+
+
+@pytest.mark.parametrize("prec", [1, 2], ids=["fp32", "mixed"])
+def test_fp64_arithmetic_products(hmg, cuda, prec):
+    """FP64 arithmetic over FP32 / mixed storage applies the stored operator exactly:
+    the product is linear to FP64 rounding (FP32 arithmetic is linear only to ~1e-7)
+    and its distance to the FP64 direct product is the storage error alone."""
+    torch = cuda
+    n = 40000
+    p = make_points("uniform", n, 3, 5)
+    rng = np.random.default_rng(5)
+    x, z = rng.uniform(-1, 1, n), rng.uniform(-1, 1, n)
+    H = engine(hmg, p, p, 1.5, 128, rule=1)
+    H.set_kernel(hmg.KERNEL_MATERN32, 0.2, 0.0)
+    H.precompute_aca(64, 1e-8, prec)
+    H.precompute_dense(prec)
+    y32 = H.matvec(x)
+    H.set_product_precision(hmg.PREC_FP64)
+    y64 = H.matvec(x)
+    np.testing.assert_array_equal(H.matvec(x), y64)
+    a, c = 0.75, -1.25
+    lin = rel_err(H.matvec(a * x + c * z), a * y64 + c * H.matvec(z))
+    assert lin < 1e-13, lin
+    dy = torch.empty(n, dtype=torch.float64, device="cuda")
+    H.full_matvec(_torch_vec(torch, x), dy)
+    torch.cuda.synchronize()
+    yd = dy.cpu().numpy()
+    assert rel_err(y64, yd) < 2.5e-7, rel_err(y64, yd)
+    assert rel_err(y64, y32) < 3e-7
+    with pytest.raises(hmg.HmgError):
+        H.set_product_precision(hmg.PREC_MIXED)
+    H.close()
