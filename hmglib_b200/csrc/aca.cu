@@ -326,8 +326,12 @@ __global__ void k_aca_compact(BlockGeom g, AcaBatch B, const int* tile_r0, const
 // FP32: with sigma_l = |u_l| |v_l| and S = |U V^T|_F, the terms l with
 // sum_{l' >= l} sigma_l' <= TAU16 * S are stored in FP16 (unit roundoff 4.9e-4,
 // error <~ 1e-3 TAU16 S) and those with a tail below TAU8 * S in FP8 e4m3 (error
-// <~ 0.07 TAU8 S).  Each short term is scaled (u by su, v by sv: to [-1, 1] in
-// FP16, to [-448, 448] in FP8) and su*sv is folded into t_l = v_l^T x.
+// <~ 0.07 TAU8 S).  The FP8 count is rounded down to a multiple of 4 and the FP16
+// count to a multiple of 2 (the remainder moves up a tier): short terms are stored
+// interleaved in pairs (FP16) and quads (FP8), so that every 16-byte chunk of every
+// tier holds four consecutive rows (U) or columns (V^T) of 1, 2 or 4 terms.  Each
+// short term is scaled (u by su, v by sv: to [-1, 1] in FP16, to [-448, 448] in FP8)
+// and su*sv is folded into t_l = v_l^T x.
 // ---------------------------------------------------------------------------
 static constexpr double TAU16 = 1e-4;
 static constexpr double TAU8 = 1.5e-6;
@@ -387,6 +391,8 @@ __global__ void __launch_bounds__(256) k_aca_tiers(BlockGeom g, AcaBatch B, Tier
             if (tail <= TAU8 * S) s8 = l;
         }
         if (s8 < s16) s8 = s16;
+        s8 = r - ((r - s8) & ~3);          // FP8 terms: a multiple of 4
+        s16 = s8 - ((s8 - s16) & ~1);      // FP16 terms: a multiple of 2
         T.r32[e] = s16;
         T.r16[e] = s8 - s16;
         const long long so = T.soff[e];
@@ -407,11 +413,12 @@ __global__ void __launch_bounds__(256) k_aca_tiers(BlockGeom g, AcaBatch B, Tier
     }
 }
 
-// Mixed storage of one block.  U tile slices: [s_pad x r32 FP32][s_pad x r16 FP16]
-// [s_pad x r8 FP8], each column-major; a slice takes s_pad * bpr bytes with
-// bpr = 4 r32 + 2 r16 + r8 rounded up to 4.  V^T: r32 rows of m2p FP32, r16 rows of
-// m2p8 (m2 rounded up to 8) FP16, r8 rows of m2p16 (m2 rounded up to 16) FP8, then
-// r FP32 factors su_l sv_l (1 for FP32 terms).
+// Mixed storage of one block (m2p = m2 rounded up to 4, s_pad = tile rows rounded up
+// to 4).  V^T: r32 FP32 rows of m2p; r16/2 FP16 pair rows, element (j, t) of pair g
+// at half index (g m2p + j) 2 + t; r8/4 FP8 quad rows, element (j, t) of quad g at
+// byte (g m2p + j) 4 + t; then r FP32 factors su_l sv_l (1 for FP32 terms).  U tile
+// slices: s_pad x r32 FP32 column-major, then the pairs [g][i][2] in FP16 and the
+// quads [g][i][4] in FP8; a slice takes s_pad * (4 r32 + 2 r16 + r8) bytes.
 __global__ void __launch_bounds__(256)
 k_aca_compact_mixed(BlockGeom g, AcaBatch B, TierOut T, const int* tile_r0, const int* tile_s,
                     const int* tile_pstart, const int* tfirst, const int* tlast, void* const* ptrU,
@@ -426,29 +433,31 @@ k_aca_compact_mixed(BlockGeom g, AcaBatch B, TierOut T, const int* tile_r0, cons
     const long long so = T.soff[e];
     const double* U = B.U + B.uoff[e];
     const double* V = B.V + B.voff[e];
-    const int m2p = (m2 + 3) & ~3, m2p8 = (m2 + 7) & ~7, m2p16 = (m2 + 15) & ~15;
+    const int m2p = (m2 + 3) & ~3;
     // V^T
     float* v32 = static_cast<float*>(ptrV[b]);
     __half* v16 = reinterpret_cast<__half*>(v32 + (size_t)r32 * m2p);
-    __nv_fp8_storage_t* v8 = reinterpret_cast<__nv_fp8_storage_t*>(v16 + (size_t)r16 * m2p8);
-    float* scal = reinterpret_cast<float*>(v8 + (size_t)r8 * m2p16);
+    __nv_fp8_storage_t* v8 = reinterpret_cast<__nv_fp8_storage_t*>(v16 + (size_t)r16 * m2p);
+    float* scal = reinterpret_cast<float*>(v8 + (size_t)r8 * m2p);
     for (long long idx = threadIdx.x; idx < (long long)r32 * m2p; idx += blockDim.x) {
-        int l = (int)(idx / m2p), j = (int)(idx % m2p);
+        const int l = (int)(idx / m2p), j = (int)(idx % m2p);
         v32[idx] = j < m2 ? (float)V[j + (size_t)l * m2] : 0.0f;
     }
-    for (long long idx = threadIdx.x; idx < (long long)r16 * m2p8; idx += blockDim.x) {
-        int l = r32 + (int)(idx / m2p8), j = (int)(idx % m2p8);
-        float v = j < m2 ? (float)(V[j + (size_t)l * m2] / (double)T.sv[so + l]) : 0.0f;
+    for (long long idx = threadIdx.x; idx < (long long)r16 * m2p; idx += blockDim.x) {
+        const int t = (int)(idx & 1), j = (int)((idx >> 1) % m2p), gp = (int)((idx >> 1) / m2p);
+        const int l = r32 + 2 * gp + t;
+        const float v = j < m2 ? (float)(V[j + (size_t)l * m2] / (double)T.sv[so + l]) : 0.0f;
         v16[idx] = __float2half_rn(v);
     }
-    for (long long idx = threadIdx.x; idx < (long long)r8 * m2p16; idx += blockDim.x) {
-        int l = r32 + r16 + (int)(idx / m2p16), j = (int)(idx % m2p16);
-        float v = j < m2 ? (float)(V[j + (size_t)l * m2] / (double)T.sv[so + l]) : 0.0f;
+    for (long long idx = threadIdx.x; idx < (long long)r8 * m2p; idx += blockDim.x) {
+        const int t = (int)(idx & 3), j = (int)((idx >> 2) % m2p), gq = (int)((idx >> 2) / m2p);
+        const int l = r32 + r16 + 4 * gq + t;
+        const float v = j < m2 ? (float)(V[j + (size_t)l * m2] / (double)T.sv[so + l]) : 0.0f;
         v8[idx] = __nv_cvt_float_to_fp8(v, __NV_SATFINITE, __NV_E4M3);
     }
     for (int l = threadIdx.x; l < r; l += blockDim.x) scal[l] = T.su[so + l] * T.sv[so + l];
     // U tile slices
-    const int bpr = (4 * r32 + 2 * r16 + r8 + 3) & ~3;
+    const int bpr = 4 * r32 + 2 * r16 + r8;
     const int p0 = tile_pstart[tfirst[b]];
     char* ubase = static_cast<char*>(ptrU[b]);
     for (int t = tfirst[b]; t <= tlast[b]; t++) {
@@ -458,22 +467,21 @@ k_aca_compact_mixed(BlockGeom g, AcaBatch B, TierOut T, const int* tile_r0, cons
         __half* u16 = reinterpret_cast<__half*>(slice + (size_t)sp * 4 * r32);
         __nv_fp8_storage_t* u8 = reinterpret_cast<__nv_fp8_storage_t*>(slice + (size_t)sp * (4 * r32 + 2 * r16));
         for (int idx = threadIdx.x; idx < sp * r32; idx += blockDim.x) {
-            int l = idx / sp, i = idx % sp;
+            const int l = idx / sp, i = idx % sp;
             u32[idx] = i < s ? (float)U[(size_t)l * m1 + tr + i] : 0.0f;
         }
         for (int idx = threadIdx.x; idx < sp * r16; idx += blockDim.x) {
-            int l = r32 + idx / sp, i = idx % sp;
-            float u = i < s ? (float)(U[(size_t)l * m1 + tr + i] / (double)T.su[so + l]) : 0.0f;
+            const int q = idx & 1, i = (idx >> 1) % sp, gp = (idx >> 1) / sp;
+            const int l = r32 + 2 * gp + q;
+            const float u = i < s ? (float)(U[(size_t)l * m1 + tr + i] / (double)T.su[so + l]) : 0.0f;
             u16[idx] = __float2half_rn(u);
         }
         for (int idx = threadIdx.x; idx < sp * r8; idx += blockDim.x) {
-            int l = r32 + r16 + idx / sp, i = idx % sp;
-            float u = i < s ? (float)(U[(size_t)l * m1 + tr + i] / (double)T.su[so + l]) : 0.0f;
+            const int q = idx & 3, i = (idx >> 2) % sp, gq = (idx >> 2) / sp;
+            const int l = r32 + r16 + 4 * gq + q;
+            const float u = i < s ? (float)(U[(size_t)l * m1 + tr + i] / (double)T.su[so + l]) : 0.0f;
             u8[idx] = __nv_cvt_float_to_fp8(u, __NV_SATFINITE, __NV_E4M3);
         }
-        // zero the slice's tail padding (bpr rounding)
-        const int used = sp * (4 * r32 + 2 * r16 + r8);
-        for (int idx = used + threadIdx.x; idx < sp * bpr; idx += blockDim.x) slice[idx] = 0;
     }
 }
 
@@ -630,12 +638,11 @@ hmg_status run_aca(hmg_matrix* h, int k, double eps, int precision)
                 const int r32 = b32[e], r16 = b16[e], r8 = r - r32 - r16;
                 r32v[bb] = r32;
                 r16v[bb] = r16;
-                const long long bpr = (4 * r32 + 2 * r16 + r8 + 3) & ~3;
+                const long long bpr = 4 * r32 + 2 * r16 + r8;
                 bytes += rows_p * bpr;
                 bytes = (bytes + 255) & ~255ll;
                 ofsV[e] = bytes;
-                bytes += (long long)r32 * ((m2 + 3) & ~3) * 4 + (long long)r16 * ((m2 + 7) & ~7) * 2 +
-                         (long long)r8 * ((m2 + 15) & ~15) + 4ll * r;
+                bytes += ((m2 + 3) & ~3) * bpr + 4ll * r;
                 alg_u += m1 * (4ll * r32 + 2ll * r16 + r8);
                 alg_v += m2 * (4ll * r32 + 2ll * r16 + r8);
             } else {

@@ -453,23 +453,25 @@ hmg_status hmg_get_ranks(hmg_matrix* h, int* ranks)
     return HMG_OK;
 }
 
-// Decodes one block of the mixed format: per tile slice [s_pad x r32 FP32 | s_pad x r16
-// FP16 | s_pad x r8 FP8-e4m3] column-major, V^T as r32 FP32 rows (stride m2 rounded to 4),
-// r16 FP16 rows (stride rounded to 8), r8 FP8 rows (stride rounded to 16), then r FP32 term
-// scales.  The scale of each term is folded into the returned U column.
+// Decodes one block of the mixed format (m2p = m2 rounded up to 4): V^T as r32 FP32
+// rows of m2p, r16/2 FP16 pair rows with element (j, t) at (g m2p + j) 2 + t, r8/4
+// FP8-e4m3 quad rows with element (j, t) at (g m2p + j) 4 + t, then r FP32 term
+// scales; each U tile slice as s_pad x r32 FP32 column-major, pairs [g][i][2] in
+// FP16, quads [g][i][4] in FP8.  The scale of each term is folded into the returned
+// U column.
 static hmg_status get_factors_mixed(hmg_matrix* h, int block, void* pu, void* pv, double* U, double* V)
 {
     const int r = h->h_rank[block], m1 = h->h_m1[block], m2 = h->h_m2[block];
     const int r32 = h->h_r32[block], r16 = h->h_r16[block], r8 = r - r32 - r16;
-    const int m2p = (m2 + 3) & ~3, m2p8 = (m2 + 7) & ~7, m2p16 = (m2 + 15) & ~15;
-    const size_t vbytes = (size_t)r32 * m2p * 4 + (size_t)r16 * m2p8 * 2 + (size_t)r8 * m2p16 + (size_t)r * 4;
+    const int m2p = (m2 + 3) & ~3;
+    const size_t vbytes = (size_t)m2p * (4 * r32 + 2 * r16 + r8) + (size_t)r * 4;
     std::vector<char> hv(vbytes);
     HMG_CUDA_TRY(cudaMemcpy(hv.data(), pv, vbytes, cudaMemcpyDeviceToHost));
     const float* v32 = (const float*)hv.data();
     const __half* v16 = (const __half*)(v32 + (size_t)r32 * m2p);
-    const __nv_fp8_storage_t* v8 = (const __nv_fp8_storage_t*)(v16 + (size_t)r16 * m2p8);
+    const __nv_fp8_storage_t* v8 = (const __nv_fp8_storage_t*)(v16 + (size_t)r16 * m2p);
     std::vector<float> scal(r);
-    std::memcpy(scal.data(), v8 + (size_t)r8 * m2p16, sizeof(float) * r);
+    std::memcpy(scal.data(), v8 + (size_t)r8 * m2p, sizeof(float) * r);
     auto fp8 = [](__nv_fp8_storage_t q) -> double {
         return (double)__half2float(__half(__nv_cvt_fp8_to_halfraw(q, __NV_E4M3)));
     };
@@ -477,12 +479,17 @@ static hmg_status get_factors_mixed(hmg_matrix* h, int block, void* pu, void* pv
         for (int j = 0; j < m2; j++) {
             double v;
             if (l < r32) v = v32[(size_t)l * m2p + j];
-            else if (l < r32 + r16) v = __half2float(v16[(size_t)(l - r32) * m2p8 + j]);
-            else v = fp8(v8[(size_t)(l - r32 - r16) * m2p16 + j]);
+            else if (l < r32 + r16) {
+                const int q = l - r32;
+                v = __half2float(v16[((size_t)(q >> 1) * m2p + j) * 2 + (q & 1)]);
+            } else {
+                const int q = l - r32 - r16;
+                v = fp8(v8[((size_t)(q >> 2) * m2p + j) * 4 + (q & 3)]);
+            }
             V[(size_t)l * m2 + j] = v;
         }
     const int tf = h->h_blk_tfirst[block], tl = h->h_blk_tlast[block];
-    const int bpr = (4 * r32 + 2 * r16 + r8 + 3) & ~3;
+    const int bpr = 4 * r32 + 2 * r16 + r8;
     const int rows_p = h->h_tile_pstart[tl + 1] - h->h_tile_pstart[tf];
     std::vector<char> hu((size_t)rows_p * bpr);
     HMG_CUDA_TRY(cudaMemcpy(hu.data(), pu, hu.size(), cudaMemcpyDeviceToHost));
@@ -500,8 +507,13 @@ static hmg_status get_factors_mixed(hmg_matrix* h, int block, void* pu, void* pv
             for (int i = 0; i < s; i++) {
                 double u;
                 if (l < r32) u = u32[(size_t)l * sp + i];
-                else if (l < r32 + r16) u = (double)__half2float(u16[(size_t)(l - r32) * sp + i]) * scal[l];
-                else u = fp8(u8[(size_t)(l - r32 - r16) * sp + i]) * scal[l];
+                else if (l < r32 + r16) {
+                    const int q = l - r32;
+                    u = (double)__half2float(u16[((size_t)(q >> 1) * sp + i) * 2 + (q & 1)]) * scal[l];
+                } else {
+                    const int q = l - r32 - r16;
+                    u = fp8(u8[((size_t)(q >> 2) * sp + i) * 4 + (q & 3)]) * scal[l];
+                }
                 U[(size_t)l * m1 + (tr0[t - tf] - r0) + i] = u;
             }
     }

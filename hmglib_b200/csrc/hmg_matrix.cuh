@@ -84,6 +84,8 @@ struct hmg_matrix {
     void* k1_units = nullptr;      // K1 pieces of V^T (rows of one storage tier), grouped by tier
     int nk1 = 0;
     int k1_count[3] = {0, 0, 0};   // pieces per tier (FP32/FP64, FP16, FP8)
+    int k1_piece_start[3][5] = {};  // per tier: first piece of each lane-group class, end
+    int k1_task_start[3][5] = {};   // per tier: first warp task of each class, task count
     int* far_list = nullptr;       // admissible blocks with rank > 0 (streaming V^T x)
     int nfar_list = 0;
     int* dev_err = nullptr;        // pipeline wait time-out flag (0 = fine)

@@ -27,14 +27,15 @@
 namespace hmg {
 
 struct K1Unit {
-    int b, l0, l1, tier;  // tier: 0 storage type (FP32/FP64), 1 FP16, 2 FP8 (mixed)
+    int b, l0, l1, tier;  // terms [l0, l1); tier: 0 storage type (FP32/FP64), 1 FP16, 2 FP8
 };
 
-// A K1 piece resolved to addresses: rows [l0, l1) of one storage tier of V_b^T.
+// A K1 piece resolved to addresses: terms [l0, l1) of one storage tier of V_b^T, as
+// rows of single terms (tier 0), interleaved pairs (FP16) or quads (FP8).
 struct K1Desc {
-    const void* v;       // row l0 of the tier
-    const float* scal;   // the rows' term scales (FP16/FP8 tiers), else null
-    long long tout;      // tbuf index of row l0
+    const void* v;       // first row of the piece
+    const float* scal;   // the terms' scales (FP16/FP8 tiers), else null
+    long long tout;      // tbuf index of term l0
     int c0, m2;          // the block's x segment
     int nrows, row_bytes;  // rows in the piece; row stride, a multiple of 16 bytes
     int pad[2];
@@ -169,7 +170,7 @@ __global__ void k_build_desc(const int* tile_pair_start, int ntiles, const int* 
         } else if (mixed) {
             // FP32 / FP16 / FP8 terms; a tile slice takes s_pad * bpr bytes
             const int r = rank[b], r32 = tier32[b], r16 = tier16[b], r8 = r - r32 - r16;
-            const int bpr = (4 * r32 + 2 * r16 + r8 + 3) & ~3;
+            const int bpr = 4 * r32 + 2 * r16 + r8;
             d.kind = PAIR_FAR_MIXED;
             d.ncol = r32;
             d.c0 = r16;
@@ -195,29 +196,37 @@ __global__ void k_build_k1desc(const K1Unit* units, int n, const int* blk_c0, co
     const K1Unit un = units[i];
     const int b = un.b, m2 = blk_m2[b], r = rank[b];
     const int r32 = mixed ? tier32[b] : r, r16 = mixed ? tier16[b] : 0, r8 = r - r32 - r16;
-    const size_t m2p = (m2 + 3) & ~3, m2p8 = (m2 + 7) & ~7, m2p16 = (m2 + 15) & ~15;
+    const size_t m2p = (m2 + 3) & ~3;
     const char* V = static_cast<const char*>(ptrV[b]);
-    const size_t b32 = (size_t)r32 * m2p * esz, b16 = (size_t)r16 * m2p8 * 2;
+    const size_t b32 = (size_t)r32 * m2p * esz, b16 = (size_t)r16 * m2p * 2;
+    // rows of a piece: single terms (tier 0), interleaved pairs (FP16), quads (FP8)
     K1Desc d;
     if (un.tier == 0) {
         d.row_bytes = (int)(m2p * esz);
         d.v = V + (size_t)un.l0 * d.row_bytes;
+        d.nrows = un.l1 - un.l0;
     } else if (un.tier == 1) {
-        d.row_bytes = (int)(m2p8 * 2);
-        d.v = V + b32 + (size_t)(un.l0 - r32) * d.row_bytes;
+        d.row_bytes = (int)(m2p * 4);
+        d.v = V + b32 + (size_t)((un.l0 - r32) >> 1) * d.row_bytes;
+        d.nrows = (un.l1 - un.l0) >> 1;
     } else {
-        d.row_bytes = (int)m2p16;
-        d.v = V + b32 + b16 + (size_t)(un.l0 - r32 - r16) * d.row_bytes;
+        d.row_bytes = (int)(m2p * 4);
+        d.v = V + b32 + b16 + (size_t)((un.l0 - r32 - r16) >> 2) * d.row_bytes;
+        d.nrows = (un.l1 - un.l0) >> 2;
     }
     d.scal = un.tier == 0 ? nullptr
-                          : reinterpret_cast<const float*>(V + b32 + b16 + (size_t)r8 * m2p16) + un.l0;
+                          : reinterpret_cast<const float*>(V + b32 + b16 + (size_t)r8 * m2p) + un.l0;
     d.tout = rank_off[b] + un.l0;
     d.c0 = blk_c0[b];
     d.m2 = m2;
-    d.nrows = un.l1 - un.l0;
     d.pad[0] = d.pad[1] = 0;
     out[i] = d;
 }
+
+// K1 step shape per tier: rows per step R = 4 / (terms per row) so that a lane holds
+// four term sums, and K1_NCH = 8 / R chunks per row, so that a lane has eight 16-byte
+// loads in flight whatever the tier.
+static constexpr int k1_nch(int tier) { return tier == 0 ? 2 : (tier == 1 ? 4 : 8); }
 
 static hmg_status ensure_desc(hmg_matrix* h, int elem)
 {
@@ -243,10 +252,12 @@ static hmg_status ensure_desc(hmg_matrix* h, int elem)
             h->far_prec == HMG_PREC_MIXED ? 1 : 0, (PairDesc*)h->pair_desc);
         HMG_LAUNCH_CHECK();
     }
-    // K1 pieces: rows of V_b^T of one storage tier, in runs of at most ~64 KB, grouped
-    // by tier (one launch per tier)
+    // K1 pieces: terms of V_b^T of one storage tier, in runs of at most ~64 KB.  Each
+    // piece gets the widest lane group 2^LG (LG 2..5) whose lanes still get k1_nch
+    // chunks of a row each; pieces are ordered by tier, then by LG (one launch per
+    // tier; a warp takes 32 / 2^LG pieces of one class at a time).
     dfree(h->k1_units, s);
-    std::vector<K1Unit> units[3];
+    std::vector<K1Unit> units[3][4];
     const bool mixed = h->far_prec == HMG_PREC_MIXED;
     for (int b = h->ndense; b < h->nblocks; b++) {
         const int r = h->h_rank[b];
@@ -254,17 +265,33 @@ static hmg_status ensure_desc(hmg_matrix* h, int elem)
         const long long m2 = h->h_m2[b];
         const int r32 = mixed ? h->h_r32[b] : r, r16 = mixed ? h->h_r16[b] : 0;
         const int lo[3] = {0, r32, r32 + r16}, hi[3] = {r32, r32 + r16, r};
-        const long long rb[3] = {((m2 + 3) & ~3ll) * far_esz, ((m2 + 7) & ~7ll) * 2, (m2 + 15) & ~15ll};
+        // bytes of one piece row: a term (tier 0), a pair of FP16 or a quad of FP8 terms
+        const long long rb[3] = {((m2 + 3) & ~3ll) * far_esz, ((m2 + 3) & ~3ll) * 4, ((m2 + 3) & ~3ll) * 4};
+        const int tg[3] = {1, 2, 4};
         for (int tier = 0; tier < 3; tier++) {
-            const int per = (int)std::max(1ll, 65536ll / rb[tier]);
+            if (lo[tier] == hi[tier]) continue;
+            const long long per_lane = rb[tier] / 16 / k1_nch(tier);  // chunks per lane at 1 lane
+            int lg = 2;
+            while (lg < 5 && (1ll << (lg + 1)) <= per_lane) lg++;
+            const int per = (int)std::max(1ll, 65536ll / rb[tier]) * tg[tier];
             for (int l = lo[tier]; l < hi[tier]; l += per)
-                units[tier].push_back({b, l, std::min(hi[tier], l + per), tier});
+                units[tier][lg - 2].push_back({b, l, std::min(hi[tier], l + per), tier});
         }
     }
     std::vector<K1Unit> all;
     for (int tier = 0; tier < 3; tier++) {
-        h->k1_count[tier] = (int)units[tier].size();
-        all.insert(all.end(), units[tier].begin(), units[tier].end());
+        const int first = (int)all.size();
+        int tasks = 0;
+        for (int c = 0; c < 4; c++) {
+            h->k1_piece_start[tier][c] = (int)all.size();
+            h->k1_task_start[tier][c] = tasks;
+            all.insert(all.end(), units[tier][c].begin(), units[tier][c].end());
+            const int g = 32 >> (c + 2);
+            tasks += ((int)units[tier][c].size() + g - 1) / g;
+        }
+        h->k1_piece_start[tier][4] = (int)all.size();
+        h->k1_task_start[tier][4] = tasks;
+        h->k1_count[tier] = (int)all.size() - first;
     }
     h->nk1 = (int)all.size();
     K1Desc* dd = nullptr;
@@ -345,10 +372,11 @@ __device__ __forceinline__ void unpack8(const uint4& u, float* o)
     }
 }
 
-// 16 bytes of one tier to values: FP32 (4), FP64 (2), FP16 (8), FP8 e4m3 (16)
+// 16 bytes of one tier to values, [column][term]: FP32 4 x 1, FP64 2 x 1, FP16 pairs
+// 4 x 2, FP8 e4m3 quads 4 x 4
 template <typename T, int TIER> struct Chunk;
 template <> struct Chunk<float, 0> {
-    static constexpr int N = 4;
+    static constexpr int NC = 4, TG = 1;
     __device__ static void get(const uint4& u, float* o)
     {
         o[0] = __uint_as_float(u.x); o[1] = __uint_as_float(u.y);
@@ -356,7 +384,7 @@ template <> struct Chunk<float, 0> {
     }
 };
 template <> struct Chunk<double, 0> {
-    static constexpr int N = 2;
+    static constexpr int NC = 2, TG = 1;
     __device__ static void get(const uint4& u, double* o)
     {
         o[0] = __hiloint2double((int)u.y, (int)u.x);
@@ -364,24 +392,31 @@ template <> struct Chunk<double, 0> {
     }
 };
 template <> struct Chunk<float, 1> {
-    static constexpr int N = 8;
+    static constexpr int NC = 4, TG = 2;
     __device__ static void get(const uint4& u, float* o) { unpack16(u, o); }
 };
 template <> struct Chunk<float, 2> {
-    static constexpr int N = 16;
+    static constexpr int NC = 4, TG = 4;
     __device__ static void get(const uint4& u, float* o) { unpack8(u, o); }
 };
 
 // K1: t_b[l] = s_l sum_j V_b^T[l][j] x[c0_b + j] over the pieces of one storage tier.
-// A warp takes a piece; its lanes split into groups of LPR = 4..32 lanes (the power of
-// two <= the row's 16-byte chunks, so short rows do not leave lanes idle), each group
-// takes four rows (FP32/FP64, two chunks per row per step) or eight rows (FP16/FP8,
-// one chunk) at a time and strides over their chunks; the row width is a compile-time
-// constant of each code path.  A group's row sums are reduced by a transposing
-// butterfly in a fixed order: t is deterministic.  The next piece's descriptor is
-// loaded while the current one streams.
-// Sum of the R row partials of an LPR-lane group: a transposing butterfly (log2 R
-// halving exchanges, then plain ones).  Afterwards lane `sub` holds the total of row
+//
+// A 16-byte chunk holds NC consecutive columns of TG terms (FP32: 4 x 1, FP64: 2 x 1,
+// FP16 pairs: 4 x 2, FP8 quads: 4 x 4), so every tier is read with the same chunk
+// loads and every x value loaded serves 4 terms of a lane.  A warp takes a task: up
+// to 32 / LPR pieces of one lane-group class, one per group of LPR = 2^LG lanes, so
+// that short pieces (the FP16/FP8 tails of small blocks) still keep 32 lanes x 8
+// loads in flight.  Each group steps through its piece R rows (4 terms) at a time
+// with NCH chunks per row per lane, then sums the four term partials over its lanes
+// with a transposing butterfly in a fixed order: t is deterministic.
+struct K1Classes {
+    int piece_start[5];  // first piece of each class (LG = 2..5), then the end
+    int task_start[5];   // first task of each class, then the task count
+};
+
+// Sum of the R partials of an LPR-lane group: a transposing butterfly (log2 R halving
+// exchanges, then plain ones).  Afterwards lane `sub` holds the total of partial
 // sub / (LPR / R); the summation order is fixed.
 template <int R, int LPR, typename T>
 __device__ __forceinline__ T rows_butterfly(T (&acc)[R], int sub)
@@ -404,25 +439,21 @@ __device__ __forceinline__ T rows_butterfly(T (&acc)[R], int sub)
     return a;
 }
 
-// One K1 piece: lane groups of LPR = 2^LG lanes, each taking R rows at a time and
-// NCH 16-byte chunks of each row per step (R * NCH loads in flight per lane).
-// S: the tier's decoded type; T: arithmetic type.
-template <typename S, typename T, int TIER, int LG, int R, int NCH>
-__device__ __forceinline__ void vtx_piece(const K1Desc& d, const T* __restrict__ xs, T* __restrict__ tbuf,
-                                          int lane)
+// One task's share of a group: piece d (when `have`), group lanes `sub` of 2^LG.
+template <typename S, typename T, int TIER, int LG>
+__device__ __forceinline__ void vtx_group(const K1Desc& d, bool have, const T* __restrict__ xs,
+                                          T* __restrict__ tbuf, int lane)
 {
     typedef Chunk<S, TIER> C;
-    constexpr int EPC = C::N;
-    constexpr int LPR = 1 << LG, G = 32 >> LG;
-    static_assert(LPR >= R, "a group needs at least R lanes");
-    const int cpr = d.row_bytes >> 4;
-    const int grp = lane >> LG, sub = lane & (LPR - 1);
+    constexpr int NC = C::NC, TG = C::TG;
+    constexpr int R = 4 / TG, NCH = k1_nch(TIER);
+    constexpr int LPR = 1 << LG;
+    const int sub = lane & (LPR - 1);
+    const int nrows = have ? d.nrows : 0;
+    const int cpr = have ? (d.row_bytes >> 4) : 0;
     const char* vb = static_cast<const char*>(d.v);
-    for (int rb = 0; rb < d.nrows; rb += G * R) {
-        const int row = rb + grp * R;
-        T acc[R];
-#pragma unroll
-        for (int k = 0; k < R; k++) acc[k] = (T)0;
+    for (int row = 0; __any_sync(0xffffffffu, row < nrows); row += R) {
+        T acc[4] = {(T)0, (T)0, (T)0, (T)0};
         for (int c = sub; c < cpr; c += NCH * LPR) {
             uint4 raw[NCH][R];
 #pragma unroll
@@ -431,29 +462,31 @@ __device__ __forceinline__ void vtx_piece(const K1Desc& d, const T* __restrict__
 #pragma unroll
                 for (int hh = 0; hh < NCH; hh++) {
                     raw[hh][k] = make_uint4(0u, 0u, 0u, 0u);
-                    if (row + k < d.nrows && c + hh * LPR < cpr) raw[hh][k] = __ldg(rp + c + hh * LPR);
+                    if (row + k < nrows && c + hh * LPR < cpr) raw[hh][k] = __ldg(rp + c + hh * LPR);
                 }
             }
 #pragma unroll
             for (int hh = 0; hh < NCH; hh++) {
-                T xv[EPC];
-                const int e0 = (c + hh * LPR) * EPC;
+                T xv[NC];
+                const int e0 = (c + hh * LPR) * NC;
 #pragma unroll
-                for (int q = 0; q < EPC; q++) xv[q] = e0 + q < d.m2 ? xs[d.c0 + e0 + q] : (T)0;
+                for (int q = 0; q < NC; q++) xv[q] = e0 + q < d.m2 ? xs[d.c0 + e0 + q] : (T)0;
 #pragma unroll
                 for (int k = 0; k < R; k++) {
-                    S f[EPC];
+                    S f[NC * TG];
                     C::get(raw[hh][k], f);
 #pragma unroll
-                    for (int q = 0; q < EPC; q++) acc[k] = fma((T)f[q], xv[q], acc[k]);
+                    for (int q = 0; q < NC; q++)
+#pragma unroll
+                        for (int t = 0; t < TG; t++) acc[k * TG + t] = fma((T)f[q * TG + t], xv[q], acc[k * TG + t]);
                 }
             }
         }
-        T a0 = rows_butterfly<R, LPR>(acc, sub);
-        const int k = sub / (LPR / R);
-        if (sub % (LPR / R) == 0 && row + k < d.nrows) {
-            if (TIER != 0) a0 *= d.scal[row + k];
-            tbuf[d.tout + row + k] = a0;
+        T a = rows_butterfly<4, LPR>(acc, sub);
+        const int k = sub / (LPR / 4);  // partial k: row row + k / TG, term k % TG
+        if (sub % (LPR / 4) == 0 && row + k / TG < nrows) {
+            if (TIER != 0) a *= d.scal[row * TG + k];
+            tbuf[d.tout + row * TG + k] = a;
         }
     }
 }
@@ -462,23 +495,37 @@ __device__ __forceinline__ void vtx_piece(const K1Desc& d, const T* __restrict__
 // FP64 arithmetic over FP32 storage needs more registers: two CTAs per SM there.
 template <typename S, typename T, int TIER>
 __global__ void __launch_bounds__(256, (sizeof(T) == 8 && sizeof(S) == 4) ? 2 : 3)
-k_vtx(const K1Desc* __restrict__ descs, int n, const T* __restrict__ xs, T* __restrict__ tbuf)
+k_vtx(const K1Desc* __restrict__ descs, K1Classes cls, const T* __restrict__ xs, T* __restrict__ tbuf)
 {
     const int lane = threadIdx.x & 31;
     const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int nw = (gridDim.x * blockDim.x) >> 5;
-    if (gw >= n) return;
-    K1Desc d = descs[gw];
-    for (int u = gw; u < n; u += nw) {
-        // unconditional (clamped) so that nothing waits on it before the end of the piece
-        const K1Desc next = descs[min(u + nw, n - 1)];
-        const int cpr = d.row_bytes >> 4;
-        // FP32/FP64 rows: 4 rows x 2 chunks per step; the short FP16/FP8 rows: 8 rows x 1
-        constexpr int RR = TIER == 0 ? 4 : 8, NCH = TIER == 0 ? 2 : 1;
-        if (cpr >= 32) vtx_piece<S, T, TIER, 5, RR, NCH>(d, xs, tbuf, lane);
-        else if (cpr >= 16) vtx_piece<S, T, TIER, 4, RR, NCH>(d, xs, tbuf, lane);
-        else if (cpr >= 8) vtx_piece<S, T, TIER, 3, RR, NCH>(d, xs, tbuf, lane);
-        else vtx_piece<S, T, TIER, 2, 4, NCH>(d, xs, tbuf, lane);
+    const int ntasks = cls.task_start[4];
+    const int last = cls.piece_start[4] - 1;
+    // class, and this lane's piece, of a task
+    auto locate = [&](int task, int& c, int& piece) {
+        c = 0;
+        while (c < 3 && task >= cls.task_start[c + 1]) c++;
+        piece = cls.piece_start[c] + (task - cls.task_start[c]) * (32 >> (c + 2)) + (lane >> (c + 2));
+    };
+    if (gw >= ntasks) return;
+    int c, piece;
+    locate(gw, c, piece);
+    K1Desc d = descs[min(piece, last)];
+    for (int task = gw; task < ntasks; task += nw) {
+        int cn = c, pn = piece;
+        if (task + nw < ntasks) locate(task + nw, cn, pn);
+        // unconditional (clamped) so that nothing waits on it before the end of the task
+        const K1Desc next = descs[min(pn, last)];
+        const bool have = piece < cls.piece_start[c + 1];
+        switch (c) {
+        case 0: vtx_group<S, T, TIER, 2>(d, have, xs, tbuf, lane); break;
+        case 1: vtx_group<S, T, TIER, 3>(d, have, xs, tbuf, lane); break;
+        case 2: vtx_group<S, T, TIER, 4>(d, have, xs, tbuf, lane); break;
+        default: vtx_group<S, T, TIER, 5>(d, have, xs, tbuf, lane); break;
+        }
+        c = cn;
+        piece = pn;
         d = next;
     }
 }
@@ -550,32 +597,34 @@ k_tile_matvec(const PairDesc* desc, const int* tile_pair_start, const int* tile_
                 }
                 if constexpr (sizeof(S) == 4) {
                     if (d.kind == PAIR_FAR_MIXED) {
-                        // FP16 then FP8 terms of the slice: 8 resp. 4 bytes per lane per column
+                        // FP16 pairs then FP8 quads of the slice: a lane's 16 bytes hold its
+                        // 4 rows x 2 resp. 4 terms
                         const char* s16 = (const char*)d.data + (size_t)sp * 4 * d.ncol;
                         const char* s8 = s16 + (size_t)sp * 2 * d.c0;
                         const T* w16 = w + d.ncol;
                         const T* w8 = w16 + d.c0;
 #pragma unroll 4
-                        for (int jj = 0; jj < d.c0; jj++) {
-                            const uint2 raw = *reinterpret_cast<const uint2*>(s16 + ((size_t)jj * sp + row0) * 2);
+                        for (int gp = 0; gp < (d.c0 >> 1); gp++) {
+                            const uint4 raw = *reinterpret_cast<const uint4*>(s16 + ((size_t)gp * sp + row0) * 4);
                             const __half2* h2 = reinterpret_cast<const __half2*>(&raw);
-                            const float2 f0 = __half22float2(h2[0]), f1 = __half22float2(h2[1]);
-                            const T wv = w16[jj];
-                            acc[0] = fma((T)f0.x, wv, acc[0]);
-                            acc[1] = fma((T)f0.y, wv, acc[1]);
-                            acc[2] = fma((T)f1.x, wv, acc[2]);
-                            acc[3] = fma((T)f1.y, wv, acc[3]);
+                            const T wa = w16[2 * gp], wb = w16[2 * gp + 1];
+#pragma unroll
+                            for (int q = 0; q < 4; q++) {
+                                const float2 f = __half22float2(h2[q]);
+                                acc[q] = fma((T)f.y, wb, fma((T)f.x, wa, acc[q]));
+                            }
                         }
 #pragma unroll 4
-                        for (int jj = 0; jj < d.pad; jj++) {
-                            const unsigned raw = *reinterpret_cast<const unsigned*>(s8 + (size_t)jj * sp + row0);
-                            const float2 f0 = fp8x2_to_float2((unsigned short)(raw & 0xffffu));
-                            const float2 f1 = fp8x2_to_float2((unsigned short)(raw >> 16));
-                            const T wv = w8[jj];
-                            acc[0] = fma((T)f0.x, wv, acc[0]);
-                            acc[1] = fma((T)f0.y, wv, acc[1]);
-                            acc[2] = fma((T)f1.x, wv, acc[2]);
-                            acc[3] = fma((T)f1.y, wv, acc[3]);
+                        for (int gq = 0; gq < (d.pad >> 2); gq++) {
+                            const uint4 raw = *reinterpret_cast<const uint4*>(s8 + ((size_t)gq * sp + row0) * 4);
+                            const unsigned wd[4] = {raw.x, raw.y, raw.z, raw.w};
+                            const T w0 = w8[4 * gq], w1 = w8[4 * gq + 1], w2 = w8[4 * gq + 2], w3 = w8[4 * gq + 3];
+#pragma unroll
+                            for (int q = 0; q < 4; q++) {
+                                const float2 f0 = fp8x2_to_float2((unsigned short)(wd[q] & 0xffffu));
+                                const float2 f1 = fp8x2_to_float2((unsigned short)(wd[q] >> 16));
+                                acc[q] = fma((T)f1.y, w3, fma((T)f1.x, w2, fma((T)f0.y, w1, fma((T)f0.x, w0, acc[q]))));
+                            }
                         }
                     }
                 }
@@ -660,31 +709,35 @@ hmg_status matvec_device(hmg_matrix* h, const double* x, double* y, bool fp64_ar
         if ((st = launch_vtx_bulk(h, fp64))) return st;
     } else if (h->nk1 > 0) {
         const K1Desc* dd = static_cast<const K1Desc*>(h->k1_units);
-        const int n0 = h->k1_count[0], n1 = h->k1_count[1], n2 = h->k1_count[2];
-        auto grid = [](int n) { return std::min(ceil_div(n, 8), 148 * 8); };
         double* t64 = static_cast<double*>(h->tbuf);
         float* t32 = static_cast<float*>(h->tbuf);
-        if (n0 > 0) {
-            if (fp64)
-                k_vtx<double, double, 0><<<grid(n0), 256, 0, s>>>(dd, n0, h->xs64, t64);
-            else if (arith64)
-                k_vtx<float, double, 0><<<grid(n0), 256, 0, s>>>(dd, n0, h->xs64, t64);
-            else
-                k_vtx<float, float, 0><<<grid(n0), 256, 0, s>>>(dd, n0, h->xs32, t32);
-            HMG_LAUNCH_CHECK();
-        }
-        if (n1 > 0) {
-            if (arith64)
-                k_vtx<float, double, 1><<<grid(n1), 256, 0, s>>>(dd + n0, n1, h->xs64, t64);
-            else
-                k_vtx<float, float, 1><<<grid(n1), 256, 0, s>>>(dd + n0, n1, h->xs32, t32);
-            HMG_LAUNCH_CHECK();
-        }
-        if (n2 > 0) {
-            if (arith64)
-                k_vtx<float, double, 2><<<grid(n2), 256, 0, s>>>(dd + n0 + n1, n2, h->xs64, t64);
-            else
-                k_vtx<float, float, 2><<<grid(n2), 256, 0, s>>>(dd + n0 + n1, n2, h->xs32, t32);
+        for (int tier = 0; tier < 3; tier++) {
+            K1Classes cls;
+            for (int c = 0; c < 5; c++) {
+                cls.piece_start[c] = h->k1_piece_start[tier][c];
+                cls.task_start[c] = h->k1_task_start[tier][c];
+            }
+            const int ntasks = cls.task_start[4];
+            if (ntasks == 0) continue;
+            const int grid = std::min(ceil_div(ntasks, 8), 148 * 8);
+            if (tier == 0) {
+                if (fp64)
+                    k_vtx<double, double, 0><<<grid, 256, 0, s>>>(dd, cls, h->xs64, t64);
+                else if (arith64)
+                    k_vtx<float, double, 0><<<grid, 256, 0, s>>>(dd, cls, h->xs64, t64);
+                else
+                    k_vtx<float, float, 0><<<grid, 256, 0, s>>>(dd, cls, h->xs32, t32);
+            } else if (tier == 1) {
+                if (arith64)
+                    k_vtx<float, double, 1><<<grid, 256, 0, s>>>(dd, cls, h->xs64, t64);
+                else
+                    k_vtx<float, float, 1><<<grid, 256, 0, s>>>(dd, cls, h->xs32, t32);
+            } else {
+                if (arith64)
+                    k_vtx<float, double, 2><<<grid, 256, 0, s>>>(dd, cls, h->xs64, t64);
+                else
+                    k_vtx<float, float, 2><<<grid, 256, 0, s>>>(dd, cls, h->xs32, t32);
+            }
             HMG_LAUNCH_CHECK();
         }
     }
