@@ -336,6 +336,23 @@ __global__ void k_gather_x(const double* x, const int* perm2, int n, double* xs6
     xs32[j] = (float)v;
 }
 
+// Loads of the stored near field and factors: each byte is read once per product, so
+// they bypass L1 (which keeps the x and t_b values reused across rows) and ask L2 to
+// fetch the whole 256-byte sector group (the neighbouring lanes' and steps' bytes).
+__device__ __forceinline__ uint4 ld_stream(const void* p)
+{
+    uint4 v;
+    asm("ld.global.nc.L1::no_allocate.L2::256B.v4.u32 {%0, %1, %2, %3}, [%4];"
+        : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w)
+        : "l"(p));
+    return v;
+}
+template <typename V4> __device__ __forceinline__ V4 ld_stream_as(const void* p)
+{
+    const uint4 u = ld_stream(p);
+    return *reinterpret_cast<const V4*>(&u);
+}
+
 template <typename T> struct Vec;
 template <> struct Vec<float> { typedef float4 type; static constexpr int N = 4; };
 template <> struct Vec<double> { typedef double2 type; static constexpr int N = 2; };
@@ -462,7 +479,7 @@ __device__ __forceinline__ void vtx_group(const K1Desc& d, bool have, const T* _
 #pragma unroll
                 for (int hh = 0; hh < NCH; hh++) {
                     raw[hh][k] = make_uint4(0u, 0u, 0u, 0u);
-                    if (row + k < nrows && c + hh * LPR < cpr) raw[hh][k] = __ldg(rp + c + hh * LPR);
+                    if (row + k < nrows && c + hh * LPR < cpr) raw[hh][k] = ld_stream(rp + c + hh * LPR);
                 }
             }
 #pragma unroll
@@ -470,7 +487,9 @@ __device__ __forceinline__ void vtx_group(const K1Desc& d, bool have, const T* _
                 T xv[NC];
                 const int e0 = (c + hh * LPR) * NC;
 #pragma unroll
-                for (int q = 0; q < NC; q++) xv[q] = e0 + q < d.m2 ? xs[d.c0 + e0 + q] : (T)0;
+                // V is zero past m2 and x is padded: no bound test (a non-finite x makes
+                // every output non-finite anyway, K having no zero columns)
+                for (int q = 0; q < NC; q++) xv[q] = xs[d.c0 + e0 + q];
 #pragma unroll
                 for (int k = 0; k < R; k++) {
                     S f[NC * TG];
@@ -568,10 +587,10 @@ k_tile_matvec(const PairDesc* desc, const int* tile_pair_start, const int* tile_
             if (active) {
                 int j = 0;
                 for (; j + 4 <= d.ncol; j += 4) {
-                    V4 v0 = *reinterpret_cast<const V4*>(base + (size_t)(j + 0) * sp);
-                    V4 v1 = *reinterpret_cast<const V4*>(base + (size_t)(j + 1) * sp);
-                    V4 v2 = *reinterpret_cast<const V4*>(base + (size_t)(j + 2) * sp);
-                    V4 v3 = *reinterpret_cast<const V4*>(base + (size_t)(j + 3) * sp);
+                    V4 v0 = ld_stream_as<V4>(base + (size_t)(j + 0) * sp);
+                    V4 v1 = ld_stream_as<V4>(base + (size_t)(j + 1) * sp);
+                    V4 v2 = ld_stream_as<V4>(base + (size_t)(j + 2) * sp);
+                    V4 v3 = ld_stream_as<V4>(base + (size_t)(j + 3) * sp);
                     T w0 = w[j], w1 = w[j + 1], w2 = w[j + 2], w3 = w[j + 3];
                     S a[NV];
                     vec_get(v0, a);
@@ -588,7 +607,7 @@ k_tile_matvec(const PairDesc* desc, const int* tile_pair_start, const int* tile_
                     for (int q = 0; q < NV; q++) acc[q] = fma((T)a[q], w3, acc[q]);
                 }
                 for (; j < d.ncol; j++) {
-                    V4 v0 = *reinterpret_cast<const V4*>(base + (size_t)j * sp);
+                    V4 v0 = ld_stream_as<V4>(base + (size_t)j * sp);
                     S a[NV];
                     vec_get(v0, a);
                     T w0 = w[j];
@@ -605,7 +624,7 @@ k_tile_matvec(const PairDesc* desc, const int* tile_pair_start, const int* tile_
                         const T* w8 = w16 + d.c0;
 #pragma unroll 4
                         for (int gp = 0; gp < (d.c0 >> 1); gp++) {
-                            const uint4 raw = *reinterpret_cast<const uint4*>(s16 + ((size_t)gp * sp + row0) * 4);
+                            const uint4 raw = ld_stream_as<uint4>(s16 + ((size_t)gp * sp + row0) * 4);
                             const __half2* h2 = reinterpret_cast<const __half2*>(&raw);
                             const T wa = w16[2 * gp], wb = w16[2 * gp + 1];
 #pragma unroll
@@ -616,7 +635,7 @@ k_tile_matvec(const PairDesc* desc, const int* tile_pair_start, const int* tile_
                         }
 #pragma unroll 4
                         for (int gq = 0; gq < (d.pad >> 2); gq++) {
-                            const uint4 raw = *reinterpret_cast<const uint4*>(s8 + ((size_t)gq * sp + row0) * 4);
+                            const uint4 raw = ld_stream_as<uint4>(s8 + ((size_t)gq * sp + row0) * 4);
                             const unsigned wd[4] = {raw.x, raw.y, raw.z, raw.w};
                             const T w0 = w8[4 * gq], w1 = w8[4 * gq + 1], w2 = w8[4 * gq + 2], w3 = w8[4 * gq + 3];
 #pragma unroll
