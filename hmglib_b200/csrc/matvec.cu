@@ -487,9 +487,8 @@ __device__ __forceinline__ void vtx_group(const K1Desc& d, bool have, const T* _
                 T xv[NC];
                 const int e0 = (c + hh * LPR) * NC;
 #pragma unroll
-                // V is zero past m2 and x is padded: no bound test (a non-finite x makes
-                // every output non-finite anyway, K having no zero columns)
-                for (int q = 0; q < NC; q++) xv[q] = xs[d.c0 + e0 + q];
+                // the bound test also covers the chunks past the row that a step skips
+                for (int q = 0; q < NC; q++) xv[q] = e0 + q < d.m2 ? xs[d.c0 + e0 + q] : (T)0;
 #pragma unroll
                 for (int k = 0; k < R; k++) {
                     S f[NC * TG];
