@@ -548,6 +548,58 @@ k_vtx(const K1Desc* __restrict__ descs, K1Classes cls, const T* __restrict__ xs,
     }
 }
 
+// The rows row0..row0+3 of a mixed-storage tile slice times t_b.  The slice is a
+// uniform run of chunk columns of s_pad * 4 bytes -- r32 FP32 columns, r16/2 FP16
+// pairs, r8/4 FP8 quads -- so the lane's 16-byte loads are issued eight at a time
+// whatever the tier, and only the decode branches (uniformly across the warp).
+template <typename T>
+__device__ __forceinline__ void mixed_slice(const PairDesc& d, int sp, int row0, T (&acc)[4])
+{
+    const char* base = static_cast<const char*>(d.data) + (size_t)row0 * 4;
+    const T* w = static_cast<const T*>(d.w);
+    const int n32 = d.ncol, n16 = d.c0 >> 1, n8 = d.pad >> 2;
+    const int nch = n32 + n16 + n8;
+    for (int k0 = 0; k0 < nch; k0 += 8) {
+        uint4 raw[8];
+#pragma unroll
+        for (int u = 0; u < 8; u++) {
+            raw[u] = make_uint4(0u, 0u, 0u, 0u);
+            if (k0 + u < nch) raw[u] = ld_stream(base + (size_t)(k0 + u) * sp * 4);
+        }
+#pragma unroll
+        for (int u = 0; u < 8; u++) {
+            const int k = k0 + u;
+            if (k >= nch) break;
+            if (k < n32) {
+                const T wv = w[k];
+                acc[0] = fma((T)__uint_as_float(raw[u].x), wv, acc[0]);
+                acc[1] = fma((T)__uint_as_float(raw[u].y), wv, acc[1]);
+                acc[2] = fma((T)__uint_as_float(raw[u].z), wv, acc[2]);
+                acc[3] = fma((T)__uint_as_float(raw[u].w), wv, acc[3]);
+            } else if (k < n32 + n16) {
+                const int t = n32 + 2 * (k - n32);
+                const T wa = w[t], wb = w[t + 1];
+                const __half2* h2 = reinterpret_cast<const __half2*>(&raw[u]);
+#pragma unroll
+                for (int q = 0; q < 4; q++) {
+                    const float2 f = __half22float2(h2[q]);
+                    acc[q] = fma((T)f.y, wb, fma((T)f.x, wa, acc[q]));
+                }
+            } else {
+                const int t = n32 + 2 * n16 + 4 * (k - n32 - n16);
+                const T w0 = w[t], w1 = w[t + 1], w2 = w[t + 2], w3 = w[t + 3];
+                const unsigned wd[4] = {raw[u].x, raw[u].y, raw[u].z, raw[u].w};
+#pragma unroll
+                for (int q = 0; q < 4; q++) {
+                    const float2 f0 = fp8x2_to_float2((unsigned short)(wd[q] & 0xffffu));
+                    const float2 f1 = fp8x2_to_float2((unsigned short)(wd[q] >> 16));
+                    acc[q] = fma((T)f1.y, w3, fma((T)f1.x, w2, fma((T)f0.y, w1, fma((T)f0.x, w0, acc[q]))));
+                }
+            }
+        }
+    }
+}
+
 // K2: one CTA (8 warps) per row tile.  A group of RW warps covers the tile's padded
 // rows with 16-byte loads (4 FP32 or 2 FP64 rows per lane); the 8/RW groups take
 // the tile's pairs round robin.
@@ -583,7 +635,14 @@ k_tile_matvec(const PairDesc* desc, const int* tile_pair_start, const int* tile_
         if (d.kind != PAIR_ONTHEFLY) {
             const S* base = (const S*)d.data + row0;
             const T* w = (const T*)d.w;
-            if (active) {
+            bool done = !active;
+            if constexpr (sizeof(S) == 4) {
+                if (active && d.kind == PAIR_FAR_MIXED) {
+                    mixed_slice<T>(d, sp, row0, acc);
+                    done = true;
+                }
+            }
+            if (!done) {
                 int j = 0;
                 for (; j + 4 <= d.ncol; j += 4) {
                     V4 v0 = ld_stream_as<V4>(base + (size_t)(j + 0) * sp);
@@ -612,39 +671,6 @@ k_tile_matvec(const PairDesc* desc, const int* tile_pair_start, const int* tile_
                     T w0 = w[j];
 #pragma unroll
                     for (int q = 0; q < NV; q++) acc[q] = fma((T)a[q], w0, acc[q]);
-                }
-                if constexpr (sizeof(S) == 4) {
-                    if (d.kind == PAIR_FAR_MIXED) {
-                        // FP16 pairs then FP8 quads of the slice: a lane's 16 bytes hold its
-                        // 4 rows x 2 resp. 4 terms
-                        const char* s16 = (const char*)d.data + (size_t)sp * 4 * d.ncol;
-                        const char* s8 = s16 + (size_t)sp * 2 * d.c0;
-                        const T* w16 = w + d.ncol;
-                        const T* w8 = w16 + d.c0;
-#pragma unroll 4
-                        for (int gp = 0; gp < (d.c0 >> 1); gp++) {
-                            const uint4 raw = ld_stream_as<uint4>(s16 + ((size_t)gp * sp + row0) * 4);
-                            const __half2* h2 = reinterpret_cast<const __half2*>(&raw);
-                            const T wa = w16[2 * gp], wb = w16[2 * gp + 1];
-#pragma unroll
-                            for (int q = 0; q < 4; q++) {
-                                const float2 f = __half22float2(h2[q]);
-                                acc[q] = fma((T)f.y, wb, fma((T)f.x, wa, acc[q]));
-                            }
-                        }
-#pragma unroll 4
-                        for (int gq = 0; gq < (d.pad >> 2); gq++) {
-                            const uint4 raw = ld_stream_as<uint4>(s8 + ((size_t)gq * sp + row0) * 4);
-                            const unsigned wd[4] = {raw.x, raw.y, raw.z, raw.w};
-                            const T w0 = w8[4 * gq], w1 = w8[4 * gq + 1], w2 = w8[4 * gq + 2], w3 = w8[4 * gq + 3];
-#pragma unroll
-                            for (int q = 0; q < 4; q++) {
-                                const float2 f0 = fp8x2_to_float2((unsigned short)(wd[q] & 0xffffu));
-                                const float2 f1 = fp8x2_to_float2((unsigned short)(wd[q] >> 16));
-                                acc[q] = fma((T)f1.y, w3, fma((T)f1.x, w2, fma((T)f0.y, w1, fma((T)f0.x, w0, acc[q]))));
-                            }
-                        }
-                    }
                 }
             }
 #pragma unroll
