@@ -153,6 +153,49 @@ def run_reference(a, rank, world):
     return 0
 
 
+def multi_rhs_timing(torch, H, x, n, nrhs, steps, stream, world, err1):
+    """Products of nrhs vectors at once (hmg_matvec_multi): vector products per second,
+    device-resident and end to end (pinned host X in, Y out, inside the timing)."""
+    import torch.distributed as dist
+    rng = np.random.default_rng(11)
+    Xh = rng.uniform(-1, 1, (nrhs, n))
+    Xh[0] = x
+    X = torch.from_numpy(Xh).cuda()
+    Y = torch.empty_like(X)
+    for _ in range(3):
+        H.matvec_multi(X, Y)
+    torch.cuda.synchronize()
+    # column 0 equals the single-vector product to FP32 rounding
+    y1 = torch.empty(n, dtype=torch.float64, device="cuda")
+    H.matvec(X[0], y1)
+    torch.cuda.synchronize()
+    diff = float(torch.linalg.norm(Y[0] - y1) / torch.linalg.norm(y1))
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        H.matvec_multi(X, Y)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    Xp = torch.from_numpy(Xh).pin_memory()
+    Yp = torch.empty(Xh.shape, dtype=torch.float64).pin_memory()
+    e0.record(stream)
+    for _ in range(steps):
+        X.copy_(Xp, non_blocking=True)
+        H.matvec_multi(X, Y)
+        Yp.copy_(Y, non_blocking=True)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms_e2e = e0.elapsed_time(e1)
+    if world > 1:
+        t = torch.tensor([ms, ms_e2e], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms, ms_e2e = float(t[0]), float(t[1])
+    return {"nrhs": nrhs, "ms_per_product": ms / steps, "value": world * nrhs * 1000.0 * steps / ms,
+            "unit": "vector products/s", "e2e_value": world * nrhs * 1000.0 * steps / ms_e2e,
+            "err_vs_fp64_col0": err1 + diff, "col0_vs_single": diff}
+
+
 def run_engine(a, rank, world):
     import torch
     import torch.distributed as dist
@@ -288,6 +331,8 @@ def run_engine(a, rank, world):
                                          "max_rank", "near_entries", "far_entries", "near_bytes", "far_bytes")},
         "clocks": clk.summary(),
     }
+    if a.nrhs > 1:
+        line["multi_rhs"] = multi_rhs_timing(torch, H, x, n, a.nrhs, a.steps, stream, world, err)
     if rank == 0 and world == 1 and not a.no_cpu:
         kind = O.KERNEL_MATERN32
         rate, nrows, dt, thr = cpu_direct_rate(p, x, kind, O.kernel_param(kind, W["rho"]), target_s=a.cpu_seconds)
@@ -308,6 +353,8 @@ def main(argv=None):
     ap.add_argument("--n", type=int, default=0, help="override the point count (default 2^20)")
     ap.add_argument("--prec", default="mixed", choices=["fp32", "fp64", "mixed"])
     ap.add_argument("--near", default="stored", choices=["stored", "onthefly"])
+    ap.add_argument("--nrhs", type=int, default=1,
+                    help="also time products of this many vectors at once (hmg_matvec_multi)")
     ap.add_argument("--arith", default="fp32", choices=["fp32", "fp64"],
                     help="arithmetic of the products over FP32/mixed storage")
     ap.add_argument("--variant", type=int, default=1, choices=[0, 1],

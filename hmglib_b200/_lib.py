@@ -62,6 +62,7 @@ _PROTOS = {
     "hmg_set_near_mode": (C.c_int, [_vp, C.c_int]),
     "hmg_matvec": (C.c_int, [_vp, _vp, _vp]),
     "hmg_matvec_host": (C.c_int, [_vp, _vp, _vp]),
+    "hmg_matvec_multi": (C.c_int, [_vp, C.c_int, _vp, C.c_int, _vp, C.c_int]),
     "hmg_full_matvec": (C.c_int, [_vp, _vp, _vp]),
     "hmg_full_matvec_rows": (C.c_int, [_vp, _vp, _vp, C.c_int, _vp]),
     "hmg_gaussian_rhs": (C.c_int, [_vp, _vp]),

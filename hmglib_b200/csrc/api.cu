@@ -219,6 +219,17 @@ hmg_status hmg_matvec(hmg_matrix* h, const double* x, double* y)
     return matvec_device(h, x, y);
 }
 
+hmg_status hmg_matvec_multi(hmg_matrix* h, int nrhs, const double* X, int ldx, double* Y, int ldy)
+{
+    HMG_REQUIRE(h && X && Y, HMG_ERR_INVALID, "hmg_matvec_multi: NULL argument");
+    HMG_REQUIRE(nrhs >= 1 && nrhs <= 32, HMG_ERR_INVALID, "hmg_matvec_multi: nrhs %d outside 1..32", nrhs);
+    HMG_REQUIRE(ldx >= h->n[1] && ldy >= h->n[0], HMG_ERR_INVALID,
+                "hmg_matvec_multi: leading dimensions %d, %d below n2 = %d, n1 = %d", ldx, ldy, h->n[1], h->n[0]);
+    hmg_status st = check_ready(h, "hmg_matvec_multi");
+    if (st) return st;
+    return matvec_multi(h, nrhs, X, ldx, Y, ldy);
+}
+
 static hmg_status check_pipeline(hmg_matrix* h);
 
 hmg_status hmg_matvec_host(hmg_matrix* h, const double* x_host, double* y_host)

@@ -26,21 +26,6 @@
 
 namespace hmg {
 
-struct K1Unit {
-    int b, l0, l1, tier;  // terms [l0, l1); tier: 0 storage type (FP32/FP64), 1 FP16, 2 FP8
-};
-
-// A K1 piece resolved to addresses: terms [l0, l1) of one storage tier of V_b^T, as
-// rows of single terms (tier 0), interleaved pairs (FP16) or quads (FP8).
-struct K1Desc {
-    const void* v;       // first row of the piece
-    const float* scal;   // the terms' scales (FP16/FP8 tiers), else null
-    long long tout;      // tbuf index of term l0
-    int c0, m2;          // the block's x segment
-    int nrows, row_bytes;  // rows in the piece; row stride, a multiple of 16 bytes
-    int pad[2];
-};
-static_assert(sizeof(K1Desc) == 48, "K1Desc layout");
 
 // ---------------------------------------------------------------------------
 // near-field fill (precompute_batched_dense_magma, linear_algebra.cu:3140-3342):
@@ -228,7 +213,7 @@ __global__ void k_build_k1desc(const K1Unit* units, int n, const int* blk_c0, co
 // loads in flight whatever the tier.
 static constexpr int k1_nch(int tier) { return tier == 0 ? 2 : (tier == 1 ? 4 : 8); }
 
-static hmg_status ensure_desc(hmg_matrix* h, int elem)
+hmg_status ensure_desc(hmg_matrix* h, int elem)
 {
     cudaStream_t s = h->stream;
     hmg_status st;
@@ -336,17 +321,6 @@ __global__ void k_gather_x(const double* x, const int* perm2, int n, double* xs6
     xs32[j] = (float)v;
 }
 
-// Loads of the stored near field and factors: each byte is read once per product, so
-// they bypass L1 (which keeps the x and t_b values reused across rows) and ask L2 to
-// fetch the whole 256-byte sector group (the neighbouring lanes' and steps' bytes).
-__device__ __forceinline__ uint4 ld_stream(const void* p)
-{
-    uint4 v;
-    asm("ld.global.nc.L1::no_allocate.L2::256B.v4.u32 {%0, %1, %2, %3}, [%4];"
-        : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w)
-        : "l"(p));
-    return v;
-}
 template <typename V4> __device__ __forceinline__ V4 ld_stream_as(const void* p)
 {
     const uint4 u = ld_stream(p);
@@ -705,7 +679,7 @@ k_tile_matvec(const PairDesc* desc, const int* tile_pair_start, const int* tile_
 
 // Z-ordered x in FP64 and FP32, padded and zeroed: the streaming kernels copy
 // 16-byte-aligned supersets of x pieces.
-static hmg_status ensure_xs(hmg_matrix* h)
+hmg_status ensure_xs(hmg_matrix* h)
 {
     if (h->xs64) return HMG_OK;
     cudaStream_t s = h->stream;

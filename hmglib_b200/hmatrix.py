@@ -98,6 +98,14 @@ class HMatrix:
 
     apply = matvec
 
+    def matvec_multi(self, X, Y):
+        """Y = H X for device FP64 tensors X (n2 x nrhs) and Y (n1 x nrhs), column-major
+        (a tensor of shape (nrhs, n) row-major is the column-major (n, nrhs) matrix);
+        asynchronous."""
+        nrhs = int(X.shape[0])
+        self._call("hmg_matvec_multi", nrhs, _ptr(X), int(X.stride(0)), _ptr(Y), int(Y.stride(0)))
+        return Y
+
     def matvec_device(self, x_ptr: int, y_ptr: int):
         self._call("hmg_matvec", C.c_void_p(x_ptr), C.c_void_p(y_ptr))
 

@@ -130,6 +130,14 @@ hmg_status hmg_full_matvec(hmg_matrix* h, const double* x, double* y);
 hmg_status hmg_full_matvec_rows(hmg_matrix* h, const double* x, const int* rows, int nrows,
                                 double* y);
 
+/* Y = H X for 1 <= nrhs <= 32 vectors: X (n2 x nrhs) and Y (n1 x nrhs) are device
+ * FP64 column-major with leading dimensions ldx >= n2, ldy >= n1, caller order.  The
+ * stored H-matrix is read once for all vectors (FP32 / FP64 storage with a stored
+ * near field; otherwise one product per vector).  Same arithmetic as hmg_matvec;
+ * asynchronous on the handle's stream.  No reference counterpart (the reference
+ * multiplies one vector per apply_h_matrix_mvp call, hmglib.cu:271-286). */
+hmg_status hmg_matvec_multi(hmg_matrix* h, int nrhs, const double* X, int ldx, double* Y, int ldy);
+
 /* Kernel-ridge solve (H + shift I) x = b by conjugate gradients with the handle's
  * H-matvec as operator (n1 == n2 and a symmetric positive definite kernel).  b and
  * x are device vectors in the caller's order; x holds the initial guess and
