@@ -217,6 +217,8 @@ hmg_status ensure_desc(hmg_matrix* h, int elem)
 {
     cudaStream_t s = h->stream;
     hmg_status st;
+    // dense-pair descriptors point into the x buffers: they must exist first
+    if ((st = ensure_xs(h))) return st;
     if (!h->pair_desc) {
         PairDesc* d = nullptr;
         if ((st = dalloc(&d, (size_t)(h->npairs > 0 ? h->npairs : 1), s))) return st;
