@@ -34,6 +34,15 @@ __global__ void k_gather_multi(const double* X, int ldx, int nrhs, const int* pe
     xm[idx] = j < nrhs ? (T)X[perm2[i] + (size_t)j * ldx] : (T)0;
 }
 
+// 16-byte asynchronous copy global -> shared; an invalid source copies nothing and
+// zeroes the 16 destination bytes.
+__device__ __forceinline__ void cp_async16(void* dst, const void* src, bool valid)
+{
+    const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(dst));
+    const int n = valid ? 16 : 0;  // 0 source bytes: the 16 destination bytes are zeroed
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(d), "l"(src), "r"(n) : "memory");
+}
+
 template <typename S> struct Lanes;
 template <> struct Lanes<float> {
     static constexpr int NC = 4;
@@ -95,6 +104,105 @@ __global__ void __launch_bounds__(256) k_vtx_multi(const K1Desc* __restrict__ de
 #pragma unroll
                 for (int k = 0; k < 4; k++)
                     if (row + k < d.nrows) tm[(size_t)(d.tout + row + k) * R + j] = acc[k];
+        }
+    }
+}
+
+// FP32 storage, R = 8, 16 or 32 vectors: t_b = V_b^T X_b with V rows streamed through
+// per-warp shared memory (cp.async, 4 rows x 128 columns per stage, double-buffered),
+// so every lane's copies are distinct coalesced 16-byte transfers.  Lane (cg, rg)
+// computes 4 rows x 4 vectors over every CGN-th group of 4 columns of a stage (V
+// from shared memory, X from global/L1), and the CGN column groups are summed by a
+// fixed xor butterfly at the end of each 4-row block.
+template <int R>
+__global__ void __launch_bounds__(256) k_vtx_multi_smem(const K1Desc* __restrict__ descs, int n,
+                                                        const float* __restrict__ xm, float* __restrict__ tm)
+{
+    constexpr int RG = R / 4, CGN = 32 / RG, SC = 128;  // vector groups, column groups, stage columns
+    __shared__ __align__(16) float Vs[8][2][4][SC];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int rg = lane % RG, cg = lane / RG;
+    const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int nw = (gridDim.x * blockDim.x) >> 5;
+    for (int u = gw; u < n; u += nw) {
+        const K1Desc d = descs[u];
+        const int cpr = d.row_bytes >> 4;  // 16-byte chunks per row
+        const int nst = (cpr + SC / 4 - 1) / (SC / 4);  // stages per 4-row block
+        const char* vb = static_cast<const char*>(d.v);
+        const int nblk = (d.nrows + 3) >> 2;
+        const int total = nblk * nst;
+        auto issue = [&](int b, int it) {
+            const int blk = it / nst, st = it - blk * nst;
+            const int ch = st * (SC / 4) + lane;  // this lane's chunk of each row
+#pragma unroll
+            for (int k = 0; k < 4; k++) {
+                const int row = blk * 4 + k;
+                const bool v = row < d.nrows && ch < cpr;
+                cp_async16(&Vs[warp][b][k][lane * 4], v ? vb + (size_t)row * d.row_bytes + (size_t)ch * 16 : vb, v);
+            }
+            asm volatile("cp.async.commit_group;" ::: "memory");
+        };
+        float acc[4][4];
+#pragma unroll
+        for (int a = 0; a < 4; a++)
+#pragma unroll
+            for (int c = 0; c < 4; c++) acc[a][c] = 0.0f;
+        issue(0, 0);
+        for (int it = 0; it < total; it++) {
+            const int b = it & 1;
+            if (it + 1 < total) {
+                issue(b ^ 1, it + 1);
+                asm volatile("cp.async.wait_group 1;" ::: "memory");
+            } else {
+                asm volatile("cp.async.wait_group 0;" ::: "memory");
+            }
+            __syncwarp();
+            const int blk = it / nst, st = it - blk * nst;
+            const int cbase = st * SC;  // first column of the stage
+#pragma unroll
+            for (int sub = 0; sub < SC / 4 / CGN; sub++) {
+                const int c4 = (sub * CGN + cg) * 4;  // first of this lane's 4 columns
+                const int col = cbase + c4;
+                float4 xv[4];
+#pragma unroll
+                for (int q = 0; q < 4; q++)
+                    xv[q] = col + q < d.m2 ? *reinterpret_cast<const float4*>(xm + (size_t)(d.c0 + col + q) * R + rg * 4)
+                                           : make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+                for (int k = 0; k < 4; k++) {
+                    const float4 v = *reinterpret_cast<const float4*>(&Vs[warp][b][k][c4]);
+                    const float vv[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+                    for (int q = 0; q < 4; q++) {
+                        acc[k][0] = fmaf(vv[q], xv[q].x, acc[k][0]);
+                        acc[k][1] = fmaf(vv[q], xv[q].y, acc[k][1]);
+                        acc[k][2] = fmaf(vv[q], xv[q].z, acc[k][2]);
+                        acc[k][3] = fmaf(vv[q], xv[q].w, acc[k][3]);
+                    }
+                }
+            }
+            __syncwarp();  // the buffer is refilled by the issue two stages on
+            if (st == nst - 1) {
+                // the block's 4 rows are complete: sum the column groups, write, reset
+#pragma unroll
+                for (int o = RG; o < 32; o <<= 1)
+#pragma unroll
+                    for (int k = 0; k < 4; k++)
+#pragma unroll
+                        for (int c = 0; c < 4; c++) acc[k][c] += __shfl_xor_sync(0xffffffffu, acc[k][c], o);
+                if (cg == 0)
+#pragma unroll
+                    for (int k = 0; k < 4; k++) {
+                        const int row = blk * 4 + k;
+                        if (row < d.nrows)
+                            *reinterpret_cast<float4*>(tm + (size_t)(d.tout + row) * R + rg * 4) =
+                                make_float4(acc[k][0], acc[k][1], acc[k][2], acc[k][3]);
+                    }
+#pragma unroll
+                for (int k = 0; k < 4; k++)
+#pragma unroll
+                    for (int c = 0; c < 4; c++) acc[k][c] = 0.0f;
+            }
         }
     }
 }
@@ -161,6 +269,119 @@ __global__ void __launch_bounds__(256) k_tile_multi(const PairDesc* __restrict__
             if (r0 + q < s) Y[perm1[tr0 + r0 + q] + (size_t)j * ldy] = acc64[q];
 }
 
+// FP32 storage, R = 8, 16 or 32 vectors: the tile's slices are streamed through
+// shared memory in stages of 16 columns (cp.async, double-buffered across pairs), and
+// each thread keeps a (R/8 rows) x (4 vectors) register tile, so every shared value
+// it reads feeds R/8 or 4 multiply-adds.  Products per pair in FP32, added in FP64.
+
+template <int R>
+__global__ void __launch_bounds__(256) k_tile_multi_smem(const PairDesc* __restrict__ desc,
+                                                         const int* tile_pair_start, const int* tile_r0,
+                                                         const int* tile_s, const int* perm1,
+                                                         const float* __restrict__ xm, const float* __restrict__ tm,
+                                                         const char* tbase, int nrhs, double* Y, int ldy)
+{
+    constexpr int KC = 16, CG = R / 4, TR = R / 8;
+    __shared__ __align__(16) float Us[2][KC][HMG_TILE_ROWS];
+    __shared__ __align__(16) float Ts[2][KC][R];
+    const int t = blockIdx.x, tid = threadIdx.x;
+    const int cg = tid % CG, rg = tid / CG;
+    const int s = tile_s[t], sp = (s + 3) & ~3, tr0 = tile_r0[t];
+    const int pbeg = tile_pair_start[t], pend = tile_pair_start[t + 1];
+    const int sp4 = sp >> 2;
+
+    // stage (pair p, first column k0) into buffer b
+    auto issue = [&](int b, int p, int k0) {
+        const PairDesc d = desc[p];
+        const float* data = static_cast<const float*>(d.data);
+        for (int idx = tid; idx < KC * sp4; idx += 256) {
+            const int kk = idx / sp4, r4 = idx - kk * sp4;
+            const bool v = k0 + kk < d.ncol;
+            cp_async16(&Us[b][kk][r4 * 4], v ? data + (size_t)(k0 + kk) * sp + r4 * 4 : data, v);
+        }
+        const float* src = d.kind == PAIR_STORED
+                               ? xm + (size_t)d.c0 * R
+                               : tm + (size_t)((static_cast<const char*>(d.w) - tbase) / 4) * R;
+        for (int idx = tid; idx < KC * (R / 4); idx += 256) {
+            const int kk = idx / (R / 4), c4 = idx - kk * (R / 4);
+            const bool v = k0 + kk < d.ncol;
+            cp_async16(&Ts[b][kk][c4 * 4], v ? src + (size_t)(k0 + kk) * R + c4 * 4 : src, v);
+        }
+        asm volatile("cp.async.commit_group;" ::: "memory");
+    };
+
+    double acc64[TR][4];
+    float acc[TR][4];
+#pragma unroll
+    for (int i = 0; i < TR; i++)
+#pragma unroll
+        for (int c = 0; c < 4; c++) acc64[i][c] = 0.0, acc[i][c] = 0.0f;
+
+    // the flattened sequence of (pair, column chunk) stages, skipping empty pairs
+    int p = pbeg, k0 = 0;
+    while (p < pend && desc[p].ncol == 0) p++;
+    int buf = 0;
+    if (p < pend) issue(0, p, 0);
+    while (p < pend) {
+        const int ncol = desc[p].ncol;
+        // the next stage
+        int pn = p, kn = k0 + KC;
+        if (kn >= ncol) {
+            pn = p + 1;
+            kn = 0;
+            while (pn < pend && desc[pn].ncol == 0) pn++;
+        }
+        if (pn < pend) {
+            issue(buf ^ 1, pn, kn);
+            asm volatile("cp.async.wait_group 1;" ::: "memory");
+        } else {
+            asm volatile("cp.async.wait_group 0;" ::: "memory");
+        }
+        __syncthreads();
+        const int kmax = min(KC, ncol - k0);
+        for (int k = 0; k < kmax; k++) {
+            float u[TR];
+            if constexpr (TR == 4) {
+                const float4 v = *reinterpret_cast<const float4*>(&Us[buf][k][rg * 4]);
+                u[0] = v.x; u[1] = v.y; u[2] = v.z; u[3] = v.w;
+            } else if constexpr (TR == 2) {
+                const float2 v = *reinterpret_cast<const float2*>(&Us[buf][k][rg * 2]);
+                u[0] = v.x; u[1] = v.y;
+            } else {
+                u[0] = Us[buf][k][rg];
+            }
+            const float4 w = *reinterpret_cast<const float4*>(&Ts[buf][k][cg * 4]);
+#pragma unroll
+            for (int i = 0; i < TR; i++) {
+                acc[i][0] = fmaf(u[i], w.x, acc[i][0]);
+                acc[i][1] = fmaf(u[i], w.y, acc[i][1]);
+                acc[i][2] = fmaf(u[i], w.z, acc[i][2]);
+                acc[i][3] = fmaf(u[i], w.w, acc[i][3]);
+            }
+        }
+        if (pn != p) {
+#pragma unroll
+            for (int i = 0; i < TR; i++)
+#pragma unroll
+                for (int c = 0; c < 4; c++) acc64[i][c] += (double)acc[i][c], acc[i][c] = 0.0f;
+        }
+        __syncthreads();  // the buffer is refilled by the issue two stages on
+        p = pn;
+        k0 = kn;
+        buf ^= 1;
+    }
+#pragma unroll
+    for (int i = 0; i < TR; i++) {
+        const int row = rg * TR + i;
+        if (row < s)
+#pragma unroll
+            for (int c = 0; c < 4; c++) {
+                const int j = cg * 4 + c;
+                if (j < nrhs) Y[perm1[tr0 + row] + (size_t)j * ldy] = acc64[i][c];
+            }
+    }
+}
+
 template <typename S, int R>
 static hmg_status launch_multi(hmg_matrix* h, int nrhs, const double* X, int ldx, double* Y, int ldy, S* xm, S* tm)
 {
@@ -171,14 +392,22 @@ static hmg_status launch_multi(hmg_matrix* h, int nrhs, const double* X, int ldx
     HMG_LAUNCH_CHECK();
     const int n0 = h->k1_count[0];
     if (n0 > 0) {
-        k_vtx_multi<S, R><<<std::min(ceil_div(n0, 8), 148 * 8), 256, 0, s>>>(
-            static_cast<const K1Desc*>(h->k1_units), n0, xm, tm);
+        const K1Desc* dd = static_cast<const K1Desc*>(h->k1_units);
+        if constexpr (sizeof(S) == 4 && R >= 8)
+            k_vtx_multi_smem<R><<<std::min(ceil_div(n0, 8), 148 * 8), 256, 0, s>>>(dd, n0, xm, tm);
+        else
+            k_vtx_multi<S, R><<<std::min(ceil_div(n0, 8), 148 * 8), 256, 0, s>>>(dd, n0, xm, tm);
         HMG_LAUNCH_CHECK();
     }
     if (h->ntiles > 0) {
-        k_tile_multi<S, R><<<h->ntiles, 256, 0, s>>>(static_cast<const PairDesc*>(h->pair_desc),
-                                                     h->tile_pair_start, h->tile_r0, h->tile_s, h->perm[0], xm, tm,
-                                                     static_cast<const char*>(h->tbuf), nrhs, Y, ldy);
+        const PairDesc* pd = static_cast<const PairDesc*>(h->pair_desc);
+        const char* tb = static_cast<const char*>(h->tbuf);
+        if constexpr (sizeof(S) == 4 && R >= 8)
+            k_tile_multi_smem<R><<<h->ntiles, 256, 0, s>>>(pd, h->tile_pair_start, h->tile_r0, h->tile_s,
+                                                           h->perm[0], xm, tm, tb, nrhs, Y, ldy);
+        else
+            k_tile_multi<S, R><<<h->ntiles, 256, 0, s>>>(pd, h->tile_pair_start, h->tile_r0, h->tile_s,
+                                                         h->perm[0], xm, tm, tb, nrhs, Y, ldy);
         HMG_LAUNCH_CHECK();
     }
     return HMG_OK;

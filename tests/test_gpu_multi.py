@@ -31,7 +31,7 @@ def _columns(torch, H, X):
 
 
 @pytest.mark.parametrize("prec,tol", [(0, 1e-13), (1, 1e-6), (2, 0.0)], ids=["fp64", "fp32", "mixed"])
-@pytest.mark.parametrize("nrhs", [2, 5, 32])
+@pytest.mark.parametrize("nrhs", [2, 5, 16, 32])
 def test_multi_matches_single(hmg, cuda, prec, tol, nrhs):
     torch = cuda
     H, n = _build(hmg, prec)
