@@ -108,8 +108,11 @@ __global__ void __launch_bounds__(256) k_vtx_multi(const K1Desc* __restrict__ de
     }
 }
 
+static constexpr int K1M_STAGES = 4;
+static constexpr size_t K1M_SMEM = 8 * K1M_STAGES * 4 * 128 * sizeof(float);  // 64 KB per CTA
+
 // FP32 storage, R = 8, 16 or 32 vectors: t_b = V_b^T X_b with V rows streamed through
-// per-warp shared memory (cp.async, 4 rows x 128 columns per stage, double-buffered),
+// per-warp shared memory (cp.async, 4 rows x 128 columns per stage, four in flight),
 // so every lane's copies are distinct coalesced 16-byte transfers.  Lane (cg, rg)
 // computes 4 rows x 4 vectors over every CGN-th group of 4 columns of a stage (V
 // from shared memory, X from global/L1), and the CGN column groups are summed by a
@@ -119,8 +122,10 @@ __global__ void __launch_bounds__(256) k_vtx_multi_smem(const K1Desc* __restrict
                                                         const float* __restrict__ xm, float* __restrict__ tm)
 {
     constexpr int RG = R / 4, CGN = 32 / RG, SC = 128;  // vector groups, column groups, stage columns
-    __shared__ __align__(16) float Vs[8][2][4][SC];
+    constexpr int NS = K1M_STAGES;                      // stages in flight per warp
+    extern __shared__ __align__(16) float k1m_smem[];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    float (*Vs)[4][SC] = reinterpret_cast<float (*)[4][SC]>(k1m_smem + (size_t)warp * NS * 4 * SC);
     const int rg = lane % RG, cg = lane / RG;
     const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int nw = (gridDim.x * blockDim.x) >> 5;
@@ -129,16 +134,17 @@ __global__ void __launch_bounds__(256) k_vtx_multi_smem(const K1Desc* __restrict
         const int cpr = d.row_bytes >> 4;  // 16-byte chunks per row
         const int nst = (cpr + SC / 4 - 1) / (SC / 4);  // stages per 4-row block
         const char* vb = static_cast<const char*>(d.v);
-        const int nblk = (d.nrows + 3) >> 2;
-        const int total = nblk * nst;
-        auto issue = [&](int b, int it) {
-            const int blk = it / nst, st = it - blk * nst;
-            const int ch = st * (SC / 4) + lane;  // this lane's chunk of each row
+        const int total = ((d.nrows + 3) >> 2) * nst;
+        auto issue = [&](int it) {
+            if (it < total) {
+                const int blk = it / nst, st = it - blk * nst;
+                const int ch = st * (SC / 4) + lane;  // this lane's chunk of each row
 #pragma unroll
-            for (int k = 0; k < 4; k++) {
-                const int row = blk * 4 + k;
-                const bool v = row < d.nrows && ch < cpr;
-                cp_async16(&Vs[warp][b][k][lane * 4], v ? vb + (size_t)row * d.row_bytes + (size_t)ch * 16 : vb, v);
+                for (int k = 0; k < 4; k++) {
+                    const int row = blk * 4 + k;
+                    const bool v = row < d.nrows && ch < cpr;
+                    cp_async16(&Vs[it % NS][k][lane * 4], v ? vb + (size_t)row * d.row_bytes + (size_t)ch * 16 : vb, v);
+                }
             }
             asm volatile("cp.async.commit_group;" ::: "memory");
         };
@@ -147,16 +153,13 @@ __global__ void __launch_bounds__(256) k_vtx_multi_smem(const K1Desc* __restrict
         for (int a = 0; a < 4; a++)
 #pragma unroll
             for (int c = 0; c < 4; c++) acc[a][c] = 0.0f;
-        issue(0, 0);
+#pragma unroll
+        for (int it = 0; it < NS - 1; it++) issue(it);
         for (int it = 0; it < total; it++) {
-            const int b = it & 1;
-            if (it + 1 < total) {
-                issue(b ^ 1, it + 1);
-                asm volatile("cp.async.wait_group 1;" ::: "memory");
-            } else {
-                asm volatile("cp.async.wait_group 0;" ::: "memory");
-            }
+            issue(it + NS - 1);
+            asm volatile("cp.async.wait_group %0;" ::"n"(NS - 1) : "memory");
             __syncwarp();
+            const int b = it % NS;
             const int blk = it / nst, st = it - blk * nst;
             const int cbase = st * SC;  // first column of the stage
 #pragma unroll
@@ -170,7 +173,7 @@ __global__ void __launch_bounds__(256) k_vtx_multi_smem(const K1Desc* __restrict
                                            : make_float4(0.f, 0.f, 0.f, 0.f);
 #pragma unroll
                 for (int k = 0; k < 4; k++) {
-                    const float4 v = *reinterpret_cast<const float4*>(&Vs[warp][b][k][c4]);
+                    const float4 v = *reinterpret_cast<const float4*>(&Vs[b][k][c4]);
                     const float vv[4] = {v.x, v.y, v.z, v.w};
 #pragma unroll
                     for (int q = 0; q < 4; q++) {
@@ -181,7 +184,7 @@ __global__ void __launch_bounds__(256) k_vtx_multi_smem(const K1Desc* __restrict
                     }
                 }
             }
-            __syncwarp();  // the buffer is refilled by the issue two stages on
+            __syncwarp();  // this buffer is refilled NS - 1 stages on
             if (st == nst - 1) {
                 // the block's 4 rows are complete: sum the column groups, write, reset
 #pragma unroll
@@ -204,6 +207,8 @@ __global__ void __launch_bounds__(256) k_vtx_multi_smem(const K1Desc* __restrict
                     for (int c = 0; c < 4; c++) acc[k][c] = 0.0f;
             }
         }
+        asm volatile("cp.async.wait_group 0;" ::: "memory");
+        __syncwarp();
     }
 }
 
@@ -270,7 +275,7 @@ __global__ void __launch_bounds__(256) k_tile_multi(const PairDesc* __restrict__
 }
 
 // FP32 storage, R = 8, 16 or 32 vectors: the tile's slices are streamed through
-// shared memory in stages of 16 columns (cp.async, double-buffered across pairs), and
+// shared memory in stages of 16 columns (cp.async, four stages in flight across pairs), and
 // each thread keeps a (R/8 rows) x (4 vectors) register tile, so every shared value
 // it reads feeds R/8 or 4 multiply-adds.  Products per pair in FP32, added in FP64.
 
@@ -281,9 +286,9 @@ __global__ void __launch_bounds__(256) k_tile_multi_smem(const PairDesc* __restr
                                                          const float* __restrict__ xm, const float* __restrict__ tm,
                                                          const char* tbase, int nrhs, double* Y, int ldy)
 {
-    constexpr int KC = 16, CG = R / 4, TR = R / 8;
-    __shared__ __align__(16) float Us[2][KC][HMG_TILE_ROWS];
-    __shared__ __align__(16) float Ts[2][KC][R];
+    constexpr int KC = 16, NS = 4, CG = R / 4, TR = R / 8;  // NS stages in flight
+    __shared__ __align__(16) float Us[NS][KC][HMG_TILE_ROWS];
+    __shared__ __align__(16) float Ts[NS][KC][R];
     const int t = blockIdx.x, tid = threadIdx.x;
     const int cg = tid % CG, rg = tid / CG;
     const int s = tile_s[t], sp = (s + 3) & ~3, tr0 = tile_r0[t];
@@ -307,8 +312,26 @@ __global__ void __launch_bounds__(256) k_tile_multi_smem(const PairDesc* __restr
             const bool v = k0 + kk < d.ncol;
             cp_async16(&Ts[b][kk][c4 * 4], v ? src + (size_t)(k0 + kk) * R + c4 * 4 : src, v);
         }
-        asm volatile("cp.async.commit_group;" ::: "memory");
     };
+    // the flattened sequence of (pair, column chunk) stages, skipping empty pairs
+    auto advance = [&](int& q, int& kq) {
+        kq += KC;
+        if (kq >= desc[q].ncol) {
+            q++;
+            kq = 0;
+            while (q < pend && desc[q].ncol == 0) q++;
+        }
+    };
+    int p = pbeg, k0 = 0;
+    while (p < pend && desc[p].ncol == 0) p++;
+    int pp = p, kp = 0;  // producer cursor, NS - 1 stages ahead
+    for (int st = 0; st < NS - 1; st++) {
+        if (pp < pend) {
+            issue(st, pp, kp);
+            advance(pp, kp);
+        }
+        asm volatile("cp.async.commit_group;" ::: "memory");
+    }
 
     double acc64[TR][4];
     float acc[TR][4];
@@ -317,28 +340,16 @@ __global__ void __launch_bounds__(256) k_tile_multi_smem(const PairDesc* __restr
 #pragma unroll
         for (int c = 0; c < 4; c++) acc64[i][c] = 0.0, acc[i][c] = 0.0f;
 
-    // the flattened sequence of (pair, column chunk) stages, skipping empty pairs
-    int p = pbeg, k0 = 0;
-    while (p < pend && desc[p].ncol == 0) p++;
-    int buf = 0;
-    if (p < pend) issue(0, p, 0);
-    while (p < pend) {
-        const int ncol = desc[p].ncol;
-        // the next stage
-        int pn = p, kn = k0 + KC;
-        if (kn >= ncol) {
-            pn = p + 1;
-            kn = 0;
-            while (pn < pend && desc[pn].ncol == 0) pn++;
+    for (int it = 0; p < pend; it++) {
+        if (pp < pend) {
+            issue((it + NS - 1) % NS, pp, kp);
+            advance(pp, kp);
         }
-        if (pn < pend) {
-            issue(buf ^ 1, pn, kn);
-            asm volatile("cp.async.wait_group 1;" ::: "memory");
-        } else {
-            asm volatile("cp.async.wait_group 0;" ::: "memory");
-        }
+        asm volatile("cp.async.commit_group;" ::: "memory");
+        asm volatile("cp.async.wait_group %0;" ::"n"(NS - 1) : "memory");
         __syncthreads();
-        const int kmax = min(KC, ncol - k0);
+        const int buf = it % NS;
+        const int kmax = min(KC, desc[p].ncol - k0);
         for (int k = 0; k < kmax; k++) {
             float u[TR];
             if constexpr (TR == 4) {
@@ -359,17 +370,19 @@ __global__ void __launch_bounds__(256) k_tile_multi_smem(const PairDesc* __restr
                 acc[i][3] = fmaf(u[i], w.w, acc[i][3]);
             }
         }
+        int pn = p, kn = k0;
+        advance(pn, kn);
         if (pn != p) {
 #pragma unroll
             for (int i = 0; i < TR; i++)
 #pragma unroll
                 for (int c = 0; c < 4; c++) acc64[i][c] += (double)acc[i][c], acc[i][c] = 0.0f;
         }
-        __syncthreads();  // the buffer is refilled by the issue two stages on
+        __syncthreads();  // this buffer is refilled NS - 1 stages on
         p = pn;
         k0 = kn;
-        buf ^= 1;
     }
+    asm volatile("cp.async.wait_group 0;" ::: "memory");
 #pragma unroll
     for (int i = 0; i < TR; i++) {
         const int row = rg * TR + i;
@@ -393,8 +406,11 @@ static hmg_status launch_multi(hmg_matrix* h, int nrhs, const double* X, int ldx
     const int n0 = h->k1_count[0];
     if (n0 > 0) {
         const K1Desc* dd = static_cast<const K1Desc*>(h->k1_units);
-        if constexpr (sizeof(S) == 4 && R >= 8)
-            k_vtx_multi_smem<R><<<std::min(ceil_div(n0, 8), 148 * 8), 256, 0, s>>>(dd, n0, xm, tm);
+        if constexpr (sizeof(S) == 4 && R >= 8) {
+            HMG_CUDA_TRY(cudaFuncSetAttribute(k_vtx_multi_smem<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                              (int)K1M_SMEM));
+            k_vtx_multi_smem<R><<<std::min(ceil_div(n0, 8), 148 * 3), 256, K1M_SMEM, s>>>(dd, n0, xm, tm);
+        }
         else
             k_vtx_multi<S, R><<<std::min(ceil_div(n0, 8), 148 * 8), 256, 0, s>>>(dd, n0, xm, tm);
         HMG_LAUNCH_CHECK();
