@@ -43,19 +43,6 @@ __device__ __forceinline__ void cp_async16(void* dst, const void* src, bool vali
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(d), "l"(src), "r"(n) : "memory");
 }
 
-// acc = a * b + acc on a pair of FP32 lanes (one packed fma.rn.f32x2; each lane
-// rounds as fmaf does)
-__device__ __forceinline__ void fma2(float2& acc, float a, float2 b)
-{
-    unsigned long long r;
-    const float2 aa = make_float2(a, a);
-    asm("fma.rn.f32x2 %0, %1, %2, %3;"
-        : "=l"(r)
-        : "l"(*reinterpret_cast<const unsigned long long*>(&aa)), "l"(*reinterpret_cast<const unsigned long long*>(&b)),
-          "l"(*reinterpret_cast<const unsigned long long*>(&acc)));
-    acc = *reinterpret_cast<const float2*>(&r);
-}
-
 template <typename S> struct Lanes;
 template <> struct Lanes<float> {
     static constexpr int NC = 4;
@@ -161,9 +148,11 @@ __global__ void __launch_bounds__(256) k_vtx_multi_smem(const K1Desc* __restrict
             }
             asm volatile("cp.async.commit_group;" ::: "memory");
         };
-        float2 acc[4][2];
+        float acc[4][4];
 #pragma unroll
-        for (int a = 0; a < 4; a++) acc[a][0] = acc[a][1] = make_float2(0.f, 0.f);
+        for (int a = 0; a < 4; a++)
+#pragma unroll
+            for (int c = 0; c < 4; c++) acc[a][c] = 0.0f;
 #pragma unroll
         for (int it = 0; it < NS - 1; it++) issue(it);
         for (int it = 0; it < total; it++) {
@@ -188,8 +177,10 @@ __global__ void __launch_bounds__(256) k_vtx_multi_smem(const K1Desc* __restrict
                     const float vv[4] = {v.x, v.y, v.z, v.w};
 #pragma unroll
                     for (int q = 0; q < 4; q++) {
-                        fma2(acc[k][0], vv[q], make_float2(xv[q].x, xv[q].y));
-                        fma2(acc[k][1], vv[q], make_float2(xv[q].z, xv[q].w));
+                        acc[k][0] = fmaf(vv[q], xv[q].x, acc[k][0]);
+                        acc[k][1] = fmaf(vv[q], xv[q].y, acc[k][1]);
+                        acc[k][2] = fmaf(vv[q], xv[q].z, acc[k][2]);
+                        acc[k][3] = fmaf(vv[q], xv[q].w, acc[k][3]);
                     }
                 }
             }
@@ -201,20 +192,19 @@ __global__ void __launch_bounds__(256) k_vtx_multi_smem(const K1Desc* __restrict
 #pragma unroll
                     for (int k = 0; k < 4; k++)
 #pragma unroll
-                        for (int c = 0; c < 2; c++) {
-                            acc[k][c].x += __shfl_xor_sync(0xffffffffu, acc[k][c].x, o);
-                            acc[k][c].y += __shfl_xor_sync(0xffffffffu, acc[k][c].y, o);
-                        }
+                        for (int c = 0; c < 4; c++) acc[k][c] += __shfl_xor_sync(0xffffffffu, acc[k][c], o);
                 if (cg == 0)
 #pragma unroll
                     for (int k = 0; k < 4; k++) {
                         const int row = blk * 4 + k;
                         if (row < d.nrows)
                             *reinterpret_cast<float4*>(tm + (size_t)(d.tout + row) * R + rg * 4) =
-                                make_float4(acc[k][0].x, acc[k][0].y, acc[k][1].x, acc[k][1].y);
+                                make_float4(acc[k][0], acc[k][1], acc[k][2], acc[k][3]);
                     }
 #pragma unroll
-                for (int k = 0; k < 4; k++) acc[k][0] = acc[k][1] = make_float2(0.f, 0.f);
+                for (int k = 0; k < 4; k++)
+#pragma unroll
+                    for (int c = 0; c < 4; c++) acc[k][c] = 0.0f;
             }
         }
         asm volatile("cp.async.wait_group 0;" ::: "memory");
@@ -344,13 +334,11 @@ __global__ void __launch_bounds__(256) k_tile_multi_smem(const PairDesc* __restr
     }
 
     double acc64[TR][4];
-    float2 acc[TR][2];
+    float acc[TR][4];
 #pragma unroll
-    for (int i = 0; i < TR; i++) {
-        acc[i][0] = acc[i][1] = make_float2(0.f, 0.f);
+    for (int i = 0; i < TR; i++)
 #pragma unroll
-        for (int c = 0; c < 4; c++) acc64[i][c] = 0.0;
-    }
+        for (int c = 0; c < 4; c++) acc64[i][c] = 0.0, acc[i][c] = 0.0f;
 
     for (int it = 0; p < pend; it++) {
         if (pp < pend) {
@@ -362,7 +350,6 @@ __global__ void __launch_bounds__(256) k_tile_multi_smem(const PairDesc* __restr
         __syncthreads();
         const int buf = it % NS;
         const int kmax = min(KC, desc[p].ncol - k0);
-#pragma unroll 4
         for (int k = 0; k < kmax; k++) {
             float u[TR];
             if constexpr (TR == 4) {
@@ -377,21 +364,19 @@ __global__ void __launch_bounds__(256) k_tile_multi_smem(const PairDesc* __restr
             const float4 w = *reinterpret_cast<const float4*>(&Ts[buf][k][cg * 4]);
 #pragma unroll
             for (int i = 0; i < TR; i++) {
-                fma2(acc[i][0], u[i], make_float2(w.x, w.y));
-                fma2(acc[i][1], u[i], make_float2(w.z, w.w));
+                acc[i][0] = fmaf(u[i], w.x, acc[i][0]);
+                acc[i][1] = fmaf(u[i], w.y, acc[i][1]);
+                acc[i][2] = fmaf(u[i], w.z, acc[i][2]);
+                acc[i][3] = fmaf(u[i], w.w, acc[i][3]);
             }
         }
         int pn = p, kn = k0;
         advance(pn, kn);
         if (pn != p) {
 #pragma unroll
-            for (int i = 0; i < TR; i++) {
-                acc64[i][0] += (double)acc[i][0].x;
-                acc64[i][1] += (double)acc[i][0].y;
-                acc64[i][2] += (double)acc[i][1].x;
-                acc64[i][3] += (double)acc[i][1].y;
-                acc[i][0] = acc[i][1] = make_float2(0.f, 0.f);
-            }
+            for (int i = 0; i < TR; i++)
+#pragma unroll
+                for (int c = 0; c < 4; c++) acc64[i][c] += (double)acc[i][c], acc[i][c] = 0.0f;
         }
         __syncthreads();  // this buffer is refilled NS - 1 stages on
         p = pn;
