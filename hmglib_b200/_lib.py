@@ -41,7 +41,8 @@ class Info(C.Structure):
                 ("near_entries", C.c_int64), ("far_entries", C.c_int64), ("far_rows", C.c_int64),
                 ("near_bytes", C.c_int64), ("far_bytes", C.c_int64), ("matvec_bytes", C.c_int64),
                 ("near_precision", C.c_int), ("far_precision", C.c_int), ("near_mode", C.c_int),
-                ("far_u_bytes", C.c_int64), ("far_v_bytes", C.c_int64), ("matvec_launches", C.c_int)]
+                ("far_u_bytes", C.c_int64), ("far_v_bytes", C.c_int64), ("matvec_launches", C.c_int),
+                ("group_count", C.c_int)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -63,6 +64,8 @@ _PROTOS = {
     "hmg_matvec": (C.c_int, [_vp, _vp, _vp]),
     "hmg_matvec_host": (C.c_int, [_vp, _vp, _vp]),
     "hmg_matvec_multi": (C.c_int, [_vp, C.c_int, _vp, C.c_int, _vp, C.c_int]),
+    "hmg_group_create": (C.c_int, [C.POINTER(_vp), C.POINTER(_vp), C.c_int, _vp]),
+    "hmg_group_offsets": (C.c_int, [_vp, C.c_int, _vp]),
     "hmg_full_matvec": (C.c_int, [_vp, _vp, _vp]),
     "hmg_full_matvec_rows": (C.c_int, [_vp, _vp, _vp, C.c_int, _vp]),
     "hmg_gaussian_rhs": (C.c_int, [_vp, _vp]),

@@ -50,6 +50,7 @@ struct AcaBatch {
 
 struct BlockGeom {
     const int *r0, *m1, *c0, *m2;
+    const double* param;  // per-block kernel parameter (grouped H-matrices), else null
 };
 
 __device__ __forceinline__ double block_sum(double v, double* red)
@@ -94,7 +95,7 @@ __device__ __forceinline__ void block_argmax(double& a, int& i, bool last, doubl
 }
 
 __global__ void __launch_bounds__(ACA_THREADS)
-k_aca(BlockGeom g, KernelSpec K, PointsView P, AcaBatch B, int k, double eps)
+k_aca(BlockGeom g, KernelSpec K0, PointsView P, AcaBatch B, int k, double eps)
 {
     __shared__ double coef[ACA_KMAX];
     __shared__ double red[ACA_WARPS];
@@ -105,6 +106,8 @@ k_aca(BlockGeom g, KernelSpec K, PointsView P, AcaBatch B, int k, double eps)
 
     const int e = blockIdx.x;
     const int b = B.blocks[e];
+    KernelSpec K = K0;
+    if (g.param) K.param = g.param[b];
     const int r0 = g.r0[b], m1 = g.m1[b], c0 = g.c0[b], m2 = g.m2[b];
     int kb = k < m1 ? k : m1;
     kb = kb < m2 ? kb : m2;
@@ -543,7 +546,7 @@ hmg_status run_aca(hmg_matrix* h, int k, double eps, int precision)
     if (budget > ((size_t)8 << 30)) budget = (size_t)8 << 30;
     if (budget < ((size_t)64 << 20)) budget = (size_t)64 << 20;
 
-    BlockGeom g{h->blk_r0, h->blk_m1, h->blk_c0, h->blk_m2};
+    BlockGeom g{h->blk_r0, h->blk_m1, h->blk_c0, h->blk_m2, h->blk_param};
     PointsView P{};
     for (int d = 0; d < h->dim; d++) {
         P.c1[d] = h->zpts[0] + (size_t)d * h->n[0];

@@ -104,6 +104,7 @@ hmg_status hmg_set_points(hmg_matrix* h, int set, const double* coords, int on_d
 {
     HMG_REQUIRE(h && coords, HMG_ERR_INVALID, "hmg_set_points: NULL argument");
     HMG_REQUIRE(set == 0 || set == 1, HMG_ERR_INVALID, "hmg_set_points: set must be 0 or 1");
+    HMG_REQUIRE(!h->group_count, HMG_ERR_UNSUPPORTED, "hmg_set_points: not available on a group handle");
     invalidate_setup(h);
     size_t bytes = sizeof(double) * (size_t)h->n[set] * h->dim;
     HMG_CUDA_TRY(cudaMemcpyAsync(h->pts[set], coords, bytes,
@@ -117,6 +118,7 @@ hmg_status hmg_setup(hmg_matrix* h, double eta, int c_leaf, int max_level, int r
                      int root_level2, int rule)
 {
     HMG_REQUIRE(h, HMG_ERR_INVALID, "hmg_setup: NULL handle");
+    HMG_REQUIRE(!h->group_count, HMG_ERR_UNSUPPORTED, "hmg_setup: not available on a group handle");
     HMG_REQUIRE(h->points_set[0] && h->points_set[1], HMG_ERR_STATE, "hmg_setup: points not set");
     HMG_REQUIRE(eta >= 0.0 && std::isfinite(eta), HMG_ERR_INVALID, "hmg_setup: eta must be finite and >= 0");
     HMG_REQUIRE(c_leaf >= 1, HMG_ERR_INVALID, "hmg_setup: c_leaf must be >= 1 (got %d)", c_leaf);
@@ -143,6 +145,7 @@ hmg_status hmg_setup(hmg_matrix* h, double eta, int c_leaf, int max_level, int r
 hmg_status hmg_set_kernel(hmg_matrix* h, int kind, double param, double regularization)
 {
     HMG_REQUIRE(h, HMG_ERR_INVALID, "hmg_set_kernel: NULL handle");
+    HMG_REQUIRE(!h->group_count, HMG_ERR_UNSUPPORTED, "hmg_set_kernel (the sets' kernels are fixed at hmg_group_create): not available on a group handle");
     HMG_REQUIRE(kind >= HMG_KERNEL_GAUSSIAN_REF && kind <= HMG_KERNEL_MATERN32, HMG_ERR_INVALID,
                 "hmg_set_kernel: unknown kernel kind %d", kind);
     HMG_REQUIRE(std::isfinite(regularization), HMG_ERR_INVALID, "hmg_set_kernel: regularization not finite");
@@ -197,6 +200,8 @@ hmg_status hmg_set_near_mode(hmg_matrix* h, int mode)
     HMG_REQUIRE(h, HMG_ERR_INVALID, "hmg_set_near_mode: NULL handle");
     HMG_REQUIRE(mode == HMG_NEAR_STORED || mode == HMG_NEAR_ONTHEFLY, HMG_ERR_INVALID,
                 "hmg_set_near_mode: unknown mode %d", mode);
+    HMG_REQUIRE(!h->group_count || mode == HMG_NEAR_STORED, HMG_ERR_UNSUPPORTED,
+                "hmg_set_near_mode: a group handle stores its near field");
     HMG_REQUIRE(mode != HMG_NEAR_STORED || h->near_prec >= 0, HMG_ERR_STATE,
                 "hmg_set_near_mode: near field not stored (call hmg_precompute_dense)");
     h->near_mode = mode;
@@ -217,6 +222,23 @@ hmg_status hmg_matvec(hmg_matrix* h, const double* x, double* y)
     hmg_status st = check_ready(h, "hmg_matvec");
     if (st) return st;
     return matvec_device(h, x, y);
+}
+
+hmg_status hmg_group_create(hmg_matrix** out, hmg_matrix* const* sets, int count, void* stream)
+{
+    HMG_REQUIRE(out && sets, HMG_ERR_INVALID, "hmg_group_create: NULL argument");
+    *out = nullptr;
+    HMG_REQUIRE(count >= 1, HMG_ERR_INVALID, "hmg_group_create: count must be >= 1 (got %d)", count);
+    return group_create(out, sets, count, (cudaStream_t)stream);
+}
+
+hmg_status hmg_group_offsets(hmg_matrix* h, int set, int64_t* offsets)
+{
+    HMG_REQUIRE(h && offsets, HMG_ERR_INVALID, "hmg_group_offsets: NULL argument");
+    HMG_REQUIRE(h->group_count > 0, HMG_ERR_STATE, "hmg_group_offsets: not a group handle");
+    HMG_REQUIRE(set == 0 || set == 1, HMG_ERR_INVALID, "hmg_group_offsets: set must be 0 or 1");
+    for (int i = 0; i <= h->group_count; i++) offsets[i] = h->group_off[set][i];
+    return HMG_OK;
 }
 
 hmg_status hmg_matvec_multi(hmg_matrix* h, int nrhs, const double* X, int ldx, double* Y, int ldy)
@@ -256,6 +278,7 @@ hmg_status hmg_matvec_host(hmg_matrix* h, const double* x_host, double* y_host)
 hmg_status hmg_full_matvec(hmg_matrix* h, const double* x, double* y)
 {
     HMG_REQUIRE(h && x && y, HMG_ERR_INVALID, "hmg_full_matvec: NULL argument");
+    HMG_REQUIRE(!h->group_count, HMG_ERR_UNSUPPORTED, "hmg_full_matvec (multiply the sets' own handles): not available on a group handle");
     HMG_REQUIRE(h->setup_done, HMG_ERR_STATE, "hmg_full_matvec: call hmg_setup first");
     HMG_REQUIRE(h->kernel_set, HMG_ERR_STATE, "hmg_full_matvec: call hmg_set_kernel first");
     return direct_matvec(h, x, nullptr, 0, y);
@@ -265,6 +288,7 @@ hmg_status hmg_full_matvec_rows(hmg_matrix* h, const double* x, const int* rows,
 {
     HMG_REQUIRE(h && x && rows && y, HMG_ERR_INVALID, "hmg_full_matvec_rows: NULL argument");
     HMG_REQUIRE(nrows >= 0, HMG_ERR_INVALID, "hmg_full_matvec_rows: nrows < 0");
+    HMG_REQUIRE(!h->group_count, HMG_ERR_UNSUPPORTED, "hmg_full_matvec_rows (multiply the sets' own handles): not available on a group handle");
     HMG_REQUIRE(h->setup_done, HMG_ERR_STATE, "hmg_full_matvec_rows: call hmg_setup first");
     HMG_REQUIRE(h->kernel_set, HMG_ERR_STATE, "hmg_full_matvec_rows: call hmg_set_kernel first");
     return direct_matvec(h, x, rows, nrows, y);
@@ -287,6 +311,7 @@ hmg_status hmg_cg_solve(hmg_matrix* h, double shift, const double* b, double* x,
 hmg_status hmg_gaussian_rhs(hmg_matrix* h, double* b)
 {
     HMG_REQUIRE(h && b, HMG_ERR_INVALID, "hmg_gaussian_rhs: NULL argument");
+    HMG_REQUIRE(!h->group_count, HMG_ERR_UNSUPPORTED, "hmg_gaussian_rhs: not available on a group handle");
     HMG_REQUIRE(h->points_set[0], HMG_ERR_STATE, "hmg_gaussian_rhs: points not set");
     return gaussian_rhs(h, b);
 }
@@ -401,6 +426,7 @@ hmg_status hmg_get_info(hmg_matrix* h, hmg_info* info)
             tier[2] |= r - r32 - r16 > 0;
         }
     info->matvec_launches = 1 + (int)tier[0] + (int)tier[1] + (int)tier[2] + (h->ntiles > 0 ? 1 : 0);
+    info->group_count = h->group_count;
     info->far_u_bytes = h->far_alg_u;
     info->far_v_bytes = h->far_alg_v;
     if (h->near_mode == HMG_NEAR_STORED && h->near_prec >= 0) mb += ne * nes;

@@ -48,6 +48,13 @@ struct hmg_matrix {
     bool kernel_set = false;
     hmg::KernelSpec kspec{};
 
+    // ---- grouped H-matrices (hmg_group_create) ---------------------------------
+    // The union of independent H-matrices: block-diagonal, each set's blocks shifted
+    // by its point offsets; the kernel parameter is per block.
+    int group_count = 0;              // 0: a single H-matrix
+    double* blk_param = nullptr;      // per block kernel parameter (groups only)
+    std::vector<int> group_off[2];    // first row / column of each set, then n
+
     // ---- near field -----------------------------------------------------------
     int near_mode = HMG_NEAR_ONTHEFLY;
     int near_prec = -1;               // -1: not stored
@@ -104,6 +111,7 @@ struct hmg_matrix {
 namespace hmg {
 hmg_status setup_tree(hmg_matrix* h);
 hmg_status build_tiles(hmg_matrix* h);
+hmg_status group_create(hmg_matrix** out, hmg_matrix* const* sets, int count, cudaStream_t s);
 hmg_status run_aca(hmg_matrix* h, int k, double eps, int precision);
 hmg_status fill_near(hmg_matrix* h, int precision);
 hmg_status matvec_device(hmg_matrix* h, const double* x, double* y, bool fp64_arith = false);

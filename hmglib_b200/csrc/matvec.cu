@@ -35,9 +35,10 @@ template <typename T>
 __global__ void k_fill_near(const int* blocks_r0, const int* blocks_c0, const int* blocks_m2,
                             const long long* near_off, const int* tfirst, const int* tlast,
                             const int* tile_r0, const int* tile_s, const int* tile_pstart,
-                            KernelSpec K, PointsView P, T* out)
+                            KernelSpec K, PointsView P, const double* bparam, T* out)
 {
     const int b = blockIdx.x;
+    if (bparam) K.param = bparam[b];
     const int c0 = blocks_c0[b], m2 = blocks_m2[b];
     (void)blocks_r0;
     T* base = out + near_off[b];
@@ -106,11 +107,11 @@ hmg_status fill_near(hmg_matrix* h, int precision)
         if (precision == HMG_PREC_FP64)
             k_fill_near<double><<<nd, 256, 0, s>>>(h->blk_r0, h->blk_c0, h->blk_m2, h->near_off,
                                                    h->blk_tfirst, h->blk_tlast, h->tile_r0, h->tile_s,
-                                                   h->tile_pstart, h->kspec, P, (double*)h->near_data);
+                                                   h->tile_pstart, h->kspec, P, h->blk_param, (double*)h->near_data);
         else
             k_fill_near<float><<<nd, 256, 0, s>>>(h->blk_r0, h->blk_c0, h->blk_m2, h->near_off,
                                                   h->blk_tfirst, h->blk_tlast, h->tile_r0, h->tile_s,
-                                                  h->tile_pstart, h->kspec, P, (float*)h->near_data);
+                                                  h->tile_pstart, h->kspec, P, h->blk_param, (float*)h->near_data);
         HMG_LAUNCH_CHECK();
     }
     HMG_CUDA_TRY(cudaStreamSynchronize(s));
@@ -697,6 +698,10 @@ hmg_status matvec_device(hmg_matrix* h, const double* x, double* y, bool fp64_ar
 {
     cudaStream_t s = h->stream;
     hmg_status st;
+    if (h->group_count && h->ndense > 0 && (h->near_mode != HMG_NEAR_STORED || h->near_prec < 0)) {
+        set_error("a group handle multiplies a stored near field: call hmg_precompute_dense first");
+        return HMG_ERR_STATE;
+    }
     if ((st = ensure_xs(h))) return st;
     const bool mixed = h->far_prec == HMG_PREC_MIXED;
     // storage element type of the stored near field and the FP32/FP64 terms

@@ -374,6 +374,7 @@ void free_tree(hmg_matrix* h)
     dfree(h->tile_r0, s); dfree(h->tile_s, s); dfree(h->tile_pstart, s);
     dfree(h->blk_tfirst, s); dfree(h->blk_tlast, s);
     dfree(h->tile_pair_start, s); dfree(h->pair_block, s);
+    dfree(h->blk_param, s);
     h->nblocks = h->ndense = h->naca = h->ntiles = h->npairs = h->levels = 0;
     h->setup_done = false;
 }

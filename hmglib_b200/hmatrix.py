@@ -138,6 +138,13 @@ class HMatrix:
         """0: streaming (bulk-copy) product kernels, 1: plain-load kernels."""
         self._call("hmg_set_matvec_variant", int(variant))
 
+    def offsets(self, which: int = 0) -> np.ndarray:
+        """Group handles: first row (which=0) or column (1) of every set, then n."""
+        cnt = self.info()["group_count"]
+        out = np.zeros(cnt + 1, dtype=np.int64)
+        self._call("hmg_group_offsets", int(which), _ptr(out))
+        return out
+
     def set_product_precision(self, precision: int):
         """Arithmetic of products over FP32/mixed storage: PREC_FP32 (default) or PREC_FP64."""
         self._call("hmg_set_product_precision", int(precision))
@@ -193,6 +200,23 @@ class HMatrix:
         V = np.zeros((max(rank, 1), m2))
         self._call("hmg_get_factors", int(block), _ptr(U), _ptr(V))
         return U[:rank], V[:rank]
+
+
+def group(sets, stream: int | None = None) -> "HMatrix":
+    """The block-diagonal union of set-up HMatrix objects (hmg_group_create): one
+    handle whose products cover every set in the same launches.  Vectors are the
+    concatenation of the sets' vectors; `offsets(0)` gives each set's first row."""
+    lib = L.lib()
+    arr = (C.c_void_p * len(sets))(*[hm._h.value for hm in sets])
+    h = C.c_void_p()
+    L.check(lib.hmg_group_create(C.byref(h), arr, len(sets), C.c_void_p(stream or 0)), "hmg_group_create")
+    g = HMatrix.__new__(HMatrix)
+    g._lib = lib
+    g._h = h
+    g.n1 = sum(hm.n1 for hm in sets)
+    g.n2 = sum(hm.n2 for hm in sets)
+    g.dim = max(hm.dim for hm in sets)
+    return g
 
 
 def radix_sort_u64(keys_ptr: int, vals_ptr: int, n: int, key_bits: int = 64, stream: int = 0):

@@ -71,6 +71,7 @@ typedef struct {
     int64_t far_u_bytes;      /* bytes of the stored U terms (sum m1 * rank * size, no padding) */
     int64_t far_v_bytes;      /* bytes of the stored V terms */
     int matvec_launches;      /* kernels one hmg_matvec launches (plain-load kernels) */
+    int group_count;          /* sets of a group handle (hmg_group_create), else 0 */
 } hmg_info;
 
 /* message of the last failed call on this thread ("" if none) */
@@ -129,6 +130,20 @@ hmg_status hmg_full_matvec(hmg_matrix* h, const double* x, double* y);
  * rows, x, y are device pointers.  Asynchronous. */
 hmg_status hmg_full_matvec_rows(hmg_matrix* h, const double* x, const int* rows, int nrows,
                                 double* y);
+
+/* Many independent H-matrices as one (no reference counterpart; the reference runs
+ * one h_matrix_data per call with its own MAGMA setup, hmglib.cu:119).  `sets` are
+ * handles after hmg_setup and hmg_set_kernel (same kernel kind and regularization,
+ * any parameter, 2D and 3D mixed).  The new handle is their block-diagonal union: its
+ * points are the sets' points in set order (rows of set i start at offset1_i, columns
+ * at offset2_i), each block keeps its set's kernel parameter.  hmg_precompute_aca,
+ * hmg_precompute_dense (required: the near field is stored), hmg_matvec,
+ * hmg_matvec_multi and hmg_cg_solve then cover all sets in the same kernel launches;
+ * vectors are the concatenation of the sets' vectors.  Each set's result equals its
+ * own handle's bit for bit.  The set handles stay valid and independent. */
+hmg_status hmg_group_create(hmg_matrix** out, hmg_matrix* const* sets, int count, void* stream);
+/* offsets[0..count] of a group's rows (set 0) or columns (set 1); offsets[count] = n */
+hmg_status hmg_group_offsets(hmg_matrix* h, int set, int64_t* offsets);
 
 /* Y = H X for 1 <= nrhs <= 32 vectors: X (n2 x nrhs) and Y (n1 x nrhs) are device
  * FP64 column-major with leading dimensions ldx >= n2, ldy >= n1, caller order.  The

@@ -1,0 +1,99 @@
+"""Many independent H-matrices multiplied as one (hmg_group_create).  No reference
+counterpart: the reference runs one h_matrix_data per call (hmglib.cu:119), so the
+check is against each set's own handle, bit for bit (a group never mixes sets inside
+a tile and keeps every tile's pair order)."""
+import numpy as np
+import pytest
+
+from helpers import engine, make_points, rel_err
+
+pytestmark = pytest.mark.gpu
+
+
+def _sets(hmg, sizes, seed=3):
+    rng = np.random.default_rng(seed)
+    out = []
+    for i, n in enumerate(sizes):
+        dim = 2 if i % 2 == 0 else 3
+        p = make_points("uniform", n, dim, seed * 1000 + i)
+        H = engine(hmg, p, p, 1.5, 64 if dim == 2 else 128, rule=1)
+        H.set_kernel(hmg.KERNEL_GAUSSIAN, float(rng.uniform(0.01, 0.2)), 0.0)
+        out.append(H)
+    return out
+
+
+@pytest.mark.parametrize("prec", [1, 0], ids=["fp32", "fp64"])
+def test_group_equals_sets(hmg, cuda, prec):
+    torch = cuda
+    sizes = [1024, 3000, 700, 5000, 64, 2500, 9000, 1500]
+    sets = _sets(hmg, sizes)
+    G = hmg.group(sets)
+    for H in sets:
+        H.precompute_aca(64, 1e-5, prec)
+        H.precompute_dense(prec)
+    G.precompute_aca(64, 1e-5, prec)
+    G.precompute_dense(prec)
+    off = G.offsets(0)
+    assert list(off) == list(np.concatenate([[0], np.cumsum(sizes)]))
+    n = int(off[-1])
+    x = np.random.default_rng(5).uniform(-1, 1, n)
+    y = G.matvec(x)
+    parts = [H.matvec(x[off[i]:off[i + 1]]) for i, H in enumerate(sets)]
+    np.testing.assert_array_equal(y, np.concatenate(parts))
+    # the admissible blocks' ranks: every set's, in set order
+    info = G.info()
+    r = G.ranks()
+    per = [H.ranks()[H.info()["dense_count"]:] for H in sets]
+    np.testing.assert_array_equal(r[info["dense_count"]:], np.concatenate(per))
+    assert info["group_count"] == len(sizes)
+    # several vectors at once
+    X = torch.from_numpy(np.random.default_rng(6).uniform(-1, 1, (4, n))).cuda()
+    Y = torch.empty_like(X)
+    G.matvec_multi(X, Y)
+    torch.cuda.synchronize()
+    for j in range(4):
+        yj = G.matvec(X[j].cpu().numpy())
+        assert rel_err(Y[j].cpu().numpy(), yj) < (1e-13 if prec == 0 else 1e-6)
+    for H in sets:
+        H.close()
+    G.close()
+
+
+def test_group_solve_and_errors(hmg, cuda):
+    torch = cuda
+    sets = _sets(hmg, [2000, 3000, 1200], seed=4)
+    G = hmg.group(sets)
+    with pytest.raises(hmg.HmgError):  # the near field must be stored first
+        G.precompute_aca(64, 1e-6, 1)
+        G.matvec(np.zeros(G.n2))
+    G.precompute_dense(1)
+    n = G.n1
+    b = torch.from_numpy(np.random.default_rng(2).uniform(-1, 1, n)).cuda()
+    x = torch.zeros(n, dtype=torch.float64, device="cuda")
+    it, rel = G.cg_solve(b, x, 0.1, tol=1e-8, maxit=2000, refine=True)
+    assert rel <= 1e-8 and it > 0
+    # the group's solution solves every set's own system
+    off = G.offsets(0)
+    for i, H in enumerate(sets):
+        H.precompute_aca(64, 1e-6, 1)
+        H.precompute_dense(1)
+        H.set_product_precision(hmg.PREC_FP64)
+        xi = x[off[i]:off[i + 1]].contiguous()
+        yi = torch.empty_like(xi)
+        H.matvec(xi, yi)
+        H.synchronize()
+        ri = b[off[i]:off[i + 1]] - (yi + 0.1 * xi)
+        assert float(torch.linalg.norm(ri)) <= 2e-8 * float(torch.linalg.norm(b))
+    d = torch.empty_like(b)
+    for call in (lambda: G.full_matvec(b, d), lambda: G.set_near_mode(hmg.NEAR_ONTHEFLY),
+                 lambda: G.set_kernel(hmg.KERNEL_GAUSSIAN, 0.1, 0.0)):
+        with pytest.raises(hmg.HmgError):
+            call()
+    # sets with different kernel kinds do not group
+    other = _sets(hmg, [500], seed=9)[0]
+    other.set_kernel(hmg.KERNEL_MATERN32, 0.2, 0.0)
+    with pytest.raises(hmg.HmgError):
+        hmg.group([sets[0], other])
+    for H in sets + [other]:
+        H.close()
+    G.close()
