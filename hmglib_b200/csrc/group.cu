@@ -47,8 +47,9 @@ hmg_status group_create(hmg_matrix** out, hmg_matrix* const* sets, int count, cu
             set_error("hmg_group_create: set %d is itself a group", i);
             return HMG_ERR_INVALID;
         }
+        // (the reference Matern kernel's normalisation depends on the dimension)
         if (h->kspec.kind != s0->kspec.kind || h->kspec.reg != s0->kspec.reg ||
-            h->kspec.matern_ref_denom != s0->kspec.matern_ref_denom) {
+            (h->kspec.kind == HMG_KERNEL_MATERN_REF && h->kspec.matern_ref_denom != s0->kspec.matern_ref_denom)) {
             set_error("hmg_group_create: set %d has another kernel kind or regularization than set 0", i);
             return HMG_ERR_INVALID;
         }
