@@ -63,3 +63,18 @@ def rhs_vector(n: int, seed: int, nrhs: int = 1) -> np.ndarray:
     """U[-1,1] right-hand side(s) from ``seed + 1000``; shape (n,) or (nrhs, n)."""
     u = uniform01(seed + 1000, n * nrhs) * 2.0 - 1.0
     return u if nrhs == 1 else u.reshape(nrhs, n)
+
+
+def group_sets(count: int = 512, seed: int = 3, log2_lo: float = 10.0, log2_hi: float = 16.0,
+               l2_lo: float = 0.01, l2_hi: float = 0.2):
+    """Many independent point sets: sizes round(2^U[log2_lo, log2_hi]), dimension
+    alternating 2, 3, points uniform in the unit box, Gaussian length^2 U[l2_lo, l2_hi].
+    Returns a list of (points (dim, n), squared length scale)."""
+    head = uniform01(seed, 2 * count)
+    out = []
+    for i in range(count):
+        n = int(round(2.0 ** (log2_lo + (log2_hi - log2_lo) * head[2 * i])))
+        l2 = l2_lo + (l2_hi - l2_lo) * head[2 * i + 1]
+        dim = 2 if i % 2 == 0 else 3
+        out.append((uniform_points(n, dim, (seed << 20) + i + 1), float(l2)))
+    return out
