@@ -470,6 +470,84 @@ def run_group(a, rank, world):
     return 0
 
 
+def run_serve(a, rank, world):
+    """The serving workload: 8 resident H-matrices (N = 2^16 .. 2^20 log-spaced, uniform
+    3D, Matern-3/2 rho 0.2, ACA eps 1e-5, mixed storage) and a Poisson stream at
+    2000 requests/s (seed 4): 80% single-vector products, 15% 8-vector kernel-ridge
+    solves (shift 1e-4 N, relative residual 1e-5), 5% new point sets of 2^14-2^18
+    points, under a 120 GB budget.  Reports p50/p99 latency and throughput against the
+    plain FP64 one-request-at-a-time path (FP64 products, one vector per call, solves
+    by hmg_cg_solve per column) on the same H-matrices and the first requests."""
+    import torch
+
+    import hmglib_b200 as hmg
+    from hmglib_b200 import serve, synth
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    sizes = [int(round(2.0 ** (16 + 4.0 * i / 7))) for i in range(8)]
+    t0 = time.perf_counter()
+    srv = serve.Server(budget_bytes=120e9)
+    for i, n in enumerate(sizes):
+        st = torch.cuda.Stream()
+        H = serve.build_hmatrix(synth.uniform_points(n, 3, 4000 + i), hmg.KERNEL_MATERN32, 0.2, 1e-5,
+                                hmg.PREC_MIXED, stream=st.cuda_stream)
+        srv.add(H, st)
+    t_build = time.perf_counter() - t0
+    resident = srv.used_bytes()
+    reqs = serve.poisson_requests(a.serve_requests, 2000.0, sizes, seed=4)
+    # warm-up: one small batch of every kind on every resident matrix
+    warm = [serve.Matvec(m, np.zeros(n)) for m, n in enumerate(sizes)]
+    srv.run(warm)
+    with ClockSampler(local) as clk:
+        done, wall = srv.run(reqs, time_limit=1200.0)
+    lat = serve.latency_summary(done)
+    n_done = sum(q.done is not None for q in done)
+    batches = [q.batch for q in done if isinstance(q, serve.Matvec)]
+    # the plain path: one request at a time, FP64 products, no batching, no overlap
+    nb = min(a.serve_baseline, len(reqs))
+    base = reqs[:nb]
+    for r in srv.res.values():
+        r.H.set_product_precision(hmg.PREC_FP64)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for q in base:
+        if isinstance(q, serve.Matvec):
+            srv.res[q.mid].H.matvec(q.x)
+        elif isinstance(q, serve.Solve):
+            H = srv.res[q.mid].H
+            for j in range(q.B.shape[0]):
+                b = torch.from_numpy(q.B[j]).cuda()
+                x = torch.zeros_like(b)
+                H.cg_solve(b, x, q.shift, tol=q.tol, maxit=q.maxit, refine=False)
+        else:
+            Hn = serve.build_hmatrix(q.points, q.kind, q.param, q.eps, hmg.PREC_FP64)
+            Hn.close()
+    torch.cuda.synchronize()
+    t_base = time.perf_counter() - t0
+    sub = [q for q in done[:nb] if q.done is not None]
+    t_sub = max(q.done for q in sub) - min(q.arrival for q in sub) if sub else float("nan")
+    line = {
+        "metric": "served requests/s (8 resident H-matrices, Poisson 2000 req/s); p50/p99 latency",
+        "value": n_done / wall, "unit": "requests/s", "n_gpus": 1, "steps": len(reqs), "warmup": len(warm),
+        "ms_per_step": 1000.0 * wall / max(1, n_done), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "serve_8resident_matern3d_poisson2000", "sizes": sizes, "aca_eps": 1e-5,
+                   "storage": "mixed", "budget_gb": 120, "requests": len(reqs), "mix": [0.8, 0.15, 0.05]},
+        "latency": lat, "matvec_batch": {"mean": float(np.mean(batches)), "max": int(np.max(batches))},
+        "plain_fp64_one_at_a_time": {"requests": nb, "seconds": t_base, "requests_per_s": nb / t_base,
+                                     "served_same_requests_s": t_sub,
+                                     "speedup": (t_base / t_sub) if sub else None},
+        "resident_gb": resident / 1e9, "build_s": t_build, "clocks": clk.summary(),
+        "e2e": {"value": n_done / wall, "unit": "requests/s", "h2d_bytes_per_step": None,
+                "d2h_bytes_per_step": None},
+    }
+    for mid in list(srv.res):
+        srv.res.pop(mid).H.close()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    return 0
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -485,8 +563,11 @@ def main(argv=None):
                     help="arithmetic of the products over FP32/mixed storage")
     ap.add_argument("--variant", type=int, default=1, choices=[0, 1],
                     help="product kernels: 1 plain 16-byte loads (default), 0 bulk-copy streaming")
-    ap.add_argument("--workload", default="uniform3d", choices=["uniform3d", "group"],
-                    help="uniform3d: the N=2^20 headline; group: many small H-matrices as one")
+    ap.add_argument("--workload", default="uniform3d", choices=["uniform3d", "group", "serve"],
+                    help="uniform3d: the N=2^20 headline; group: many small H-matrices as one; "
+                         "serve: the request loop over resident H-matrices")
+    ap.add_argument("--serve-requests", type=int, default=600)
+    ap.add_argument("--serve-baseline", type=int, default=60)
     ap.add_argument("--group-count", type=int, default=512)
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--no-cpu", action="store_true")
@@ -498,6 +579,8 @@ def main(argv=None):
         return run_reference(a, rank, world)
     if a.workload == "group":
         return run_group(a, rank, world) if rank == 0 else 0
+    if a.workload == "serve":
+        return run_serve(a, rank, world) if rank == 0 else 0
     if world > 1:
         import datetime
 

@@ -1,0 +1,367 @@
+"""A serving loop over resident H-matrices: continuous batching of products and
+kernel-ridge solves, construction of new point sets under an HBM budget, and
+per-request latency.
+
+No reference counterpart (hmglib is a library of blocking calls on one H-matrix).
+The loop keeps compressed H-matrices resident on the device, each with its own CUDA
+stream so that work on different H-matrices overlaps on the GPU, and admits requests
+as they arrive:
+
+* ``Matvec(mid, x)``: requests queued on the same H-matrix are packed, up to 32 at a
+  time, into one ``hmg_matvec_multi`` call (the stored H-matrix is read once for the
+  whole batch).  A request that arrives while a batch is on the GPU joins the next.
+* ``Solve(mid, B, shift)``: kernel-ridge CG on (H + shift I) X = B for the columns of
+  B, advanced in lockstep: one multi-vector product per iteration for all columns,
+  the vector updates on the H-matrix's stream, residual norms read back
+  asynchronously (up to two iterations in flight, no host synchronisation), converged
+  columns frozen.  Solve iterations and product batches on the same H-matrix
+  interleave.  Products use the handle's arithmetic (FP32 by default), so the
+  attainable residual is ~1e-7 times the condition number.
+* ``Build(points, ...)``: a new point set compressed on a worker thread with its own
+  stream, admitted only when the budget holds its estimated bytes (idle H-matrices
+  built by earlier requests are evicted, least recently used first).
+
+``run(requests)`` replays an arrival timeline (seconds from the start) and returns
+the requests with their completion times; latency = completion - arrival, measured
+on the host clock when the result's CUDA event has completed.
+"""
+from __future__ import annotations
+
+import collections
+import threading
+import time
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _lib as L
+from .hmatrix import HMatrix
+
+MAX_BATCH = 32
+
+
+@dataclass
+class Matvec:
+    mid: int
+    x: np.ndarray
+    arrival: float = 0.0
+    y: np.ndarray | None = None
+    done: float | None = None
+    batch: int = 0
+
+
+@dataclass
+class Solve:
+    mid: int
+    B: np.ndarray            # (k, n) right-hand sides
+    shift: float
+    tol: float = 1e-5
+    maxit: int = 2000
+    arrival: float = 0.0
+    X: np.ndarray | None = None
+    iters: int = 0
+    relres: np.ndarray | None = None
+    done: float | None = None
+
+
+@dataclass
+class Build:
+    points: np.ndarray       # (dim, n)
+    kind: int
+    param: float
+    eps: float
+    precision: int
+    arrival: float = 0.0
+    mid: int | None = None
+    done: float | None = None
+    rejected: str | None = None
+
+
+@dataclass
+class _Resident:
+    H: HMatrix
+    stream: object
+    nbytes: int
+    pinned: bool
+    last_use: float = 0.0
+    matvecs: collections.deque = field(default_factory=collections.deque)
+    solves: list = field(default_factory=list)
+    inflight: list = field(default_factory=list)   # (event, finisher)
+
+
+def build_hmatrix(points, kind, param, eps, precision, stream=None, max_rank=64, eta=1.5, leaf=None):
+    """Set up and compress one H-matrix (synchronous on `stream`)."""
+    dim, n = points.shape
+    H = HMatrix(n, n, dim, stream=stream)
+    H.set_points(0, points)
+    H.set_points(1, points)
+    H.setup(eta, leaf or (64 if dim == 2 else 128), rule=L.ADMISSIBLE_MIN)
+    H.set_kernel(kind, param, 0.0)
+    H.precompute_aca(max_rank, eps, precision)
+    H.precompute_dense(L.PREC_FP32 if precision == L.PREC_MIXED else precision)
+    H.synchronize()
+    return H
+
+
+def resident_bytes(H: HMatrix) -> int:
+    i = H.info()
+    return int(i["near_bytes"] + i["far_bytes"] + 8 * 4 * (i["n1"] + i["n2"]))
+
+
+class Server:
+    def __init__(self, budget_bytes: float, device: int = 0):
+        import torch
+        self.torch = torch
+        self.device = device
+        self.budget = int(budget_bytes)
+        self.res: dict[int, _Resident] = {}
+        self.next_id = 0
+        self.builds: collections.deque = collections.deque()
+        self.build_thread: threading.Thread | None = None
+        self.build_result = None
+        self.bytes_per_point = None
+
+    # -- residency -------------------------------------------------------------
+    def used_bytes(self) -> int:
+        return sum(r.nbytes for r in self.res.values())
+
+    def add(self, H: HMatrix, stream, pinned: bool = True) -> int:
+        mid = self.next_id
+        self.next_id += 1
+        self.res[mid] = _Resident(H, stream, resident_bytes(H), pinned)
+        bpp = self.res[mid].nbytes / max(1, H.n1)
+        self.bytes_per_point = bpp if self.bytes_per_point is None else max(self.bytes_per_point, bpp)
+        return mid
+
+    def _evict_for(self, need: int) -> bool:
+        while self.used_bytes() + need > self.budget:
+            idle = [(r.last_use, mid) for mid, r in self.res.items()
+                    if not r.pinned and not r.matvecs and not r.solves and not r.inflight]
+            if not idle:
+                return False
+            _, mid = min(idle)
+            self.res.pop(mid).H.close()
+        return True
+
+    # -- request intake ----------------------------------------------------------
+    def submit(self, req, now: float):
+        if isinstance(req, Matvec):
+            self.res[req.mid].matvecs.append(req)
+        elif isinstance(req, Solve):
+            self.res[req.mid].solves.append(self._start_solve(req))
+        else:
+            self.builds.append(req)
+
+    # -- products ----------------------------------------------------------------
+    def _launch_matvecs(self, r: _Resident, now: float):
+        torch = self.torch
+        batch = [r.matvecs.popleft() for _ in range(min(MAX_BATCH, len(r.matvecs)))]
+        with torch.cuda.stream(r.stream):
+            X = torch.from_numpy(np.stack([q.x for q in batch])).pin_memory().cuda(non_blocking=True)
+            Y = torch.empty(len(batch), r.H.n1, dtype=torch.float64, device="cuda")
+            if len(batch) == 1:
+                r.H.matvec(X[0], Y[0])
+            else:
+                r.H.matvec_multi(X, Y)
+            Yh = torch.empty(Y.shape, dtype=torch.float64, pin_memory=True)
+            Yh.copy_(Y, non_blocking=True)
+            ev = torch.cuda.Event()
+            ev.record(r.stream)
+
+        def finish(t):
+            for j, q in enumerate(batch):
+                q.y = Yh[j].numpy().copy()
+                q.done = t
+                q.batch = len(batch)
+        r.inflight.append((ev, finish, (X, Y)))
+        r.last_use = now
+
+    # -- block CG (one multi-vector product per iteration) -------------------------
+    def _start_solve(self, req: Solve):
+        torch = self.torch
+        r = self.res[req.mid]
+        with torch.cuda.stream(r.stream):
+            B = torch.from_numpy(np.ascontiguousarray(req.B)).pin_memory().cuda(non_blocking=True)
+            st = {"req": req, "B": B, "X": torch.zeros_like(B), "R": B.clone(), "P": B.clone(),
+                  "Q": torch.empty_like(B), "rr": (B * B).sum(1), "it": 0,
+                  "checks": collections.deque(), "final": None}
+            st["rr0"] = st["rr"].clone()
+            st["active"] = torch.ones(B.shape[0], dtype=torch.bool, device="cuda")
+        return st
+
+    def _step_solve(self, r: _Resident, st, now: float):
+        """Advance one solve; True once its result has reached the host."""
+        torch = self.torch
+        req = st["req"]
+        if st["final"] is not None:
+            ev, Xh, rel, it = st["final"]
+            if not ev.query():
+                return False
+            req.X, req.iters, req.relres, req.done = Xh.numpy().copy(), it, rel, time.perf_counter()
+            return True
+        # residual norms come back one iteration late; at most two iterations in flight
+        converged = False
+        while st["checks"] and st["checks"][0][0].query():
+            ev, host, it = st["checks"].popleft()
+            rel = np.sqrt(host[0].numpy() / np.maximum(host[1].numpy(), 1e-300))
+            if (rel <= req.tol).all() or it >= req.maxit:
+                converged = True
+                break
+        with torch.cuda.stream(r.stream):
+            if converged:
+                Xh = torch.empty(st["X"].shape, dtype=torch.float64, pin_memory=True)
+                Xh.copy_(st["X"], non_blocking=True)
+                ev = torch.cuda.Event()
+                ev.record(r.stream)
+                st["final"] = (ev, Xh, rel, it)
+                st["checks"].clear()
+                return False
+            if len(st["checks"]) >= 2:
+                return False
+            P, Q, R, X = st["P"], st["Q"], st["R"], st["X"]
+            if P.shape[0] == 1:
+                r.H.matvec(P[0], Q[0])
+            else:
+                r.H.matvec_multi(P, Q)
+            Q.add_(P, alpha=req.shift)
+            pq = (P * Q).sum(1)
+            rr = st["rr"]
+            act = st["active"]
+            # converged columns are frozen (alpha = beta = 0)
+            alpha = torch.where(act & (pq > 0), rr / torch.where(pq > 0, pq, torch.ones_like(pq)),
+                                torch.zeros_like(pq))
+            X.addcmul_(alpha[:, None], P)
+            R.addcmul_(-alpha[:, None], Q)
+            rr_new = torch.where(act, (R * R).sum(1), rr)
+            beta = torch.where(act, rr_new / torch.where(rr > 0, rr, torch.ones_like(rr)), torch.zeros_like(rr))
+            P.mul_(beta[:, None]).add_(R)
+            st["active"] = act & (rr_new > (req.tol ** 2) * st["rr0"])
+            st["rr"] = rr_new
+            st["it"] += 1
+            host = (torch.empty(rr_new.shape, dtype=torch.float64, pin_memory=True),
+                    torch.empty(rr_new.shape, dtype=torch.float64, pin_memory=True))
+            host[0].copy_(rr_new, non_blocking=True)
+            host[1].copy_(st["rr0"], non_blocking=True)
+            ev = torch.cuda.Event()
+            ev.record(r.stream)
+            st["checks"].append((ev, host, st["it"]))
+        r.last_use = now
+        return False
+
+    # -- construction on a worker thread -----------------------------------------------
+    def _poll_builds(self, now: float):
+        torch = self.torch
+        if self.build_thread is not None:
+            if self.build_thread.is_alive():
+                return
+            self.build_thread.join()
+            req, H, stream, err = self.build_result
+            self.build_thread = None
+            if err is not None:
+                req.rejected = err
+            else:
+                req.mid = self.add(H, stream, pinned=False)
+            req.done = time.perf_counter()
+        if not self.builds:
+            return
+        req = self.builds[0]
+        est = int((self.bytes_per_point or 0) * req.points.shape[1] * 1.5)
+        if not self._evict_for(est):
+            return  # wait for resident work to drain
+        self.builds.popleft()
+        stream = torch.cuda.Stream()
+
+        def work():
+            torch.cuda.set_device(self.device)
+            try:
+                H = build_hmatrix(req.points, req.kind, req.param, req.eps, req.precision,
+                                  stream=stream.cuda_stream)
+                self.build_result = (req, H, stream, None)
+            except Exception as e:  # the request fails, the server goes on
+                self.build_result = (req, None, stream, str(e))
+        self.build_thread = threading.Thread(target=work, daemon=True)
+        self.build_thread.start()
+
+    # -- the loop --------------------------------------------------------------------------
+    def _poll(self, now: float) -> bool:
+        busy = False
+        for r in list(self.res.values()):
+            keep = []
+            for ev, finish, hold in r.inflight:
+                if ev.query():
+                    finish(time.perf_counter())
+                else:
+                    keep.append((ev, finish, hold))
+            r.inflight = keep
+            # one product batch in flight per H-matrix; solves advance between batches
+            if r.matvecs and not r.inflight:
+                self._launch_matvecs(r, now)
+            still = []
+            for st in r.solves:
+                if not self._step_solve(r, st, now):
+                    still.append(st)
+            r.solves = still
+            busy |= bool(r.matvecs or r.inflight or r.solves)
+        self._poll_builds(now)
+        busy |= bool(self.builds or self.build_thread is not None)
+        return busy
+
+    def run(self, requests, time_limit: float = 600.0):
+        """Replay `requests` (each with .arrival in seconds from the start)."""
+        order = sorted(requests, key=lambda q: q.arrival)
+        t0 = time.perf_counter()
+        i = 0
+        while True:
+            now = time.perf_counter() - t0
+            while i < len(order) and order[i].arrival <= now:
+                self.submit(order[i], now)
+                i += 1
+            busy = self._poll(now)
+            if i >= len(order) and not busy:
+                break
+            if now > time_limit:
+                raise TimeoutError("serving run exceeded its time limit")
+            if not busy and i < len(order):
+                time.sleep(max(0.0, min(order[i].arrival - now, 1e-3)))
+        for q in order:
+            if q.done is not None:
+                q.done -= t0
+        return order, time.perf_counter() - t0
+
+
+def latency_summary(reqs):
+    out = {}
+    for name, cls in (("matvec", Matvec), ("solve", Solve), ("build", Build), ("all", object)):
+        lat = np.array([q.done - q.arrival for q in reqs if isinstance(q, cls) and q.done is not None])
+        if lat.size:
+            out[name] = {"count": int(lat.size), "p50_ms": float(np.percentile(lat, 50) * 1e3),
+                         "p99_ms": float(np.percentile(lat, 99) * 1e3), "max_ms": float(lat.max() * 1e3)}
+    return out
+
+
+def poisson_requests(n_requests: int, rate: float, sizes, seed: int = 4, mix=(0.80, 0.15, 0.05),
+                     solve_rhs: int = 8, build_lo: float = 14.0, build_hi: float = 18.0,
+                     kind: int = L.KERNEL_MATERN32, param: float = 0.2, eps: float = 1e-5,
+                     precision: int = L.PREC_MIXED, shift_per_point: float = 1e-4, tol: float = 1e-5):
+    """The serving mix: Poisson arrivals at `rate` per second (SplitMix64 stream
+    `seed`); each request is a single-vector product (mix[0]), a `solve_rhs`-vector
+    kernel-ridge solve (mix[1]) or a new uniform 3D point set of 2^U[build_lo,
+    build_hi] points (mix[2]).  Products and solves pick one of the resident
+    H-matrices (`sizes[i]` points each) uniformly; vectors are U[-1, 1]."""
+    from . import synth
+    u = synth.uniform01(seed, 4 * n_requests)
+    t = np.cumsum(-np.log1p(-u[:n_requests]) / rate)
+    out = []
+    for i in range(n_requests):
+        a, b = u[n_requests + i], u[2 * n_requests + i]
+        mid = min(int(b * len(sizes)), len(sizes) - 1)
+        vseed = (seed << 24) + i
+        if a < mix[0]:
+            out.append(Matvec(mid, synth.uniform01(vseed, sizes[mid]) * 2.0 - 1.0, arrival=float(t[i])))
+        elif a < mix[0] + mix[1]:
+            B = (synth.uniform01(vseed, solve_rhs * sizes[mid]) * 2.0 - 1.0).reshape(solve_rhs, sizes[mid])
+            out.append(Solve(mid, B, shift_per_point * sizes[mid], tol=tol, arrival=float(t[i])))
+        else:
+            n = int(round(2.0 ** (build_lo + (build_hi - build_lo) * u[3 * n_requests + i])))
+            out.append(Build(synth.uniform_points(n, 3, vseed), kind, param, eps, precision, arrival=float(t[i])))
+    return out
