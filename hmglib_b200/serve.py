@@ -11,7 +11,7 @@ as they arrive:
   time, into one ``hmg_matvec_multi`` call (the stored H-matrix is read once for the
   whole batch).  A request that arrives while a batch is on the GPU joins the next.
 * ``Solve(mid, B, shift)``: kernel-ridge CG on (H + shift I) X = B for the columns of
-  B, advanced in lockstep: one multi-vector product per iteration for all columns,
+  B (at most MAX_SOLVES per H-matrix at a time, the others wait), advanced in lockstep: one multi-vector product per iteration for all columns,
   the vector updates on the H-matrix's stream, residual norms read back
   asynchronously (up to two iterations in flight, no host synchronisation), converged
   columns frozen.  Solve iterations and product batches on the same H-matrix
@@ -37,7 +37,8 @@ import numpy as np
 from . import _lib as L
 from .hmatrix import HMatrix
 
-MAX_BATCH = 32
+MAX_BATCH = 32       # vectors per product pass
+MAX_SOLVES = 2       # solves advancing at once per H-matrix (their vectors live on the device)
 
 
 @dataclass
@@ -85,11 +86,13 @@ class _Resident:
     pinned: bool
     last_use: float = 0.0
     matvecs: collections.deque = field(default_factory=collections.deque)
+    waiting_solves: collections.deque = field(default_factory=collections.deque)
     solves: list = field(default_factory=list)
     inflight: list = field(default_factory=list)   # (event, finisher)
 
 
 def build_hmatrix(points, kind, param, eps, precision, stream=None, max_rank=64, eta=1.5, leaf=None):
+    # leaf: 64 (2D) / 128 (3D) unless given
     """Set up and compress one H-matrix (synchronous on `stream`)."""
     dim, n = points.shape
     H = HMatrix(n, n, dim, stream=stream)
@@ -136,7 +139,8 @@ class Server:
     def _evict_for(self, need: int) -> bool:
         while self.used_bytes() + need > self.budget:
             idle = [(r.last_use, mid) for mid, r in self.res.items()
-                    if not r.pinned and not r.matvecs and not r.solves and not r.inflight]
+                    if not r.pinned and not r.matvecs and not r.solves and not r.waiting_solves
+                    and not r.inflight]
             if not idle:
                 return False
             _, mid = min(idle)
@@ -148,7 +152,7 @@ class Server:
         if isinstance(req, Matvec):
             self.res[req.mid].matvecs.append(req)
         elif isinstance(req, Solve):
-            self.res[req.mid].solves.append(self._start_solve(req))
+            self.res[req.mid].waiting_solves.append(req)
         else:
             self.builds.append(req)
 
@@ -296,12 +300,14 @@ class Server:
             # one product batch in flight per H-matrix; solves advance between batches
             if r.matvecs and not r.inflight:
                 self._launch_matvecs(r, now)
+            while r.waiting_solves and len(r.solves) < MAX_SOLVES:
+                r.solves.append(self._start_solve(r.waiting_solves.popleft()))
             still = []
             for st in r.solves:
                 if not self._step_solve(r, st, now):
                     still.append(st)
             r.solves = still
-            busy |= bool(r.matvecs or r.inflight or r.solves)
+            busy |= bool(r.matvecs or r.inflight or r.solves or r.waiting_solves)
         self._poll_builds(now)
         busy |= bool(self.builds or self.build_thread is not None)
         return busy
