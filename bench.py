@@ -471,8 +471,9 @@ def run_group(a, rank, world):
 
 
 def run_serve(a, rank, world):
-    """The serving workload: 8 resident H-matrices (N = 2^16 .. 2^20 log-spaced, uniform
-    3D, Matern-3/2 rho 0.2, leaf 64, ACA eps 1e-4, mixed storage) and a Poisson stream at
+    """The serving workload: 8 resident H-matrices (four of 2^16 points, then 2^17, 2^18,
+    2^19, 2^20; uniform 3D, Matern-3/2 rho 0.2, leaf 64, ACA eps 1e-4, mixed storage:
+    ~96 GB) and a Poisson stream at
     2000 requests/s (seed 4): 80% single-vector products, 15% 8-vector kernel-ridge
     solves (shift 1e-3 N, relative residual 1e-4), 5% new point sets of 2^14-2^18
     points, under a 120 GB budget.  Reports p50/p99 latency and throughput against the
@@ -484,7 +485,7 @@ def run_serve(a, rank, world):
     from hmglib_b200 import serve, synth
     local = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(local)
-    sizes = [int(round(2.0 ** (16 + 4.0 * i / 7))) for i in range(8)]
+    sizes = [1 << 16] * 4 + [1 << 17, 1 << 18, 1 << 19, 1 << 20]
     t0 = time.perf_counter()
     srv = serve.Server(budget_bytes=120e9)
     for i, n in enumerate(sizes):

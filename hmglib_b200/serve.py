@@ -270,6 +270,13 @@ class Server:
             return
         req = self.builds[0]
         est = int((self.bytes_per_point or 0) * req.points.shape[1] * 1.5)
+        pinned = sum(r.nbytes for r in self.res.values() if r.pinned)
+        if pinned + est > self.budget:
+            # can never fit beside the pinned H-matrices: refuse it now
+            self.builds.popleft()
+            req.rejected = f"needs ~{est / 1e9:.1f} GB beside {pinned / 1e9:.1f} GB pinned (budget {self.budget / 1e9:.1f} GB)"
+            req.done = time.perf_counter()
+            return
         if not self._evict_for(est):
             return  # wait for resident work to drain
         self.builds.popleft()
@@ -326,7 +333,8 @@ class Server:
             if i >= len(order) and not busy:
                 break
             if now > time_limit:
-                raise TimeoutError("serving run exceeded its time limit")
+                left = collections.Counter(type(q).__name__ for q in order if q.done is None)
+                raise TimeoutError(f"serving run exceeded its time limit; unfinished: {dict(left)}")
             if not busy and i < len(order):
                 time.sleep(max(0.0, min(order[i].arrival - now, 1e-3)))
         for q in order:
