@@ -374,7 +374,7 @@ def poisson_requests(n_requests: int, rate: float, sizes, seed: int = 4, mix=(0.
             out.append(Matvec(mid, synth.uniform01(vseed, sizes[mid]) * 2.0 - 1.0, arrival=float(t[i])))
         elif a < mix[0] + mix[1]:
             B = (synth.uniform01(vseed, solve_rhs * sizes[mid]) * 2.0 - 1.0).reshape(solve_rhs, sizes[mid])
-            out.append(Solve(mid, B, shift_per_point * sizes[mid], tol=tol, arrival=float(t[i])))
+            out.append(Solve(mid, B, shift_per_point * sizes[mid], tol=tol, maxit=300, arrival=float(t[i])))
         else:
             n = int(round(2.0 ** (build_lo + (build_hi - build_lo) * u[3 * n_requests + i])))
             out.append(Build(synth.uniform_points(n, 3, vseed), kind, param, eps, precision, arrival=float(t[i])))
