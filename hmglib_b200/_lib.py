@@ -66,6 +66,8 @@ _PROTOS = {
     "hmg_matvec_multi": (C.c_int, [_vp, C.c_int, _vp, C.c_int, _vp, C.c_int]),
     "hmg_group_create": (C.c_int, [C.POINTER(_vp), C.POINTER(_vp), C.c_int, _vp]),
     "hmg_group_offsets": (C.c_int, [_vp, C.c_int, _vp]),
+    "hmg_save": (C.c_int, [_vp, C.c_char_p]),
+    "hmg_load": (C.c_int, [C.POINTER(_vp), C.c_char_p, _vp]),
     "hmg_full_matvec": (C.c_int, [_vp, _vp, _vp]),
     "hmg_full_matvec_rows": (C.c_int, [_vp, _vp, _vp, C.c_int, _vp]),
     "hmg_gaussian_rhs": (C.c_int, [_vp, _vp]),

@@ -493,6 +493,7 @@ void free_far(hmg_matrix* h)
     cudaStream_t s = h->stream;
     for (void* p : h->far_chunks) cudaFree(p);
     h->far_chunks.clear();
+    h->far_chunk_bytes.clear();
     dfree(h->rank, s);
     dfree(h->rank_off, s);
     dfree(h->ptrU, s);
@@ -669,6 +670,7 @@ hmg_status run_aca(hmg_matrix* h, int k, double eps, int precision)
                 return ce == cudaErrorMemoryAllocation ? HMG_ERR_NOMEM : HMG_ERR_CUDA;
             }
             h->far_chunks.push_back(chunk);
+            h->far_chunk_bytes.push_back((size_t)bytes);
             h->far_stored += bytes;
             for (int e = 0; e < ne; e++) {
                 pU[idx[e]] = chunk + ofsU[e];

@@ -224,6 +224,20 @@ hmg_status hmg_matvec(hmg_matrix* h, const double* x, double* y)
     return matvec_device(h, x, y);
 }
 
+hmg_status hmg_save(hmg_matrix* h, const char* path)
+{
+    HMG_REQUIRE(h && path, HMG_ERR_INVALID, "hmg_save: NULL argument");
+    HMG_REQUIRE(h->setup_done, HMG_ERR_STATE, "hmg_save: call hmg_setup first");
+    return save(h, path);
+}
+
+hmg_status hmg_load(hmg_matrix** out, const char* path, void* stream)
+{
+    HMG_REQUIRE(out && path, HMG_ERR_INVALID, "hmg_load: NULL argument");
+    *out = nullptr;
+    return load(out, path, (cudaStream_t)stream);
+}
+
 hmg_status hmg_group_create(hmg_matrix** out, hmg_matrix* const* sets, int count, void* stream)
 {
     HMG_REQUIRE(out && sets, HMG_ERR_INVALID, "hmg_group_create: NULL argument");

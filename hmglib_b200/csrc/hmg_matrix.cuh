@@ -73,6 +73,7 @@ struct hmg_matrix {
     void** ptrU = nullptr;            // per block device pointer (ACA blocks)
     void** ptrV = nullptr;
     std::vector<void*> far_chunks;    // allocations holding the factors
+    std::vector<size_t> far_chunk_bytes;
     std::vector<int> h_rank;
     int* tier32 = nullptr;            // mixed storage: per block terms in FP32
     int* tier16 = nullptr;            // ... in FP16 (the rest of the rank in FP8)
@@ -112,6 +113,8 @@ namespace hmg {
 hmg_status setup_tree(hmg_matrix* h);
 hmg_status build_tiles(hmg_matrix* h);
 hmg_status group_create(hmg_matrix** out, hmg_matrix* const* sets, int count, cudaStream_t s);
+hmg_status save(hmg_matrix* h, const char* path);
+hmg_status load(hmg_matrix** out, const char* path, cudaStream_t s);
 hmg_status run_aca(hmg_matrix* h, int k, double eps, int precision);
 hmg_status fill_near(hmg_matrix* h, int precision);
 hmg_status matvec_device(hmg_matrix* h, const double* x, double* y, bool fp64_arith = false);

@@ -138,6 +138,10 @@ class HMatrix:
         """0: streaming (bulk-copy) product kernels, 1: plain-load kernels."""
         self._call("hmg_set_matvec_variant", int(variant))
 
+    def save(self, path: str):
+        """Write the H-matrix to `path` (hmg_save)."""
+        self._call("hmg_save", str(path).encode())
+
     def offsets(self, which: int = 0) -> np.ndarray:
         """Group handles: first row (which=0) or column (1) of every set, then n."""
         cnt = self.info()["group_count"]
@@ -200,6 +204,19 @@ class HMatrix:
         V = np.zeros((max(rank, 1), m2))
         self._call("hmg_get_factors", int(block), _ptr(U), _ptr(V))
         return U[:rank], V[:rank]
+
+
+def load(path: str, stream: int | None = None) -> "HMatrix":
+    """An H-matrix written by HMatrix.save (hmg_load)."""
+    lib = L.lib()
+    h = C.c_void_p()
+    L.check(lib.hmg_load(C.byref(h), str(path).encode(), C.c_void_p(stream or 0)), "hmg_load")
+    H = HMatrix.__new__(HMatrix)
+    H._lib = lib
+    H._h = h
+    i = H.info()
+    H.n1, H.n2, H.dim = i["n1"], i["n2"], i["dim"]
+    return H
 
 
 def group(sets, stream: int | None = None) -> "HMatrix":

@@ -131,6 +131,15 @@ hmg_status hmg_full_matvec(hmg_matrix* h, const double* x, double* y);
 hmg_status hmg_full_matvec_rows(hmg_matrix* h, const double* x, const int* rows, int nrows,
                                 double* y);
 
+/* Write a set-up H-matrix to `path` (points, permutations, block list, ranks and
+ * storage tiers, factors, stored near field) and read it back into a new handle on
+ * `stream`; the loaded H-matrix multiplies bit-identically to the saved one.  The
+ * format is this library's own (versioned; other versions are refused with
+ * HMG_ERR_UNSUPPORTED).  Synchronous.  No reference counterpart (the reference only
+ * prints its tree for debugging, tree.cu:173-183). */
+hmg_status hmg_save(hmg_matrix* h, const char* path);
+hmg_status hmg_load(hmg_matrix** out, const char* path, void* stream);
+
 /* Many independent H-matrices as one (no reference counterpart; the reference runs
  * one h_matrix_data per call with its own MAGMA setup, hmglib.cu:119).  `sets` are
  * handles after hmg_setup and hmg_set_kernel (same kernel kind and regularization,
