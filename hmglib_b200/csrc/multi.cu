@@ -395,167 +395,6 @@ __global__ void __launch_bounds__(256) k_tile_multi_smem(const PairDesc* __restr
     }
 }
 
-// FP32 storage, R = 8, 16 or 32 vectors, small pairs packed: a tile's pairs are read
-// in windows of 128 descriptors, and their columns form one stream cut into stages of
-// 32 columns regardless of pair boundaries (three stages in flight, cp.async), so a
-// pair of rank 5 costs 5 columns of a stage, not a stage.  Each stage carries, per
-// column, the slice column, the vector row (x for dense pairs, t_b for low-rank ones)
-// and whether the column ends its pair (FP32 sum added into FP64 there).
-struct PackCol {
-    const float* u;  // slice column (s_pad floats), null past the stream's end
-    const float* t;  // R floats multiplying it
-    int flush;       // last column of its pair
-    int pad;
-};
-
-static constexpr int PK_KC = 32, PK_NS = 3, PK_W = 128;
-
-template <int R>
-constexpr size_t pack_smem()
-{
-    return sizeof(float) * PK_NS * PK_KC * (HMG_TILE_ROWS + R) + sizeof(PackCol) * PK_NS * PK_KC +
-           sizeof(PairDesc) * PK_W + sizeof(int) * (PK_W + 1);
-}
-
-template <int R>
-__global__ void __launch_bounds__(256) k_tile_multi_pack(const PairDesc* __restrict__ desc,
-                                                         const int* tile_pair_start, const int* tile_r0,
-                                                         const int* tile_s, const int* perm1,
-                                                         const float* __restrict__ xm, const float* __restrict__ tm,
-                                                         const char* tbase, int nrhs, double* Y, int ldy)
-{
-    constexpr int KC = PK_KC, NS = PK_NS, W = PK_W, CG = R / 4, TR = R / 8;
-    extern __shared__ __align__(16) float pk_smem[];
-    float (*Us)[KC][HMG_TILE_ROWS] = reinterpret_cast<float (*)[KC][HMG_TILE_ROWS]>(pk_smem);
-    float (*Ts)[KC][R] = reinterpret_cast<float (*)[KC][R]>(pk_smem + NS * KC * HMG_TILE_ROWS);
-    PackCol (*meta)[KC] = reinterpret_cast<PackCol (*)[KC]>(pk_smem + NS * KC * (HMG_TILE_ROWS + R));
-    PairDesc* wdesc = reinterpret_cast<PairDesc*>(meta + NS);
-    int* pref = reinterpret_cast<int*>(wdesc + W);
-
-    const int t = blockIdx.x, tid = threadIdx.x;
-    const int cg = tid % CG, rg = tid / CG;
-    const int s = tile_s[t], sp = (s + 3) & ~3, tr0 = tile_r0[t];
-    const int pend = tile_pair_start[t + 1];
-    const int sp4 = sp >> 2;
-
-    int wnext = tile_pair_start[t];  // first pair of the next window
-    int wn = 0, wtotal = 0, pc = 0;  // pairs and columns of the current window, producer cursor
-    auto more = [&]() { return pc < wtotal || wnext < pend; };
-    // fill stage buffer b with the next (up to) KC columns of the stream
-    auto issue = [&](int b) {
-        if (pc >= wtotal) {  // next window of descriptors and their column prefix sums
-            const int nwin = min(W, pend - wnext);
-            if (tid < nwin) wdesc[tid] = desc[wnext + tid];
-            __syncthreads();
-            if (tid == 0) {
-                int acc = 0;
-                for (int j = 0; j < nwin; j++) {
-                    pref[j] = acc;
-                    acc += wdesc[j].ncol;
-                }
-                pref[nwin] = acc;
-            }
-            __syncthreads();
-            wtotal = pref[nwin];
-            wn = nwin;
-            wnext += nwin;
-            pc = 0;
-            // a window whose pairs are all empty contributes no column
-        }
-        if (tid < KC) {
-            const int col = pc + tid;
-            PackCol m{nullptr, nullptr, 0, 0};
-            if (col < wtotal) {
-                int lo = 0, hi = wn;  // pref[lo] <= col < pref[hi]: ends at the pair holding col
-                while (hi - lo > 1) {
-                    const int mid = (lo + hi) >> 1;
-                    if (pref[mid] <= col) lo = mid; else hi = mid;
-                }
-                const PairDesc& d = wdesc[lo];
-                const int k = col - pref[lo];
-                m.u = static_cast<const float*>(d.data) + (size_t)k * sp;
-                m.t = d.kind == PAIR_STORED
-                          ? xm + (size_t)(d.c0 + k) * R
-                          : tm + (size_t)((static_cast<const char*>(d.w) - tbase) / 4 + k) * R;
-                m.flush = k == d.ncol - 1;
-            }
-            meta[b][tid] = m;
-        }
-        __syncthreads();
-        for (int idx = tid; idx < KC * sp4; idx += 256) {
-            const int kk = idx / sp4, r4 = idx - kk * sp4;
-            const float* u = meta[b][kk].u;
-            cp_async16(&Us[b][kk][r4 * 4], u ? u + r4 * 4 : xm, u != nullptr);
-        }
-        for (int idx = tid; idx < KC * (R / 4); idx += 256) {
-            const int kk = idx / (R / 4), c4 = idx - kk * (R / 4);
-            const float* tp = meta[b][kk].t;
-            cp_async16(&Ts[b][kk][c4 * 4], tp ? tp + c4 * 4 : xm, tp != nullptr);
-        }
-        pc += KC;
-        if (pc > wtotal) pc = wtotal;
-    };
-
-    double acc64[TR][4];
-    float acc[TR][4];
-#pragma unroll
-    for (int i = 0; i < TR; i++)
-#pragma unroll
-        for (int c = 0; c < 4; c++) acc64[i][c] = 0.0, acc[i][c] = 0.0f;
-
-    int issued = 0;
-    for (int st = 0; st < NS - 1; st++) {
-        if (more()) issue(issued++ % NS);
-        asm volatile("cp.async.commit_group;" ::: "memory");
-    }
-    for (int done = 0; done < issued; done++) {
-        if (more()) issue(issued++ % NS);
-        asm volatile("cp.async.commit_group;" ::: "memory");
-        asm volatile("cp.async.wait_group %0;" ::"n"(NS - 1) : "memory");
-        __syncthreads();
-        const int b = done % NS;
-        for (int k = 0; k < KC; k++) {
-            if (meta[b][k].u == nullptr) break;
-            float u[TR];
-            if constexpr (TR == 4) {
-                const float4 v = *reinterpret_cast<const float4*>(&Us[b][k][rg * 4]);
-                u[0] = v.x; u[1] = v.y; u[2] = v.z; u[3] = v.w;
-            } else if constexpr (TR == 2) {
-                const float2 v = *reinterpret_cast<const float2*>(&Us[b][k][rg * 2]);
-                u[0] = v.x; u[1] = v.y;
-            } else {
-                u[0] = Us[b][k][rg];
-            }
-            const float4 w = *reinterpret_cast<const float4*>(&Ts[b][k][cg * 4]);
-#pragma unroll
-            for (int i = 0; i < TR; i++) {
-                acc[i][0] = fmaf(u[i], w.x, acc[i][0]);
-                acc[i][1] = fmaf(u[i], w.y, acc[i][1]);
-                acc[i][2] = fmaf(u[i], w.z, acc[i][2]);
-                acc[i][3] = fmaf(u[i], w.w, acc[i][3]);
-            }
-            if (meta[b][k].flush) {
-#pragma unroll
-                for (int i = 0; i < TR; i++)
-#pragma unroll
-                    for (int c = 0; c < 4; c++) acc64[i][c] += (double)acc[i][c], acc[i][c] = 0.0f;
-            }
-        }
-        __syncthreads();  // this buffer is refilled NS - 1 stages on
-    }
-    asm volatile("cp.async.wait_group 0;" ::: "memory");
-#pragma unroll
-    for (int i = 0; i < TR; i++) {
-        const int row = rg * TR + i;
-        if (row < s)
-#pragma unroll
-            for (int c = 0; c < 4; c++) {
-                const int j = cg * 4 + c;
-                if (j < nrhs) Y[perm1[tr0 + row] + (size_t)j * ldy] = acc64[i][c];
-            }
-    }
-}
-
 template <typename S, int R>
 static hmg_status launch_multi(hmg_matrix* h, int nrhs, const double* X, int ldx, double* Y, int ldy, S* xm, S* tm)
 {
@@ -579,13 +418,9 @@ static hmg_status launch_multi(hmg_matrix* h, int nrhs, const double* X, int ldx
     if (h->ntiles > 0) {
         const PairDesc* pd = static_cast<const PairDesc*>(h->pair_desc);
         const char* tb = static_cast<const char*>(h->tbuf);
-        if constexpr (sizeof(S) == 4 && R >= 8) {
-            HMG_CUDA_TRY(cudaFuncSetAttribute(k_tile_multi_pack<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                              (int)pack_smem<R>()));
-            k_tile_multi_pack<R><<<h->ntiles, 256, pack_smem<R>(), s>>>(pd, h->tile_pair_start, h->tile_r0,
-                                                                       h->tile_s, h->perm[0], xm, tm, tb, nrhs,
-                                                                       Y, ldy);
-        }
+        if constexpr (sizeof(S) == 4 && R >= 8)
+            k_tile_multi_smem<R><<<h->ntiles, 256, 0, s>>>(pd, h->tile_pair_start, h->tile_r0, h->tile_s,
+                                                           h->perm[0], xm, tm, tb, nrhs, Y, ldy);
         else
             k_tile_multi<S, R><<<h->ntiles, 256, 0, s>>>(pd, h->tile_pair_start, h->tile_r0, h->tile_s,
                                                          h->perm[0], xm, tm, tb, nrhs, Y, ldy);
