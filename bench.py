@@ -350,6 +350,84 @@ def run_engine(a, rank, world):
     return 0
 
 
+def run_precision(a, rank, world):
+    """The precision workload: N = 2^21 points in 2D from a 16-component Gaussian
+    mixture (seed 2), Gaussian kernel length^2 0.05, ACA eps 1e-6.  Products of 32
+    vectors per pass with FP32 factors and with mixed (FP32/FP16/FP8) factors, FP32
+    near field, FP32 products summed in FP64, and a kernel-ridge CG solve of
+    (K + 1e-3 I) x = b to relative residual 1e-8 with refinement (FP64 residuals,
+    relaxed-precision inner products).  Each result's error against FP64 direct sums
+    over 2,048 sampled rows is reported."""
+    import torch
+
+    import hmglib_b200 as hmg
+    from hmglib_b200 import synth
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    n, nrhs = a.n or (1 << 21), 32
+    p = synth.gmm_points(n, 2, 2)
+    X = torch.from_numpy(synth.rhs_vector(n, 2, nrhs)).cuda()
+    rows = torch.from_numpy(np.random.default_rng(9).choice(n, 2048, replace=False).astype(np.int32)).cuda()
+    out = {}
+    stream = torch.cuda.default_stream()
+    for name, prec in (("fp32", hmg.PREC_FP32), ("mixed", hmg.PREC_MIXED)):
+        t0 = time.perf_counter()
+        H = hmg.HMatrix(n, n, 2)
+        H.set_points(0, p)
+        H.set_points(1, p)
+        H.setup(1.5, 64, rule=hmg.ADMISSIBLE_MIN)
+        H.set_kernel(hmg.KERNEL_GAUSSIAN, 0.05, 0.0)
+        H.precompute_aca(64, 1e-6, prec)
+        H.precompute_dense(hmg.PREC_FP32)
+        torch.cuda.synchronize()
+        t_build = time.perf_counter() - t0
+        Y = torch.empty_like(X)
+        for _ in range(2):
+            H.matvec_multi(X, Y)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(a.steps):
+            H.matvec_multi(X, Y)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / a.steps
+        errs = []
+        for j in range(0, nrhs, 8):
+            yd = torch.empty(rows.shape[0], dtype=torch.float64, device="cuda")
+            H.full_matvec_rows(X[j], rows, yd)
+            torch.cuda.synchronize()
+            errs.append(float(torch.linalg.norm(Y[j][rows.long()] - yd) / torch.linalg.norm(yd)))
+        info = H.info()
+        res = {"ms_per_32_vectors": ms, "vectors_per_s": nrhs * 1000.0 / ms, "err_vs_fp64_max": max(errs),
+               "build_s": t_build, "far_gb": info["far_bytes"] / 1e9, "near_gb": info["near_bytes"] / 1e9,
+               "max_rank": info["max_rank"]}
+        if name == "fp32":
+            b = X[0].clone()
+            x = torch.zeros_like(b)
+            t0 = time.perf_counter()
+            it, rel = H.cg_solve(b, x, 1e-3, tol=1e-8, maxit=a.cg_maxit, refine=True)
+            t_cg = time.perf_counter() - t0
+            yx = torch.empty(rows.shape[0], dtype=torch.float64, device="cuda")
+            H.full_matvec_rows(x, rows, yx)
+            torch.cuda.synchronize()
+            r_ex = float(torch.linalg.norm(b[rows.long()] - (yx + 1e-3 * x[rows.long()])) / torch.linalg.norm(b[rows.long()]))
+            res["cg"] = {"iterations": it, "relres_operator": rel, "relres_exact_kernel_rows": r_ex, "seconds": t_cg,
+                         "tol": 1e-8, "maxit": a.cg_maxit}
+        out[name] = res
+        H.close()
+    line = {"metric": "32-vector H-matvecs at N=2^21 (GMM 2D, Gaussian l^2 0.05, eps 1e-6)",
+            "value": out["fp32"]["vectors_per_s"], "unit": "vector products/s", "n_gpus": 1, "steps": a.steps,
+            "warmup": 2, "ms_per_step": out["fp32"]["ms_per_32_vectors"], "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "precision_gmm2d_2m_32rhs", "n": n, "nrhs": nrhs, "aca_eps": 1e-6,
+                       "near": "fp32"},
+            "results": out}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    return 0
+
+
 def run_group(a, rank, world):
     """Many independent H-matrices (512 sets, sizes log-uniform in [2^10, 2^16], half 2D
     and half 3D, Gaussian length^2 U[0.01, 0.2], FP32 factors, ACA eps 1e-5): one
@@ -578,10 +656,11 @@ def main(argv=None):
                     help="arithmetic of the products over FP32/mixed storage")
     ap.add_argument("--variant", type=int, default=1, choices=[0, 1],
                     help="product kernels: 1 plain 16-byte loads (default), 0 bulk-copy streaming")
-    ap.add_argument("--workload", default="uniform3d", choices=["uniform3d", "group", "serve"],
+    ap.add_argument("--workload", default="uniform3d", choices=["uniform3d", "group", "serve", "precision"],
                     help="uniform3d: the N=2^20 headline; group: many small H-matrices as one; "
                          "serve: the request loop over resident H-matrices")
     ap.add_argument("--serve-requests", type=int, default=300)
+    ap.add_argument("--cg-maxit", type=int, default=600)
     ap.add_argument("--serve-baseline", type=int, default=60)
     ap.add_argument("--group-count", type=int, default=512)
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
@@ -596,6 +675,8 @@ def main(argv=None):
         return run_group(a, rank, world) if rank == 0 else 0
     if a.workload == "serve":
         return run_serve(a, rank, world) if rank == 0 else 0
+    if a.workload == "precision":
+        return run_precision(a, rank, world) if rank == 0 else 0
     if world > 1:
         import datetime
 
