@@ -67,6 +67,7 @@ _PROTOS = {
     "hmg_group_create": (C.c_int, [C.POINTER(_vp), C.POINTER(_vp), C.c_int, _vp]),
     "hmg_group_offsets": (C.c_int, [_vp, C.c_int, _vp]),
     "hmg_save": (C.c_int, [_vp, C.c_char_p]),
+    "hmg_build_bf16_factors": (C.c_int, [_vp]),
     "hmg_load": (C.c_int, [C.POINTER(_vp), C.c_char_p, _vp]),
     "hmg_full_matvec": (C.c_int, [_vp, _vp, _vp]),
     "hmg_full_matvec_rows": (C.c_int, [_vp, _vp, _vp, C.c_int, _vp]),

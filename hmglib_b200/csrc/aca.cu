@@ -491,6 +491,7 @@ k_aca_compact_mixed(BlockGeom g, AcaBatch B, TierOut T, const int* tile_r0, cons
 void free_far(hmg_matrix* h)
 {
     cudaStream_t s = h->stream;
+    free_tc(h);
     for (void* p : h->far_chunks) cudaFree(p);
     h->far_chunks.clear();
     h->far_chunk_bytes.clear();

@@ -224,6 +224,12 @@ hmg_status hmg_matvec(hmg_matrix* h, const double* x, double* y)
     return matvec_device(h, x, y);
 }
 
+hmg_status hmg_build_bf16_factors(hmg_matrix* h)
+{
+    HMG_REQUIRE(h, HMG_ERR_INVALID, "hmg_build_bf16_factors: NULL handle");
+    return build_bf16_factors(h);
+}
+
 hmg_status hmg_save(hmg_matrix* h, const char* path)
 {
     HMG_REQUIRE(h && path, HMG_ERR_INVALID, "hmg_save: NULL argument");

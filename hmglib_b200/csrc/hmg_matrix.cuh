@@ -83,6 +83,16 @@ struct hmg_matrix {
     long long far_alg_v = 0;          // bytes of the stored V terms
     int max_rank = 0;
 
+    // ---- BF16 copy of the factors for tensor-core products (tc.cu) ----------------
+    bool tc_ready = false;
+    void* tc_u = nullptr;              // U slices as BF16 operand cores, per low-rank pair
+    long long* tc_uoff = nullptr;      // per pair: byte offset into tc_u (-1: not low rank)
+    long long* tc_toff = nullptr;      // per block: first 16-term group of t_b
+    int* tc_pair_tile = nullptr;       // per pair: its tile
+    int* tc_far_blocks = nullptr;      // low-rank blocks with rank > 0
+    int tc_nfar = 0;
+    long long tc_tgroups = 0, tc_bytes = 0;
+
     // ---- matvec workspace -------------------------------------------------------
     double* xs64 = nullptr;   // Z-ordered x
     float* xs32 = nullptr;
@@ -119,6 +129,10 @@ hmg_status run_aca(hmg_matrix* h, int k, double eps, int precision);
 hmg_status fill_near(hmg_matrix* h, int precision);
 hmg_status matvec_device(hmg_matrix* h, const double* x, double* y, bool fp64_arith = false);
 hmg_status matvec_multi(hmg_matrix* h, int nrhs, const double* X, int ldx, double* Y, int ldy);
+hmg_status matvec_multi_tc(hmg_matrix* h, int nrhs, const double* X, int ldx, double* Y, int ldy);
+hmg_status build_bf16_factors(hmg_matrix* h);
+void free_tc(hmg_matrix* h);
+void launch_gather_multi32(hmg_matrix* h, const double* X, int ldx, int nrhs, float* xm);
 hmg_status direct_matvec(hmg_matrix* h, const double* x, const int* rows, int nrows,
                          double* y);
 hmg_status gaussian_rhs(hmg_matrix* h, double* b);

@@ -456,8 +456,18 @@ static hmg_status multi_typed(hmg_matrix* h, int nrhs, const double* X, int ldx,
     return st;
 }
 
+void launch_gather_multi32(hmg_matrix* h, const double* X, int ldx, int nrhs, float* xm)
+{
+    k_gather_multi<float><<<ceil_div((long long)h->n[1] * 32, 256), 256, 0, h->stream>>>(X, ldx, nrhs, h->perm[1],
+                                                                                        h->n[1], 5, xm);
+}
+
 hmg_status matvec_multi(hmg_matrix* h, int nrhs, const double* X, int ldx, double* Y, int ldy)
 {
+    // tensor cores: a BF16 copy of the FP32 factors and an FP32 stored near field
+    if (h->tc_ready && nrhs >= 2 && h->far_prec == HMG_PREC_FP32 && h->near_mode == HMG_NEAR_STORED &&
+        (h->ndense == 0 || h->near_prec == HMG_PREC_FP32) && h->arith_prec == HMG_PREC_FP32)
+        return matvec_multi_tc(h, nrhs, X, ldx, Y, ldy);
     const bool per_vector = nrhs == 1 || h->far_prec == HMG_PREC_MIXED || h->near_mode != HMG_NEAR_STORED ||
                             (h->naca > 0 && h->near_prec != h->far_prec) || h->arith_prec == HMG_PREC_FP64;
     if (per_vector) {

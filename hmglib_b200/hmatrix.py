@@ -138,6 +138,10 @@ class HMatrix:
         """0: streaming (bulk-copy) product kernels, 1: plain-load kernels."""
         self._call("hmg_set_matvec_variant", int(variant))
 
+    def build_bf16_factors(self):
+        """BF16 operand copy of the FP32 factors for tensor-core multi-vector products."""
+        self._call("hmg_build_bf16_factors")
+
     def save(self, path: str):
         """Write the H-matrix to `path` (hmg_save)."""
         self._call("hmg_save", str(path).encode())
