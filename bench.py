@@ -339,6 +339,9 @@ def run_engine(a, rank, world):
     }
     if a.nrhs > 1:
         line["multi_rhs"] = multi_rhs_timing(torch, H, x, n, a.nrhs, a.steps, stream, world, err)
+        if a.tc:
+            H.build_bf16_factors()
+            line["multi_rhs_tensor_cores"] = multi_rhs_timing(torch, H, x, n, a.nrhs, a.steps, stream, world, err)
     if rank == 0 and world == 1 and not a.no_cpu:
         kind = O.KERNEL_MATERN32
         rate, nrows, dt, thr = cpu_direct_rate(p, x, kind, O.kernel_param(kind, W["rho"]), target_s=a.cpu_seconds)
@@ -399,9 +402,30 @@ def run_precision(a, rank, world):
             torch.cuda.synchronize()
             errs.append(float(torch.linalg.norm(Y[j][rows.long()] - yd) / torch.linalg.norm(yd)))
         info = H.info()
+        if prec == hmg.PREC_FP32:
+            H.build_bf16_factors()
+            Yt = torch.empty_like(X)
+            for _ in range(2):
+                H.matvec_multi(X, Yt)
+            torch.cuda.synchronize()
+            e0.record(stream)
+            for _ in range(a.steps):
+                H.matvec_multi(X, Yt)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            ms_tc = e0.elapsed_time(e1) / a.steps
+            errs_tc = []
+            for j in range(0, nrhs, 8):
+                yd = torch.empty(rows.shape[0], dtype=torch.float64, device="cuda")
+                H.full_matvec_rows(X[j], rows, yd)
+                torch.cuda.synchronize()
+                errs_tc.append(float(torch.linalg.norm(Yt[j][rows.long()] - yd) / torch.linalg.norm(yd)))
+            tc = {"ms_per_32_vectors": ms_tc, "vectors_per_s": nrhs * 1000.0 / ms_tc, "err_vs_fp64_max": max(errs_tc)}
         res = {"ms_per_32_vectors": ms, "vectors_per_s": nrhs * 1000.0 / ms, "err_vs_fp64_max": max(errs),
                "build_s": t_build, "far_gb": info["far_bytes"] / 1e9, "near_gb": info["near_bytes"] / 1e9,
                "max_rank": info["max_rank"]}
+        if prec == hmg.PREC_FP32:
+            res["bf16_tensor_cores"] = tc
         if name == "fp32":
             b = X[0].clone()
             x = torch.zeros_like(b)
@@ -652,6 +676,8 @@ def main(argv=None):
     ap.add_argument("--near", default="stored", choices=["stored", "onthefly"])
     ap.add_argument("--nrhs", type=int, default=1,
                     help="also time products of this many vectors at once (hmg_matvec_multi)")
+    ap.add_argument("--tc", action="store_true",
+                    help="with --nrhs and --prec fp32: also time the tensor-core path (BF16 factor copy)")
     ap.add_argument("--arith", default="fp32", choices=["fp32", "fp64"],
                     help="arithmetic of the products over FP32/mixed storage")
     ap.add_argument("--variant", type=int, default=1, choices=[0, 1],
