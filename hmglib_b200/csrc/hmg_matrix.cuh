@@ -133,6 +133,7 @@ hmg_status matvec_multi_tc(hmg_matrix* h, int nrhs, const double* X, int ldx, do
 hmg_status build_bf16_factors(hmg_matrix* h);
 void free_tc(hmg_matrix* h);
 void launch_gather_multi32(hmg_matrix* h, const double* X, int ldx, int nrhs, float* xm);
+hmg_status launch_vtx_multi32(hmg_matrix* h, const float* xm, float* tm);
 hmg_status direct_matvec(hmg_matrix* h, const double* x, const int* rows, int nrows,
                          double* y);
 hmg_status gaussian_rhs(hmg_matrix* h, double* b);

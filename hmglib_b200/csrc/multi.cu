@@ -456,6 +456,20 @@ static hmg_status multi_typed(hmg_matrix* h, int nrhs, const double* X, int ldx,
     return st;
 }
 
+// t_b = V_b^T X_b for 32 vectors of an FP32-storage handle (the multi-vector K1), into
+// tm[term][32]
+hmg_status launch_vtx_multi32(hmg_matrix* h, const float* xm, float* tm)
+{
+    const int n0 = h->k1_count[0];
+    if (n0 <= 0) return HMG_OK;
+    HMG_CUDA_TRY(cudaFuncSetAttribute(k_vtx_multi_smem<32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)K1M_SMEM));
+    k_vtx_multi_smem<32><<<std::min(ceil_div(n0, 8), 148 * 3), 256, K1M_SMEM, h->stream>>>(
+        static_cast<const K1Desc*>(h->k1_units), n0, xm, tm);
+    HMG_LAUNCH_CHECK();
+    return HMG_OK;
+}
+
 void launch_gather_multi32(hmg_matrix* h, const double* X, int ldx, int nrhs, float* xm)
 {
     k_gather_multi<float><<<ceil_div((long long)h->n[1] * 32, 256), 256, 0, h->stream>>>(X, ldx, nrhs, h->perm[1],

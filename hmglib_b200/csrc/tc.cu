@@ -5,10 +5,11 @@
 // per pass with it.  Per row tile (M = 128 rows) and admissible block of rank r the
 // far-field product is D += U_slice (128 x r16, BF16) * T_b (r16 x 32, BF16) with
 // r16 = r rounded up to 16, accumulated in FP32 in tensor memory across all of the
-// tile's low-rank pairs; the dense pairs of the tile run on the CUDA cores (FP32,
-// one thread per row, 32 vectors per thread) and are added when the accumulator is
-// read back.  t_b = V_b^T X_b comes from the CUDA cores in FP32 and is rounded to
-// BF16 for the MMA (the factors' own BF16 rounding, ~4e-3 per entry, dominates the
+// tile's low-rank pairs (operands copied two stages deep with cp.async, so one pair's
+// copy overlaps the previous pair's MMAs); the dense pairs of the tile run on the CUDA
+// cores (FP32, one thread per row, 32 vectors per thread) and are added when the
+// accumulator is read back.  t_b = V_b^T X_b comes from the multi-vector K1 on the
+// CUDA cores in FP32 and is rounded to BF16 for the MMA (the factors' own BF16 rounding, ~4e-3 per entry, dominates the
 // error: products agree with FP32 factors to ~1e-3).
 //
 // Operand layout (no swizzle, K-major "core matrices" of 8 rows x 16 bytes):
@@ -60,36 +61,23 @@ __global__ void k_tc_u(const PairDesc* desc, const int* pair_tile, const long lo
 }
 
 // ---------------------------------------------------------------------------
-// t_b = V_b^T X_b on the CUDA cores (a warp per block, a lane per vector), written
-// as BF16 operand cores; terms r..r16-1 are zero
+// t_b (FP32, [term][32] from the multi-vector K1) -> BF16 operand cores; terms
+// r..r16-1 are zero
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(256) k_tc_vtx(const int* far_blocks, int nfar, const int* rank, const int* blk_c0,
-                                                const int* blk_m2, void* const* ptrV, const long long* toff,
-                                                const float* __restrict__ xm, __nv_bfloat16* tb)
+__global__ void k_tc_t(const int* far_blocks, int nfar, const int* rank, const long long* rank_off,
+                       const long long* toff, const float* __restrict__ tm, __nv_bfloat16* tb)
 {
-    const int lane = threadIdx.x & 31;
-    const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int nw = (gridDim.x * blockDim.x) >> 5;
-    for (int u = gw; u < nfar; u += nw) {
-        const int b = far_blocks[u];
-        const int r = rank[b], r16 = (r + 15) & ~15, m2 = blk_m2[b], c0 = blk_c0[b], m2p = (m2 + 3) & ~3;
-        const float* V = static_cast<const float*>(ptrV[b]);
-        __nv_bfloat16* out = tb + toff[b] * (16 * TC_N);
-        for (int l0 = 0; l0 < r16; l0 += 4) {
-            float acc[4] = {0.f, 0.f, 0.f, 0.f};
-            for (int c = 0; c < m2; c++) {
-                const float x = xm[(size_t)(c0 + c) * TC_N + lane];
-#pragma unroll
-                for (int q = 0; q < 4; q++)
-                    if (l0 + q < r) acc[q] = fmaf(V[(size_t)(l0 + q) * m2p + c], x, acc[q]);
-            }
-#pragma unroll
-            for (int q = 0; q < 4; q++) {
-                const int k = l0 + q;
-                const int idx = ((k >> 3) * 4 + (lane >> 3)) * 64 + (lane & 7) * 8 + (k & 7);
-                out[idx] = __float2bfloat16_rn(acc[q]);
-            }
-        }
+    const int u = blockIdx.x;
+    if (u >= nfar) return;
+    const int b = far_blocks[u];
+    const int r = rank[b], r16 = (r + 15) & ~15;
+    const float* src = tm + (size_t)rank_off[b] * TC_N;
+    __nv_bfloat16* out = tb + toff[b] * (16 * TC_N);
+    for (int idx = threadIdx.x; idx < r16 * TC_N; idx += blockDim.x) {
+        const int core = idx >> 6, e = idx & 63;
+        const int kc = core >> 2, nc = core & 3;
+        const int n = nc * 8 + (e >> 3), k = kc * 8 + (e & 7);
+        out[idx] = __float2bfloat16_rn(k < r ? src[(size_t)k * TC_N + n] : 0.0f);
     }
 }
 
@@ -111,13 +99,33 @@ static constexpr uint32_t TC_IDESC = (1u << 4) | (1u << 7) | (1u << 10) | ((uint
                                      ((uint32_t)(128 >> 4) << 24);
 
 struct TcSmem {
-    __nv_bfloat16 A[TC_MAXR16 / 8][16][64];    // K cores x row cores x 8 rows x 8 terms
-    __nv_bfloat16 B[TC_MAXR16 / 8][4][64];     // K cores x vector cores x 8 x 8
-    unsigned long long mbar;
+    __nv_bfloat16 A[2][TC_MAXR16 / 8][16][64];    // 2 stages x K cores x row cores x 8 rows x 8 terms
+    __nv_bfloat16 B[2][TC_MAXR16 / 8][4][64];     // 2 stages x K cores x vector cores x 8 x 8
+    unsigned long long mbar[2];
     uint32_t tmem;
     int fail;
 };
 
+__device__ __forceinline__ void tc_cp16(void* dst, const void* src)
+{
+    const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(dst));
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(src) : "memory");
+}
+
+__device__ __forceinline__ bool tc_wait(uint32_t mbar, uint32_t phase)
+{
+    uint32_t ok = 0;
+    for (long long it = 0; it < TC_SPIN && !ok; it++)
+        asm volatile(
+            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+            : "=r"(ok)
+            : "r"(mbar), "r"(phase)
+            : "memory");
+    return ok != 0;
+}
+
+// one CTA (4 warps) per row tile; the low-rank pairs' operands are copied two stages
+// deep (cp.async), so the copy of one pair overlaps the MMAs of the previous one
 __global__ void __launch_bounds__(128) k_tile_tc(const PairDesc* __restrict__ desc, const int* pair_block,
                                                  const long long* __restrict__ uoff, const char* __restrict__ tcu,
                                                  const __nv_bfloat16* __restrict__ tb, const long long* toff,
@@ -125,19 +133,19 @@ __global__ void __launch_bounds__(128) k_tile_tc(const PairDesc* __restrict__ de
                                                  const int* perm1, const float* __restrict__ xm, int nrhs, double* Y,
                                                  int ldy, int* err)
 {
-    __shared__ __align__(1024) TcSmem sm;
+    extern __shared__ __align__(1024) unsigned char tc_raw[];
+    TcSmem& sm = *reinterpret_cast<TcSmem*>(tc_raw);
     const int t = blockIdx.x, tid = threadIdx.x, warp = tid >> 5;
     const int s = tile_s[t], sp = (s + 3) & ~3, s8 = (s + 7) & ~7, tr0 = tile_r0[t];
     const int pbeg = tile_pair_start[t], pend = tile_pair_start[t + 1];
-    const uint32_t mbar = static_cast<uint32_t>(__cvta_generic_to_shared(&sm.mbar));
-    const uint32_t a_base = static_cast<uint32_t>(__cvta_generic_to_shared(&sm.A[0][0][0]));
-    const uint32_t b_base = static_cast<uint32_t>(__cvta_generic_to_shared(&sm.B[0][0][0]));
+    const uint32_t mbar0 = static_cast<uint32_t>(__cvta_generic_to_shared(&sm.mbar[0]));
+    const int mcores = s8 / 8;
 
-    // zero the operand buffers (rows past s8 stay zero), tensor memory, barrier
-    for (int i = tid; i < (int)(sizeof(sm.A) / 16); i += 128) reinterpret_cast<uint4*>(&sm.A[0][0][0])[i] = make_uint4(0, 0, 0, 0);
+    for (int i = tid; i < (int)(sizeof(sm.A) / 16); i += 128) reinterpret_cast<uint4*>(&sm.A[0][0][0][0])[i] = make_uint4(0, 0, 0, 0);
     if (tid == 0) {
         sm.fail = 0;
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(mbar));
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(mbar0));
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(mbar0 + 8));
     }
     if (warp == 0) {
         const uint32_t slot = static_cast<uint32_t>(__cvta_generic_to_shared(&sm.tmem));
@@ -170,27 +178,53 @@ __global__ void __launch_bounds__(128) k_tile_tc(const PairDesc* __restrict__ de
         }
     }
 
-    // low-rank pairs on the tensor cores, accumulated in tensor memory
-    uint32_t phase = 0;
-    bool any = false;
-    const int mcores = s8 / 8;
-    for (int p = pbeg; p < pend; p++) {
-        const PairDesc d = desc[p];
-        if (d.kind != PAIR_FAR || d.ncol == 0 || uoff[p] < 0) continue;
-        const int r16 = (d.ncol + 15) & ~15, kcores = r16 / 8;
-        // operands into shared memory
-        const uint4* su = reinterpret_cast<const uint4*>(tcu + uoff[p]);
+    // low-rank pairs on the tensor cores
+    auto next_far = [&](int p) {
+        while (p < pend) {
+            const PairDesc& d = desc[p];
+            if (d.kind == PAIR_FAR && d.ncol > 0 && uoff[p] >= 0) break;
+            p++;
+        }
+        return p;
+    };
+    auto copy = [&](int p, int b) {
+        const int r16 = (desc[p].ncol + 15) & ~15, kcores = r16 / 8;
+        const char* su = tcu + uoff[p];
         for (int i = tid; i < kcores * mcores * 8; i += 128) {
             const int core = i >> 3, part = i & 7;
             const int kc = core / mcores, mc = core - kc * mcores;
-            reinterpret_cast<uint4*>(&sm.A[kc][mc][0])[part] = su[i];
+            tc_cp16(reinterpret_cast<uint4*>(&sm.A[b][kc][mc][0]) + part, su + (size_t)i * 16);
         }
-        const uint4* st = reinterpret_cast<const uint4*>(tb + toff[pair_block[p]] * (16 * TC_N));
-        for (int i = tid; i < kcores * 4 * 8; i += 128) reinterpret_cast<uint4*>(&sm.B[0][0][0])[i] = st[i];
+        const char* st = reinterpret_cast<const char*>(tb + toff[pair_block[p]] * (16 * TC_N));
+        for (int i = tid; i < kcores * 4 * 8; i += 128)
+            tc_cp16(reinterpret_cast<uint4*>(&sm.B[b][0][0][0]) + i, st + (size_t)i * 16);
+    };
+    uint32_t phase[2] = {0u, 0u};
+    bool busy[2] = {false, false};
+    bool any = false;
+    int cur = next_far(pbeg), b = 0;
+    if (cur < pend) copy(cur, 0);
+    asm volatile("cp.async.commit_group;" ::: "memory");
+    while (cur < pend) {
+        const int nxt = next_far(cur + 1);
+        if (nxt < pend) {
+            if (busy[b ^ 1]) {  // the MMAs that read buffer b^1 must be done before it is refilled
+                if (!tc_wait(mbar0 + 8 * (b ^ 1), phase[b ^ 1])) sm.fail = 1;
+                phase[b ^ 1] ^= 1u;
+                busy[b ^ 1] = false;
+            }
+            copy(nxt, b ^ 1);
+        }
+        asm volatile("cp.async.commit_group;" ::: "memory");
+        asm volatile("cp.async.wait_group 1;" ::: "memory");
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         __syncthreads();
+        if (sm.fail) break;
         if (tid == 0) {
             asm volatile("tcgen05.fence::after_thread_sync;");
+            const int r16 = (desc[cur].ncol + 15) & ~15;
+            const uint32_t a_base = static_cast<uint32_t>(__cvta_generic_to_shared(&sm.A[b][0][0][0]));
+            const uint32_t b_base = static_cast<uint32_t>(__cvta_generic_to_shared(&sm.B[b][0][0][0]));
             for (int q = 0; q < r16 / 16; q++) {
                 const uint64_t ad = smem_desc(a_base + q * 2 * (16 * 128), 16 * 128, 128);
                 const uint64_t bd = smem_desc(b_base + q * 2 * (4 * 128), 4 * 128, 128);
@@ -200,26 +234,22 @@ __global__ void __launch_bounds__(128) k_tile_tc(const PairDesc* __restrict__ de
                     " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, pd;\n}" ::"r"(tmem),
                     "l"(ad), "l"(bd), "r"(TC_IDESC), "r"(accumulate));
             }
-            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(mbar)
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(mbar0 + 8 * b)
                          : "memory");
         }
+        busy[b] = true;
         any = true;
-        // wait for the MMAs (they read the buffers that the next pair overwrites)
-        uint32_t ok = 0;
-        for (long long it = 0; it < TC_SPIN && !ok; it++)
-            asm volatile(
-                "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
-                : "=r"(ok)
-                : "r"(mbar), "r"(phase)
-                : "memory");
-        if (!ok) {
-            sm.fail = 1;
-            atomicExch(err, 1);
-        }
-        phase ^= 1u;
-        __syncthreads();
-        if (sm.fail) break;
+        cur = nxt;
+        b ^= 1;
     }
+    asm volatile("cp.async.wait_group 0;" ::: "memory");
+    for (int q = 0; q < 2; q++)
+        if (busy[q]) {
+            if (!tc_wait(mbar0 + 8 * q, phase[q])) sm.fail = 1;
+            busy[q] = false;
+        }
+    if (sm.fail && tid == 0) atomicExch(err, 1);
+    __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;");
     if (any && !sm.fail) {
         uint32_t v[32];
@@ -353,12 +383,27 @@ hmg_status matvec_multi_tc(hmg_matrix* h, int nrhs, const double* X, int ldx, do
     }
     launch_gather_multi32(h, X, ldx, nrhs, xm);
     if (h->tc_nfar > 0) {
-        k_tc_vtx<<<std::min(ceil_div(h->tc_nfar, 8), 148 * 8), 256, 0, s>>>(
-            h->tc_far_blocks, h->tc_nfar, h->rank, h->blk_c0, h->blk_m2, h->ptrV, h->tc_toff, xm, tb);
-        HMG_LAUNCH_CHECK();
+        float* tm = nullptr;
+        if ((st = dalloc(&tm, (size_t)(h->rank_total + 1) * TC_N, s))) {
+            dfree(xm, s);
+            dfree(tb, s);
+            return st;
+        }
+        st = launch_vtx_multi32(h, xm, tm);
+        if (!st) {
+            k_tc_t<<<h->tc_nfar, 256, 0, s>>>(h->tc_far_blocks, h->tc_nfar, h->rank, h->rank_off, h->tc_toff, tm, tb);
+            if (cudaGetLastError() != cudaSuccess) st = HMG_ERR_CUDA;
+        }
+        dfree(tm, s);
+        if (st) {
+            dfree(xm, s);
+            dfree(tb, s);
+            return st;
+        }
     }
     if (h->ntiles > 0) {
-        k_tile_tc<<<h->ntiles, 128, 0, s>>>(static_cast<const PairDesc*>(h->pair_desc), h->pair_block, h->tc_uoff,
+        HMG_CUDA_TRY(cudaFuncSetAttribute(k_tile_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(TcSmem)));
+        k_tile_tc<<<h->ntiles, 128, sizeof(TcSmem), s>>>(static_cast<const PairDesc*>(h->pair_desc), h->pair_block, h->tc_uoff,
                                            static_cast<const char*>(h->tc_u), tb, h->tc_toff, h->tile_pair_start,
                                            h->tile_r0, h->tile_s, h->perm[0], xm, nrhs, Y, ldy, h->dev_err);
         HMG_LAUNCH_CHECK();
