@@ -33,8 +33,7 @@
 namespace hmg {
 
 static constexpr int TC_N = 32;           // vectors per pass (MMA N)
-static constexpr int TC_MAXR16 = 96;      // largest rank accepted (rounded to 16)
-static constexpr int TC_KSTAGE = 128;     // terms per operand stage: several pairs share one
+static constexpr int TC_MAXR16 = 96;      // largest rank (rounded to 16) with room in shared memory
 static constexpr long long TC_SPIN = 1ll << 26;
 
 // ---------------------------------------------------------------------------
@@ -100,8 +99,8 @@ static constexpr uint32_t TC_IDESC = (1u << 4) | (1u << 7) | (1u << 10) | ((uint
                                      ((uint32_t)(128 >> 4) << 24);
 
 struct TcSmem {
-    __nv_bfloat16 A[2][TC_KSTAGE / 8][16][64];    // 2 stages x K cores x row cores x 8 rows x 8 terms
-    __nv_bfloat16 B[2][TC_KSTAGE / 8][4][64];     // 2 stages x K cores x vector cores x 8 x 8
+    __nv_bfloat16 A[2][TC_MAXR16 / 8][16][64];    // 2 stages x K cores x row cores x 8 rows x 8 terms
+    __nv_bfloat16 B[2][TC_MAXR16 / 8][4][64];     // 2 stages x K cores x vector cores x 8 x 8
     unsigned long long mbar[2];
     uint32_t tmem;
     int fail;
@@ -188,50 +187,33 @@ __global__ void __launch_bounds__(128) k_tile_tc(const PairDesc* __restrict__ de
         }
         return p;
     };
-    // a stage packs consecutive low-rank pairs along K (their products add up in D)
-    auto copy_pair = [&](int p, int b, int kc0) {
+    auto copy = [&](int p, int b) {
         const int r16 = (desc[p].ncol + 15) & ~15, kcores = r16 / 8;
         const char* su = tcu + uoff[p];
         for (int i = tid; i < kcores * mcores * 8; i += 128) {
             const int core = i >> 3, part = i & 7;
             const int kc = core / mcores, mc = core - kc * mcores;
-            tc_cp16(reinterpret_cast<uint4*>(&sm.A[b][kc0 + kc][mc][0]) + part, su + (size_t)i * 16);
+            tc_cp16(reinterpret_cast<uint4*>(&sm.A[b][kc][mc][0]) + part, su + (size_t)i * 16);
         }
         const char* st = reinterpret_cast<const char*>(tb + toff[pair_block[p]] * (16 * TC_N));
         for (int i = tid; i < kcores * 4 * 8; i += 128)
-            tc_cp16(reinterpret_cast<uint4*>(&sm.B[b][kc0][0][0]) + i, st + (size_t)i * 16);
-    };
-    // fill stage b from pair p on; returns the first pair of the next stage, sets K
-    auto fill = [&](int p, int b, int& kk) {
-        kk = 0;
-        while (p < pend) {
-            const int r16 = (desc[p].ncol + 15) & ~15;
-            if (kk + r16 > TC_KSTAGE) break;
-            copy_pair(p, b, kk / 8);
-            kk += r16;
-            p = next_far(p + 1);
-        }
-        return p;
+            tc_cp16(reinterpret_cast<uint4*>(&sm.B[b][0][0][0]) + i, st + (size_t)i * 16);
     };
     uint32_t phase[2] = {0u, 0u};
     bool busy[2] = {false, false};
     bool any = false;
-    int kst[2] = {0, 0};
-    int b = 0;
-    int nxt = next_far(pbeg);
-    if (nxt < pend) nxt = fill(nxt, 0, kst[0]);
-    bool have = kst[0] > 0;
+    int cur = next_far(pbeg), b = 0;
+    if (cur < pend) copy(cur, 0);
     asm volatile("cp.async.commit_group;" ::: "memory");
-    while (have) {
-        bool have_next = false;
+    while (cur < pend) {
+        const int nxt = next_far(cur + 1);
         if (nxt < pend) {
             if (busy[b ^ 1]) {  // the MMAs that read buffer b^1 must be done before it is refilled
                 if (!tc_wait(mbar0 + 8 * (b ^ 1), phase[b ^ 1])) sm.fail = 1;
                 phase[b ^ 1] ^= 1u;
                 busy[b ^ 1] = false;
             }
-            nxt = fill(nxt, b ^ 1, kst[b ^ 1]);
-            have_next = kst[b ^ 1] > 0;
+            copy(nxt, b ^ 1);
         }
         asm volatile("cp.async.commit_group;" ::: "memory");
         asm volatile("cp.async.wait_group 1;" ::: "memory");
@@ -240,9 +222,10 @@ __global__ void __launch_bounds__(128) k_tile_tc(const PairDesc* __restrict__ de
         if (sm.fail) break;
         if (tid == 0) {
             asm volatile("tcgen05.fence::after_thread_sync;");
+            const int r16 = (desc[cur].ncol + 15) & ~15;
             const uint32_t a_base = static_cast<uint32_t>(__cvta_generic_to_shared(&sm.A[b][0][0][0]));
             const uint32_t b_base = static_cast<uint32_t>(__cvta_generic_to_shared(&sm.B[b][0][0][0]));
-            for (int q = 0; q < kst[b] / 16; q++) {
+            for (int q = 0; q < r16 / 16; q++) {
                 const uint64_t ad = smem_desc(a_base + q * 2 * (16 * 128), 16 * 128, 128);
                 const uint64_t bd = smem_desc(b_base + q * 2 * (4 * 128), 4 * 128, 128);
                 const uint32_t accumulate = (any || q > 0) ? 1u : 0u;
@@ -256,7 +239,7 @@ __global__ void __launch_bounds__(128) k_tile_tc(const PairDesc* __restrict__ de
         }
         busy[b] = true;
         any = true;
-        have = have_next;
+        cur = nxt;
         b ^= 1;
     }
     asm volatile("cp.async.wait_group 0;" ::: "memory");
