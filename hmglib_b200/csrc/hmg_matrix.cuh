@@ -134,6 +134,7 @@ hmg_status build_bf16_factors(hmg_matrix* h);
 void free_tc(hmg_matrix* h);
 void launch_gather_multi32(hmg_matrix* h, const double* X, int ldx, int nrhs, float* xm);
 hmg_status launch_vtx_multi32(hmg_matrix* h, const float* xm, float* tm);
+hmg_status launch_tile_multi32_dense(hmg_matrix* h, const float* xm, int nrhs, double* Y, int ldy);
 hmg_status direct_matvec(hmg_matrix* h, const double* x, const int* rows, int nrows,
                          double* y);
 hmg_status gaussian_rhs(hmg_matrix* h, double* b);

@@ -284,7 +284,8 @@ __global__ void __launch_bounds__(256) k_tile_multi_smem(const PairDesc* __restr
                                                          const int* tile_pair_start, const int* tile_r0,
                                                          const int* tile_s, const int* perm1,
                                                          const float* __restrict__ xm, const float* __restrict__ tm,
-                                                         const char* tbase, int nrhs, double* Y, int ldy)
+                                                         const char* tbase, int nrhs, double* Y, int ldy,
+                                                         int only_kind)
 {
     constexpr int KC = 16, NS = 4, CG = R / 4, TR = R / 8;  // NS stages in flight
     __shared__ __align__(16) float Us[NS][KC][HMG_TILE_ROWS];
@@ -313,17 +314,19 @@ __global__ void __launch_bounds__(256) k_tile_multi_smem(const PairDesc* __restr
             cp_async16(&Ts[b][kk][c4 * 4], v ? src + (size_t)(k0 + kk) * R + c4 * 4 : src, v);
         }
     };
-    // the flattened sequence of (pair, column chunk) stages, skipping empty pairs
+    // the flattened sequence of (pair, column chunk) stages, skipping empty pairs and
+    // (only_kind >= 0) pairs of another kind
+    auto skip = [&](int q) { return desc[q].ncol == 0 || (only_kind >= 0 && desc[q].kind != only_kind); };
     auto advance = [&](int& q, int& kq) {
         kq += KC;
         if (kq >= desc[q].ncol) {
             q++;
             kq = 0;
-            while (q < pend && desc[q].ncol == 0) q++;
+            while (q < pend && skip(q)) q++;
         }
     };
     int p = pbeg, k0 = 0;
-    while (p < pend && desc[p].ncol == 0) p++;
+    while (p < pend && skip(p)) p++;
     int pp = p, kp = 0;  // producer cursor, NS - 1 stages ahead
     for (int st = 0; st < NS - 1; st++) {
         if (pp < pend) {
@@ -420,7 +423,7 @@ static hmg_status launch_multi(hmg_matrix* h, int nrhs, const double* X, int ldx
         const char* tb = static_cast<const char*>(h->tbuf);
         if constexpr (sizeof(S) == 4 && R >= 8)
             k_tile_multi_smem<R><<<h->ntiles, 256, 0, s>>>(pd, h->tile_pair_start, h->tile_r0, h->tile_s,
-                                                           h->perm[0], xm, tm, tb, nrhs, Y, ldy);
+                                                           h->perm[0], xm, tm, tb, nrhs, Y, ldy, -1);
         else
             k_tile_multi<S, R><<<h->ntiles, 256, 0, s>>>(pd, h->tile_pair_start, h->tile_r0, h->tile_s,
                                                          h->perm[0], xm, tm, tb, nrhs, Y, ldy);
@@ -466,6 +469,17 @@ hmg_status launch_vtx_multi32(hmg_matrix* h, const float* xm, float* tm)
                                       (int)K1M_SMEM));
     k_vtx_multi_smem<32><<<std::min(ceil_div(n0, 8), 148 * 3), 256, K1M_SMEM, h->stream>>>(
         static_cast<const K1Desc*>(h->k1_units), n0, xm, tm);
+    HMG_LAUNCH_CHECK();
+    return HMG_OK;
+}
+
+// Y = the dense (near-field) part of H X for 32 vectors (FP32 stored near field)
+hmg_status launch_tile_multi32_dense(hmg_matrix* h, const float* xm, int nrhs, double* Y, int ldy)
+{
+    if (h->ntiles <= 0) return HMG_OK;
+    k_tile_multi_smem<32><<<h->ntiles, 256, 0, h->stream>>>(
+        static_cast<const PairDesc*>(h->pair_desc), h->tile_pair_start, h->tile_r0, h->tile_s, h->perm[0], xm,
+        nullptr, static_cast<const char*>(h->tbuf), nrhs, Y, ldy, PAIR_STORED);
     HMG_LAUNCH_CHECK();
     return HMG_OK;
 }

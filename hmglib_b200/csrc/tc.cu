@@ -6,9 +6,8 @@
 // far-field product is D += U_slice (128 x r16, BF16) * T_b (r16 x 32, BF16) with
 // r16 = r rounded up to 16, accumulated in FP32 in tensor memory across all of the
 // tile's low-rank pairs (operands copied two stages deep with cp.async, so one pair's
-// copy overlaps the previous pair's MMAs); the dense pairs of the tile run on the CUDA
-// cores (FP32, one thread per row, 32 vectors per thread) and are added when the
-// accumulator is read back.  t_b = V_b^T X_b comes from the multi-vector K1 on the
+// copy overlaps the previous pair's MMAs) and added to Y, which the CUDA-core
+// multi-vector tile kernel has filled with the dense pairs' FP32 sums just before.  t_b = V_b^T X_b comes from the multi-vector K1 on the
 // CUDA cores in FP32 and is rounded to BF16 for the MMA (the factors' own BF16 rounding, ~4e-3 per entry, dominates the
 // error: products agree with FP32 factors to ~1e-3).
 //
@@ -156,27 +155,10 @@ __global__ void __launch_bounds__(128) k_tile_tc(const PairDesc* __restrict__ de
     asm volatile("tcgen05.fence::after_thread_sync;");
     const uint32_t tmem = sm.tmem;
 
-    // dense pairs on the CUDA cores: thread = row, 32 vectors
+    // the dense pairs ran before this kernel (CUDA cores, FP32); Y holds their sums
     float acc[TC_N];
 #pragma unroll
     for (int j = 0; j < TC_N; j++) acc[j] = 0.0f;
-    for (int p = pbeg; p < pend; p++) {
-        const PairDesc d = desc[p];
-        if (d.kind != PAIR_STORED || tid >= s) continue;
-        const float* a = static_cast<const float*>(d.data) + tid;
-        for (int k = 0; k < d.ncol; k++) {
-            const float av = a[(size_t)k * sp];
-            const float4* xr = reinterpret_cast<const float4*>(xm + (size_t)(d.c0 + k) * TC_N);
-#pragma unroll
-            for (int q = 0; q < TC_N / 4; q++) {
-                const float4 xv = xr[q];
-                acc[4 * q + 0] = fmaf(av, xv.x, acc[4 * q + 0]);
-                acc[4 * q + 1] = fmaf(av, xv.y, acc[4 * q + 1]);
-                acc[4 * q + 2] = fmaf(av, xv.z, acc[4 * q + 2]);
-                acc[4 * q + 3] = fmaf(av, xv.w, acc[4 * q + 3]);
-            }
-        }
-    }
 
     // low-rank pairs on the tensor cores
     auto next_far = [&](int p) {
@@ -267,11 +249,11 @@ __global__ void __launch_bounds__(128) k_tile_tc(const PairDesc* __restrict__ de
 #pragma unroll
         for (int j = 0; j < TC_N; j++) acc[j] += __uint_as_float(v[j]);
     }
-    if (tid < s && !sm.fail) {
+    if (any && tid < s && !sm.fail) {
         const size_t row = (size_t)perm1[tr0 + tid];
 #pragma unroll
         for (int j = 0; j < TC_N; j++)
-            if (j < nrhs) Y[row + (size_t)j * ldy] = (double)acc[j];
+            if (j < nrhs) Y[row + (size_t)j * ldy] += (double)acc[j];
     }
     __syncthreads();
     if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 32;" ::"r"(tmem));
@@ -401,7 +383,12 @@ hmg_status matvec_multi_tc(hmg_matrix* h, int nrhs, const double* X, int ldx, do
             return st;
         }
     }
-    if (h->ntiles > 0) {
+    if ((st = launch_tile_multi32_dense(h, xm, nrhs, Y, ldy))) {
+        dfree(xm, s);
+        dfree(tb, s);
+        return st;
+    }
+    if (h->ntiles > 0 && h->tc_nfar > 0) {
         HMG_CUDA_TRY(cudaFuncSetAttribute(k_tile_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(TcSmem)));
         k_tile_tc<<<h->ntiles, 128, sizeof(TcSmem), s>>>(static_cast<const PairDesc*>(h->pair_desc), h->pair_block, h->tc_uoff,
                                            static_cast<const char*>(h->tc_u), tb, h->tc_toff, h->tile_pair_start,
