@@ -18,6 +18,9 @@
 // Deterministic (fixed summation orders, no atomics).  FP32 and FP64 storage with a
 // stored near field; mixed storage and on-the-fly near fields use one product per
 // vector.
+#include <cuda_fp16.h>
+#include <cuda_fp8.h>
+
 #include <algorithm>
 
 #include "hmg_matrix.cuh"
@@ -117,12 +120,40 @@ static constexpr size_t K1M_SMEM = 8 * K1M_STAGES * 4 * 128 * sizeof(float);  //
 // computes 4 rows x 4 vectors over every CGN-th group of 4 columns of a stage (V
 // from shared memory, X from global/L1), and the CGN column groups are summed by a
 // fixed xor butterfly at the end of each 4-row block.
-template <int R>
+// 16 bytes of a K1 piece row of tier TIER as [column q][term t] floats: 4 columns of
+// TG = 1 (FP32), 2 (FP16 pairs) or 4 (FP8 quads) terms
+template <int TIER>
+__device__ __forceinline__ void tier_chunk(const uint4& u, float* o)
+{
+    if constexpr (TIER == 0) {
+        o[0] = __uint_as_float(u.x); o[1] = __uint_as_float(u.y);
+        o[2] = __uint_as_float(u.z); o[3] = __uint_as_float(u.w);
+    } else {
+        const unsigned w[4] = {u.x, u.y, u.z, u.w};
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            if constexpr (TIER == 1) {
+                const float2 f = __half22float2(*reinterpret_cast<const __half2*>(&w[q]));
+                o[2 * q] = f.x;
+                o[2 * q + 1] = f.y;
+            } else {
+                __half2_raw lo = __nv_cvt_fp8x2_to_halfraw2((__nv_fp8x2_storage_t)(w[q] & 0xffffu), __NV_E4M3);
+                __half2_raw hi = __nv_cvt_fp8x2_to_halfraw2((__nv_fp8x2_storage_t)(w[q] >> 16), __NV_E4M3);
+                const float2 a = __half22float2(*reinterpret_cast<const __half2*>(&lo));
+                const float2 c = __half22float2(*reinterpret_cast<const __half2*>(&hi));
+                o[4 * q] = a.x; o[4 * q + 1] = a.y; o[4 * q + 2] = c.x; o[4 * q + 3] = c.y;
+            }
+        }
+    }
+}
+
+template <int R, int TIER>
 __global__ void __launch_bounds__(256) k_vtx_multi_smem(const K1Desc* __restrict__ descs, int n,
                                                         const float* __restrict__ xm, float* __restrict__ tm)
 {
     constexpr int RG = R / 4, CGN = 32 / RG, SC = 128;  // vector groups, column groups, stage columns
     constexpr int NS = K1M_STAGES;                      // stages in flight per warp
+    constexpr int TG = TIER == 0 ? 1 : (TIER == 1 ? 2 : 4), NR = 4 / TG;  // terms per row, rows per block
     extern __shared__ __align__(16) float k1m_smem[];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     float (*Vs)[4][SC] = reinterpret_cast<float (*)[4][SC]>(k1m_smem + (size_t)warp * NS * 4 * SC);
@@ -132,23 +163,23 @@ __global__ void __launch_bounds__(256) k_vtx_multi_smem(const K1Desc* __restrict
     for (int u = gw; u < n; u += nw) {
         const K1Desc d = descs[u];
         const int cpr = d.row_bytes >> 4;  // 16-byte chunks per row
-        const int nst = (cpr + SC / 4 - 1) / (SC / 4);  // stages per 4-row block
+        const int nst = (cpr + SC / 4 - 1) / (SC / 4);  // stages per block of 4 terms
         const char* vb = static_cast<const char*>(d.v);
-        const int total = ((d.nrows + 3) >> 2) * nst;
+        const int total = ((d.nrows + NR - 1) / NR) * nst;
         auto issue = [&](int it) {
             if (it < total) {
                 const int blk = it / nst, st = it - blk * nst;
                 const int ch = st * (SC / 4) + lane;  // this lane's chunk of each row
 #pragma unroll
-                for (int k = 0; k < 4; k++) {
-                    const int row = blk * 4 + k;
+                for (int k = 0; k < NR; k++) {
+                    const int row = blk * NR + k;
                     const bool v = row < d.nrows && ch < cpr;
                     cp_async16(&Vs[it % NS][k][lane * 4], v ? vb + (size_t)row * d.row_bytes + (size_t)ch * 16 : vb, v);
                 }
             }
             asm volatile("cp.async.commit_group;" ::: "memory");
         };
-        float acc[4][4];
+        float acc[4][4];  // [term of the block][vector]
 #pragma unroll
         for (int a = 0; a < 4; a++)
 #pragma unroll
@@ -172,21 +203,25 @@ __global__ void __launch_bounds__(256) k_vtx_multi_smem(const K1Desc* __restrict
                     xv[q] = col + q < d.m2 ? *reinterpret_cast<const float4*>(xm + (size_t)(d.c0 + col + q) * R + rg * 4)
                                            : make_float4(0.f, 0.f, 0.f, 0.f);
 #pragma unroll
-                for (int k = 0; k < 4; k++) {
-                    const float4 v = *reinterpret_cast<const float4*>(&Vs[b][k][c4]);
-                    const float vv[4] = {v.x, v.y, v.z, v.w};
+                for (int k = 0; k < NR; k++) {
+                    float f[4 * TG];
+                    tier_chunk<TIER>(*reinterpret_cast<const uint4*>(&Vs[b][k][c4]), f);
 #pragma unroll
-                    for (int q = 0; q < 4; q++) {
-                        acc[k][0] = fmaf(vv[q], xv[q].x, acc[k][0]);
-                        acc[k][1] = fmaf(vv[q], xv[q].y, acc[k][1]);
-                        acc[k][2] = fmaf(vv[q], xv[q].z, acc[k][2]);
-                        acc[k][3] = fmaf(vv[q], xv[q].w, acc[k][3]);
-                    }
+                    for (int q = 0; q < 4; q++)
+#pragma unroll
+                        for (int tt = 0; tt < TG; tt++) {
+                            const float vv = f[q * TG + tt];
+                            float* ac = acc[k * TG + tt];
+                            ac[0] = fmaf(vv, xv[q].x, ac[0]);
+                            ac[1] = fmaf(vv, xv[q].y, ac[1]);
+                            ac[2] = fmaf(vv, xv[q].z, ac[2]);
+                            ac[3] = fmaf(vv, xv[q].w, ac[3]);
+                        }
                 }
             }
             __syncwarp();  // this buffer is refilled NS - 1 stages on
             if (st == nst - 1) {
-                // the block's 4 rows are complete: sum the column groups, write, reset
+                // the block's 4 terms are complete: sum the column groups, scale, write, reset
 #pragma unroll
                 for (int o = RG; o < 32; o <<= 1)
 #pragma unroll
@@ -196,10 +231,12 @@ __global__ void __launch_bounds__(256) k_vtx_multi_smem(const K1Desc* __restrict
                 if (cg == 0)
 #pragma unroll
                     for (int k = 0; k < 4; k++) {
-                        const int row = blk * 4 + k;
-                        if (row < d.nrows)
-                            *reinterpret_cast<float4*>(tm + (size_t)(d.tout + row) * R + rg * 4) =
-                                make_float4(acc[k][0], acc[k][1], acc[k][2], acc[k][3]);
+                        const int term = blk * 4 + k;
+                        if (term < d.nrows * TG) {
+                            const float sc = TIER == 0 ? 1.0f : d.scal[term];
+                            *reinterpret_cast<float4*>(tm + (size_t)(d.tout + term) * R + rg * 4) =
+                                make_float4(acc[k][0] * sc, acc[k][1] * sc, acc[k][2] * sc, acc[k][3] * sc);
+                        }
                     }
 #pragma unroll
                 for (int k = 0; k < 4; k++)
@@ -398,6 +435,241 @@ __global__ void __launch_bounds__(256) k_tile_multi_smem(const PairDesc* __restr
     }
 }
 
+// Mixed storage (FP32 / FP16-pair / FP8-quad chunk columns), R = 8, 16 or 32
+// vectors: the tile kernel above with each chunk column decoded at use.  A chunk
+// column holds TG = 1, 2 or 4 terms for 4 rows per 16 bytes; the stage carries the TG
+// vector rows (t_b, already scaled) that multiply it.
+template <int R>
+constexpr size_t mixed_tile_smem()
+{
+    return (size_t)4 * 16 * (HMG_TILE_ROWS + 4 * R) * sizeof(float) + 4 * 16 * sizeof(int);
+}
+
+template <int R>
+__global__ void __launch_bounds__(256) k_tile_multi_mixed(const PairDesc* __restrict__ desc,
+                                                          const int* tile_pair_start, const int* tile_r0,
+                                                          const int* tile_s, const int* perm1,
+                                                          const float* __restrict__ xm, const float* __restrict__ tm,
+                                                          const char* tbase, int nrhs, double* Y, int ldy)
+{
+    constexpr int KC = 16, NS = 4, CG = R / 4, TR = R / 8;
+    extern __shared__ __align__(16) float mx_smem[];
+    float (*Us)[KC][HMG_TILE_ROWS] = reinterpret_cast<float (*)[KC][HMG_TILE_ROWS]>(mx_smem);
+    float (*Ts)[KC][4][R] = reinterpret_cast<float (*)[KC][4][R]>(mx_smem + NS * KC * HMG_TILE_ROWS);
+    int (*Tg)[KC] = reinterpret_cast<int (*)[KC]>(mx_smem + NS * KC * (HMG_TILE_ROWS + 4 * R));
+    const int t = blockIdx.x, tid = threadIdx.x;
+    const int cg = tid % CG, rg = tid / CG;
+    const int s = tile_s[t], sp = (s + 3) & ~3, tr0 = tile_r0[t];
+    const int pbeg = tile_pair_start[t], pend = tile_pair_start[t + 1];
+    const int sp4 = sp >> 2;
+    // chunk columns of a pair
+    auto cols = [&](const PairDesc& d) {
+        return d.kind == PAIR_FAR_MIXED ? d.ncol + (d.c0 >> 1) + (d.pad >> 2) : d.ncol;
+    };
+    auto issue = [&](int b, int p, int k0) {
+        const PairDesc d = desc[p];
+        const int nc = cols(d);
+        const char* data = static_cast<const char*>(d.data);
+        for (int idx = tid; idx < KC * sp4; idx += 256) {
+            const int kk = idx / sp4, r4 = idx - kk * sp4;
+            const bool v = k0 + kk < nc;
+            cp_async16(&Us[b][kk][r4 * 4], v ? data + ((size_t)(k0 + kk) * sp + r4 * 4) * 4 : data, v);
+        }
+        const bool far = d.kind == PAIR_FAR_MIXED;
+        const float* tb = far ? tm + (size_t)((static_cast<const char*>(d.w) - tbase) / 4) * R : xm + (size_t)d.c0 * R;
+        const int n32 = d.ncol, n16 = d.c0 >> 1;
+        for (int idx = tid; idx < KC * 4 * (R / 4); idx += 256) {
+            const int kk = idx / (4 * (R / 4)), rem = idx - kk * (4 * (R / 4));
+            const int tt = rem / (R / 4), c4 = rem - tt * (R / 4);
+            const int k = k0 + kk;
+            int tg = 1, term = k;
+            if (far) {
+                if (k >= n32 + n16) tg = 4, term = n32 + 2 * n16 + 4 * (k - n32 - n16);
+                else if (k >= n32) tg = 2, term = n32 + 2 * (k - n32);
+            }
+            const bool v = k < nc && tt < tg;
+            cp_async16(&Ts[b][kk][tt][c4 * 4], v ? tb + (size_t)(term + tt) * R + c4 * 4 : tb, v);
+            if (tt == 0 && c4 == 0) Tg[b][kk] = tg;
+        }
+    };
+    auto skip = [&](int q) { return cols(desc[q]) == 0; };
+    auto advance = [&](int& q, int& kq) {
+        kq += KC;
+        if (kq >= cols(desc[q])) {
+            q++;
+            kq = 0;
+            while (q < pend && skip(q)) q++;
+        }
+    };
+    int p = pbeg, k0 = 0;
+    while (p < pend && skip(p)) p++;
+    int pp = p, kp = 0;
+    for (int st = 0; st < NS - 1; st++) {
+        if (pp < pend) {
+            issue(st, pp, kp);
+            advance(pp, kp);
+        }
+        asm volatile("cp.async.commit_group;" ::: "memory");
+    }
+    double acc64[TR][4];
+    float acc[TR][4];
+#pragma unroll
+    for (int i = 0; i < TR; i++)
+#pragma unroll
+        for (int c = 0; c < 4; c++) acc64[i][c] = 0.0, acc[i][c] = 0.0f;
+    for (int it = 0; p < pend; it++) {
+        if (pp < pend) {
+            issue((it + NS - 1) % NS, pp, kp);
+            advance(pp, kp);
+        }
+        asm volatile("cp.async.commit_group;" ::: "memory");
+        asm volatile("cp.async.wait_group %0;" ::"n"(NS - 1) : "memory");
+        __syncthreads();
+        const int buf = it % NS;
+        const int kmax = min(KC, cols(desc[p]) - k0);
+        for (int k = 0; k < kmax; k++) {
+            unsigned w[TR];
+            if constexpr (TR == 4) {
+                const uint4 v = *reinterpret_cast<const uint4*>(&Us[buf][k][rg * 4]);
+                w[0] = v.x; w[1] = v.y; w[2] = v.z; w[3] = v.w;
+            } else if constexpr (TR == 2) {
+                const uint2 v = *reinterpret_cast<const uint2*>(&Us[buf][k][rg * 2]);
+                w[0] = v.x; w[1] = v.y;
+            } else {
+                w[0] = __float_as_uint(Us[buf][k][rg]);
+            }
+            const int tg = Tg[buf][k];
+            if (tg == 1) {
+                const float4 x = *reinterpret_cast<const float4*>(&Ts[buf][k][0][cg * 4]);
+#pragma unroll
+                for (int i = 0; i < TR; i++) {
+                    const float u = __uint_as_float(w[i]);
+                    acc[i][0] = fmaf(u, x.x, acc[i][0]);
+                    acc[i][1] = fmaf(u, x.y, acc[i][1]);
+                    acc[i][2] = fmaf(u, x.z, acc[i][2]);
+                    acc[i][3] = fmaf(u, x.w, acc[i][3]);
+                }
+            } else if (tg == 2) {
+                const float4 x0 = *reinterpret_cast<const float4*>(&Ts[buf][k][0][cg * 4]);
+                const float4 x1 = *reinterpret_cast<const float4*>(&Ts[buf][k][1][cg * 4]);
+#pragma unroll
+                for (int i = 0; i < TR; i++) {
+                    const float2 f = __half22float2(*reinterpret_cast<const __half2*>(&w[i]));
+                    acc[i][0] = fmaf(f.y, x1.x, fmaf(f.x, x0.x, acc[i][0]));
+                    acc[i][1] = fmaf(f.y, x1.y, fmaf(f.x, x0.y, acc[i][1]));
+                    acc[i][2] = fmaf(f.y, x1.z, fmaf(f.x, x0.z, acc[i][2]));
+                    acc[i][3] = fmaf(f.y, x1.w, fmaf(f.x, x0.w, acc[i][3]));
+                }
+            } else {
+                float4 x[4];
+#pragma unroll
+                for (int tt = 0; tt < 4; tt++) x[tt] = *reinterpret_cast<const float4*>(&Ts[buf][k][tt][cg * 4]);
+#pragma unroll
+                for (int i = 0; i < TR; i++) {
+                    __half2_raw lo = __nv_cvt_fp8x2_to_halfraw2((__nv_fp8x2_storage_t)(w[i] & 0xffffu), __NV_E4M3);
+                    __half2_raw hi = __nv_cvt_fp8x2_to_halfraw2((__nv_fp8x2_storage_t)(w[i] >> 16), __NV_E4M3);
+                    const float2 a = __half22float2(*reinterpret_cast<const __half2*>(&lo));
+                    const float2 c = __half22float2(*reinterpret_cast<const __half2*>(&hi));
+                    const float f[4] = {a.x, a.y, c.x, c.y};
+#pragma unroll
+                    for (int tt = 0; tt < 4; tt++) {
+                        acc[i][0] = fmaf(f[tt], x[tt].x, acc[i][0]);
+                        acc[i][1] = fmaf(f[tt], x[tt].y, acc[i][1]);
+                        acc[i][2] = fmaf(f[tt], x[tt].z, acc[i][2]);
+                        acc[i][3] = fmaf(f[tt], x[tt].w, acc[i][3]);
+                    }
+                }
+            }
+        }
+        int pn = p, kn = k0;
+        advance(pn, kn);
+        if (pn != p) {
+#pragma unroll
+            for (int i = 0; i < TR; i++)
+#pragma unroll
+                for (int c = 0; c < 4; c++) acc64[i][c] += (double)acc[i][c], acc[i][c] = 0.0f;
+        }
+        __syncthreads();  // this buffer is refilled NS - 1 stages on
+        p = pn;
+        k0 = kn;
+    }
+    asm volatile("cp.async.wait_group 0;" ::: "memory");
+#pragma unroll
+    for (int i = 0; i < TR; i++) {
+        const int row = rg * TR + i;
+        if (row < s)
+#pragma unroll
+            for (int c = 0; c < 4; c++) {
+                const int j = cg * 4 + c;
+                if (j < nrhs) Y[perm1[tr0 + row] + (size_t)j * ldy] = acc64[i][c];
+            }
+    }
+}
+
+// mixed storage, 8, 16 or 32 vectors per pass
+template <int R>
+static hmg_status launch_multi_mixed(hmg_matrix* h, int nrhs, const double* X, int ldx, double* Y, int ldy,
+                                     float* xm, float* tm)
+{
+    cudaStream_t s = h->stream;
+    constexpr int LGR = R == 32 ? 5 : (R == 16 ? 4 : 3);
+    k_gather_multi<float><<<ceil_div((long long)h->n[1] * R, 256), 256, 0, s>>>(X, ldx, nrhs, h->perm[1], h->n[1],
+                                                                                LGR, xm);
+    HMG_LAUNCH_CHECK();
+    const K1Desc* dd = static_cast<const K1Desc*>(h->k1_units);
+    const int cnt[3] = {h->k1_count[0], h->k1_count[1], h->k1_count[2]};
+    int first = 0;
+    for (int tier = 0; tier < 3; tier++) {
+        if (cnt[tier] > 0) {
+            const int grid = std::min(ceil_div(cnt[tier], 8), 148 * 3);
+            if (tier == 0) {
+                HMG_CUDA_TRY(cudaFuncSetAttribute(k_vtx_multi_smem<R, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)K1M_SMEM));
+                k_vtx_multi_smem<R, 0><<<grid, 256, K1M_SMEM, s>>>(dd + first, cnt[tier], xm, tm);
+            } else if (tier == 1) {
+                HMG_CUDA_TRY(cudaFuncSetAttribute(k_vtx_multi_smem<R, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)K1M_SMEM));
+                k_vtx_multi_smem<R, 1><<<grid, 256, K1M_SMEM, s>>>(dd + first, cnt[tier], xm, tm);
+            } else {
+                HMG_CUDA_TRY(cudaFuncSetAttribute(k_vtx_multi_smem<R, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)K1M_SMEM));
+                k_vtx_multi_smem<R, 2><<<grid, 256, K1M_SMEM, s>>>(dd + first, cnt[tier], xm, tm);
+            }
+            HMG_LAUNCH_CHECK();
+        }
+        first += cnt[tier];
+    }
+    if (h->ntiles > 0) {
+        HMG_CUDA_TRY(cudaFuncSetAttribute(k_tile_multi_mixed<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          (int)mixed_tile_smem<R>()));
+        k_tile_multi_mixed<R><<<h->ntiles, 256, mixed_tile_smem<R>(), s>>>(
+            static_cast<const PairDesc*>(h->pair_desc), h->tile_pair_start, h->tile_r0, h->tile_s, h->perm[0], xm, tm,
+            static_cast<const char*>(h->tbuf), nrhs, Y, ldy);
+        HMG_LAUNCH_CHECK();
+    }
+    return HMG_OK;
+}
+
+static hmg_status multi_mixed(hmg_matrix* h, int nrhs, const double* X, int ldx, double* Y, int ldy)
+{
+    cudaStream_t s = h->stream;
+    hmg_status st;
+    int R = 8;
+    while (R < nrhs) R <<= 1;
+    if ((st = ensure_desc(h, 4))) return st;
+    float* xm = nullptr;
+    float* tm = nullptr;
+    if ((st = dalloc(&xm, (size_t)h->n[1] * R, s)) || (st = dalloc(&tm, (size_t)(h->rank_total + 1) * R, s))) {
+        dfree(xm, s);
+        return st;
+    }
+    switch (R) {
+    case 8: st = launch_multi_mixed<8>(h, nrhs, X, ldx, Y, ldy, xm, tm); break;
+    case 16: st = launch_multi_mixed<16>(h, nrhs, X, ldx, Y, ldy, xm, tm); break;
+    default: st = launch_multi_mixed<32>(h, nrhs, X, ldx, Y, ldy, xm, tm); break;
+    }
+    dfree(xm, s);
+    dfree(tm, s);
+    return st;
+}
+
 template <typename S, int R>
 static hmg_status launch_multi(hmg_matrix* h, int nrhs, const double* X, int ldx, double* Y, int ldy, S* xm, S* tm)
 {
@@ -410,9 +682,9 @@ static hmg_status launch_multi(hmg_matrix* h, int nrhs, const double* X, int ldx
     if (n0 > 0) {
         const K1Desc* dd = static_cast<const K1Desc*>(h->k1_units);
         if constexpr (sizeof(S) == 4 && R >= 8) {
-            HMG_CUDA_TRY(cudaFuncSetAttribute(k_vtx_multi_smem<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+            HMG_CUDA_TRY(cudaFuncSetAttribute(k_vtx_multi_smem<R, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                               (int)K1M_SMEM));
-            k_vtx_multi_smem<R><<<std::min(ceil_div(n0, 8), 148 * 3), 256, K1M_SMEM, s>>>(dd, n0, xm, tm);
+            k_vtx_multi_smem<R, 0><<<std::min(ceil_div(n0, 8), 148 * 3), 256, K1M_SMEM, s>>>(dd, n0, xm, tm);
         }
         else
             k_vtx_multi<S, R><<<std::min(ceil_div(n0, 8), 148 * 8), 256, 0, s>>>(dd, n0, xm, tm);
@@ -465,9 +737,9 @@ hmg_status launch_vtx_multi32(hmg_matrix* h, const float* xm, float* tm)
 {
     const int n0 = h->k1_count[0];
     if (n0 <= 0) return HMG_OK;
-    HMG_CUDA_TRY(cudaFuncSetAttribute(k_vtx_multi_smem<32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    HMG_CUDA_TRY(cudaFuncSetAttribute(k_vtx_multi_smem<32, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)K1M_SMEM));
-    k_vtx_multi_smem<32><<<std::min(ceil_div(n0, 8), 148 * 3), 256, K1M_SMEM, h->stream>>>(
+    k_vtx_multi_smem<32, 0><<<std::min(ceil_div(n0, 8), 148 * 3), 256, K1M_SMEM, h->stream>>>(
         static_cast<const K1Desc*>(h->k1_units), n0, xm, tm);
     HMG_LAUNCH_CHECK();
     return HMG_OK;
@@ -496,6 +768,9 @@ hmg_status matvec_multi(hmg_matrix* h, int nrhs, const double* X, int ldx, doubl
     if (h->tc_ready && nrhs >= 2 && h->far_prec == HMG_PREC_FP32 && h->near_mode == HMG_NEAR_STORED &&
         (h->ndense == 0 || h->near_prec == HMG_PREC_FP32) && h->arith_prec == HMG_PREC_FP32)
         return matvec_multi_tc(h, nrhs, X, ldx, Y, ldy);
+    if (nrhs > 1 && h->far_prec == HMG_PREC_MIXED && h->near_mode == HMG_NEAR_STORED &&
+        (h->ndense == 0 || h->near_prec == HMG_PREC_FP32) && h->arith_prec == HMG_PREC_FP32)
+        return multi_mixed(h, nrhs, X, ldx, Y, ldy);
     const bool per_vector = nrhs == 1 || h->far_prec == HMG_PREC_MIXED || h->near_mode != HMG_NEAR_STORED ||
                             (h->naca > 0 && h->near_prec != h->far_prec) || h->arith_prec == HMG_PREC_FP64;
     if (per_vector) {
