@@ -154,10 +154,21 @@ def run_reference(a, rank, world):
     return 0
 
 
+def max_over_ranks(values, world, device=None):
+    """Element-wise maximum of per-rank timings (the slowest rank sets the step time).
+    With one rank the values pass through; otherwise one all-reduce on `device`."""
+    if world <= 1:
+        return [float(v) for v in values]
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(v) for v in values], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return [float(v) for v in t.tolist()]
+
+
 def multi_rhs_timing(torch, H, x, n, nrhs, steps, stream, world, err1):
     """Products of nrhs vectors at once (hmg_matvec_multi): vector products per second,
     device-resident and end to end (pinned host X in, Y out, inside the timing)."""
-    import torch.distributed as dist
     rng = np.random.default_rng(11)
     Xh = rng.uniform(-1, 1, (nrhs, n))
     Xh[0] = x
@@ -188,10 +199,7 @@ def multi_rhs_timing(torch, H, x, n, nrhs, steps, stream, world, err1):
     e1.record(stream)
     torch.cuda.synchronize()
     ms_e2e = e0.elapsed_time(e1)
-    if world > 1:
-        t = torch.tensor([ms, ms_e2e], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms, ms_e2e = float(t[0]), float(t[1])
+    ms, ms_e2e = max_over_ranks([ms, ms_e2e], world, "cuda")
     return {"nrhs": nrhs, "ms_per_product": ms / steps, "value": world * nrhs * 1000.0 * steps / ms,
             "unit": "vector products/s", "e2e_value": world * nrhs * 1000.0 * steps / ms_e2e,
             "err_vs_fp64_col0": err1 + diff, "col0_vs_single": diff}
@@ -293,10 +301,7 @@ def run_engine(a, rank, world):
         e1.record(stream)
         torch.cuda.synchronize()
         ms_e2e = e0.elapsed_time(e1)
-    if world > 1:
-        t = torch.tensor([ms, ms_e2e], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms, ms_e2e = float(t[0]), float(t[1])
+    ms, ms_e2e = max_over_ranks([ms, ms_e2e], world, "cuda")
     ms_step = ms / a.steps
     value = world * 1000.0 / ms_step
     e2e_value = world * 1000.0 * a.steps / ms_e2e
