@@ -83,15 +83,19 @@ struct hmg_matrix {
     long long far_alg_v = 0;          // bytes of the stored V terms
     int max_rank = 0;
 
-    // ---- BF16 copy of the factors for tensor-core products (tc.cu) ----------------
+    // ---- BF16 operands for tensor-core multi-vector products (tc.cu) -------------
     bool tc_ready = false;
-    void* tc_u = nullptr;              // U slices as BF16 operand cores, per low-rank pair
-    long long* tc_uoff = nullptr;      // per pair: byte offset into tc_u (-1: not low rank)
-    long long* tc_toff = nullptr;      // per block: first 16-term group of t_b
-    int* tc_pair_tile = nullptr;       // per pair: its tile
-    int* tc_far_blocks = nullptr;      // low-rank blocks with rank > 0
-    int tc_nfar = 0;
-    long long tc_tgroups = 0, tc_bytes = 0;
+    void* tc_u = nullptr;                     // pass 2 A operands: U slices, near slices
+    void* tc_v = nullptr;                     // pass 1 A operands: V_b^T
+    void* tc_bbuf = nullptr;                  // per product: X cores, then t_b cores
+    char* tc_steps[2] = {nullptr, nullptr};   // per pass: steps, CTA by CTA
+    char* tc_jobs[2] = {nullptr, nullptr};    // per pass: jobs, CTA by CTA
+    char* tc_cta[2] = {nullptr, nullptr};     // per CTA: first job and step (int2), then the ends
+    int tc_njobs[2] = {0, 0};
+    int tc_grid = 0;
+    bool tc_all_tiles = false;                // every row tile has a pass-2 job
+    long long tc_xbytes = 0, tc_tbytes = 0;   // per product: X cores, t_b cores
+    long long tc_bytes = 0;                   // BF16 operands held
 
     // ---- matvec workspace -------------------------------------------------------
     double* xs64 = nullptr;   // Z-ordered x
@@ -132,9 +136,6 @@ hmg_status matvec_multi(hmg_matrix* h, int nrhs, const double* X, int ldx, doubl
 hmg_status matvec_multi_tc(hmg_matrix* h, int nrhs, const double* X, int ldx, double* Y, int ldy);
 hmg_status build_bf16_factors(hmg_matrix* h);
 void free_tc(hmg_matrix* h);
-void launch_gather_multi32(hmg_matrix* h, const double* X, int ldx, int nrhs, float* xm);
-hmg_status launch_vtx_multi32(hmg_matrix* h, const float* xm, float* tm);
-hmg_status launch_tile_multi32_dense(hmg_matrix* h, const float* xm, int nrhs, double* Y, int ldy);
 hmg_status direct_matvec(hmg_matrix* h, const double* x, const int* rows, int nrows,
                          double* y);
 hmg_status gaussian_rhs(hmg_matrix* h, double* b);

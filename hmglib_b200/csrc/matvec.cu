@@ -62,6 +62,7 @@ void free_near(hmg_matrix* h)
     h->near_stored = 0;
     h->desc_near_mode = -1;
     if (h->near_mode == HMG_NEAR_STORED) h->near_mode = HMG_NEAR_ONTHEFLY;
+    free_tc(h);  // its BF16 near slices are copies of this storage
 }
 
 static PointsView points_view(hmg_matrix* h)

@@ -1,87 +1,164 @@
-// tc.cu -- multi-vector products on the tensor cores (tcgen05), BF16 factors.
+// tc.cu -- multi-vector products on the tensor cores (tcgen05), BF16 operands.
 //
-// hmg_build_bf16_factors converts the FP32 low-rank factors of a handle into a BF16
-// copy laid out as tcgen05 operands; hmg_matvec_multi then multiplies 2..32 vectors
-// per pass with it.  Per row tile (M = 128 rows) and admissible block of rank r the
-// far-field product is D += U_slice (128 x r16, BF16) * T_b (r16 x 32, BF16) with
-// r16 = r rounded up to 16, accumulated in FP32 in tensor memory across all of the
-// tile's low-rank pairs (operands copied two stages deep with cp.async, so one pair's
-// copy overlaps the previous pair's MMAs) and added to Y, which the CUDA-core
-// multi-vector tile kernel has filled with the dense pairs' FP32 sums just before.  t_b = V_b^T X_b comes from the multi-vector K1 on the
-// CUDA cores in FP32 and is rounded to BF16 for the MMA (the factors' own BF16 rounding, ~4e-3 per entry, dominates the
-// error: products agree with FP32 factors to ~1e-3).
+// hmg_build_bf16_factors converts the FP32 low-rank factors and the FP32 stored near
+// field of a handle into BF16 tcgen05 operands; hmg_matvec_multi then multiplies 2..32
+// vectors per pass with them, every product on the tensor cores:
 //
-// Operand layout (no swizzle, K-major "core matrices" of 8 rows x 16 bytes):
-//   U slice of a (tile, block) pair: core (mc, kc) = rows 8mc..8mc+7, terms 8kc..8kc+7,
-//   stored core-by-core with mc fastest: ((kc * (s8 / 8)) + mc) * 128 bytes, s8 = tile
-//   rows rounded to 8.  In shared memory the same cores sit at (kc * 16 + mc) * 128
-//   bytes (16 row cores for M = 128; the rows past s8 stay zero).
-//   T_b: core (nc, kc) = vectors 8nc..8nc+7, terms 8kc..8kc+7 at (kc * 4 + nc) * 128.
-// Descriptors: leading byte offset = stride between K cores, stride byte offset =
-// stride between row cores; instruction kind::f16 with BF16 A/B, FP32 D, M 128, N 32.
-// Every wait on the MMA's mbarrier is bounded; on a time-out the kernel records an
-// error flag (read by the host), skips the remaining work and frees its tensor memory.
+//   pass 1 (k_tc_pass<0>): per admissible block, t_b = V_b^T X_b (M = rank rounded to
+//     16, padded to 128; N = 32 vectors; K = the block's columns), written as BF16
+//     operand cores of pass 2;
+//   pass 2 (k_tc_pass<1>): per row tile (M = 128 rows), the sum over its pairs of
+//     U_slice * t_b (low rank; K = rank) and D_slice * X_b (near field; K = columns),
+//     accumulated in tensor memory and written to the tile's rows of Y (caller order).
+//
+// Both passes run one persistent kernel: one CTA per SM walks a job list balanced on
+// the host (longest job first onto the least loaded CTA).  A job (a block in pass 1, a
+// tile in pass 2) is a run of "steps", each an A chunk (<= 24 KB) and the B chunk it
+// multiplies (<= 8 KB).  Warp 4 copies steps with bulk copies (cp.async.bulk,
+// completion counted on the step slot's mbarrier) into a 208 KB byte ring that holds up
+// to 16 steps of any size; warp 5 issues the MMAs (one elected lane, accumulating in one
+// of two 32-column tensor-memory buffers) and frees each step's bytes with
+// tcgen05.commit; warps 0-3 drain a finished buffer (tcgen05.ld, one 32-row quarter
+// each) while the next job accumulates in the other.
+//
+// Operand layout (no swizzle, K-major core matrices of 8 rows x 16 bytes), K cores
+// outermost so that every K range of an operand is one contiguous byte range:
+//   A (U slice, near slice or V_b^T): core (kc, mc) at (kc * rc + mc) * 128 bytes, rc
+//     = stored row cores (tile rows or rank rounded to 8).  The MMA's M is 128: rows
+//     past 8 rc read the next K core's bytes (or the rest of the stage) and only reach
+//     accumulator rows that are never read back.
+//   B (X or t_b): core (nc, kc) = vectors 8nc..8nc+7, K 8kc..8kc+7 at (kc * 4 + nc) * 128.
+//   X is kept over the Z-ordered column index with 8 columns per K core; a block whose
+//   columns start at c0 reads K cores from c0 / 8 on, and its A operand carries
+//   c0 mod 8 leading zero columns so the K positions line up.
+// Descriptors: leading byte offset = stride between K cores (A: rc * 128, B: 512),
+// stride byte offset = stride between row cores (128).  Instruction kind::f16 with BF16
+// A/B, FP32 D, M 128, N 32.
+// Every wait is bounded (pipeline.cuh): on a time-out the waiting role records an error
+// code in the handle's flag, leaves its loop, and the CTA waits for its own copies and
+// MMAs before freeing tensor memory.  BF16 rounding of factors, near field, X and t_b
+// (~4e-3 per entry) bounds the accuracy: products agree with FP32 ones to ~1e-3.
 #include <cuda_bf16.h>
 
 #include <algorithm>
+#include <queue>
 #include <vector>
 
 #include "hmg_matrix.cuh"
+#include "pipeline.cuh"
 #include "stream.cuh"
 
 namespace hmg {
 
-static constexpr int TC_N = 32;           // vectors per pass (MMA N)
-static constexpr int TC_MAXR16 = 96;      // largest rank (rounded to 16) with room in shared memory
-static constexpr long long TC_SPIN = 1ll << 26;
+static constexpr int TC_N = 32;            // vectors per pass (MMA N)
+static constexpr int TC_MAXR16 = 128;      // largest rank rounded to 16 (pass 1's M)
+static constexpr int TC_SLOTS = 16;        // steps in flight per CTA at most
+static constexpr int TC_RING = 212992;     // bytes of the operand ring (208 KB)
+static constexpr int TC_ISSUERS = 8;       // lanes of the copy warp issuing at once
+static constexpr int TC_ABYTES = 24576;    // A chunk of a step: at most 192 core matrices
+static constexpr int TC_BBYTES = 8192;     // B chunk: at most 16 K cores x 4 vector cores
+static constexpr int TC_THREADS = 192;     // warps 0-3 epilogue, 4 copies, 5 MMAs
+static constexpr int TC_XGROUP = 512;      // bytes of one K core of X or t_b (4 vector cores)
+
+struct TcStep {
+    long long a_off;  // bytes into the A arena
+    long long b_off;  // bytes into the B buffer (X cores, then t_b cores)
+    int ksteps;       // MMAs of K = 16 (two K cores each)
+    int meta;         // bits 0-7: row cores of A (its K-core stride / 128); bit 8: first step of a job; bit 9: last
+};
+static_assert(sizeof(TcStep) == 24, "TcStep layout");
+
+struct TcJob {
+    int r0;    // pass 2: first Z row of the tile; pass 1: t_b's first 16-term group
+    int rows;  // pass 2: rows of the tile; pass 1: rank rounded to 16
+};
 
 // ---------------------------------------------------------------------------
-// conversion of the FP32 factors
+// conversion of the FP32 factors and near field (once, by hmg_build_bf16_factors)
 // ---------------------------------------------------------------------------
-// one CTA per pair: FP32 slice (s_pad x r, column-major) -> BF16 cores
-__global__ void k_tc_u(const PairDesc* desc, const int* pair_tile, const long long* uoff, const int* tile_s,
-                       int npairs, __nv_bfloat16* out)
-{
-    const int p = blockIdx.x;
-    if (p >= npairs || uoff[p] < 0) return;
-    const PairDesc d = desc[p];
-    const int s = tile_s[pair_tile[p]], sp = (s + 3) & ~3, s8 = (s + 7) & ~7;
-    const int r = d.ncol, r16 = (r + 15) & ~15;
-    const float* src = static_cast<const float*>(d.data);
-    __nv_bfloat16* dst = out + uoff[p] / 2;
-    const int mcores = s8 / 8;
-    for (int idx = threadIdx.x; idx < s8 * r16; idx += blockDim.x) {
-        const int core = idx >> 6, e = idx & 63;
-        const int kc = core / mcores, mc = core - kc * mcores;
-        const int i = mc * 8 + (e >> 3), k = kc * 8 + (e & 7);
-        const float v = (i < s && k < r) ? src[(size_t)k * sp + i] : 0.0f;
-        dst[idx] = __float2bfloat16_rn(v);
-    }
-}
-
-// ---------------------------------------------------------------------------
-// t_b (FP32, [term][32] from the multi-vector K1) -> BF16 operand cores; terms
-// r..r16-1 are zero
-// ---------------------------------------------------------------------------
-__global__ void k_tc_t(const int* far_blocks, int nfar, const int* rank, const long long* rank_off,
-                       const long long* toff, const float* __restrict__ tm, __nv_bfloat16* tb)
+// far pair: U slice (s_pad x r, column-major) -> A cores, rc = s8 / 8, K = r16
+__global__ void k_tc_u(const PairDesc* desc, const int* plist, const long long* aoff, const int* ptile,
+                       const int* tile_s, int n, __nv_bfloat16* out)
 {
     const int u = blockIdx.x;
-    if (u >= nfar) return;
-    const int b = far_blocks[u];
-    const int r = rank[b], r16 = (r + 15) & ~15;
-    const float* src = tm + (size_t)rank_off[b] * TC_N;
-    __nv_bfloat16* out = tb + toff[b] * (16 * TC_N);
-    for (int idx = threadIdx.x; idx < r16 * TC_N; idx += blockDim.x) {
+    if (u >= n) return;
+    const int p = plist[u];
+    const PairDesc d = desc[p];
+    const int s = tile_s[ptile[u]], sp = (s + 3) & ~3, s8 = (s + 7) & ~7;
+    const int r = d.ncol, r16 = (r + 15) & ~15;
+    const float* src = static_cast<const float*>(d.data);
+    __nv_bfloat16* dst = out + aoff[u] / 2;
+    const int rc = s8 / 8;
+    for (int idx = threadIdx.x; idx < s8 * r16; idx += blockDim.x) {
         const int core = idx >> 6, e = idx & 63;
-        const int kc = core >> 2, nc = core & 3;
-        const int n = nc * 8 + (e >> 3), k = kc * 8 + (e & 7);
-        out[idx] = __float2bfloat16_rn(k < r ? src[(size_t)k * TC_N + n] : 0.0f);
+        const int kc = core / rc, mc = core - kc * rc;
+        const int i = mc * 8 + (e >> 3), k = kc * 8 + (e & 7);
+        dst[idx] = __float2bfloat16_rn((i < s && k < r) ? src[(size_t)k * sp + i] : 0.0f);
+    }
+}
+
+// near pair: slice (s_pad x m2, column-major) -> A cores with c0 mod 8 leading zero columns
+__global__ void k_tc_near(const PairDesc* desc, const int* plist, const long long* aoff, const int* ptile,
+                          const int* tile_s, int n, __nv_bfloat16* out)
+{
+    const int u = blockIdx.x;
+    if (u >= n) return;
+    const PairDesc d = desc[plist[u]];
+    const int s = tile_s[ptile[u]], sp = (s + 3) & ~3, s8 = (s + 7) & ~7;
+    const int m2 = d.ncol, a = d.c0 & 7, kw = (a + m2 + 15) & ~15;
+    const float* src = static_cast<const float*>(d.data);
+    __nv_bfloat16* dst = out + aoff[u] / 2;
+    const int rc = s8 / 8;
+    for (long long idx = threadIdx.x; idx < (long long)s8 * kw; idx += blockDim.x) {
+        const int core = (int)(idx >> 6), e = (int)(idx & 63);
+        const int kc = core / rc, mc = core - kc * rc;
+        const int i = mc * 8 + (e >> 3), c = kc * 8 + (e & 7) - a;
+        dst[idx] = __float2bfloat16_rn((i < s && c >= 0 && c < m2) ? src[(size_t)c * sp + i] : 0.0f);
+    }
+}
+
+// admissible block: V_b^T (rows of m2p FP32 entries per term) -> A cores, rc = r16 / 8
+__global__ void k_tc_v(const int* blist, const long long* voff, int n, void* const* ptrV, const int* rank,
+                       const int* blk_c0, const int* blk_m2, __nv_bfloat16* out)
+{
+    const int u = blockIdx.x;
+    if (u >= n) return;
+    const int b = blist[u];
+    const int r = rank[b], r16 = (r + 15) & ~15, m2 = blk_m2[b], m2p = (m2 + 3) & ~3;
+    const int a = blk_c0[b] & 7, kw = (a + m2 + 15) & ~15;
+    const float* V = static_cast<const float*>(ptrV[b]);
+    __nv_bfloat16* dst = out + voff[u] / 2;
+    const int rc = r16 / 8;
+    for (long long idx = threadIdx.x; idx < (long long)r16 * kw; idx += blockDim.x) {
+        const int core = (int)(idx >> 6), e = (int)(idx & 63);
+        const int kc = core / rc, mc = core - kc * rc;
+        const int m = mc * 8 + (e >> 3), c = kc * 8 + (e & 7) - a;
+        dst[idx] = __float2bfloat16_rn((m < r && c >= 0 && c < m2) ? V[(size_t)m * m2p + c] : 0.0f);
     }
 }
 
 // ---------------------------------------------------------------------------
-// the tile kernel
+// per product: X -> BF16 cores (Z-ordered columns), FP32 rows -> Y
+// ---------------------------------------------------------------------------
+// thread (g, j): columns 8g..8g+7 of vector j, one 16-byte row of K core g
+__global__ void k_tc_x(const double* __restrict__ X, int ldx, int nrhs, const int* __restrict__ perm1, int n,
+                       long long ngroups, uint4* xb)
+{
+    const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= ngroups * TC_N) return;
+    const long long g = idx >> 5;
+    const int j = (int)(idx & 31);
+    __nv_bfloat16 v[8];
+#pragma unroll
+    for (int e = 0; e < 8; e++) {
+        const long long c = g * 8 + e;
+        v[e] = __float2bfloat16_rn(c < n && j < nrhs ? (float)X[(size_t)perm1[c] + (size_t)j * ldx] : 0.0f);
+    }
+    xb[(g * 4 + (j >> 3)) * 8 + (j & 7)] = *reinterpret_cast<const uint4*>(v);
+}
+
+// ---------------------------------------------------------------------------
+// the persistent pass kernel
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ uint64_t smem_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo)
 {
@@ -98,184 +175,450 @@ static constexpr uint32_t TC_IDESC = (1u << 4) | (1u << 7) | (1u << 10) | ((uint
                                      ((uint32_t)(128 >> 4) << 24);
 
 struct TcSmem {
-    __nv_bfloat16 A[2][TC_MAXR16 / 8][16][64];    // 2 stages x K cores x row cores x 8 rows x 8 terms
-    __nv_bfloat16 B[2][TC_MAXR16 / 8][4][64];     // 2 stages x K cores x vector cores x 8 x 8
-    unsigned long long mbar[2];
+    unsigned char ring[TC_RING];   // operand ring: each step's A chunk, then its B chunk
+    __nv_bfloat16 stg[4][1024];    // pass 1 epilogue: 4 K cores of t_b per warp (also takes
+                                   // the MMA's reads of unused A rows past the ring's end)
+    uint64_t full[TC_SLOTS], empty[TC_SLOTS], accf[2], acce[2], fin;
+    uint32_t slot_a[TC_SLOTS], slot_b[TC_SLOTS];  // shared addresses of a step's A and B
+    int slot_meta[TC_SLOTS];                       // a step's meta word, MMAs in bits 16+
+    int slot_pos[TC_SLOTS];                        // ring offset of a step (copy warp only)
+    int step_bytes[32];                            // bytes of the copy warp's current 32 steps
     uint32_t tmem;
     int fail;
 };
 
-__device__ __forceinline__ void tc_cp16(void* dst, const void* src)
+static_assert(sizeof(TcSmem) <= 227 * 1024, "TcSmem exceeds the shared memory of a CTA");
+
+__device__ __forceinline__ void bulk_g2s_first(void* dst, const void* src, unsigned bytes, uint64_t* bar,
+                                               uint64_t policy)
 {
-    const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(dst));
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(src) : "memory");
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes.L2::cache_hint [%0], [%1], %2, [%3], "
+        "%4;" ::"r"(smem_u32(dst)),
+        "l"(src), "r"(bytes), "r"(smem_u32(bar)), "l"(policy)
+        : "memory");
 }
 
-__device__ __forceinline__ bool tc_wait(uint32_t mbar, uint32_t phase)
+__device__ __forceinline__ void tc_mma(uint32_t d, uint64_t ad, uint64_t bd, uint32_t acc)
 {
-    uint32_t ok = 0;
-    for (long long it = 0; it < TC_SPIN && !ok; it++)
-        asm volatile(
-            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
-            : "=r"(ok)
-            : "r"(mbar), "r"(phase)
-            : "memory");
+    asm volatile(
+        "{\n .reg .pred pd;\n setp.ne.b32 pd, %4, 0;\n"
+        " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, pd;\n}" ::"r"(d),
+        "l"(ad), "l"(bd), "r"(TC_IDESC), "r"(acc));
+}
+
+__device__ __forceinline__ void tc_commit(uint64_t* bar)
+{
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+                 : "memory");
+}
+
+// non-blocking: has the phase of this parity completed?
+__device__ __forceinline__ bool mbar_test_wait(uint64_t* bar, unsigned parity)
+{
+    unsigned ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
     return ok != 0;
 }
 
-// one CTA (4 warps) per row tile; the low-rank pairs' operands are copied two stages
-// deep (cp.async), so the copy of one pair overlaps the MMAs of the previous one
-__global__ void __launch_bounds__(128) k_tile_tc(const PairDesc* __restrict__ desc, const int* pair_block,
-                                                 const long long* __restrict__ uoff, const char* __restrict__ tcu,
-                                                 const __nv_bfloat16* __restrict__ tb, const long long* toff,
-                                                 const int* tile_pair_start, const int* tile_r0, const int* tile_s,
-                                                 const int* perm1, const float* __restrict__ xm, int nrhs, double* Y,
-                                                 int ldy, int* err)
+__device__ __forceinline__ TcStep load_step(const TcStep* steps, int i, int n)
+{
+    TcStep st{};
+    if (i < n) st = steps[i];
+    return st;
+}
+
+__device__ __forceinline__ uint32_t pack_bf16(float lo, float hi)
+{
+    const __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
+    return *reinterpret_cast<const uint32_t*>(&v);
+}
+
+// Steps of CTA c: [cta[c].y, cta[c+1].y); its jobs: [cta[c].x, cta[c+1].x).
+// Pass 1 (MODE 0) writes t_b cores at Bbuf + tb_off; pass 2 (MODE 1) writes rows of Y.
+template <int MODE>
+__global__ void __launch_bounds__(TC_THREADS, 1)
+    k_tc_pass(const TcStep* __restrict__ steps, const TcJob* __restrict__ jobs, const int2* __restrict__ cta,
+              const char* __restrict__ A, char* Bbuf, long long tb_off, const int* __restrict__ perm0, int nrhs,
+              double* Y, int ldy, int* err)
 {
     extern __shared__ __align__(1024) unsigned char tc_raw[];
     TcSmem& sm = *reinterpret_cast<TcSmem*>(tc_raw);
-    const int t = blockIdx.x, tid = threadIdx.x, warp = tid >> 5;
-    const int s = tile_s[t], sp = (s + 3) & ~3, s8 = (s + 7) & ~7, tr0 = tile_r0[t];
-    const int pbeg = tile_pair_start[t], pend = tile_pair_start[t + 1];
-    const uint32_t mbar0 = static_cast<uint32_t>(__cvta_generic_to_shared(&sm.mbar[0]));
-    const int mcores = s8 / 8;
-
-    for (int i = tid; i < (int)(sizeof(sm.A) / 16); i += 128) reinterpret_cast<uint4*>(&sm.A[0][0][0][0])[i] = make_uint4(0, 0, 0, 0);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int2 lo = cta[blockIdx.x], hi = cta[blockIdx.x + 1];
+    const int nsteps = hi.y - lo.y;
+    const TcStep* my_steps = steps + lo.y;
+    volatile int* fail = &sm.fail;
     if (tid == 0) {
+        for (int s = 0; s < TC_SLOTS; s++) {
+            mbar_init(&sm.full[s], 1);
+            mbar_init(&sm.empty[s], 1);
+        }
+        for (int b = 0; b < 2; b++) {
+            mbar_init(&sm.accf[b], 1);
+            mbar_init(&sm.acce[b], 4);
+        }
+        mbar_init(&sm.fin, 1);
         sm.fail = 0;
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(mbar0));
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(mbar0 + 8));
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
-    if (warp == 0) {
-        const uint32_t slot = static_cast<uint32_t>(__cvta_generic_to_shared(&sm.tmem));
-        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 32;" ::"r"(slot));
+    if (warp == 5) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 64;" ::"r"(smem_u32(&sm.tmem)));
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
     }
     __syncthreads();
-    asm volatile("tcgen05.fence::after_thread_sync;");
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const uint32_t tmem = sm.tmem;
 
-    // the dense pairs ran before this kernel (CUDA cores, FP32); Y holds their sums
-    float acc[TC_N];
-#pragma unroll
-    for (int j = 0; j < TC_N; j++) acc[j] = 0.0f;
-
-    // low-rank pairs on the tensor cores
-    auto next_far = [&](int p) {
-        while (p < pend) {
-            const PairDesc& d = desc[p];
-            if (d.kind == PAIR_FAR && d.ncol > 0 && uoff[p] >= 0) break;
-            p++;
-        }
-        return p;
-    };
-    auto copy = [&](int p, int b) {
-        const int r16 = (desc[p].ncol + 15) & ~15, kcores = r16 / 8;
-        const char* su = tcu + uoff[p];
-        for (int i = tid; i < kcores * mcores * 8; i += 128) {
-            const int core = i >> 3, part = i & 7;
-            const int kc = core / mcores, mc = core - kc * mcores;
-            tc_cp16(reinterpret_cast<uint4*>(&sm.A[b][kc][mc][0]) + part, su + (size_t)i * 16);
-        }
-        const char* st = reinterpret_cast<const char*>(tb + toff[pair_block[p]] * (16 * TC_N));
-        for (int i = tid; i < kcores * 4 * 8; i += 128)
-            tc_cp16(reinterpret_cast<uint4*>(&sm.B[b][0][0][0]) + i, st + (size_t)i * 16);
-    };
-    uint32_t phase[2] = {0u, 0u};
-    bool busy[2] = {false, false};
-    bool any = false;
-    int cur = next_far(pbeg), b = 0;
-    if (cur < pend) copy(cur, 0);
-    asm volatile("cp.async.commit_group;" ::: "memory");
-    while (cur < pend) {
-        const int nxt = next_far(cur + 1);
-        if (nxt < pend) {
-            if (busy[b ^ 1]) {  // the MMAs that read buffer b^1 must be done before it is refilled
-                if (!tc_wait(mbar0 + 8 * (b ^ 1), phase[b ^ 1])) sm.fail = 1;
-                phase[b ^ 1] ^= 1u;
-                busy[b ^ 1] = false;
+    if (warp == 4) {
+        // ---- copies.  Lane l holds step i0 + l (the next 32 are loaded meanwhile).  In
+        // rounds, lane 0 places up to TC_ISSUERS steps at the ring's head (after the steps
+        // they would overwrite, oldest first, have been freed by their MMAs) and the lanes
+        // holding them issue their copies side by side: one thread issues one bulk copy
+        // every few hundred cycles, so small steps need several issuers to keep HBM busy. ----
+        uint64_t pol;
+        asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(pol));
+        int issued = 0, tail = 0, head = 0;  // lane 0's ring state
+        bool ok = true;
+        TcStep nxt = load_step(my_steps, lane, nsteps);
+        for (int i0 = 0; i0 < nsteps && ok; i0 += 32) {
+            const TcStep mine = nxt;
+            nxt = load_step(my_steps, i0 + 32 + lane, nsteps);
+            const int cnt = min(32, nsteps - i0);
+            const int ab = mine.ksteps * 2 * (mine.meta & 0xff) * 128, bb = mine.ksteps * 1024;
+            __syncwarp();
+            sm.step_bytes[lane] = ab + bb;
+            __syncwarp();
+            for (int k = 0; k < cnt && ok;) {
+                int m = 0;
+                if (lane == 0) {
+                    while (k + m < cnt && m < TC_ISSUERS) {
+                        const int i = i0 + k + m, z = sm.step_bytes[k + m];
+                        int pos = -1;
+                        if (tail == i) {
+                            pos = 0;  // nothing in flight
+                        } else if (i - tail < TC_SLOTS) {
+                            const int tpos = sm.slot_pos[tail % TC_SLOTS];  // oldest step in flight
+                            if (tpos < head) {                              // in flight: [tpos, head)
+                                if (head + z <= TC_RING) pos = head;
+                                else if (z <= tpos) pos = 0;
+                            } else if (head + z <= tpos) {                  // in flight: [tpos, end) + [0, head)
+                                pos = head;
+                            }
+                        }
+                        if (pos >= 0) {
+                            sm.slot_pos[i % TC_SLOTS] = pos;
+                            head = pos + z;
+                            m++;
+                            continue;
+                        }
+                        if (mbar_test_wait(&sm.empty[tail % TC_SLOTS], (tail / TC_SLOTS) & 1)) {
+                            tail++;  // the oldest step's MMAs are done: its bytes and slot are free
+                            continue;
+                        }
+                        if (m > 0) break;  // issue what is placed; wait in the next round
+                        if (*fail || !mbar_wait(&sm.empty[tail % TC_SLOTS], (tail / TC_SLOTS) & 1, err, 11)) {
+                            ok = false;
+                            break;
+                        }
+                        tail++;
+                    }
+                    issued += m;
+                }
+                m = __shfl_sync(~0u, m, 0);
+                ok = __shfl_sync(~0u, ok, 0);
+                __syncwarp();
+                if (lane >= k && lane < k + m) {
+                    const int slot = (i0 + lane) % TC_SLOTS, pos = sm.slot_pos[slot];
+                    const uint32_t a = smem_u32(sm.ring + pos);
+                    sm.slot_a[slot] = a;
+                    sm.slot_b[slot] = a + ab;
+                    sm.slot_meta[slot] = mine.meta | (mine.ksteps << 16);
+                    mbar_arrive_expect_tx(&sm.full[slot], ab + bb);
+                    bulk_g2s_first(sm.ring + pos, A + mine.a_off, ab, &sm.full[slot], pol);
+                    bulk_g2s(sm.ring + pos + ab, Bbuf + mine.b_off, bb, &sm.full[slot]);
+                }
+                k += m;
             }
-            copy(nxt, b ^ 1);
         }
-        asm volatile("cp.async.commit_group;" ::: "memory");
-        asm volatile("cp.async.wait_group 1;" ::: "memory");
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        __syncthreads();
-        if (sm.fail) break;
-        if (tid == 0) {
-            asm volatile("tcgen05.fence::after_thread_sync;");
-            const int r16 = (desc[cur].ncol + 15) & ~15;
-            const uint32_t a_base = static_cast<uint32_t>(__cvta_generic_to_shared(&sm.A[b][0][0][0]));
-            const uint32_t b_base = static_cast<uint32_t>(__cvta_generic_to_shared(&sm.B[b][0][0][0]));
-            for (int q = 0; q < r16 / 16; q++) {
-                const uint64_t ad = smem_desc(a_base + q * 2 * (16 * 128), 16 * 128, 128);
-                const uint64_t bd = smem_desc(b_base + q * 2 * (4 * 128), 4 * 128, 128);
-                const uint32_t accumulate = (any || q > 0) ? 1u : 0u;
+        if (!ok) *fail = 1;
+        // the last copy into every slot has landed before the CTA leaves (a no-op unless a wait failed)
+        issued = __shfl_sync(~0u, issued, 0);
+        if (lane == 0)
+            for (int s = 0; s < TC_SLOTS && s < issued; s++)
+                mbar_wait(&sm.full[s], ((issued - 1 - s) / TC_SLOTS) & 1, err, 12);
+    } else if (warp == 5) {
+        // ---- MMAs: lane 0 alone; each step's parameters come with its slot ----
+        if (lane == 0) {
+            int jc = 0;
+            for (int i = 0; i < nsteps; i++) {
+                const int slot = i % TC_SLOTS, buf = jc & 1;
+                if (*fail || !mbar_wait(&sm.full[slot], (i / TC_SLOTS) & 1, err, 14)) {
+                    *fail = 1;
+                    break;
+                }
+                const uint32_t a0 = sm.slot_a[slot], b0 = sm.slot_b[slot];
+                const int meta = sm.slot_meta[slot], ks = meta >> 16;
+                const bool first = meta & 256, last = meta & 512;
+                if (first && jc >= 2 && !mbar_wait(&sm.acce[buf], ((jc >> 1) - 1) & 1, err, 13)) {
+                    *fail = 1;
+                    break;
+                }
+                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                const uint32_t lbo = (uint32_t)(meta & 0xff) * 128u;
+                const uint32_t d = tmem + (uint32_t)(buf * TC_N);
+                for (int q = 0; q < ks; q++) {
+                    const uint64_t ad = smem_desc(a0 + q * 2 * lbo, lbo, 128);
+                    const uint64_t bd = smem_desc(b0 + q * 1024, TC_XGROUP, 128);
+                    tc_mma(d, ad, bd, (first && q == 0) ? 0u : 1u);
+                }
+                tc_commit(&sm.empty[slot]);
+                if (last) {
+                    tc_commit(&sm.accf[buf]);
+                    jc++;
+                }
+            }
+            tc_commit(&sm.fin);  // every MMA issued here has completed before tensor memory is freed
+            mbar_wait(&sm.fin, 0, err, 15);
+        }
+        __syncwarp();
+    } else {
+        // ---- epilogue: warp w owns accumulator rows 32w..32w+31; lane l holds job j0 + l ----
+        const int njobs = hi.x - lo.x;
+        const int2* my_jobs = reinterpret_cast<const int2*>(jobs) + lo.x;
+        int2 nxt = lane < njobs ? my_jobs[lane] : make_int2(0, 0);
+        bool ok = true;
+        for (int j0 = 0; j0 < njobs && ok; j0 += 32) {
+            const int2 mine = nxt;
+            if (j0 + 32 + lane < njobs) nxt = my_jobs[j0 + 32 + lane];
+            const int cnt = min(32, njobs - j0);
+            for (int k = 0; k < cnt; k++) {
+                const int r0 = __shfl_sync(~0u, mine.x, k), rows = __shfl_sync(~0u, mine.y, k);
+                const int jc = j0 + k, buf = jc & 1;
+                const int row = warp * 32 + lane;
+                // pass 2: this row's place in Y, fetched before the wait
+                const int yrow = (MODE == 1 && row < rows) ? perm0[r0 + row] : 0;
+                ok = !*fail && mbar_wait(&sm.accf[buf], (jc >> 1) & 1, err, 16);
+                if (!__all_sync(~0u, ok)) {
+                    ok = false;
+                    break;
+                }
+                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                uint32_t v[32];
+                const uint32_t taddr = tmem + (uint32_t)(buf * TC_N) + ((uint32_t)(warp * 32) << 16);
                 asm volatile(
-                    "{\n .reg .pred pd;\n setp.ne.b32 pd, %4, 0;\n"
-                    " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, pd;\n}" ::"r"(tmem),
-                    "l"(ad), "l"(bd), "r"(TC_IDESC), "r"(accumulate));
+                    "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, "
+                    "%13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, "
+                    "[%32];"
+                    : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+                      "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]),
+                      "=r"(v[15]), "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]),
+                      "=r"(v[22]), "=r"(v[23]), "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]),
+                      "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
+                    : "r"(taddr));
+                asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+                asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+                __syncwarp();
+                if (lane == 0) mbar_arrive(&sm.acce[buf]);
+                if (MODE == 1) {
+                    if (row < rows) {
+                        double* y = Y + yrow;
+#pragma unroll
+                        for (int q = 0; q < TC_N; q++)
+                            if (q < nrhs) y[(size_t)q * ldy] = (double)__uint_as_float(v[q]);
+                    }
+                } else {
+                    // term row -> B cores of pass 2 (K = term): element (term m, vector q) at byte
+                    // ((m / 8) * 4 + q / 8) * 128 + (q % 8) * 16 + (m % 8) * 2; this warp's 32 terms
+                    // fill K cores 4w..4w+3.  Lanes 2p, 2p+1 pair their terms into 32-bit words
+                    // (even lane: vector 2t, odd lane: vector 2t+1); 16-byte row u of the staging
+                    // sits at u ^ (2 (u / 32)), which spreads the four K cores over all banks.
+                    uint32_t* stg = reinterpret_cast<uint32_t*>(sm.stg[warp]);
+                    const bool odd = lane & 1;
+#pragma unroll
+                    for (int t = 0; t < 16; t++) {
+                        const float v0 = __uint_as_float(v[2 * t]), v1 = __uint_as_float(v[2 * t + 1]);
+                        const float x = __shfl_xor_sync(~0u, odd ? v0 : v1, 1);
+                        const int q = odd ? 2 * t + 1 : 2 * t;
+                        const uint32_t w = odd ? pack_bf16(x, v1) : pack_bf16(v0, x);
+                        const int u = (lane >> 3) * 32 + (q >> 3) * 8 + (q & 7);
+                        stg[(u ^ ((u >> 5) * 2)) * 4 + ((lane & 7) >> 1)] = w;
+                    }
+                    __syncwarp();
+                    uint4* dst = reinterpret_cast<uint4*>(Bbuf + tb_off + (size_t)r0 * 1024);
+                    const uint4* src = reinterpret_cast<const uint4*>(stg);
+#pragma unroll
+                    for (int q = 0; q < 4; q++) {
+                        const int u = q * 32 + lane;
+                        if (warp * 4 + q < (rows >> 3)) dst[(warp * 4 + q) * 32 + lane] = src[u ^ (q * 2)];
+                    }
+                    __syncwarp();
+                }
             }
-            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(mbar0 + 8 * b)
-                         : "memory");
+            ok = __all_sync(~0u, ok);
         }
-        busy[b] = true;
-        any = true;
-        cur = nxt;
-        b ^= 1;
-    }
-    asm volatile("cp.async.wait_group 0;" ::: "memory");
-    for (int q = 0; q < 2; q++)
-        if (busy[q]) {
-            if (!tc_wait(mbar0 + 8 * q, phase[q])) sm.fail = 1;
-            busy[q] = false;
-        }
-    if (sm.fail && tid == 0) atomicExch(err, 1);
-    __syncthreads();
-    asm volatile("tcgen05.fence::after_thread_sync;");
-    if (any && !sm.fail) {
-        uint32_t v[32];
-        const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16);
-        asm volatile(
-            "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
-            "%15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
-            : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
-              "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15]),
-              "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]), "=r"(v[22]),
-              "=r"(v[23]), "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]),
-              "=r"(v[30]), "=r"(v[31])
-            : "r"(taddr));
-        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-#pragma unroll
-        for (int j = 0; j < TC_N; j++) acc[j] += __uint_as_float(v[j]);
-    }
-    if (any && tid < s && !sm.fail) {
-        const size_t row = (size_t)perm1[tr0 + tid];
-#pragma unroll
-        for (int j = 0; j < TC_N; j++)
-            if (j < nrhs) Y[row + (size_t)j * ldy] += (double)acc[j];
+        if (!ok) *fail = 1;
     }
     __syncthreads();
-    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 32;" ::"r"(tmem));
+    if (warp == 5) {
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 64;" ::"r"(tmem));
+    }
 }
 
 // ---------------------------------------------------------------------------
 // host side
 // ---------------------------------------------------------------------------
+static int tc_num_sms()
+{
+    int dev = 0, n = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+    return n > 0 ? n : 148;
+}
+
 void free_tc(hmg_matrix* h)
 {
     cudaStream_t s = h->stream;
     if (h->tc_u) cudaFree(h->tc_u);
-    h->tc_u = nullptr;
-    dfree(h->tc_uoff, s);
-    dfree(h->tc_toff, s);
-    dfree(h->tc_pair_tile, s);
-    dfree(h->tc_far_blocks, s);
+    if (h->tc_v) cudaFree(h->tc_v);
+    if (h->tc_bbuf) {
+        cudaStreamSynchronize(s);  // a product in flight may still read it
+        cudaFree(h->tc_bbuf);
+    }
+    h->tc_u = h->tc_v = h->tc_bbuf = nullptr;
+    for (int q = 0; q < 2; q++) {
+        dfree(h->tc_steps[q], s);
+        dfree(h->tc_jobs[q], s);
+        dfree(h->tc_cta[q], s);
+        h->tc_njobs[q] = 0;
+    }
     h->tc_ready = false;
     h->tc_bytes = 0;
-    h->tc_tgroups = 0;
-    h->tc_nfar = 0;
+    h->tc_xbytes = h->tc_tbytes = 0;
+    h->tc_grid = 0;
+    h->tc_all_tiles = false;
 }
+
+namespace {
+
+struct JobList {
+    std::vector<TcStep> steps;   // in job order
+    std::vector<int> step0;      // per job: first step (then end)
+    std::vector<TcJob> info;
+    std::vector<double> cost;
+    void begin(TcJob j)
+    {
+        step0.push_back((int)steps.size());
+        info.push_back(j);
+        cost.push_back(0.0);
+    }
+    // K cores [0, kcores) of an A operand with rc row cores, in chunks of at most kcc
+    void add(long long a_off, long long b_off, int rc, int kcores, int kcc, double b_weight)
+    {
+        for (int kc0 = 0; kc0 < kcores; kc0 += kcc) {
+            const int nk = std::min(kcc, kcores - kc0);
+            TcStep st;
+            st.a_off = a_off + (long long)kc0 * rc * 128;
+            st.b_off = b_off + (long long)kc0 * TC_XGROUP;
+            st.ksteps = nk / 2;
+            st.meta = rc;
+            steps.push_back(st);
+            cost.back() += (double)nk * rc * 128 + b_weight * nk * TC_XGROUP;
+        }
+    }
+};
+
+// Every copy a step issues stays inside its arena and its stage, and every job's
+// output inside its buffer: checked here, on the host, before any launch.
+bool steps_in_bounds(const JobList& L, long long abytes, long long bbytes, long long out_limit, int q)
+{
+    for (const TcStep& st : L.steps) {
+        const long long rc = st.meta & 0xff, ab = (long long)st.ksteps * 2 * rc * 128, bb = (long long)st.ksteps * 1024;
+        if (st.ksteps < 1 || st.ksteps > 8 || rc < 1 || rc > 16 || ab > TC_ABYTES || bb > TC_BBYTES ||
+            st.a_off < 0 || st.a_off % 16 || st.a_off + ab > abytes || st.b_off < 0 || st.b_off % 16 ||
+            st.b_off + bb > bbytes)
+            return false;
+    }
+    for (const TcJob& j : L.info) {
+        if (j.rows < 1 || j.rows > 128 || j.r0 < 0) return false;
+        if (q == 1 ? (long long)j.r0 + j.rows > out_limit : (long long)j.r0 + j.rows / 16 > out_limit) return false;
+    }
+    return true;
+}
+
+// longest job first onto the least loaded CTA; emits steps and jobs CTA by CTA
+hmg_status upload_jobs(hmg_matrix* h, int q, JobList& L, double job_cost, int grid)
+{
+    cudaStream_t s = h->stream;
+    const int nj = (int)L.info.size();
+    L.step0.push_back((int)L.steps.size());
+    std::vector<int> order(nj);
+    for (int j = 0; j < nj; j++) order[j] = j;
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return L.cost[a] > L.cost[b]; });
+    using Load = std::pair<double, int>;
+    std::priority_queue<Load, std::vector<Load>, std::greater<Load>> heap;
+    for (int c = 0; c < grid; c++) heap.push({0.0, c});
+    std::vector<std::vector<int>> mine(grid);
+    for (int j : order) {
+        Load l = heap.top();
+        heap.pop();
+        mine[l.second].push_back(j);
+        heap.push({l.first + L.cost[j] + job_cost, l.second});
+    }
+    std::vector<TcStep> steps;
+    std::vector<TcJob> jobs;
+    std::vector<int2> cta(grid + 1);
+    steps.reserve(L.steps.size());
+    jobs.reserve(nj);
+    for (int c = 0; c < grid; c++) {
+        cta[c] = make_int2((int)jobs.size(), (int)steps.size());
+        for (int j : mine[c]) {
+            jobs.push_back(L.info[j]);
+            const int a = L.step0[j], b = L.step0[j + 1];
+            for (int i = a; i < b; i++) {
+                TcStep st = L.steps[i];
+                if (i == a) st.meta |= 256;
+                if (i == b - 1) st.meta |= 512;
+                steps.push_back(st);
+            }
+        }
+    }
+    cta[grid] = make_int2((int)jobs.size(), (int)steps.size());
+    hmg_status st;
+    if ((st = dalloc(&h->tc_steps[q], std::max(steps.size(), (size_t)1) * sizeof(TcStep), s)) ||
+        (st = dalloc(&h->tc_jobs[q], std::max(jobs.size(), (size_t)1) * sizeof(TcJob), s)) ||
+        (st = dalloc(&h->tc_cta[q], (size_t)(grid + 1) * sizeof(int2), s)))
+        return st;
+    if (!steps.empty())
+        HMG_CUDA_TRY(cudaMemcpyAsync(h->tc_steps[q], steps.data(), steps.size() * sizeof(TcStep), cudaMemcpyHostToDevice, s));
+    if (!jobs.empty())
+        HMG_CUDA_TRY(cudaMemcpyAsync(h->tc_jobs[q], jobs.data(), jobs.size() * sizeof(TcJob), cudaMemcpyHostToDevice, s));
+    HMG_CUDA_TRY(cudaMemcpyAsync(h->tc_cta[q], cta.data(), cta.size() * sizeof(int2), cudaMemcpyHostToDevice, s));
+    HMG_CUDA_TRY(cudaStreamSynchronize(s));  // the host vectors go out of scope
+    h->tc_njobs[q] = nj;
+    return HMG_OK;
+}
+
+hmg_status alloc_arena(void** p, long long bytes, const char* what)
+{
+    cudaError_t ce = cudaMalloc(p, (size_t)std::max(bytes, 16ll));
+    if (ce != cudaSuccess) {
+        cudaGetLastError();
+        *p = nullptr;
+        set_error("hmg_build_bf16_factors: allocating %lld bytes for %s failed: %s", bytes, what, cudaGetErrorString(ce));
+        return ce == cudaErrorMemoryAllocation ? HMG_ERR_NOMEM : HMG_ERR_CUDA;
+    }
+    return HMG_OK;
+}
+
+}  // namespace
 
 hmg_status build_bf16_factors(hmg_matrix* h)
 {
@@ -284,6 +627,10 @@ hmg_status build_bf16_factors(hmg_matrix* h)
     free_tc(h);
     if (h->far_prec != HMG_PREC_FP32) {
         set_error("hmg_build_bf16_factors: needs FP32 factors (hmg_precompute_aca with HMG_PREC_FP32)");
+        return HMG_ERR_STATE;
+    }
+    if (h->ndense > 0 && !(h->near_mode == HMG_NEAR_STORED && h->near_prec == HMG_PREC_FP32)) {
+        set_error("hmg_build_bf16_factors: needs an FP32 stored near field (hmg_precompute_dense with HMG_PREC_FP32)");
         return HMG_ERR_STATE;
     }
     if (h->group_count) {
@@ -296,57 +643,126 @@ hmg_status build_bf16_factors(hmg_matrix* h)
             return HMG_ERR_UNSUPPORTED;
         }
     if ((st = ensure_desc(h, 4))) return st;
-    const int np = h->npairs, nt = h->ntiles, nb = h->nblocks;
-    std::vector<int> tps(nt + 1), pblock(np), ts(nt);
+    const int np = h->npairs, nt = h->ntiles, nb = h->nblocks, grid = tc_num_sms();
+    std::vector<int> tps(nt + 1), pblock(np), ts(nt), tr0(nt);
     HMG_CUDA_TRY(cudaMemcpy(tps.data(), h->tile_pair_start, sizeof(int) * (nt + 1), cudaMemcpyDeviceToHost));
     HMG_CUDA_TRY(cudaMemcpy(pblock.data(), h->pair_block, sizeof(int) * np, cudaMemcpyDeviceToHost));
     HMG_CUDA_TRY(cudaMemcpy(ts.data(), h->tile_s, sizeof(int) * nt, cudaMemcpyDeviceToHost));
-    std::vector<long long> uoff(np, -1), toff(nb, 0);
-    std::vector<int> ptile(np), farb;
-    long long bytes = 0;
-    for (int t = 0; t < nt; t++)
-        for (int p = tps[t]; p < tps[t + 1]; p++) {
-            ptile[p] = t;
-            const int b = pblock[p];
-            if (b < h->ndense || h->h_rank[b] == 0) continue;
-            uoff[p] = bytes;
-            bytes += (long long)((ts[t] + 7) & ~7) * ((h->h_rank[b] + 15) & ~15) * 2;
-            bytes = (bytes + 15) & ~15ll;
-        }
-    long long groups = 0;
+    HMG_CUDA_TRY(cudaMemcpy(tr0.data(), h->tile_r0, sizeof(int) * nt, cudaMemcpyDeviceToHost));
+
+    // t_b cores (16 terms = 1 KB per group) after the X cores in the per-product B buffer
+    const long long xgroups = (h->n[1] + 7) / 8 + 4;
+    const long long xbytes = (xgroups * TC_XGROUP + 1023) & ~1023ll;
+    std::vector<long long> toff(nb, -1);
+    long long tgroups = 0;
+    JobList k1, k2;
+    std::vector<int> vlist;
+    std::vector<long long> voff;
+    long long vbytes = 0;
     for (int b = h->ndense; b < nb; b++) {
-        if (h->h_rank[b] == 0) continue;
-        toff[b] = groups;
-        groups += (h->h_rank[b] + 15) / 16;
-        farb.push_back(b);
+        const int r = h->h_rank[b];
+        if (r == 0) continue;
+        const int r16 = (r + 15) & ~15, rc = r16 / 8;
+        const int a = h->h_c0[b] & 7, kw = (a + h->h_m2[b] + 15) & ~15;
+        toff[b] = tgroups;
+        tgroups += r16 / 16;
+        vlist.push_back(b);
+        voff.push_back(vbytes);
+        k1.begin(TcJob{(int)toff[b], r16});
+        k1.add(vbytes, (long long)(h->h_c0[b] >> 3) * TC_XGROUP, rc, kw / 8, std::min(16, (192 / rc) & ~1), 0.25);
+        vbytes += (long long)r16 * kw * 2;
     }
-    cudaError_t ce = cudaMalloc(&h->tc_u, (size_t)std::max(bytes, 16ll));
-    if (ce != cudaSuccess) {
-        cudaGetLastError();
-        h->tc_u = nullptr;
-        set_error("hmg_build_bf16_factors: allocating %lld bytes failed: %s", bytes, cudaGetErrorString(ce));
-        return ce == cudaErrorMemoryAllocation ? HMG_ERR_NOMEM : HMG_ERR_CUDA;
+    // pass 2: per tile, its low-rank pairs (B = t_b) and near pairs (B = X)
+    std::vector<int> ulist, nlist, utile, ntile;
+    std::vector<long long> uoff, noff;
+    long long ubytes = 0;
+    bool all_tiles = true;
+    for (int t = 0; t < nt; t++) {
+        const int rc = ((ts[t] + 7) & ~7) / 8;
+        bool started = false;
+        for (int p = tps[t]; p < tps[t + 1]; p++) {
+            const int b = pblock[p];
+            const bool dense = b < h->ndense;
+            if (!dense && h->h_rank[b] == 0) continue;
+            if (!started) {
+                k2.begin(TcJob{tr0[t], ts[t]});
+                started = true;
+            }
+            if (dense) {
+                const int a = h->h_c0[b] & 7, kw = (a + h->h_m2[b] + 15) & ~15;
+                nlist.push_back(p);
+                ntile.push_back(t);
+                noff.push_back(ubytes);
+                k2.add(ubytes, (long long)(h->h_c0[b] >> 3) * TC_XGROUP, rc, kw / 8, 12, 0.25);
+                ubytes += (long long)rc * 8 * kw * 2;
+            } else {
+                const int r16 = (h->h_rank[b] + 15) & ~15;
+                ulist.push_back(p);
+                utile.push_back(t);
+                uoff.push_back(ubytes);
+                k2.add(ubytes, xbytes + toff[b] * 2 * TC_XGROUP, rc, r16 / 8, 12, 1.0);
+                ubytes += (long long)rc * 8 * r16 * 2;
+            }
+        }
+        all_tiles = all_tiles && started;
     }
-    if ((st = dalloc(&h->tc_uoff, (size_t)std::max(np, 1), s)) || (st = dalloc(&h->tc_toff, (size_t)std::max(nb, 1), s)) ||
-        (st = dalloc(&h->tc_pair_tile, (size_t)std::max(np, 1), s)) ||
-        (st = dalloc(&h->tc_far_blocks, std::max(farb.size(), (size_t)1), s)))
+
+    if (!steps_in_bounds(k1, vbytes, xbytes + tgroups * 2 * TC_XGROUP, tgroups, 0) ||
+        !steps_in_bounds(k2, ubytes, xbytes + tgroups * 2 * TC_XGROUP, h->n[0], 1)) {
+        set_error("hmg_build_bf16_factors: internal error: an operand step leaves its buffer");
+        return HMG_ERR_UNSUPPORTED;
+    }
+    if ((st = alloc_arena(&h->tc_u, ubytes, "the tile operands"))) return st;
+    if ((st = alloc_arena(&h->tc_v, vbytes, "the V^T operands"))) {
+        free_tc(h);
         return st;
-    if (np > 0) {
-        HMG_CUDA_TRY(cudaMemcpyAsync(h->tc_uoff, uoff.data(), sizeof(long long) * np, cudaMemcpyHostToDevice, s));
-        HMG_CUDA_TRY(cudaMemcpyAsync(h->tc_pair_tile, ptile.data(), sizeof(int) * np, cudaMemcpyHostToDevice, s));
     }
-    HMG_CUDA_TRY(cudaMemcpyAsync(h->tc_toff, toff.data(), sizeof(long long) * nb, cudaMemcpyHostToDevice, s));
-    if (!farb.empty())
-        HMG_CUDA_TRY(cudaMemcpyAsync(h->tc_far_blocks, farb.data(), sizeof(int) * farb.size(), cudaMemcpyHostToDevice, s));
-    if (np > 0) {
-        k_tc_u<<<np, 256, 0, s>>>(static_cast<const PairDesc*>(h->pair_desc), h->tc_pair_tile, h->tc_uoff, h->tile_s,
-                                  np, static_cast<__nv_bfloat16*>(h->tc_u));
+    int* dlist = nullptr;
+    int* dtile = nullptr;
+    long long* doff = nullptr;
+    auto convert = [&](const std::vector<int>& list, const std::vector<int>& tiles, const std::vector<long long>& off,
+                       int which) -> hmg_status {
+        const int n = (int)list.size();
+        if (n == 0) return HMG_OK;
+        hmg_status e;
+        if ((e = dalloc(&dlist, (size_t)n, s)) || (e = dalloc(&doff, (size_t)n, s)) ||
+            (!tiles.empty() && (e = dalloc(&dtile, (size_t)n, s))))
+            return e;
+        HMG_CUDA_TRY(cudaMemcpyAsync(dlist, list.data(), sizeof(int) * n, cudaMemcpyHostToDevice, s));
+        HMG_CUDA_TRY(cudaMemcpyAsync(doff, off.data(), sizeof(long long) * n, cudaMemcpyHostToDevice, s));
+        if (!tiles.empty())
+            HMG_CUDA_TRY(cudaMemcpyAsync(dtile, tiles.data(), sizeof(int) * n, cudaMemcpyHostToDevice, s));
+        const PairDesc* desc = static_cast<const PairDesc*>(h->pair_desc);
+        if (which == 0)
+            k_tc_u<<<n, 256, 0, s>>>(desc, dlist, doff, dtile, h->tile_s, n, static_cast<__nv_bfloat16*>(h->tc_u));
+        else if (which == 1)
+            k_tc_near<<<n, 256, 0, s>>>(desc, dlist, doff, dtile, h->tile_s, n, static_cast<__nv_bfloat16*>(h->tc_u));
+        else
+            k_tc_v<<<n, 256, 0, s>>>(dlist, doff, n, h->ptrV, h->rank, h->blk_c0, h->blk_m2,
+                                     static_cast<__nv_bfloat16*>(h->tc_v));
         HMG_LAUNCH_CHECK();
+        HMG_CUDA_TRY(cudaStreamSynchronize(s));
+        dfree(dlist, s);
+        dfree(doff, s);
+        dfree(dtile, s);
+        dlist = dtile = nullptr;
+        doff = nullptr;
+        return HMG_OK;
+    };
+    if ((st = convert(ulist, utile, uoff, 0)) || (st = convert(nlist, ntile, noff, 1)) ||
+        (st = convert(vlist, {}, voff, 2)) || (st = upload_jobs(h, 0, k1, 1024.0, grid)) ||
+        (st = upload_jobs(h, 1, k2, 4096.0, grid))) {
+        dfree(dlist, s);
+        dfree(doff, s);
+        dfree(dtile, s);
+        free_tc(h);
+        return st;
     }
-    HMG_CUDA_TRY(cudaStreamSynchronize(s));
-    h->tc_bytes = bytes;
-    h->tc_tgroups = groups;
-    h->tc_nfar = (int)farb.size();
+    h->tc_bytes = ubytes + vbytes;
+    h->tc_xbytes = xbytes;
+    h->tc_tbytes = tgroups * 2 * TC_XGROUP;
+    h->tc_grid = grid;
+    h->tc_all_tiles = all_tiles;
     h->tc_ready = true;
     return HMG_OK;
 }
@@ -355,48 +771,41 @@ hmg_status matvec_multi_tc(hmg_matrix* h, int nrhs, const double* X, int ldx, do
 {
     cudaStream_t s = h->stream;
     hmg_status st;
-    if ((st = ensure_desc(h, 4))) return st;
-    float* xm = nullptr;
-    __nv_bfloat16* tb = nullptr;
-    if ((st = dalloc(&xm, (size_t)h->n[1] * TC_N, s)) ||
-        (st = dalloc(&tb, (size_t)std::max(h->tc_tgroups, 1ll) * 16 * TC_N, s))) {
-        dfree(xm, s);
-        return st;
-    }
-    launch_gather_multi32(h, X, ldx, nrhs, xm);
-    if (h->tc_nfar > 0) {
-        float* tm = nullptr;
-        if ((st = dalloc(&tm, (size_t)(h->rank_total + 1) * TC_N, s))) {
-            dfree(xm, s);
-            dfree(tb, s);
-            return st;
-        }
-        st = launch_vtx_multi32(h, xm, tm);
-        if (!st) {
-            k_tc_t<<<h->tc_nfar, 256, 0, s>>>(h->tc_far_blocks, h->tc_nfar, h->rank, h->rank_off, h->tc_toff, tm, tb);
-            if (cudaGetLastError() != cudaSuccess) st = HMG_ERR_CUDA;
-        }
-        dfree(tm, s);
-        if (st) {
-            dfree(xm, s);
-            dfree(tb, s);
-            return st;
+    if (!h->tc_bbuf) {  // X and t_b cores, kept with the handle (sized by hmg_build_bf16_factors)
+        cudaError_t ce = cudaMalloc(&h->tc_bbuf, (size_t)(h->tc_xbytes + h->tc_tbytes));
+        if (ce != cudaSuccess) {
+            cudaGetLastError();
+            h->tc_bbuf = nullptr;
+            set_error("hmg_matvec_multi: allocating %lld bytes of operand space failed: %s",
+                      h->tc_xbytes + h->tc_tbytes, cudaGetErrorString(ce));
+            return ce == cudaErrorMemoryAllocation ? HMG_ERR_NOMEM : HMG_ERR_CUDA;
         }
     }
-    if ((st = launch_tile_multi32_dense(h, xm, nrhs, Y, ldy))) {
-        dfree(xm, s);
-        dfree(tb, s);
-        return st;
-    }
-    if (h->ntiles > 0 && h->tc_nfar > 0) {
-        HMG_CUDA_TRY(cudaFuncSetAttribute(k_tile_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(TcSmem)));
-        k_tile_tc<<<h->ntiles, 128, sizeof(TcSmem), s>>>(static_cast<const PairDesc*>(h->pair_desc), h->pair_block, h->tc_uoff,
-                                           static_cast<const char*>(h->tc_u), tb, h->tc_toff, h->tile_pair_start,
-                                           h->tile_r0, h->tile_s, h->perm[0], xm, nrhs, Y, ldy, h->dev_err);
+    char* bbuf = static_cast<char*>(h->tc_bbuf);
+    const long long xgroups = h->tc_xbytes / TC_XGROUP;
+    k_tc_x<<<(unsigned)((xgroups * TC_N + 255) / 256), 256, 0, s>>>(X, ldx, nrhs, h->perm[1], h->n[1], xgroups,
+                                                                      reinterpret_cast<uint4*>(bbuf));
+    HMG_LAUNCH_CHECK();
+    const size_t smem = sizeof(TcSmem);
+    HMG_CUDA_TRY(cudaFuncSetAttribute(k_tc_pass<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    HMG_CUDA_TRY(cudaFuncSetAttribute(k_tc_pass<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    if (h->tc_njobs[0] > 0) {
+        k_tc_pass<0><<<h->tc_grid, TC_THREADS, smem, s>>>(
+            reinterpret_cast<const TcStep*>(h->tc_steps[0]), reinterpret_cast<const TcJob*>(h->tc_jobs[0]),
+            reinterpret_cast<const int2*>(h->tc_cta[0]), static_cast<const char*>(h->tc_v), bbuf, h->tc_xbytes,
+            nullptr, 0, nullptr, 0, h->dev_err);
         HMG_LAUNCH_CHECK();
     }
-    dfree(xm, s);
-    dfree(tb, s);
+    // rows of tiles without products (all their blocks of rank 0) are zero
+    if (!h->tc_all_tiles)
+        HMG_CUDA_TRY(cudaMemset2DAsync(Y, sizeof(double) * ldy, 0, sizeof(double) * h->n[0], nrhs, s));
+    if (h->tc_njobs[1] > 0) {
+        k_tc_pass<1><<<h->tc_grid, TC_THREADS, smem, s>>>(
+            reinterpret_cast<const TcStep*>(h->tc_steps[1]), reinterpret_cast<const TcJob*>(h->tc_jobs[1]),
+            reinterpret_cast<const int2*>(h->tc_cta[1]), static_cast<const char*>(h->tc_u), bbuf, 0, h->perm[0], nrhs,
+            Y, ldy, h->dev_err);
+        HMG_LAUNCH_CHECK();
+    }
     return HMG_OK;
 }
 

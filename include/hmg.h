@@ -132,12 +132,13 @@ hmg_status hmg_full_matvec_rows(hmg_matrix* h, const double* x, const int* rows,
                                 double* y);
 
 /* Tensor-core products (no reference counterpart): converts the handle's FP32 low-rank
- * factors (hmg_precompute_aca with HMG_PREC_FP32, ranks <= 96) into a BF16 copy laid
- * out as tcgen05 operands.  Afterwards hmg_matvec_multi with 2..32 vectors and an FP32
- * stored near field runs the low-rank part on the tensor cores (U in BF16, t_b rounded
- * to BF16, FP32 accumulation) and the dense part on the CUDA cores in FP32; results
- * agree with the FP32 factors to ~1e-3 (BF16 rounding).  Single-vector products keep
- * using the FP32 factors.  Recomputing the factors drops the copy. */
+ * factors (hmg_precompute_aca with HMG_PREC_FP32, ranks <= 128) and its FP32 stored near
+ * field (hmg_precompute_dense with HMG_PREC_FP32) into BF16 copies laid out as tcgen05
+ * operands.  Afterwards hmg_matvec_multi with 2..32 vectors runs every product on the
+ * tensor cores: t_b = V_b^T X_b, U t_b and the near blocks times X, with BF16 operands
+ * (X and t_b rounded to BF16) and FP32 accumulation; results agree with the FP32
+ * products to ~1e-3 (BF16 rounding).  Single-vector products keep using the FP32
+ * storage.  Recomputing the factors or the near field drops the copies. */
 hmg_status hmg_build_bf16_factors(hmg_matrix* h);
 
 /* Write a set-up H-matrix to `path` (points, permutations, block list, ranks and

@@ -1,8 +1,8 @@
-"""Tensor-core multi-vector products (hmg_build_bf16_factors + hmg_matvec_multi): the
-low-rank part on tcgen05 with BF16 operands agrees with the FP32 CUDA-core product to
-the BF16 rounding of the factors and of t_b (relative 5e-3 per vector), is
-deterministic, and leaves single-vector products on the FP32 factors unchanged.  No
-reference counterpart."""
+"""Tensor-core multi-vector products (hmg_build_bf16_factors + hmg_matvec_multi): every
+product (V^T X, U t_b and the near field times X) on tcgen05 with BF16 operands agrees
+with the FP32 CUDA-core product to the BF16 rounding of factors, near field, X and t_b
+(relative 5e-3 per vector), is deterministic, writes every row of Y, and leaves
+single-vector products on the FP32 storage unchanged.  No reference counterpart."""
 import numpy as np
 import pytest
 
@@ -10,18 +10,25 @@ from helpers import engine, make_points, rel_err
 
 pytestmark = pytest.mark.gpu
 
+MATERN, GAUSS = 4, 3
 
-@pytest.mark.parametrize("case", [("uniform", 20000, 3, 128, 4, 0.2), ("gmm", 30000, 2, 64, 3, 0.05)],
-                         ids=["uniform3d-matern", "gmm2d-gauss"])
+
+@pytest.mark.parametrize("case", [
+    ("uniform", 20000, 3, 128, MATERN, 0.2, 64, 1e-6, 12),
+    ("gmm", 30000, 2, 64, GAUSS, 0.05, 64, 1e-6, 12),
+    # ranks up to 128 (two K chunks per low-rank pair) and tiles of at most 32 rows
+    ("uniform", 12000, 3, 32, MATERN, 0.2, 128, 1e-10, 32),
+    ("uniform", 9000, 2, 128, GAUSS, 0.1, 64, 1e-6, 2),
+], ids=["uniform3d-matern", "gmm2d-gauss", "rank128-leaf32", "two-vectors"])
 def test_tensor_core_products(hmg, cuda, case):
     torch = cuda
-    gen, n, dim, leaf, kind, param = case
+    gen, n, dim, leaf, kind, param, kmax, eps, nrhs = case
     p = make_points(gen, n, dim, 13)
     H = engine(hmg, p, p, 1.5, leaf, rule=1)
     H.set_kernel(kind, param, 0.0)
-    H.precompute_aca(64, 1e-6, hmg.PREC_FP32)
+    H.precompute_aca(kmax, eps, hmg.PREC_FP32)
     H.precompute_dense(hmg.PREC_FP32)
-    X = torch.from_numpy(np.random.default_rng(3).uniform(-1, 1, (12, n))).cuda()
+    X = torch.from_numpy(np.random.default_rng(3).uniform(-1, 1, (nrhs, n))).cuda()
     Y32 = torch.empty_like(X)
     H.matvec_multi(X, Y32)
     y1 = H.matvec(X[0].cpu().numpy())
@@ -31,11 +38,37 @@ def test_tensor_core_products(hmg, cuda, case):
     H.synchronize()
     a, b = Ytc.cpu().numpy(), Y32.cpu().numpy()
     assert np.isfinite(a).all()
-    for j in range(X.shape[0]):
+    for j in range(nrhs):
         assert rel_err(a[j], b[j]) < 5e-3, (j, rel_err(a[j], b[j]))
     Y2 = torch.empty_like(X)
     H.matvec_multi(X, Y2)
     H.synchronize()
     np.testing.assert_array_equal(Y2.cpu().numpy(), a)
     np.testing.assert_array_equal(H.matvec(X[0].cpu().numpy()), y1)
+    if kmax == 128:
+        assert H.info()["max_rank"] > 96  # the two-chunk path ran
+    H.close()
+
+
+def test_copies_follow_the_storage(hmg, cuda):
+    """Recomputing the near field drops the BF16 copies (products fall back to the
+    FP32 CUDA-core kernels); a handle without an FP32 stored near field is refused."""
+    torch = cuda
+    p = make_points("uniform", 8000, 3, 5)
+    H = engine(hmg, p, p, 1.5, 64, rule=1)
+    H.set_kernel(MATERN, 0.2, 0.0)
+    H.precompute_aca(64, 1e-6, hmg.PREC_FP32)
+    with pytest.raises(hmg.HmgError):
+        H.build_bf16_factors()  # near field not stored
+    H.precompute_dense(hmg.PREC_FP32)
+    H.build_bf16_factors()
+    X = torch.from_numpy(np.random.default_rng(4).uniform(-1, 1, (4, 8000))).cuda()
+    Ytc, Y32 = torch.empty_like(X), torch.empty_like(X)
+    H.matvec_multi(X, Ytc)
+    H.precompute_dense(hmg.PREC_FP32)  # drops the copies
+    H.matvec_multi(X, Y32)
+    H.synchronize()
+    ref = np.stack([H.matvec(X[j].cpu().numpy()) for j in range(4)])
+    assert max(rel_err(Y32.cpu().numpy()[j], ref[j]) for j in range(4)) < 1e-6
+    assert 1e-6 < max(rel_err(Ytc.cpu().numpy()[j], ref[j]) for j in range(4)) < 5e-3
     H.close()
