@@ -91,6 +91,7 @@ struct hmg_matrix {
     char* tc_steps[2] = {nullptr, nullptr};   // per pass: steps, CTA by CTA
     char* tc_jobs[2] = {nullptr, nullptr};    // per pass: jobs, CTA by CTA
     char* tc_cta[2] = {nullptr, nullptr};     // per CTA: first job and step (int2), then the ends
+    int* tc_kmap = nullptr;                   // pass 1: per stack, t_b destination of its 16 K cores
     int tc_njobs[2] = {0, 0};
     int tc_grid = 0;
     bool tc_all_tiles = false;                // every row tile has a pass-2 job

@@ -13,8 +13,8 @@
 //
 // Both passes run one persistent kernel: one CTA per SM walks a job list balanced on
 // the host (longest job first onto the least loaded CTA).  A job (a block in pass 1, a
-// tile in pass 2) is a run of "steps", each an A chunk (<= 24 KB) and the B chunk it
-// multiplies (<= 8 KB).  Warp 4 copies steps with bulk copies (cp.async.bulk,
+// tile in pass 2) is a run of "steps", each an A chunk (<= 48 KB) and the B chunk it
+// multiplies (<= 16 KB).  Warp 4 copies steps with bulk copies (cp.async.bulk,
 // completion counted on the step slot's mbarrier) into a 208 KB byte ring that holds up
 // to 16 steps of any size; warp 5 issues the MMAs (one elected lane, accumulating in one
 // of two 32-column tensor-memory buffers) and frees each step's bytes with
@@ -55,8 +55,9 @@ static constexpr int TC_MAXR16 = 128;      // largest rank rounded to 16 (pass 1
 static constexpr int TC_SLOTS = 16;        // steps in flight per CTA at most
 static constexpr int TC_RING = 212992;     // bytes of the operand ring (208 KB)
 static constexpr int TC_ISSUERS = 8;       // lanes of the copy warp issuing at once
-static constexpr int TC_ABYTES = 24576;    // A chunk of a step: at most 192 core matrices
-static constexpr int TC_BBYTES = 8192;     // B chunk: at most 16 K cores x 4 vector cores
+static constexpr int TC_ABYTES = 49152;    // A chunk of a step: at most 384 core matrices
+static constexpr int TC_BBYTES = 16384;    // B chunk: at most 32 K cores x 4 vector cores
+static constexpr int TC_MAXKS = 16;        // MMAs per step
 static constexpr int TC_THREADS = 192;     // warps 0-3 epilogue, 4 copies, 5 MMAs
 static constexpr int TC_XGROUP = 512;      // bytes of one K core of X or t_b (4 vector cores)
 
@@ -117,23 +118,26 @@ __global__ void k_tc_near(const PairDesc* desc, const int* plist, const long lon
     }
 }
 
-// admissible block: V_b^T (rows of m2p FP32 entries per term) -> A cores, rc = r16 / 8
-__global__ void k_tc_v(const int* blist, const long long* voff, int n, void* const* ptrV, const int* rank,
-                       const int* blk_c0, const int* blk_m2, __nv_bfloat16* out)
+// admissible block: V_b^T (rows of m2p FP32 entries per term) -> its rows of a stack's A
+// cores.  A stack holds the V^T of blocks with the same columns, one under the other
+// (vaux: stack row cores << 8 | the block's first row core in the stack).
+__global__ void k_tc_v(const int* blist, const long long* voff, const int* vaux, int n, void* const* ptrV,
+                       const int* rank, const int* blk_c0, const int* blk_m2, __nv_bfloat16* out)
 {
     const int u = blockIdx.x;
     if (u >= n) return;
-    const int b = blist[u];
+    const int b = blist[u], rc = vaux[u] >> 8, off8 = vaux[u] & 255;
     const int r = rank[b], r16 = (r + 15) & ~15, m2 = blk_m2[b], m2p = (m2 + 3) & ~3;
     const int a = blk_c0[b] & 7, kw = (a + m2 + 15) & ~15;
     const float* V = static_cast<const float*>(ptrV[b]);
     __nv_bfloat16* dst = out + voff[u] / 2;
-    const int rc = r16 / 8;
+    const int rb = r16 / 8;
     for (long long idx = threadIdx.x; idx < (long long)r16 * kw; idx += blockDim.x) {
         const int core = (int)(idx >> 6), e = (int)(idx & 63);
-        const int kc = core / rc, mc = core - kc * rc;
+        const int kc = core / rb, mc = core - kc * rb;
         const int m = mc * 8 + (e >> 3), c = kc * 8 + (e & 7) - a;
-        dst[idx] = __float2bfloat16_rn((m < r && c >= 0 && c < m2) ? V[(size_t)m * m2p + c] : 0.0f);
+        dst[((size_t)kc * rc + off8 + mc) * 64 + e] =
+            __float2bfloat16_rn((m < r && c >= 0 && c < m2) ? V[(size_t)m * m2p + c] : 0.0f);
     }
 }
 
@@ -241,11 +245,12 @@ __device__ __forceinline__ uint32_t pack_bf16(float lo, float hi)
 }
 
 // Steps of CTA c: [cta[c].y, cta[c+1].y); its jobs: [cta[c].x, cta[c+1].x).
-// Pass 1 (MODE 0) writes t_b cores at Bbuf + tb_off; pass 2 (MODE 1) writes rows of Y.
+// Pass 1 (MODE 0) writes t_b cores at Bbuf + tb_off, K core kc of job j (a stack) to 512-byte
+// unit map[16 j + kc]; pass 2 (MODE 1) writes rows of Y, tile row i to Y row map[r0 + i].
 template <int MODE>
 __global__ void __launch_bounds__(TC_THREADS, 1)
     k_tc_pass(const TcStep* __restrict__ steps, const TcJob* __restrict__ jobs, const int2* __restrict__ cta,
-              const char* __restrict__ A, char* Bbuf, long long tb_off, const int* __restrict__ perm0, int nrhs,
+              const char* __restrict__ A, char* Bbuf, long long tb_off, const int* __restrict__ map, int nrhs,
               double* Y, int ldy, int* err)
 {
     extern __shared__ __align__(1024) unsigned char tc_raw[];
@@ -366,11 +371,13 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                 const uint32_t a0 = sm.slot_a[slot], b0 = sm.slot_b[slot];
                 const int meta = sm.slot_meta[slot], ks = meta >> 16;
                 const bool first = meta & 256, last = meta & 512;
-                if (first && jc >= 2 && !mbar_wait(&sm.acce[buf], ((jc >> 1) - 1) & 1, err, 13)) {
-                    *fail = 1;
-                    break;
+                if (first && jc >= 2) {  // the epilogue has read this accumulator's previous job
+                    if (!mbar_wait(&sm.acce[buf], ((jc >> 1) - 1) & 1, err, 13)) {
+                        *fail = 1;
+                        break;
+                    }
+                    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
                 }
-                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
                 const uint32_t lbo = (uint32_t)(meta & 0xff) * 128u;
                 const uint32_t d = tmem + (uint32_t)(buf * TC_N);
                 for (int q = 0; q < ks; q++) {
@@ -403,7 +410,12 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                 const int jc = j0 + k, buf = jc & 1;
                 const int row = warp * 32 + lane;
                 // pass 2: this row's place in Y, fetched before the wait
-                const int yrow = (MODE == 1 && row < rows) ? perm0[r0 + row] : 0;
+                const int yrow = (MODE == 1 && row < rows) ? map[r0 + row] : 0;
+                int tdst[4];
+                if (MODE == 0) {
+#pragma unroll
+                    for (int q = 0; q < 4; q++) tdst[q] = warp * 4 + q < (rows >> 3) ? map[r0 * 16 + warp * 4 + q] : 0;
+                }
                 ok = !*fail && mbar_wait(&sm.accf[buf], (jc >> 1) & 1, err, 16);
                 if (!__all_sync(~0u, ok)) {
                     ok = false;
@@ -435,8 +447,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                     }
                 } else {
                     // term row -> B cores of pass 2 (K = term): element (term m, vector q) at byte
-                    // ((m / 8) * 4 + q / 8) * 128 + (q % 8) * 16 + (m % 8) * 2; this warp's 32 terms
-                    // fill K cores 4w..4w+3.  Lanes 2p, 2p+1 pair their terms into 32-bit words
+                    // ((m / 8) * 4 + q / 8) * 128 + (q % 8) * 16 + (m % 8) * 2 of its block's t_b;
+                    // this warp's 32 stack rows fill the stack's K cores 4w..4w+3.  Lanes 2p, 2p+1 pair their terms into 32-bit words
                     // (even lane: vector 2t, odd lane: vector 2t+1); 16-byte row u of the staging
                     // sits at u ^ (2 (u / 32)), which spreads the four K cores over all banks.
                     uint32_t* stg = reinterpret_cast<uint32_t*>(sm.stg[warp]);
@@ -451,12 +463,12 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                         stg[(u ^ ((u >> 5) * 2)) * 4 + ((lane & 7) >> 1)] = w;
                     }
                     __syncwarp();
-                    uint4* dst = reinterpret_cast<uint4*>(Bbuf + tb_off + (size_t)r0 * 1024);
+                    uint4* dst = reinterpret_cast<uint4*>(Bbuf + tb_off);
                     const uint4* src = reinterpret_cast<const uint4*>(stg);
 #pragma unroll
                     for (int q = 0; q < 4; q++) {
                         const int u = q * 32 + lane;
-                        if (warp * 4 + q < (rows >> 3)) dst[(warp * 4 + q) * 32 + lane] = src[u ^ (q * 2)];
+                        if (warp * 4 + q < (rows >> 3)) dst[(size_t)tdst[q] * 32 + lane] = src[u ^ (q * 2)];
                     }
                     __syncwarp();
                 }
@@ -493,6 +505,7 @@ void free_tc(hmg_matrix* h)
         cudaFree(h->tc_bbuf);
     }
     h->tc_u = h->tc_v = h->tc_bbuf = nullptr;
+    dfree(h->tc_kmap, s);
     for (int q = 0; q < 2; q++) {
         dfree(h->tc_steps[q], s);
         dfree(h->tc_jobs[q], s);
@@ -541,14 +554,14 @@ bool steps_in_bounds(const JobList& L, long long abytes, long long bbytes, long 
 {
     for (const TcStep& st : L.steps) {
         const long long rc = st.meta & 0xff, ab = (long long)st.ksteps * 2 * rc * 128, bb = (long long)st.ksteps * 1024;
-        if (st.ksteps < 1 || st.ksteps > 8 || rc < 1 || rc > 16 || ab > TC_ABYTES || bb > TC_BBYTES ||
+        if (st.ksteps < 1 || st.ksteps > TC_MAXKS || rc < 1 || rc > 16 || ab > TC_ABYTES || bb > TC_BBYTES ||
             st.a_off < 0 || st.a_off % 16 || st.a_off + ab > abytes || st.b_off < 0 || st.b_off % 16 ||
             st.b_off + bb > bbytes)
             return false;
     }
     for (const TcJob& j : L.info) {
         if (j.rows < 1 || j.rows > 128 || j.r0 < 0) return false;
-        if (q == 1 ? (long long)j.r0 + j.rows > out_limit : (long long)j.r0 + j.rows / 16 > out_limit) return false;
+        if (q == 1 ? (long long)j.r0 + j.rows > out_limit : j.r0 >= out_limit) return false;
     }
     return true;
 }
@@ -656,21 +669,58 @@ hmg_status build_bf16_factors(hmg_matrix* h)
     std::vector<long long> toff(nb, -1);
     long long tgroups = 0;
     JobList k1, k2;
-    std::vector<int> vlist;
+    // pass 1 jobs: stacks of the V^T of blocks with the same columns (one X chunk, one
+    // MMA sequence for all of them), at most 128 terms, largest ranks first
+    std::vector<int> vlist, vaux, kmap;
     std::vector<long long> voff;
     long long vbytes = 0;
-    for (int b = h->ndense; b < nb; b++) {
-        const int r = h->h_rank[b];
-        if (r == 0) continue;
-        const int r16 = (r + 15) & ~15, rc = r16 / 8;
-        const int a = h->h_c0[b] & 7, kw = (a + h->h_m2[b] + 15) & ~15;
-        toff[b] = tgroups;
-        tgroups += r16 / 16;
-        vlist.push_back(b);
-        voff.push_back(vbytes);
-        k1.begin(TcJob{(int)toff[b], r16});
-        k1.add(vbytes, (long long)(h->h_c0[b] >> 3) * TC_XGROUP, rc, kw / 8, std::min(16, (192 / rc) & ~1), 0.25);
-        vbytes += (long long)r16 * kw * 2;
+    {
+        std::vector<int> far;
+        for (int b = h->ndense; b < nb; b++)
+            if (h->h_rank[b] > 0) far.push_back(b);
+        std::stable_sort(far.begin(), far.end(), [&](int x, int y) {
+            if (h->h_c0[x] != h->h_c0[y]) return h->h_c0[x] < h->h_c0[y];
+            if (h->h_m2[x] != h->h_m2[y]) return h->h_m2[x] < h->h_m2[y];
+            return h->h_rank[x] > h->h_rank[y];
+        });
+        for (size_t g0 = 0; g0 < far.size();) {
+            size_t g1 = g0;
+            while (g1 < far.size() && h->h_c0[far[g1]] == h->h_c0[far[g0]] && h->h_m2[far[g1]] == h->h_m2[far[g0]]) g1++;
+            std::vector<std::vector<int>> stacks;
+            std::vector<int> fill;
+            for (size_t i = g0; i < g1; i++) {  // first fit, ranks decreasing
+                const int b = far[i], r16 = (h->h_rank[b] + 15) & ~15;
+                size_t k = 0;
+                while (k < stacks.size() && fill[k] + r16 > 128) k++;
+                if (k == stacks.size()) {
+                    stacks.emplace_back();
+                    fill.push_back(0);
+                }
+                stacks[k].push_back(b);
+                fill[k] += r16;
+            }
+            const int c0 = h->h_c0[far[g0]], kw = ((c0 & 7) + h->h_m2[far[g0]] + 15) & ~15;
+            for (size_t k = 0; k < stacks.size(); k++) {
+                const int rows = fill[k], rc = rows / 8, job = (int)(kmap.size() / 16);
+                kmap.resize(kmap.size() + 16, 0);
+                int off8 = 0;
+                for (int b : stacks[k]) {
+                    const int r16 = (h->h_rank[b] + 15) & ~15;
+                    toff[b] = tgroups;
+                    for (int kc = 0; kc < r16 / 8; kc++) kmap[job * 16 + off8 + kc] = (int)(tgroups * 2 + kc);
+                    tgroups += r16 / 16;
+                    vlist.push_back(b);
+                    voff.push_back(vbytes);
+                    vaux.push_back(rc << 8 | off8);
+                    off8 += r16 / 8;
+                }
+                k1.begin(TcJob{job, rows});
+                k1.add(vbytes, (long long)(c0 >> 3) * TC_XGROUP, rc, kw / 8, std::min(2 * TC_MAXKS, (TC_ABYTES / 128 / rc) & ~1),
+                       0.25);
+                vbytes += (long long)rows * kw * 2;
+            }
+            g0 = g1;
+        }
     }
     // pass 2: per tile, its low-rank pairs (B = t_b) and near pairs (B = X)
     std::vector<int> ulist, nlist, utile, ntile;
@@ -693,26 +743,37 @@ hmg_status build_bf16_factors(hmg_matrix* h)
                 nlist.push_back(p);
                 ntile.push_back(t);
                 noff.push_back(ubytes);
-                k2.add(ubytes, (long long)(h->h_c0[b] >> 3) * TC_XGROUP, rc, kw / 8, 12, 0.25);
+                k2.add(ubytes, (long long)(h->h_c0[b] >> 3) * TC_XGROUP, rc, kw / 8, TC_ABYTES / 128 / 16, 0.25);
                 ubytes += (long long)rc * 8 * kw * 2;
             } else {
                 const int r16 = (h->h_rank[b] + 15) & ~15;
                 ulist.push_back(p);
                 utile.push_back(t);
                 uoff.push_back(ubytes);
-                k2.add(ubytes, xbytes + toff[b] * 2 * TC_XGROUP, rc, r16 / 8, 12, 1.0);
+                k2.add(ubytes, xbytes + toff[b] * 2 * TC_XGROUP, rc, r16 / 8, TC_ABYTES / 128 / 16, 1.0);
                 ubytes += (long long)rc * 8 * r16 * 2;
             }
         }
         all_tiles = all_tiles && started;
     }
 
-    if (!steps_in_bounds(k1, vbytes, xbytes + tgroups * 2 * TC_XGROUP, tgroups, 0) ||
+    if (!steps_in_bounds(k1, vbytes, xbytes + tgroups * 2 * TC_XGROUP, (long long)kmap.size() / 16, 0) ||
         !steps_in_bounds(k2, ubytes, xbytes + tgroups * 2 * TC_XGROUP, h->n[0], 1)) {
         set_error("hmg_build_bf16_factors: internal error: an operand step leaves its buffer");
         return HMG_ERR_UNSUPPORTED;
     }
+    for (int v : kmap)
+        if (v < 0 || v >= tgroups * 2) {
+            set_error("hmg_build_bf16_factors: internal error: a t_b core lies outside its buffer");
+            return HMG_ERR_UNSUPPORTED;
+        }
     if ((st = alloc_arena(&h->tc_u, ubytes, "the tile operands"))) return st;
+    if ((st = dalloc(&h->tc_kmap, std::max(kmap.size(), (size_t)1), s))) {
+        free_tc(h);
+        return st;
+    }
+    if (!kmap.empty())
+        HMG_CUDA_TRY(cudaMemcpyAsync(h->tc_kmap, kmap.data(), sizeof(int) * kmap.size(), cudaMemcpyHostToDevice, s));
     if ((st = alloc_arena(&h->tc_v, vbytes, "the V^T operands"))) {
         free_tc(h);
         return st;
@@ -738,7 +799,7 @@ hmg_status build_bf16_factors(hmg_matrix* h)
         else if (which == 1)
             k_tc_near<<<n, 256, 0, s>>>(desc, dlist, doff, dtile, h->tile_s, n, static_cast<__nv_bfloat16*>(h->tc_u));
         else
-            k_tc_v<<<n, 256, 0, s>>>(dlist, doff, n, h->ptrV, h->rank, h->blk_c0, h->blk_m2,
+            k_tc_v<<<n, 256, 0, s>>>(dlist, doff, dtile, n, h->ptrV, h->rank, h->blk_c0, h->blk_m2,
                                      static_cast<__nv_bfloat16*>(h->tc_v));
         HMG_LAUNCH_CHECK();
         HMG_CUDA_TRY(cudaStreamSynchronize(s));
@@ -750,7 +811,7 @@ hmg_status build_bf16_factors(hmg_matrix* h)
         return HMG_OK;
     };
     if ((st = convert(ulist, utile, uoff, 0)) || (st = convert(nlist, ntile, noff, 1)) ||
-        (st = convert(vlist, {}, voff, 2)) || (st = upload_jobs(h, 0, k1, 1024.0, grid)) ||
+        (st = convert(vlist, vaux, voff, 2)) || (st = upload_jobs(h, 0, k1, 1024.0, grid)) ||
         (st = upload_jobs(h, 1, k2, 4096.0, grid))) {
         dfree(dlist, s);
         dfree(doff, s);
@@ -793,7 +854,7 @@ hmg_status matvec_multi_tc(hmg_matrix* h, int nrhs, const double* X, int ldx, do
         k_tc_pass<0><<<h->tc_grid, TC_THREADS, smem, s>>>(
             reinterpret_cast<const TcStep*>(h->tc_steps[0]), reinterpret_cast<const TcJob*>(h->tc_jobs[0]),
             reinterpret_cast<const int2*>(h->tc_cta[0]), static_cast<const char*>(h->tc_v), bbuf, h->tc_xbytes,
-            nullptr, 0, nullptr, 0, h->dev_err);
+            h->tc_kmap, 0, nullptr, 0, h->dev_err);
         HMG_LAUNCH_CHECK();
     }
     // rows of tiles without products (all their blocks of rank 0) are zero
