@@ -56,18 +56,22 @@ static constexpr int TC_SLOTS = 16;        // steps in flight per CTA at most
 static constexpr int TC_RING = 212992;     // bytes of the operand ring (208 KB)
 static constexpr int TC_ISSUERS = 8;       // lanes of the copy warp issuing at once
 static constexpr int TC_ABYTES = 49152;    // A chunk of a step: at most 384 core matrices
-static constexpr int TC_BBYTES = 16384;    // B chunk: at most 32 K cores x 4 vector cores
-static constexpr int TC_MAXKS = 16;        // MMAs per step
+static constexpr int TC_BBYTES = 24576;    // B chunks of a step: at most 48 K cores x 4 vector cores
+static constexpr int TC_MAXKS = 16;        // MMAs per sub-step
+static constexpr int TC_MAXSUB = 4;        // sub-steps (B copies) per step
 static constexpr int TC_THREADS = 192;     // warps 0-3 epilogue, 4 copies, 5 MMAs
 static constexpr int TC_XGROUP = 512;      // bytes of one K core of X or t_b (4 vector cores)
 
+// A step: one copy of A (the A chunks of up to TC_MAXSUB sub-steps, one after another in
+// the A arena) and one copy of B per sub-step (X or t_b cores), placed after A in the ring.
 struct TcStep {
-    long long a_off;  // bytes into the A arena
-    long long b_off;  // bytes into the B buffer (X cores, then t_b cores)
-    int ksteps;       // MMAs of K = 16 (two K cores each)
-    int meta;         // bits 0-7: row cores of A (its K-core stride / 128); bit 8: first step of a job; bit 9: last
+    long long a_off;               // bytes into the A arena
+    long long b_off[TC_MAXSUB];    // bytes into the B buffer (X cores, then t_b cores), per sub-step
+    int meta;                      // bits 0-7: row cores of A (its K-core stride / 128); bit 8: first step
+                                   // of a job; bit 9: last; bits 10-11: sub-steps - 1; bits 16-23: MMAs
+    int kss;                       // MMAs (of K = 16) of sub-step j, minus 1, in bits 4j..4j+3
 };
-static_assert(sizeof(TcStep) == 24, "TcStep layout");
+static_assert(sizeof(TcStep) == 48, "TcStep layout");
 
 struct TcJob {
     int r0;    // pass 2: first Z row of the tile; pass 1: t_b's first 16-term group
@@ -184,7 +188,7 @@ struct TcSmem {
                                    // the MMA's reads of unused A rows past the ring's end)
     uint64_t full[TC_SLOTS], empty[TC_SLOTS], accf[2], acce[2], fin;
     uint32_t slot_a[TC_SLOTS], slot_b[TC_SLOTS];  // shared addresses of a step's A and B
-    int slot_meta[TC_SLOTS];                       // a step's meta word, MMAs in bits 16+
+    int slot_meta[TC_SLOTS], slot_kss[TC_SLOTS];   // a step's meta and sub-step words
     int slot_pos[TC_SLOTS];                        // ring offset of a step (copy warp only)
     int step_bytes[32];                            // bytes of the copy warp's current 32 steps
     uint32_t tmem;
@@ -296,7 +300,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
             const TcStep mine = nxt;
             nxt = load_step(my_steps, i0 + 32 + lane, nsteps);
             const int cnt = min(32, nsteps - i0);
-            const int ab = mine.ksteps * 2 * (mine.meta & 0xff) * 128, bb = mine.ksteps * 1024;
+            const int ks_all = (mine.meta >> 16) & 0xff;
+            const int ab = ks_all * 2 * (mine.meta & 0xff) * 128, bb = ks_all * 1024;
             __syncwarp();
             sm.step_bytes[lane] = ab + bb;
             __syncwarp();
@@ -344,10 +349,19 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                     const uint32_t a = smem_u32(sm.ring + pos);
                     sm.slot_a[slot] = a;
                     sm.slot_b[slot] = a + ab;
-                    sm.slot_meta[slot] = mine.meta | (mine.ksteps << 16);
+                    sm.slot_meta[slot] = mine.meta;
+                    sm.slot_kss[slot] = mine.kss;
                     mbar_arrive_expect_tx(&sm.full[slot], ab + bb);
                     bulk_g2s_first(sm.ring + pos, A + mine.a_off, ab, &sm.full[slot], pol);
-                    bulk_g2s(sm.ring + pos + ab, Bbuf + mine.b_off, bb, &sm.full[slot]);
+                    const int nsub = ((mine.meta >> 10) & 3) + 1;
+                    int boff = ab;
+#pragma unroll
+                    for (int j = 0; j < TC_MAXSUB; j++)
+                        if (j < nsub) {
+                            const int kb = (((mine.kss >> (4 * j)) & 15) + 1) * 1024;
+                            bulk_g2s(sm.ring + pos + boff, Bbuf + mine.b_off[j], kb, &sm.full[slot]);
+                            boff += kb;
+                        }
                 }
                 k += m;
             }
@@ -368,8 +382,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                     *fail = 1;
                     break;
                 }
-                const uint32_t a0 = sm.slot_a[slot], b0 = sm.slot_b[slot];
-                const int meta = sm.slot_meta[slot], ks = meta >> 16;
+                uint32_t a0 = sm.slot_a[slot], b0 = sm.slot_b[slot];
+                const int meta = sm.slot_meta[slot], kss = sm.slot_kss[slot], nsub = ((meta >> 10) & 3) + 1;
                 const bool first = meta & 256, last = meta & 512;
                 if (first && jc >= 2) {  // the epilogue has read this accumulator's previous job
                     if (!mbar_wait(&sm.acce[buf], ((jc >> 1) - 1) & 1, err, 13)) {
@@ -380,10 +394,15 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                 }
                 const uint32_t lbo = (uint32_t)(meta & 0xff) * 128u;
                 const uint32_t d = tmem + (uint32_t)(buf * TC_N);
-                for (int q = 0; q < ks; q++) {
-                    const uint64_t ad = smem_desc(a0 + q * 2 * lbo, lbo, 128);
-                    const uint64_t bd = smem_desc(b0 + q * 1024, TC_XGROUP, 128);
-                    tc_mma(d, ad, bd, (first && q == 0) ? 0u : 1u);
+                for (int j = 0; j < nsub; j++) {
+                    const int ks = ((kss >> (4 * j)) & 15) + 1;
+                    for (int q = 0; q < ks; q++) {
+                        const uint64_t ad = smem_desc(a0 + q * 2 * lbo, lbo, 128);
+                        const uint64_t bd = smem_desc(b0 + q * 1024, TC_XGROUP, 128);
+                        tc_mma(d, ad, bd, (first && j == 0 && q == 0) ? 0u : 1u);
+                    }
+                    a0 += ks * 2 * lbo;
+                    b0 += ks * 1024;
                 }
                 tc_commit(&sm.empty[slot]);
                 if (last) {
@@ -521,14 +540,21 @@ void free_tc(hmg_matrix* h)
 
 namespace {
 
+struct Chunk {
+    long long a_off, b_off;  // A arena, B buffer
+    int ks, rc;              // MMAs; row cores of A
+};
+
 struct JobList {
-    std::vector<TcStep> steps;   // in job order
-    std::vector<int> step0;      // per job: first step (then end)
+    std::vector<Chunk> chunks;   // in job order
+    std::vector<int> chunk0;     // per job: first chunk (then the end)
     std::vector<TcJob> info;
     std::vector<double> cost;
+    std::vector<TcStep> steps;   // built by make_steps, in job order
+    std::vector<int> step0;
     void begin(TcJob j)
     {
-        step0.push_back((int)steps.size());
+        chunk0.push_back((int)chunks.size());
         info.push_back(j);
         cost.push_back(0.0);
     }
@@ -537,14 +563,49 @@ struct JobList {
     {
         for (int kc0 = 0; kc0 < kcores; kc0 += kcc) {
             const int nk = std::min(kcc, kcores - kc0);
-            TcStep st;
-            st.a_off = a_off + (long long)kc0 * rc * 128;
-            st.b_off = b_off + (long long)kc0 * TC_XGROUP;
-            st.ksteps = nk / 2;
-            st.meta = rc;
-            steps.push_back(st);
+            chunks.push_back(Chunk{a_off + (long long)kc0 * rc * 128, b_off + (long long)kc0 * TC_XGROUP, nk / 2, rc});
             cost.back() += (double)nk * rc * 128 + b_weight * nk * TC_XGROUP;
         }
+    }
+    // Steps of every job: consecutive chunks share a step (merge) while their A chunks
+    // are adjacent and the step stays within TC_MAXSUB sub-steps, TC_ABYTES and TC_BBYTES.
+    void make_steps(bool merge)
+    {
+        chunk0.push_back((int)chunks.size());
+        for (size_t j = 0; j + 1 < chunk0.size(); j++) {
+            step0.push_back((int)steps.size());
+            TcStep cur{};
+            int nsub = 0, ks_all = 0;
+            long long ab = 0;
+            auto flush = [&]() {
+                if (!nsub) return;
+                cur.meta |= (nsub - 1) << 10 | ks_all << 16;
+                steps.push_back(cur);
+                cur = TcStep{};
+                nsub = ks_all = 0;
+                ab = 0;
+            };
+            for (int c = chunk0[j]; c < chunk0[j + 1]; c++) {
+                const Chunk& k = chunks[c];
+                const long long kab = (long long)k.ks * 2 * k.rc * 128;
+                if (!(merge && nsub > 0 && nsub < TC_MAXSUB && k.rc == (cur.meta & 0xff) && k.a_off == cur.a_off + ab &&
+                      ab + kab <= TC_ABYTES && (ks_all + k.ks) * 1024 <= TC_BBYTES))
+                    flush();
+                if (!nsub) {
+                    cur.a_off = k.a_off;
+                    cur.meta = k.rc;
+                }
+                cur.b_off[nsub] = k.b_off;
+                cur.kss |= (k.ks - 1) << (4 * nsub);
+                nsub++;
+                ks_all += k.ks;
+                ab += kab;
+            }
+            flush();
+            steps[step0.back()].meta |= 256;
+            steps.back().meta |= 512;
+        }
+        step0.push_back((int)steps.size());
     }
 };
 
@@ -553,10 +614,16 @@ struct JobList {
 bool steps_in_bounds(const JobList& L, long long abytes, long long bbytes, long long out_limit, int q)
 {
     for (const TcStep& st : L.steps) {
-        const long long rc = st.meta & 0xff, ab = (long long)st.ksteps * 2 * rc * 128, bb = (long long)st.ksteps * 1024;
-        if (st.ksteps < 1 || st.ksteps > TC_MAXKS || rc < 1 || rc > 16 || ab > TC_ABYTES || bb > TC_BBYTES ||
-            st.a_off < 0 || st.a_off % 16 || st.a_off + ab > abytes || st.b_off < 0 || st.b_off % 16 ||
-            st.b_off + bb > bbytes)
+        const int rc = st.meta & 0xff, nsub = ((st.meta >> 10) & 3) + 1, ks_all = (st.meta >> 16) & 0xff;
+        const long long ab = (long long)ks_all * 2 * rc * 128, bb = (long long)ks_all * 1024;
+        int sum = 0;
+        for (int j = 0; j < nsub; j++) {
+            const int ks = ((st.kss >> (4 * j)) & 15) + 1;
+            if (st.b_off[j] < 0 || st.b_off[j] % 16 || st.b_off[j] + ks * 1024ll > bbytes) return false;
+            sum += ks;
+        }
+        if (sum != ks_all || rc < 1 || rc > 16 || ab > TC_ABYTES || bb > TC_BBYTES || st.a_off < 0 || st.a_off % 16 ||
+            st.a_off + ab > abytes)
             return false;
     }
     for (const TcJob& j : L.info) {
@@ -571,7 +638,6 @@ hmg_status upload_jobs(hmg_matrix* h, int q, JobList& L, double job_cost, int gr
 {
     cudaStream_t s = h->stream;
     const int nj = (int)L.info.size();
-    L.step0.push_back((int)L.steps.size());
     std::vector<int> order(nj);
     for (int j = 0; j < nj; j++) order[j] = j;
     std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return L.cost[a] > L.cost[b]; });
@@ -595,12 +661,7 @@ hmg_status upload_jobs(hmg_matrix* h, int q, JobList& L, double job_cost, int gr
         for (int j : mine[c]) {
             jobs.push_back(L.info[j]);
             const int a = L.step0[j], b = L.step0[j + 1];
-            for (int i = a; i < b; i++) {
-                TcStep st = L.steps[i];
-                if (i == a) st.meta |= 256;
-                if (i == b - 1) st.meta |= 512;
-                steps.push_back(st);
-            }
+            for (int i = a; i < b; i++) steps.push_back(L.steps[i]);
         }
     }
     cta[grid] = make_int2((int)jobs.size(), (int)steps.size());
@@ -757,6 +818,8 @@ hmg_status build_bf16_factors(hmg_matrix* h)
         all_tiles = all_tiles && started;
     }
 
+    k1.make_steps(false);
+    k2.make_steps(true);
     if (!steps_in_bounds(k1, vbytes, xbytes + tgroups * 2 * TC_XGROUP, (long long)kmap.size() / 16, 0) ||
         !steps_in_bounds(k2, ubytes, xbytes + tgroups * 2 * TC_XGROUP, h->n[0], 1)) {
         set_error("hmg_build_bf16_factors: internal error: an operand step leaves its buffer");
