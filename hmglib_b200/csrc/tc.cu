@@ -188,7 +188,7 @@ struct TcSmem {
                                    // the MMA's reads of unused A rows past the ring's end)
     uint64_t full[TC_SLOTS], empty[TC_SLOTS], accf[2], acce[2], fin;
     uint32_t slot_a[TC_SLOTS], slot_b[TC_SLOTS];  // shared addresses of a step's A and B
-    int slot_meta[TC_SLOTS], slot_kss[TC_SLOTS];   // a step's meta and sub-step words
+    int slot_meta[TC_SLOTS];                       // a step's meta word
     int slot_pos[TC_SLOTS];                        // ring offset of a step (copy warp only)
     int step_bytes[32];                            // bytes of the copy warp's current 32 steps
     uint32_t tmem;
@@ -350,7 +350,6 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                     sm.slot_a[slot] = a;
                     sm.slot_b[slot] = a + ab;
                     sm.slot_meta[slot] = mine.meta;
-                    sm.slot_kss[slot] = mine.kss;
                     mbar_arrive_expect_tx(&sm.full[slot], ab + bb);
                     bulk_g2s_first(sm.ring + pos, A + mine.a_off, ab, &sm.full[slot], pol);
                     const int nsub = ((mine.meta >> 10) & 3) + 1;
@@ -382,8 +381,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                     *fail = 1;
                     break;
                 }
-                uint32_t a0 = sm.slot_a[slot], b0 = sm.slot_b[slot];
-                const int meta = sm.slot_meta[slot], kss = sm.slot_kss[slot], nsub = ((meta >> 10) & 3) + 1;
+                const uint32_t a0 = sm.slot_a[slot], b0 = sm.slot_b[slot];
+                const int meta = sm.slot_meta[slot], ks_all = (meta >> 16) & 0xff;
                 const bool first = meta & 256, last = meta & 512;
                 if (first && jc >= 2) {  // the epilogue has read this accumulator's previous job
                     if (!mbar_wait(&sm.acce[buf], ((jc >> 1) - 1) & 1, err, 13)) {
@@ -392,17 +391,21 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                     }
                     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
                 }
+                // The step's A chunks lie one after another, so do its B chunks: MMA q reads A
+                // 2q K cores and B 2q K cores further on.  The descriptors advance by plain
+                // adds to their start-address field (16-byte units; shared addresses stay
+                // below 2^18, so the field never carries): this lane's issue rate bounds the pass.
                 const uint32_t lbo = (uint32_t)(meta & 0xff) * 128u;
                 const uint32_t d = tmem + (uint32_t)(buf * TC_N);
-                for (int j = 0; j < nsub; j++) {
-                    const int ks = ((kss >> (4 * j)) & 15) + 1;
-                    for (int q = 0; q < ks; q++) {
-                        const uint64_t ad = smem_desc(a0 + q * 2 * lbo, lbo, 128);
-                        const uint64_t bd = smem_desc(b0 + q * 1024, TC_XGROUP, 128);
-                        tc_mma(d, ad, bd, (first && j == 0 && q == 0) ? 0u : 1u);
-                    }
-                    a0 += ks * 2 * lbo;
-                    b0 += ks * 1024;
+                const uint64_t da = (2 * lbo) >> 4, db = 1024 >> 4;
+                uint64_t ad = smem_desc(a0, lbo, 128), bd = smem_desc(b0, TC_XGROUP, 128);
+                uint32_t acc = first ? 0u : 1u;
+#pragma unroll 4
+                for (int q = 0; q < ks_all; q++) {
+                    tc_mma(d, ad, bd, acc);
+                    acc = 1u;
+                    ad += da;
+                    bd += db;
                 }
                 tc_commit(&sm.empty[slot]);
                 if (last) {
