@@ -345,8 +345,11 @@ def run_engine(a, rank, world):
     if a.nrhs > 1:
         line["multi_rhs"] = multi_rhs_timing(torch, H, x, n, a.nrhs, a.steps, stream, world, err)
         if a.tc:
-            H.build_bf16_factors()
+            H.build_bf16_factors(near=hmg.PREC_BF16)
             line["multi_rhs_tensor_cores"] = multi_rhs_timing(torch, H, x, n, a.nrhs, a.steps, stream, world, err)
+            H.build_bf16_factors(near=hmg.PREC_FP32)
+            line["multi_rhs_tensor_cores_near_fp32"] = multi_rhs_timing(torch, H, x, n, a.nrhs, a.steps, stream,
+                                                                        world, err)
     if rank == 0 and world == 1 and not a.no_cpu:
         kind = O.KERNEL_MATERN32
         rate, nrows, dt, thr = cpu_direct_rate(p, x, kind, O.kernel_param(kind, W["rho"]), target_s=a.cpu_seconds)
@@ -408,24 +411,29 @@ def run_precision(a, rank, world):
             errs.append(float(torch.linalg.norm(Y[j][rows.long()] - yd) / torch.linalg.norm(yd)))
         info = H.info()
         if prec == hmg.PREC_FP32:
-            H.build_bf16_factors()
-            Yt = torch.empty_like(X)
-            for _ in range(2):
-                H.matvec_multi(X, Yt)
-            torch.cuda.synchronize()
-            e0.record(stream)
-            for _ in range(a.steps):
-                H.matvec_multi(X, Yt)
-            e1.record(stream)
-            torch.cuda.synchronize()
-            ms_tc = e0.elapsed_time(e1) / a.steps
-            errs_tc = []
-            for j in range(0, nrhs, 8):
-                yd = torch.empty(rows.shape[0], dtype=torch.float64, device="cuda")
-                H.full_matvec_rows(X[j], rows, yd)
+            # tensor cores: BF16 factors with the near field in FP32 on the CUDA cores (the
+            # configuration as specified), then with the near field in BF16 as well
+            tc = {}
+            for near in (hmg.PREC_FP32, hmg.PREC_BF16):
+                H.build_bf16_factors(near=near)
+                Yt = torch.empty_like(X)
+                for _ in range(2):
+                    H.matvec_multi(X, Yt)
                 torch.cuda.synchronize()
-                errs_tc.append(float(torch.linalg.norm(Yt[j][rows.long()] - yd) / torch.linalg.norm(yd)))
-            tc = {"ms_per_32_vectors": ms_tc, "vectors_per_s": nrhs * 1000.0 / ms_tc, "err_vs_fp64_max": max(errs_tc)}
+                e0.record(stream)
+                for _ in range(a.steps):
+                    H.matvec_multi(X, Yt)
+                e1.record(stream)
+                torch.cuda.synchronize()
+                ms_tc = e0.elapsed_time(e1) / a.steps
+                errs_tc = []
+                for j in range(0, nrhs, 8):
+                    yd = torch.empty(rows.shape[0], dtype=torch.float64, device="cuda")
+                    H.full_matvec_rows(X[j], rows, yd)
+                    torch.cuda.synchronize()
+                    errs_tc.append(float(torch.linalg.norm(Yt[j][rows.long()] - yd) / torch.linalg.norm(yd)))
+                tc["near_fp32_cuda_cores" if near == hmg.PREC_FP32 else "near_bf16_tensor_cores"] = {
+                    "ms_per_32_vectors": ms_tc, "vectors_per_s": nrhs * 1000.0 / ms_tc, "err_vs_fp64_max": max(errs_tc)}
         res = {"ms_per_32_vectors": ms, "vectors_per_s": nrhs * 1000.0 / ms, "err_vs_fp64_max": max(errs),
                "build_s": t_build, "far_gb": info["far_bytes"] / 1e9, "near_gb": info["near_bytes"] / 1e9,
                "max_rank": info["max_rank"]}

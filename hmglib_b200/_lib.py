@@ -24,6 +24,7 @@ ADMISSIBLE_MIN = 1
 PREC_FP64 = 0
 PREC_FP32 = 1
 PREC_MIXED = 2
+PREC_BF16 = 3
 NEAR_STORED = 0
 NEAR_ONTHEFLY = 1
 
@@ -68,6 +69,7 @@ _PROTOS = {
     "hmg_group_offsets": (C.c_int, [_vp, C.c_int, _vp]),
     "hmg_save": (C.c_int, [_vp, C.c_char_p]),
     "hmg_build_bf16_factors": (C.c_int, [_vp]),
+    "hmg_build_tensor_core_operands": (C.c_int, [_vp, C.c_int]),
     "hmg_load": (C.c_int, [C.POINTER(_vp), C.c_char_p, _vp]),
     "hmg_full_matvec": (C.c_int, [_vp, _vp, _vp]),
     "hmg_full_matvec_rows": (C.c_int, [_vp, _vp, _vp, C.c_int, _vp]),

@@ -95,6 +95,7 @@ struct hmg_matrix {
     int tc_njobs[2] = {0, 0};
     int tc_grid = 0;
     bool tc_all_tiles = false;                // every row tile has a pass-2 job
+    bool tc_near = false;                     // near field on the tensor cores (else FP32 CUDA cores)
     long long tc_xbytes = 0, tc_tbytes = 0;   // per product: X cores, t_b cores
     long long tc_bytes = 0;                   // BF16 operands held
 
@@ -135,8 +136,10 @@ hmg_status fill_near(hmg_matrix* h, int precision);
 hmg_status matvec_device(hmg_matrix* h, const double* x, double* y, bool fp64_arith = false);
 hmg_status matvec_multi(hmg_matrix* h, int nrhs, const double* X, int ldx, double* Y, int ldy);
 hmg_status matvec_multi_tc(hmg_matrix* h, int nrhs, const double* X, int ldx, double* Y, int ldy);
-hmg_status build_bf16_factors(hmg_matrix* h);
+hmg_status build_bf16_factors(hmg_matrix* h, bool near_on_tensor_cores);
 void free_tc(hmg_matrix* h);
+void launch_gather_multi32(hmg_matrix* h, const double* X, int ldx, int nrhs, float* xm);
+hmg_status launch_tile_multi32_dense(hmg_matrix* h, const float* xm, int nrhs, double* Y, int ldy);
 hmg_status direct_matvec(hmg_matrix* h, const double* x, const int* rows, int nrows,
                          double* y);
 hmg_status gaussian_rhs(hmg_matrix* h, double* b);

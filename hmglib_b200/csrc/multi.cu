@@ -731,6 +731,24 @@ static hmg_status multi_typed(hmg_matrix* h, int nrhs, const double* X, int ldx,
     return st;
 }
 
+// Y = the near-field part of H X for up to 32 vectors, FP32 stored near field, FP32
+// products summed in FP64 (the tensor-core path with its near field on the CUDA cores)
+hmg_status launch_tile_multi32_dense(hmg_matrix* h, const float* xm, int nrhs, double* Y, int ldy)
+{
+    if (h->ntiles <= 0) return HMG_OK;
+    k_tile_multi_smem<32><<<h->ntiles, 256, 0, h->stream>>>(
+        static_cast<const PairDesc*>(h->pair_desc), h->tile_pair_start, h->tile_r0, h->tile_s, h->perm[0], xm,
+        nullptr, static_cast<const char*>(h->tbuf), nrhs, Y, ldy, PAIR_STORED);
+    HMG_LAUNCH_CHECK();
+    return HMG_OK;
+}
+
+void launch_gather_multi32(hmg_matrix* h, const double* X, int ldx, int nrhs, float* xm)
+{
+    k_gather_multi<float><<<ceil_div((long long)h->n[1] * 32, 256), 256, 0, h->stream>>>(X, ldx, nrhs, h->perm[1],
+                                                                                        h->n[1], 5, xm);
+}
+
 hmg_status matvec_multi(hmg_matrix* h, int nrhs, const double* X, int ldx, double* Y, int ldy)
 {
     // tensor cores: a BF16 copy of the FP32 factors and an FP32 stored near field

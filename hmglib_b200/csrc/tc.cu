@@ -250,12 +250,13 @@ __device__ __forceinline__ uint32_t pack_bf16(float lo, float hi)
 
 // Steps of CTA c: [cta[c].y, cta[c+1].y); its jobs: [cta[c].x, cta[c+1].x).
 // Pass 1 (MODE 0) writes t_b cores at Bbuf + tb_off, K core kc of job j (a stack) to 512-byte
-// unit map[16 j + kc]; pass 2 (MODE 1) writes rows of Y, tile row i to Y row map[r0 + i].
+// unit map[16 j + kc]; pass 2 (MODE 1) writes (add_y: adds to) rows of Y, tile row i to Y
+// row map[r0 + i].
 template <int MODE>
 __global__ void __launch_bounds__(TC_THREADS, 1)
     k_tc_pass(const TcStep* __restrict__ steps, const TcJob* __restrict__ jobs, const int2* __restrict__ cta,
               const char* __restrict__ A, char* Bbuf, long long tb_off, const int* __restrict__ map, int nrhs,
-              double* Y, int ldy, int* err)
+              double* Y, int ldy, int add_y, int* err)
 {
     extern __shared__ __align__(1024) unsigned char tc_raw[];
     TcSmem& sm = *reinterpret_cast<TcSmem*>(tc_raw);
@@ -465,7 +466,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                         double* y = Y + yrow;
 #pragma unroll
                         for (int q = 0; q < TC_N; q++)
-                            if (q < nrhs) y[(size_t)q * ldy] = (double)__uint_as_float(v[q]);
+                            if (q < nrhs) y[(size_t)q * ldy] = (add_y ? y[(size_t)q * ldy] : 0.0) + (double)__uint_as_float(v[q]);
                     }
                 } else {
                     // term row -> B cores of pass 2 (K = term): element (term m, vector q) at byte
@@ -539,6 +540,7 @@ void free_tc(hmg_matrix* h)
     h->tc_xbytes = h->tc_tbytes = 0;
     h->tc_grid = 0;
     h->tc_all_tiles = false;
+    h->tc_near = false;
 }
 
 namespace {
@@ -697,7 +699,7 @@ hmg_status alloc_arena(void** p, long long bytes, const char* what)
 
 }  // namespace
 
-hmg_status build_bf16_factors(hmg_matrix* h)
+hmg_status build_bf16_factors(hmg_matrix* h, bool near_tc)
 {
     cudaStream_t s = h->stream;
     hmg_status st;
@@ -797,7 +799,7 @@ hmg_status build_bf16_factors(hmg_matrix* h)
         for (int p = tps[t]; p < tps[t + 1]; p++) {
             const int b = pblock[p];
             const bool dense = b < h->ndense;
-            if (!dense && h->h_rank[b] == 0) continue;
+            if ((!dense && h->h_rank[b] == 0) || (dense && !near_tc)) continue;
             if (!started) {
                 k2.begin(TcJob{tr0[t], ts[t]});
                 started = true;
@@ -890,6 +892,7 @@ hmg_status build_bf16_factors(hmg_matrix* h)
     h->tc_tbytes = tgroups * 2 * TC_XGROUP;
     h->tc_grid = grid;
     h->tc_all_tiles = all_tiles;
+    h->tc_near = near_tc;
     h->tc_ready = true;
     return HMG_OK;
 }
@@ -920,17 +923,27 @@ hmg_status matvec_multi_tc(hmg_matrix* h, int nrhs, const double* X, int ldx, do
         k_tc_pass<0><<<h->tc_grid, TC_THREADS, smem, s>>>(
             reinterpret_cast<const TcStep*>(h->tc_steps[0]), reinterpret_cast<const TcJob*>(h->tc_jobs[0]),
             reinterpret_cast<const int2*>(h->tc_cta[0]), static_cast<const char*>(h->tc_v), bbuf, h->tc_xbytes,
-            h->tc_kmap, 0, nullptr, 0, h->dev_err);
+            h->tc_kmap, 0, nullptr, 0, 0, h->dev_err);
         HMG_LAUNCH_CHECK();
     }
-    // rows of tiles without products (all their blocks of rank 0) are zero
-    if (!h->tc_all_tiles)
+    if (!h->tc_near && h->ndense > 0) {
+        // the near field in FP32 on the CUDA cores writes every row of Y first
+        float* xm = nullptr;
+        if ((st = dalloc(&xm, (size_t)h->n[1] * TC_N, s))) return st;
+        launch_gather_multi32(h, X, ldx, nrhs, xm);
+        st = launch_tile_multi32_dense(h, xm, nrhs, Y, ldy);
+        dfree(xm, s);
+        if (st) return st;
+    } else if (!h->tc_all_tiles) {
+        // rows of tiles without products (all their blocks of rank 0) are zero
         HMG_CUDA_TRY(cudaMemset2DAsync(Y, sizeof(double) * ldy, 0, sizeof(double) * h->n[0], nrhs, s));
+    }
+    const int add_y = !h->tc_near && h->ndense > 0;
     if (h->tc_njobs[1] > 0) {
         k_tc_pass<1><<<h->tc_grid, TC_THREADS, smem, s>>>(
             reinterpret_cast<const TcStep*>(h->tc_steps[1]), reinterpret_cast<const TcJob*>(h->tc_jobs[1]),
             reinterpret_cast<const int2*>(h->tc_cta[1]), static_cast<const char*>(h->tc_u), bbuf, 0, h->perm[0], nrhs,
-            Y, ldy, h->dev_err);
+            Y, ldy, add_y, h->dev_err);
         HMG_LAUNCH_CHECK();
     }
     return HMG_OK;

@@ -138,9 +138,11 @@ class HMatrix:
         """0: streaming (bulk-copy) product kernels, 1: plain-load kernels."""
         self._call("hmg_set_matvec_variant", int(variant))
 
-    def build_bf16_factors(self):
-        """BF16 operand copy of the FP32 factors for tensor-core multi-vector products."""
-        self._call("hmg_build_bf16_factors")
+    def build_bf16_factors(self, near: int = L.PREC_BF16):
+        """BF16 tcgen05 operands of the FP32 factors for tensor-core multi-vector products
+        (hmg_build_tensor_core_operands); the near field on the tensor cores too
+        (near=PREC_BF16) or in FP32 on the CUDA cores (near=PREC_FP32)."""
+        self._call("hmg_build_tensor_core_operands", int(near))
 
     def save(self, path: str):
         """Write the H-matrix to `path` (hmg_save)."""

@@ -51,6 +51,8 @@ typedef enum {
  * Frobenius norm in FP16 and below 1.5e-6 in FP8 e4m3, each scaled; the added error
  * is ~1e-7 of the block norm.  hmg_precompute_dense with this value stores FP32. */
 #define HMG_PREC_MIXED 2
+/* Tensor-core operands only (hmg_build_tensor_core_operands): BF16 */
+#define HMG_PREC_BF16 3
 
 /* near-field mode for hmg_matvec */
 #define HMG_NEAR_STORED 0   /* read the blocks stored by hmg_precompute_dense          */
@@ -132,13 +134,16 @@ hmg_status hmg_full_matvec_rows(hmg_matrix* h, const double* x, const int* rows,
                                 double* y);
 
 /* Tensor-core products (no reference counterpart): converts the handle's FP32 low-rank
- * factors (hmg_precompute_aca with HMG_PREC_FP32, ranks <= 128) and its FP32 stored near
- * field (hmg_precompute_dense with HMG_PREC_FP32) into BF16 copies laid out as tcgen05
- * operands.  Afterwards hmg_matvec_multi with 2..32 vectors runs every product on the
- * tensor cores: t_b = V_b^T X_b, U t_b and the near blocks times X, with BF16 operands
- * (X and t_b rounded to BF16) and FP32 accumulation; results agree with the FP32
- * products to ~1e-3 (BF16 rounding).  Single-vector products keep using the FP32
- * storage.  Recomputing the factors or the near field drops the copies. */
+ * factors (hmg_precompute_aca with HMG_PREC_FP32, ranks <= 128) into BF16 copies laid
+ * out as tcgen05 operands, and with near_precision HMG_PREC_BF16 its FP32 stored near
+ * field (hmg_precompute_dense with HMG_PREC_FP32) too.  Afterwards hmg_matvec_multi
+ * with 2..32 vectors computes t_b = V_b^T X_b and U t_b on the tensor cores with BF16
+ * operands (X and t_b rounded to BF16) and FP32 accumulation; the near field runs
+ * there as well (HMG_PREC_BF16) or on the CUDA cores in FP32 (HMG_PREC_FP32).  Results
+ * agree with the FP32 products to ~1e-3 (BF16 rounding).  Single-vector products keep
+ * using the FP32 storage.  Recomputing the factors or the near field drops the copies.
+ * hmg_build_bf16_factors(h) is hmg_build_tensor_core_operands(h, HMG_PREC_BF16). */
+hmg_status hmg_build_tensor_core_operands(hmg_matrix* h, int near_precision);
 hmg_status hmg_build_bf16_factors(hmg_matrix* h);
 
 /* Write a set-up H-matrix to `path` (points, permutations, block list, ranks and

@@ -50,6 +50,34 @@ def test_tensor_core_products(hmg, cuda, case):
     H.close()
 
 
+def test_fp32_near_field_on_cuda_cores(hmg, cuda):
+    """near=PREC_FP32: only the low-rank part on the tensor cores; the near field stays
+    FP32 on the CUDA cores and the low-rank sums are added to it.  Closer to the FP32
+    product than the all-BF16 variant, within the same 5e-3."""
+    torch = cuda
+    p = make_points("uniform", 20000, 3, 21)
+    H = engine(hmg, p, p, 1.5, 128, rule=1)
+    H.set_kernel(MATERN, 0.2, 0.0)
+    H.precompute_aca(64, 1e-6, hmg.PREC_FP32)
+    H.precompute_dense(hmg.PREC_FP32)
+    X = torch.from_numpy(np.random.default_rng(5).uniform(-1, 1, (16, 20000))).cuda()
+    Y32, Ya, Yb = torch.empty_like(X), torch.empty_like(X), torch.full_like(X, float("nan"))
+    H.matvec_multi(X, Y32)
+    H.build_bf16_factors(near=hmg.PREC_BF16)
+    H.matvec_multi(X, Ya)
+    H.build_bf16_factors(near=hmg.PREC_FP32)
+    H.matvec_multi(X, Yb)
+    H.synchronize()
+    ref, a, b = Y32.cpu().numpy(), Ya.cpu().numpy(), Yb.cpu().numpy()
+    assert np.isfinite(b).all()
+    ea = max(rel_err(a[j], ref[j]) for j in range(16))
+    eb = max(rel_err(b[j], ref[j]) for j in range(16))
+    assert eb < 5e-3 and eb < ea, (ea, eb)
+    with pytest.raises(hmg.HmgError):
+        H.build_bf16_factors(near=hmg.PREC_MIXED)
+    H.close()
+
+
 def test_copies_follow_the_storage(hmg, cuda):
     """Recomputing the near field drops the BF16 copies (products fall back to the
     FP32 CUDA-core kernels); a handle without an FP32 stored near field is refused."""
