@@ -375,6 +375,14 @@ hmg_status hmg_set_matvec_variant(hmg_matrix* h, int variant)
     return HMG_OK;
 }
 
+hmg_status hmg_set_graphs(hmg_matrix* h, int on)
+{
+    HMG_REQUIRE(h, HMG_ERR_INVALID, "hmg_set_graphs: NULL handle");
+    h->use_graphs = on != 0;
+    if (!h->use_graphs) free_product_graph(h);
+    return HMG_OK;
+}
+
 hmg_status hmg_set_product_precision(hmg_matrix* h, int precision)
 {
     HMG_REQUIRE(h, HMG_ERR_INVALID, "hmg_set_product_precision: NULL handle");
@@ -410,6 +418,8 @@ hmg_status hmg_get_profile(hmg_matrix* h, double* ms4)
 hmg_status hmg_destroy(hmg_matrix* h)
 {
     if (!h) return HMG_OK;
+    free_product_graph(h);
+    if (h->capture_stream) cudaStreamDestroy(static_cast<cudaStream_t>(h->capture_stream));
     cudaStreamSynchronize(h->stream);
     for (int i = 0; i < 4; i++)
         if (h->ev[i]) cudaEventDestroy(h->ev[i]);

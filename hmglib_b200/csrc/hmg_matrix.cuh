@@ -114,6 +114,10 @@ struct hmg_matrix {
     int nfar_list = 0;
     int* dev_err = nullptr;        // pipeline wait time-out flag (0 = fine)
     int matvec_variant = 1;        // 0: streaming kernels where applicable, 1: plain-load kernels
+    bool use_graphs = false;       // replay products as a captured CUDA graph (hmg_set_graphs)
+    void* graph_exec = nullptr;    // cudaGraphExec_t of the last product's launches
+    void* graph_key = nullptr;     // what it was captured for (matvec.cu)
+    void* capture_stream = nullptr;  // cudaStream_t the graph is captured on
     int arith_prec = HMG_PREC_FP32;  // products over FP32 / mixed storage: FP32 or FP64 arithmetic
     int last_variant_k1 = -1, last_variant_k2 = -1;
     double* host_x = nullptr; // pinned staging
@@ -138,6 +142,7 @@ hmg_status matvec_multi(hmg_matrix* h, int nrhs, const double* X, int ldx, doubl
 hmg_status matvec_multi_tc(hmg_matrix* h, int nrhs, const double* X, int ldx, double* Y, int ldy);
 hmg_status build_bf16_factors(hmg_matrix* h, bool near_on_tensor_cores);
 void free_tc(hmg_matrix* h);
+void free_product_graph(hmg_matrix* h);
 void launch_gather_multi32(hmg_matrix* h, const double* X, int ldx, int nrhs, float* xm);
 hmg_status launch_tile_multi32_dense(hmg_matrix* h, const float* xm, int nrhs, double* Y, int ldy);
 hmg_status direct_matvec(hmg_matrix* h, const double* x, const int* rows, int nrows,

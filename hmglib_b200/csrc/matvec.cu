@@ -19,6 +19,8 @@
 #include <cuda_fp8.h>
 
 #include <algorithm>
+#include <cstdlib>
+#include <cstring>
 #include <vector>
 
 #include "hmg_matrix.cuh"
@@ -695,9 +697,12 @@ hmg_status ensure_xs(hmg_matrix* h)
     return HMG_OK;
 }
 
+static hmg_status launch_product(hmg_matrix* h, const double* x, double* y, bool fp64, bool arith64, bool bulk_k1,
+                                 bool bulk_k2);
+static hmg_status launch_product_graph(hmg_matrix* h, const double* x, double* y, bool fp64, bool arith64);
+
 hmg_status matvec_device(hmg_matrix* h, const double* x, double* y, bool fp64_arith)
 {
-    cudaStream_t s = h->stream;
     hmg_status st;
     if (h->group_count && h->ndense > 0 && (h->near_mode != HMG_NEAR_STORED || h->near_prec < 0)) {
         set_error("a group handle multiplies a stored near field: call hmg_precompute_dense first");
@@ -719,11 +724,6 @@ hmg_status matvec_device(hmg_matrix* h, const double* x, double* y, bool fp64_ar
     }
     const int elem = arith64 ? 8 : 4;
     if ((st = ensure_desc(h, elem))) return st;
-    PointsView P = points_view(h);
-    if (h->profiling) HMG_CUDA_TRY(cudaEventRecord(h->ev[0], s));
-    k_gather_x<<<ceil_div(h->n[1], 256), 256, 0, s>>>(x, h->perm[1], h->n[1], h->xs64, h->xs32);
-    HMG_LAUNCH_CHECK();
-    if (h->profiling) HMG_CUDA_TRY(cudaEventRecord(h->ev[1], s));
     // the streaming kernels read FP32/FP64 storage in its own arithmetic only
     const bool plain_types = !mixed && arith64 == fp64;
     const bool bulk_k1 = h->matvec_variant == 0 && plain_types && h->max_rank <= K1_MAXRANK;
@@ -731,6 +731,117 @@ hmg_status matvec_device(hmg_matrix* h, const double* x, double* y, bool fp64_ar
                          (h->near_mode == HMG_NEAR_STORED || h->ndense == 0);
     h->last_variant_k1 = bulk_k1 ? 0 : 1;
     h->last_variant_k2 = bulk_k2 ? 0 : 1;
+    if (h->use_graphs && !h->profiling && !bulk_k1 && !bulk_k2) return launch_product_graph(h, x, y, fp64, arith64);
+    return launch_product(h, x, y, fp64, arith64, bulk_k1, bulk_k2);
+}
+
+// Everything a product's launches depend on besides the contents of device memory: two
+// products with equal keys issue the same launches with the same arguments, so the
+// graph captured for one replays the other.
+struct ProductKey {
+    const double* x;
+    double* y;
+    int fp64, arith64, ntiles, nk1, near_mode, near_prec, far_prec;
+    int k1_task_start[3][5], k1_piece_start[3][5];
+    const void *k1_units, *tbuf, *pair_desc, *xs64, *xs32;
+    const int *tile_pair_start, *tile_r0, *tile_s, *perm0, *perm1;
+    KernelSpec kspec;
+    PointsView P;
+};
+
+static ProductKey product_key(hmg_matrix* h, const double* x, double* y, bool fp64, bool arith64)
+{
+    ProductKey k;
+    memset(&k, 0, sizeof(k));  // padding included: keys are compared bytewise
+    k.x = x;
+    k.y = y;
+    k.fp64 = fp64;
+    k.arith64 = arith64;
+    k.ntiles = h->ntiles;
+    k.nk1 = h->nk1;
+    k.near_mode = h->near_mode;
+    k.near_prec = h->near_prec;
+    k.far_prec = h->far_prec;
+    memcpy(k.k1_task_start, h->k1_task_start, sizeof(k.k1_task_start));
+    memcpy(k.k1_piece_start, h->k1_piece_start, sizeof(k.k1_piece_start));
+    k.k1_units = h->k1_units;
+    k.tbuf = h->tbuf;
+    k.pair_desc = h->pair_desc;
+    k.xs64 = h->xs64;
+    k.xs32 = h->xs32;
+    k.tile_pair_start = h->tile_pair_start;
+    k.tile_r0 = h->tile_r0;
+    k.tile_s = h->tile_s;
+    k.perm0 = h->perm[0];
+    k.perm1 = h->perm[1];
+    k.kspec = h->kspec;
+    k.P = points_view(h);
+    return k;
+}
+
+void free_product_graph(hmg_matrix* h)
+{
+    if (h->graph_exec) cudaGraphExecDestroy(static_cast<cudaGraphExec_t>(h->graph_exec));
+    h->graph_exec = nullptr;
+    free(h->graph_key);
+    h->graph_key = nullptr;
+}
+
+// The product as one CUDA graph: captured on the first call with a new key, replayed
+// with cudaGraphLaunch while the key holds (one graph per handle).
+static hmg_status launch_product_graph(hmg_matrix* h, const double* x, double* y, bool fp64, bool arith64)
+{
+    cudaStream_t s = h->stream;
+    const ProductKey key = product_key(h, x, y, fp64, arith64);
+    if (!h->graph_exec || memcmp(h->graph_key, &key, sizeof(key)) != 0) {
+        free_product_graph(h);
+        // captured on a stream of its own (the handle's may be the legacy default stream,
+        // which cannot be captured); capturing runs nothing
+        if (!h->capture_stream) {
+            cudaStream_t cs = nullptr;
+            HMG_CUDA_TRY(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+            h->capture_stream = cs;
+        }
+        cudaStream_t cs = static_cast<cudaStream_t>(h->capture_stream);
+        HMG_CUDA_TRY(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
+        h->stream = cs;
+        const hmg_status st = launch_product(h, x, y, fp64, arith64, false, false);
+        h->stream = s;
+        cudaGraph_t g = nullptr;
+        const cudaError_t ce = cudaStreamEndCapture(cs, &g);
+        if (st || ce != cudaSuccess) {
+            if (g) cudaGraphDestroy(g);
+            cudaGetLastError();
+            if (!st) set_error("capturing the product graph failed: %s", cudaGetErrorString(ce));
+            return st ? st : HMG_ERR_CUDA;
+        }
+        cudaGraphExec_t ex = nullptr;
+        const cudaError_t ie = cudaGraphInstantiate(&ex, g, 0);
+        cudaGraphDestroy(g);
+        if (ie != cudaSuccess) {
+            cudaGetLastError();
+            set_error("instantiating the product graph failed: %s", cudaGetErrorString(ie));
+            return HMG_ERR_CUDA;
+        }
+        h->graph_exec = ex;
+        h->graph_key = malloc(sizeof(key));
+        memcpy(h->graph_key, &key, sizeof(key));
+    }
+    HMG_CUDA_TRY(cudaGraphLaunch(static_cast<cudaGraphExec_t>(h->graph_exec), s));
+    return HMG_OK;
+}
+
+// The launches of one product (x gather, V^T x per storage tier, tile kernel).
+static hmg_status launch_product(hmg_matrix* h, const double* x, double* y, bool fp64, bool arith64, bool bulk_k1,
+                                 bool bulk_k2)
+{
+    cudaStream_t s = h->stream;
+    hmg_status st;
+    PointsView P = points_view(h);
+    if (h->profiling) HMG_CUDA_TRY(cudaEventRecord(h->ev[0], s));
+    k_gather_x<<<ceil_div(h->n[1], 256), 256, 0, s>>>(x, h->perm[1], h->n[1], h->xs64, h->xs32);
+    HMG_LAUNCH_CHECK();
+    if (h->profiling) HMG_CUDA_TRY(cudaEventRecord(h->ev[1], s));
     if (bulk_k1 && h->nfar_list > 0) {
         if ((st = launch_vtx_bulk(h, fp64))) return st;
     } else if (h->nk1 > 0) {

@@ -138,6 +138,10 @@ class HMatrix:
         """0: streaming (bulk-copy) product kernels, 1: plain-load kernels."""
         self._call("hmg_set_matvec_variant", int(variant))
 
+    def set_graphs(self, on: bool = True):
+        """Replay products as a captured CUDA graph (hmg_set_graphs)."""
+        self._call("hmg_set_graphs", int(bool(on)))
+
     def build_bf16_factors(self, near: int = L.PREC_BF16):
         """BF16 tcgen05 operands of the FP32 factors for tensor-core multi-vector products
         (hmg_build_tensor_core_operands); the near field on the tensor cores too

@@ -213,6 +213,13 @@ hmg_status hmg_get_profile(hmg_matrix* h, double* ms4);
  * variant 1 sums each slice in FP32 and the slices in FP64). */
 hmg_status hmg_set_matvec_variant(hmg_matrix* h, int variant);
 
+/* Products as CUDA graphs (no reference counterpart): with on != 0, hmg_matvec and
+ * hmg_matvec_host capture the launches of a product into a CUDA graph on the first call
+ * and replay it (cudaGraphLaunch) while the arguments and the handle's storage stay the
+ * same; any change (other x or y, other storage, modes or kernel) captures anew.
+ * Results are bit-identical to direct launches.  Default off. */
+hmg_status hmg_set_graphs(hmg_matrix* h, int on);
+
 /* Arithmetic of the products over FP32 or mixed storage (no reference counterpart):
  * HMG_PREC_FP32 (default) multiplies each slice in FP32 and sums the slices in FP64;
  * HMG_PREC_FP64 converts every stored value and multiplies in FP64, so the stored
