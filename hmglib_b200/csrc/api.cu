@@ -273,7 +273,7 @@ hmg_status hmg_group_offsets(hmg_matrix* h, int set, int64_t* offsets)
 hmg_status hmg_matvec_multi(hmg_matrix* h, int nrhs, const double* X, int ldx, double* Y, int ldy)
 {
     HMG_REQUIRE(h && X && Y, HMG_ERR_INVALID, "hmg_matvec_multi: NULL argument");
-    HMG_REQUIRE(nrhs >= 1 && nrhs <= 32, HMG_ERR_INVALID, "hmg_matvec_multi: nrhs %d outside 1..32", nrhs);
+    HMG_REQUIRE(nrhs >= 1 && nrhs <= 64, HMG_ERR_INVALID, "hmg_matvec_multi: nrhs %d outside 1..64", nrhs);
     HMG_REQUIRE(ldx >= h->n[1] && ldy >= h->n[0], HMG_ERR_INVALID,
                 "hmg_matvec_multi: leading dimensions %d, %d below n2 = %d, n1 = %d", ldx, ldy, h->n[1], h->n[0]);
     hmg_status st = check_ready(h, "hmg_matvec_multi");

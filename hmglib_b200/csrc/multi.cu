@@ -751,10 +751,14 @@ void launch_gather_multi32(hmg_matrix* h, const double* X, int ldx, int nrhs, fl
 
 hmg_status matvec_multi(hmg_matrix* h, int nrhs, const double* X, int ldx, double* Y, int ldy)
 {
-    // tensor cores: a BF16 copy of the FP32 factors and an FP32 stored near field
+    // tensor cores: a BF16 copy of the FP32 factors and an FP32 stored near field (up to 64 vectors a pass)
     if (h->tc_ready && nrhs >= 2 && h->far_prec == HMG_PREC_FP32 && h->near_mode == HMG_NEAR_STORED &&
         (h->ndense == 0 || h->near_prec == HMG_PREC_FP32) && h->arith_prec == HMG_PREC_FP32)
         return matvec_multi_tc(h, nrhs, X, ldx, Y, ldy);
+    if (nrhs > 32) {  // the CUDA-core kernels take 32 vectors a pass
+        hmg_status st = matvec_multi(h, 32, X, ldx, Y, ldy);
+        return st ? st : matvec_multi(h, nrhs - 32, X + (size_t)32 * ldx, ldx, Y + (size_t)32 * ldy, ldy);
+    }
     if (nrhs > 1 && h->far_prec == HMG_PREC_MIXED && h->near_mode == HMG_NEAR_STORED &&
         (h->ndense == 0 || h->near_prec == HMG_PREC_FP32) && h->arith_prec == HMG_PREC_FP32)
         return multi_mixed(h, nrhs, X, ldx, Y, ldy);

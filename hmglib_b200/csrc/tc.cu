@@ -1,11 +1,11 @@
 // tc.cu -- multi-vector products on the tensor cores (tcgen05), BF16 operands.
 //
 // hmg_build_bf16_factors converts the FP32 low-rank factors and the FP32 stored near
-// field of a handle into BF16 tcgen05 operands; hmg_matvec_multi then multiplies 2..32
+// field of a handle into BF16 tcgen05 operands; hmg_matvec_multi then multiplies 2..64
 // vectors per pass with them, every product on the tensor cores:
 //
 //   pass 1 (k_tc_pass<0>): per admissible block, t_b = V_b^T X_b (M = rank rounded to
-//     16, padded to 128; N = 32 vectors; K = the block's columns), written as BF16
+//     16, padded to 128; N = 32 or 64 vectors; K = the block's columns), written as BF16
 //     operand cores of pass 2;
 //   pass 2 (k_tc_pass<1>): per row tile (M = 128 rows), the sum over its pairs of
 //     U_slice * t_b (low rank; K = rank) and D_slice * X_b (near field; K = columns),
@@ -17,7 +17,7 @@
 // multiplies (<= 16 KB).  Warp 4 copies steps with bulk copies (cp.async.bulk,
 // completion counted on the step slot's mbarrier) into a 208 KB byte ring that holds up
 // to 16 steps of any size; warp 5 issues the MMAs (one elected lane, accumulating in one
-// of two 32-column tensor-memory buffers) and frees each step's bytes with
+// of two N-column tensor-memory buffers) and frees each step's bytes with
 // tcgen05.commit; warps 0-3 drain a finished buffer (tcgen05.ld, one 32-row quarter
 // each) while the next job accumulates in the other.
 //
@@ -27,13 +27,13 @@
 //     = stored row cores (tile rows or rank rounded to 8).  The MMA's M is 128: rows
 //     past 8 rc read the next K core's bytes (or the rest of the stage) and only reach
 //     accumulator rows that are never read back.
-//   B (X or t_b): core (nc, kc) = vectors 8nc..8nc+7, K 8kc..8kc+7 at (kc * 4 + nc) * 128.
+//   B (X or t_b): core (nc, kc) = vectors 8nc..8nc+7, K 8kc..8kc+7 at (kc * N / 8 + nc) * 128.
 //   X is kept over the Z-ordered column index with 8 columns per K core; a block whose
 //   columns start at c0 reads K cores from c0 / 8 on, and its A operand carries
 //   c0 mod 8 leading zero columns so the K positions line up.
-// Descriptors: leading byte offset = stride between K cores (A: rc * 128, B: 512),
+// Descriptors: leading byte offset = stride between K cores (A: rc * 128, B: N * 16),
 // stride byte offset = stride between row cores (128).  Instruction kind::f16 with BF16
-// A/B, FP32 D, M 128, N 32.
+// A/B, FP32 D, M 128, N 32 (up to 32 vectors) or 64.
 // Every wait is bounded (pipeline.cuh): on a time-out the waiting role records an error
 // code in the handle's flag, leaves its loop, and the CTA waits for its own copies and
 // MMAs before freeing tensor memory.  BF16 rounding of factors, near field, X and t_b
@@ -50,23 +50,24 @@
 
 namespace hmg {
 
-static constexpr int TC_N = 32;            // vectors per pass (MMA N)
+static constexpr int TC_NMAX = 64;         // vectors per pass at most (MMA N: 32 or 64)
 static constexpr int TC_MAXR16 = 128;      // largest rank rounded to 16 (pass 1's M)
 static constexpr int TC_SLOTS = 16;        // steps in flight per CTA at most
-static constexpr int TC_RING = 212992;     // bytes of the operand ring (208 KB)
+static constexpr int TC_RING = 204800;     // bytes of the operand ring (200 KB)
 static constexpr int TC_ISSUERS = 8;       // lanes of the copy warp issuing at once
 static constexpr int TC_ABYTES = 49152;    // A chunk of a step: at most 384 core matrices
-static constexpr int TC_BBYTES = 24576;    // B chunks of a step: at most 48 K cores x 4 vector cores
+static constexpr int TC_BBYTES = 32768;    // B chunks of a step: at most 32 K cores x 8 vector cores
+static constexpr int TC_MAXSTEP = 16;      // MMAs per step
 static constexpr int TC_MAXKS = 16;        // MMAs per sub-step
 static constexpr int TC_MAXSUB = 4;        // sub-steps (B copies) per step
 static constexpr int TC_THREADS = 192;     // warps 0-3 epilogue, 4 copies, 5 MMAs
-static constexpr int TC_XGROUP = 512;      // bytes of one K core of X or t_b (4 vector cores)
+// B operands (X and t_b) are addressed in K cores: 8 columns or terms x NV vectors, NV * 16 bytes
 
 // A step: one copy of A (the A chunks of up to TC_MAXSUB sub-steps, one after another in
 // the A arena) and one copy of B per sub-step (X or t_b cores), placed after A in the ring.
 struct TcStep {
     long long a_off;               // bytes into the A arena
-    long long b_off[TC_MAXSUB];    // bytes into the B buffer (X cores, then t_b cores), per sub-step
+    long long b_off[TC_MAXSUB];    // first K core in the B buffer (X cores, then t_b cores), per sub-step
     int meta;                      // bits 0-7: row cores of A (its K-core stride / 128); bit 8: first step
                                    // of a job; bit 9: last; bits 10-11: sub-steps - 1; bits 16-23: MMAs
     int kss;                       // MMAs (of K = 16) of sub-step j, minus 1, in bits 4j..4j+3
@@ -149,20 +150,21 @@ __global__ void k_tc_v(const int* blist, const long long* voff, const int* vaux,
 // per product: X -> BF16 cores (Z-ordered columns), FP32 rows -> Y
 // ---------------------------------------------------------------------------
 // thread (g, j): columns 8g..8g+7 of vector j, one 16-byte row of K core g
+template <int NV>
 __global__ void k_tc_x(const double* __restrict__ X, int ldx, int nrhs, const int* __restrict__ perm1, int n,
                        long long ngroups, uint4* xb)
 {
     const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (idx >= ngroups * TC_N) return;
-    const long long g = idx >> 5;
-    const int j = (int)(idx & 31);
+    if (idx >= ngroups * NV) return;
+    const long long g = idx / NV;
+    const int j = (int)(idx % NV);
     __nv_bfloat16 v[8];
 #pragma unroll
     for (int e = 0; e < 8; e++) {
         const long long c = g * 8 + e;
         v[e] = __float2bfloat16_rn(c < n && j < nrhs ? (float)X[(size_t)perm1[c] + (size_t)j * ldx] : 0.0f);
     }
-    xb[(g * 4 + (j >> 3)) * 8 + (j & 7)] = *reinterpret_cast<const uint4*>(v);
+    xb[(g * (NV / 8) + (j >> 3)) * 8 + (j & 7)] = *reinterpret_cast<const uint4*>(v);
 }
 
 // ---------------------------------------------------------------------------
@@ -179,13 +181,16 @@ __device__ __forceinline__ uint64_t smem_desc(uint32_t saddr, uint32_t lbo, uint
 
 // kind::f16, D FP32 (bits 4-5 = 1), A and B BF16 (bits 7-9, 10-12 = 1), both K-major,
 // N >> 3 at bits 17-22, M >> 4 at bits 24-28
-static constexpr uint32_t TC_IDESC = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(TC_N >> 3) << 17) |
-                                     ((uint32_t)(128 >> 4) << 24);
+template <int NV>
+__host__ __device__ constexpr uint32_t tc_idesc()
+{
+    return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(NV >> 3) << 17) | ((uint32_t)(128 >> 4) << 24);
+}
 
 struct TcSmem {
     unsigned char ring[TC_RING];   // operand ring: each step's A chunk, then its B chunk
-    __nv_bfloat16 stg[4][1024];    // pass 1 epilogue: 4 K cores of t_b per warp (also takes
-                                   // the MMA's reads of unused A rows past the ring's end)
+    __nv_bfloat16 stg[4][32 * TC_NMAX];  // pass 1 epilogue: 4 K cores of t_b per warp (also
+                                         // takes the MMA's reads of unused A rows past the ring)
     uint64_t full[TC_SLOTS], empty[TC_SLOTS], accf[2], acce[2], fin;
     uint32_t slot_a[TC_SLOTS], slot_b[TC_SLOTS];  // shared addresses of a step's A and B
     int slot_meta[TC_SLOTS];                       // a step's meta word
@@ -207,12 +212,25 @@ __device__ __forceinline__ void bulk_g2s_first(void* dst, const void* src, unsig
         : "memory");
 }
 
-__device__ __forceinline__ void tc_mma(uint32_t d, uint64_t ad, uint64_t bd, uint32_t acc)
+__device__ __forceinline__ void tc_mma(uint32_t d, uint64_t ad, uint64_t bd, uint32_t idesc, uint32_t acc)
 {
     asm volatile(
         "{\n .reg .pred pd;\n setp.ne.b32 pd, %4, 0;\n"
         " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, pd;\n}" ::"r"(d),
-        "l"(ad), "l"(bd), "r"(TC_IDESC), "r"(acc));
+        "l"(ad), "l"(bd), "r"(idesc), "r"(acc));
+}
+
+__device__ __forceinline__ void tc_ld32(uint32_t taddr, uint32_t (&v)[32])
+{
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, "
+        "%13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, "
+        "[%32];"
+        : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+          "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15]),
+          "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23]),
+          "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
+        : "r"(taddr));
 }
 
 __device__ __forceinline__ void tc_commit(uint64_t* bar)
@@ -248,16 +266,17 @@ __device__ __forceinline__ uint32_t pack_bf16(float lo, float hi)
     return *reinterpret_cast<const uint32_t*>(&v);
 }
 
-// Steps of CTA c: [cta[c].y, cta[c+1].y); its jobs: [cta[c].x, cta[c+1].x).
-// Pass 1 (MODE 0) writes t_b cores at Bbuf + tb_off, K core kc of job j (a stack) to 512-byte
-// unit map[16 j + kc]; pass 2 (MODE 1) writes (add_y: adds to) rows of Y, tile row i to Y
-// row map[r0 + i].
-template <int MODE>
+// Steps of CTA c: [cta[c].y, cta[c+1].y); its jobs: [cta[c].x, cta[c+1].x).  NV vectors per
+// pass (MMA N); B K cores are NV * 16 bytes.  Pass 1 (MODE 0) writes t_b cores, K core kc of
+// job j (a stack) to B K core tb_kc + map[16 j + kc]; pass 2 (MODE 1) writes (add_y: adds
+// to) rows of Y, tile row i to Y row map[r0 + i].
+template <int MODE, int NV>
 __global__ void __launch_bounds__(TC_THREADS, 1)
     k_tc_pass(const TcStep* __restrict__ steps, const TcJob* __restrict__ jobs, const int2* __restrict__ cta,
-              const char* __restrict__ A, char* Bbuf, long long tb_off, const int* __restrict__ map, int nrhs,
+              const char* __restrict__ A, char* Bbuf, long long tb_kc, const int* __restrict__ map, int nrhs,
               double* Y, int ldy, int add_y, int* err)
 {
+    constexpr int KB = NV * 16;
     extern __shared__ __align__(1024) unsigned char tc_raw[];
     TcSmem& sm = *reinterpret_cast<TcSmem*>(tc_raw);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -279,7 +298,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     if (warp == 5) {
-        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 64;" ::"r"(smem_u32(&sm.tmem)));
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&sm.tmem)),
+                     "n"(2 * NV));
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
     }
     __syncthreads();
@@ -302,7 +322,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
             nxt = load_step(my_steps, i0 + 32 + lane, nsteps);
             const int cnt = min(32, nsteps - i0);
             const int ks_all = (mine.meta >> 16) & 0xff;
-            const int ab = ks_all * 2 * (mine.meta & 0xff) * 128, bb = ks_all * 1024;
+            const int ab = ks_all * 2 * (mine.meta & 0xff) * 128, bb = ks_all * 2 * KB;
             __syncwarp();
             sm.step_bytes[lane] = ab + bb;
             __syncwarp();
@@ -358,8 +378,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
 #pragma unroll
                     for (int j = 0; j < TC_MAXSUB; j++)
                         if (j < nsub) {
-                            const int kb = (((mine.kss >> (4 * j)) & 15) + 1) * 1024;
-                            bulk_g2s(sm.ring + pos + boff, Bbuf + mine.b_off[j], kb, &sm.full[slot]);
+                            const int kb = (((mine.kss >> (4 * j)) & 15) + 1) * 2 * KB;
+                            bulk_g2s(sm.ring + pos + boff, Bbuf + mine.b_off[j] * KB, kb, &sm.full[slot]);
                             boff += kb;
                         }
                 }
@@ -397,13 +417,13 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                 // adds to their start-address field (16-byte units; shared addresses stay
                 // below 2^18, so the field never carries): this lane's issue rate bounds the pass.
                 const uint32_t lbo = (uint32_t)(meta & 0xff) * 128u;
-                const uint32_t d = tmem + (uint32_t)(buf * TC_N);
-                const uint64_t da = (2 * lbo) >> 4, db = 1024 >> 4;
-                uint64_t ad = smem_desc(a0, lbo, 128), bd = smem_desc(b0, TC_XGROUP, 128);
+                const uint32_t d = tmem + (uint32_t)(buf * NV);
+                const uint64_t da = (2 * lbo) >> 4, db = (2 * KB) >> 4;
+                uint64_t ad = smem_desc(a0, lbo, 128), bd = smem_desc(b0, KB, 128);
                 uint32_t acc = first ? 0u : 1u;
 #pragma unroll 4
                 for (int q = 0; q < ks_all; q++) {
-                    tc_mma(d, ad, bd, acc);
+                    tc_mma(d, ad, bd, tc_idesc<NV>(), acc);
                     acc = 1u;
                     ad += da;
                     bd += db;
@@ -445,18 +465,10 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                     break;
                 }
                 asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-                uint32_t v[32];
-                const uint32_t taddr = tmem + (uint32_t)(buf * TC_N) + ((uint32_t)(warp * 32) << 16);
-                asm volatile(
-                    "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, "
-                    "%13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, "
-                    "[%32];"
-                    : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
-                      "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]),
-                      "=r"(v[15]), "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]),
-                      "=r"(v[22]), "=r"(v[23]), "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]),
-                      "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
-                    : "r"(taddr));
+                uint32_t v[NV];
+                const uint32_t taddr = tmem + (uint32_t)(buf * NV) + ((uint32_t)(warp * 32) << 16);
+                tc_ld32(taddr, reinterpret_cast<uint32_t(&)[32]>(v[0]));
+                if (NV == 64) tc_ld32(taddr + 32, reinterpret_cast<uint32_t(&)[32]>(v[NV - 32]));
                 asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
                 asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
                 __syncwarp();
@@ -465,33 +477,35 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                     if (row < rows) {
                         double* y = Y + yrow;
 #pragma unroll
-                        for (int q = 0; q < TC_N; q++)
+                        for (int q = 0; q < NV; q++)
                             if (q < nrhs) y[(size_t)q * ldy] = (add_y ? y[(size_t)q * ldy] : 0.0) + (double)__uint_as_float(v[q]);
                     }
                 } else {
                     // term row -> B cores of pass 2 (K = term): element (term m, vector q) at byte
-                    // ((m / 8) * 4 + q / 8) * 128 + (q % 8) * 16 + (m % 8) * 2 of its block's t_b;
-                    // this warp's 32 stack rows fill the stack's K cores 4w..4w+3.  Lanes 2p, 2p+1 pair their terms into 32-bit words
-                    // (even lane: vector 2t, odd lane: vector 2t+1); 16-byte row u of the staging
-                    // sits at u ^ (2 (u / 32)), which spreads the four K cores over all banks.
+                    // ((m / 8) * NV / 8 + q / 8) * 128 + (q % 8) * 16 + (m % 8) * 2 of its block's
+                    // t_b; this warp's 32 stack rows fill the stack's K cores 4w..4w+3.  Lanes 2p,
+                    // 2p+1 pair their terms into 32-bit words (even lane: vector 2t, odd lane:
+                    // vector 2t+1); 16-byte row u of the staging (K core u / NV, vector u % NV) sits
+                    // at u ^ (2 (u / NV)), which spreads the four K cores over all banks.
                     uint32_t* stg = reinterpret_cast<uint32_t*>(sm.stg[warp]);
                     const bool odd = lane & 1;
 #pragma unroll
-                    for (int t = 0; t < 16; t++) {
+                    for (int t = 0; t < NV / 2; t++) {
                         const float v0 = __uint_as_float(v[2 * t]), v1 = __uint_as_float(v[2 * t + 1]);
                         const float x = __shfl_xor_sync(~0u, odd ? v0 : v1, 1);
                         const int q = odd ? 2 * t + 1 : 2 * t;
                         const uint32_t w = odd ? pack_bf16(x, v1) : pack_bf16(v0, x);
-                        const int u = (lane >> 3) * 32 + (q >> 3) * 8 + (q & 7);
-                        stg[(u ^ ((u >> 5) * 2)) * 4 + ((lane & 7) >> 1)] = w;
+                        const int u = (lane >> 3) * NV + q;
+                        stg[(u ^ ((lane >> 3) * 2)) * 4 + ((lane & 7) >> 1)] = w;
                     }
                     __syncwarp();
-                    uint4* dst = reinterpret_cast<uint4*>(Bbuf + tb_off);
+                    uint4* dst = reinterpret_cast<uint4*>(Bbuf);
                     const uint4* src = reinterpret_cast<const uint4*>(stg);
 #pragma unroll
-                    for (int q = 0; q < 4; q++) {
-                        const int u = q * 32 + lane;
-                        if (warp * 4 + q < (rows >> 3)) dst[(size_t)tdst[q] * 32 + lane] = src[u ^ (q * 2)];
+                    for (int it = 0; it < NV / 8; it++) {
+                        const int u = it * 32 + lane, kcl = u / NV;
+                        if (warp * 4 + kcl < (rows >> 3))
+                            dst[(size_t)(tb_kc + tdst[kcl]) * (KB / 16) + (u % NV)] = src[u ^ (kcl * 2)];
                     }
                     __syncwarp();
                 }
@@ -503,7 +517,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
     __syncthreads();
     if (warp == 5) {
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 64;" ::"r"(tmem));
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "n"(2 * NV));
     }
 }
 
@@ -537,7 +551,7 @@ void free_tc(hmg_matrix* h)
     }
     h->tc_ready = false;
     h->tc_bytes = 0;
-    h->tc_xbytes = h->tc_tbytes = 0;
+    h->tc_xkc = h->tc_tkc = 0;
     h->tc_grid = 0;
     h->tc_all_tiles = false;
     h->tc_near = false;
@@ -546,7 +560,7 @@ void free_tc(hmg_matrix* h)
 namespace {
 
 struct Chunk {
-    long long a_off, b_off;  // A arena, B buffer
+    long long a_off, b_kc;   // A arena byte, B buffer K core
     int ks, rc;              // MMAs; row cores of A
 };
 
@@ -563,13 +577,14 @@ struct JobList {
         info.push_back(j);
         cost.push_back(0.0);
     }
-    // K cores [0, kcores) of an A operand with rc row cores, in chunks of at most kcc
-    void add(long long a_off, long long b_off, int rc, int kcores, int kcc, double b_weight)
+    // K cores [0, kcores) of an A operand with rc row cores (B from K core b_kc on), in
+    // chunks of at most kcc; cost in bytes with 64 vectors
+    void add(long long a_off, long long b_kc, int rc, int kcores, int kcc, double b_weight)
     {
         for (int kc0 = 0; kc0 < kcores; kc0 += kcc) {
             const int nk = std::min(kcc, kcores - kc0);
-            chunks.push_back(Chunk{a_off + (long long)kc0 * rc * 128, b_off + (long long)kc0 * TC_XGROUP, nk / 2, rc});
-            cost.back() += (double)nk * rc * 128 + b_weight * nk * TC_XGROUP;
+            chunks.push_back(Chunk{a_off + (long long)kc0 * rc * 128, b_kc + kc0, nk / 2, rc});
+            cost.back() += (double)nk * rc * 128 + b_weight * nk * 16 * TC_NMAX;
         }
     }
     // Steps of every job: consecutive chunks share a step (merge) while their A chunks
@@ -594,13 +609,13 @@ struct JobList {
                 const Chunk& k = chunks[c];
                 const long long kab = (long long)k.ks * 2 * k.rc * 128;
                 if (!(merge && nsub > 0 && nsub < TC_MAXSUB && k.rc == (cur.meta & 0xff) && k.a_off == cur.a_off + ab &&
-                      ab + kab <= TC_ABYTES && (ks_all + k.ks) * 1024 <= TC_BBYTES))
+                      ab + kab <= TC_ABYTES && ks_all + k.ks <= TC_MAXSTEP))
                     flush();
                 if (!nsub) {
                     cur.a_off = k.a_off;
                     cur.meta = k.rc;
                 }
-                cur.b_off[nsub] = k.b_off;
+                cur.b_off[nsub] = k.b_kc;
                 cur.kss |= (k.ks - 1) << (4 * nsub);
                 nsub++;
                 ks_all += k.ks;
@@ -616,15 +631,15 @@ struct JobList {
 
 // Every copy a step issues stays inside its arena and its stage, and every job's
 // output inside its buffer: checked here, on the host, before any launch.
-bool steps_in_bounds(const JobList& L, long long abytes, long long bbytes, long long out_limit, int q)
+bool steps_in_bounds(const JobList& L, long long abytes, long long bkcores, long long out_limit, int q)
 {
     for (const TcStep& st : L.steps) {
         const int rc = st.meta & 0xff, nsub = ((st.meta >> 10) & 3) + 1, ks_all = (st.meta >> 16) & 0xff;
-        const long long ab = (long long)ks_all * 2 * rc * 128, bb = (long long)ks_all * 1024;
+        const long long ab = (long long)ks_all * 2 * rc * 128, bb = (long long)ks_all * 2 * 16 * TC_NMAX;
         int sum = 0;
         for (int j = 0; j < nsub; j++) {
             const int ks = ((st.kss >> (4 * j)) & 15) + 1;
-            if (st.b_off[j] < 0 || st.b_off[j] % 16 || st.b_off[j] + ks * 1024ll > bbytes) return false;
+            if (st.b_off[j] < 0 || st.b_off[j] + 2ll * ks > bkcores) return false;
             sum += ks;
         }
         if (sum != ks_all || rc < 1 || rc > 16 || ab > TC_ABYTES || bb > TC_BBYTES || st.a_off < 0 || st.a_off % 16 ||
@@ -729,9 +744,8 @@ hmg_status build_bf16_factors(hmg_matrix* h, bool near_tc)
     HMG_CUDA_TRY(cudaMemcpy(ts.data(), h->tile_s, sizeof(int) * nt, cudaMemcpyDeviceToHost));
     HMG_CUDA_TRY(cudaMemcpy(tr0.data(), h->tile_r0, sizeof(int) * nt, cudaMemcpyDeviceToHost));
 
-    // t_b cores (16 terms = 1 KB per group) after the X cores in the per-product B buffer
-    const long long xgroups = (h->n[1] + 7) / 8 + 4;
-    const long long xbytes = (xgroups * TC_XGROUP + 1023) & ~1023ll;
+    // B buffer of a product, in K cores: X (8 columns each), then t_b (16 terms = 2 K cores per group)
+    const long long xkc = (h->n[1] + 7) / 8 + 4;
     std::vector<long long> toff(nb, -1);
     long long tgroups = 0;
     JobList k1, k2;
@@ -781,7 +795,7 @@ hmg_status build_bf16_factors(hmg_matrix* h, bool near_tc)
                     off8 += r16 / 8;
                 }
                 k1.begin(TcJob{job, rows});
-                k1.add(vbytes, (long long)(c0 >> 3) * TC_XGROUP, rc, kw / 8, std::min(2 * TC_MAXKS, (TC_ABYTES / 128 / rc) & ~1),
+                k1.add(vbytes, c0 >> 3, rc, kw / 8, std::min(2 * TC_MAXKS, (TC_ABYTES / 128 / rc) & ~1),
                        0.25);
                 vbytes += (long long)rows * kw * 2;
             }
@@ -809,14 +823,14 @@ hmg_status build_bf16_factors(hmg_matrix* h, bool near_tc)
                 nlist.push_back(p);
                 ntile.push_back(t);
                 noff.push_back(ubytes);
-                k2.add(ubytes, (long long)(h->h_c0[b] >> 3) * TC_XGROUP, rc, kw / 8, TC_ABYTES / 128 / 16, 0.25);
+                k2.add(ubytes, h->h_c0[b] >> 3, rc, kw / 8, TC_ABYTES / 128 / 16, 0.25);
                 ubytes += (long long)rc * 8 * kw * 2;
             } else {
                 const int r16 = (h->h_rank[b] + 15) & ~15;
                 ulist.push_back(p);
                 utile.push_back(t);
                 uoff.push_back(ubytes);
-                k2.add(ubytes, xbytes + toff[b] * 2 * TC_XGROUP, rc, r16 / 8, TC_ABYTES / 128 / 16, 1.0);
+                k2.add(ubytes, xkc + toff[b] * 2, rc, r16 / 8, TC_ABYTES / 128 / 16, 1.0);
                 ubytes += (long long)rc * 8 * r16 * 2;
             }
         }
@@ -825,8 +839,8 @@ hmg_status build_bf16_factors(hmg_matrix* h, bool near_tc)
 
     k1.make_steps(false);
     k2.make_steps(true);
-    if (!steps_in_bounds(k1, vbytes, xbytes + tgroups * 2 * TC_XGROUP, (long long)kmap.size() / 16, 0) ||
-        !steps_in_bounds(k2, ubytes, xbytes + tgroups * 2 * TC_XGROUP, h->n[0], 1)) {
+    if (!steps_in_bounds(k1, vbytes, xkc + tgroups * 2, (long long)kmap.size() / 16, 0) ||
+        !steps_in_bounds(k2, ubytes, xkc + tgroups * 2, h->n[0], 1)) {
         set_error("hmg_build_bf16_factors: internal error: an operand step leaves its buffer");
         return HMG_ERR_UNSUPPORTED;
     }
@@ -888,8 +902,8 @@ hmg_status build_bf16_factors(hmg_matrix* h, bool near_tc)
         return st;
     }
     h->tc_bytes = ubytes + vbytes;
-    h->tc_xbytes = xbytes;
-    h->tc_tbytes = tgroups * 2 * TC_XGROUP;
+    h->tc_xkc = xkc;
+    h->tc_tkc = tgroups * 2;
     h->tc_grid = grid;
     h->tc_all_tiles = all_tiles;
     h->tc_near = near_tc;
@@ -897,41 +911,34 @@ hmg_status build_bf16_factors(hmg_matrix* h, bool near_tc)
     return HMG_OK;
 }
 
-hmg_status matvec_multi_tc(hmg_matrix* h, int nrhs, const double* X, int ldx, double* Y, int ldy)
+template <int NV>
+static hmg_status tc_product(hmg_matrix* h, int nrhs, const double* X, int ldx, double* Y, int ldy)
 {
     cudaStream_t s = h->stream;
     hmg_status st;
-    if (!h->tc_bbuf) {  // X and t_b cores, kept with the handle (sized by hmg_build_bf16_factors)
-        cudaError_t ce = cudaMalloc(&h->tc_bbuf, (size_t)(h->tc_xbytes + h->tc_tbytes));
-        if (ce != cudaSuccess) {
-            cudaGetLastError();
-            h->tc_bbuf = nullptr;
-            set_error("hmg_matvec_multi: allocating %lld bytes of operand space failed: %s",
-                      h->tc_xbytes + h->tc_tbytes, cudaGetErrorString(ce));
-            return ce == cudaErrorMemoryAllocation ? HMG_ERR_NOMEM : HMG_ERR_CUDA;
-        }
-    }
     char* bbuf = static_cast<char*>(h->tc_bbuf);
-    const long long xgroups = h->tc_xbytes / TC_XGROUP;
-    k_tc_x<<<(unsigned)((xgroups * TC_N + 255) / 256), 256, 0, s>>>(X, ldx, nrhs, h->perm[1], h->n[1], xgroups,
-                                                                      reinterpret_cast<uint4*>(bbuf));
+    const long long xkc = h->tc_xkc;
+    k_tc_x<NV><<<(unsigned)((xkc * NV + 255) / 256), 256, 0, s>>>(X, ldx, nrhs, h->perm[1], h->n[1], xkc,
+                                                                    reinterpret_cast<uint4*>(bbuf));
     HMG_LAUNCH_CHECK();
     const size_t smem = sizeof(TcSmem);
-    HMG_CUDA_TRY(cudaFuncSetAttribute(k_tc_pass<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    HMG_CUDA_TRY(cudaFuncSetAttribute(k_tc_pass<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    HMG_CUDA_TRY(cudaFuncSetAttribute(k_tc_pass<0, NV>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    HMG_CUDA_TRY(cudaFuncSetAttribute(k_tc_pass<1, NV>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     if (h->tc_njobs[0] > 0) {
-        k_tc_pass<0><<<h->tc_grid, TC_THREADS, smem, s>>>(
+        k_tc_pass<0, NV><<<h->tc_grid, TC_THREADS, smem, s>>>(
             reinterpret_cast<const TcStep*>(h->tc_steps[0]), reinterpret_cast<const TcJob*>(h->tc_jobs[0]),
-            reinterpret_cast<const int2*>(h->tc_cta[0]), static_cast<const char*>(h->tc_v), bbuf, h->tc_xbytes,
-            h->tc_kmap, 0, nullptr, 0, 0, h->dev_err);
+            reinterpret_cast<const int2*>(h->tc_cta[0]), static_cast<const char*>(h->tc_v), bbuf, xkc, h->tc_kmap, 0,
+            nullptr, 0, 0, h->dev_err);
         HMG_LAUNCH_CHECK();
     }
     if (!h->tc_near && h->ndense > 0) {
-        // the near field in FP32 on the CUDA cores writes every row of Y first
+        // the near field in FP32 on the CUDA cores writes every row of Y first (32 vectors a pass)
         float* xm = nullptr;
-        if ((st = dalloc(&xm, (size_t)h->n[1] * TC_N, s))) return st;
-        launch_gather_multi32(h, X, ldx, nrhs, xm);
-        st = launch_tile_multi32_dense(h, xm, nrhs, Y, ldy);
+        if ((st = dalloc(&xm, (size_t)h->n[1] * 32, s))) return st;
+        for (int j0 = 0; j0 < nrhs && !st; j0 += 32) {
+            launch_gather_multi32(h, X + (size_t)j0 * ldx, ldx, std::min(32, nrhs - j0), xm);
+            st = launch_tile_multi32_dense(h, xm, std::min(32, nrhs - j0), Y + (size_t)j0 * ldy, ldy);
+        }
         dfree(xm, s);
         if (st) return st;
     } else if (!h->tc_all_tiles) {
@@ -940,13 +947,29 @@ hmg_status matvec_multi_tc(hmg_matrix* h, int nrhs, const double* X, int ldx, do
     }
     const int add_y = !h->tc_near && h->ndense > 0;
     if (h->tc_njobs[1] > 0) {
-        k_tc_pass<1><<<h->tc_grid, TC_THREADS, smem, s>>>(
+        k_tc_pass<1, NV><<<h->tc_grid, TC_THREADS, smem, s>>>(
             reinterpret_cast<const TcStep*>(h->tc_steps[1]), reinterpret_cast<const TcJob*>(h->tc_jobs[1]),
             reinterpret_cast<const int2*>(h->tc_cta[1]), static_cast<const char*>(h->tc_u), bbuf, 0, h->perm[0], nrhs,
             Y, ldy, add_y, h->dev_err);
         HMG_LAUNCH_CHECK();
     }
     return HMG_OK;
+}
+
+// up to 64 vectors in one pass: MMAs of N = 32 for 2..32 vectors, N = 64 for 33..64
+hmg_status matvec_multi_tc(hmg_matrix* h, int nrhs, const double* X, int ldx, double* Y, int ldy)
+{
+    if (!h->tc_bbuf) {  // X and t_b cores, kept with the handle, sized for 64 vectors
+        const size_t bytes = (size_t)(h->tc_xkc + h->tc_tkc) * 16 * TC_NMAX;
+        cudaError_t ce = cudaMalloc(&h->tc_bbuf, bytes);
+        if (ce != cudaSuccess) {
+            cudaGetLastError();
+            h->tc_bbuf = nullptr;
+            set_error("hmg_matvec_multi: allocating %zu bytes of operand space failed: %s", bytes, cudaGetErrorString(ce));
+            return ce == cudaErrorMemoryAllocation ? HMG_ERR_NOMEM : HMG_ERR_CUDA;
+        }
+    }
+    return nrhs > 32 ? tc_product<64>(h, nrhs, X, ldx, Y, ldy) : tc_product<32>(h, nrhs, X, ldx, Y, ldy);
 }
 
 }  // namespace hmg

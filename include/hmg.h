@@ -137,7 +137,7 @@ hmg_status hmg_full_matvec_rows(hmg_matrix* h, const double* x, const int* rows,
  * factors (hmg_precompute_aca with HMG_PREC_FP32, ranks <= 128) into BF16 copies laid
  * out as tcgen05 operands, and with near_precision HMG_PREC_BF16 its FP32 stored near
  * field (hmg_precompute_dense with HMG_PREC_FP32) too.  Afterwards hmg_matvec_multi
- * with 2..32 vectors computes t_b = V_b^T X_b and U t_b on the tensor cores with BF16
+ * with 2..64 vectors computes t_b = V_b^T X_b and U t_b on the tensor cores with BF16
  * operands (X and t_b rounded to BF16) and FP32 accumulation; the near field runs
  * there as well (HMG_PREC_BF16) or on the CUDA cores in FP32 (HMG_PREC_FP32).  Results
  * agree with the FP32 products to ~1e-3 (BF16 rounding).  Single-vector products keep
@@ -169,10 +169,11 @@ hmg_status hmg_group_create(hmg_matrix** out, hmg_matrix* const* sets, int count
 /* offsets[0..count] of a group's rows (set 0) or columns (set 1); offsets[count] = n */
 hmg_status hmg_group_offsets(hmg_matrix* h, int set, int64_t* offsets);
 
-/* Y = H X for 1 <= nrhs <= 32 vectors: X (n2 x nrhs) and Y (n1 x nrhs) are device
+/* Y = H X for 1 <= nrhs <= 64 vectors: X (n2 x nrhs) and Y (n1 x nrhs) are device
  * FP64 column-major with leading dimensions ldx >= n2, ldy >= n1, caller order.  The
- * stored H-matrix is read once for all vectors (FP32 / FP64 storage with a stored
- * near field; otherwise one product per vector).  Same arithmetic as hmg_matvec;
+ * stored H-matrix is read once per 32 vectors (FP32 / FP64 storage with a stored near
+ * field; otherwise one product per vector), once for all 64 with tensor-core operands
+ * (hmg_build_tensor_core_operands).  Same arithmetic as hmg_matvec;
  * asynchronous on the handle's stream.  No reference counterpart (the reference
  * multiplies one vector per apply_h_matrix_mvp call, hmglib.cu:271-286). */
 hmg_status hmg_matvec_multi(hmg_matrix* h, int nrhs, const double* X, int ldx, double* Y, int ldy);

@@ -30,7 +30,7 @@ def _columns(torch, H, X):
 
 
 @pytest.mark.parametrize("prec,tol", [(0, 1e-13), (1, 1e-6), (2, 1e-6)], ids=["fp64", "fp32", "mixed"])
-@pytest.mark.parametrize("nrhs", [2, 5, 16, 32])
+@pytest.mark.parametrize("nrhs", [2, 5, 16, 32, 45])
 def test_multi_matches_single(hmg, cuda, prec, tol, nrhs):
     torch = cuda
     H, n = _build(hmg, prec)
@@ -68,7 +68,7 @@ def test_multi_leading_dimensions_and_errors(hmg, cuda):
     for j in range(nrhs):
         assert rel_err(Y[j].cpu().numpy(), ref[j].cpu().numpy()) < 1e-6
     assert float(Yb[:, n:].abs().max()) == 0.0  # nothing written past n rows
-    for bad in (0, 33):
+    for bad in (0, 65):
         Xe = torch.zeros(bad if bad else 1, n, dtype=torch.float64, device="cuda")
         with pytest.raises(hmg.HmgError):
             H._call("hmg_matvec_multi", bad, Xe.data_ptr(), n, Xe.data_ptr(), n)
