@@ -691,6 +691,71 @@ def run_serve(a, rank, world):
     return 0
 
 
+def run_legacy(a, rank, world):
+    """The reference's own configurations (tests/golden: config 1, N=16384 2D, exp(-r^2)
+    with coordinates scaled by 1/sqrt(0.1), leaf 64, max rule, fixed rank 64; and the
+    N=8192 3D case of its Bessel-Y kernel, rank 16), in its arithmetic (FP64 factors and
+    near field, fixed-rank ACA): the engine's setup, compression, near-field fill and
+    H-matvec timed with CUDA events, beside the reference's own GPU build timed on a
+    B200 by the fixture generator (the same inputs; tests/golden/make_golden.py)."""
+    import torch
+
+    import hmglib_b200 as hmg
+    sys.path.insert(0, os.path.join(os.path.dirname(os.path.abspath(__file__)), "tests"))
+    from golden.make_golden import CASES, case_inputs
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    stream = torch.cuda.default_stream()
+    out = {}
+    for name in ("config1_parity", "uniform3d_matern"):
+        c = CASES[name]
+        p1, p2, x = case_inputs(c)
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(10)]
+        H = hmg.HMatrix(p1.shape[1], p2.shape[1], p1.shape[0])
+        ev[0].record(stream)
+        H.set_points(0, p1)
+        H.set_points(1, p2)
+        H.setup(c["eta"], c["c_leaf"], rule=hmg.ADMISSIBLE_MAX)
+        H.set_kernel(c["kernel"], 0.0, 0.0)
+        ev[1].record(stream)
+        H.precompute_aca(c["k"], 0.0, hmg.PREC_FP64)
+        ev[2].record(stream)
+        H.precompute_dense(hmg.PREC_FP64)
+        ev[3].record(stream)
+        dx = torch.from_numpy(x).cuda()
+        dy = torch.empty(p1.shape[1], dtype=torch.float64, device="cuda")
+        for _ in range(a.warmup):
+            H.matvec(dx, dy)
+        ev[4].record(stream)
+        for _ in range(a.steps):
+            H.matvec(dx, dy)
+        ev[5].record(stream)
+        H.full_matvec(dx, dy)
+        ev[6].record(stream)
+        torch.cuda.synchronize()
+        g = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "tests", "golden", name + ".npz"))
+        ref = [float(v) for v in g["timings_ms"]]
+        out[name] = {
+            "n": int(p1.shape[1]), "dim": int(p1.shape[0]), "rank": c["k"], "leaf": c["c_leaf"],
+            "engine_ms": {"setup": ev[0].elapsed_time(ev[1]), "precompute_aca": ev[1].elapsed_time(ev[2]),
+                          "precompute_dense": ev[2].elapsed_time(ev[3]),
+                          "apply": ev[4].elapsed_time(ev[5]) / a.steps, "apply_full": ev[5].elapsed_time(ev[6])},
+            "reference_gpu_ms": {"setup": ref[0], "precompute_aca": ref[1], "precompute_dense": ref[2],
+                                 "apply": ref[3], "apply_full": ref[4]},
+        }
+        out[name]["apply_speedup"] = ref[3] / out[name]["engine_ms"]["apply"]
+        H.close()
+    c1 = out["config1_parity"]
+    line = {"metric": "H-matvecs/s, the reference's configuration 1 (N=16384 2D, FP64, fixed rank 64)",
+            "value": 1000.0 / c1["engine_ms"]["apply"], "unit": "matvec/s", "n_gpus": 1, "steps": a.steps,
+            "warmup": a.warmup, "ms_per_step": c1["engine_ms"]["apply"], "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "reference_configurations", "cases": list(out)}, "results": out}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    return 0
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -708,7 +773,7 @@ def main(argv=None):
                     help="arithmetic of the products over FP32/mixed storage")
     ap.add_argument("--variant", type=int, default=1, choices=[0, 1],
                     help="product kernels: 1 plain 16-byte loads (default), 0 bulk-copy streaming")
-    ap.add_argument("--workload", default="uniform3d", choices=["uniform3d", "group", "serve", "precision"],
+    ap.add_argument("--workload", default="uniform3d", choices=["uniform3d", "group", "serve", "precision", "legacy"],
                     help="uniform3d: the N=2^20 headline; group: many small H-matrices as one; "
                          "serve: the request loop over resident H-matrices")
     ap.add_argument("--serve-requests", type=int, default=300)
@@ -727,6 +792,8 @@ def main(argv=None):
         return run_group(a, rank, world) if rank == 0 else 0
     if a.workload == "serve":
         return run_serve(a, rank, world) if rank == 0 else 0
+    if a.workload == "legacy":
+        return run_legacy(a, rank, world)
     if a.workload == "precision":
         return run_precision(a, rank, world) if rank == 0 else 0
     if world > 1:
