@@ -610,9 +610,12 @@ def run_serve(a, rank, world):
     ~96 GB) and a Poisson stream at
     2000 requests/s (seed 4): 80% single-vector products, 15% 8-vector kernel-ridge
     solves (shift 1e-3 N, relative residual 1e-4), 5% new point sets of 2^14-2^18
-    points, under a 120 GB budget.  Reports p50/p99 latency and throughput against the
-    plain FP64 one-request-at-a-time path (FP64 products, one vector per call, solves
-    by hmg_cg_solve per column) on the same H-matrices and the first requests."""
+    points, under a 120 GB budget, with latency targets (--serve-slo-matvec,
+    --serve-slo-solve seconds): a request whose predicted completion misses its target
+    is refused on arrival.  Reports p50/p99 latency of the completed requests, the
+    refused counts and throughput against the plain FP64 one-request-at-a-time path
+    (FP64 products, one vector per call, solves by hmg_cg_solve per column) on the same
+    H-matrices and the first requests."""
     import torch
 
     import hmglib_b200 as hmg
@@ -621,7 +624,8 @@ def run_serve(a, rank, world):
     torch.cuda.set_device(local)
     sizes = [1 << 16] * 4 + [1 << 17, 1 << 18, 1 << 19, 1 << 20]
     t0 = time.perf_counter()
-    srv = serve.Server(budget_bytes=120e9)
+    slo = {"matvec": a.serve_slo_matvec, "solve": a.serve_slo_solve}
+    srv = serve.Server(budget_bytes=120e9, slo_s=slo)
     for i, n in enumerate(sizes):
         st = torch.cuda.Stream()
         H = serve.build_hmatrix(synth.uniform_points(n, 3, 4000 + i), hmg.KERNEL_MATERN32, 0.2, 1e-4,
@@ -633,21 +637,26 @@ def run_serve(a, rank, world):
                                   tol=1e-4)
     print(f"serve: resident {srv.used_bytes() / 1e9:.1f} GB built in {t_build:.1f} s; {len(reqs)} requests",
           file=sys.stderr, flush=True)
-    # warm-up: one small batch of every kind on every resident matrix
+    # warm-up: a product and three solve iterations on every resident matrix (seeds the
+    # service-time estimates the latency targets are checked against)
     warm = [serve.Matvec(m, np.zeros(n)) for m, n in enumerate(sizes)]
+    warm += [serve.Solve(m, synth.uniform01(77 + m, 8 * n).reshape(8, n), 1e-3 * n, tol=1e-12, maxit=3)
+             for m, n in enumerate(sizes)]
     srv.run(warm)
+    srv.iters_per_solve = 30.0  # the warm-up solves stop at 3 iterations: not a solve length
     with ClockSampler(local) as clk:
         done, wall = srv.run(reqs, time_limit=300.0)
     print(f"serve: {len(reqs)} requests served in {wall:.1f} s", file=sys.stderr, flush=True)
     lat = serve.latency_summary(done)
-    solves = [q for q in done if isinstance(q, serve.Solve) and q.done is not None]
+    solves = [q for q in done if isinstance(q, serve.Solve) and q.done is not None and q.rejected is None]
     solve_stats = {"iters_mean": float(np.mean([q.iters for q in solves])) if solves else None,
                    "converged": int(sum(bool((q.relres <= q.tol).all()) for q in solves)),
                    "count": len(solves)}
     builds = [q for q in done if isinstance(q, serve.Build)]
     build_stats = {"admitted": sum(q.mid is not None for q in builds), "refused": sum(q.rejected is not None for q in builds)}
-    n_done = sum(q.done is not None for q in done)
-    batches = [q.batch for q in done if isinstance(q, serve.Matvec)]
+    n_done = sum(q.done is not None and getattr(q, "rejected", None) is None for q in done)
+    n_refused = sum(getattr(q, "rejected", None) is not None for q in done)
+    batches = [q.batch for q in done if isinstance(q, serve.Matvec) and q.rejected is None]
     # the plain path: one request at a time, FP64 products, no batching, no overlap
     nb = min(a.serve_baseline, len(reqs))
     base = reqs[:nb]
@@ -675,8 +684,11 @@ def run_serve(a, rank, world):
         "ms_per_step": 1000.0 * wall / max(1, n_done), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": "serve_8resident_matern3d_poisson2000", "sizes": sizes, "aca_eps": 1e-4, "leaf": 64,
-                   "storage": "mixed", "budget_gb": 120, "requests": len(reqs), "mix": [0.8, 0.15, 0.05]},
-        "latency": lat, "matvec_batch": {"mean": float(np.mean(batches)), "max": int(np.max(batches))},
+                   "storage": "mixed", "budget_gb": 120, "requests": len(reqs), "mix": [0.8, 0.15, 0.05],
+                   "latency_targets_s": slo},
+        "latency": lat, "refused": n_refused, "admitted_fraction": 1.0 - n_refused / max(1, len(reqs)),
+        "matvec_batch": {"mean": float(np.mean(batches)) if batches else None,
+                         "max": int(np.max(batches)) if batches else None},
         "solves": solve_stats, "builds": build_stats,
         "plain_fp64_one_at_a_time": {"requests": nb, "seconds": t_base, "requests_per_s": nb / t_base,
                                      "throughput_ratio_served_vs_plain": (n_done / wall) / (nb / t_base)},
@@ -777,6 +789,8 @@ def main(argv=None):
                     help="uniform3d: the N=2^20 headline; group: many small H-matrices as one; "
                          "serve: the request loop over resident H-matrices")
     ap.add_argument("--serve-requests", type=int, default=300)
+    ap.add_argument("--serve-slo-matvec", type=float, default=1.0, help="latency target of a product, seconds")
+    ap.add_argument("--serve-slo-solve", type=float, default=10.0, help="latency target of a solve, seconds")
     ap.add_argument("--cg-maxit", type=int, default=600)
     ap.add_argument("--serve-baseline", type=int, default=60)
     ap.add_argument("--group-count", type=int, default=512)

@@ -24,6 +24,15 @@ as they arrive:
 ``run(requests)`` replays an arrival timeline (seconds from the start) and returns
 the requests with their completion times; latency = completion - arrival, measured
 on the host clock when the result's CUDA event has completed.
+
+Latency targets (``Server(slo_s={"matvec": ..., "solve": ...})``): a product or solve
+is admitted only if its predicted completion fits its class's target; otherwise it is
+refused at once (``rejected`` set, no result).  The prediction: the work queued and
+running on its own H-matrix's stream plus its own runs in order (A seconds); the other
+H-matrices' streams interleave with it on the GPU, adding at most their outstanding
+work and at most (busy streams - 1) x A.  Work is counted in GPU seconds of a product
+batch and of a solve iteration per resident H-matrix (exponential averages of CUDA-event
+timings, seeded from the stored bytes at HBM speed) and the mean iterations per solve.
 """
 from __future__ import annotations
 
@@ -39,6 +48,8 @@ from .hmatrix import HMatrix
 
 MAX_BATCH = 32       # vectors per product pass
 MAX_SOLVES = 2       # solves advancing at once per H-matrix (their vectors live on the device)
+HBM_BYTES_PER_S = 5.0e12   # seed of the service-time estimates: stored bytes read at this rate
+EWMA = 0.25          # weight of a new timing in the service-time estimates
 
 
 @dataclass
@@ -49,6 +60,7 @@ class Matvec:
     y: np.ndarray | None = None
     done: float | None = None
     batch: int = 0
+    rejected: str | None = None
 
 
 @dataclass
@@ -63,6 +75,7 @@ class Solve:
     iters: int = 0
     relres: np.ndarray | None = None
     done: float | None = None
+    rejected: str | None = None
 
 
 @dataclass
@@ -89,6 +102,33 @@ class _Resident:
     waiting_solves: collections.deque = field(default_factory=collections.deque)
     solves: list = field(default_factory=list)
     inflight: list = field(default_factory=list)   # (event, finisher)
+    batch_s: float = 0.0     # GPU seconds of one product batch (estimate)
+    iter_s: float = 0.0      # GPU seconds of one solve iteration (estimate)
+
+
+def outstanding_seconds(queued_batches, running_batches, solve_iters_left, batch_s, iter_s):
+    """GPU seconds of the work queued and running, per resident H-matrix: its product
+    batches (queued and in flight) times the batch estimate plus the solve iterations
+    still to run times the iteration estimate."""
+    return [(q + r) * b + it * i for q, r, it, b, i in
+            zip(queued_batches, running_batches, solve_iters_left, batch_s, iter_s)]
+
+
+def predict_latency(own_queue_s: float, own_s: float, others_s: float, busy_streams: int) -> float:
+    """Completion of a request: its stream's work and its own in order (A), plus the
+    other streams' work interleaved with it: at most all of it and at most
+    (busy streams - 1) x A."""
+    a = own_queue_s + own_s
+    return a + min(others_s, max(0, busy_streams - 1) * a)
+
+
+def admit(predicted_s: float, target_s: float | None) -> bool:
+    """A request is admitted when its predicted completion fits its latency target."""
+    return target_s is None or predicted_s <= target_s
+
+
+def ewma(old: float, new: float, w: float = EWMA) -> float:
+    return new if old <= 0.0 else (1.0 - w) * old + w * new
 
 
 def build_hmatrix(points, kind, param, eps, precision, stream=None, max_rank=64, eta=1.5, leaf=None):
@@ -112,11 +152,13 @@ def resident_bytes(H: HMatrix) -> int:
 
 
 class Server:
-    def __init__(self, budget_bytes: float, device: int = 0):
+    def __init__(self, budget_bytes: float, device: int = 0, slo_s: dict | None = None):
         import torch
         self.torch = torch
         self.device = device
         self.budget = int(budget_bytes)
+        self.slo = dict(slo_s or {})   # class name ("matvec", "solve") -> latency target, seconds
+        self.iters_per_solve = 30.0    # estimate, updated as solves finish
         self.res: dict[int, _Resident] = {}
         self.next_id = 0
         self.builds: collections.deque = collections.deque()
@@ -131,7 +173,11 @@ class Server:
     def add(self, H: HMatrix, stream, pinned: bool = True) -> int:
         mid = self.next_id
         self.next_id += 1
-        self.res[mid] = _Resident(H, stream, resident_bytes(H), pinned)
+        nb = resident_bytes(H)
+        # seeds: one read of the stored bytes per batch; a solve iteration reads them once
+        # for all its vectors plus the vector updates
+        self.res[mid] = _Resident(H, stream, nb, pinned, batch_s=nb / HBM_BYTES_PER_S,
+                                  iter_s=1.5 * nb / HBM_BYTES_PER_S)
         bpp = self.res[mid].nbytes / max(1, H.n1)
         self.bytes_per_point = bpp if self.bytes_per_point is None else max(self.bytes_per_point, bpp)
         return mid
@@ -148,11 +194,28 @@ class Server:
         return True
 
     # -- request intake ----------------------------------------------------------
+    def outstanding(self) -> dict:
+        mids = list(self.res)
+        rs = [self.res[m] for m in mids]
+        left = [sum(max(1.0, self.iters_per_solve - st["it"]) for st in r.solves if st["final"] is None)
+                + self.iters_per_solve * len(r.waiting_solves) for r in rs]
+        w = outstanding_seconds([-(-len(r.matvecs) // MAX_BATCH) for r in rs], [len(r.inflight) for r in rs],
+                                left, [r.batch_s for r in rs], [r.iter_s for r in rs])
+        return dict(zip(mids, w))
+
     def submit(self, req, now: float):
-        if isinstance(req, Matvec):
-            self.res[req.mid].matvecs.append(req)
-        elif isinstance(req, Solve):
-            self.res[req.mid].waiting_solves.append(req)
+        if isinstance(req, (Matvec, Solve)):
+            r = self.res[req.mid]
+            own = r.batch_s if isinstance(req, Matvec) else self.iters_per_solve * r.iter_s
+            cls = "matvec" if isinstance(req, Matvec) else "solve"
+            w = self.outstanding()
+            busy = 1 + sum(1 for m, v in w.items() if m != req.mid and v > 0)
+            pred = predict_latency(w[req.mid], own, sum(v for m, v in w.items() if m != req.mid), busy)
+            if not admit(pred, self.slo.get(cls)):
+                req.rejected = f"predicted {pred:.2f} s > {cls} target {self.slo[cls]:.2f} s"
+                req.done = time.perf_counter()
+                return
+            (r.matvecs if isinstance(req, Matvec) else r.waiting_solves).append(req)
         else:
             self.builds.append(req)
 
@@ -161,6 +224,8 @@ class Server:
         torch = self.torch
         batch = [r.matvecs.popleft() for _ in range(min(MAX_BATCH, len(r.matvecs)))]
         with torch.cuda.stream(r.stream):
+            e_start = torch.cuda.Event(enable_timing=True)
+            e_start.record(r.stream)
             X = torch.from_numpy(np.stack([q.x for q in batch])).pin_memory().cuda(non_blocking=True)
             Y = torch.empty(len(batch), r.H.n1, dtype=torch.float64, device="cuda")
             if len(batch) == 1:
@@ -169,7 +234,7 @@ class Server:
                 r.H.matvec_multi(X, Y)
             Yh = torch.empty(Y.shape, dtype=torch.float64, pin_memory=True)
             Yh.copy_(Y, non_blocking=True)
-            ev = torch.cuda.Event()
+            ev = torch.cuda.Event(enable_timing=True)
             ev.record(r.stream)
 
         def finish(t):
@@ -177,6 +242,7 @@ class Server:
                 q.y = Yh[j].numpy().copy()
                 q.done = t
                 q.batch = len(batch)
+            r.batch_s = ewma(r.batch_s, e_start.elapsed_time(ev) * 1e-3)
         r.inflight.append((ev, finish, (X, Y)))
         r.last_use = now
 
@@ -202,11 +268,15 @@ class Server:
             if not ev.query():
                 return False
             req.X, req.iters, req.relres, req.done = Xh.numpy().copy(), it, rel, time.perf_counter()
+            self.iters_per_solve = ewma(self.iters_per_solve, float(it))
             return True
         # residual norms come back one iteration late; at most two iterations in flight
         converged = False
         while st["checks"] and st["checks"][0][0].query():
             ev, host, it = st["checks"].popleft()
+            if st.get("last_ev") is not None:
+                r.iter_s = ewma(r.iter_s, st["last_ev"].elapsed_time(ev) * 1e-3)
+            st["last_ev"] = ev
             rel = np.sqrt(host[0].numpy() / np.maximum(host[1].numpy(), 1e-300))
             if (rel <= req.tol).all() or it >= req.maxit:
                 converged = True
@@ -246,7 +316,7 @@ class Server:
                     torch.empty(rr_new.shape, dtype=torch.float64, pin_memory=True))
             host[0].copy_(rr_new, non_blocking=True)
             host[1].copy_(st["rr0"], non_blocking=True)
-            ev = torch.cuda.Event()
+            ev = torch.cuda.Event(enable_timing=True)
             ev.record(r.stream)
             st["checks"].append((ev, host, st["it"]))
         r.last_use = now
@@ -344,12 +414,18 @@ class Server:
 
 
 def latency_summary(reqs):
+    """p50 / p99 / max latency per request class over the requests that completed
+    (refused ones are counted apart)."""
     out = {}
     for name, cls in (("matvec", Matvec), ("solve", Solve), ("build", Build), ("all", object)):
-        lat = np.array([q.done - q.arrival for q in reqs if isinstance(q, cls) and q.done is not None])
-        if lat.size:
-            out[name] = {"count": int(lat.size), "p50_ms": float(np.percentile(lat, 50) * 1e3),
-                         "p99_ms": float(np.percentile(lat, 99) * 1e3), "max_ms": float(lat.max() * 1e3)}
+        mine = [q for q in reqs if isinstance(q, cls)]
+        lat = np.array([q.done - q.arrival for q in mine if q.done is not None and getattr(q, "rejected", None) is None])
+        refused = sum(1 for q in mine if getattr(q, "rejected", None) is not None)
+        if lat.size or refused:
+            out[name] = {"count": int(lat.size), "refused": int(refused)}
+            if lat.size:
+                out[name].update({"p50_ms": float(np.percentile(lat, 50) * 1e3),
+                                  "p99_ms": float(np.percentile(lat, 99) * 1e3), "max_ms": float(lat.max() * 1e3)})
     return out
 
 

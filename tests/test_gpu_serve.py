@@ -38,7 +38,8 @@ def test_mixed_stream_matches_alone(hmg, cuda):
     done, wall = srv.run(reqs, time_limit=300.0)
     assert all(q.done is not None for q in done)
     lat = serve.latency_summary(done)
-    assert lat["all"]["count"] == len(reqs) and lat["all"]["p99_ms"] >= lat["all"]["p50_ms"] > 0
+    assert lat["all"]["count"] + lat["all"]["refused"] == len(reqs)
+    assert lat["all"]["p99_ms"] >= lat["all"]["p50_ms"] > 0
     batched = 0
     for q in done:
         if isinstance(q, serve.Matvec):
@@ -66,3 +67,29 @@ def test_mixed_stream_matches_alone(hmg, cuda):
     assert srv.used_bytes() <= srv.budget
     for mid in list(srv.res):
         srv.res.pop(mid).H.close()
+
+
+def test_latency_targets_refuse_on_arrival(hmg, cuda):
+    """With a latency target of a few batch times, products arriving behind a backlog
+    are refused at once (no result) while the admitted ones still equal their products
+    served alone."""
+    torch = cuda
+    from hmglib_b200 import serve, synth
+    hmg.synth = synth
+    sizes = [6000]
+    res = _resident(hmg, serve, torch, sizes, [hmg.PREC_FP32])
+    # a target of 2.5 batch times (the seed estimate): the first products are admitted,
+    # those that arrive behind a batch in flight and a queued one are refused
+    target = 2.5 * serve.resident_bytes(res[0][0]) / serve.HBM_BYTES_PER_S
+    srv = serve.Server(budget_bytes=16e9, slo_s={"matvec": target})
+    for H, st in res:
+        srv.add(H, st)
+    reqs = serve.poisson_requests(40, 1e5, sizes, seed=6, mix=(1.0, 0.0, 0.0))
+    done, _ = srv.run(reqs, time_limit=120.0)
+    refused = [q for q in done if q.rejected is not None]
+    served = [q for q in done if q.rejected is None]
+    assert refused and served and all(q.y is None for q in refused)
+    for q in served:
+        assert rel_err(q.y, res[0][0].matvec(q.x)) < 1e-6
+    for H, _ in res:
+        H.close()

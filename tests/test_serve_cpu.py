@@ -24,3 +24,30 @@ def test_poisson_mix_is_seeded_and_shaped():
             assert q.B.shape == (8, sizes[q.mid]) and q.shift > 0
         else:
             assert q.points.shape[0] == 3 and 2 ** 14 - 1 <= q.points.shape[1] <= 2 ** 18 + 1
+
+
+def test_admission_against_latency_targets():
+    # outstanding work: per H-matrix (queued + running batches) x batch time + solve
+    # iterations left x iteration time, summed over the H-matrices sharing the GPU
+    w = serve.outstanding_seconds([2, 0], [1, 1], [10.0, 0.0], [0.1, 0.2], [0.01, 0.5])
+    assert abs(w[0] - (3 * 0.1 + 10 * 0.01)) < 1e-12 and abs(w[1] - 0.2) < 1e-12
+    # own stream in order (A = 0.3 + 0.1); others interleave: at most their work, at
+    # most (busy - 1) x A
+    assert abs(serve.predict_latency(0.3, 0.1, 5.0, 3) - (0.4 + 0.8)) < 1e-12
+    assert abs(serve.predict_latency(0.3, 0.1, 0.2, 3) - (0.4 + 0.2)) < 1e-12
+    assert abs(serve.predict_latency(0.0, 0.1, 9.0, 1) - 0.1) < 1e-12
+    assert serve.admit(0.9, 1.0) and not serve.admit(1.1, 1.0) and serve.admit(1e9, None)
+    assert serve.ewma(0.0, 2.0) == 2.0 and abs(serve.ewma(1.0, 2.0, 0.25) - 1.25) < 1e-12
+
+
+def test_latency_summary_counts_refused_apart():
+    a = serve.Matvec(0, np.zeros(3), arrival=0.0)
+    a.done = 0.5
+    b = serve.Matvec(0, np.zeros(3), arrival=0.1)
+    b.done, b.rejected = 0.1, "predicted 2.00 s > matvec target 1.00 s"
+    c = serve.Solve(0, np.zeros((2, 3)), 1.0, arrival=0.0)
+    c.done = 2.0
+    lat = serve.latency_summary([a, b, c])
+    assert lat["matvec"]["count"] == 1 and lat["matvec"]["refused"] == 1
+    assert abs(lat["matvec"]["p99_ms"] - 500.0) < 1e-9
+    assert lat["all"]["count"] == 2 and lat["all"]["refused"] == 1 and lat["solve"]["refused"] == 0
