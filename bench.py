@@ -253,6 +253,8 @@ def run_engine(a, rank, world):
     dx = torch.from_numpy(x).cuda()
     dy = torch.empty(n, dtype=torch.float64, device="cuda")
     stream = torch.cuda.default_stream()
+    # the V^T x task size and grid for this H-matrix (hmg_autotune), before any timing
+    tuned = H.autotune(reps=3) if not a.no_autotune else None
     for _ in range(max(3, a.warmup)):
         H.matvec(dx, dy)
     H.synchronize()
@@ -354,6 +356,7 @@ def run_engine(a, rank, world):
         "clocks": clk.summary(),
         "graph_replay": {"ms_per_step": ms_graph / a.steps, "value": world * 1000.0 * a.steps / ms_graph,
                          "unit": "matvec/s"},
+        "autotune": tuned,
     }
     if a.nrhs > 1:
         line["multi_rhs"] = multi_rhs_timing(torch, H, x, n, a.nrhs, a.steps, stream, world, err)
@@ -788,6 +791,7 @@ def main(argv=None):
     ap.add_argument("--workload", default="uniform3d", choices=["uniform3d", "group", "serve", "precision", "legacy"],
                     help="uniform3d: the N=2^20 headline; group: many small H-matrices as one; "
                          "serve: the request loop over resident H-matrices")
+    ap.add_argument("--no-autotune", action="store_true", help="keep the default V^T x task size and grid")
     ap.add_argument("--serve-requests", type=int, default=300)
     ap.add_argument("--serve-slo-matvec", type=float, default=1.0, help="latency target of a product, seconds")
     ap.add_argument("--serve-slo-solve", type=float, default=10.0, help="latency target of a solve, seconds")

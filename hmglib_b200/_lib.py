@@ -71,6 +71,7 @@ _PROTOS = {
     "hmg_build_bf16_factors": (C.c_int, [_vp]),
     "hmg_build_tensor_core_operands": (C.c_int, [_vp, C.c_int]),
     "hmg_set_graphs": (C.c_int, [_vp, C.c_int]),
+    "hmg_autotune": (C.c_int, [_vp, C.c_int, _vp, _vp, _vp]),
     "hmg_load": (C.c_int, [C.POINTER(_vp), C.c_char_p, _vp]),
     "hmg_full_matvec": (C.c_int, [_vp, _vp, _vp]),
     "hmg_full_matvec_rows": (C.c_int, [_vp, _vp, _vp, C.c_int, _vp]),

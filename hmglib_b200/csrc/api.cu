@@ -292,7 +292,8 @@ hmg_status hmg_matvec_host(hmg_matrix* h, const double* x_host, double* y_host)
     if (!h->host_x) {
         HMG_CUDA_TRY(cudaMallocHost((void**)&h->host_x, sizeof(double) * h->n[1]));
         HMG_CUDA_TRY(cudaMallocHost((void**)&h->host_y, sizeof(double) * h->n[0]));
-        if ((st = dalloc(&h->dev_x, (size_t)h->n[1], s)) || (st = dalloc(&h->dev_y, (size_t)h->n[0], s)))
+        // the device staging vectors may exist already (hmg_autotune)
+        if (!h->dev_x && ((st = dalloc(&h->dev_x, (size_t)h->n[1], s)) || (st = dalloc(&h->dev_y, (size_t)h->n[0], s))))
             return st;
     }
     memcpy(h->host_x, x_host, sizeof(double) * h->n[1]);
@@ -373,6 +374,15 @@ hmg_status hmg_set_matvec_variant(hmg_matrix* h, int variant)
     HMG_REQUIRE(variant == 0 || variant == 1, HMG_ERR_INVALID, "hmg_set_matvec_variant: variant must be 0 or 1");
     h->matvec_variant = variant;
     return HMG_OK;
+}
+
+hmg_status hmg_autotune(hmg_matrix* h, int reps, int* piece_bytes, int* ctas_per_sm, double* ms)
+{
+    HMG_REQUIRE(h, HMG_ERR_INVALID, "hmg_autotune: NULL handle");
+    HMG_REQUIRE(reps >= 1 && reps <= 100, HMG_ERR_INVALID, "hmg_autotune: reps %d outside 1..100", reps);
+    hmg_status st = check_ready(h, "hmg_autotune");
+    if (st) return st;
+    return autotune(h, reps, piece_bytes, ctas_per_sm, ms);
 }
 
 hmg_status hmg_set_graphs(hmg_matrix* h, int on)

@@ -114,6 +114,8 @@ struct hmg_matrix {
     int nfar_list = 0;
     int* dev_err = nullptr;        // pipeline wait time-out flag (0 = fine)
     int matvec_variant = 1;        // 0: streaming kernels where applicable, 1: plain-load kernels
+    int k1_piece_bytes = 65536;    // K1 warp-task unit: V^T rows of one tier up to these bytes (hmg_autotune)
+    int k1_ctas_per_sm = 8;        // K1 grid: CTAs per SM (hmg_autotune)
     bool use_graphs = false;       // replay products as a captured CUDA graph (hmg_set_graphs)
     void* graph_exec = nullptr;    // cudaGraphExec_t of the last product's launches
     void* graph_key = nullptr;     // what it was captured for (matvec.cu)
@@ -141,6 +143,7 @@ hmg_status matvec_device(hmg_matrix* h, const double* x, double* y, bool fp64_ar
 hmg_status matvec_multi(hmg_matrix* h, int nrhs, const double* X, int ldx, double* Y, int ldy);
 hmg_status matvec_multi_tc(hmg_matrix* h, int nrhs, const double* X, int ldx, double* Y, int ldy);
 hmg_status build_bf16_factors(hmg_matrix* h, bool near_on_tensor_cores);
+hmg_status autotune(hmg_matrix* h, int reps, int* best_piece, int* best_ctas, double* best_ms);
 void free_tc(hmg_matrix* h);
 void free_product_graph(hmg_matrix* h);
 void launch_gather_multi32(hmg_matrix* h, const double* X, int ldx, int nrhs, float* xm);

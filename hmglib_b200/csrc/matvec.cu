@@ -243,7 +243,8 @@ hmg_status ensure_desc(hmg_matrix* h, int elem)
             h->far_prec == HMG_PREC_MIXED ? 1 : 0, (PairDesc*)h->pair_desc);
         HMG_LAUNCH_CHECK();
     }
-    // K1 pieces: terms of V_b^T of one storage tier, in runs of at most ~64 KB.  Each
+    // K1 pieces: terms of V_b^T of one storage tier, in runs of at most k1_piece_bytes
+    // (64 KB unless hmg_autotune chose otherwise).  Each
     // piece gets the widest lane group 2^LG (LG 2..5) whose lanes still get k1_nch
     // chunks of a row each; pieces are ordered by tier, then by LG (one launch per
     // tier; a warp takes 32 / 2^LG pieces of one class at a time).
@@ -264,7 +265,7 @@ hmg_status ensure_desc(hmg_matrix* h, int elem)
             const long long per_lane = rb[tier] / 16 / k1_nch(tier);  // chunks per lane at 1 lane
             int lg = 2;
             while (lg < 5 && (1ll << (lg + 1)) <= per_lane) lg++;
-            const int per = (int)std::max(1ll, 65536ll / rb[tier]) * tg[tier];
+            const int per = (int)std::max(1ll, (long long)h->k1_piece_bytes / rb[tier]) * tg[tier];
             for (int l = lo[tier]; l < hi[tier]; l += per)
                 units[tier][lg - 2].push_back({b, l, std::min(hi[tier], l + per), tier});
         }
@@ -856,7 +857,7 @@ static hmg_status launch_product(hmg_matrix* h, const double* x, double* y, bool
             }
             const int ntasks = cls.task_start[4];
             if (ntasks == 0) continue;
-            const int grid = std::min(ceil_div(ntasks, 8), 148 * 8);
+            const int grid = std::min(ceil_div(ntasks, 8), 148 * h->k1_ctas_per_sm);
             if (tier == 0) {
                 if (fp64)
                     k_vtx<double, double, 0><<<grid, 256, 0, s>>>(dd, cls, h->xs64, t64);
@@ -990,6 +991,67 @@ hmg_status gaussian_rhs(hmg_matrix* h, double* b)
 {
     k_gaussian_rhs<<<ceil_div(h->n[0], 256), 256, 0, h->stream>>>(h->pts[0], h->n[0], h->dim, b);
     HMG_LAUNCH_CHECK();
+    return HMG_OK;
+}
+
+// ---------------------------------------------------------------------------
+// autotuning of the product's launch shapes (hmg_autotune)
+// ---------------------------------------------------------------------------
+// Times the single-vector product on this handle's own H-matrix for each pair of
+// V^T piece size (the unit of K1's warp tasks) and K1 grid (CTAs per SM), with CUDA
+// events around `reps` products after one untimed product (the first after a piece
+// size change also rebuilds the descriptors), and keeps the fastest.  x is the
+// handle's device staging vector (its values do not change the work).
+hmg_status autotune(hmg_matrix* h, int reps, int* best_piece, int* best_ctas, double* best_ms)
+{
+    cudaStream_t s = h->stream;
+    hmg_status st;
+    if (!h->dev_x) {
+        if ((st = dalloc(&h->dev_x, (size_t)h->n[1], s)) || (st = dalloc(&h->dev_y, (size_t)h->n[0], s))) return st;
+        HMG_CUDA_TRY(cudaMemsetAsync(h->dev_x, 0, sizeof(double) * h->n[1], s));
+    }
+    static const int pieces[] = {32768, 65536, 131072};
+    static const int ctas[] = {4, 8, 16};
+    cudaEvent_t e0, e1;
+    HMG_CUDA_TRY(cudaEventCreate(&e0));
+    HMG_CUDA_TRY(cudaEventCreate(&e1));
+    const bool prof = h->profiling;
+    h->profiling = false;
+    const int piece0 = h->k1_piece_bytes, ctas0 = h->k1_ctas_per_sm;
+    double best = 1e300;
+    int bp = piece0, bc = ctas0;
+    st = HMG_OK;
+    for (int pi = 0; pi < 3 && !st; pi++)
+        for (int ci = 0; ci < 3 && !st; ci++) {
+            if (h->k1_piece_bytes != pieces[pi]) {
+                h->k1_piece_bytes = pieces[pi];
+                h->desc_near_mode = -1;  // rebuild the K1 pieces
+            }
+            h->k1_ctas_per_sm = ctas[ci];
+            if ((st = matvec_device(h, h->dev_x, h->dev_y))) break;
+            cudaEventRecord(e0, s);
+            for (int r = 0; r < reps && !st; r++) st = matvec_device(h, h->dev_x, h->dev_y);
+            cudaEventRecord(e1, s);
+            if (cudaEventSynchronize(e1) != cudaSuccess) st = HMG_ERR_CUDA;
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, e0, e1);
+            if (!st && ms / reps < best) {
+                best = ms / reps;
+                bp = pieces[pi];
+                bc = ctas[ci];
+            }
+        }
+    h->profiling = prof;
+    if (h->k1_piece_bytes != bp) h->desc_near_mode = -1;
+    h->k1_piece_bytes = st ? piece0 : bp;
+    h->k1_ctas_per_sm = st ? ctas0 : bc;
+    if (st) h->desc_near_mode = -1;
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (st) return st;
+    if (best_piece) *best_piece = bp;
+    if (best_ctas) *best_ctas = bc;
+    if (best_ms) *best_ms = best;
     return HMG_OK;
 }
 

@@ -138,6 +138,12 @@ class HMatrix:
         """0: streaming (bulk-copy) product kernels, 1: plain-load kernels."""
         self._call("hmg_set_matvec_variant", int(variant))
 
+    def autotune(self, reps: int = 3) -> dict:
+        """Choose the product's V^T task size and grid by timing them (hmg_autotune)."""
+        piece, ctas, ms = C.c_int(0), C.c_int(0), C.c_double(0.0)
+        self._call("hmg_autotune", int(reps), C.byref(piece), C.byref(ctas), C.byref(ms))
+        return {"piece_bytes": piece.value, "ctas_per_sm": ctas.value, "ms": ms.value}
+
     def set_graphs(self, on: bool = True):
         """Replay products as a captured CUDA graph (hmg_set_graphs)."""
         self._call("hmg_set_graphs", int(bool(on)))

@@ -214,6 +214,14 @@ hmg_status hmg_get_profile(hmg_matrix* h, double* ms4);
  * variant 1 sums each slice in FP32 and the slices in FP64). */
 hmg_status hmg_set_matvec_variant(hmg_matrix* h, int variant);
 
+/* Autotuning (no reference counterpart): times the single-vector product of this
+ * H-matrix for each V^T x task size (32, 64, 128 KB of V^T rows per warp task) and
+ * grid (4, 8, 16 CTAs per SM), `reps` products each after an untimed one, and keeps
+ * the fastest for later products.  Returns the choice and its ms per product (any
+ * output pointer may be NULL).  Synchronous; results of products do not depend on it
+ * beyond FP32 summation order within a piece. */
+hmg_status hmg_autotune(hmg_matrix* h, int reps, int* piece_bytes, int* ctas_per_sm, double* ms);
+
 /* Products as CUDA graphs (no reference counterpart): with on != 0, hmg_matvec and
  * hmg_matvec_host capture the launches of a product into a CUDA graph on the first call
  * and replay it (cudaGraphLaunch) while the arguments and the handle's storage stay the
