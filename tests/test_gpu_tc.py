@@ -104,3 +104,30 @@ def test_copies_follow_the_storage(hmg, cuda):
     assert max(rel_err(Y32.cpu().numpy()[j], ref[j]) for j in range(4)) < 1e-6
     assert 1e-6 < max(rel_err(Ytc.cpu().numpy()[j], ref[j]) for j in range(4)) < 5e-3
     H.close()
+
+
+def test_leading_dimensions_and_33_vectors(hmg, cuda):
+    """Column-major X and Y with leading dimensions past n (X: n + 17, Y: n + 5) and
+    33 vectors (MMAs of N = 64 with 31 zero columns): rows past n are never written."""
+    torch = cuda
+    n = 12000
+    p = make_points("uniform", n, 3, 23)
+    H = engine(hmg, p, p, 1.5, 128, rule=1)
+    H.set_kernel(MATERN, 0.2, 0.0)
+    H.precompute_aca(64, 1e-6, hmg.PREC_FP32)
+    H.precompute_dense(hmg.PREC_FP32)
+    nrhs = 33
+    Xb = torch.from_numpy(np.random.default_rng(8).uniform(-1, 1, (nrhs, n + 17))).cuda()
+    X = Xb[:, :n]
+    Yref = torch.empty(nrhs, n, dtype=torch.float64, device="cuda")
+    H.matvec_multi(X.contiguous(), Yref)
+    H.build_bf16_factors()
+    Yb = torch.full((nrhs, n + 5), 7.0, dtype=torch.float64, device="cuda")
+    Y = Yb[:, :n]
+    H.matvec_multi(X, Y)
+    H.synchronize()
+    a, b = Y.cpu().numpy(), Yref.cpu().numpy()
+    for j in range(nrhs):
+        assert rel_err(a[j], b[j]) < 1e-2, (j, rel_err(a[j], b[j]))
+    assert float((Yb[:, n:] - 7.0).abs().max()) == 0.0
+    H.close()
