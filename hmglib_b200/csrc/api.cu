@@ -66,7 +66,8 @@ hmg_status hmg_create(hmg_matrix** out, int n1, int n2, int dim, int bits, void*
     h->bits = bits;
     h->stream = (cudaStream_t)stream;
     cudaError_t e = cudaGetDevice(&h->device);
-    if (e != cudaSuccess) {
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&h->nsm, cudaDevAttrMultiProcessorCount, h->device);
+    if (e != cudaSuccess || h->nsm <= 0) {
         set_error("hmg_create: no CUDA device: %s", cudaGetErrorString(e));
         delete h;
         return HMG_ERR_CUDA;

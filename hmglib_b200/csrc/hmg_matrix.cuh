@@ -10,6 +10,7 @@ struct hmg_matrix {
     int n[2] = {0, 0};
     int dim = 0, bits = 0;
     int device = 0;
+    int nsm = 0;          // SMs of the device (grid sizes)
     cudaStream_t stream = nullptr;
 
     // ---- points -------------------------------------------------------------

@@ -857,7 +857,7 @@ static hmg_status launch_product(hmg_matrix* h, const double* x, double* y, bool
             }
             const int ntasks = cls.task_start[4];
             if (ntasks == 0) continue;
-            const int grid = std::min(ceil_div(ntasks, 8), 148 * h->k1_ctas_per_sm);
+            const int grid = std::min(ceil_div(ntasks, 8), h->nsm * h->k1_ctas_per_sm);
             if (tier == 0) {
                 if (fp64)
                     k_vtx<double, double, 0><<<grid, 256, 0, s>>>(dd, cls, h->xs64, t64);

@@ -621,7 +621,7 @@ static hmg_status launch_multi_mixed(hmg_matrix* h, int nrhs, const double* X, i
     int first = 0;
     for (int tier = 0; tier < 3; tier++) {
         if (cnt[tier] > 0) {
-            const int grid = std::min(ceil_div(cnt[tier], 8), 148 * 3);
+            const int grid = std::min(ceil_div(cnt[tier], 8), h->nsm * 3);
             if (tier == 0) {
                 HMG_CUDA_TRY(cudaFuncSetAttribute(k_vtx_multi_smem<R, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)K1M_SMEM));
                 k_vtx_multi_smem<R, 0><<<grid, 256, K1M_SMEM, s>>>(dd + first, cnt[tier], xm, tm);
@@ -684,10 +684,10 @@ static hmg_status launch_multi(hmg_matrix* h, int nrhs, const double* X, int ldx
         if constexpr (sizeof(S) == 4 && R >= 8) {
             HMG_CUDA_TRY(cudaFuncSetAttribute(k_vtx_multi_smem<R, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                               (int)K1M_SMEM));
-            k_vtx_multi_smem<R, 0><<<std::min(ceil_div(n0, 8), 148 * 3), 256, K1M_SMEM, s>>>(dd, n0, xm, tm);
+            k_vtx_multi_smem<R, 0><<<std::min(ceil_div(n0, 8), h->nsm * 3), 256, K1M_SMEM, s>>>(dd, n0, xm, tm);
         }
         else
-            k_vtx_multi<S, R><<<std::min(ceil_div(n0, 8), 148 * 8), 256, 0, s>>>(dd, n0, xm, tm);
+            k_vtx_multi<S, R><<<std::min(ceil_div(n0, 8), h->nsm * 8), 256, 0, s>>>(dd, n0, xm, tm);
         HMG_LAUNCH_CHECK();
     }
     if (h->ntiles > 0) {

@@ -431,17 +431,6 @@ k_vtx_bulk(const int* __restrict__ blocks, int nblocks, const int* __restrict__ 
 // ---------------------------------------------------------------------------
 // host side
 // ---------------------------------------------------------------------------
-static int num_sms()
-{
-    static int n = 0;
-    if (!n) {
-        int dev = 0;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
-        if (n <= 0) n = 148;
-    }
-    return n;
-}
 
 size_t k2_smem_bytes()
 {
@@ -458,7 +447,7 @@ size_t k1_smem_bytes()
 hmg_status launch_tiles_bulk(hmg_matrix* h, bool fp64, double* y)
 {
     const size_t smem = k2_smem_bytes();
-    const int grid = std::min(num_sms(), std::max(1, h->ntiles));
+    const int grid = std::min(h->nsm, std::max(1, h->ntiles));
     HMG_CUDA_TRY(cudaMemsetAsync(h->dev_err + 1, 0, sizeof(int), h->stream));
     if (fp64) {
         HMG_CUDA_TRY(cudaFuncSetAttribute(k_tiles_bulk<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
@@ -478,7 +467,7 @@ hmg_status launch_tiles_bulk(hmg_matrix* h, bool fp64, double* y)
 hmg_status launch_vtx_bulk(hmg_matrix* h, bool fp64)
 {
     const size_t smem = k1_smem_bytes();
-    const int grid = std::min(num_sms(), std::max(1, h->nfar_list));
+    const int grid = std::min(h->nsm, std::max(1, h->nfar_list));
     HMG_CUDA_TRY(cudaMemsetAsync(h->dev_err + 2, 0, sizeof(int), h->stream));
     if (fp64) {
         HMG_CUDA_TRY(cudaFuncSetAttribute(k_vtx_bulk<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));

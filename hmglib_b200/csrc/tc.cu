@@ -524,13 +524,6 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
 // ---------------------------------------------------------------------------
 // host side
 // ---------------------------------------------------------------------------
-static int tc_num_sms()
-{
-    int dev = 0, n = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
-    return n > 0 ? n : 148;
-}
 
 void free_tc(hmg_matrix* h)
 {
@@ -737,7 +730,7 @@ hmg_status build_bf16_factors(hmg_matrix* h, bool near_tc)
             return HMG_ERR_UNSUPPORTED;
         }
     if ((st = ensure_desc(h, 4))) return st;
-    const int np = h->npairs, nt = h->ntiles, nb = h->nblocks, grid = tc_num_sms();
+    const int np = h->npairs, nt = h->ntiles, nb = h->nblocks, grid = h->nsm;
     std::vector<int> tps(nt + 1), pblock(np), ts(nt), tr0(nt);
     HMG_CUDA_TRY(cudaMemcpy(tps.data(), h->tile_pair_start, sizeof(int) * (nt + 1), cudaMemcpyDeviceToHost));
     HMG_CUDA_TRY(cudaMemcpy(pblock.data(), h->pair_block, sizeof(int) * np, cudaMemcpyDeviceToHost));
