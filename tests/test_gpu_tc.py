@@ -131,3 +131,27 @@ def test_leading_dimensions_and_33_vectors(hmg, cuda):
         assert rel_err(a[j], b[j]) < 1e-2, (j, rel_err(a[j], b[j]))
     assert float((Yb[:, n:] - 7.0).abs().max()) == 0.0
     H.close()
+
+
+@pytest.mark.parametrize("eta", [0.05, 1e6], ids=["all-dense", "mostly-low-rank"])
+def test_extreme_partitions(hmg, cuda, eta):
+    """Tensor-core operands of an H-matrix with (almost) no admissible blocks (pass 1
+    has no jobs) and of one where nearly everything is low rank."""
+    torch = cuda
+    n = 5000
+    p = make_points("uniform", n, 2, 29)
+    H = engine(hmg, p, p, eta, 64, rule=1)
+    H.set_kernel(GAUSS, 0.1, 0.0)
+    H.precompute_aca(64, 1e-6, hmg.PREC_FP32)
+    H.precompute_dense(hmg.PREC_FP32)
+    X = torch.from_numpy(np.random.default_rng(2).uniform(-1, 1, (4, n))).cuda()
+    Yref, Ytc = torch.empty_like(X), torch.full_like(X, float("nan"))
+    H.matvec_multi(X, Yref)
+    H.build_bf16_factors()
+    H.matvec_multi(X, Ytc)
+    H.synchronize()
+    a, b = Ytc.cpu().numpy(), Yref.cpu().numpy()
+    assert np.isfinite(a).all()
+    for j in range(4):
+        assert rel_err(a[j], b[j]) < 1e-2, (j, rel_err(a[j], b[j]))
+    H.close()
