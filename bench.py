@@ -366,6 +366,9 @@ def run_engine(a, rank, world):
             H.build_bf16_factors(near=hmg.PREC_FP32)
             line["multi_rhs_tensor_cores_near_fp32"] = multi_rhs_timing(torch, H, x, n, a.nrhs, a.steps, stream,
                                                                         world, err)
+            H.build_bf16_factors(near=hmg.PREC_BF16X3)
+            line["multi_rhs_tensor_cores_bf16x3"] = multi_rhs_timing(torch, H, x, n, a.nrhs, a.steps, stream,
+                                                                     world, err)
     if rank == 0 and world == 1 and not a.no_cpu:
         kind = O.KERNEL_MATERN32
         rate, nrows, dt, thr = cpu_direct_rate(p, x, kind, O.kernel_param(kind, W["rho"]), target_s=a.cpu_seconds)

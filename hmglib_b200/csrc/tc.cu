@@ -37,7 +37,8 @@
 // Every wait is bounded (pipeline.cuh): on a time-out the waiting role records an error
 // code in the handle's flag, leaves its loop, and the CTA waits for its own copies and
 // MMAs before freeing tensor memory.  BF16 rounding of factors, near field, X and t_b
-// (~4e-3 per entry) bounds the accuracy: products agree with FP32 ones to ~1e-3.
+// (~4e-3 per entry) bounds the accuracy: products agree with FP32 ones to ~1e-3.  With
+// split operands (hi + lo BF16 pairs, three MMAs per K step) they agree to ~1e-5.
 #include <cuda_bf16.h>
 
 #include <algorithm>
@@ -82,9 +83,18 @@ struct TcJob {
 // ---------------------------------------------------------------------------
 // conversion of the FP32 factors and near field (once, by hmg_build_bf16_factors)
 // ---------------------------------------------------------------------------
+// v as BF16, and (split operands, lo != nullptr) the BF16 rounding of what that misses:
+// hi + lo carries 16 significant bits of v
+__device__ __forceinline__ void store_split(__nv_bfloat16* hi, __nv_bfloat16* lo, size_t i, float v)
+{
+    const __nv_bfloat16 h = __float2bfloat16_rn(v);
+    hi[i] = h;
+    if (lo) lo[i] = __float2bfloat16_rn(v - __bfloat162float(h));
+}
+
 // far pair: U slice (s_pad x r, column-major) -> A cores, rc = s8 / 8, K = r16
 __global__ void k_tc_u(const PairDesc* desc, const int* plist, const long long* aoff, const int* ptile,
-                       const int* tile_s, int n, __nv_bfloat16* out)
+                       const int* tile_s, int n, __nv_bfloat16* out, __nv_bfloat16* out_lo)
 {
     const int u = blockIdx.x;
     if (u >= n) return;
@@ -94,18 +104,19 @@ __global__ void k_tc_u(const PairDesc* desc, const int* plist, const long long* 
     const int r = d.ncol, r16 = (r + 15) & ~15;
     const float* src = static_cast<const float*>(d.data);
     __nv_bfloat16* dst = out + aoff[u] / 2;
+    __nv_bfloat16* dlo = out_lo ? out_lo + aoff[u] / 2 : nullptr;
     const int rc = s8 / 8;
     for (int idx = threadIdx.x; idx < s8 * r16; idx += blockDim.x) {
         const int core = idx >> 6, e = idx & 63;
         const int kc = core / rc, mc = core - kc * rc;
         const int i = mc * 8 + (e >> 3), k = kc * 8 + (e & 7);
-        dst[idx] = __float2bfloat16_rn((i < s && k < r) ? src[(size_t)k * sp + i] : 0.0f);
+        store_split(dst, dlo, idx, (i < s && k < r) ? src[(size_t)k * sp + i] : 0.0f);
     }
 }
 
 // near pair: slice (s_pad x m2, column-major) -> A cores with c0 mod 8 leading zero columns
 __global__ void k_tc_near(const PairDesc* desc, const int* plist, const long long* aoff, const int* ptile,
-                          const int* tile_s, int n, __nv_bfloat16* out)
+                          const int* tile_s, int n, __nv_bfloat16* out, __nv_bfloat16* out_lo)
 {
     const int u = blockIdx.x;
     if (u >= n) return;
@@ -114,12 +125,13 @@ __global__ void k_tc_near(const PairDesc* desc, const int* plist, const long lon
     const int m2 = d.ncol, a = d.c0 & 7, kw = (a + m2 + 15) & ~15;
     const float* src = static_cast<const float*>(d.data);
     __nv_bfloat16* dst = out + aoff[u] / 2;
+    __nv_bfloat16* dlo = out_lo ? out_lo + aoff[u] / 2 : nullptr;
     const int rc = s8 / 8;
     for (long long idx = threadIdx.x; idx < (long long)s8 * kw; idx += blockDim.x) {
         const int core = (int)(idx >> 6), e = (int)(idx & 63);
         const int kc = core / rc, mc = core - kc * rc;
         const int i = mc * 8 + (e >> 3), c = kc * 8 + (e & 7) - a;
-        dst[idx] = __float2bfloat16_rn((i < s && c >= 0 && c < m2) ? src[(size_t)c * sp + i] : 0.0f);
+        store_split(dst, dlo, idx, (i < s && c >= 0 && c < m2) ? src[(size_t)c * sp + i] : 0.0f);
     }
 }
 
@@ -127,7 +139,8 @@ __global__ void k_tc_near(const PairDesc* desc, const int* plist, const long lon
 // cores.  A stack holds the V^T of blocks with the same columns, one under the other
 // (vaux: stack row cores << 8 | the block's first row core in the stack).
 __global__ void k_tc_v(const int* blist, const long long* voff, const int* vaux, int n, void* const* ptrV,
-                       const int* rank, const int* blk_c0, const int* blk_m2, __nv_bfloat16* out)
+                       const int* rank, const int* blk_c0, const int* blk_m2, __nv_bfloat16* out,
+                       __nv_bfloat16* out_lo)
 {
     const int u = blockIdx.x;
     if (u >= n) return;
@@ -136,13 +149,14 @@ __global__ void k_tc_v(const int* blist, const long long* voff, const int* vaux,
     const int a = blk_c0[b] & 7, kw = (a + m2 + 15) & ~15;
     const float* V = static_cast<const float*>(ptrV[b]);
     __nv_bfloat16* dst = out + voff[u] / 2;
+    __nv_bfloat16* dlo = out_lo ? out_lo + voff[u] / 2 : nullptr;
     const int rb = r16 / 8;
     for (long long idx = threadIdx.x; idx < (long long)r16 * kw; idx += blockDim.x) {
         const int core = (int)(idx >> 6), e = (int)(idx & 63);
         const int kc = core / rb, mc = core - kc * rb;
         const int m = mc * 8 + (e >> 3), c = kc * 8 + (e & 7) - a;
-        dst[((size_t)kc * rc + off8 + mc) * 64 + e] =
-            __float2bfloat16_rn((m < r && c >= 0 && c < m2) ? V[(size_t)m * m2p + c] : 0.0f);
+        store_split(dst, dlo, ((size_t)kc * rc + off8 + mc) * 64 + e,
+                    (m < r && c >= 0 && c < m2) ? V[(size_t)m * m2p + c] : 0.0f);
     }
 }
 
@@ -152,19 +166,22 @@ __global__ void k_tc_v(const int* blist, const long long* voff, const int* vaux,
 // thread (g, j): columns 8g..8g+7 of vector j, one 16-byte row of K core g
 template <int NV>
 __global__ void k_tc_x(const double* __restrict__ X, int ldx, int nrhs, const int* __restrict__ perm1, int n,
-                       long long ngroups, uint4* xb)
+                       long long ngroups, uint4* xb, uint4* xb_lo)
 {
     const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (idx >= ngroups * NV) return;
     const long long g = idx / NV;
     const int j = (int)(idx % NV);
-    __nv_bfloat16 v[8];
+    __nv_bfloat16 v[8], w[8];
 #pragma unroll
     for (int e = 0; e < 8; e++) {
         const long long c = g * 8 + e;
-        v[e] = __float2bfloat16_rn(c < n && j < nrhs ? (float)X[(size_t)perm1[c] + (size_t)j * ldx] : 0.0f);
+        const float f = c < n && j < nrhs ? (float)X[(size_t)perm1[c] + (size_t)j * ldx] : 0.0f;
+        v[e] = __float2bfloat16_rn(f);
+        w[e] = __float2bfloat16_rn(f - __bfloat162float(v[e]));
     }
     xb[(g * (NV / 8) + (j >> 3)) * 8 + (j & 7)] = *reinterpret_cast<const uint4*>(v);
+    if (xb_lo) xb_lo[(g * (NV / 8) + (j >> 3)) * 8 + (j & 7)] = *reinterpret_cast<const uint4*>(w);
 }
 
 // ---------------------------------------------------------------------------
@@ -269,12 +286,14 @@ __device__ __forceinline__ uint32_t pack_bf16(float lo, float hi)
 // Steps of CTA c: [cta[c].y, cta[c+1].y); its jobs: [cta[c].x, cta[c+1].x).  NV vectors per
 // pass (MMA N); B K cores are NV * 16 bytes.  Pass 1 (MODE 0) writes t_b cores, K core kc of
 // job j (a stack) to B K core tb_kc + map[16 j + kc]; pass 2 (MODE 1) writes (add_y: adds
-// to) rows of Y, tile row i to Y row map[r0 + i].
-template <int MODE, int NV>
+// to) rows of Y, tile row i to Y row map[r0 + i].  SPLIT: every operand also has its low
+// part (A_lo, B_lo: the BF16 rounding of what the BF16 value misses, same layout); a step
+// then brings A hi, A lo, B hi, B lo and each K step runs hi*hi + hi*lo + lo*hi.
+template <int MODE, int NV, bool SPLIT>
 __global__ void __launch_bounds__(TC_THREADS, 1)
     k_tc_pass(const TcStep* __restrict__ steps, const TcJob* __restrict__ jobs, const int2* __restrict__ cta,
-              const char* __restrict__ A, char* Bbuf, long long tb_kc, const int* __restrict__ map, int nrhs,
-              double* Y, int ldy, int add_y, int* err)
+              const char* __restrict__ A, const char* __restrict__ A_lo, char* Bbuf, char* B_lo, long long tb_kc,
+              const int* __restrict__ map, int nrhs, double* Y, int ldy, int add_y, int* err)
 {
     constexpr int KB = NV * 16;
     extern __shared__ __align__(1024) unsigned char tc_raw[];
@@ -324,7 +343,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
             const int ks_all = (mine.meta >> 16) & 0xff;
             const int ab = ks_all * 2 * (mine.meta & 0xff) * 128, bb = ks_all * 2 * KB;
             __syncwarp();
-            sm.step_bytes[lane] = ab + bb;
+            sm.step_bytes[lane] = SPLIT ? 2 * (ab + bb) : ab + bb;
             __syncwarp();
             for (int k = 0; k < cnt && ok;) {
                 int m = 0;
@@ -368,18 +387,21 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                 if (lane >= k && lane < k + m) {
                     const int slot = (i0 + lane) % TC_SLOTS, pos = sm.slot_pos[slot];
                     const uint32_t a = smem_u32(sm.ring + pos);
+                    const int a_span = SPLIT ? 2 * ab : ab;  // A hi [, A lo], then B hi [, B lo]
                     sm.slot_a[slot] = a;
-                    sm.slot_b[slot] = a + ab;
+                    sm.slot_b[slot] = a + a_span;
                     sm.slot_meta[slot] = mine.meta;
-                    mbar_arrive_expect_tx(&sm.full[slot], ab + bb);
+                    mbar_arrive_expect_tx(&sm.full[slot], SPLIT ? 2 * (ab + bb) : ab + bb);
                     bulk_g2s_first(sm.ring + pos, A + mine.a_off, ab, &sm.full[slot], pol);
+                    if (SPLIT) bulk_g2s_first(sm.ring + pos + ab, A_lo + mine.a_off, ab, &sm.full[slot], pol);
                     const int nsub = ((mine.meta >> 10) & 3) + 1;
-                    int boff = ab;
+                    int boff = a_span;
 #pragma unroll
                     for (int j = 0; j < TC_MAXSUB; j++)
                         if (j < nsub) {
                             const int kb = (((mine.kss >> (4 * j)) & 15) + 1) * 2 * KB;
                             bulk_g2s(sm.ring + pos + boff, Bbuf + mine.b_off[j] * KB, kb, &sm.full[slot]);
+                            if (SPLIT) bulk_g2s(sm.ring + pos + boff + bb, B_lo + mine.b_off[j] * KB, kb, &sm.full[slot]);
                             boff += kb;
                         }
                 }
@@ -420,10 +442,16 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                 const uint32_t d = tmem + (uint32_t)(buf * NV);
                 const uint64_t da = (2 * lbo) >> 4, db = (2 * KB) >> 4;
                 uint64_t ad = smem_desc(a0, lbo, 128), bd = smem_desc(b0, KB, 128);
+                // low parts: A lo right after A hi, B lo right after B hi (16-byte units)
+                const uint64_t alo = (uint64_t)(ks_all * 2 * lbo) >> 4, blo = (uint64_t)(ks_all * 2 * KB) >> 4;
                 uint32_t acc = first ? 0u : 1u;
 #pragma unroll 4
                 for (int q = 0; q < ks_all; q++) {
                     tc_mma(d, ad, bd, tc_idesc<NV>(), acc);
+                    if (SPLIT) {
+                        tc_mma(d, ad, bd + blo, tc_idesc<NV>(), 1u);
+                        tc_mma(d, ad + alo, bd, tc_idesc<NV>(), 1u);
+                    }
                     acc = 1u;
                     ad += da;
                     bd += db;
@@ -490,24 +518,32 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                     uint32_t* stg = reinterpret_cast<uint32_t*>(sm.stg[warp]);
                     const bool odd = lane & 1;
 #pragma unroll
-                    for (int t = 0; t < NV / 2; t++) {
-                        const float v0 = __uint_as_float(v[2 * t]), v1 = __uint_as_float(v[2 * t + 1]);
-                        const float x = __shfl_xor_sync(~0u, odd ? v0 : v1, 1);
-                        const int q = odd ? 2 * t + 1 : 2 * t;
-                        const uint32_t w = odd ? pack_bf16(x, v1) : pack_bf16(v0, x);
-                        const int u = (lane >> 3) * NV + q;
-                        stg[(u ^ ((lane >> 3) * 2)) * 4 + ((lane & 7) >> 1)] = w;
-                    }
-                    __syncwarp();
-                    uint4* dst = reinterpret_cast<uint4*>(Bbuf);
-                    const uint4* src = reinterpret_cast<const uint4*>(stg);
+                    for (int part = 0; part < (SPLIT ? 2 : 1); part++) {
+                        // part 0: BF16 of t; part 1 (split): BF16 of what part 0 misses
 #pragma unroll
-                    for (int it = 0; it < NV / 8; it++) {
-                        const int u = it * 32 + lane, kcl = u / NV;
-                        if (warp * 4 + kcl < (rows >> 3))
-                            dst[(size_t)(tb_kc + tdst[kcl]) * (KB / 16) + (u % NV)] = src[u ^ (kcl * 2)];
+                        for (int t = 0; t < NV / 2; t++) {
+                            float v0 = __uint_as_float(v[2 * t]), v1 = __uint_as_float(v[2 * t + 1]);
+                            if (part) {
+                                v0 -= __bfloat162float(__float2bfloat16_rn(v0));
+                                v1 -= __bfloat162float(__float2bfloat16_rn(v1));
+                            }
+                            const float x = __shfl_xor_sync(~0u, odd ? v0 : v1, 1);
+                            const int q = odd ? 2 * t + 1 : 2 * t;
+                            const uint32_t w = odd ? pack_bf16(x, v1) : pack_bf16(v0, x);
+                            const int u = (lane >> 3) * NV + q;
+                            stg[(u ^ ((lane >> 3) * 2)) * 4 + ((lane & 7) >> 1)] = w;
+                        }
+                        __syncwarp();
+                        uint4* dst = reinterpret_cast<uint4*>(part ? B_lo : Bbuf);
+                        const uint4* src = reinterpret_cast<const uint4*>(stg);
+#pragma unroll
+                        for (int it = 0; it < NV / 8; it++) {
+                            const int u = it * 32 + lane, kcl = u / NV;
+                            if (warp * 4 + kcl < (rows >> 3))
+                                dst[(size_t)(tb_kc + tdst[kcl]) * (KB / 16) + (u % NV)] = src[u ^ (kcl * 2)];
+                        }
+                        __syncwarp();
                     }
-                    __syncwarp();
                 }
             }
             ok = __all_sync(~0u, ok);
@@ -530,6 +566,14 @@ void free_tc(hmg_matrix* h)
     cudaStream_t s = h->stream;
     if (h->tc_u) cudaFree(h->tc_u);
     if (h->tc_v) cudaFree(h->tc_v);
+    if (h->tc_u_lo) cudaFree(h->tc_u_lo);
+    if (h->tc_v_lo) cudaFree(h->tc_v_lo);
+    h->tc_u_lo = h->tc_v_lo = nullptr;
+    if (h->tc_bbuf_lo) {
+        cudaStreamSynchronize(s);
+        cudaFree(h->tc_bbuf_lo);
+        h->tc_bbuf_lo = nullptr;
+    }
     if (h->tc_bbuf) {
         cudaStreamSynchronize(s);  // a product in flight may still read it
         cudaFree(h->tc_bbuf);
@@ -548,6 +592,7 @@ void free_tc(hmg_matrix* h)
     h->tc_grid = 0;
     h->tc_all_tiles = false;
     h->tc_near = false;
+    h->tc_split = false;
 }
 
 namespace {
@@ -581,8 +626,9 @@ struct JobList {
         }
     }
     // Steps of every job: consecutive chunks share a step (merge) while their A chunks
-    // are adjacent and the step stays within TC_MAXSUB sub-steps, TC_ABYTES and TC_BBYTES.
-    void make_steps(bool merge)
+    // are adjacent and the step stays within TC_MAXSUB sub-steps, a_limit bytes of A and
+    // ks_limit MMAs (B bytes).
+    void make_steps(bool merge, long long a_limit, int ks_limit)
     {
         chunk0.push_back((int)chunks.size());
         for (size_t j = 0; j + 1 < chunk0.size(); j++) {
@@ -602,7 +648,7 @@ struct JobList {
                 const Chunk& k = chunks[c];
                 const long long kab = (long long)k.ks * 2 * k.rc * 128;
                 if (!(merge && nsub > 0 && nsub < TC_MAXSUB && k.rc == (cur.meta & 0xff) && k.a_off == cur.a_off + ab &&
-                      ab + kab <= TC_ABYTES && ks_all + k.ks <= TC_MAXSTEP))
+                      ab + kab <= a_limit && ks_all + k.ks <= ks_limit))
                     flush();
                 if (!nsub) {
                     cur.a_off = k.a_off;
@@ -624,7 +670,7 @@ struct JobList {
 
 // Every copy a step issues stays inside its arena and its stage, and every job's
 // output inside its buffer: checked here, on the host, before any launch.
-bool steps_in_bounds(const JobList& L, long long abytes, long long bkcores, long long out_limit, int q)
+bool steps_in_bounds(const JobList& L, long long abytes, long long bkcores, long long out_limit, int q, bool split)
 {
     for (const TcStep& st : L.steps) {
         const int rc = st.meta & 0xff, nsub = ((st.meta >> 10) & 3) + 1, ks_all = (st.meta >> 16) & 0xff;
@@ -635,7 +681,8 @@ bool steps_in_bounds(const JobList& L, long long abytes, long long bkcores, long
             if (st.b_off[j] < 0 || st.b_off[j] + 2ll * ks > bkcores) return false;
             sum += ks;
         }
-        if (sum != ks_all || rc < 1 || rc > 16 || ab > TC_ABYTES || bb > TC_BBYTES || st.a_off < 0 || st.a_off % 16 ||
+        if (sum != ks_all || rc < 1 || rc > 16 || (split ? 2 : 1) * ab > TC_ABYTES || (split ? 2 : 1) * bb > TC_BBYTES ||
+            st.a_off < 0 || st.a_off % 16 ||
             st.a_off + ab > abytes)
             return false;
     }
@@ -707,7 +754,7 @@ hmg_status alloc_arena(void** p, long long bytes, const char* what)
 
 }  // namespace
 
-hmg_status build_bf16_factors(hmg_matrix* h, bool near_tc)
+hmg_status build_bf16_factors(hmg_matrix* h, bool near_tc, bool split)
 {
     cudaStream_t s = h->stream;
     hmg_status st;
@@ -739,6 +786,9 @@ hmg_status build_bf16_factors(hmg_matrix* h, bool near_tc)
 
     // B buffer of a product, in K cores: X (8 columns each), then t_b (16 terms = 2 K cores per group)
     const long long xkc = (h->n[1] + 7) / 8 + 4;
+    // split operands bring hi and lo of every chunk: half the A and MMAs per step
+    const long long a_half = split ? TC_ABYTES / 2 : TC_ABYTES;
+    const int ks_limit = split ? TC_MAXSTEP / 2 : TC_MAXSTEP;
     std::vector<long long> toff(nb, -1);
     long long tgroups = 0;
     JobList k1, k2;
@@ -788,7 +838,7 @@ hmg_status build_bf16_factors(hmg_matrix* h, bool near_tc)
                     off8 += r16 / 8;
                 }
                 k1.begin(TcJob{job, rows});
-                k1.add(vbytes, c0 >> 3, rc, kw / 8, std::min(2 * TC_MAXKS, (TC_ABYTES / 128 / rc) & ~1),
+                k1.add(vbytes, c0 >> 3, rc, kw / 8, std::min(2 * ks_limit, (int)(a_half / 128 / rc) & ~1),
                        0.25);
                 vbytes += (long long)rows * kw * 2;
             }
@@ -816,24 +866,24 @@ hmg_status build_bf16_factors(hmg_matrix* h, bool near_tc)
                 nlist.push_back(p);
                 ntile.push_back(t);
                 noff.push_back(ubytes);
-                k2.add(ubytes, h->h_c0[b] >> 3, rc, kw / 8, TC_ABYTES / 128 / 16, 0.25);
+                k2.add(ubytes, h->h_c0[b] >> 3, rc, kw / 8, (int)(a_half / 128 / 16), 0.25);
                 ubytes += (long long)rc * 8 * kw * 2;
             } else {
                 const int r16 = (h->h_rank[b] + 15) & ~15;
                 ulist.push_back(p);
                 utile.push_back(t);
                 uoff.push_back(ubytes);
-                k2.add(ubytes, xkc + toff[b] * 2, rc, r16 / 8, TC_ABYTES / 128 / 16, 1.0);
+                k2.add(ubytes, xkc + toff[b] * 2, rc, r16 / 8, (int)(a_half / 128 / 16), 1.0);
                 ubytes += (long long)rc * 8 * r16 * 2;
             }
         }
         all_tiles = all_tiles && started;
     }
 
-    k1.make_steps(false);
-    k2.make_steps(true);
-    if (!steps_in_bounds(k1, vbytes, xkc + tgroups * 2, (long long)kmap.size() / 16, 0) ||
-        !steps_in_bounds(k2, ubytes, xkc + tgroups * 2, h->n[0], 1)) {
+    k1.make_steps(false, a_half, ks_limit);
+    k2.make_steps(true, a_half, ks_limit);
+    if (!steps_in_bounds(k1, vbytes, xkc + tgroups * 2, (long long)kmap.size() / 16, 0, split) ||
+        !steps_in_bounds(k2, ubytes, xkc + tgroups * 2, h->n[0], 1, split)) {
         set_error("hmg_build_bf16_factors: internal error: an operand step leaves its buffer");
         return HMG_ERR_UNSUPPORTED;
     }
@@ -849,7 +899,9 @@ hmg_status build_bf16_factors(hmg_matrix* h, bool near_tc)
     }
     if (!kmap.empty())
         HMG_CUDA_TRY(cudaMemcpyAsync(h->tc_kmap, kmap.data(), sizeof(int) * kmap.size(), cudaMemcpyHostToDevice, s));
-    if ((st = alloc_arena(&h->tc_v, vbytes, "the V^T operands"))) {
+    if ((st = alloc_arena(&h->tc_v, vbytes, "the V^T operands")) ||
+        (split && ((st = alloc_arena(&h->tc_u_lo, ubytes, "the tile operands' low parts")) ||
+                   (st = alloc_arena(&h->tc_v_lo, vbytes, "the V^T operands' low parts"))))) {
         free_tc(h);
         return st;
     }
@@ -869,13 +921,16 @@ hmg_status build_bf16_factors(hmg_matrix* h, bool near_tc)
         if (!tiles.empty())
             HMG_CUDA_TRY(cudaMemcpyAsync(dtile, tiles.data(), sizeof(int) * n, cudaMemcpyHostToDevice, s));
         const PairDesc* desc = static_cast<const PairDesc*>(h->pair_desc);
+        __nv_bfloat16* ulo = static_cast<__nv_bfloat16*>(h->tc_u_lo);  // null unless split
+        __nv_bfloat16* vlo = static_cast<__nv_bfloat16*>(h->tc_v_lo);
         if (which == 0)
-            k_tc_u<<<n, 256, 0, s>>>(desc, dlist, doff, dtile, h->tile_s, n, static_cast<__nv_bfloat16*>(h->tc_u));
+            k_tc_u<<<n, 256, 0, s>>>(desc, dlist, doff, dtile, h->tile_s, n, static_cast<__nv_bfloat16*>(h->tc_u), ulo);
         else if (which == 1)
-            k_tc_near<<<n, 256, 0, s>>>(desc, dlist, doff, dtile, h->tile_s, n, static_cast<__nv_bfloat16*>(h->tc_u));
+            k_tc_near<<<n, 256, 0, s>>>(desc, dlist, doff, dtile, h->tile_s, n, static_cast<__nv_bfloat16*>(h->tc_u),
+                                        ulo);
         else
             k_tc_v<<<n, 256, 0, s>>>(dlist, doff, dtile, n, h->ptrV, h->rank, h->blk_c0, h->blk_m2,
-                                     static_cast<__nv_bfloat16*>(h->tc_v));
+                                     static_cast<__nv_bfloat16*>(h->tc_v), vlo);
         HMG_LAUNCH_CHECK();
         HMG_CUDA_TRY(cudaStreamSynchronize(s));
         dfree(dlist, s);
@@ -900,28 +955,31 @@ hmg_status build_bf16_factors(hmg_matrix* h, bool near_tc)
     h->tc_grid = grid;
     h->tc_all_tiles = all_tiles;
     h->tc_near = near_tc;
+    h->tc_split = split;
     h->tc_ready = true;
     return HMG_OK;
 }
 
-template <int NV>
+template <int NV, bool SPLIT>
 static hmg_status tc_product(hmg_matrix* h, int nrhs, const double* X, int ldx, double* Y, int ldy)
 {
     cudaStream_t s = h->stream;
     hmg_status st;
     char* bbuf = static_cast<char*>(h->tc_bbuf);
+    char* blo = static_cast<char*>(h->tc_bbuf_lo);  // null unless split
     const long long xkc = h->tc_xkc;
     k_tc_x<NV><<<(unsigned)((xkc * NV + 255) / 256), 256, 0, s>>>(X, ldx, nrhs, h->perm[1], h->n[1], xkc,
-                                                                    reinterpret_cast<uint4*>(bbuf));
+                                                                    reinterpret_cast<uint4*>(bbuf),
+                                                                    reinterpret_cast<uint4*>(blo));
     HMG_LAUNCH_CHECK();
     const size_t smem = sizeof(TcSmem);
-    HMG_CUDA_TRY(cudaFuncSetAttribute(k_tc_pass<0, NV>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    HMG_CUDA_TRY(cudaFuncSetAttribute(k_tc_pass<1, NV>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    HMG_CUDA_TRY(cudaFuncSetAttribute(k_tc_pass<0, NV, SPLIT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    HMG_CUDA_TRY(cudaFuncSetAttribute(k_tc_pass<1, NV, SPLIT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     if (h->tc_njobs[0] > 0) {
-        k_tc_pass<0, NV><<<h->tc_grid, TC_THREADS, smem, s>>>(
+        k_tc_pass<0, NV, SPLIT><<<h->tc_grid, TC_THREADS, smem, s>>>(
             reinterpret_cast<const TcStep*>(h->tc_steps[0]), reinterpret_cast<const TcJob*>(h->tc_jobs[0]),
-            reinterpret_cast<const int2*>(h->tc_cta[0]), static_cast<const char*>(h->tc_v), bbuf, xkc, h->tc_kmap, 0,
-            nullptr, 0, 0, h->dev_err);
+            reinterpret_cast<const int2*>(h->tc_cta[0]), static_cast<const char*>(h->tc_v),
+            static_cast<const char*>(h->tc_v_lo), bbuf, blo, xkc, h->tc_kmap, 0, nullptr, 0, 0, h->dev_err);
         HMG_LAUNCH_CHECK();
     }
     if (!h->tc_near && h->ndense > 0) {
@@ -940,10 +998,10 @@ static hmg_status tc_product(hmg_matrix* h, int nrhs, const double* X, int ldx, 
     }
     const int add_y = !h->tc_near && h->ndense > 0;
     if (h->tc_njobs[1] > 0) {
-        k_tc_pass<1, NV><<<h->tc_grid, TC_THREADS, smem, s>>>(
+        k_tc_pass<1, NV, SPLIT><<<h->tc_grid, TC_THREADS, smem, s>>>(
             reinterpret_cast<const TcStep*>(h->tc_steps[1]), reinterpret_cast<const TcJob*>(h->tc_jobs[1]),
-            reinterpret_cast<const int2*>(h->tc_cta[1]), static_cast<const char*>(h->tc_u), bbuf, 0, h->perm[0], nrhs,
-            Y, ldy, add_y, h->dev_err);
+            reinterpret_cast<const int2*>(h->tc_cta[1]), static_cast<const char*>(h->tc_u),
+            static_cast<const char*>(h->tc_u_lo), bbuf, blo, 0, h->perm[0], nrhs, Y, ldy, add_y, h->dev_err);
         HMG_LAUNCH_CHECK();
     }
     return HMG_OK;
@@ -962,7 +1020,19 @@ hmg_status matvec_multi_tc(hmg_matrix* h, int nrhs, const double* X, int ldx, do
             return ce == cudaErrorMemoryAllocation ? HMG_ERR_NOMEM : HMG_ERR_CUDA;
         }
     }
-    return nrhs > 32 ? tc_product<64>(h, nrhs, X, ldx, Y, ldy) : tc_product<32>(h, nrhs, X, ldx, Y, ldy);
+    if (h->tc_split && !h->tc_bbuf_lo) {
+        const size_t bytes = (size_t)(h->tc_xkc + h->tc_tkc) * 16 * TC_NMAX;
+        cudaError_t ce = cudaMalloc(&h->tc_bbuf_lo, bytes);
+        if (ce != cudaSuccess) {
+            cudaGetLastError();
+            h->tc_bbuf_lo = nullptr;
+            set_error("hmg_matvec_multi: allocating %zu bytes of operand space failed: %s", bytes, cudaGetErrorString(ce));
+            return ce == cudaErrorMemoryAllocation ? HMG_ERR_NOMEM : HMG_ERR_CUDA;
+        }
+    }
+    if (h->tc_split)
+        return nrhs > 32 ? tc_product<64, true>(h, nrhs, X, ldx, Y, ldy) : tc_product<32, true>(h, nrhs, X, ldx, Y, ldy);
+    return nrhs > 32 ? tc_product<64, false>(h, nrhs, X, ldx, Y, ldy) : tc_product<32, false>(h, nrhs, X, ldx, Y, ldy);
 }
 
 }  // namespace hmg

@@ -151,7 +151,8 @@ class HMatrix:
     def build_bf16_factors(self, near: int = L.PREC_BF16):
         """BF16 tcgen05 operands of the FP32 factors for tensor-core multi-vector products
         (hmg_build_tensor_core_operands); the near field on the tensor cores too
-        (near=PREC_BF16) or in FP32 on the CUDA cores (near=PREC_FP32)."""
+        (near=PREC_BF16), in FP32 on the CUDA cores (near=PREC_FP32), or every operand
+        as a BF16 hi + lo pair (near=PREC_BF16X3, ~1e-5)."""
         self._call("hmg_build_tensor_core_operands", int(near))
 
     def save(self, path: str):

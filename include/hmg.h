@@ -51,8 +51,10 @@ typedef enum {
  * Frobenius norm in FP16 and below 1.5e-6 in FP8 e4m3, each scaled; the added error
  * is ~1e-7 of the block norm.  hmg_precompute_dense with this value stores FP32. */
 #define HMG_PREC_MIXED 2
-/* Tensor-core operands only (hmg_build_tensor_core_operands): BF16 */
+/* Tensor-core operands only (hmg_build_tensor_core_operands): BF16; BF16 pairs hi + lo
+ * (16 significant bits, three MMAs per K step: hi*hi + hi*lo + lo*hi) */
 #define HMG_PREC_BF16 3
+#define HMG_PREC_BF16X3 4
 
 /* near-field mode for hmg_matvec */
 #define HMG_NEAR_STORED 0   /* read the blocks stored by hmg_precompute_dense          */
@@ -140,7 +142,10 @@ hmg_status hmg_full_matvec_rows(hmg_matrix* h, const double* x, const int* rows,
  * with 2..64 vectors computes t_b = V_b^T X_b and U t_b on the tensor cores with BF16
  * operands (X and t_b rounded to BF16) and FP32 accumulation; the near field runs
  * there as well (HMG_PREC_BF16) or on the CUDA cores in FP32 (HMG_PREC_FP32).  Results
- * agree with the FP32 products to ~1e-3 (BF16 rounding).  Single-vector products keep
+ * agree with the FP32 products to ~1e-3 (BF16 rounding).  HMG_PREC_BF16X3 keeps every
+ * operand, the near field included, as a BF16 pair (hi and the rounding of what hi
+ * misses) and multiplies hi*hi + hi*lo + lo*hi: ~1e-5, with twice the operand bytes
+ * and three times the MMAs.  Single-vector products keep
  * using the FP32 storage.  Recomputing the factors or the near field drops the copies.
  * hmg_build_bf16_factors(h) is hmg_build_tensor_core_operands(h, HMG_PREC_BF16). */
 hmg_status hmg_build_tensor_core_operands(hmg_matrix* h, int near_precision);

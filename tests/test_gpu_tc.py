@@ -155,3 +155,35 @@ def test_extreme_partitions(hmg, cuda, eta):
     for j in range(4):
         assert rel_err(a[j], b[j]) < 1e-2, (j, rel_err(a[j], b[j]))
     H.close()
+
+
+@pytest.mark.parametrize("nrhs", [8, 40])
+def test_split_operands(hmg, cuda, nrhs):
+    """HMG_PREC_BF16X3: operands as BF16 hi + lo pairs, three MMAs per K step; the
+    products agree with the FP32 ones to ~1e-5 (bound 1e-4), far closer than the
+    single-BF16 operands, and are deterministic."""
+    torch = cuda
+    n = 20000
+    p = make_points("uniform", n, 3, 37)
+    H = engine(hmg, p, p, 1.5, 128, rule=1)
+    H.set_kernel(MATERN, 0.2, 0.0)
+    H.precompute_aca(64, 1e-8, hmg.PREC_FP32)
+    H.precompute_dense(hmg.PREC_FP32)
+    X = torch.from_numpy(np.random.default_rng(9).uniform(-1, 1, (nrhs, n))).cuda()
+    Y32, Y1, Y3 = torch.empty_like(X), torch.empty_like(X), torch.full_like(X, float("nan"))
+    H.matvec_multi(X, Y32)
+    H.build_bf16_factors(near=hmg.PREC_BF16)
+    H.matvec_multi(X, Y1)
+    H.build_bf16_factors(near=hmg.PREC_BF16X3)
+    H.matvec_multi(X, Y3)
+    H.synchronize()
+    ref, a1, a3 = Y32.cpu().numpy(), Y1.cpu().numpy(), Y3.cpu().numpy()
+    assert np.isfinite(a3).all()
+    e1 = max(rel_err(a1[j], ref[j]) for j in range(nrhs))
+    e3 = max(rel_err(a3[j], ref[j]) for j in range(nrhs))
+    assert e3 < 1e-4 and e3 < e1 / 20, (e1, e3)
+    Y4 = torch.empty_like(X)
+    H.matvec_multi(X, Y4)
+    H.synchronize()
+    np.testing.assert_array_equal(Y4.cpu().numpy(), a3)
+    H.close()
