@@ -8,7 +8,7 @@
 // rebuilt on load (they are a deterministic function of the block list), so a loaded
 // H-matrix multiplies bit-identically to the one saved.
 //
-// Format (little endian, native struct layouts of this build; version 1):
+// Format (little endian, native struct layouts of this library; version 1):
 //   "HMGB200\0", u32 version, u32 header bytes, the Header struct, then sections in
 //   order: points, blocks, [group parameters], [far field], [near field].  Each
 //   array is written as its raw bytes; lengths follow from the header.
@@ -208,7 +208,7 @@ hmg_status load(hmg_matrix** out, const char* path, cudaStream_t s)
         return HMG_ERR_INVALID;
     }
     if (ver != VERSION || hb != sizeof(Header) || !get(f, &H, sizeof H)) {
-        set_error("hmg_load: %s has format version %u / header %u bytes; this build reads %u / %zu", path, ver, hb,
+        set_error("hmg_load: %s has format version %u / header %u bytes; this library reads %u / %zu", path, ver, hb,
                   VERSION, sizeof(Header));
         return HMG_ERR_UNSUPPORTED;
     }

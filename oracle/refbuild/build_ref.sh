@@ -12,7 +12,7 @@
 #   * tree.cu relies on thrust/remove.h arriving through another header, which the
 #     CUDA 12.9 Thrust no longer does -> -include thrust/remove.h;
 #   * src/ must not be on the include path (its vendored CUB 1.x shadows the
-#     toolkit's and fails Thrust's version check) -> the headers the driver needs
+#     toolkit's and fails Thrust's version check) -> the headers the dump program needs
 #     are linked into oracle/_ref/include instead;
 #   * sm_100a instead of sm_61, no -G.
 set -euo pipefail

@@ -1,6 +1,6 @@
 """The multi-GPU plumbing of bench.py on CPU ranks (gloo, world size 2): replicas time
 the same workload independently and rank 0 reports the slowest rank's time.  The
-H-matvec itself does not shard across GPUs in this build (replicas only)."""
+H-matvec itself does not shard across GPUs in this engine (replicas only)."""
 import os
 import socket
 
