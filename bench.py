@@ -361,14 +361,13 @@ def run_engine(a, rank, world):
     if a.nrhs > 1:
         line["multi_rhs"] = multi_rhs_timing(torch, H, x, n, a.nrhs, a.steps, stream, world, err)
         if a.tc:
-            H.build_bf16_factors(near=hmg.PREC_BF16)
-            line["multi_rhs_tensor_cores"] = multi_rhs_timing(torch, H, x, n, a.nrhs, a.steps, stream, world, err)
-            H.build_bf16_factors(near=hmg.PREC_FP32)
-            line["multi_rhs_tensor_cores_near_fp32"] = multi_rhs_timing(torch, H, x, n, a.nrhs, a.steps, stream,
-                                                                        world, err)
-            H.build_bf16_factors(near=hmg.PREC_BF16X3)
-            line["multi_rhs_tensor_cores_bf16x3"] = multi_rhs_timing(torch, H, x, n, a.nrhs, a.steps, stream,
-                                                                     world, err)
+            modes = {"bf16": ("multi_rhs_tensor_cores", hmg.PREC_BF16),
+                     "near-fp32": ("multi_rhs_tensor_cores_near_fp32", hmg.PREC_FP32),
+                     "bf16x3": ("multi_rhs_tensor_cores_bf16x3", hmg.PREC_BF16X3)}
+            for name in (modes if a.tc_mode == "all" else [a.tc_mode]):
+                key, prec = modes[name]
+                H.build_bf16_factors(near=prec)
+                line[key] = multi_rhs_timing(torch, H, x, n, a.nrhs, a.steps, stream, world, err)
     if rank == 0 and world == 1 and not a.no_cpu:
         kind = O.KERNEL_MATERN32
         rate, nrows, dt, thr = cpu_direct_rate(p, x, kind, O.kernel_param(kind, W["rho"]), target_s=a.cpu_seconds)
@@ -785,6 +784,8 @@ def main(argv=None):
     ap.add_argument("--near", default="stored", choices=["stored", "onthefly"])
     ap.add_argument("--nrhs", type=int, default=1,
                     help="also time products of this many vectors at once (hmg_matvec_multi)")
+    ap.add_argument("--tc-mode", default="all", choices=["all", "bf16", "near-fp32", "bf16x3"],
+                    help="tensor-core operand modes --tc measures")
     ap.add_argument("--tc", action="store_true",
                     help="with --nrhs and --prec fp32: also time the tensor-core path (BF16 factor copy)")
     ap.add_argument("--arith", default="fp32", choices=["fp32", "fp64"],
