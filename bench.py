@@ -363,7 +363,8 @@ def run_engine(a, rank, world):
         if a.tc:
             modes = {"bf16": ("multi_rhs_tensor_cores", hmg.PREC_BF16),
                      "near-fp32": ("multi_rhs_tensor_cores_near_fp32", hmg.PREC_FP32),
-                     "bf16x3": ("multi_rhs_tensor_cores_bf16x3", hmg.PREC_BF16X3)}
+                     "bf16x3": ("multi_rhs_tensor_cores_bf16x3", hmg.PREC_BF16X3),
+                     "bf16x6": ("multi_rhs_tensor_cores_bf16x6", hmg.PREC_BF16X6)}
             for name in (modes if a.tc_mode == "all" else [a.tc_mode]):
                 key, prec = modes[name]
                 H.build_bf16_factors(near=prec)
@@ -784,7 +785,7 @@ def main(argv=None):
     ap.add_argument("--near", default="stored", choices=["stored", "onthefly"])
     ap.add_argument("--nrhs", type=int, default=1,
                     help="also time products of this many vectors at once (hmg_matvec_multi)")
-    ap.add_argument("--tc-mode", default="all", choices=["all", "bf16", "near-fp32", "bf16x3"],
+    ap.add_argument("--tc-mode", default="all", choices=["all", "bf16", "near-fp32", "bf16x3", "bf16x6"],
                     help="tensor-core operand modes --tc measures")
     ap.add_argument("--tc", action="store_true",
                     help="with --nrhs and --prec fp32: also time the tensor-core path (BF16 factor copy)")

@@ -26,6 +26,7 @@ PREC_FP32 = 1
 PREC_MIXED = 2
 PREC_BF16 = 3
 PREC_BF16X3 = 4
+PREC_BF16X6 = 5
 NEAR_STORED = 0
 NEAR_ONTHEFLY = 1
 

@@ -229,17 +229,19 @@ hmg_status hmg_build_tensor_core_operands(hmg_matrix* h, int near_precision)
 {
     HMG_REQUIRE(h, HMG_ERR_INVALID, "hmg_build_tensor_core_operands: NULL handle");
     HMG_REQUIRE(near_precision == HMG_PREC_BF16 || near_precision == HMG_PREC_FP32 ||
-                    near_precision == HMG_PREC_BF16X3,
+                    near_precision == HMG_PREC_BF16X3 || near_precision == HMG_PREC_BF16X6,
                 HMG_ERR_INVALID,
-                "hmg_build_tensor_core_operands: precision %d is not HMG_PREC_BF16, HMG_PREC_FP32 or HMG_PREC_BF16X3",
+                "hmg_build_tensor_core_operands: precision %d is not HMG_PREC_BF16, HMG_PREC_FP32, "
+                "HMG_PREC_BF16X3 or HMG_PREC_BF16X6",
                 near_precision);
-    return build_bf16_factors(h, near_precision != HMG_PREC_FP32, near_precision == HMG_PREC_BF16X3);
+    const int parts = near_precision == HMG_PREC_BF16X6 ? 3 : near_precision == HMG_PREC_BF16X3 ? 2 : 1;
+    return build_bf16_factors(h, near_precision != HMG_PREC_FP32, parts);
 }
 
 hmg_status hmg_build_bf16_factors(hmg_matrix* h)
 {
     HMG_REQUIRE(h, HMG_ERR_INVALID, "hmg_build_bf16_factors: NULL handle");
-    return build_bf16_factors(h, true, false);
+    return build_bf16_factors(h, true, 1);
 }
 
 hmg_status hmg_save(hmg_matrix* h, const char* path)

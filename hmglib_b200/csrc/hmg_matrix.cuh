@@ -89,10 +89,10 @@ struct hmg_matrix {
     void* tc_u = nullptr;                     // pass 2 A operands: U slices, near slices
     void* tc_v = nullptr;                     // pass 1 A operands: V_b^T
     void* tc_bbuf = nullptr;                  // per product: X cores, then t_b cores
-    void* tc_u_lo = nullptr;                  // split operands: low parts of tc_u, tc_v, tc_bbuf
-    void* tc_v_lo = nullptr;
-    void* tc_bbuf_lo = nullptr;
-    bool tc_split = false;                    // operands as BF16 hi + lo (three MMAs per K step)
+    void* tc_u_part[2] = {nullptr, nullptr};  // split operands: the further BF16 parts of
+    void* tc_v_part[2] = {nullptr, nullptr};  // tc_u, tc_v and tc_bbuf (what the parts before
+    void* tc_bbuf_part[2] = {nullptr, nullptr};  // them miss, rounded to BF16)
+    int tc_parts = 1;                         // BF16 parts per operand: 1, 2 (hi + lo) or 3
     char* tc_steps[2] = {nullptr, nullptr};   // per pass: steps, CTA by CTA
     char* tc_jobs[2] = {nullptr, nullptr};    // per pass: jobs, CTA by CTA
     char* tc_cta[2] = {nullptr, nullptr};     // per CTA: first job and step (int2), then the ends
@@ -147,7 +147,7 @@ hmg_status fill_near(hmg_matrix* h, int precision);
 hmg_status matvec_device(hmg_matrix* h, const double* x, double* y, bool fp64_arith = false);
 hmg_status matvec_multi(hmg_matrix* h, int nrhs, const double* X, int ldx, double* Y, int ldy);
 hmg_status matvec_multi_tc(hmg_matrix* h, int nrhs, const double* X, int ldx, double* Y, int ldy);
-hmg_status build_bf16_factors(hmg_matrix* h, bool near_on_tensor_cores, bool split);
+hmg_status build_bf16_factors(hmg_matrix* h, bool near_on_tensor_cores, int parts);
 hmg_status autotune(hmg_matrix* h, int reps, int* best_piece, int* best_ctas, double* best_ms);
 void free_tc(hmg_matrix* h);
 void free_product_graph(hmg_matrix* h);

@@ -59,7 +59,6 @@ static constexpr int TC_ISSUERS = 8;       // lanes of the copy warp issuing at 
 static constexpr int TC_ABYTES = 49152;    // A chunk of a step: at most 384 core matrices
 static constexpr int TC_BBYTES = 32768;    // B chunks of a step: at most 32 K cores x 8 vector cores
 static constexpr int TC_MAXSTEP = 16;      // MMAs per step
-static constexpr int TC_MAXKS = 16;        // MMAs per sub-step
 static constexpr int TC_MAXSUB = 4;        // sub-steps (B copies) per step
 static constexpr int TC_THREADS = 192;     // warps 0-3 epilogue, 4 copies, 5 MMAs
 // B operands (X and t_b) are addressed in K cores: 8 columns or terms x NV vectors, NV * 16 bytes
@@ -83,18 +82,28 @@ struct TcJob {
 // ---------------------------------------------------------------------------
 // conversion of the FP32 factors and near field (once, by hmg_build_bf16_factors)
 // ---------------------------------------------------------------------------
-// v as BF16, and (split operands, lo != nullptr) the BF16 rounding of what that misses:
-// hi + lo carries 16 significant bits of v
-__device__ __forceinline__ void store_split(__nv_bfloat16* hi, __nv_bfloat16* lo, size_t i, float v)
+// Destinations of an operand's BF16 parts: part 0 is the BF16 rounding of a value, part
+// p the BF16 rounding of what parts 0..p-1 miss (each difference is exact in FP32), so
+// that 1, 2 or 3 parts carry 8, 16 or 24 significant bits of it.
+struct TcParts {
+    __nv_bfloat16* p[3];
+    int n;
+};
+
+__device__ __forceinline__ void store_parts(const TcParts& out, long long base, size_t i, float v)
 {
-    const __nv_bfloat16 h = __float2bfloat16_rn(v);
-    hi[i] = h;
-    if (lo) lo[i] = __float2bfloat16_rn(v - __bfloat162float(h));
+#pragma unroll
+    for (int q = 0; q < 3; q++)
+        if (q < out.n) {
+            const __nv_bfloat16 h = __float2bfloat16_rn(v);
+            out.p[q][base + i] = h;
+            v -= __bfloat162float(h);
+        }
 }
 
 // far pair: U slice (s_pad x r, column-major) -> A cores, rc = s8 / 8, K = r16
 __global__ void k_tc_u(const PairDesc* desc, const int* plist, const long long* aoff, const int* ptile,
-                       const int* tile_s, int n, __nv_bfloat16* out, __nv_bfloat16* out_lo)
+                       const int* tile_s, int n, TcParts out)
 {
     const int u = blockIdx.x;
     if (u >= n) return;
@@ -103,20 +112,19 @@ __global__ void k_tc_u(const PairDesc* desc, const int* plist, const long long* 
     const int s = tile_s[ptile[u]], sp = (s + 3) & ~3, s8 = (s + 7) & ~7;
     const int r = d.ncol, r16 = (r + 15) & ~15;
     const float* src = static_cast<const float*>(d.data);
-    __nv_bfloat16* dst = out + aoff[u] / 2;
-    __nv_bfloat16* dlo = out_lo ? out_lo + aoff[u] / 2 : nullptr;
+    const long long base = aoff[u] / 2;
     const int rc = s8 / 8;
     for (int idx = threadIdx.x; idx < s8 * r16; idx += blockDim.x) {
         const int core = idx >> 6, e = idx & 63;
         const int kc = core / rc, mc = core - kc * rc;
         const int i = mc * 8 + (e >> 3), k = kc * 8 + (e & 7);
-        store_split(dst, dlo, idx, (i < s && k < r) ? src[(size_t)k * sp + i] : 0.0f);
+        store_parts(out, base, idx, (i < s && k < r) ? src[(size_t)k * sp + i] : 0.0f);
     }
 }
 
 // near pair: slice (s_pad x m2, column-major) -> A cores with c0 mod 8 leading zero columns
 __global__ void k_tc_near(const PairDesc* desc, const int* plist, const long long* aoff, const int* ptile,
-                          const int* tile_s, int n, __nv_bfloat16* out, __nv_bfloat16* out_lo)
+                          const int* tile_s, int n, TcParts out)
 {
     const int u = blockIdx.x;
     if (u >= n) return;
@@ -124,14 +132,13 @@ __global__ void k_tc_near(const PairDesc* desc, const int* plist, const long lon
     const int s = tile_s[ptile[u]], sp = (s + 3) & ~3, s8 = (s + 7) & ~7;
     const int m2 = d.ncol, a = d.c0 & 7, kw = (a + m2 + 15) & ~15;
     const float* src = static_cast<const float*>(d.data);
-    __nv_bfloat16* dst = out + aoff[u] / 2;
-    __nv_bfloat16* dlo = out_lo ? out_lo + aoff[u] / 2 : nullptr;
+    const long long base = aoff[u] / 2;
     const int rc = s8 / 8;
     for (long long idx = threadIdx.x; idx < (long long)s8 * kw; idx += blockDim.x) {
         const int core = (int)(idx >> 6), e = (int)(idx & 63);
         const int kc = core / rc, mc = core - kc * rc;
         const int i = mc * 8 + (e >> 3), c = kc * 8 + (e & 7) - a;
-        store_split(dst, dlo, idx, (i < s && c >= 0 && c < m2) ? src[(size_t)c * sp + i] : 0.0f);
+        store_parts(out, base, idx, (i < s && c >= 0 && c < m2) ? src[(size_t)c * sp + i] : 0.0f);
     }
 }
 
@@ -139,8 +146,7 @@ __global__ void k_tc_near(const PairDesc* desc, const int* plist, const long lon
 // cores.  A stack holds the V^T of blocks with the same columns, one under the other
 // (vaux: stack row cores << 8 | the block's first row core in the stack).
 __global__ void k_tc_v(const int* blist, const long long* voff, const int* vaux, int n, void* const* ptrV,
-                       const int* rank, const int* blk_c0, const int* blk_m2, __nv_bfloat16* out,
-                       __nv_bfloat16* out_lo)
+                       const int* rank, const int* blk_c0, const int* blk_m2, TcParts out)
 {
     const int u = blockIdx.x;
     if (u >= n) return;
@@ -148,14 +154,13 @@ __global__ void k_tc_v(const int* blist, const long long* voff, const int* vaux,
     const int r = rank[b], r16 = (r + 15) & ~15, m2 = blk_m2[b], m2p = (m2 + 3) & ~3;
     const int a = blk_c0[b] & 7, kw = (a + m2 + 15) & ~15;
     const float* V = static_cast<const float*>(ptrV[b]);
-    __nv_bfloat16* dst = out + voff[u] / 2;
-    __nv_bfloat16* dlo = out_lo ? out_lo + voff[u] / 2 : nullptr;
+    const long long base = voff[u] / 2;
     const int rb = r16 / 8;
     for (long long idx = threadIdx.x; idx < (long long)r16 * kw; idx += blockDim.x) {
         const int core = (int)(idx >> 6), e = (int)(idx & 63);
         const int kc = core / rb, mc = core - kc * rb;
         const int m = mc * 8 + (e >> 3), c = kc * 8 + (e & 7) - a;
-        store_split(dst, dlo, ((size_t)kc * rc + off8 + mc) * 64 + e,
+        store_parts(out, base, ((size_t)kc * rc + off8 + mc) * 64 + e,
                     (m < r && c >= 0 && c < m2) ? V[(size_t)m * m2p + c] : 0.0f);
     }
 }
@@ -166,22 +171,29 @@ __global__ void k_tc_v(const int* blist, const long long* voff, const int* vaux,
 // thread (g, j): columns 8g..8g+7 of vector j, one 16-byte row of K core g
 template <int NV>
 __global__ void k_tc_x(const double* __restrict__ X, int ldx, int nrhs, const int* __restrict__ perm1, int n,
-                       long long ngroups, uint4* xb, uint4* xb_lo)
+                       long long ngroups, TcParts xb)
 {
     const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (idx >= ngroups * NV) return;
     const long long g = idx / NV;
     const int j = (int)(idx % NV);
-    __nv_bfloat16 v[8], w[8];
+    float f[8];
 #pragma unroll
     for (int e = 0; e < 8; e++) {
         const long long c = g * 8 + e;
-        const float f = c < n && j < nrhs ? (float)X[(size_t)perm1[c] + (size_t)j * ldx] : 0.0f;
-        v[e] = __float2bfloat16_rn(f);
-        w[e] = __float2bfloat16_rn(f - __bfloat162float(v[e]));
+        f[e] = c < n && j < nrhs ? (float)X[(size_t)perm1[c] + (size_t)j * ldx] : 0.0f;
     }
-    xb[(g * (NV / 8) + (j >> 3)) * 8 + (j & 7)] = *reinterpret_cast<const uint4*>(v);
-    if (xb_lo) xb_lo[(g * (NV / 8) + (j >> 3)) * 8 + (j & 7)] = *reinterpret_cast<const uint4*>(w);
+#pragma unroll
+    for (int q = 0; q < 3; q++)
+        if (q < xb.n) {
+            __nv_bfloat16 v[8];
+#pragma unroll
+            for (int e = 0; e < 8; e++) {
+                v[e] = __float2bfloat16_rn(f[e]);
+                f[e] -= __bfloat162float(v[e]);
+            }
+            reinterpret_cast<uint4*>(xb.p[q])[(g * (NV / 8) + (j >> 3)) * 8 + (j & 7)] = *reinterpret_cast<const uint4*>(v);
+        }
 }
 
 // ---------------------------------------------------------------------------
@@ -286,16 +298,26 @@ __device__ __forceinline__ uint32_t pack_bf16(float lo, float hi)
 // Steps of CTA c: [cta[c].y, cta[c+1].y); its jobs: [cta[c].x, cta[c+1].x).  NV vectors per
 // pass (MMA N); B K cores are NV * 16 bytes.  Pass 1 (MODE 0) writes t_b cores, K core kc of
 // job j (a stack) to B K core tb_kc + map[16 j + kc]; pass 2 (MODE 1) writes (add_y: adds
-// to) rows of Y, tile row i to Y row map[r0 + i].  SPLIT: every operand also has its low
-// part (A_lo, B_lo: the BF16 rounding of what the BF16 value misses, same layout); a step
-// then brings A hi, A lo, B hi, B lo and each K step runs hi*hi + hi*lo + lo*hi.
-template <int MODE, int NV, bool SPLIT>
+// to) rows of Y, tile row i to Y row map[r0 + i].  PARTS > 1 (split operands): every
+// operand comes as PARTS BF16 parts of the same layout (A.p[q], B.p[q]); a step brings
+// the A parts, then the B parts, and each K step runs hi*hi plus the correction terms
+// down to 2^-16 of it: hi*lo + lo*hi (2 parts), and hi*lo2 + lo2*hi + lo*lo (3 parts).
+struct TcOperands {
+    const char* a[3];  // A arena, per part
+    char* b[3];        // B buffer (X cores, then t_b cores), per part
+};
+
+template <int MODE, int NV, int PARTS>
 __global__ void __launch_bounds__(TC_THREADS, 1)
     k_tc_pass(const TcStep* __restrict__ steps, const TcJob* __restrict__ jobs, const int2* __restrict__ cta,
-              const char* __restrict__ A, const char* __restrict__ A_lo, char* Bbuf, char* B_lo, long long tb_kc,
-              const int* __restrict__ map, int nrhs, double* Y, int ldy, int add_y, int* err)
+              const TcOperands op, long long tb_kc, const int* __restrict__ map, int nrhs, double* Y, int ldy,
+              int add_y, int* err)
 {
     constexpr int KB = NV * 16;
+    constexpr bool SPLIT = PARTS > 1;
+    // two accumulator buffers; split: each holds hi*hi (columns 0..NV-1) and the
+    // correction terms (NV..2NV-1)
+    constexpr int TMEM_COLS = SPLIT ? 4 * NV : 2 * NV;
     extern __shared__ __align__(1024) unsigned char tc_raw[];
     TcSmem& sm = *reinterpret_cast<TcSmem*>(tc_raw);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -318,7 +340,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
     }
     if (warp == 5) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&sm.tmem)),
-                     "n"(2 * NV));
+                     "n"(TMEM_COLS));
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
     }
     __syncthreads();
@@ -343,7 +365,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
             const int ks_all = (mine.meta >> 16) & 0xff;
             const int ab = ks_all * 2 * (mine.meta & 0xff) * 128, bb = ks_all * 2 * KB;
             __syncwarp();
-            sm.step_bytes[lane] = SPLIT ? 2 * (ab + bb) : ab + bb;
+            sm.step_bytes[lane] = PARTS * (ab + bb);
             __syncwarp();
             for (int k = 0; k < cnt && ok;) {
                 int m = 0;
@@ -387,21 +409,23 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                 if (lane >= k && lane < k + m) {
                     const int slot = (i0 + lane) % TC_SLOTS, pos = sm.slot_pos[slot];
                     const uint32_t a = smem_u32(sm.ring + pos);
-                    const int a_span = SPLIT ? 2 * ab : ab;  // A hi [, A lo], then B hi [, B lo]
+                    const int a_span = PARTS * ab;  // the A parts, then the B parts
                     sm.slot_a[slot] = a;
                     sm.slot_b[slot] = a + a_span;
                     sm.slot_meta[slot] = mine.meta;
-                    mbar_arrive_expect_tx(&sm.full[slot], SPLIT ? 2 * (ab + bb) : ab + bb);
-                    bulk_g2s_first(sm.ring + pos, A + mine.a_off, ab, &sm.full[slot], pol);
-                    if (SPLIT) bulk_g2s_first(sm.ring + pos + ab, A_lo + mine.a_off, ab, &sm.full[slot], pol);
+                    mbar_arrive_expect_tx(&sm.full[slot], PARTS * (ab + bb));
+#pragma unroll
+                    for (int q = 0; q < PARTS; q++)
+                        bulk_g2s_first(sm.ring + pos + q * ab, op.a[q] + mine.a_off, ab, &sm.full[slot], pol);
                     const int nsub = ((mine.meta >> 10) & 3) + 1;
                     int boff = a_span;
 #pragma unroll
                     for (int j = 0; j < TC_MAXSUB; j++)
                         if (j < nsub) {
                             const int kb = (((mine.kss >> (4 * j)) & 15) + 1) * 2 * KB;
-                            bulk_g2s(sm.ring + pos + boff, Bbuf + mine.b_off[j] * KB, kb, &sm.full[slot]);
-                            if (SPLIT) bulk_g2s(sm.ring + pos + boff + bb, B_lo + mine.b_off[j] * KB, kb, &sm.full[slot]);
+#pragma unroll
+                            for (int q = 0; q < PARTS; q++)
+                                bulk_g2s(sm.ring + pos + boff + q * bb, op.b[q] + mine.b_off[j] * KB, kb, &sm.full[slot]);
                             boff += kb;
                         }
                 }
@@ -419,7 +443,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
         if (lane == 0) {
             int jc = 0;
             for (int i = 0; i < nsteps; i++) {
-                const int slot = i % TC_SLOTS, buf = jc & 1;
+                const int slot = i % TC_SLOTS;
                 if (*fail || !mbar_wait(&sm.full[slot], (i / TC_SLOTS) & 1, err, 14)) {
                     *fail = 1;
                     break;
@@ -427,8 +451,12 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                 const uint32_t a0 = sm.slot_a[slot], b0 = sm.slot_b[slot];
                 const int meta = sm.slot_meta[slot], ks_all = (meta >> 16) & 0xff;
                 const bool first = meta & 256, last = meta & 512;
-                if (first && jc >= 2) {  // the epilogue has read this accumulator's previous job
-                    if (!mbar_wait(&sm.acce[buf], ((jc >> 1) - 1) & 1, err, 13)) {
+                // split: every step has its own accumulator (drained by the epilogue, which
+                // sums the steps of a job in FP32 on the CUDA cores), so that no accumulator
+                // runs through more than one step's MMAs; otherwise one per job
+                const int u = SPLIT ? i : jc, buf = u & 1;
+                if ((SPLIT || first) && u >= 2) {  // the epilogue has read this buffer's previous use
+                    if (!mbar_wait(&sm.acce[buf], ((u >> 1) - 1) & 1, err, 13)) {
                         *fail = 1;
                         break;
                     }
@@ -439,121 +467,166 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                 // adds to their start-address field (16-byte units; shared addresses stay
                 // below 2^18, so the field never carries): this lane's issue rate bounds the pass.
                 const uint32_t lbo = (uint32_t)(meta & 0xff) * 128u;
-                const uint32_t d = tmem + (uint32_t)(buf * NV);
+                const uint32_t d = tmem + (uint32_t)(buf * (SPLIT ? 2 * NV : NV));
                 const uint64_t da = (2 * lbo) >> 4, db = (2 * KB) >> 4;
                 uint64_t ad = smem_desc(a0, lbo, 128), bd = smem_desc(b0, KB, 128);
-                // low parts: A lo right after A hi, B lo right after B hi (16-byte units)
+                // part q of A (of B) lies q * alo (q * blo) 16-byte units after part 0
                 const uint64_t alo = (uint64_t)(ks_all * 2 * lbo) >> 4, blo = (uint64_t)(ks_all * 2 * KB) >> 4;
-                uint32_t acc = first ? 0u : 1u;
+                uint32_t acc = (SPLIT || first) ? 0u : 1u;
 #pragma unroll 4
                 for (int q = 0; q < ks_all; q++) {
                     tc_mma(d, ad, bd, tc_idesc<NV>(), acc);
                     if (SPLIT) {
-                        tc_mma(d, ad, bd + blo, tc_idesc<NV>(), 1u);
-                        tc_mma(d, ad + alo, bd, tc_idesc<NV>(), 1u);
+                        // the correction terms in their own accumulator: added to hi*hi they
+                        // would each be truncated at the scale of the (256x larger) sum
+                        tc_mma(d + NV, ad, bd + blo, tc_idesc<NV>(), acc);
+                        tc_mma(d + NV, ad + alo, bd, tc_idesc<NV>(), 1u);
+                    }
+                    if (PARTS == 3) {
+                        tc_mma(d + NV, ad, bd + 2 * blo, tc_idesc<NV>(), 1u);
+                        tc_mma(d + NV, ad + 2 * alo, bd, tc_idesc<NV>(), 1u);
+                        tc_mma(d + NV, ad + alo, bd + blo, tc_idesc<NV>(), 1u);
                     }
                     acc = 1u;
                     ad += da;
                     bd += db;
                 }
                 tc_commit(&sm.empty[slot]);
-                if (last) {
-                    tc_commit(&sm.accf[buf]);
-                    jc++;
-                }
+                if (SPLIT || last) tc_commit(&sm.accf[buf]);
+                if (last) jc++;
             }
             tc_commit(&sm.fin);  // every MMA issued here has completed before tensor memory is freed
             mbar_wait(&sm.fin, 0, err, 15);
         }
         __syncwarp();
     } else {
-        // ---- epilogue: warp w owns accumulator rows 32w..32w+31; lane l holds job j0 + l ----
+        // ---- epilogue: warp w owns accumulator rows 32w..32w+31 ----
+        const int row = warp * 32 + lane;
+        // a finished job's sums f (row `row`, vectors 0..NV-1) to their destination
+        auto emit = [&](const float (&f)[NV], int rows, int yrow, const int (&tdst)[4]) {
+            if (MODE == 1) {
+                if (row < rows) {
+                    double* y = Y + yrow;
+#pragma unroll
+                    for (int q = 0; q < NV; q++)
+                        if (q < nrhs) y[(size_t)q * ldy] = (add_y ? y[(size_t)q * ldy] : 0.0) + (double)f[q];
+                }
+            } else {
+                // term row -> B cores of pass 2 (K = term): element (term m, vector q) at byte
+                // ((m / 8) * NV / 8 + q / 8) * 128 + (q % 8) * 16 + (m % 8) * 2 of its block's
+                // t_b; this warp's 32 stack rows fill the stack's K cores 4w..4w+3.  Lanes 2p,
+                // 2p+1 pair their terms into 32-bit words (even lane: vector 2t, odd lane:
+                // vector 2t+1); 16-byte row u of the staging (K core u / NV, vector u % NV) sits
+                // at u ^ (2 (u / NV)), which spreads the four K cores over all banks.
+                uint32_t* stg = reinterpret_cast<uint32_t*>(sm.stg[warp]);
+                const bool odd = lane & 1;
+#pragma unroll
+                for (int part = 0; part < PARTS; part++) {
+                    // part 0: BF16 of t; part p: BF16 of what parts 0..p-1 miss
+#pragma unroll
+                    for (int t = 0; t < NV / 2; t++) {
+                        float v0 = f[2 * t], v1 = f[2 * t + 1];
+#pragma unroll
+                        for (int pp = 0; pp < part; pp++) {
+                            v0 -= __bfloat162float(__float2bfloat16_rn(v0));
+                            v1 -= __bfloat162float(__float2bfloat16_rn(v1));
+                        }
+                        const float x = __shfl_xor_sync(~0u, odd ? v0 : v1, 1);
+                        const int q = odd ? 2 * t + 1 : 2 * t;
+                        const uint32_t w = odd ? pack_bf16(x, v1) : pack_bf16(v0, x);
+                        const int u = (lane >> 3) * NV + q;
+                        stg[(u ^ ((lane >> 3) * 2)) * 4 + ((lane & 7) >> 1)] = w;
+                    }
+                    __syncwarp();
+                    uint4* dst = reinterpret_cast<uint4*>(op.b[part]);
+                    const uint4* src = reinterpret_cast<const uint4*>(stg);
+#pragma unroll
+                    for (int it = 0; it < NV / 8; it++) {
+                        const int u = it * 32 + lane, kcl = u / NV;
+                        if (warp * 4 + kcl < (rows >> 3))
+                            dst[(size_t)(tb_kc + tdst[kcl]) * (KB / 16) + (u % NV)] = src[u ^ (kcl * 2)];
+                    }
+                    __syncwarp();
+                }
+            }
+        };
+        // where job (r0, rows)'s rows go, fetched before its accumulator is waited for
+        auto dests = [&](int r0, int rows, int& yrow, int (&tdst)[4]) {
+            yrow = (MODE == 1 && row < rows) ? map[r0 + row] : 0;
+#pragma unroll
+            for (int q = 0; q < 4; q++)
+                tdst[q] = (MODE == 0 && warp * 4 + q < (rows >> 3)) ? map[r0 * 16 + warp * 4 + q] : 0;
+        };
+        // the next drain of accumulator buffer buf (use u of it) -> this thread's row
+        auto drain = [&](int u, int buf, float (&f)[NV], bool fresh) -> bool {
+            if (!__all_sync(~0u, !*fail && mbar_wait(&sm.accf[buf], (u >> 1) & 1, err, 16))) return false;
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const uint32_t taddr = tmem + (uint32_t)(buf * (SPLIT ? 2 * NV : NV)) + ((uint32_t)(warp * 32) << 16);
+#pragma unroll
+            for (int h = 0; h < NV / 32; h++) {
+                uint32_t v[32], c[32];
+                tc_ld32(taddr + 32 * h, v);
+                if (SPLIT) tc_ld32(taddr + NV + 32 * h, c);
+                asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+                for (int q = 0; q < 32; q++) {
+                    const float t = SPLIT ? __uint_as_float(v[q]) + __uint_as_float(c[q]) : __uint_as_float(v[q]);
+                    f[32 * h + q] = fresh ? t : f[32 * h + q] + t;
+                }
+            }
+            asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&sm.acce[buf]);
+            return true;
+        };
         const int njobs = hi.x - lo.x;
         const int2* my_jobs = reinterpret_cast<const int2*>(jobs) + lo.x;
-        int2 nxt = lane < njobs ? my_jobs[lane] : make_int2(0, 0);
         bool ok = true;
-        for (int j0 = 0; j0 < njobs && ok; j0 += 32) {
-            const int2 mine = nxt;
-            if (j0 + 32 + lane < njobs) nxt = my_jobs[j0 + 32 + lane];
-            const int cnt = min(32, njobs - j0);
-            for (int k = 0; k < cnt; k++) {
-                const int r0 = __shfl_sync(~0u, mine.x, k), rows = __shfl_sync(~0u, mine.y, k);
-                const int jc = j0 + k, buf = jc & 1;
-                const int row = warp * 32 + lane;
-                // pass 2: this row's place in Y, fetched before the wait
-                const int yrow = (MODE == 1 && row < rows) ? map[r0 + row] : 0;
-                int tdst[4];
-                if (MODE == 0) {
-#pragma unroll
-                    for (int q = 0; q < 4; q++) tdst[q] = warp * 4 + q < (rows >> 3) ? map[r0 * 16 + warp * 4 + q] : 0;
-                }
-                ok = !*fail && mbar_wait(&sm.accf[buf], (jc >> 1) & 1, err, 16);
-                if (!__all_sync(~0u, ok)) {
-                    ok = false;
-                    break;
-                }
-                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-                uint32_t v[NV];
-                const uint32_t taddr = tmem + (uint32_t)(buf * NV) + ((uint32_t)(warp * 32) << 16);
-                tc_ld32(taddr, reinterpret_cast<uint32_t(&)[32]>(v[0]));
-                if (NV == 64) tc_ld32(taddr + 32, reinterpret_cast<uint32_t(&)[32]>(v[NV - 32]));
-                asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-                asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-                __syncwarp();
-                if (lane == 0) mbar_arrive(&sm.acce[buf]);
-                if (MODE == 1) {
-                    if (row < rows) {
-                        double* y = Y + yrow;
-#pragma unroll
-                        for (int q = 0; q < NV; q++)
-                            if (q < nrhs) y[(size_t)q * ldy] = (add_y ? y[(size_t)q * ldy] : 0.0) + (double)__uint_as_float(v[q]);
+        float f[NV];
+        if (SPLIT) {
+            // one drain per step; lane l holds the meta word of step i0 + l
+            int jc = 0, rows = 0, yrow = 0, tdst[4] = {0, 0, 0, 0};
+            for (int i0 = 0; i0 < nsteps && ok; i0 += 32) {
+                const int mt = i0 + lane < nsteps ? my_steps[i0 + lane].meta : 0;
+                const int cnt = min(32, nsteps - i0);
+                for (int k = 0; k < cnt; k++) {
+                    const int i = i0 + k, meta = __shfl_sync(~0u, mt, k);
+                    const bool first = meta & 256, last = meta & 512;
+                    if (first) {
+                        const int2 jb = jc < njobs ? my_jobs[jc] : make_int2(0, 0);
+                        rows = jb.y;
+                        dests(jb.x, rows, yrow, tdst);
                     }
-                } else {
-                    // term row -> B cores of pass 2 (K = term): element (term m, vector q) at byte
-                    // ((m / 8) * NV / 8 + q / 8) * 128 + (q % 8) * 16 + (m % 8) * 2 of its block's
-                    // t_b; this warp's 32 stack rows fill the stack's K cores 4w..4w+3.  Lanes 2p,
-                    // 2p+1 pair their terms into 32-bit words (even lane: vector 2t, odd lane:
-                    // vector 2t+1); 16-byte row u of the staging (K core u / NV, vector u % NV) sits
-                    // at u ^ (2 (u / NV)), which spreads the four K cores over all banks.
-                    uint32_t* stg = reinterpret_cast<uint32_t*>(sm.stg[warp]);
-                    const bool odd = lane & 1;
-#pragma unroll
-                    for (int part = 0; part < (SPLIT ? 2 : 1); part++) {
-                        // part 0: BF16 of t; part 1 (split): BF16 of what part 0 misses
-#pragma unroll
-                        for (int t = 0; t < NV / 2; t++) {
-                            float v0 = __uint_as_float(v[2 * t]), v1 = __uint_as_float(v[2 * t + 1]);
-                            if (part) {
-                                v0 -= __bfloat162float(__float2bfloat16_rn(v0));
-                                v1 -= __bfloat162float(__float2bfloat16_rn(v1));
-                            }
-                            const float x = __shfl_xor_sync(~0u, odd ? v0 : v1, 1);
-                            const int q = odd ? 2 * t + 1 : 2 * t;
-                            const uint32_t w = odd ? pack_bf16(x, v1) : pack_bf16(v0, x);
-                            const int u = (lane >> 3) * NV + q;
-                            stg[(u ^ ((lane >> 3) * 2)) * 4 + ((lane & 7) >> 1)] = w;
-                        }
-                        __syncwarp();
-                        uint4* dst = reinterpret_cast<uint4*>(part ? B_lo : Bbuf);
-                        const uint4* src = reinterpret_cast<const uint4*>(stg);
-#pragma unroll
-                        for (int it = 0; it < NV / 8; it++) {
-                            const int u = it * 32 + lane, kcl = u / NV;
-                            if (warp * 4 + kcl < (rows >> 3))
-                                dst[(size_t)(tb_kc + tdst[kcl]) * (KB / 16) + (u % NV)] = src[u ^ (kcl * 2)];
-                        }
-                        __syncwarp();
+                    if (!(ok = drain(i, i & 1, f, first))) break;
+                    if (last) {
+                        emit(f, rows, yrow, tdst);
+                        jc++;
                     }
                 }
             }
-            ok = __all_sync(~0u, ok);
+        } else {
+            // one drain per job; lane l holds job j0 + l
+            int2 nxt = lane < njobs ? my_jobs[lane] : make_int2(0, 0);
+            for (int j0 = 0; j0 < njobs && ok; j0 += 32) {
+                const int2 mine = nxt;
+                if (j0 + 32 + lane < njobs) nxt = my_jobs[j0 + 32 + lane];
+                const int cnt = min(32, njobs - j0);
+                for (int k = 0; k < cnt; k++) {
+                    const int r0 = __shfl_sync(~0u, mine.x, k), rows = __shfl_sync(~0u, mine.y, k);
+                    const int jc = j0 + k;
+                    int yrow, tdst[4];
+                    dests(r0, rows, yrow, tdst);
+                    if (!(ok = drain(jc, jc & 1, f, true))) break;
+                    emit(f, rows, yrow, tdst);
+                }
+            }
         }
         if (!ok) *fail = 1;
     }
     __syncthreads();
     if (warp == 5) {
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "n"(2 * NV));
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "n"(TMEM_COLS));
     }
 }
 
@@ -566,17 +639,14 @@ void free_tc(hmg_matrix* h)
     cudaStream_t s = h->stream;
     if (h->tc_u) cudaFree(h->tc_u);
     if (h->tc_v) cudaFree(h->tc_v);
-    if (h->tc_u_lo) cudaFree(h->tc_u_lo);
-    if (h->tc_v_lo) cudaFree(h->tc_v_lo);
-    h->tc_u_lo = h->tc_v_lo = nullptr;
-    if (h->tc_bbuf_lo) {
-        cudaStreamSynchronize(s);
-        cudaFree(h->tc_bbuf_lo);
-        h->tc_bbuf_lo = nullptr;
-    }
-    if (h->tc_bbuf) {
-        cudaStreamSynchronize(s);  // a product in flight may still read it
-        cudaFree(h->tc_bbuf);
+    if (h->tc_bbuf || h->tc_bbuf_part[0] || h->tc_bbuf_part[1])
+        cudaStreamSynchronize(s);  // a product in flight may still read them
+    if (h->tc_bbuf) cudaFree(h->tc_bbuf);
+    for (int q = 0; q < 2; q++) {
+        if (h->tc_u_part[q]) cudaFree(h->tc_u_part[q]);
+        if (h->tc_v_part[q]) cudaFree(h->tc_v_part[q]);
+        if (h->tc_bbuf_part[q]) cudaFree(h->tc_bbuf_part[q]);
+        h->tc_u_part[q] = h->tc_v_part[q] = h->tc_bbuf_part[q] = nullptr;
     }
     h->tc_u = h->tc_v = h->tc_bbuf = nullptr;
     dfree(h->tc_kmap, s);
@@ -592,7 +662,7 @@ void free_tc(hmg_matrix* h)
     h->tc_grid = 0;
     h->tc_all_tiles = false;
     h->tc_near = false;
-    h->tc_split = false;
+    h->tc_parts = 1;
 }
 
 namespace {
@@ -670,7 +740,7 @@ struct JobList {
 
 // Every copy a step issues stays inside its arena and its stage, and every job's
 // output inside its buffer: checked here, on the host, before any launch.
-bool steps_in_bounds(const JobList& L, long long abytes, long long bkcores, long long out_limit, int q, bool split)
+bool steps_in_bounds(const JobList& L, long long abytes, long long bkcores, long long out_limit, int q, int parts)
 {
     for (const TcStep& st : L.steps) {
         const int rc = st.meta & 0xff, nsub = ((st.meta >> 10) & 3) + 1, ks_all = (st.meta >> 16) & 0xff;
@@ -681,7 +751,7 @@ bool steps_in_bounds(const JobList& L, long long abytes, long long bkcores, long
             if (st.b_off[j] < 0 || st.b_off[j] + 2ll * ks > bkcores) return false;
             sum += ks;
         }
-        if (sum != ks_all || rc < 1 || rc > 16 || (split ? 2 : 1) * ab > TC_ABYTES || (split ? 2 : 1) * bb > TC_BBYTES ||
+        if (sum != ks_all || rc < 1 || rc > 16 || parts * ab > TC_ABYTES || parts * bb > TC_BBYTES ||
             st.a_off < 0 || st.a_off % 16 ||
             st.a_off + ab > abytes)
             return false;
@@ -754,7 +824,7 @@ hmg_status alloc_arena(void** p, long long bytes, const char* what)
 
 }  // namespace
 
-hmg_status build_bf16_factors(hmg_matrix* h, bool near_tc, bool split)
+hmg_status build_bf16_factors(hmg_matrix* h, bool near_tc, int parts)
 {
     cudaStream_t s = h->stream;
     hmg_status st;
@@ -786,9 +856,9 @@ hmg_status build_bf16_factors(hmg_matrix* h, bool near_tc, bool split)
 
     // B buffer of a product, in K cores: X (8 columns each), then t_b (16 terms = 2 K cores per group)
     const long long xkc = (h->n[1] + 7) / 8 + 4;
-    // split operands bring hi and lo of every chunk: half the A and MMAs per step
-    const long long a_half = split ? TC_ABYTES / 2 : TC_ABYTES;
-    const int ks_limit = split ? TC_MAXSTEP / 2 : TC_MAXSTEP;
+    // split operands bring every part of a chunk: 1 / parts of the A bytes and MMAs per step
+    const long long a_half = TC_ABYTES / parts;
+    const int ks_limit = TC_MAXSTEP / parts;
     std::vector<long long> toff(nb, -1);
     long long tgroups = 0;
     JobList k1, k2;
@@ -882,8 +952,8 @@ hmg_status build_bf16_factors(hmg_matrix* h, bool near_tc, bool split)
 
     k1.make_steps(false, a_half, ks_limit);
     k2.make_steps(true, a_half, ks_limit);
-    if (!steps_in_bounds(k1, vbytes, xkc + tgroups * 2, (long long)kmap.size() / 16, 0, split) ||
-        !steps_in_bounds(k2, ubytes, xkc + tgroups * 2, h->n[0], 1, split)) {
+    if (!steps_in_bounds(k1, vbytes, xkc + tgroups * 2, (long long)kmap.size() / 16, 0, parts) ||
+        !steps_in_bounds(k2, ubytes, xkc + tgroups * 2, h->n[0], 1, parts)) {
         set_error("hmg_build_bf16_factors: internal error: an operand step leaves its buffer");
         return HMG_ERR_UNSUPPORTED;
     }
@@ -899,12 +969,16 @@ hmg_status build_bf16_factors(hmg_matrix* h, bool near_tc, bool split)
     }
     if (!kmap.empty())
         HMG_CUDA_TRY(cudaMemcpyAsync(h->tc_kmap, kmap.data(), sizeof(int) * kmap.size(), cudaMemcpyHostToDevice, s));
-    if ((st = alloc_arena(&h->tc_v, vbytes, "the V^T operands")) ||
-        (split && ((st = alloc_arena(&h->tc_u_lo, ubytes, "the tile operands' low parts")) ||
-                   (st = alloc_arena(&h->tc_v_lo, vbytes, "the V^T operands' low parts"))))) {
+    if ((st = alloc_arena(&h->tc_v, vbytes, "the V^T operands"))) {
         free_tc(h);
         return st;
     }
+    for (int q = 0; q + 1 < parts; q++)
+        if ((st = alloc_arena(&h->tc_u_part[q], ubytes, "the tile operands' further parts")) ||
+            (st = alloc_arena(&h->tc_v_part[q], vbytes, "the V^T operands' further parts"))) {
+            free_tc(h);
+            return st;
+        }
     int* dlist = nullptr;
     int* dtile = nullptr;
     long long* doff = nullptr;
@@ -921,16 +995,18 @@ hmg_status build_bf16_factors(hmg_matrix* h, bool near_tc, bool split)
         if (!tiles.empty())
             HMG_CUDA_TRY(cudaMemcpyAsync(dtile, tiles.data(), sizeof(int) * n, cudaMemcpyHostToDevice, s));
         const PairDesc* desc = static_cast<const PairDesc*>(h->pair_desc);
-        __nv_bfloat16* ulo = static_cast<__nv_bfloat16*>(h->tc_u_lo);  // null unless split
-        __nv_bfloat16* vlo = static_cast<__nv_bfloat16*>(h->tc_v_lo);
+        TcParts up{{static_cast<__nv_bfloat16*>(h->tc_u), static_cast<__nv_bfloat16*>(h->tc_u_part[0]),
+                    static_cast<__nv_bfloat16*>(h->tc_u_part[1])},
+                   parts};
+        TcParts vp{{static_cast<__nv_bfloat16*>(h->tc_v), static_cast<__nv_bfloat16*>(h->tc_v_part[0]),
+                    static_cast<__nv_bfloat16*>(h->tc_v_part[1])},
+                   parts};
         if (which == 0)
-            k_tc_u<<<n, 256, 0, s>>>(desc, dlist, doff, dtile, h->tile_s, n, static_cast<__nv_bfloat16*>(h->tc_u), ulo);
+            k_tc_u<<<n, 256, 0, s>>>(desc, dlist, doff, dtile, h->tile_s, n, up);
         else if (which == 1)
-            k_tc_near<<<n, 256, 0, s>>>(desc, dlist, doff, dtile, h->tile_s, n, static_cast<__nv_bfloat16*>(h->tc_u),
-                                        ulo);
+            k_tc_near<<<n, 256, 0, s>>>(desc, dlist, doff, dtile, h->tile_s, n, up);
         else
-            k_tc_v<<<n, 256, 0, s>>>(dlist, doff, dtile, n, h->ptrV, h->rank, h->blk_c0, h->blk_m2,
-                                     static_cast<__nv_bfloat16*>(h->tc_v), vlo);
+            k_tc_v<<<n, 256, 0, s>>>(dlist, doff, dtile, n, h->ptrV, h->rank, h->blk_c0, h->blk_m2, vp);
         HMG_LAUNCH_CHECK();
         HMG_CUDA_TRY(cudaStreamSynchronize(s));
         dfree(dlist, s);
@@ -955,31 +1031,37 @@ hmg_status build_bf16_factors(hmg_matrix* h, bool near_tc, bool split)
     h->tc_grid = grid;
     h->tc_all_tiles = all_tiles;
     h->tc_near = near_tc;
-    h->tc_split = split;
+    h->tc_parts = parts;
     h->tc_ready = true;
     return HMG_OK;
 }
 
-template <int NV, bool SPLIT>
+template <int NV, int PARTS>
 static hmg_status tc_product(hmg_matrix* h, int nrhs, const double* X, int ldx, double* Y, int ldy)
 {
     cudaStream_t s = h->stream;
     hmg_status st;
-    char* bbuf = static_cast<char*>(h->tc_bbuf);
-    char* blo = static_cast<char*>(h->tc_bbuf_lo);  // null unless split
+    TcOperands op1{{static_cast<const char*>(h->tc_v), static_cast<const char*>(h->tc_v_part[0]),
+                    static_cast<const char*>(h->tc_v_part[1])},
+                   {static_cast<char*>(h->tc_bbuf), static_cast<char*>(h->tc_bbuf_part[0]),
+                    static_cast<char*>(h->tc_bbuf_part[1])}};
+    TcOperands op2 = op1;
+    op2.a[0] = static_cast<const char*>(h->tc_u);
+    op2.a[1] = static_cast<const char*>(h->tc_u_part[0]);
+    op2.a[2] = static_cast<const char*>(h->tc_u_part[1]);
     const long long xkc = h->tc_xkc;
-    k_tc_x<NV><<<(unsigned)((xkc * NV + 255) / 256), 256, 0, s>>>(X, ldx, nrhs, h->perm[1], h->n[1], xkc,
-                                                                    reinterpret_cast<uint4*>(bbuf),
-                                                                    reinterpret_cast<uint4*>(blo));
+    TcParts xp{{reinterpret_cast<__nv_bfloat16*>(op1.b[0]), reinterpret_cast<__nv_bfloat16*>(op1.b[1]),
+                reinterpret_cast<__nv_bfloat16*>(op1.b[2])},
+               PARTS};
+    k_tc_x<NV><<<(unsigned)((xkc * NV + 255) / 256), 256, 0, s>>>(X, ldx, nrhs, h->perm[1], h->n[1], xkc, xp);
     HMG_LAUNCH_CHECK();
     const size_t smem = sizeof(TcSmem);
-    HMG_CUDA_TRY(cudaFuncSetAttribute(k_tc_pass<0, NV, SPLIT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    HMG_CUDA_TRY(cudaFuncSetAttribute(k_tc_pass<1, NV, SPLIT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    HMG_CUDA_TRY(cudaFuncSetAttribute(k_tc_pass<0, NV, PARTS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    HMG_CUDA_TRY(cudaFuncSetAttribute(k_tc_pass<1, NV, PARTS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     if (h->tc_njobs[0] > 0) {
-        k_tc_pass<0, NV, SPLIT><<<h->tc_grid, TC_THREADS, smem, s>>>(
+        k_tc_pass<0, NV, PARTS><<<h->tc_grid, TC_THREADS, smem, s>>>(
             reinterpret_cast<const TcStep*>(h->tc_steps[0]), reinterpret_cast<const TcJob*>(h->tc_jobs[0]),
-            reinterpret_cast<const int2*>(h->tc_cta[0]), static_cast<const char*>(h->tc_v),
-            static_cast<const char*>(h->tc_v_lo), bbuf, blo, xkc, h->tc_kmap, 0, nullptr, 0, 0, h->dev_err);
+            reinterpret_cast<const int2*>(h->tc_cta[0]), op1, xkc, h->tc_kmap, 0, nullptr, 0, 0, h->dev_err);
         HMG_LAUNCH_CHECK();
     }
     if (!h->tc_near && h->ndense > 0) {
@@ -998,41 +1080,40 @@ static hmg_status tc_product(hmg_matrix* h, int nrhs, const double* X, int ldx, 
     }
     const int add_y = !h->tc_near && h->ndense > 0;
     if (h->tc_njobs[1] > 0) {
-        k_tc_pass<1, NV, SPLIT><<<h->tc_grid, TC_THREADS, smem, s>>>(
+        k_tc_pass<1, NV, PARTS><<<h->tc_grid, TC_THREADS, smem, s>>>(
             reinterpret_cast<const TcStep*>(h->tc_steps[1]), reinterpret_cast<const TcJob*>(h->tc_jobs[1]),
-            reinterpret_cast<const int2*>(h->tc_cta[1]), static_cast<const char*>(h->tc_u),
-            static_cast<const char*>(h->tc_u_lo), bbuf, blo, 0, h->perm[0], nrhs, Y, ldy, add_y, h->dev_err);
+            reinterpret_cast<const int2*>(h->tc_cta[1]), op2, 0, h->perm[0], nrhs, Y, ldy, add_y, h->dev_err);
         HMG_LAUNCH_CHECK();
     }
     return HMG_OK;
 }
 
+template <int PARTS>
+static hmg_status tc_product_parts(hmg_matrix* h, int nrhs, const double* X, int ldx, double* Y, int ldy)
+{
+    return nrhs > 32 ? tc_product<64, PARTS>(h, nrhs, X, ldx, Y, ldy) : tc_product<32, PARTS>(h, nrhs, X, ldx, Y, ldy);
+}
+
 // up to 64 vectors in one pass: MMAs of N = 32 for 2..32 vectors, N = 64 for 33..64
 hmg_status matvec_multi_tc(hmg_matrix* h, int nrhs, const double* X, int ldx, double* Y, int ldy)
 {
-    if (!h->tc_bbuf) {  // X and t_b cores, kept with the handle, sized for 64 vectors
-        const size_t bytes = (size_t)(h->tc_xkc + h->tc_tkc) * 16 * TC_NMAX;
-        cudaError_t ce = cudaMalloc(&h->tc_bbuf, bytes);
-        if (ce != cudaSuccess) {
-            cudaGetLastError();
-            h->tc_bbuf = nullptr;
-            set_error("hmg_matvec_multi: allocating %zu bytes of operand space failed: %s", bytes, cudaGetErrorString(ce));
-            return ce == cudaErrorMemoryAllocation ? HMG_ERR_NOMEM : HMG_ERR_CUDA;
+    // X and t_b cores (every part), kept with the handle, sized for 64 vectors
+    const size_t bytes = (size_t)(h->tc_xkc + h->tc_tkc) * 16 * TC_NMAX;
+    void** bufs[3] = {&h->tc_bbuf, &h->tc_bbuf_part[0], &h->tc_bbuf_part[1]};
+    for (int q = 0; q < h->tc_parts; q++)
+        if (!*bufs[q]) {
+            cudaError_t ce = cudaMalloc(bufs[q], bytes);
+            if (ce != cudaSuccess) {
+                cudaGetLastError();
+                *bufs[q] = nullptr;
+                set_error("hmg_matvec_multi: allocating %zu bytes of operand space failed: %s", bytes,
+                          cudaGetErrorString(ce));
+                return ce == cudaErrorMemoryAllocation ? HMG_ERR_NOMEM : HMG_ERR_CUDA;
+            }
         }
-    }
-    if (h->tc_split && !h->tc_bbuf_lo) {
-        const size_t bytes = (size_t)(h->tc_xkc + h->tc_tkc) * 16 * TC_NMAX;
-        cudaError_t ce = cudaMalloc(&h->tc_bbuf_lo, bytes);
-        if (ce != cudaSuccess) {
-            cudaGetLastError();
-            h->tc_bbuf_lo = nullptr;
-            set_error("hmg_matvec_multi: allocating %zu bytes of operand space failed: %s", bytes, cudaGetErrorString(ce));
-            return ce == cudaErrorMemoryAllocation ? HMG_ERR_NOMEM : HMG_ERR_CUDA;
-        }
-    }
-    if (h->tc_split)
-        return nrhs > 32 ? tc_product<64, true>(h, nrhs, X, ldx, Y, ldy) : tc_product<32, true>(h, nrhs, X, ldx, Y, ldy);
-    return nrhs > 32 ? tc_product<64, false>(h, nrhs, X, ldx, Y, ldy) : tc_product<32, false>(h, nrhs, X, ldx, Y, ldy);
+    if (h->tc_parts == 3) return tc_product_parts<3>(h, nrhs, X, ldx, Y, ldy);
+    if (h->tc_parts == 2) return tc_product_parts<2>(h, nrhs, X, ldx, Y, ldy);
+    return tc_product_parts<1>(h, nrhs, X, ldx, Y, ldy);
 }
 
 }  // namespace hmg

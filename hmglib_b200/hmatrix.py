@@ -152,7 +152,8 @@ class HMatrix:
         """BF16 tcgen05 operands of the FP32 factors for tensor-core multi-vector products
         (hmg_build_tensor_core_operands); the near field on the tensor cores too
         (near=PREC_BF16), in FP32 on the CUDA cores (near=PREC_FP32), or every operand
-        as a BF16 hi + lo pair (near=PREC_BF16X3, ~1e-5)."""
+        as a BF16 hi + lo pair (near=PREC_BF16X3, ~5e-6) or as three BF16 parts
+        (near=PREC_BF16X6, 24 bits)."""
         self._call("hmg_build_tensor_core_operands", int(near))
 
     def save(self, path: str):

@@ -52,9 +52,12 @@ typedef enum {
  * is ~1e-7 of the block norm.  hmg_precompute_dense with this value stores FP32. */
 #define HMG_PREC_MIXED 2
 /* Tensor-core operands only (hmg_build_tensor_core_operands): BF16; BF16 pairs hi + lo
- * (16 significant bits, three MMAs per K step: hi*hi + hi*lo + lo*hi) */
+ * (16 significant bits, three MMAs per K step: hi*hi + hi*lo + lo*hi); BF16 triples
+ * hi + lo + lo2 (24 significant bits, six MMAs per K step: hi*hi + hi*lo + lo*hi +
+ * hi*lo2 + lo2*hi + lo*lo) */
 #define HMG_PREC_BF16 3
 #define HMG_PREC_BF16X3 4
+#define HMG_PREC_BF16X6 5
 
 /* near-field mode for hmg_matvec */
 #define HMG_NEAR_STORED 0   /* read the blocks stored by hmg_precompute_dense          */
@@ -144,8 +147,12 @@ hmg_status hmg_full_matvec_rows(hmg_matrix* h, const double* x, const int* rows,
  * there as well (HMG_PREC_BF16) or on the CUDA cores in FP32 (HMG_PREC_FP32).  Results
  * agree with the FP32 products to ~1e-3 (BF16 rounding).  HMG_PREC_BF16X3 keeps every
  * operand, the near field included, as a BF16 pair (hi and the rounding of what hi
- * misses) and multiplies hi*hi + hi*lo + lo*hi: ~1e-5, with twice the operand bytes
- * and three times the MMAs.  Single-vector products keep
+ * misses) and multiplies hi*hi + hi*lo + lo*hi: ~5e-6, with twice the operand bytes
+ * and three times the MMAs.  HMG_PREC_BF16X6 keeps three parts (24 bits, as FP32) and
+ * adds the terms down to 2^-16 of hi*hi: 1.5 times the bytes of X3.  With split
+ * operands hi*hi and the correction terms accumulate apart and every accumulator is
+ * drained after at most 128 K positions; the sums continue in FP32 on the CUDA cores.
+ * Single-vector products keep
  * using the FP32 storage.  Recomputing the factors or the near field drops the copies.
  * hmg_build_bf16_factors(h) is hmg_build_tensor_core_operands(h, HMG_PREC_BF16). */
 hmg_status hmg_build_tensor_core_operands(hmg_matrix* h, int near_precision);
