@@ -13,6 +13,11 @@ over 4,096 rows is reported beside every number (err_vs_fp64).
   value  H-matvecs/s with x and y resident in HBM (device-timed with CUDA events);
   e2e    the same through the host-buffer C-ABI call hmg_matvec_host: x copied
          in from pinned memory and y copied out, every step, inside the timing.
+  multi_rhs  products of 32 vectors a pass on the same H-matrix (hmg_matvec_multi,
+         CUDA cores), vectors per second.
+  batched_tensor_cores  64 vectors a pass on the tensor cores with three-part BF16
+         operands at N=2^18 (error <= 1e-6), beside the plain FP64 form at that size
+         (the FP64 form of N=2^20 does not fit one B200).
 The stored H-matrix (~95 GB mixed) is far larger than L2, so no L2 flush is needed
 between steps.  --impl reference times the FP64 direct product (the reference's
 apply_full_mvp, restated by the CPU oracle) on the host cores on a row sample.
@@ -205,6 +210,91 @@ def multi_rhs_timing(torch, H, x, n, nrhs, steps, stream, world, err1):
             "err_vs_fp64_col0": err1 + diff, "col0_vs_single": diff}
 
 
+def batched_tensor_cores(steps):
+    """Batched products on the tensor cores at error <= 1e-6 beside the plain FP64 form,
+    at N = 2^18 points of this workload: the largest power of two at which the FP32
+    storage and its three-part BF16 operand copy fit one B200 together.  FP32 factors
+    and near field, converted to three-part BF16 operands (HMG_PREC_BF16X6), 64 vectors
+    a pass (x ~ U[-1,1], seed 11); the plain FP64 form (FP64 factors, near field and
+    products, the reference's arithmetic) one vector at a time on the same H-matrix
+    structure.  Errors: the largest over 4 vectors of the relative error against FP64
+    direct sums over 4,096 rows.  Device-timed with CUDA events; e2e copies X in from
+    pinned host memory and Y out, every step."""
+    import torch
+
+    import hmglib_b200 as hmg
+    from hmglib_b200 import synth
+    W = WORKLOAD
+    n, nrhs = 1 << 18, 64
+    p = synth.uniform_points(n, W["dim"], W["seed"])
+    Xh = np.random.default_rng(11).uniform(-1, 1, (nrhs, n))
+    X = torch.from_numpy(Xh).cuda()
+    rows = torch.from_numpy(np.random.default_rng(7).choice(n, 4096, replace=False).astype(np.int32)).cuda()
+    stream = torch.cuda.default_stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+    def build(prec):
+        H = hmg.HMatrix(n, n, W["dim"])
+        H.set_points(0, p)
+        H.set_points(1, p)
+        H.setup(W["eta"], W["leaf"], rule=hmg.ADMISSIBLE_MIN)
+        H.set_kernel(hmg.KERNEL_MATERN32, W["rho"], 0.0)
+        H.precompute_aca(W["max_rank"], W["aca_eps"], prec)
+        H.precompute_dense(prec)
+        return H
+
+    def timed(fn):
+        for _ in range(3):
+            fn()
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for _ in range(steps):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / steps
+
+    def max_error(H, Y, cols):
+        yd = torch.empty(rows.shape[0], dtype=torch.float64, device="cuda")
+        worst = 0.0
+        for j in cols:
+            H.full_matvec_rows(X[j], rows, yd)
+            torch.cuda.synchronize()
+            worst = max(worst, float(torch.linalg.norm(Y[j][rows.long()] - yd) / torch.linalg.norm(yd)))
+        return worst
+
+    out = {"n": n, "nrhs": nrhs, "operands": "BF16 x3 parts (HMG_PREC_BF16X6)"}
+    H = build(hmg.PREC_FP32)
+    H.build_bf16_factors(near=hmg.PREC_BF16X6)
+    info = H.info()
+    Y = torch.empty_like(X)
+    with ClockSampler(torch.cuda.current_device()) as clk:
+        ms = timed(lambda: H.matvec_multi(X, Y))
+        Xp = torch.from_numpy(Xh).pin_memory()
+        Yp = torch.empty(Xh.shape, dtype=torch.float64).pin_memory()
+
+        def e2e_step():
+            X.copy_(Xp, non_blocking=True)
+            H.matvec_multi(X, Y)
+            Yp.copy_(Y, non_blocking=True)
+        ms_e2e = timed(e2e_step)
+    out.update({"ms_per_product": ms, "value": nrhs * 1000.0 / ms, "unit": "vector products/s",
+                "e2e_value": nrhs * 1000.0 / ms_e2e, "err_vs_fp64": max_error(H, Y, [0, 1, 31, 63]),
+                "operand_bytes": info["tc_bytes"], "fp32_storage_bytes": info["far_bytes"] + info["near_bytes"],
+                "clocks": clk.summary()})
+    H.close()
+    G = build(hmg.PREC_FP64)
+    y = torch.empty(n, dtype=torch.float64, device="cuda")
+    ms64 = timed(lambda: G.matvec(X[0], y))
+    gi = G.info()
+    out["fp64_form"] = {"ms_per_product": ms64, "value": 1000.0 / ms64, "unit": "vector products/s",
+                        "err_vs_fp64": max_error(G, y.unsqueeze(0), [0]),
+                        "storage_bytes": gi["far_bytes"] + gi["near_bytes"]}
+    G.close()
+    out["speedup_vs_fp64_form"] = out["value"] / out["fp64_form"]["value"]
+    return out
+
+
 def run_engine(a, rank, world):
     import torch
     import torch.distributed as dist
@@ -375,6 +465,8 @@ def run_engine(a, rank, world):
         line["cpu_baseline"] = {"value": rate / n, "unit": "matvec/s", "cores": thr, "kind": "port",
                                 "sample": f"FP64 direct sum over {nrows} random rows ({dt:.1f} s), scaled to N={n}"}
     H.close()
+    if world == 1 and not a.no_batched_tc:
+        line["batched_tensor_cores"] = batched_tensor_cores(a.steps)
     if rank == 0:
         print(json.dumps(line), flush=True)
     return 0
@@ -783,7 +875,7 @@ def main(argv=None):
     ap.add_argument("--n", type=int, default=0, help="override the point count (default 2^20)")
     ap.add_argument("--prec", default="mixed", choices=["fp32", "fp64", "mixed"])
     ap.add_argument("--near", default="stored", choices=["stored", "onthefly"])
-    ap.add_argument("--nrhs", type=int, default=1,
+    ap.add_argument("--nrhs", type=int, default=32,
                     help="also time products of this many vectors at once (hmg_matvec_multi)")
     ap.add_argument("--tc-mode", default="all", choices=["all", "bf16", "near-fp32", "bf16x3", "bf16x6"],
                     help="tensor-core operand modes --tc measures")
@@ -805,6 +897,8 @@ def main(argv=None):
     ap.add_argument("--group-count", type=int, default=512)
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-batched-tc", action="store_true",
+                    help="skip the tensor-core batched products at N=2^18 beside the FP64 form")
     a = ap.parse_args(argv)
     a.warmup = max(3, a.warmup)
     rank = int(os.environ.get("RANK", "0"))

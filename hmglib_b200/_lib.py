@@ -45,7 +45,7 @@ class Info(C.Structure):
                 ("near_bytes", C.c_int64), ("far_bytes", C.c_int64), ("matvec_bytes", C.c_int64),
                 ("near_precision", C.c_int), ("far_precision", C.c_int), ("near_mode", C.c_int),
                 ("far_u_bytes", C.c_int64), ("far_v_bytes", C.c_int64), ("matvec_launches", C.c_int),
-                ("group_count", C.c_int)]
+                ("group_count", C.c_int), ("tc_parts", C.c_int), ("tc_bytes", C.c_int64)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}

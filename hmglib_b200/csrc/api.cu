@@ -26,7 +26,7 @@ extern "C" {
 
 const char* hmg_last_error(void) { return hmg::last_error(); }
 
-int hmg_version(void) { return 100; }
+int hmg_version(void) { return 101; }
 
 static void free_matrix_buffers(hmg_matrix* h)
 {
@@ -481,6 +481,8 @@ hmg_status hmg_get_info(hmg_matrix* h, hmg_info* info)
         }
     info->matvec_launches = 1 + (int)tier[0] + (int)tier[1] + (int)tier[2] + (h->ntiles > 0 ? 1 : 0);
     info->group_count = h->group_count;
+    info->tc_parts = h->tc_ready ? h->tc_parts : 0;
+    info->tc_bytes = h->tc_ready ? h->tc_bytes * h->tc_parts : 0;
     info->far_u_bytes = h->far_alg_u;
     info->far_v_bytes = h->far_alg_v;
     if (h->near_mode == HMG_NEAR_STORED && h->near_prec >= 0) mb += ne * nes;

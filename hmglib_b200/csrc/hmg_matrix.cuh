@@ -102,7 +102,7 @@ struct hmg_matrix {
     bool tc_all_tiles = false;                // every row tile has a pass-2 job
     bool tc_near = false;                     // near field on the tensor cores (else FP32 CUDA cores)
     long long tc_xkc = 0, tc_tkc = 0;         // per product: K cores of X, of t_b (8 columns / terms each)
-    long long tc_bytes = 0;                   // BF16 operands held
+    long long tc_bytes = 0;                   // bytes of one part of the BF16 operands
 
     // ---- matvec workspace -------------------------------------------------------
     double* xs64 = nullptr;   // Z-ordered x

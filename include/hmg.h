@@ -79,6 +79,8 @@ typedef struct {
     int64_t far_v_bytes;      /* bytes of the stored V terms */
     int matvec_launches;      /* kernels one hmg_matvec launches (plain-load kernels) */
     int group_count;          /* sets of a group handle (hmg_group_create), else 0 */
+    int tc_parts;             /* BF16 parts per tensor-core operand (0: none built) */
+    int64_t tc_bytes;         /* bytes of the tensor-core operands, all parts */
 } hmg_info;
 
 /* message of the last failed call on this thread ("" if none) */
