@@ -37,6 +37,30 @@ def test_every_declared_symbol_is_exported(hmg):
         getattr(L, name)
 
 
+def test_constants_and_info_match_the_header(hmg):
+    """The binding's constants and its hmg_info layout are those of include/hmg.h."""
+    from hmglib_b200 import _lib as L
+    src = open(os.path.join(ROOT, "include", "hmg.h")).read()
+    defines = dict(re.findall(r"^#define (HMG_[A-Z0-9_]+) (-?\d+)\b", src, re.M))
+    checked = 0
+    for name, value in defines.items():
+        short = name[len("HMG_"):]
+        if hasattr(L, short):
+            assert getattr(L, short) == int(value), name
+            checked += 1
+    assert checked >= 10
+    body = re.search(r"typedef struct \{(.*?)\} hmg_info;", src, re.S).group(1)
+    body = re.sub(r"/\*.*?\*/", "", body, flags=re.S)
+    fields = []
+    for decl in body.split(";"):
+        decl = decl.strip()
+        if decl:
+            ctype, names = decl.split(None, 1)
+            fields += [(n.strip(), ctype) for n in names.split(",")]
+    ctypes_of = {"int": C.c_int, "int64_t": C.c_int64}
+    assert [(n, ctypes_of[t]) for n, t in fields] == list(L.Info._fields_)
+
+
 def test_argument_errors_need_no_gpu(hmg):
     L = hmg.lib()
     h = C.c_void_p()
