@@ -89,10 +89,7 @@ struct hmg_matrix {
     void* tc_u = nullptr;                     // pass 2 A operands: U slices, near slices
     void* tc_v = nullptr;                     // pass 1 A operands: V_b^T
     void* tc_bbuf = nullptr;                  // per product: X cores, then t_b cores
-    void* tc_u_part[2] = {nullptr, nullptr};  // split operands: the further BF16 parts of
-    void* tc_v_part[2] = {nullptr, nullptr};  // tc_u, tc_v and tc_bbuf (what the parts before
-    void* tc_bbuf_part[2] = {nullptr, nullptr};  // them miss, rounded to BF16)
-    int tc_parts = 1;                         // BF16 parts per operand: 1, 2 (hi + lo) or 3
+    int tc_parts = 1;                         // BF16 parts per operand (1, 2 or 3), interleaved by K core
     char* tc_steps[2] = {nullptr, nullptr};   // per pass: steps, CTA by CTA
     char* tc_jobs[2] = {nullptr, nullptr};    // per pass: jobs, CTA by CTA
     char* tc_cta[2] = {nullptr, nullptr};     // per CTA: first job and step (int2), then the ends

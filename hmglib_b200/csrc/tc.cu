@@ -85,28 +85,28 @@ struct TcJob {
 // ---------------------------------------------------------------------------
 // conversion of the FP32 factors and near field (once, by hmg_build_bf16_factors)
 // ---------------------------------------------------------------------------
-// Destinations of an operand's BF16 parts: part 0 is the BF16 rounding of a value, part
-// p the BF16 rounding of what parts 0..p-1 miss (each difference is exact in FP32), so
-// that 1, 2 or 3 parts carry 8, 16 or 24 significant bits of it.
-struct TcParts {
-    __nv_bfloat16* p[3];
-    int n;
-};
-
-__device__ __forceinline__ void store_parts(const TcParts& out, long long base, size_t i, float v)
+// An operand's BF16 parts: part 0 is the BF16 rounding of a value, part p the BF16
+// rounding of what parts 0..p-1 miss (each difference is exact in FP32), so that 1, 2
+// or 3 parts carry 8, 16 or 24 significant bits of it.  The parts are interleaved by K
+// core: K core kc of an operand with rc row cores holds part 0's rc cores, then part
+// 1's, then part 2's, so that one copy brings every part of a K range.  Element
+// `within` (core mc * 64 + position) of K core kc, part q, sits at
+// base + ((kc * parts + q) * rc) * 64 + within.
+__device__ __forceinline__ void store_parts(__nv_bfloat16* out, int parts, long long base, long long kc, int rc,
+                                            int within, float v)
 {
 #pragma unroll
     for (int q = 0; q < 3; q++)
-        if (q < out.n) {
+        if (q < parts) {
             const __nv_bfloat16 h = __float2bfloat16_rn(v);
-            out.p[q][base + i] = h;
+            out[base + ((kc * parts + q) * rc) * 64 + within] = h;
             v -= __bfloat162float(h);
         }
 }
 
 // far pair: U slice (s_pad x r, column-major) -> A cores, rc = s8 / 8, K = r16
 __global__ void k_tc_u(const PairDesc* desc, const int* plist, const long long* aoff, const int* ptile,
-                       const int* tile_s, int n, TcParts out)
+                       const int* tile_s, int n, __nv_bfloat16* out, int parts)
 {
     const int u = blockIdx.x;
     if (u >= n) return;
@@ -121,13 +121,13 @@ __global__ void k_tc_u(const PairDesc* desc, const int* plist, const long long* 
         const int core = idx >> 6, e = idx & 63;
         const int kc = core / rc, mc = core - kc * rc;
         const int i = mc * 8 + (e >> 3), k = kc * 8 + (e & 7);
-        store_parts(out, base, idx, (i < s && k < r) ? src[(size_t)k * sp + i] : 0.0f);
+        store_parts(out, parts, base, kc, rc, mc * 64 + e, (i < s && k < r) ? src[(size_t)k * sp + i] : 0.0f);
     }
 }
 
 // near pair: slice (s_pad x m2, column-major) -> A cores with c0 mod 8 leading zero columns
 __global__ void k_tc_near(const PairDesc* desc, const int* plist, const long long* aoff, const int* ptile,
-                          const int* tile_s, int n, TcParts out)
+                          const int* tile_s, int n, __nv_bfloat16* out, int parts)
 {
     const int u = blockIdx.x;
     if (u >= n) return;
@@ -141,7 +141,7 @@ __global__ void k_tc_near(const PairDesc* desc, const int* plist, const long lon
         const int core = (int)(idx >> 6), e = (int)(idx & 63);
         const int kc = core / rc, mc = core - kc * rc;
         const int i = mc * 8 + (e >> 3), c = kc * 8 + (e & 7) - a;
-        store_parts(out, base, idx, (i < s && c >= 0 && c < m2) ? src[(size_t)c * sp + i] : 0.0f);
+        store_parts(out, parts, base, kc, rc, mc * 64 + e, (i < s && c >= 0 && c < m2) ? src[(size_t)c * sp + i] : 0.0f);
     }
 }
 
@@ -149,7 +149,7 @@ __global__ void k_tc_near(const PairDesc* desc, const int* plist, const long lon
 // cores.  A stack holds the V^T of blocks with the same columns, one under the other
 // (vaux: stack row cores << 8 | the block's first row core in the stack).
 __global__ void k_tc_v(const int* blist, const long long* voff, const int* vaux, int n, void* const* ptrV,
-                       const int* rank, const int* blk_c0, const int* blk_m2, TcParts out)
+                       const int* rank, const int* blk_c0, const int* blk_m2, __nv_bfloat16* out, int parts)
 {
     const int u = blockIdx.x;
     if (u >= n) return;
@@ -163,7 +163,7 @@ __global__ void k_tc_v(const int* blist, const long long* voff, const int* vaux,
         const int core = (int)(idx >> 6), e = (int)(idx & 63);
         const int kc = core / rb, mc = core - kc * rb;
         const int m = mc * 8 + (e >> 3), c = kc * 8 + (e & 7) - a;
-        store_parts(out, base, ((size_t)kc * rc + off8 + mc) * 64 + e,
+        store_parts(out, parts, base, kc, rc, (off8 + mc) * 64 + e,
                     (m < r && c >= 0 && c < m2) ? V[(size_t)m * m2p + c] : 0.0f);
     }
 }
@@ -171,10 +171,11 @@ __global__ void k_tc_v(const int* blist, const long long* voff, const int* vaux,
 // ---------------------------------------------------------------------------
 // per product: X -> BF16 cores (Z-ordered columns), FP32 rows -> Y
 // ---------------------------------------------------------------------------
-// thread (g, j): columns 8g..8g+7 of vector j, one 16-byte row of K core g
+// thread (g, j): columns 8g..8g+7 of vector j, one 16-byte row of K core g in each part
+// (K core g holds its parts one after another, NV * 16 bytes each)
 template <int NV>
 __global__ void k_tc_x(const double* __restrict__ X, int ldx, int nrhs, const int* __restrict__ perm1, int n,
-                       long long ngroups, TcParts xb)
+                       long long ngroups, uint4* xb, int parts)
 {
     const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (idx >= ngroups * NV) return;
@@ -188,14 +189,14 @@ __global__ void k_tc_x(const double* __restrict__ X, int ldx, int nrhs, const in
     }
 #pragma unroll
     for (int q = 0; q < 3; q++)
-        if (q < xb.n) {
+        if (q < parts) {
             __nv_bfloat16 v[8];
 #pragma unroll
             for (int e = 0; e < 8; e++) {
                 v[e] = __float2bfloat16_rn(f[e]);
                 f[e] -= __bfloat162float(v[e]);
             }
-            reinterpret_cast<uint4*>(xb.p[q])[(g * (NV / 8) + (j >> 3)) * 8 + (j & 7)] = *reinterpret_cast<const uint4*>(v);
+            xb[(g * parts + q) * NV + j] = *reinterpret_cast<const uint4*>(v);
         }
 }
 
@@ -302,21 +303,17 @@ __device__ __forceinline__ uint32_t pack_bf16(float lo, float hi)
 // pass (MMA N); B K cores are NV * 16 bytes.  Pass 1 (MODE 0) writes t_b cores, K core kc of
 // job j (a stack) to B K core tb_kc + map[16 j + kc]; pass 2 (MODE 1) writes (add_y: adds
 // to) rows of Y, tile row i to Y row map[r0 + i].  PARTS > 1 (split operands): every
-// operand comes as PARTS BF16 parts of the same layout (A.p[q], B.p[q]); a step brings
-// the A parts, then the B parts, and each K step runs hi*hi plus the correction terms
-// down to 2^-16 of it: hi*lo + lo*hi (2 parts), and hi*lo2 + lo2*hi + lo*lo (3 parts).
-struct TcOperands {
-    const char* a[3];  // A arena, per part
-    char* b[3];        // B buffer (X cores, then t_b cores), per part
-};
-
+// operand comes as PARTS BF16 parts interleaved by K core (A: a step's row cores field
+// counts the row cores of all parts; B: a K core is PARTS * NV * 16 bytes), and each K
+// step runs hi*hi plus the correction terms down to 2^-16 of it: hi*lo + lo*hi (2
+// parts), and hi*lo2 + lo2*hi + lo*lo (3 parts).
 template <int MODE, int NV, int PARTS>
 __global__ void __launch_bounds__(TC_THREADS, 1)
     k_tc_pass(const TcStep* __restrict__ steps, const TcJob* __restrict__ jobs, const int2* __restrict__ cta,
-              const TcOperands op, long long tb_kc, const int* __restrict__ map, int nrhs, double* Y, int ldy,
-              int add_y, int* err)
+              const char* __restrict__ A, char* Bbuf, long long tb_kc, const int* __restrict__ map, int nrhs,
+              double* Y, int ldy, int add_y, int* err)
 {
-    constexpr int KB = NV * 16;
+    constexpr int KB = NV * 16 * PARTS;  // bytes of a B K core, all parts
     constexpr bool SPLIT = PARTS > 1;
     // two accumulator buffers; split: each holds hi*hi (columns 0..NV-1) and the
     // correction terms (NV..2NV-1)
@@ -368,7 +365,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
             const int ks_all = (mine.meta >> 16) & 0xff;
             const int ab = ks_all * 2 * (mine.meta & 0xff) * 128, bb = ks_all * 2 * KB;
             __syncwarp();
-            sm.step_bytes[lane] = PARTS * (ab + bb);
+            sm.step_bytes[lane] = ab + bb;
             __syncwarp();
             for (int k = 0; k < cnt && ok;) {
                 int m = 0;
@@ -412,23 +409,18 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                 if (lane >= k && lane < k + m) {
                     const int slot = (i0 + lane) % TC_SLOTS, pos = sm.slot_pos[slot];
                     const uint32_t a = smem_u32(sm.ring + pos);
-                    const int a_span = PARTS * ab;  // the A parts, then the B parts
                     sm.slot_a[slot] = a;
-                    sm.slot_b[slot] = a + a_span;
+                    sm.slot_b[slot] = a + ab;
                     sm.slot_meta[slot] = mine.meta;
-                    mbar_arrive_expect_tx(&sm.full[slot], PARTS * (ab + bb));
-#pragma unroll
-                    for (int q = 0; q < PARTS; q++)
-                        bulk_g2s_first(sm.ring + pos + q * ab, op.a[q] + mine.a_off, ab, &sm.full[slot], pol);
+                    mbar_arrive_expect_tx(&sm.full[slot], ab + bb);
+                    bulk_g2s_first(sm.ring + pos, A + mine.a_off, ab, &sm.full[slot], pol);
                     const int nsub = ((mine.meta >> 10) & 3) + 1;
-                    int boff = a_span;
+                    int boff = ab;
 #pragma unroll
                     for (int j = 0; j < TC_MAXSUB; j++)
                         if (j < nsub) {
                             const int kb = (((mine.kss >> (4 * j)) & 15) + 1) * 2 * KB;
-#pragma unroll
-                            for (int q = 0; q < PARTS; q++)
-                                bulk_g2s(sm.ring + pos + boff + q * bb, op.b[q] + mine.b_off[j] * KB, kb, &sm.full[slot]);
+                            bulk_g2s(sm.ring + pos + boff, Bbuf + mine.b_off[j] * KB, kb, &sm.full[slot]);
                             boff += kb;
                         }
                 }
@@ -473,8 +465,9 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                 const uint32_t d = tmem + (uint32_t)(buf * (SPLIT ? 2 * NV : NV));
                 const uint64_t da = (2 * lbo) >> 4, db = (2 * KB) >> 4;
                 uint64_t ad = smem_desc(a0, lbo, 128), bd = smem_desc(b0, KB, 128);
-                // part q of A (of B) lies q * alo (q * blo) 16-byte units after part 0
-                const uint64_t alo = (uint64_t)(ks_all * 2 * lbo) >> 4, blo = (uint64_t)(ks_all * 2 * KB) >> 4;
+                // in each K core, part q of A (of B) lies q * alo (q * blo) 16-byte units
+                // after part 0: the row cores of one part (the vector cores of one part)
+                const uint64_t alo = (uint64_t)((meta & 0xff) / PARTS) * 8, blo = (uint64_t)NV;
                 uint32_t acc = (SPLIT || first) ? 0u : 1u;
 #pragma unroll 4
                 for (int q = 0; q < ks_all; q++) {
@@ -541,13 +534,13 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                         stg[(u ^ ((lane >> 3) * 2)) * 4 + ((lane & 7) >> 1)] = w;
                     }
                     __syncwarp();
-                    uint4* dst = reinterpret_cast<uint4*>(op.b[part]);
+                    uint4* dst = reinterpret_cast<uint4*>(Bbuf);
                     const uint4* src = reinterpret_cast<const uint4*>(stg);
 #pragma unroll
                     for (int it = 0; it < NV / 8; it++) {
                         const int u = it * 32 + lane, kcl = u / NV;
                         if (warp * 4 + kcl < (rows >> 3))
-                            dst[(size_t)(tb_kc + tdst[kcl]) * (KB / 16) + (u % NV)] = src[u ^ (kcl * 2)];
+                            dst[((size_t)(tb_kc + tdst[kcl]) * PARTS + part) * NV + (u % NV)] = src[u ^ (kcl * 2)];
                     }
                     __syncwarp();
                 }
@@ -642,14 +635,9 @@ void free_tc(hmg_matrix* h)
     cudaStream_t s = h->stream;
     if (h->tc_u) cudaFree(h->tc_u);
     if (h->tc_v) cudaFree(h->tc_v);
-    if (h->tc_bbuf || h->tc_bbuf_part[0] || h->tc_bbuf_part[1])
-        cudaStreamSynchronize(s);  // a product in flight may still read them
-    if (h->tc_bbuf) cudaFree(h->tc_bbuf);
-    for (int q = 0; q < 2; q++) {
-        if (h->tc_u_part[q]) cudaFree(h->tc_u_part[q]);
-        if (h->tc_v_part[q]) cudaFree(h->tc_v_part[q]);
-        if (h->tc_bbuf_part[q]) cudaFree(h->tc_bbuf_part[q]);
-        h->tc_u_part[q] = h->tc_v_part[q] = h->tc_bbuf_part[q] = nullptr;
+    if (h->tc_bbuf) {
+        cudaStreamSynchronize(s);  // a product in flight may still read it
+        cudaFree(h->tc_bbuf);
     }
     h->tc_u = h->tc_v = h->tc_bbuf = nullptr;
     dfree(h->tc_kmap, s);
@@ -747,14 +735,15 @@ bool steps_in_bounds(const JobList& L, long long abytes, long long bkcores, long
 {
     for (const TcStep& st : L.steps) {
         const int rc = st.meta & 0xff, nsub = ((st.meta >> 10) & 3) + 1, ks_all = (st.meta >> 16) & 0xff;
-        const long long ab = (long long)ks_all * 2 * rc * 128, bb = (long long)ks_all * 2 * 16 * TC_NMAX;
+        // rc counts the row cores of all parts; a B K core holds every part
+        const long long ab = (long long)ks_all * 2 * rc * 128, bb = (long long)ks_all * 2 * 16 * TC_NMAX * parts;
         int sum = 0;
         for (int j = 0; j < nsub; j++) {
             const int ks = ((st.kss >> (4 * j)) & 15) + 1;
             if (st.b_off[j] < 0 || st.b_off[j] + 2ll * ks > bkcores) return false;
             sum += ks;
         }
-        if (sum != ks_all || rc < 1 || rc > 16 || parts * ab > TC_ABYTES || parts * bb > TC_BBYTES ||
+        if (sum != ks_all || rc < 1 || rc > 16 * parts || rc % parts || ab > TC_ABYTES || bb > TC_BBYTES ||
             st.a_off < 0 || st.a_off % 16 ||
             st.a_off + ab > abytes)
             return false;
@@ -859,7 +848,9 @@ hmg_status build_bf16_factors(hmg_matrix* h, bool near_tc, int parts)
 
     // B buffer of a product, in K cores: X (8 columns each), then t_b (16 terms = 2 K cores per group)
     const long long xkc = (h->n[1] + 7) / 8 + 4;
-    // split operands bring every part of a chunk: 1 / parts of the A bytes and MMAs per step
+    // Split operands: the parts of a K core lie together (A: parts * rc row cores per K
+    // core, B: parts * NV * 16 bytes per K core), so a chunk of K cores brings every part;
+    // 1 / parts of the K cores and MMAs per step
     const long long a_half = TC_ABYTES / parts;
     const int ks_limit = TC_MAXSTEP / parts;
     std::vector<long long> toff(nb, -1);
@@ -911,9 +902,9 @@ hmg_status build_bf16_factors(hmg_matrix* h, bool near_tc, int parts)
                     off8 += r16 / 8;
                 }
                 k1.begin(TcJob{job, rows});
-                k1.add(vbytes, c0 >> 3, rc, kw / 8, std::min(2 * ks_limit, (int)(a_half / 128 / rc) & ~1),
-                       0.25);
-                vbytes += (long long)rows * kw * 2;
+                k1.add(vbytes, c0 >> 3, rc * parts, kw / 8, std::min(2 * ks_limit, (int)(a_half / 128 / rc) & ~1),
+                       0.25 * parts);
+                vbytes += (long long)rows * kw * 2 * parts;
             }
             g0 = g1;
         }
@@ -939,22 +930,22 @@ hmg_status build_bf16_factors(hmg_matrix* h, bool near_tc, int parts)
                 nlist.push_back(p);
                 ntile.push_back(t);
                 noff.push_back(ubytes);
-                k2.add(ubytes, h->h_c0[b] >> 3, rc, kw / 8, (int)(a_half / 128 / 16), 0.25);
-                ubytes += (long long)rc * 8 * kw * 2;
+                k2.add(ubytes, h->h_c0[b] >> 3, rc * parts, kw / 8, (int)(a_half / 128 / 16), 0.25 * parts);
+                ubytes += (long long)rc * 8 * kw * 2 * parts;
             } else {
                 const int r16 = (h->h_rank[b] + 15) & ~15;
                 ulist.push_back(p);
                 utile.push_back(t);
                 uoff.push_back(ubytes);
-                k2.add(ubytes, xkc + toff[b] * 2, rc, r16 / 8, (int)(a_half / 128 / 16), 1.0);
-                ubytes += (long long)rc * 8 * r16 * 2;
+                k2.add(ubytes, xkc + toff[b] * 2, rc * parts, r16 / 8, (int)(a_half / 128 / 16), 1.0 * parts);
+                ubytes += (long long)rc * 8 * r16 * 2 * parts;
             }
         }
         all_tiles = all_tiles && started;
     }
 
-    k1.make_steps(false, a_half, ks_limit);
-    k2.make_steps(true, a_half, ks_limit);
+    k1.make_steps(false, TC_ABYTES, ks_limit);
+    k2.make_steps(true, TC_ABYTES, ks_limit);
     if (!steps_in_bounds(k1, vbytes, xkc + tgroups * 2, (long long)kmap.size() / 16, 0, parts) ||
         !steps_in_bounds(k2, ubytes, xkc + tgroups * 2, h->n[0], 1, parts)) {
         set_error("hmg_build_bf16_factors: internal error: an operand step leaves its buffer");
@@ -976,12 +967,6 @@ hmg_status build_bf16_factors(hmg_matrix* h, bool near_tc, int parts)
         free_tc(h);
         return st;
     }
-    for (int q = 0; q + 1 < parts; q++)
-        if ((st = alloc_arena(&h->tc_u_part[q], ubytes, "the tile operands' further parts")) ||
-            (st = alloc_arena(&h->tc_v_part[q], vbytes, "the V^T operands' further parts"))) {
-            free_tc(h);
-            return st;
-        }
     int* dlist = nullptr;
     int* dtile = nullptr;
     long long* doff = nullptr;
@@ -998,18 +983,14 @@ hmg_status build_bf16_factors(hmg_matrix* h, bool near_tc, int parts)
         if (!tiles.empty())
             HMG_CUDA_TRY(cudaMemcpyAsync(dtile, tiles.data(), sizeof(int) * n, cudaMemcpyHostToDevice, s));
         const PairDesc* desc = static_cast<const PairDesc*>(h->pair_desc);
-        TcParts up{{static_cast<__nv_bfloat16*>(h->tc_u), static_cast<__nv_bfloat16*>(h->tc_u_part[0]),
-                    static_cast<__nv_bfloat16*>(h->tc_u_part[1])},
-                   parts};
-        TcParts vp{{static_cast<__nv_bfloat16*>(h->tc_v), static_cast<__nv_bfloat16*>(h->tc_v_part[0]),
-                    static_cast<__nv_bfloat16*>(h->tc_v_part[1])},
-                   parts};
+        __nv_bfloat16* up = static_cast<__nv_bfloat16*>(h->tc_u);
+        __nv_bfloat16* vp = static_cast<__nv_bfloat16*>(h->tc_v);
         if (which == 0)
-            k_tc_u<<<n, 256, 0, s>>>(desc, dlist, doff, dtile, h->tile_s, n, up);
+            k_tc_u<<<n, 256, 0, s>>>(desc, dlist, doff, dtile, h->tile_s, n, up, parts);
         else if (which == 1)
-            k_tc_near<<<n, 256, 0, s>>>(desc, dlist, doff, dtile, h->tile_s, n, up);
+            k_tc_near<<<n, 256, 0, s>>>(desc, dlist, doff, dtile, h->tile_s, n, up, parts);
         else
-            k_tc_v<<<n, 256, 0, s>>>(dlist, doff, dtile, n, h->ptrV, h->rank, h->blk_c0, h->blk_m2, vp);
+            k_tc_v<<<n, 256, 0, s>>>(dlist, doff, dtile, n, h->ptrV, h->rank, h->blk_c0, h->blk_m2, vp, parts);
         HMG_LAUNCH_CHECK();
         HMG_CUDA_TRY(cudaStreamSynchronize(s));
         dfree(dlist, s);
@@ -1028,7 +1009,7 @@ hmg_status build_bf16_factors(hmg_matrix* h, bool near_tc, int parts)
         free_tc(h);
         return st;
     }
-    h->tc_bytes = ubytes + vbytes;
+    h->tc_bytes = (ubytes + vbytes) / parts;
     h->tc_xkc = xkc;
     h->tc_tkc = tgroups * 2;
     h->tc_grid = grid;
@@ -1044,19 +1025,10 @@ static hmg_status tc_product(hmg_matrix* h, int nrhs, const double* X, int ldx, 
 {
     cudaStream_t s = h->stream;
     hmg_status st;
-    TcOperands op1{{static_cast<const char*>(h->tc_v), static_cast<const char*>(h->tc_v_part[0]),
-                    static_cast<const char*>(h->tc_v_part[1])},
-                   {static_cast<char*>(h->tc_bbuf), static_cast<char*>(h->tc_bbuf_part[0]),
-                    static_cast<char*>(h->tc_bbuf_part[1])}};
-    TcOperands op2 = op1;
-    op2.a[0] = static_cast<const char*>(h->tc_u);
-    op2.a[1] = static_cast<const char*>(h->tc_u_part[0]);
-    op2.a[2] = static_cast<const char*>(h->tc_u_part[1]);
+    char* bbuf = static_cast<char*>(h->tc_bbuf);
     const long long xkc = h->tc_xkc;
-    TcParts xp{{reinterpret_cast<__nv_bfloat16*>(op1.b[0]), reinterpret_cast<__nv_bfloat16*>(op1.b[1]),
-                reinterpret_cast<__nv_bfloat16*>(op1.b[2])},
-               PARTS};
-    k_tc_x<NV><<<(unsigned)((xkc * NV + 255) / 256), 256, 0, s>>>(X, ldx, nrhs, h->perm[1], h->n[1], xkc, xp);
+    k_tc_x<NV><<<(unsigned)((xkc * NV + 255) / 256), 256, 0, s>>>(X, ldx, nrhs, h->perm[1], h->n[1], xkc,
+                                                                    reinterpret_cast<uint4*>(bbuf), PARTS);
     HMG_LAUNCH_CHECK();
     const size_t smem = sizeof(TcSmem);
     HMG_CUDA_TRY(cudaFuncSetAttribute(k_tc_pass<0, NV, PARTS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
@@ -1064,7 +1036,8 @@ static hmg_status tc_product(hmg_matrix* h, int nrhs, const double* X, int ldx, 
     if (h->tc_njobs[0] > 0) {
         k_tc_pass<0, NV, PARTS><<<h->tc_grid, TC_THREADS, smem, s>>>(
             reinterpret_cast<const TcStep*>(h->tc_steps[0]), reinterpret_cast<const TcJob*>(h->tc_jobs[0]),
-            reinterpret_cast<const int2*>(h->tc_cta[0]), op1, xkc, h->tc_kmap, 0, nullptr, 0, 0, h->dev_err);
+            reinterpret_cast<const int2*>(h->tc_cta[0]), static_cast<const char*>(h->tc_v), bbuf, xkc, h->tc_kmap, 0,
+            nullptr, 0, 0, h->dev_err);
         HMG_LAUNCH_CHECK();
     }
     if (!h->tc_near && h->ndense > 0) {
@@ -1085,7 +1058,8 @@ static hmg_status tc_product(hmg_matrix* h, int nrhs, const double* X, int ldx, 
     if (h->tc_njobs[1] > 0) {
         k_tc_pass<1, NV, PARTS><<<h->tc_grid, TC_THREADS, smem, s>>>(
             reinterpret_cast<const TcStep*>(h->tc_steps[1]), reinterpret_cast<const TcJob*>(h->tc_jobs[1]),
-            reinterpret_cast<const int2*>(h->tc_cta[1]), op2, 0, h->perm[0], nrhs, Y, ldy, add_y, h->dev_err);
+            reinterpret_cast<const int2*>(h->tc_cta[1]), static_cast<const char*>(h->tc_u), bbuf, 0, h->perm[0], nrhs, Y,
+            ldy, add_y, h->dev_err);
         HMG_LAUNCH_CHECK();
     }
     return HMG_OK;
@@ -1101,19 +1075,16 @@ static hmg_status tc_product_parts(hmg_matrix* h, int nrhs, const double* X, int
 hmg_status matvec_multi_tc(hmg_matrix* h, int nrhs, const double* X, int ldx, double* Y, int ldy)
 {
     // X and t_b cores (every part), kept with the handle, sized for 64 vectors
-    const size_t bytes = (size_t)(h->tc_xkc + h->tc_tkc) * 16 * TC_NMAX;
-    void** bufs[3] = {&h->tc_bbuf, &h->tc_bbuf_part[0], &h->tc_bbuf_part[1]};
-    for (int q = 0; q < h->tc_parts; q++)
-        if (!*bufs[q]) {
-            cudaError_t ce = cudaMalloc(bufs[q], bytes);
-            if (ce != cudaSuccess) {
-                cudaGetLastError();
-                *bufs[q] = nullptr;
-                set_error("hmg_matvec_multi: allocating %zu bytes of operand space failed: %s", bytes,
-                          cudaGetErrorString(ce));
-                return ce == cudaErrorMemoryAllocation ? HMG_ERR_NOMEM : HMG_ERR_CUDA;
-            }
+    if (!h->tc_bbuf) {
+        const size_t bytes = (size_t)(h->tc_xkc + h->tc_tkc) * 16 * TC_NMAX * h->tc_parts;
+        cudaError_t ce = cudaMalloc(&h->tc_bbuf, bytes);
+        if (ce != cudaSuccess) {
+            cudaGetLastError();
+            h->tc_bbuf = nullptr;
+            set_error("hmg_matvec_multi: allocating %zu bytes of operand space failed: %s", bytes, cudaGetErrorString(ce));
+            return ce == cudaErrorMemoryAllocation ? HMG_ERR_NOMEM : HMG_ERR_CUDA;
         }
+    }
     if (h->tc_parts == 3) return tc_product_parts<3>(h, nrhs, X, ldx, Y, ldy);
     if (h->tc_parts == 2) return tc_product_parts<2>(h, nrhs, X, ldx, Y, ldy);
     return tc_product_parts<1>(h, nrhs, X, ldx, Y, ldy);
