@@ -14,12 +14,12 @@
 // Both passes run one persistent kernel: one CTA per SM walks a job list balanced on
 // the host (longest job first onto the least loaded CTA).  A job (a block in pass 1, a
 // tile in pass 2) is a run of "steps", each an A chunk (<= 48 KB) and the B chunk it
-// multiplies (<= 16 KB).  Warp 4 copies steps with bulk copies (cp.async.bulk,
+// multiplies (<= 32 KB).  Warp 4 copies steps with bulk copies (cp.async.bulk,
 // completion counted on the step slot's mbarrier) into a 208 KB byte ring that holds up
 // to 16 steps of any size; warp 5 issues the MMAs (one elected lane, accumulating in one
-// of two N-column tensor-memory buffers) and frees each step's bytes with
-// tcgen05.commit; warps 0-3 drain a finished buffer (tcgen05.ld, one 32-row quarter
-// each) while the next job accumulates in the other.
+// of two tensor-memory buffers) and frees each step's bytes with tcgen05.commit; warps
+// 0-3 drain a finished buffer (tcgen05.ld, one 32-row quarter each) while the next job
+// (split operands: the next step) accumulates in the other.
 //
 // Operand layout (no swizzle, K-major core matrices of 8 rows x 16 bytes), K cores
 // outermost so that every K range of an operand is one contiguous byte range:
@@ -31,9 +31,13 @@
 //   X is kept over the Z-ordered column index with 8 columns per K core; a block whose
 //   columns start at c0 reads K cores from c0 / 8 on, and its A operand carries
 //   c0 mod 8 leading zero columns so the K positions line up.
-// Descriptors: leading byte offset = stride between K cores (A: rc * 128, B: N * 16),
-// stride byte offset = stride between row cores (128).  Instruction kind::f16 with BF16
-// A/B, FP32 D, M 128, N 32 (up to 32 vectors) or 64.
+//   Split operands (P = 2 or 3 BF16 parts) are interleaved by K core: K core kc holds
+//   part 0's cores, then part 1's, then part 2's (A: P * rc row cores per K core; B: P *
+//   N * 16 bytes per K core), so that one copy brings every part of a K range.
+// Descriptors: leading byte offset = stride between K cores (A: P * rc * 128, B: P * N *
+// 16), stride byte offset = stride between row cores (128); part q starts q * rc * 128
+// (A) or q * N * 16 (B) bytes into each K core.  Instruction kind::f16 with BF16 A/B,
+// FP32 D, M 128, N 32 (up to 32 vectors) or 64.
 // Every wait is bounded (pipeline.cuh): on a time-out the waiting role records an error
 // code in the handle's flag, leaves its loop, and the CTA waits for its own copies and
 // MMAs before freeing tensor memory.  BF16 rounding of factors, near field, X and t_b
