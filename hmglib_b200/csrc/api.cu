@@ -685,7 +685,6 @@ __global__ void k_fill_work_items(const int* r0, const int* m1, const int* c0, c
     if (b >= nb) return;
     __shared__ double red[4][3][4];
     int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    double vals[4][3];
     for (int d = 0; d < dim; d++) {
         double lo1 = 1e308, hi1 = -1e308, lo2 = 1e308, hi2 = -1e308;
         for (int i = threadIdx.x; i < m1[b]; i += blockDim.x) {
@@ -702,7 +701,6 @@ __global__ void k_fill_work_items(const int* r0, const int* m1, const int* c0, c
             lo2 = fmin(lo2, __shfl_xor_sync(0xffffffffu, lo2, o));
             hi2 = fmax(hi2, __shfl_xor_sync(0xffffffffu, hi2, o));
         }
-        vals[0][d] = lo1; vals[1][d] = hi1; vals[2][d] = lo2; vals[3][d] = hi2;
         if (lane == 0) { red[0][d][warp] = lo1; red[1][d][warp] = hi1; red[2][d][warp] = lo2; red[3][d][warp] = hi2; }
     }
     __syncthreads();
@@ -723,7 +721,6 @@ __global__ void k_fill_work_items(const int* r0, const int* m1, const int* c0, c
         }
         out[b] = w;
     }
-    (void)vals;
 }
 
 __global__ void k_perm_to_u64(const int* perm, int n, uint64_t* order, unsigned int* ids)

@@ -430,7 +430,6 @@ hmg_status setup_tree(hmg_matrix* h)
     long long* packed = nullptr;
     signed char* ltype = nullptr;
     int* ccnt = nullptr;
-    int* totals = nullptr;  // [0] leaves+children packed low/high via long long below
     long long* ptot = nullptr;
     int nn = 1;
     int levels = 0;
@@ -584,7 +583,6 @@ done:
     dfree(ltype, s);
     dfree(ccnt, s);
     dfree(ptot, s);
-    (void)totals;
     free_cluster_set(cs[0], s);
     free_cluster_set(cs[1], s);
     return st;
