@@ -71,6 +71,13 @@ def test_argument_errors_need_no_gpu(hmg):
     assert L.hmg_matvec(None, None, None) == 1
     assert L.hmg_destroy(None) == 0
     assert L.hmg_version() >= 100
+    # the multi-vector, tensor-core, graph and autotuning entry points check their
+    # handle before touching the device
+    assert L.hmg_matvec_multi(None, 2, None, 10, None, 10) == 1
+    assert L.hmg_build_tensor_core_operands(None, 5) == 1
+    assert b"NULL" in L.hmg_last_error()
+    assert L.hmg_set_graphs(None, 1) == 1
+    assert L.hmg_autotune(None, 3, None, None, None) == 1
 
 
 def test_splitmix64_known_answer():
