@@ -149,13 +149,14 @@ hmg_status hmg_full_matvec_rows(hmg_matrix* h, const double* x, const int* rows,
  * there as well (HMG_PREC_BF16) or on the CUDA cores in FP32 (HMG_PREC_FP32).  Results
  * agree with the FP32 products to ~1e-3 (BF16 rounding).  HMG_PREC_BF16X3 keeps every
  * operand, the near field included, as a BF16 pair (hi and the rounding of what hi
- * misses) and multiplies hi*hi + hi*lo + lo*hi: ~5e-6, with twice the operand bytes
+ * misses) and multiplies hi*hi + hi*lo + lo*hi: ~7e-6, with twice the operand bytes
  * and three times the MMAs.  HMG_PREC_BF16X6 keeps three parts (24 bits, as FP32) and
- * adds the terms down to 2^-16 of hi*hi: 1.5 times the bytes of X3.  With split
+ * adds the terms down to 2^-16 of hi*hi: ~4e-7, 1.5 times the bytes of X3.  With split
  * operands hi*hi and the correction terms accumulate apart and every accumulator is
  * drained after at most 128 K positions; the sums continue in FP32 on the CUDA cores.
- * Single-vector products keep
- * using the FP32 storage.  Recomputing the factors or the near field drops the copies.
+ * The copies sit beside the FP32 storage (hmg_info.tc_bytes; one part holds ~0.6x its
+ * bytes).  Single-vector products keep using the FP32 storage.  Recomputing the
+ * factors or the near field drops the copies.
  * hmg_build_bf16_factors(h) is hmg_build_tensor_core_operands(h, HMG_PREC_BF16). */
 hmg_status hmg_build_tensor_core_operands(hmg_matrix* h, int near_precision);
 hmg_status hmg_build_bf16_factors(hmg_matrix* h);
