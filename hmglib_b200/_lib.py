@@ -66,6 +66,7 @@ _PROTOS = {
     "hmg_set_near_mode": (C.c_int, [_vp, C.c_int]),
     "hmg_matvec": (C.c_int, [_vp, _vp, _vp]),
     "hmg_matvec_host": (C.c_int, [_vp, _vp, _vp]),
+    "hmg_matvec_unbatched": (C.c_int, [_vp, _vp, _vp]),
     "hmg_matvec_multi": (C.c_int, [_vp, C.c_int, _vp, C.c_int, _vp, C.c_int]),
     "hmg_group_create": (C.c_int, [C.POINTER(_vp), C.POINTER(_vp), C.c_int, _vp]),
     "hmg_group_offsets": (C.c_int, [_vp, C.c_int, _vp]),

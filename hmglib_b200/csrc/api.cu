@@ -225,6 +225,14 @@ hmg_status hmg_matvec(hmg_matrix* h, const double* x, double* y)
     return matvec_device(h, x, y);
 }
 
+hmg_status hmg_matvec_unbatched(hmg_matrix* h, const double* x, double* y)
+{
+    HMG_REQUIRE(h && x && y, HMG_ERR_INVALID, "hmg_matvec_unbatched: NULL argument");
+    hmg_status st = check_ready(h, "hmg_matvec_unbatched");
+    if (st) return st;
+    return matvec_unbatched(h, x, y);
+}
+
 hmg_status hmg_build_tensor_core_operands(hmg_matrix* h, int near_precision)
 {
     HMG_REQUIRE(h, HMG_ERR_INVALID, "hmg_build_tensor_core_operands: NULL handle");
@@ -788,16 +796,9 @@ void setup_h_matrix(struct h_matrix_data* data)
         cudaMemcpy(h->pts[i], h->zpts[i], sizeof(double) * n * h->dim, cudaMemcpyDeviceToDevice);
         if (!data->order[i]) cudaMalloc((void**)&data->order[i], sizeof(uint64_t) * n);
         k_perm_to_u64<<<ceil_div(n, 256), 256>>>(h->perm[i], n, data->order[i], data->point_ids_d[i]);
-        // per-dimension extremes
-        std::vector<double> z((size_t)n * h->dim), mn(h->dim), mx(h->dim);
-        cudaMemcpy(z.data(), h->zpts[i], sizeof(double) * z.size(), cudaMemcpyDeviceToHost);
-        for (int d = 0; d < h->dim; d++) {
-            double a = z[(size_t)d * n], b = a;
-            for (int k = 1; k < n; k++) { a = std::fmin(a, z[(size_t)d * n + k]); b = std::fmax(b, z[(size_t)d * n + k]); }
-            mn[d] = a; mx[d] = b;
-        }
-        cudaMemcpy(data->min_per_dim_d[i], mn.data(), sizeof(double) * h->dim, cudaMemcpyHostToDevice);
-        cudaMemcpy(data->max_per_dim_d[i], mx.data(), sizeof(double) * h->dim, cudaMemcpyHostToDevice);
+        // per-dimension extremes (point_set.min_per_dim / max_per_dim), on the device
+        st = minmax_device(h->zpts[i], n, h->dim, data->min_per_dim_d[i], data->max_per_dim_d[i], h->stream);
+        if (st) { legacy_fail("setup_h_matrix", st); return; }
     }
     data->mat_vec_data_count = h->nblocks;
     data->mat_vec_info.dense_count = h->ndense;
@@ -876,7 +877,15 @@ void apply_h_matrix_mvp(double* x, double* y, struct h_matrix_data* data)
 
 void apply_h_matrix_mvp_without_batching(double* x, double* y, struct h_matrix_data* data)
 {
-    apply_h_matrix_mvp(x, y, data);
+    hmg_matrix* h = legacy_handle(data);
+    if (!h) return;
+    hmg_status st = legacy_kernel(data, h);
+    // the reference compresses each admissible block inside this call
+    // (apply_aca_for_current_work_item); here the ACA is computed once and kept
+    if (!st && h->naca > 0 && h->far_prec < 0) st = hmg_precompute_aca(h, data->k, 0.0, HMG_PREC_FP64);
+    if (!st) st = hmg_matvec_unbatched(h, x, y);
+    if (!st) st = hmg_synchronize(h);
+    if (st) legacy_fail("apply_h_matrix_mvp_without_batching", st);
 }
 
 void apply_full_mvp(double* x, double* y, struct h_matrix_data* data)

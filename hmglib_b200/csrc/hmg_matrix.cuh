@@ -142,6 +142,7 @@ hmg_status load(hmg_matrix** out, const char* path, cudaStream_t s);
 hmg_status run_aca(hmg_matrix* h, int k, double eps, int precision);
 hmg_status fill_near(hmg_matrix* h, int precision);
 hmg_status matvec_device(hmg_matrix* h, const double* x, double* y, bool fp64_arith = false);
+hmg_status matvec_unbatched(hmg_matrix* h, const double* x, double* y);
 hmg_status matvec_multi(hmg_matrix* h, int nrhs, const double* X, int ldx, double* Y, int ldy);
 hmg_status matvec_multi_tc(hmg_matrix* h, int nrhs, const double* X, int ldx, double* Y, int ldy);
 hmg_status build_bf16_factors(hmg_matrix* h, bool near_on_tensor_cores, int parts);
@@ -157,6 +158,7 @@ hmg_status cg_solve(hmg_matrix* h, double shift, const double* b, double* x, dou
                     int* iters_out, double* relres_out);
 hmg_status morton_codes(const double* coords, int n, int dim, int bits, uint64_t* codes,
                         cudaStream_t s);
+hmg_status minmax_device(const double* coords, int n, int dim, double* mn, double* mx, cudaStream_t s);
 void free_far(hmg_matrix* h);
 void free_near(hmg_matrix* h);
 void free_tree(hmg_matrix* h);

@@ -8,35 +8,40 @@
 // them, hmg_radix_sort_u64_noalloc sorts with scratch that lives in a fixed,
 // file-scope device array of this library instead:
 //
-//   * capacity: HMG_NOALLOC_SORT_MAX_KEYS keys (2^20); larger n is rejected
-//     with HMG_ERR_INVALID and nothing is touched;
+//   * capacity: NA_MAX_KEYS = 2^20 keys; larger n is rejected with
+//     HMG_ERR_INVALID and nothing is touched;
 //   * every GPU that loads the library holds the array (12 MB + 0.27 MB) until
 //     the process exits;
 //   * the first call on a device looks up the array's device address
 //     (cudaGetSymbolAddress, with that device current) and caches it, so make that
-//     first call before any stream capture on the device;
+//     first call before any stream capture on the device; the cached address is
+//     not looked up again, so a cudaDeviceReset on that device ends the entry
+//     point's use in this process;
 //   * all calls share the one array: calls whose work overlaps on the GPU (two
 //     streams, two host threads) race on it and corrupt each other's results --
 //     order them on one stream or synchronise between them;
 //   * the array keeps the previous call's contents; the counters that must start
-//     at zero are cleared on the stream by each call.
+//     at zero are cleared on the stream by each call;
+//   * the call only enqueues work on `stream` and returns: it neither copies to
+//     the host nor waits for the stream.  Every digit pass is launched; a pass
+//     whose digit is the same for all keys (read on the device from the histogram
+//     of all digits) skips its counting and scan and copies the keys through
+//     unchanged, which is what the stable pass would produce.
 // The sort is the same stable LSD radix sort as hmg_radix_sort_u64, with the same
-// kernels, and gives bit-identical results.
+// per-tile steps, and gives bit-identical results.
 #include <mutex>
 
 #include "hmg_internal.cuh"
+#include "radix.cuh"
 #include "../../include/hmg.h"
 
 namespace hmg {
 
-// kernels of the allocating sort (util.cu)
+// histogram of all eight digits (util.cu)
 __global__ void k_rs_hist_all(const uint64_t* keys, int n, unsigned* hist);
-__global__ void k_rs_tile_hist(const uint64_t* keys, int n, int shift, int ntiles, unsigned* counts);
-__global__ void k_rs_scatter(const uint64_t* kin, const uint32_t* vin, uint64_t* kout, uint32_t* vout,
-                             int n, int shift, int ntiles, const unsigned* offsets);
 
 static constexpr int NA_MAX_KEYS = 1 << 20;
-static constexpr int NA_TILE = 4096;  // keys per tile of the radix kernels
+static constexpr int NA_TILE = RS_TILE;  // keys per tile of the radix steps
 static constexpr int NA_MAX_TILES = NA_MAX_KEYS / NA_TILE;
 static constexpr int NA_COUNTS = 256 * NA_MAX_TILES;
 
@@ -49,10 +54,47 @@ struct NoAllocScratch {
 
 static __device__ __align__(256) NoAllocScratch g_sort_scratch;
 
-// exclusive scan of the (digit, tile) counts in place: one CTA, 1024 threads,
-// each owning a contiguous run
-__global__ void __launch_bounds__(1024) k_na_scan(unsigned* a, int n)
+// A pass is trivial when every key has the same digit: the histogram of all
+// digits (of the input keys; any permutation of them has the same one) then holds
+// n for the digit of the current first key.
+__device__ __forceinline__ bool na_pass_trivial(const unsigned* hist, const uint64_t* keys, int n, int shift)
 {
+    const unsigned d = (unsigned)((keys[0] >> shift) & 255u);
+    return hist[(shift >> 3) * 256 + d] == (unsigned)n;
+}
+
+__global__ void k_na_tile_hist(const uint64_t* keys, int n, int shift, int ntiles, unsigned* counts,
+                               const unsigned* hist)
+{
+    if (na_pass_trivial(hist, keys, n, shift)) return;
+    rs_tile_hist(keys, n, shift, ntiles, blockIdx.x, counts);
+}
+
+// stable scatter of the pass, or a plain copy of the tile when the pass is trivial
+// (the stable order of equal digits is the input order)
+__global__ void k_na_scatter(const uint64_t* kin, const uint32_t* vin, uint64_t* kout, uint32_t* vout, int n,
+                             int shift, int ntiles, const unsigned* offsets, const unsigned* hist)
+{
+    if (na_pass_trivial(hist, kin, n, shift)) {
+        const long long base = (long long)blockIdx.x * RS_TILE;
+        for (int k = threadIdx.x; k < RS_TILE; k += blockDim.x) {
+            const long long i = base + k;
+            if (i < n) {
+                kout[i] = kin[i];
+                vout[i] = vin[i];
+            }
+        }
+        return;
+    }
+    rs_scatter(kin, vin, kout, vout, n, shift, ntiles, blockIdx.x, offsets);
+}
+
+// exclusive scan of the (digit, tile) counts in place: one CTA, 1024 threads,
+// each owning a contiguous run; nothing to do for a trivial pass
+__global__ void __launch_bounds__(1024) k_na_scan(unsigned* a, int n, const uint64_t* keys, int nkeys,
+                                                  int shift, const unsigned* hist)
+{
+    if (na_pass_trivial(hist, keys, nkeys, shift)) return;
     __shared__ unsigned warp_tot[32];
     const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
     const int per = (n + 1023) / 1024;
@@ -133,25 +175,18 @@ extern "C" hmg_status hmg_radix_sort_u64_noalloc(uint64_t* keys, uint32_t* value
     const int ntiles = (n + NA_TILE - 1) / NA_TILE;
     HMG_CUDA_TRY(cudaMemsetAsync(w->hist, 0, sizeof(w->hist), s));
     const int hb = ntiles < 1184 ? ntiles : 1184;
-    k_rs_hist_all<<<hb, 256, 0, s>>>(keys, n, w->hist);
+    k_rs_hist_all<<<hb, RS_THREADS, 0, s>>>(keys, n, w->hist);
     HMG_LAUNCH_CHECK();
-    unsigned h_hist[8 * 256];
-    HMG_CUDA_TRY(cudaMemcpyAsync(h_hist, w->hist, sizeof(h_hist), cudaMemcpyDeviceToHost, s));
-    HMG_CUDA_TRY(cudaStreamSynchronize(s));
     uint64_t *ka = keys, *kb = w->keys;
     uint32_t *va = values, *vb = w->vals;
     const int npasses = (key_bits + 7) / 8;
     for (int p = 0; p < npasses; p++) {
-        bool trivial = false;
-        for (int d = 0; d < 256; d++)
-            if (h_hist[p * 256 + d] == (unsigned)n) trivial = true;
-        if (trivial) continue;
         const int shift = 8 * p;
-        k_rs_tile_hist<<<ntiles, 256, 0, s>>>(ka, n, shift, ntiles, w->counts);
+        k_na_tile_hist<<<ntiles, RS_THREADS, 0, s>>>(ka, n, shift, ntiles, w->counts, w->hist);
         HMG_LAUNCH_CHECK();
-        k_na_scan<<<1, 1024, 0, s>>>(w->counts, 256 * ntiles);
+        k_na_scan<<<1, 1024, 0, s>>>(w->counts, 256 * ntiles, ka, n, shift, w->hist);
         HMG_LAUNCH_CHECK();
-        k_rs_scatter<<<ntiles, 256, 0, s>>>(ka, va, kb, vb, n, shift, ntiles, w->counts);
+        k_na_scatter<<<ntiles, RS_THREADS, 0, s>>>(ka, va, kb, vb, n, shift, ntiles, w->counts, w->hist);
         HMG_LAUNCH_CHECK();
         uint64_t* tk = ka; ka = kb; kb = tk;
         uint32_t* tv = va; va = vb; vb = tv;

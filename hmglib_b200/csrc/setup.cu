@@ -101,6 +101,36 @@ __global__ void k_gather_points(const double* src, double* dst, const uint32_t* 
     iperm[o] = i;
 }
 
+__global__ void k_keys_to_double(const unsigned long long* mn_key, const unsigned long long* mx_key, int dim,
+                                 double* mn, double* mx)
+{
+    int d = threadIdx.x;
+    if (d < dim) {
+        mn[d] = order_key_inv(mn_key[d]);
+        mx[d] = order_key_inv(mx_key[d]);
+    }
+}
+
+// Per-dimension minimum and maximum of n points (SoA coords[d*n+i]) into the device
+// arrays mn[dim], mx[dim] (helper.cu:108-138, compute_minmax); exact.
+hmg_status minmax_device(const double* coords, int n, int dim, double* mn, double* mx, cudaStream_t s)
+{
+    if (n <= 0 || dim <= 0) return HMG_OK;
+    unsigned long long* mm = nullptr;
+    hmg_status st = dalloc(&mm, (size_t)2 * dim, s);
+    if (st) return st;
+    HMG_CUDA_TRY(cudaMemsetAsync(mm, 0xff, sizeof(unsigned long long) * dim, s));
+    HMG_CUDA_TRY(cudaMemsetAsync(mm + dim, 0, sizeof(unsigned long long) * dim, s));
+    int g = ceil_div(n, 256);
+    if (g > 1184) g = 1184;
+    k_minmax<<<g, 256, 0, s>>>(coords, n, dim, mm, mm + dim);
+    HMG_LAUNCH_CHECK();
+    k_keys_to_double<<<1, 32, 0, s>>>(mm, mm + dim, dim, mn, mx);
+    HMG_LAUNCH_CHECK();
+    dfree(mm, s);
+    return HMG_OK;
+}
+
 static bool morton_supported(int dim, int bits)
 {
     return (dim == 2 && bits == 32) || (dim == 3 && bits == 20) || (dim == 10 && bits == 4);

@@ -9,6 +9,7 @@
 // pass of 3D codes (60 significant bits).
 #include <cstdarg>
 
+#include "radix.cuh"
 #include "util.cuh"
 
 namespace hmg {
@@ -125,11 +126,6 @@ template hmg_status scan_exclusive<long long>(const long long*, long long*, long
 // ---------------------------------------------------------------------------
 // radix sort
 // ---------------------------------------------------------------------------
-static constexpr int RS_THREADS = 256;          // 8 warps
-static constexpr int RS_ITEMS = 16;             // items per lane
-static constexpr int RS_TILE = RS_THREADS * RS_ITEMS;  // 4096 keys per tile
-static constexpr int RS_WARP_SPAN = 32 * RS_ITEMS;     // contiguous keys per warp
-
 // histogram of all eight 8-bit digits over all keys
 __global__ void k_rs_hist_all(const uint64_t* keys, int n, unsigned* hist /* [8][256] */)
 {
@@ -153,70 +149,14 @@ __global__ void k_rs_hist_all(const uint64_t* keys, int n, unsigned* hist /* [8]
 __global__ void k_rs_tile_hist(const uint64_t* keys, int n, int shift, int ntiles,
                                unsigned* counts)
 {
-    __shared__ unsigned h[256];
-    h[threadIdx.x] = 0;
-    __syncthreads();
-    long long base = (long long)blockIdx.x * RS_TILE;
-#pragma unroll 4
-    for (int k = 0; k < RS_ITEMS; k++) {
-        long long i = base + (long long)k * RS_THREADS + threadIdx.x;
-        if (i < n) atomicAdd(&h[(keys[i] >> shift) & 255u], 1u);
-    }
-    __syncthreads();
-    counts[(size_t)threadIdx.x * ntiles + blockIdx.x] = h[threadIdx.x];
+    rs_tile_hist(keys, n, shift, ntiles, blockIdx.x, counts);
 }
 
 __global__ void k_rs_scatter(const uint64_t* kin, const uint32_t* vin, uint64_t* kout,
                              uint32_t* vout, int n, int shift, int ntiles,
                              const unsigned* offsets /* scanned counts */)
 {
-    __shared__ unsigned wcount[8][256];
-    __shared__ unsigned wbase[8][256];
-    int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    for (int t = lane; t < 256; t += 32) wcount[warp][t] = 0;
-    __syncwarp();
-    long long wstart = (long long)blockIdx.x * RS_TILE + (long long)warp * RS_WARP_SPAN;
-    uint64_t key[RS_ITEMS];
-    uint32_t val[RS_ITEMS];
-    unsigned rank[RS_ITEMS];
-    unsigned lt_mask = (1u << lane) - 1u;
-#pragma unroll
-    for (int it = 0; it < RS_ITEMS; it++) {
-        long long i = wstart + it * 32 + lane;
-        bool valid = i < n;
-        key[it] = valid ? kin[i] : 0;
-        val[it] = valid ? vin[i] : 0;
-        unsigned digit = valid ? (unsigned)((key[it] >> shift) & 255u) : 256u;
-        unsigned peers = __match_any_sync(0xffffffffu, digit);
-        unsigned before = __popc(peers & lt_mask);
-        unsigned cnt = __popc(peers);
-        unsigned basecnt = valid ? wcount[warp][digit] : 0u;
-        rank[it] = basecnt + before;
-        __syncwarp();
-        if (valid && before == 0) wcount[warp][digit] = basecnt + cnt;
-        __syncwarp();
-    }
-    __syncthreads();
-    {
-        int d = threadIdx.x;  // 256 threads, one digit each
-        unsigned run = offsets[(size_t)d * ntiles + blockIdx.x];
-#pragma unroll
-        for (int w = 0; w < 8; w++) {
-            wbase[w][d] = run;
-            run += wcount[w][d];
-        }
-    }
-    __syncthreads();
-#pragma unroll
-    for (int it = 0; it < RS_ITEMS; it++) {
-        long long i = wstart + it * 32 + lane;
-        if (i < n) {
-            unsigned digit = (unsigned)((key[it] >> shift) & 255u);
-            unsigned pos = wbase[warp][digit] + rank[it];
-            kout[pos] = key[it];
-            vout[pos] = val[it];
-        }
-    }
+    rs_scatter(kin, vin, kout, vout, n, shift, ntiles, blockIdx.x, offsets);
 }
 
 hmg_status radix_sort_pairs(uint64_t* keys, uint32_t* vals, int n, int key_bits,

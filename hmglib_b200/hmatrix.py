@@ -106,6 +106,12 @@ class HMatrix:
         self._call("hmg_matvec_multi", nrhs, _ptr(X), int(X.stride(0)), _ptr(Y), int(Y.stride(0)))
         return Y
 
+    def matvec_unbatched(self, x, y):
+        """y = H x one block per launch on device tensors (hmg_matvec_unbatched, the
+        reference's sequential_h_matrix_mvp_without_batching); asynchronous."""
+        self._call("hmg_matvec_unbatched", _ptr(x), _ptr(y))
+        return y
+
     def matvec_device(self, x_ptr: int, y_ptr: int):
         self._call("hmg_matvec", C.c_void_p(x_ptr), C.c_void_p(y_ptr))
 

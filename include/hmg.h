@@ -124,8 +124,17 @@ hmg_status hmg_set_near_mode(hmg_matrix* h, int mode);
 
 /* y = H x on device vectors in the caller's point order; x is not modified.
  * Asynchronous on the handle's stream.  Replaces apply_h_matrix_mvp
- * (hmglib.cu:271-286) and apply_h_matrix_mvp_without_batching (:288-301). */
+ * (hmglib.cu:271-286). */
 hmg_status hmg_matvec(hmg_matrix* h, const double* x, double* y);
+
+/* y = H x one block at a time: every dense block (entries generated in FP64) and
+ * then every admissible block (FP64 arithmetic over the stored FP64 or FP32
+ * factors) is applied by its own kernel launch, in work-list order.  A second,
+ * independent implementation of the product for checking, launch-bound by design.
+ * Not on group handles or mixed storage.  Asynchronous on the handle's stream.
+ * Replaces sequential_h_matrix_mvp_without_batching (linear_algebra.cu:4384-4443),
+ * which apply_h_matrix_mvp_without_batching (hmglib.cu:288-301) calls. */
+hmg_status hmg_matvec_unbatched(hmg_matrix* h, const double* x, double* y);
 
 /* Same product with host vectors: copies x in, multiplies, copies y out, returns
  * when y is written.  The copies use a pinned staging buffer of the handle. */
@@ -273,7 +282,9 @@ hmg_status hmg_get_factors(hmg_matrix* h, int block, double* U, double* V);
 
 /* ---- primitives (device pointers, asynchronous on `stream`) ----------------- */
 /* stable LSD radix sort of 64-bit keys carrying 32-bit values, in place;
- * `key_bits` = number of low key bits that can be nonzero (64 if unknown) */
+ * `key_bits` = number of low key bits that can be nonzero (64 if unknown).  The
+ * call reads the histogram of all digits back to the host to skip passes whose
+ * digit is the same for every key, so it waits for `stream` once per call. */
 hmg_status hmg_radix_sort_u64(uint64_t* keys, uint32_t* values, int n, int key_bits,
                               void* stream);
 /* The same sort without any device allocation, for callers that must not have the
@@ -282,8 +293,12 @@ hmg_status hmg_radix_sort_u64(uint64_t* keys, uint32_t* values, int n, int key_b
  * No counterpart in the reference.  Scratch is a fixed array compiled into the
  * library (held on every GPU that loads it): n above 2^20 keys is rejected with
  * HMG_ERR_INVALID.  The first call on a device looks the array up (make it before
- * any stream capture); calls share the array, so calls that overlap on the GPU race
- * -- keep them on one stream.  Result identical to hmg_radix_sort_u64. */
+ * any stream capture) and keeps its address for the rest of the process (after a
+ * cudaDeviceReset of that device the entry point cannot be used again).  The call
+ * only enqueues work on `stream` and returns without waiting for it: the passes
+ * whose digit is the same for every key are recognised on the device.  Calls share
+ * the array, so calls that overlap on the GPU race -- keep them on one stream.
+ * Result identical to hmg_radix_sort_u64. */
 hmg_status hmg_radix_sort_u64_noalloc(uint64_t* keys, uint32_t* values, int n, int key_bits,
                                       void* stream);
 

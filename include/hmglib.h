@@ -21,6 +21,16 @@
  *
  * Like the reference, setup_h_matrix permutes data->coords_d[i][d] into Z order
  * and leaves the sorted Morton codes in code_d and the permutation in order.
+ *
+ * U, V and dA: as in the reference, they are NULL until precompute_aca /
+ * precompute_dense and non-NULL afterwards (the reference tests them to decide
+ * whether a compression exists, hmglib.cu:277-278).  They point into the engine's
+ * own storage -- U and V both at the first factor allocation, whose blocks are laid
+ * out as tile slices (hmg_internal.cuh), and dA at the near field in the same tile
+ * layout -- not at the reference's rank-major concatenated U / V
+ * (linear_algebra.cu:3808-3824) or column-major dense blocks (:3140-3342).  Read a
+ * block's factors with hmg_get_factors; the library frees this storage in
+ * destroy_h_matrix_data, so a caller must not.
  */
 #ifndef HMGLIB_H
 #define HMGLIB_H
@@ -138,7 +148,8 @@ void init_h_matrix_data(struct h_matrix_data* data, int point_count[2], int dim,
 void setup_h_matrix(struct h_matrix_data* data);
 /* hmglib.cu:271-286; x, y device vectors in the caller's order */
 void apply_h_matrix_mvp(double* x, double* y, struct h_matrix_data* data);
-/* hmglib.cu:288-301 (same product, same result as the batched path) */
+/* hmglib.cu:288-301: one launch per block (hmg_matvec_unbatched), an independent
+ * second product; FP64 factors */
 void apply_h_matrix_mvp_without_batching(double* x, double* y, struct h_matrix_data* data);
 /* hmglib.cu:305-348 */
 void destroy_h_matrix_data(struct h_matrix_data* data);

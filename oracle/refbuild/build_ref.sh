@@ -4,7 +4,9 @@
 # plus the ref_dump driver.  TEST INFRASTRUCTURE ONLY: the result is the oracle the
 # parity fixtures are generated with; the product never links it.
 #
-# usage: oracle/refbuild/build_ref.sh [reference_src_dir]   (default /root/reference/src)
+# usage: oracle/refbuild/build_ref.sh REFERENCE_SRC_DIR
+#    or: HMG_REFERENCE_SRC=REFERENCE_SRC_DIR oracle/refbuild/build_ref.sh
+# (REFERENCE_SRC_DIR is the reference checkout's src/ folder)
 #
 # Needed deviations from the reference's own Makefile (src/Makefile:19-71):
 #   * MAGMA is neither installed nor vendored -> magma_v2.h / magma_lapack.h /
@@ -17,7 +19,11 @@
 #   * sm_100a instead of sm_61, no -G.
 set -euo pipefail
 HERE="$(cd "$(dirname "$0")" && pwd)"
-REF="${1:-/root/reference/src}"
+REF="${1:-${HMG_REFERENCE_SRC:-}}"
+if [ -z "$REF" ] || [ ! -d "$REF" ]; then
+  echo "usage: $0 REFERENCE_SRC_DIR (or set HMG_REFERENCE_SRC)" >&2
+  exit 2
+fi
 OUT="$HERE/../_ref"
 NVCC="${NVCC:-/usr/local/cuda/bin/nvcc}"
 mkdir -p "$OUT/obj" "$OUT/include"

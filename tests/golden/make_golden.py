@@ -7,11 +7,11 @@ where it was built:
    builds ``oracle/_ref/ref_dump`` (the reference's sources + a MAGMA stand-in +
    a dump driver, sm_100a);
 2. on a B200:  ``python tests/golden/make_golden.py run --ref oracle/_ref/ref_dump
-   --out gpurun_out/golden`` writes the inputs of every case below, runs the
-   reference on each and keeps its raw outputs;
-3. here:  ``python tests/golden/make_golden.py pack --raw gpurun_out/golden``
-   converts the raw outputs into ``tests/golden/<case>.npz`` (inputs are not
-   stored: they are regenerated from the seeds in CASES).
+   --out RAW_DIR`` writes the inputs of every case below, runs the reference on
+   each and keeps its raw outputs in RAW_DIR;
+3. with RAW_DIR copied back:  ``python tests/golden/make_golden.py pack --raw
+   RAW_DIR`` converts the raw outputs into ``tests/golden/<case>.npz`` (inputs are
+   not stored: they are regenerated from the seeds in CASES).
 
 Each fixture holds the reference's sorted Morton codes, its permutation
 (``order``), its work-item list after organize_mat_vec_data (bounds inclusive,

@@ -51,3 +51,50 @@ def rel_err(a, b):
     a = np.asarray(a, dtype=np.float64)
     b = np.asarray(b, dtype=np.float64)
     return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
+def fp64_rows(torch, H, x, rows):
+    """FP64 direct sums (K x)[rows] on the GPU (hmg_full_matvec_rows); x a device
+    vector in caller order, rows a host int array."""
+    r = torch.from_numpy(np.ascontiguousarray(rows, dtype=np.int32)).cuda()
+    y = torch.empty(len(rows), dtype=torch.float64, device="cuda")
+    H.full_matvec_rows(x, r, y)
+    torch.cuda.synchronize()
+    return y.cpu().numpy()
+
+
+def hmg_file_layout(buf: bytes) -> dict:
+    """Byte offsets of the sections of a file written by hmg_save (format version 1,
+    csrc/io.cu): magic, u32 version, u32 header bytes, the header struct (fields
+    read below at their offsets in it), then per point set pts, zpts, codes, perm,
+    iperm; the five int32 block arrays; [group offsets and parameters]; [ranks, two
+    tier arrays, allocation sizes, (chunk, U offset, V offset) per block, the
+    allocations]; [near-field offsets, near field]."""
+    import struct
+    hb = struct.unpack_from("<I", buf, 12)[0]
+    h = 16
+    n1, n2, dim = struct.unpack_from("<3i", buf, h)
+    nb, nd = struct.unpack_from("<2i", buf, h + 40)
+    gc, far_prec = struct.unpack_from("<2i", buf, h + 88)
+    near_prec = struct.unpack_from("<i", buf, h + 112)[0]
+    nchunks = struct.unpack_from("<i", buf, h + 172)[0]
+    out = dict(header_bytes=hb, n=(n1, n2), dim=dim, nblocks=nb, ndense=nd, far_prec=far_prec,
+               near_prec=near_prec, nchunks=nchunks, perm=[], iperm=[])
+    o = 16 + hb
+    for n in (n1, n2):
+        p = o + n * dim * 16 + n * 8
+        out["perm"].append(p)
+        out["iperm"].append(p + 4 * n)
+        o = p + 8 * n
+    out["blocks"] = {k: o + i * 4 * nb for i, k in enumerate(("r0", "m1", "c0", "m2", "type"))}
+    o += 20 * nb
+    if gc:
+        o += 8 * (gc + 1) + 8 * nb
+    if far_prec >= 0:
+        out["rank"] = o
+        out["place"] = o + 12 * nb + 8 * nchunks
+        cb = struct.unpack_from(f"<{nchunks}q", buf, o + 12 * nb) if nchunks else ()
+        o = out["place"] + 24 * nb + sum(cb)
+    if near_prec >= 0:
+        out["near_off"] = o
+    return out

@@ -22,6 +22,9 @@ CASES = [
     ("uniform", 50, 50, 3, 3, 1.5, 64, 0),     # a single dense block
     ("line", 5000, 5000, 3, 5, 1.5, 16, 0),    # degenerate dimensions (max == min)
     ("uniform", 1, 1, 2, 4, 1.5, 1, 0),        # one point
+    # the batching workload's tree: N = 2^20 uniform 3D, leaf 128, eta 1.5, min rule
+    # (1,661,755 blocks, 15 levels, more than 2^16 radix tiles)
+    ("uniform", 1 << 20, 1 << 20, 3, 1, 1.5, 128, 1),
 ]
 
 

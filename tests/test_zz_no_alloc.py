@@ -35,10 +35,14 @@ def test_noalloc_sort_matches_allocating_sort(hmg, cuda):
     noalloc.restype = C.c_int
     noalloc.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_void_p]
     rng = np.random.default_rng(2024)
-    # two calls in a row: Morton-like 60-bit keys with repeats, then full 64-bit keys
-    cases = [(MAX_KEYS, 60, 1 << 40), (300007, 64, None)]
+    # calls in a row: Morton-like 60-bit keys with repeats (the two low digits are
+    # the same for every key, so those passes are skipped on the device), full 64-bit
+    # keys, then keys that are all equal (every pass skipped) on a ragged last tile
+    cases = [(MAX_KEYS, 60, 1 << 40), (300007, 64, None), (5000, 64, 1)]
     for n, key_bits, distinct in cases:
-        if distinct is None:
+        if distinct == 1:
+            keys = np.full(n, 0x0123456789ABCDEF, dtype=np.uint64)
+        elif distinct is None:
             keys = rng.integers(0, 1 << 63, size=n, dtype=np.uint64) | (
                 rng.integers(0, 2, size=n, dtype=np.uint64) << np.uint64(63))
         else:
