@@ -18,6 +18,9 @@ over 4,096 rows is reported beside every number (err_vs_fp64).
   batched_tensor_cores  64 vectors a pass on the tensor cores with three-part BF16
          operands at N=2^18 (error <= 1e-6), beside the plain FP64 form at that size
          (the FP64 form of N=2^20 does not fit one B200).
+  serve  a short run of the serving workload (60 requests of the Poisson stream over
+         8 resident H-matrices, bench.py --workload serve for the full one): p50/p99
+         latency of the completed requests.
 The stored H-matrix (~95 GB mixed) is far larger than L2, so no L2 flush is needed
 between steps.  --impl reference times the FP64 direct product (the reference's
 apply_full_mvp, restated by the CPU oracle) on the host cores on a row sample.
@@ -467,9 +470,76 @@ def run_engine(a, rank, world):
     H.close()
     if world == 1 and not a.no_batched_tc:
         line["batched_tensor_cores"] = batched_tensor_cores(a.steps)
+    if world == 1 and a.serve_in_default > 0:
+        # the serving workload, short: p50/p99 latency of products and solves
+        r = serve_measure(a, a.serve_in_default, 0, local)
+        lat = r["latency"]
+        line["serve"] = {"requests": r["requests"], "completed": r["completed"], "refused": r["refused"],
+                         "p50_ms": lat.get("all", {}).get("p50_ms"), "p99_ms": lat.get("all", {}).get("p99_ms"),
+                         "by_class": {k: v for k, v in lat.items() if k != "all"},
+                         "requests_per_s": r["requests_per_s"], "solves": r["solves"],
+                         "matvec_batch": r["matvec_batch"], "resident_gb": r["resident_gb"],
+                         "latency_targets_s": r["latency_targets_s"]}
     if rank == 0:
         print(json.dumps(line), flush=True)
     return 0
+
+
+def ridge_feasibility(torch, hmg, H, n, shifts, steps=60, cg_maxit=600, seed=5):
+    """Is (H + shift I) positive definite, as CG needs?  Arnoldi on H with FP64-
+    arithmetic products (full reorthogonalisation, `steps` vectors) gives V^T H V; its
+    symmetric part is the Rayleigh-Ritz projection of S = (H + H^T) / 2, whose
+    eigenvalues lie in [lambda_min(S), lambda_max(S)], so its smallest one theta_min
+    bounds lambda_min(S) from above, and x^T (H + shift I) x = x^T (S + shift I) x for
+    every x.  theta_min + shift < 0 therefore proves that CG can meet p^T A p <= 0;
+    the Ritz vector's quadratic form, recomputed with one more FP64 product, confirms
+    it.  Then the CG solve (with refinement) at each shift, to 1e-8."""
+    H.set_product_precision(hmg.PREC_FP64)
+    V = torch.empty(steps + 1, n, dtype=torch.float64, device="cuda")
+    g = torch.Generator(device="cpu").manual_seed(seed)
+    v = torch.rand(n, generator=g, dtype=torch.float64).cuda() - 0.5
+    V[0] = v / torch.linalg.norm(v)
+    Hm = torch.zeros(steps + 1, steps, dtype=torch.float64)
+    w = torch.empty(n, dtype=torch.float64, device="cuda")
+    m = steps
+    for j in range(steps):
+        H.matvec(V[j], w)
+        torch.cuda.synchronize()
+        for _ in range(2):  # Gram-Schmidt twice
+            c = V[:j + 1] @ w
+            w -= V[:j + 1].T @ c
+            Hm[:j + 1, j] += c.cpu()
+        nb = float(torch.linalg.norm(w))
+        Hm[j + 1, j] = nb
+        if nb < 1e-12:
+            m = j + 1
+            break
+        V[j + 1] = w / nb
+    T = Hm[:m, :m].numpy()
+    S = 0.5 * (T + T.T)
+    theta, Y = np.linalg.eigh(S)
+    x = (V[:m].T @ torch.from_numpy(Y[:, 0]).cuda()).contiguous()
+    H.matvec(x, w)
+    torch.cuda.synchronize()
+    q = float(x @ w) / float(x @ x)
+    asym = float(np.abs(T - T.T)[np.triu_indices(m, 2)].max()) if m > 2 else 0.0
+    out = {"arnoldi_steps": m, "theta_min": float(theta[0]), "theta_max": float(theta[-1]),
+           "rayleigh_min_ritz_vector": q, "hessenberg_above_band_max": asym, "shifts": {}}
+    del V
+    H.set_product_precision(hmg.PREC_FP32)
+    b = torch.from_numpy(np.random.default_rng(seed).uniform(-1, 1, n)).cuda()
+    for sh in shifts:
+        xs = torch.zeros_like(b)
+        t0 = time.perf_counter()
+        try:
+            it, rel = H.cg_solve(b, xs, sh, tol=1e-8, maxit=cg_maxit, refine=True)
+            res = {"iterations": it, "relres": rel, "converged": rel <= 1e-8}
+        except hmg.HmgError as e:  # p^T A p <= 0 met by CG
+            res = {"error": str(e), "converged": False}
+        res["seconds"] = time.perf_counter() - t0
+        res["lambda_min_upper_bound"] = float(theta[0]) + sh
+        out["shifts"][str(sh)] = res
+    return out
 
 
 def run_precision(a, rank, world):
@@ -550,6 +620,9 @@ def run_precision(a, rank, world):
                "max_rank": info["max_rank"]}
         if prec == hmg.PREC_FP32:
             res["bf16_tensor_cores"] = tc
+        if name == "fp32" and not a.no_feasibility:
+            res["ridge_feasibility"] = ridge_feasibility(torch, hmg, H, n, [1e-3, 1e-2, 1e-1, 1.0],
+                                                         cg_maxit=a.cg_maxit)
         if name == "fp32":
             b = X[0].clone()
             x = torch.zeros_like(b)
@@ -702,25 +775,26 @@ def run_group(a, rank, world):
     return 0
 
 
-def run_serve(a, rank, world):
+SERVE_SIZES = [1 << 16] * 4 + [1 << 17, 1 << 18, 1 << 19, 1 << 20]
+
+
+def serve_measure(a, n_requests, n_baseline, local=0):
     """The serving workload: 8 resident H-matrices (four of 2^16 points, then 2^17, 2^18,
     2^19, 2^20; uniform 3D, Matern-3/2 rho 0.2, leaf 64, ACA eps 1e-4, mixed storage:
-    ~96 GB) and a Poisson stream at
-    2000 requests/s (seed 4): 80% single-vector products, 15% 8-vector kernel-ridge
-    solves (shift 1e-3 N, relative residual 1e-4), 5% new point sets of 2^14-2^18
+    ~96 GB) and a Poisson stream at 2000 requests/s (seed 4): 80% single-vector
+    products, 15% 8-vector kernel-ridge solves (shift 1e-3 N, relative residual 1e-4,
+    the library's block CG with FP64 refinement), 5% new point sets of 2^14-2^18
     points, under a 120 GB budget, with latency targets (--serve-slo-matvec,
     --serve-slo-solve seconds): a request whose predicted completion misses its target
-    is refused on arrival.  Reports p50/p99 latency of the completed requests, the
-    refused counts and throughput against the plain FP64 one-request-at-a-time path
-    (FP64 products, one vector per call, solves by hmg_cg_solve per column) on the same
-    H-matrices and the first requests."""
+    is refused on arrival.  Returns p50/p99 latency of the completed requests, the
+    refused counts and (n_baseline > 0) throughput against the plain FP64
+    one-request-at-a-time path (FP64 products, one vector per call, solves by
+    hmg_cg_solve per column) on the same H-matrices and the first n_baseline requests."""
     import torch
 
     import hmglib_b200 as hmg
     from hmglib_b200 import serve, synth
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    torch.cuda.set_device(local)
-    sizes = [1 << 16] * 4 + [1 << 17, 1 << 18, 1 << 19, 1 << 20]
+    sizes = SERVE_SIZES
     t0 = time.perf_counter()
     slo = {"matvec": a.serve_slo_matvec, "solve": a.serve_slo_solve}
     srv = serve.Server(budget_bytes=120e9, slo_s=slo)
@@ -731,7 +805,7 @@ def run_serve(a, rank, world):
         srv.add(H, st)
     t_build = time.perf_counter() - t0
     resident = srv.used_bytes()
-    reqs = serve.poisson_requests(a.serve_requests, 2000.0, sizes, seed=4, eps=1e-4, shift_per_point=1e-3,
+    reqs = serve.poisson_requests(n_requests, 2000.0, sizes, seed=4, eps=1e-4, shift_per_point=1e-3,
                                   tol=1e-4)
     print(f"serve: resident {srv.used_bytes() / 1e9:.1f} GB built in {t_build:.1f} s; {len(reqs)} requests",
           file=sys.stderr, flush=True)
@@ -755,47 +829,61 @@ def run_serve(a, rank, world):
     n_done = sum(q.done is not None and getattr(q, "rejected", None) is None for q in done)
     n_refused = sum(getattr(q, "rejected", None) is not None for q in done)
     batches = [q.batch for q in done if isinstance(q, serve.Matvec) and q.rejected is None]
-    # the plain path: one request at a time, FP64 products, no batching, no overlap
-    nb = min(a.serve_baseline, len(reqs))
-    base = reqs[:nb]
-    for r in srv.res.values():
-        r.H.set_product_precision(hmg.PREC_FP64)
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    for q in base:
-        if isinstance(q, serve.Matvec):
-            srv.res[q.mid].H.matvec(q.x)
-        elif isinstance(q, serve.Solve):
-            H = srv.res[q.mid].H
-            for j in range(q.B.shape[0]):
-                b = torch.from_numpy(q.B[j]).cuda()
-                x = torch.zeros_like(b)
-                H.cg_solve(b, x, q.shift, tol=q.tol, maxit=q.maxit, refine=False)
-        else:
-            Hn = serve.build_hmatrix(q.points, q.kind, q.param, q.eps, hmg.PREC_FP64)
-            Hn.close()
-    torch.cuda.synchronize()
-    t_base = time.perf_counter() - t0
-    line = {
-        "metric": "served requests/s (8 resident H-matrices, Poisson 2000 req/s); p50/p99 latency",
-        "value": n_done / wall, "unit": "requests/s", "n_gpus": 1, "steps": len(reqs), "warmup": len(warm),
-        "ms_per_step": 1000.0 * wall / max(1, n_done), "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": "serve_8resident_matern3d_poisson2000", "sizes": sizes, "aca_eps": 1e-4, "leaf": 64,
-                   "storage": "mixed", "budget_gb": 120, "requests": len(reqs), "mix": [0.8, 0.15, 0.05],
-                   "latency_targets_s": slo},
+    out = {
+        "requests": len(reqs), "completed": n_done, "seconds": wall, "requests_per_s": n_done / wall,
         "latency": lat, "refused": n_refused, "admitted_fraction": 1.0 - n_refused / max(1, len(reqs)),
         "matvec_batch": {"mean": float(np.mean(batches)) if batches else None,
                          "max": int(np.max(batches)) if batches else None},
-        "solves": solve_stats, "builds": build_stats,
-        "plain_fp64_one_at_a_time": {"requests": nb, "seconds": t_base, "requests_per_s": nb / t_base,
-                                     "throughput_ratio_served_vs_plain": (n_done / wall) / (nb / t_base)},
-        "resident_gb": resident / 1e9, "build_s": t_build, "clocks": clk.summary(),
-        "e2e": {"value": n_done / wall, "unit": "requests/s", "h2d_bytes_per_step": None,
-                "d2h_bytes_per_step": None},
+        "solves": solve_stats, "builds": build_stats, "resident_gb": resident / 1e9, "build_s": t_build,
+        "clocks": clk.summary(), "latency_targets_s": slo,
     }
+    # the plain path: one request at a time, FP64 products, no batching, no overlap
+    nb = min(n_baseline, len(reqs))
+    if nb > 0:
+        base = reqs[:nb]
+        for r in srv.res.values():
+            r.H.set_product_precision(hmg.PREC_FP64)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for q in base:
+            if isinstance(q, serve.Matvec):
+                srv.res[q.mid].H.matvec(q.x)
+            elif isinstance(q, serve.Solve):
+                H = srv.res[q.mid].H
+                for j in range(q.B.shape[0]):
+                    b = torch.from_numpy(q.B[j]).cuda()
+                    x = torch.zeros_like(b)
+                    H.cg_solve(b, x, q.shift, tol=q.tol, maxit=q.maxit, refine=False)
+            else:
+                Hn = serve.build_hmatrix(q.points, q.kind, q.param, q.eps, hmg.PREC_FP64)
+                Hn.close()
+        torch.cuda.synchronize()
+        t_base = time.perf_counter() - t0
+        out["plain_fp64_one_at_a_time"] = {"requests": nb, "seconds": t_base, "requests_per_s": nb / t_base,
+                                           "throughput_ratio_served_vs_plain": (n_done / wall) / (nb / t_base)}
     for mid in list(srv.res):
         srv.res.pop(mid).H.close()
+    return out
+
+
+def run_serve(a, rank, world):
+    """The serving workload on its own (serve_measure), as its own JSON line."""
+    import torch
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    r = serve_measure(a, a.serve_requests, a.serve_baseline, local)
+    line = {
+        "metric": "served requests/s (8 resident H-matrices, Poisson 2000 req/s); p50/p99 latency",
+        "value": r["requests_per_s"], "unit": "requests/s", "n_gpus": 1, "steps": r["requests"], "warmup": 16,
+        "ms_per_step": 1000.0 * r["seconds"] / max(1, r["completed"]), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "serve_8resident_matern3d_poisson2000", "sizes": SERVE_SIZES, "aca_eps": 1e-4,
+                   "leaf": 64, "storage": "mixed", "budget_gb": 120, "requests": r["requests"],
+                   "mix": [0.8, 0.15, 0.05], "latency_targets_s": r["latency_targets_s"]},
+        "e2e": {"value": r["requests_per_s"], "unit": "requests/s", "h2d_bytes_per_step": None,
+                "d2h_bytes_per_step": None},
+    }
+    line.update({k: v for k, v in r.items() if k not in ("requests_per_s", "latency_targets_s")})
     if rank == 0:
         print(json.dumps(line), flush=True)
     return 0
@@ -890,9 +978,13 @@ def main(argv=None):
                          "serve: the request loop over resident H-matrices")
     ap.add_argument("--no-autotune", action="store_true", help="keep the default V^T x task size and grid")
     ap.add_argument("--serve-requests", type=int, default=300)
+    ap.add_argument("--serve-in-default", type=int, default=60,
+                    help="requests of the short serving run added to the default line (0: none)")
     ap.add_argument("--serve-slo-matvec", type=float, default=1.0, help="latency target of a product, seconds")
     ap.add_argument("--serve-slo-solve", type=float, default=10.0, help="latency target of a solve, seconds")
     ap.add_argument("--cg-maxit", type=int, default=600)
+    ap.add_argument("--no-feasibility", action="store_true",
+                    help="precision workload: skip the positive-definiteness study of H + shift I")
     ap.add_argument("--serve-baseline", type=int, default=60)
     ap.add_argument("--group-count", type=int, default=512)
     ap.add_argument("--cpu-seconds", type=float, default=10.0)

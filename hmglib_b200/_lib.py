@@ -81,6 +81,13 @@ _PROTOS = {
     "hmg_gaussian_rhs": (C.c_int, [_vp, _vp]),
     "hmg_cg_solve": (C.c_int, [_vp, C.c_double, _vp, _vp, C.c_double, C.c_int, C.c_int,
                                C.POINTER(C.c_int), C.POINTER(C.c_double)]),
+    "hmg_cg_solve_multi": (C.c_int, [_vp, C.c_int, C.c_double, _vp, C.c_int, _vp, C.c_int, C.c_double,
+                                     C.c_int, C.c_int, C.POINTER(C.c_int), _vp]),
+    "hmg_cg_multi_begin": (C.c_int, [C.POINTER(_vp), _vp, C.c_int, C.c_double, _vp, C.c_int, _vp, C.c_int,
+                                     C.c_double, C.c_int, C.c_int]),
+    "hmg_cg_multi_advance": (C.c_int, [_vp, C.POINTER(C.c_int)]),
+    "hmg_cg_multi_poll": (C.c_int, [_vp, C.POINTER(C.c_int), C.POINTER(C.c_int), _vp]),
+    "hmg_cg_multi_end": (C.c_int, [_vp]),
     "hmg_synchronize": (C.c_int, [_vp]),
     "hmg_set_profiling": (C.c_int, [_vp, C.c_int]),
     "hmg_get_profile": (C.c_int, [_vp, _vp]),

@@ -133,6 +133,21 @@ class HMatrix:
                    1 if refine else 0, C.byref(it), C.byref(rel))
         return it.value, rel.value
 
+    def cg_solve_multi(self, B, X, shift: float, tol: float = 1e-8, maxit: int = 1000, refine: bool = True):
+        """Solve (H + shift I) X = B for the rows of device tensors B, X of shape
+        (nrhs, n) (column-major n x nrhs); X holds the initial guesses.  Returns
+        (iterations, per-column final relative residuals)."""
+        nrhs = int(B.shape[0])
+        it = C.c_int(0)
+        rel = np.zeros(nrhs)
+        self._call("hmg_cg_solve_multi", nrhs, float(shift), _ptr(B), int(B.stride(0)), _ptr(X),
+                   int(X.stride(0)), float(tol), int(maxit), 1 if refine else 0, C.byref(it), _ptr(rel))
+        return it.value, rel
+
+    def cg_multi(self, B, X, shift: float, tol: float = 1e-8, maxit: int = 1000, refine: bool = True):
+        """A step-driven block CG solve (hmg_cg_multi_*): see CgMulti."""
+        return CgMulti(self, B, X, shift, tol, maxit, refine)
+
     def gaussian_rhs(self, b):
         self._call("hmg_gaussian_rhs", _ptr(b))
         return b
@@ -228,6 +243,47 @@ class HMatrix:
         V = np.zeros((max(rank, 1), m2))
         self._call("hmg_get_factors", int(block), _ptr(U), _ptr(V))
         return U[:rank], V[:rank]
+
+
+class CgMulti:
+    """(H + shift I) X = B advanced one enqueued piece of work at a time: ``advance()``
+    enqueues at most one CG iteration (or a true residual and restart) on the
+    H-matrix's stream without waiting for the GPU and returns whether it did;
+    ``poll()`` returns (done, iterations, relative residuals) without blocking;
+    ``close()`` waits for the stream and frees the work vectors.  B and X (device
+    tensors of shape (nrhs, n)) must stay alive until then."""
+
+    def __init__(self, H: HMatrix, B, X, shift, tol, maxit, refine):
+        self._lib = H._lib
+        self._s = C.c_void_p()
+        self.nrhs = int(B.shape[0])
+        self._keep = (H, B, X)
+        L.check(self._lib.hmg_cg_multi_begin(C.byref(self._s), H._h, self.nrhs, float(shift), _ptr(B),
+                                             int(B.stride(0)), _ptr(X), int(X.stride(0)), float(tol), int(maxit),
+                                             1 if refine else 0), "hmg_cg_multi_begin")
+
+    def advance(self) -> bool:
+        e = C.c_int(0)
+        L.check(self._lib.hmg_cg_multi_advance(self._s, C.byref(e)), "hmg_cg_multi_advance")
+        return bool(e.value)
+
+    def poll(self):
+        done, it = C.c_int(0), C.c_int(0)
+        rel = np.zeros(self.nrhs)
+        L.check(self._lib.hmg_cg_multi_poll(self._s, C.byref(done), C.byref(it), _ptr(rel)), "hmg_cg_multi_poll")
+        return bool(done.value), it.value, rel
+
+    def close(self):
+        if self._s:
+            self._lib.hmg_cg_multi_end(self._s)
+            self._s = None
+            self._keep = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def load(path: str, stream: int | None = None) -> "HMatrix":

@@ -11,12 +11,14 @@ as they arrive:
   time, into one ``hmg_matvec_multi`` call (the stored H-matrix is read once for the
   whole batch).  A request that arrives while a batch is on the GPU joins the next.
 * ``Solve(mid, B, shift)``: kernel-ridge CG on (H + shift I) X = B for the columns of
-  B (at most MAX_SOLVES per H-matrix at a time, the others wait), advanced in lockstep: one multi-vector product per iteration for all columns,
-  the vector updates on the H-matrix's stream, residual norms read back
-  asynchronously (up to two iterations in flight, no host synchronisation), converged
-  columns frozen.  Solve iterations and product batches on the same H-matrix
-  interleave.  Products use the handle's arithmetic (FP32 by default), so the
-  attainable residual is ~1e-7 times the condition number.
+  B (at most MAX_SOLVES per H-matrix at a time, the others wait), run by the
+  library's block CG (``hmg_cg_multi_*``): one multi-vector product per iteration for
+  all columns, FP64 vector updates and inner products on the H-matrix's stream,
+  residual norms read back asynchronously (no host synchronisation), converged
+  columns frozen, and FP64-product refinement of the true residual, so the result
+  solves the stored operator to ``tol``.  Each poll of the loop enqueues at most one
+  iteration, so solve iterations and product batches on the same H-matrix
+  interleave.
 * ``Build(points, ...)``: a new point set compressed on a worker thread with its own
   stream, admitted only when the budget holds its estimated bytes (idle H-matrices
   built by earlier requests are evicted, least recently used first).
@@ -246,21 +248,20 @@ class Server:
         r.inflight.append((ev, finish, (X, Y)))
         r.last_use = now
 
-    # -- block CG (one multi-vector product per iteration) -------------------------
+    # -- block CG on the library (hmg_cg_multi_*: one multi-vector product per iteration) --
     def _start_solve(self, req: Solve):
         torch = self.torch
         r = self.res[req.mid]
         with torch.cuda.stream(r.stream):
             B = torch.from_numpy(np.ascontiguousarray(req.B)).pin_memory().cuda(non_blocking=True)
-            st = {"req": req, "B": B, "X": torch.zeros_like(B), "R": B.clone(), "P": B.clone(),
-                  "Q": torch.empty_like(B), "rr": (B * B).sum(1), "it": 0,
-                  "checks": collections.deque(), "final": None}
-            st["rr0"] = st["rr"].clone()
-            st["active"] = torch.ones(B.shape[0], dtype=torch.bool, device="cuda")
-        return st
+            X = torch.zeros_like(B)
+        cg = r.H.cg_multi(B, X, req.shift, tol=req.tol, maxit=req.maxit, refine=True)
+        return {"req": req, "B": B, "X": X, "cg": cg, "final": None, "events": collections.deque()}
 
     def _step_solve(self, r: _Resident, st, now: float):
-        """Advance one solve; True once its result has reached the host."""
+        """Advance one solve by at most one enqueued iteration; True once its result
+        has reached the host.  The library keeps the recurrence on the device and
+        decides convergence from residual norms read back asynchronously."""
         torch = self.torch
         req = st["req"]
         if st["final"] is not None:
@@ -269,56 +270,27 @@ class Server:
                 return False
             req.X, req.iters, req.relres, req.done = Xh.numpy().copy(), it, rel, time.perf_counter()
             self.iters_per_solve = ewma(self.iters_per_solve, float(it))
+            st["cg"].close()
             return True
-        # residual norms come back one iteration late; at most two iterations in flight
-        converged = False
-        while st["checks"] and st["checks"][0][0].query():
-            ev, host, it = st["checks"].popleft()
-            if st.get("last_ev") is not None:
-                r.iter_s = ewma(r.iter_s, st["last_ev"].elapsed_time(ev) * 1e-3)
-            st["last_ev"] = ev
-            rel = np.sqrt(host[0].numpy() / np.maximum(host[1].numpy(), 1e-300))
-            if (rel <= req.tol).all() or it >= req.maxit:
-                converged = True
-                break
-        with torch.cuda.stream(r.stream):
-            if converged:
+        # iteration timings: consecutive recorded events that have completed
+        evs = st["events"]
+        while len(evs) >= 2 and evs[1].query():
+            r.iter_s = ewma(r.iter_s, evs[0].elapsed_time(evs[1]) * 1e-3)
+            evs.popleft()
+        cg = st["cg"]
+        done, it, rel = cg.poll()
+        if done:
+            with torch.cuda.stream(r.stream):
                 Xh = torch.empty(st["X"].shape, dtype=torch.float64, pin_memory=True)
                 Xh.copy_(st["X"], non_blocking=True)
                 ev = torch.cuda.Event()
                 ev.record(r.stream)
-                st["final"] = (ev, Xh, rel, it)
-                st["checks"].clear()
-                return False
-            if len(st["checks"]) >= 2:
-                return False
-            P, Q, R, X = st["P"], st["Q"], st["R"], st["X"]
-            if P.shape[0] == 1:
-                r.H.matvec(P[0], Q[0])
-            else:
-                r.H.matvec_multi(P, Q)
-            Q.add_(P, alpha=req.shift)
-            pq = (P * Q).sum(1)
-            rr = st["rr"]
-            act = st["active"]
-            # converged columns are frozen (alpha = beta = 0)
-            alpha = torch.where(act & (pq > 0), rr / torch.where(pq > 0, pq, torch.ones_like(pq)),
-                                torch.zeros_like(pq))
-            X.addcmul_(alpha[:, None], P)
-            R.addcmul_(-alpha[:, None], Q)
-            rr_new = torch.where(act, (R * R).sum(1), rr)
-            beta = torch.where(act, rr_new / torch.where(rr > 0, rr, torch.ones_like(rr)), torch.zeros_like(rr))
-            P.mul_(beta[:, None]).add_(R)
-            st["active"] = act & (rr_new > (req.tol ** 2) * st["rr0"])
-            st["rr"] = rr_new
-            st["it"] += 1
-            host = (torch.empty(rr_new.shape, dtype=torch.float64, pin_memory=True),
-                    torch.empty(rr_new.shape, dtype=torch.float64, pin_memory=True))
-            host[0].copy_(rr_new, non_blocking=True)
-            host[1].copy_(st["rr0"], non_blocking=True)
+            st["final"] = (ev, Xh, rel, it)
+            return False
+        if cg.advance():
             ev = torch.cuda.Event(enable_timing=True)
             ev.record(r.stream)
-            st["checks"].append((ev, host, st["it"]))
+            evs.append(ev)
         r.last_use = now
         return False
 

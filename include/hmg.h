@@ -218,6 +218,38 @@ hmg_status hmg_matvec_multi(hmg_matrix* h, int nrhs, const double* X, int ldx, d
 hmg_status hmg_cg_solve(hmg_matrix* h, double shift, const double* b, double* x, double tol, int maxit,
                         int refine, int* iters, double* relres);
 
+/* Kernel-ridge solves with several right-hand sides: (H + shift I) X = B for
+ * 1 <= nrhs <= 64 columns (device FP64, column-major, leading dimensions ldb, ldx >=
+ * n; X holds the initial guesses and receives the solutions).  Every column runs its
+ * own conjugate-gradient recurrence; the columns share one hmg_matvec_multi product
+ * per iteration, and vectors, inner products, step lengths and stopping tests are
+ * FP64 on the device.  refine != 0 targets the stored operator applied in FP64 as
+ * hmg_cg_solve does: true residuals with FP64-arithmetic products, inner CG with
+ * FP64-arithmetic products until the largest relative residual is below
+ * 5e5 tol and the handle's arithmetic after that, restarts from the true residual.
+ * Stops when every column has |b_j - (H + shift I) x_j| <= tol |b_j| or after maxit
+ * iterations; iters (may be NULL) receives the iterations, relres[nrhs] (may be
+ * NULL) the final true relative residuals.  Synchronous.  No reference counterpart
+ * (kernel_system_assembler.h:47-48 is the shift). */
+hmg_status hmg_cg_solve_multi(hmg_matrix* h, int nrhs, double shift, const double* B, int ldb, double* X, int ldx,
+                              double tol, int maxit, int refine, int* iters, double* relres);
+
+/* The same solve driven step by step, for callers that interleave it with other
+ * work (a serving loop): hmg_cg_multi_begin allocates the solve's work vectors;
+ * each hmg_cg_multi_advance enqueues at most one piece of work on the handle's
+ * stream (one CG iteration, or a true residual and restart) and never waits for the
+ * GPU -- *enqueued (may be NULL) says whether it did; residual norms come back
+ * through pinned buffers, at most two iterations behind; hmg_cg_multi_poll (non-
+ * blocking) reports *done once the stopping test holds, with the iterations and the
+ * latest true relative residuals; hmg_cg_multi_end waits for the stream and frees
+ * the state.  B and X must stay valid until hmg_cg_multi_end. */
+typedef struct hmg_cg_multi hmg_cg_multi;
+hmg_status hmg_cg_multi_begin(hmg_cg_multi** out, hmg_matrix* h, int nrhs, double shift, const double* B, int ldb,
+                              double* X, int ldx, double tol, int maxit, int refine);
+hmg_status hmg_cg_multi_advance(hmg_cg_multi* s, int* enqueued);
+hmg_status hmg_cg_multi_poll(hmg_cg_multi* s, int* done, int* iters, double* relres);
+hmg_status hmg_cg_multi_end(hmg_cg_multi* s);
+
 /* b_i = prod_d sqrt(pi)/2 (erf(1 - x_id) - erf(-x_id)) for set 0, caller order, device b.
  * Replaces set_gaussian_kernel_rhs (hmglib.cu:403-439). */
 hmg_status hmg_gaussian_rhs(hmg_matrix* h, double* b);

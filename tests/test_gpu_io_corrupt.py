@@ -45,7 +45,7 @@ def test_load_refuses_corrupt_files(hmg, cuda, tmp_path):
     nd, nb = L["ndense"], L["nblocks"]
     b = nd + int(np.argmax(ranks[nd:] > 0))  # an admissible block with factors
     # a block range past the last row
-    msg = _refused(hmg, path, buf, [(L["blocks"]["m1"] + 4 * b, "<i", n1)])
+    msg = _refused(hmg, path, buf, [(L["blocks"]["m1"] + 4 * b, "<i", n1 + 1)])
     assert "outside" in msg
     # a negative column start
     _refused(hmg, path, buf, [(L["blocks"]["c0"] + 4 * 3, "<i", -1)])
