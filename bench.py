@@ -213,6 +213,57 @@ def multi_rhs_timing(torch, H, x, n, nrhs, steps, stream, world, err1):
             "err_vs_fp64_col0": err1 + diff, "col0_vs_single": diff}
 
 
+def onchip_tensor_cores(torch, hmg, H, x, n, steps, stream, world, peak, nrhs=64):
+    """64 vectors a pass on the tensor cores over the handle's own (mixed) storage: the
+    pass kernels convert factors and near field into three BF16 parts on chip
+    (HMG_PREC_BF16X6_ONCHIP).  Error against FP64 direct sums on 2,048 rows of four of
+    the vectors; e2e includes copying X in and Y out through pinned host memory."""
+    from hmglib_b200 import synth
+    t0 = time.perf_counter()
+    H.build_bf16_factors(near=hmg.PREC_BF16X6_ONCHIP)
+    t_plan = time.perf_counter() - t0
+    X = torch.from_numpy(synth.rhs_vector(n, 11, nrhs)).cuda()
+    Y = torch.empty_like(X)
+    for _ in range(2):
+        H.matvec_multi(X, Y)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(int(os.environ.get("LOCAL_RANK", "0"))) as clk:
+        e0.record(stream)
+        for _ in range(steps):
+            H.matvec_multi(X, Y)
+        e1.record(stream)
+        torch.cuda.synchronize()
+    ms = max_over_ranks([e0.elapsed_time(e1) / steps], world, "cuda")[0]
+    # end to end: X from pinned host memory in, Y out, every step
+    Xh = torch.from_numpy(synth.rhs_vector(n, 11, nrhs)).pin_memory()
+    Yh = torch.empty(Y.shape, dtype=torch.float64, pin_memory=True)
+    e0.record(stream)
+    for _ in range(steps):
+        X.copy_(Xh, non_blocking=True)
+        H.matvec_multi(X, Y)
+        Yh.copy_(Y, non_blocking=True)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms_e2e = e0.elapsed_time(e1) / steps
+    rng = np.random.default_rng(3)
+    rows = torch.from_numpy(rng.choice(n, 2048, replace=False).astype(np.int32)).cuda()
+    errs = []
+    for j in (0, 21, 42, nrhs - 1):
+        yd = torch.empty(rows.shape[0], dtype=torch.float64, device="cuda")
+        H.full_matvec_rows(X[j], rows, yd)
+        torch.cuda.synchronize()
+        errs.append(float(torch.linalg.norm(Y[j][rows.long()] - yd) / torch.linalg.norm(yd)))
+    info = H.info()
+    stored = info["near_bytes"] + info["far_bytes"]
+    return {"n": n, "nrhs": nrhs, "operands": "3 BF16 parts converted on chip from the mixed storage",
+            "ms_per_product": ms, "value": nrhs * world * 1000.0 / ms, "unit": "vector products/s",
+            "e2e_value": nrhs * world * 1000.0 / ms_e2e, "err_vs_fp64_max": max(errs),
+            "err_vs_fp64_cols": errs, "stored_bytes": stored,
+            "stored_GBps": stored / (ms * 1e-3) / 1e9, "stored_frac_of_peak": stored / (ms * 1e-3) / 1e9 / peak,
+            "plan_s": t_plan, "clocks": clk.summary()}
+
+
 def batched_tensor_cores(steps):
     """Batched products on the tensor cores at error <= 1e-6 beside the plain FP64 form,
     at N = 2^18 points of this workload: the largest power of two at which the FP32
@@ -462,6 +513,8 @@ def run_engine(a, rank, world):
                 key, prec = modes[name]
                 H.build_bf16_factors(near=prec)
                 line[key] = multi_rhs_timing(torch, H, x, n, a.nrhs, a.steps, stream, world, err)
+    if a.nrhs > 1 and not a.no_onchip:
+        line["onchip_tensor_cores"] = onchip_tensor_cores(torch, hmg, H, x, n, a.steps, stream, world, peak)
     if rank == 0 and world == 1 and not a.no_cpu:
         kind = O.KERNEL_MATERN32
         rate, nrows, dt, thr = cpu_direct_rate(p, x, kind, O.kernel_param(kind, W["rho"]), target_s=a.cpu_seconds)
@@ -989,6 +1042,8 @@ def main(argv=None):
     ap.add_argument("--group-count", type=int, default=512)
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-onchip", action="store_true",
+                    help="skip the 64-vector tensor-core products over the mixed storage (on-chip operands)")
     ap.add_argument("--no-batched-tc", action="store_true",
                     help="skip the tensor-core batched products at N=2^18 beside the FP64 form")
     a = ap.parse_args(argv)

@@ -27,6 +27,7 @@ PREC_MIXED = 2
 PREC_BF16 = 3
 PREC_BF16X3 = 4
 PREC_BF16X6 = 5
+PREC_BF16X6_ONCHIP = 6
 NEAR_STORED = 0
 NEAR_ONTHEFLY = 1
 
@@ -45,7 +46,8 @@ class Info(C.Structure):
                 ("near_bytes", C.c_int64), ("far_bytes", C.c_int64), ("matvec_bytes", C.c_int64),
                 ("near_precision", C.c_int), ("far_precision", C.c_int), ("near_mode", C.c_int),
                 ("far_u_bytes", C.c_int64), ("far_v_bytes", C.c_int64), ("matvec_launches", C.c_int),
-                ("group_count", C.c_int), ("tc_parts", C.c_int), ("tc_bytes", C.c_int64)]
+                ("group_count", C.c_int), ("tc_parts", C.c_int), ("tc_bytes", C.c_int64),
+                ("tc_onchip", C.c_int)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}

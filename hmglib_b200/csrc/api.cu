@@ -237,11 +237,15 @@ hmg_status hmg_build_tensor_core_operands(hmg_matrix* h, int near_precision)
 {
     HMG_REQUIRE(h, HMG_ERR_INVALID, "hmg_build_tensor_core_operands: NULL handle");
     HMG_REQUIRE(near_precision == HMG_PREC_BF16 || near_precision == HMG_PREC_FP32 ||
-                    near_precision == HMG_PREC_BF16X3 || near_precision == HMG_PREC_BF16X6,
+                    near_precision == HMG_PREC_BF16X3 || near_precision == HMG_PREC_BF16X6 ||
+                    near_precision == HMG_PREC_BF16X6_ONCHIP,
                 HMG_ERR_INVALID,
                 "hmg_build_tensor_core_operands: precision %d is not HMG_PREC_BF16, HMG_PREC_FP32, "
-                "HMG_PREC_BF16X3 or HMG_PREC_BF16X6",
+                "HMG_PREC_BF16X3, HMG_PREC_BF16X6 or HMG_PREC_BF16X6_ONCHIP",
                 near_precision);
+    HMG_REQUIRE(h->setup_done && h->kernel_set && (h->naca == 0 || h->far_prec >= 0), HMG_ERR_STATE,
+                "hmg_build_tensor_core_operands: the H-matrix is not compressed");
+    if (near_precision == HMG_PREC_BF16X6_ONCHIP) return build_tcm(h);
     const int parts = near_precision == HMG_PREC_BF16X6 ? 3 : near_precision == HMG_PREC_BF16X3 ? 2 : 1;
     return build_bf16_factors(h, near_precision != HMG_PREC_FP32, parts);
 }
@@ -489,8 +493,9 @@ hmg_status hmg_get_info(hmg_matrix* h, hmg_info* info)
         }
     info->matvec_launches = 1 + (int)tier[0] + (int)tier[1] + (int)tier[2] + (h->ntiles > 0 ? 1 : 0);
     info->group_count = h->group_count;
-    info->tc_parts = h->tc_ready ? h->tc_parts : 0;
+    info->tc_parts = h->tc_ready ? h->tc_parts : (h->tcm_ready ? 3 : 0);
     info->tc_bytes = h->tc_ready ? h->tc_bytes * h->tc_parts : 0;
+    info->tc_onchip = h->tcm_ready ? 1 : 0;
     info->far_u_bytes = h->far_alg_u;
     info->far_v_bytes = h->far_alg_v;
     if (h->near_mode == HMG_NEAR_STORED && h->near_prec >= 0) mb += ne * nes;

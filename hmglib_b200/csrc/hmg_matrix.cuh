@@ -101,6 +101,18 @@ struct hmg_matrix {
     long long tc_xkc = 0, tc_tkc = 0;         // per product: K cores of X, of t_b (8 columns / terms each)
     long long tc_bytes = 0;                   // bytes of one part of the BF16 operands
 
+    // ---- tensor-core products with operands converted on chip (tcm.cu) ------------
+    bool tcm_ready = false;
+    char* tcm_steps[2] = {nullptr, nullptr};  // per pass: steps, CTA by CTA
+    char* tcm_jobs[2] = {nullptr, nullptr};   // per pass: jobs, CTA by CTA
+    char* tcm_cta[2] = {nullptr, nullptr};    // per CTA: first job and step (int2), then the ends
+    void* tcm_stacks = nullptr;               // pass 1: the stacks of V_b^T
+    int* tcm_kmap = nullptr;                  // pass 1: per stack, t_b destination of its 16 K cores
+    int tcm_njobs[2] = {0, 0};
+    long long tcm_xkc = 0, tcm_tkc = 0;       // K cores of X, of t_b
+    void* tcm_bbuf = nullptr;                 // per product: X cores, then t_b cores (3 parts, 64 vectors)
+    bool tcm_all_tiles = false;               // every row tile has a pass-2 job
+
     // ---- matvec workspace -------------------------------------------------------
     double* xs64 = nullptr;   // Z-ordered x
     float* xs32 = nullptr;
@@ -146,6 +158,9 @@ hmg_status matvec_unbatched(hmg_matrix* h, const double* x, double* y);
 hmg_status matvec_multi(hmg_matrix* h, int nrhs, const double* X, int ldx, double* Y, int ldy);
 hmg_status matvec_multi_tc(hmg_matrix* h, int nrhs, const double* X, int ldx, double* Y, int ldy);
 hmg_status build_bf16_factors(hmg_matrix* h, bool near_on_tensor_cores, int parts);
+hmg_status build_tcm(hmg_matrix* h);
+hmg_status matvec_multi_tcm(hmg_matrix* h, int nrhs, const double* X, int ldx, double* Y, int ldy);
+void free_tcm(hmg_matrix* h);
 hmg_status autotune(hmg_matrix* h, int reps, int* best_piece, int* best_ctas, double* best_ms);
 void free_tc(hmg_matrix* h);
 void free_product_graph(hmg_matrix* h);

@@ -256,7 +256,7 @@ class Server:
             B = torch.from_numpy(np.ascontiguousarray(req.B)).pin_memory().cuda(non_blocking=True)
             X = torch.zeros_like(B)
         cg = r.H.cg_multi(B, X, req.shift, tol=req.tol, maxit=req.maxit, refine=True)
-        return {"req": req, "B": B, "X": X, "cg": cg, "final": None, "events": collections.deque()}
+        return {"req": req, "B": B, "X": X, "cg": cg, "final": None, "events": collections.deque(), "it": 0}
 
     def _step_solve(self, r: _Resident, st, now: float):
         """Advance one solve by at most one enqueued iteration; True once its result
@@ -279,6 +279,7 @@ class Server:
             evs.popleft()
         cg = st["cg"]
         done, it, rel = cg.poll()
+        st["it"] = it
         if done:
             with torch.cuda.stream(r.stream):
                 Xh = torch.empty(st["X"].shape, dtype=torch.float64, pin_memory=True)

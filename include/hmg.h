@@ -58,6 +58,12 @@ typedef enum {
 #define HMG_PREC_BF16 3
 #define HMG_PREC_BF16X3 4
 #define HMG_PREC_BF16X6 5
+/* Tensor-core operands converted on chip: no copy is stored.  The product kernels read
+ * the handle's own FP32 near field and FP32 or mixed factors and split every value
+ * into three BF16 parts in shared memory (FP16 and FP8 terms are exact in two and one
+ * parts and run fewer MMAs); accuracy as HMG_PREC_BF16X6, memory only for the X and
+ * t_b operands of a product (6 bytes x 64 vectors per column and per term). */
+#define HMG_PREC_BF16X6_ONCHIP 6
 
 /* near-field mode for hmg_matvec */
 #define HMG_NEAR_STORED 0   /* read the blocks stored by hmg_precompute_dense          */
@@ -80,7 +86,8 @@ typedef struct {
     int matvec_launches;      /* kernels one hmg_matvec launches (plain-load kernels) */
     int group_count;          /* sets of a group handle (hmg_group_create), else 0 */
     int tc_parts;             /* BF16 parts per tensor-core operand (0: none built) */
-    int64_t tc_bytes;         /* bytes of the tensor-core operands, all parts */
+    int64_t tc_bytes;         /* bytes of the stored tensor-core operands, all parts */
+    int tc_onchip;            /* 1: tensor-core operands converted on chip (HMG_PREC_BF16X6_ONCHIP) */
 } hmg_info;
 
 /* message of the last failed call on this thread ("" if none) */
@@ -166,6 +173,13 @@ hmg_status hmg_full_matvec_rows(hmg_matrix* h, const double* x, const int* rows,
  * The copies sit beside the FP32 storage (hmg_info.tc_bytes; one part holds ~0.6x its
  * bytes).  Single-vector products keep using the FP32 storage.  Recomputing the
  * factors or the near field drops the copies.
+ * HMG_PREC_BF16X6_ONCHIP stores no copy: it plans the same two passes over the
+ * handle's own storage -- FP32 or mixed (HMG_PREC_MIXED) factors and the FP32 near
+ * field -- and the pass kernels split every value into three BF16 parts on chip while
+ * they stream it (FP16 / FP8 terms into the parts that hold them exactly, with fewer
+ * MMAs).  Products agree with FP64 to ~4e-7 like HMG_PREC_BF16X6, and the only memory
+ * added is the X and t_b operand buffer (3 x 2 bytes x 64 vectors per column and per
+ * term): this is the form that fits at N = 2^20.
  * hmg_build_bf16_factors(h) is hmg_build_tensor_core_operands(h, HMG_PREC_BF16). */
 hmg_status hmg_build_tensor_core_operands(hmg_matrix* h, int near_precision);
 hmg_status hmg_build_bf16_factors(hmg_matrix* h);
