@@ -107,7 +107,7 @@ struct hmg_matrix {
     char* tcm_jobs[2] = {nullptr, nullptr};   // per pass: jobs, CTA by CTA
     char* tcm_cta[2] = {nullptr, nullptr};    // per CTA: first job and step (int2), then the ends
     void* tcm_stacks = nullptr;               // pass 1: the stacks of V_b^T
-    int* tcm_kmap = nullptr;                  // pass 1: per stack, t_b destination of its 16 K cores
+    float* tcm_tscale = nullptr;              // pass 1: scale of every t_b term (FP16 / FP8 terms), else 1
     int tcm_njobs[2] = {0, 0};
     long long tcm_xkc = 0, tcm_tkc = 0;       // K cores of X, of t_b
     void* tcm_bbuf = nullptr;                 // per product: X cores, then t_b cores (3 parts, 64 vectors)

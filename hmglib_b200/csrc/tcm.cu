@@ -5,33 +5,44 @@
 // storage; with three parts (24 bits) those copies take 1.73x the FP32 bytes, so at
 // N = 2^20 they do not fit.  Here nothing is copied: the pass kernels read the
 // handle's own storage -- FP32 near-field slices and FP32 or mixed FP32 / FP16 / FP8
-// factors (the layouts of hmg_internal.cuh) -- and converter warps split every value
-// into three BF16 parts (hi, the rounding of what hi misses, the rounding of what both
-// miss) in shared memory, in the canonical K-major core layout of the MMA:
+// factors (the layouts of hmg_internal.cuh) -- and split every value on chip into
+// three BF16 parts (hi, then what hi misses, then what both miss), in the canonical
+// K-major core layout of the MMA:
 //
 //   pass 1 (k_tcm_pass<0>): per stack of V_b^T with the same columns (M = stacked
 //     terms <= 128, K = the columns, N = the vectors): t_b = V_b^T X_b, times the
-//     terms' scales (FP16 / FP8 terms are stored scaled), written as BF16 operand cores
-//     of pass 2 (three parts);
-//   pass 2 (k_tcm_pass<1>): per row tile (M = 128 rows), the sum over its pairs of
+//     terms' scales (FP16 / FP8 terms are stored scaled), written as the three-part
+//     BF16 operand cores of pass 2;
+//   pass 2 (k_tcm_pass<1>): per row tile (M <= 128 rows), the sum over its pairs of
 //     U_slice t_b (K = terms) and D_slice X_b (K = columns), written to Y rows.
 //
 // A step is 32 K positions (4 K cores) of one pair or stack.  Roles of a CTA (one per
-// SM, persistent, 10 warps):
-//   warps 6-9, the converters: warp g converts the steps i = g (mod 4) into stage i mod
-//     5 -- coalesced loads from HBM (several items' loads in flight per lane), the 3-part
-//     split on the CUDA cores, 16-byte shared stores, a proxy fence, then an arrival on
-//     the stage's "full" barrier; four steps' loads are in flight per SM;
-//   warp 4, lane 0: the B operand of each step (3-part X or t_b cores, mostly L2) by one
-//     bulk copy into the same stage, counted on the same barrier;
-//   warp 5, lane 0: the MMAs of a step (per K16: hi*hi into one accumulator and the
-//     correction terms into another -- 5 of them when the step holds FP32 values, 2 when
-//     it holds FP16 terms only, none for FP8 terms only, whose BF16 parts are exact with
-//     fewer), then tcgen05.commit frees the stage and signals the accumulators;
-//   warps 0-3: drain both accumulators after every step (tcgen05.ld) and keep the sums
-//     in FP32 registers, so no tensor-core accumulation runs longer than one step.
-// Every wait is bounded (pipeline.cuh); on a time-out the CTA records an error code in
-// the handle's flag, waits for its own copies and MMAs and frees tensor memory.
+// SM, persistent, 12 warps), each a ring of stages with its own full / empty barriers:
+//   warp 6, the raw producer: copies the stored bytes of a step (pass 2: one run of
+//     whole slice columns; pass 1: 9 16-byte chunks of every V row of the stack, the
+//     out-of-range ones zero-filled) into one of 5 raw stages with 16-byte cp.async,
+//     L2 evict-first, and writes the step's header (geometry, pass 1's row table);
+//   warps 7-11, the converters: all five share each step, an item being 32 rows x 1
+//     K core (one 16-byte row of each part per lane): they read the raw stage
+//     (conflict-free), decode FP16 / FP8 with warp-uniform branches, split, and store
+//     the parts into one of 3 A stages in shared memory;
+//   warp 4, lane 0: the B operand of each step (3-part X or t_b cores) by one bulk
+//     copy into one of 3 B stages;
+//   warp 5, lane 0: the MMAs of a step.  The parts of a B K core lie side by side
+//     along N, so per K16 one MMA of N = 3 NV gives A0 B0 (hi), A0 B1 and A0 B2, one of
+//     N = 2 NV adds A1 B0 and A1 B1 to the last two, and one of N = NV adds A2 B0 to the
+//     first correction: every part of A is read once, into three accumulators (hi,
+//     c1 = A0 B1 + A1 B0 + A2 B0, c2 = A0 B2 + A1 B1).  A step that starts in the FP16
+//     terms (A exact in two parts) runs A0 [B0 B1] and A1 B0; one in the FP8 terms
+//     (exact in one part) A0 B0.  tcgen05.commit then frees the A and B stages and
+//     signals the accumulators;
+//   warps 0-3: drain the accumulators after every step (tcgen05.ld) and keep the sums
+//     hi + (c1 + c2) in FP32 registers, so no tensor-core accumulation runs longer than
+//     one step.
+// Every role reads its per-step records 32 at a time (one per lane) and the epilogue
+// prefetches the next job's rows, so no role waits on a global load per step.  Every
+// wait is bounded (pipeline.cuh); on a time-out the CTA records an error code in the
+// handle's flag, waits for its own copies and MMAs and frees tensor memory.
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
 #include <cuda_fp8.h>
@@ -47,268 +58,269 @@
 
 namespace hmg {
 
-static constexpr int TCM_NMAX = 64;                         // vectors per pass at most
-static constexpr int TCM_STAGES = 5;                        // stages of the converted-operand ring
-static constexpr int TCM_KC = 4;                            // K cores per step (32 K positions)
-static constexpr int TCM_PARTS = 3;                         // BF16 parts of every operand
-static constexpr int TCM_AST = TCM_KC * TCM_PARTS * 16 * 128;        // A of a step: 128 rows, 24 KB
-static constexpr int TCM_BST = TCM_KC * TCM_PARTS * TCM_NMAX * 16;   // B of a step at 64 vectors, 12 KB
-static constexpr int TCM_GROUPS = 4;                        // converter groups (steps in conversion at once)
-static constexpr int TCM_GWARPS = 1;                        // warps per converter group
-static constexpr int TCM_THREADS = (6 + TCM_GROUPS * TCM_GWARPS) * 32;
-static constexpr int TCM_MAXMEM = 8;                        // blocks of a pass-1 stack (ranks rounded to 16)
+static constexpr int TCM_NMAX = 64;                          // vectors per pass at most
+static constexpr int TCM_KC = 4;                             // K cores per step (32 K positions)
+static constexpr int TCM_PARTS = 3;                          // BF16 parts of every operand
+static constexpr int TCM_NR = 5;                             // raw stages
+static constexpr int TCM_NA = 3;                             // converted A stages
+static constexpr int TCM_NB = 3;                             // B stages
+static constexpr int TCM_RROW = 144;                         // pass 1: bytes of a raw V row (9 chunks)
+static constexpr int TCM_RAW = 128 * TCM_RROW;               // a raw stage (>= 32 columns x 128 rows x 4)
+static constexpr int TCM_AST = TCM_KC * TCM_PARTS * 16 * 128;       // A of a step: 128 rows, 24 KB
+static constexpr int TCM_BST = TCM_KC * TCM_PARTS * TCM_NMAX * 16;  // B of a step at 64 vectors, 12 KB
+static constexpr int TCM_TMEM_COLS = 512;                    // two buffers of 3 NV accumulator columns
+static constexpr int TCM_CONV = 5;                           // converter warps
+static constexpr int TCM_THREADS = (7 + TCM_CONV) * 32;
+static constexpr int TCM_MAXMEM = 8;                         // blocks of a pass-1 stack (ranks rounded to 16)
+static constexpr int TCM_STGR = 40;                          // pass 1 epilogue staging: row stride (BF16)
+static_assert(2 * 3 * TCM_NMAX <= TCM_TMEM_COLS, "accumulators exceed the tensor memory allocation");
 
+// One step.  Pass 2 (one pair): raw = first byte of its raw copy, n16 chunks of 16
+// bytes; cc0 = the slice's chunk column there (a column of s_pad FP32 rows, a column of
+// FP16 pairs or of FP8 quads); near pair: t0 = a = c0 mod 8 (K position of column 0),
+// t1 = m2, t2 = -1; low-rank pair: K positions < t0 are FP32 terms, < t1 FP16, < t2
+// FP8.  Pass 1 (one stack): n16 = the stack, cc0 = first 16-byte chunk of the step's
+// columns in a V row (may be negative), t0 = a, t1 = 16-byte chunks of a V row.
 struct TcmStep {
+    const char* raw;
     long long b_kc;  // first K core of B in the operand buffer (X cores, then t_b cores)
-    int src;         // pass 1: stack index; pass 2: pair index
-    int kp0;         // first K position of the step
     int meta;        // bits 0-1: K16 groups (1 or 2); bit 8: first step of a job; bit 9: last;
                      // bits 12-15: MMAs per K16 (1, 3 or 6)
     int rows;        // rows of the job's M (tile rows or stack rows)
+    int kp0;         // first K position of the step
+    int n16;
+    int cc0;
+    int t0, t1, t2;
 };
-static_assert(sizeof(TcmStep) == 24, "TcmStep layout");
+static_assert(sizeof(TcmStep) == 48, "TcmStep layout");
 
-// pass-1 job: the V^T of blocks with the same columns, one under the other
+// pass-1 job: the V^T of blocks with the same columns, one under the other.  A block's
+// V^T is a run of 16-byte-aligned rows of m2p words -- r32 FP32 term rows, r16 / 2 FP16
+// pair rows, r8 / 4 FP8 quad rows -- and raw row q of the stack is row q - qb[k] of
+// member k.  rtab[m] for stack row m: raw row (bits 0-7), tier (bits 8-9: 0 FP32, 1
+// FP16, 2 FP8, 3 none) and the term's place in its pair or quad (bits 10-11).
 struct TcmStack {
-    int c0, m2, rows, nmem;
-    int blk[TCM_MAXMEM];
-    int off[TCM_MAXMEM];  // first stack row of each block (a multiple of 16)
+    const char* vptr[TCM_MAXMEM];
+    int qb[TCM_MAXMEM];
+    int nmem, nq, m2p4, pad;
+    uint16_t rtab[128];
 };
+static_assert(sizeof(TcmStack) == 368, "TcmStack layout");
 
 struct TcmJob {
-    int r0;    // pass 2: first Z row of the tile; pass 1: the stack
+    int r0;    // pass 2: first Z row of the tile; pass 1: first t_b term of the stack
     int rows;  // pass 2: rows of the tile; pass 1: stack rows
 };
 
+// written by the raw producer beside each raw stage
+struct TcmHdr {
+    int kp0, meta, rows, cc0, t0, t1, t2, pad;
+    uint16_t rtab[128];
+};
+
 struct TcmSmem {
-    unsigned char a[TCM_STAGES][TCM_AST];
-    unsigned char b[TCM_STAGES][TCM_BST];
-    __nv_bfloat16 stg[4][32 * TCM_NMAX];  // pass 1 epilogue: 4 K cores of t_b per warp
-    uint64_t full[TCM_STAGES], empty[TCM_STAGES], accf[2], acce[2], fin;
+    unsigned char raw[TCM_NR][TCM_RAW];
+    unsigned char a[TCM_NA][TCM_AST];
+    unsigned char b[TCM_NB][TCM_BST];
+    __nv_bfloat16 stg[4][TCM_NMAX * TCM_STGR];  // pass 1 epilogue: per warp, [vector][row] of t_b
+    TcmHdr hdr[TCM_NR];
+    const char* rowptr[128];                    // raw producer, pass 1: the stack's V rows
+    uint64_t raw_full[TCM_NR], raw_empty[TCM_NR], a_full[TCM_NA], a_empty[TCM_NA], b_full[TCM_NB], b_empty[TCM_NB];
+    uint64_t accf[2], acce[2], fin;
     uint32_t tmem;
     int fail;
 };
 static_assert(sizeof(TcmSmem) <= 227 * 1024, "TcmSmem exceeds the shared memory of a CTA");
 
 // ---------------------------------------------------------------------------
-// decoding the stored values
+// copies and decoding
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ float fp8_value(unsigned byte)
+__device__ __forceinline__ void cpa16(void* dst, const void* src, unsigned n, uint64_t pol)
 {
-    const __half_raw h = __nv_cvt_fp8_to_halfraw((__nv_fp8_storage_t)byte, __NV_E4M3);
-    return __half2float(__half(h));
+    asm volatile("cp.async.cg.shared.global.L2::cache_hint [%0], [%1], 16, %2, %3;" ::"r"(smem_u32(dst)), "l"(src),
+                 "r"(n), "l"(pol)
+                 : "memory");
 }
 
-__device__ __forceinline__ float half_value(unsigned word, int hi)
+// arrives on bar once every cp.async this thread issued so far has landed
+__device__ __forceinline__ void cpa_arrive(uint64_t* bar)
 {
-    const unsigned short u = (unsigned short)(hi ? word >> 16 : word & 0xffffu);
-    __half_raw r;
-    r.x = u;
-    return __half2float(__half(r));
+    asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" ::"r"(smem_u32(bar)) : "memory");
 }
 
-// the three BF16 parts of 8 values of one operand row, one uint4 (8 K positions) each
-__device__ __forceinline__ void split3(const float (&v)[8], uint4& p0, uint4& p1, uint4& p2)
+__device__ __forceinline__ float2 h2f2(unsigned w)
+{
+    __half2 h;
+    *reinterpret_cast<unsigned*>(&h) = w;
+    return __half22float2(h);
+}
+
+__device__ __forceinline__ float2 e4m3x2_f2(unsigned w16)
+{
+    const __half2_raw hr = __nv_cvt_fp8x2_to_halfraw2((__nv_fp8x2_storage_t)(w16 & 0xffffu), __NV_E4M3);
+    return __half22float2(*reinterpret_cast<const __half2*>(&hr));
+}
+
+// 8 FP8 values starting at byte p (0..3) of the 12 bytes w0 w1 w2
+__device__ __forceinline__ void fp8_run(unsigned w0, unsigned w1, unsigned w2, int p, float (&v)[8])
+{
+    const unsigned sel = 0x3210u + 0x1111u * (unsigned)p;
+    const unsigned lo = __byte_perm(w0, w1, sel), hi = __byte_perm(w1, w2, sel);
+    const float2 a = e4m3x2_f2(lo), b = e4m3x2_f2(lo >> 16), c = e4m3x2_f2(hi), d = e4m3x2_f2(hi >> 16);
+    v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
+    v[4] = c.x; v[5] = c.y; v[6] = d.x; v[7] = d.y;
+}
+
+// the parts of 8 values of one operand row, one uint4 (8 K positions) each: part 0 is
+// the BF16 rounding, each further part the rounding of what the parts before miss
+// (exact differences in FP32; three parts hold an FP32 value exactly)
+__device__ __forceinline__ void store_parts(unsigned char* stage, int kc, int m, const float (&v)[8], int nparts)
 {
     uint32_t w0[4], w1[4], w2[4];
 #pragma unroll
     for (int k = 0; k < 4; k++) {
         const float a = v[2 * k], b = v[2 * k + 1];
         const __nv_bfloat162 h = __floats2bfloat162_rn(a, b);
-        const float2 hf = __bfloat1622float2(h);
-        const float ra = a - hf.x, rb = b - hf.y;
-        const __nv_bfloat162 l = __floats2bfloat162_rn(ra, rb);
-        const float2 lf = __bfloat1622float2(l);
-        const __nv_bfloat162 l2 = __floats2bfloat162_rn(ra - lf.x, rb - lf.y);
         w0[k] = *reinterpret_cast<const uint32_t*>(&h);
-        w1[k] = *reinterpret_cast<const uint32_t*>(&l);
-        w2[k] = *reinterpret_cast<const uint32_t*>(&l2);
+        if (nparts > 1) {
+            const float2 hf = __bfloat1622float2(h);
+            const float ra = a - hf.x, rb = b - hf.y;
+            const __nv_bfloat162 l = __floats2bfloat162_rn(ra, rb);
+            w1[k] = *reinterpret_cast<const uint32_t*>(&l);
+            if (nparts > 2) {
+                const float2 lf = __bfloat1622float2(l);
+                const __nv_bfloat162 l2 = __floats2bfloat162_rn(ra - lf.x, rb - lf.y);
+                w2[k] = *reinterpret_cast<const uint32_t*>(&l2);
+            }
+        }
     }
-    p0 = make_uint4(w0[0], w0[1], w0[2], w0[3]);
-    p1 = make_uint4(w1[0], w1[1], w1[2], w1[3]);
-    p2 = make_uint4(w2[0], w2[1], w2[2], w2[3]);
-}
-
-// row `m` of K core `kc` of a step's A stage: part q at ((kc * 3 + q) * 16 + m / 8) * 128 + (m % 8) * 16
-__device__ __forceinline__ void store_row(unsigned char* stage, int kc, int m, const float (&v)[8])
-{
-    uint4 p0, p1, p2;
-    split3(v, p0, p1, p2);
+    // row m of K core kc, part q: ((kc * 3 + q) * 16 + m / 8) * 128 + (m % 8) * 16
     unsigned char* base = stage + ((size_t)(kc * TCM_PARTS) * 16 + (m >> 3)) * 128 + (m & 7) * 16;
-    *reinterpret_cast<uint4*>(base) = p0;
-    *reinterpret_cast<uint4*>(base + 16 * 128) = p1;
-    *reinterpret_cast<uint4*>(base + 2 * 16 * 128) = p2;
+    *reinterpret_cast<uint4*>(base) = make_uint4(w0[0], w0[1], w0[2], w0[3]);
+    if (nparts > 1) *reinterpret_cast<uint4*>(base + 16 * 128) = make_uint4(w1[0], w1[1], w1[2], w1[3]);
+    if (nparts > 2) *reinterpret_cast<uint4*>(base + 2 * 16 * 128) = make_uint4(w2[0], w2[1], w2[2], w2[3]);
 }
 
-// Pass 2: a converter warp's items of a step, an item being 4 consecutive rows of one
-// K core (8 K positions x 4 rows, one 16-byte load per K position).  Near slices are
-// FP32 column-major (s_pad rows, column j at K position a + j, a = c0 mod 8); U slices
-// are chunk columns of s_pad * 4 bytes: r32 FP32 terms, r16 / 2 FP16 pairs, r8 / 4 FP8
-// quads.  Two items per lane are loaded before either is converted (16 loads in flight).
-__device__ __forceinline__ void convert_pass2(const PairDesc& d, int rows, int kp0, int nkc, unsigned char* stage,
-                                              int lane)
+// Pass 2, one item: row m (lane) of K core kc.  Word (c, m) of raw chunk column c is at
+// rw[(c - cc0) * sp + m]: consecutive lanes read consecutive words.
+__device__ __forceinline__ void load_pass2(const TcmHdr& H, const unsigned* rw, int sp, int m, int k0, float (&v)[8])
 {
-    const int sp = (rows + 3) & ~3, nq = sp >> 2, n = nq * nkc;
-    const bool near = d.kind == PAIR_STORED;
-    const bool mixed = d.kind == PAIR_FAR_MIXED;
-    const int a = d.c0 & 7, m2 = d.ncol;
-    const int r32 = d.ncol, r16 = mixed ? d.c0 : 0, r = r32 + r16 + (mixed ? d.pad : 0);
-    const char* slice = static_cast<const char*>(d.data);
-    const char* s16 = slice + (size_t)sp * 4 * r32;
-    const char* s8 = s16 + (size_t)sp * 2 * r16;
-    // tier of K position kp: 0 FP32 (or near), 1 FP16, 2 FP8, 3 none (zero)
-    auto tier_of = [&](int kp) -> int {
-        if (near) return (kp - a >= 0 && kp - a < m2) ? 0 : 3;
-        return kp < r32 ? 0 : (kp < r32 + r16 ? 1 : (kp < r ? 2 : 3));
-    };
-    for (int base = 0; base < n; base += 64) {
-        uint4 w[2][8];
+    const int cc0 = H.cc0;
+    auto word = [&](int c) -> unsigned { return rw[(c - cc0) * sp + m]; };
+    if (H.t2 < 0) {  // near slice: FP32 columns [0, m2) at K positions a ..
+        const int j0 = k0 - H.t0, m2 = H.t1;
+        if (j0 >= 0 && j0 + 8 <= m2) {
 #pragma unroll
-        for (int u = 0; u < 2; u++) {
-            const int it = base + 32 * u + lane;
-            const int kc = it / nq, i4 = it - kc * nq;
+            for (int e = 0; e < 8; e++) v[e] = __uint_as_float(word(j0 + e));
+        } else {
 #pragma unroll
-            for (int e = 0; e < 8; e++) {
-                const int kp = kp0 + kc * 8 + e, t = it < n ? tier_of(kp) : 3;
-                const char* p = nullptr;
-                if (t == 0) p = near ? slice + ((size_t)(kp - a) * sp + 4 * i4) * 4 : slice + ((size_t)kp * sp + 4 * i4) * 4;
-                else if (t == 1) p = s16 + ((size_t)((kp - r32) >> 1) * sp + 4 * i4) * 4;
-                else if (t == 2) p = s8 + ((size_t)((kp - r32 - r16) >> 2) * sp + 4 * i4) * 4;
-                w[u][e] = t == 0 ? ld_stream(p) : (t < 3 ? __ldg(reinterpret_cast<const uint4*>(p)) : make_uint4(0u, 0u, 0u, 0u));
-            }
+            for (int e = 0; e < 8; e++) v[e] = (j0 + e >= 0 && j0 + e < m2) ? __uint_as_float(word(j0 + e)) : 0.0f;
         }
+        return;
+    }
+    const int r32 = H.t0, e16 = H.t1, r = H.t2, c8 = r32 + ((e16 - r32) >> 1);  // chunk column of FP8 quad 0
+    if (k0 + 8 <= r32) {
 #pragma unroll
-        for (int u = 0; u < 2; u++) {
-            const int it = base + 32 * u + lane;
-            if (it >= n) continue;
-            const int kc = it / nq, i4 = it - kc * nq;
-            float v[4][8];
+        for (int e = 0; e < 8; e++) v[e] = __uint_as_float(word(k0 + e));
+    } else if (k0 >= r32 && k0 + 8 <= e16) {
+        // FP16 pairs: term r32 + 2g + t in half t of word g; p = the first term's half
+        const int g0 = r32 + ((k0 - r32) >> 1), p = (k0 - r32) & 1;
+        unsigned w[5];
 #pragma unroll
-            for (int e = 0; e < 8; e++) {
-                const int kp = kp0 + kc * 8 + e, t = tier_of(kp);
-                const unsigned ww[4] = {w[u][e].x, w[u][e].y, w[u][e].z, w[u][e].w};
-                const int q = t == 1 ? ((kp - r32) & 1) : ((kp - r32 - r16) & 3);
+        for (int i = 0; i < 4; i++) w[i] = word(g0 + i);
+        w[4] = p ? word(g0 + 4) : 0u;
 #pragma unroll
-                for (int ii = 0; ii < 4; ii++)
-                    v[ii][e] = t == 0 ? __uint_as_float(ww[ii])
-                                      : (t == 1 ? half_value(ww[ii], q) : (t == 2 ? fp8_value((ww[ii] >> (8 * q)) & 255u) : 0.0f));
+        for (int i = 0; i < 4; i++) {
+            const float2 f = h2f2(p ? __byte_perm(w[i], w[i + 1], 0x5432) : w[i]);
+            v[2 * i] = f.x;
+            v[2 * i + 1] = f.y;
+        }
+    } else if (k0 >= e16 && k0 + 8 <= r) {
+        // FP8 quads: term e16 + 4g + t in byte t of word g
+        const int g0 = c8 + ((k0 - e16) >> 2), p = (k0 - e16) & 3;
+        fp8_run(word(g0), word(g0 + 1), p ? word(g0 + 2) : 0u, p, v);
+    } else {
+#pragma unroll
+        for (int e = 0; e < 8; e++) {
+            const int kp = k0 + e;
+            float x = 0.0f;
+            if (kp < r32) {
+                x = __uint_as_float(word(kp));
+            } else if (kp < e16) {
+                const unsigned w = word(r32 + ((kp - r32) >> 1));
+                const float2 f = h2f2(w);
+                x = ((kp - r32) & 1) ? f.y : f.x;
+            } else if (kp < r) {
+                const unsigned w = word(c8 + ((kp - e16) >> 2));
+                const float2 f = e4m3x2_f2(w >> (8 * ((kp - e16) & 2)));
+                x = ((kp - e16) & 1) ? f.y : f.x;
             }
-#pragma unroll
-            for (int ii = 0; ii < 4; ii++)
-                if (4 * i4 + ii < rows) store_row(stage, kc, 4 * i4 + ii, v[ii]);
+            v[e] = x;
         }
     }
 }
 
-// Pass 1: items are (stack row, K core): 8 columns of one term of V_b^T, read as three
-// aligned 16-byte quads of 32-bit words (columns j0 - sh .. j0 - sh + 11, sh = j0 mod 4,
-// the same for the whole step).  V_b^T holds r32 FP32 rows of m2p words, then r16 / 2
-// FP16 pair rows (word (g m2p + j) holds column j of terms 2g, 2g+1), then r8 / 4 FP8
-// quad rows (word (g m2p + j): column j of terms 4g..4g+3).  Four items per lane are
-// loaded before any is converted.
-__device__ __forceinline__ void convert_pass1(const TcmStack& sk, void* const* ptrV, const int* rank,
-                                              const int* tier32, const int* tier16, int kp0, int nkc,
-                                              unsigned char* stage, int lane)
+// Pass 1, one item: stack row m (lane) of K core kc: the 8 words at sh + 8 kc of its raw
+// row (three 16-byte reads; rows 144 bytes apart, so 8 consecutive rows hit 8 distinct
+// bank groups), decoded by the row's tier.
+__device__ __forceinline__ void load_pass1(const TcmHdr& H, const unsigned char* raw, int sh, int m, int kc,
+                                           float (&v)[8])
 {
-    const int a = sk.c0 & 7, m2 = sk.m2, m2p = (m2 + 3) & ~3, n = sk.rows * nkc;
-    const int sh = (4 - (a & 3)) & 3;  // j0 mod 4 for every item (kp0 and 8 kc are multiples of 4)
-    for (int base = 0; base < n; base += 128) {
-        uint4 w[4][3];
-        int tier[4], sel[4];
+    const unsigned ent = H.rtab[m];
+    const int tier = (ent >> 8) & 3, sel = (ent >> 10) & 3;
 #pragma unroll
-        for (int u = 0; u < 4; u++) {
-            const int it = base + 32 * u + lane;
-            const int m = it / nkc, kc = it - m * nkc;
-            tier[u] = 3;
-            sel[u] = 0;
-            const uint4* row = nullptr;
-            if (it < n) {
-                int k = 0;
-                while (k + 1 < sk.nmem && sk.off[k + 1] <= m) k++;
-                const int b = sk.blk[k], l = m - sk.off[k];
-                const int r = rank[b], r32 = tier32[b], r16 = tier16[b];
-                const char* V = static_cast<const char*>(ptrV[b]);
-                if (l < r32) {
-                    tier[u] = 0;
-                    row = reinterpret_cast<const uint4*>(V + (size_t)l * m2p * 4);
-                } else if (l < r32 + r16) {
-                    tier[u] = 1;
-                    sel[u] = (l - r32) & 1;
-                    row = reinterpret_cast<const uint4*>(V + (size_t)r32 * m2p * 4 + (size_t)((l - r32) >> 1) * m2p * 4);
-                } else if (l < r) {
-                    tier[u] = 2;
-                    sel[u] = (l - r32 - r16) & 3;
-                    row = reinterpret_cast<const uint4*>(V + (size_t)r32 * m2p * 4 + (size_t)r16 * m2p * 2 +
-                                                         (size_t)((l - r32 - r16) >> 2) * m2p * 4);
-                }
-            }
-            const int qs = kp0 + kc * 8 - a - sh;  // first column of the first quad (a multiple of 4)
+    for (int e = 0; e < 8; e++) v[e] = 0.0f;
+    if (tier == 3) return;
+    const uint4* rr = reinterpret_cast<const uint4*>(raw + (ent & 255) * TCM_RROW) + 2 * kc;
+    const uint4 c0 = rr[0], c1 = rr[1], c2 = rr[2];
+    const unsigned words[12] = {c0.x, c0.y, c0.z, c0.w, c1.x, c1.y, c1.z, c1.w, c2.x, c2.y, c2.z, c2.w};
+    unsigned w[8];
 #pragma unroll
-            for (int k = 0; k < 3; k++) {
-                const int c = qs + 4 * k;
-                w[u][k] = (row && c >= 0 && c < m2p) ? __ldg(row + (c >> 2)) : make_uint4(0u, 0u, 0u, 0u);
-            }
-        }
-#pragma unroll
-        for (int u = 0; u < 4; u++) {
-            const int it = base + 32 * u + lane;
-            if (it >= n) continue;
-            const int m = it / nkc, kc = it - m * nkc;
-            const int j0 = kp0 + kc * 8 - a;
-            const unsigned words[12] = {w[u][0].x, w[u][0].y, w[u][0].z, w[u][0].w, w[u][1].x, w[u][1].y,
-                                        w[u][1].z, w[u][1].w, w[u][2].x, w[u][2].y, w[u][2].z, w[u][2].w};
-            float v[8];
-#pragma unroll
-            for (int e = 0; e < 8; e++) {
-                // sh is the same for every lane: the compiler selects among four unrolled copies
-                unsigned wd;
-                switch (sh) {
-                case 0: wd = words[e]; break;
-                case 1: wd = words[e + 1]; break;
-                case 2: wd = words[e + 2]; break;
-                default: wd = words[e + 3]; break;
-                }
-                const bool in = j0 + e >= 0 && j0 + e < m2;
-                const int t = in ? tier[u] : 3;
-                v[e] = t == 0 ? __uint_as_float(wd)
-                              : (t == 1 ? half_value(wd, sel[u]) : (t == 2 ? fp8_value((wd >> (8 * sel[u])) & 255u) : 0.0f));
-            }
-            store_row(stage, kc, m, v);
+    for (int e = 0; e < 8; e++) {
+        // sh is the same for every lane of the step
+        switch (sh) {
+        case 0: w[e] = words[e]; break;
+        case 1: w[e] = words[e + 1]; break;
+        case 2: w[e] = words[e + 2]; break;
+        default: w[e] = words[e + 3]; break;
         }
     }
-}
-
-// the scale of stack row m's term (FP16 / FP8 terms of mixed storage), else 1
-__device__ __forceinline__ float stack_scale(const TcmStack& sk, void* const* ptrV, const int* rank, const int* tier32,
-                                             const int* tier16, int m)
-{
-    int k = 0;
-    while (k + 1 < sk.nmem && sk.off[k + 1] <= m) k++;
-    const int b = sk.blk[k], l = m - sk.off[k];
-    const int r = rank[b], r32 = tier32[b], r16 = tier16[b];
-    if (l < r32 || l >= r) return 1.0f;
-    const size_t m2p = (sk.m2 + 3) & ~3;
-    const char* V = static_cast<const char*>(ptrV[b]);
-    const float* scal = reinterpret_cast<const float*>(V + m2p * (4 * (size_t)r32 + 2 * (size_t)r16 + (size_t)(r - r32 - r16)));
-    return scal[l];
+    if (tier == 0) {
+#pragma unroll
+        for (int e = 0; e < 8; e++) v[e] = __uint_as_float(w[e]);
+    } else if (tier == 1) {
+#pragma unroll
+        for (int i = 0; i < 4; i++) {
+            const float2 f = h2f2(__byte_perm(w[2 * i], w[2 * i + 1], sel ? 0x7632u : 0x5410u));
+            v[2 * i] = f.x;
+            v[2 * i + 1] = f.y;
+        }
+    } else {
+        const unsigned s2 = (unsigned)sel | ((unsigned)sel + 4u) << 4;
+#pragma unroll
+        for (int i = 0; i < 4; i++) {
+            const float2 f = e4m3x2_f2(__byte_perm(w[2 * i], w[2 * i + 1], s2));
+            v[2 * i] = f.x;
+            v[2 * i + 1] = f.y;
+        }
+    }
 }
 
 // ---------------------------------------------------------------------------
 // the pass kernel
 // ---------------------------------------------------------------------------
 // Steps of CTA c: [cta[c].y, cta[c+1].y); its jobs: [cta[c].x, cta[c+1].x).  MODE 0
-// (pass 1) writes t_b cores: K core kc of stack j to B K core tb_kc + map[16 j + kc];
-// MODE 1 (pass 2) writes tile row i to Y row map[r0 + i].
+// (pass 1) writes t_b cores: K core kc of the stack whose first t_b term is r0 to B K core
+// tb_kc + r0 / 8 + kc, times tscale per term; MODE 1 (pass 2) writes tile row i to Y
+// row map[r0 + i].
 template <int MODE, int NV>
 __global__ void __launch_bounds__(TCM_THREADS, 1)
     k_tcm_pass(const TcmStep* __restrict__ steps, const TcmJob* __restrict__ jobs, const int2* __restrict__ cta,
-               const PairDesc* __restrict__ desc, const TcmStack* __restrict__ stacks, void* const* ptrV,
-               const int* __restrict__ rank, const int* __restrict__ tier32, const int* __restrict__ tier16,
-               char* Bbuf, long long tb_kc, const int* __restrict__ map, int nrhs, double* Y, int ldy, int* err)
+               const TcmStack* __restrict__ stacks, char* Bbuf, long long tb_kc, const float* __restrict__ tscale,
+               const int* __restrict__ map, int nrhs, double* Y, int ldy, int* err)
 {
     constexpr int P = TCM_PARTS;
     constexpr int KB = NV * 16 * P;  // bytes of a B K core, all parts
-    constexpr int TMEM_COLS = 4 * NV;  // two buffers of hi*hi and correction accumulators
     extern __shared__ __align__(1024) unsigned char tcm_raw[];
     TcmSmem& sm = *reinterpret_cast<TcmSmem*>(tcm_raw);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -317,9 +329,17 @@ __global__ void __launch_bounds__(TCM_THREADS, 1)
     const TcmStep* my_steps = steps + lo.y;
     volatile int* fail = &sm.fail;
     if (tid == 0) {
-        for (int s = 0; s < TCM_STAGES; s++) {
-            mbar_init(&sm.full[s], 1 + TCM_GWARPS);
-            mbar_init(&sm.empty[s], 1);
+        for (int s = 0; s < TCM_NR; s++) {
+            mbar_init(&sm.raw_full[s], 33);  // the 32 producer lanes' copies + the header
+            mbar_init(&sm.raw_empty[s], TCM_CONV);
+        }
+        for (int s = 0; s < TCM_NA; s++) {
+            mbar_init(&sm.a_full[s], TCM_CONV);
+            mbar_init(&sm.a_empty[s], 1);
+        }
+        for (int s = 0; s < TCM_NB; s++) {
+            mbar_init(&sm.b_full[s], 1);
+            mbar_init(&sm.b_empty[s], 1);
         }
         for (int b = 0; b < 2; b++) {
             mbar_init(&sm.accf[b], 1);
@@ -331,101 +351,231 @@ __global__ void __launch_bounds__(TCM_THREADS, 1)
     }
     if (warp == 5) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&sm.tmem)),
-                     "n"(TMEM_COLS));
+                     "n"(TCM_TMEM_COLS));
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
     }
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const uint32_t tmem = sm.tmem;
 
-    if (warp >= 6) {
-        // ---- converters: group g takes steps g, g + 4, ... ----
-        const int g = (warp - 6) / TCM_GWARPS, gt = tid - (6 + g * TCM_GWARPS) * 32;
-        for (int i = g; i < nsteps; i += TCM_GROUPS) {
-            const int slot = i % TCM_STAGES;
-            if (i >= TCM_STAGES) {
-                bool ok = true;
-                if (lane == 0) ok = !*fail && mbar_wait(&sm.empty[slot], ((i / TCM_STAGES) - 1) & 1, err, 21);
-                if (!__shfl_sync(~0u, ok, 0)) {
-                    *fail = 1;
-                    break;
+    if (warp >= 7) {
+        // ---- converters: every step, items (32 rows, 1 K core) dealt over the warps ----
+        const int cw = warp - 7;
+        for (int i = 0; i < nsteps; i++) {
+            const int slot = i % TCM_NR, as = i % TCM_NA;
+            bool ok = !*fail && mbar_wait(&sm.raw_full[slot], (i / TCM_NR) & 1, err, 31);
+            if (ok && i >= TCM_NA) ok = mbar_wait(&sm.a_empty[as], ((i / TCM_NA) - 1) & 1, err, 32);
+            if (!__all_sync(~0u, ok)) {
+                *fail = 1;
+                break;
+            }
+            const TcmHdr& H = sm.hdr[slot];
+            const int meta = H.meta, rows = H.rows, kp0 = H.kp0;
+            const int lg = (meta & 3) == 2 ? 2 : 1, nkc = 1 << lg;  // K cores of the step
+            const int mode = (meta >> 12) & 15, nparts = MODE == 0 ? 3 : (mode >= 6 ? 3 : (mode >= 3 ? 2 : 1));
+            const int nitems = ((rows + 31) >> 5) << lg;
+            unsigned char* stage = sm.a[as];
+            if (MODE == 1) {
+                const int sp = (rows + 3) & ~3;
+                const unsigned* rw = reinterpret_cast<const unsigned*>(sm.raw[slot]);
+#pragma unroll 1
+                for (int it = cw; it < nitems; it += TCM_CONV) {
+                    const int kc = it & (nkc - 1), m = (it >> lg) * 32 + lane;
+                    float v[8];
+                    load_pass2(H, rw, sp, m, kp0 + 8 * kc, v);
+                    store_parts(stage, kc, m, v, nparts);
+                }
+            } else {
+                const int sh = (kp0 - H.t0) & 3;
+#pragma unroll 1
+                for (int it = cw; it < nitems; it += TCM_CONV) {
+                    const int kc = it & (nkc - 1), m = (it >> lg) * 32 + lane;
+                    float v[8];
+                    load_pass1(H, sm.raw[slot], sh, m, kc, v);
+                    store_parts(stage, kc, m, v, 3);
                 }
             }
-            const TcmStep st = my_steps[i];
-            const int nkc = 2 * (st.meta & 3);
-            if (MODE == 1)
-                convert_pass2(desc[st.src], st.rows, st.kp0, nkc, sm.a[slot], gt);
-            else
-                convert_pass1(stacks[st.src], ptrV, rank, tier32, tier16, st.kp0, nkc, sm.a[slot], gt);
             // the generic-proxy stores become visible to the tensor cores' (async) proxy
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
             __syncwarp();
-            if (lane == 0) mbar_arrive(&sm.full[slot]);
-        }
-    } else if (warp == 4) {
-        // ---- B operand of every step: one bulk copy, lane 0 ----
-        if (lane == 0) {
-            int issued = 0;
-            for (int i = 0; i < nsteps; i++) {
-                const int slot = i % TCM_STAGES;
-                if (i >= TCM_STAGES &&
-                    (*fail || !mbar_wait(&sm.empty[slot], ((i / TCM_STAGES) - 1) & 1, err, 22))) {
-                    *fail = 1;
-                    break;
-                }
-                const TcmStep st = my_steps[i];
-                const unsigned bytes = (unsigned)(2 * (st.meta & 3)) * KB;
-                mbar_arrive_expect_tx(&sm.full[slot], bytes);
-                bulk_g2s(sm.b[slot], Bbuf + st.b_kc * KB, bytes, &sm.full[slot]);
-                issued++;
+            if (lane == 0) {
+                mbar_arrive(&sm.a_full[as]);
+                mbar_arrive(&sm.raw_empty[slot]);
             }
-            // the last copy into every stage has landed before the CTA leaves
-            for (int s = 0; s < TCM_STAGES && s < issued; s++)
-                mbar_wait(&sm.full[s], ((issued - 1 - s) / TCM_STAGES) & 1, err, 23);
         }
-        __syncwarp();
-    } else if (warp == 5) {
-        // ---- MMAs, lane 0 ----
-        if (lane == 0) {
-            constexpr uint32_t LBA = P * 16 * 128, LBB = KB;  // K-core strides of A and B
-            for (int i = 0; i < nsteps; i++) {
-                const int slot = i % TCM_STAGES, buf = i & 1;
-                if (*fail || !mbar_wait(&sm.full[slot], (i / TCM_STAGES) & 1, err, 24)) {
-                    *fail = 1;
-                    break;
+    } else if (warp == 6) {
+        // ---- raw producer: the stored bytes of every step, 16-byte cp.async per lane ----
+        uint64_t pol;
+        asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(pol));
+        int cur_stack = -1, nq = 0, m2p4 = 0;
+        const TcmStack* sk = nullptr;
+        const char** rowptr = sm.rowptr;
+        bool ok = true;
+        for (int i0 = 0; i0 < nsteps && ok; i0 += 32) {
+            TcmStep rec{};
+            if (i0 + lane < nsteps) rec = my_steps[i0 + lane];
+            const int cnt = min(32, nsteps - i0);
+            for (int k = 0; k < cnt; k++) {
+                const int i = i0 + k, slot = i % TCM_NR;
+                const long long rawp = __shfl_sync(~0u, (long long)rec.raw, k);
+                const int meta = __shfl_sync(~0u, rec.meta, k), rows = __shfl_sync(~0u, rec.rows, k);
+                const int kp0 = __shfl_sync(~0u, rec.kp0, k), n16 = __shfl_sync(~0u, rec.n16, k);
+                const int cc0 = __shfl_sync(~0u, rec.cc0, k), t0 = __shfl_sync(~0u, rec.t0, k);
+                const int t1 = __shfl_sync(~0u, rec.t1, k), t2 = __shfl_sync(~0u, rec.t2, k);
+                if (MODE == 0 && n16 != cur_stack) {
+                    // the stack's V rows: member k's rows from vptr[k], m2p4 chunks each
+                    cur_stack = n16;
+                    sk = stacks + n16;
+                    nq = sk->nq;
+                    m2p4 = sk->m2p4;
+                    const int nmem = sk->nmem;
+                    const char* vp = lane < nmem ? sk->vptr[lane] : nullptr;
+                    const int qb = lane < nmem ? sk->qb[lane] : 0x7fffffff;
+                    for (int q = lane; q < 128; q += 32) {
+                        int kk = 0;
+                        for (int u = 1; u < nmem; u++)
+                            if (__shfl_sync(~0u, qb, u) <= q) kk = u;
+                        const char* base = reinterpret_cast<const char*>(__shfl_sync(~0u, (long long)vp, kk));
+                        const int q0 = __shfl_sync(~0u, qb, kk);
+                        rowptr[q] = base + (size_t)(q - q0) * m2p4 * 16;
+                    }
+                    __syncwarp();
                 }
-                if (i >= 2) {  // the epilogue has read this buffer's previous step
-                    if (!mbar_wait(&sm.acce[buf], ((i >> 1) - 1) & 1, err, 25)) {
+                if (i >= TCM_NR) {
+                    bool w = true;
+                    if (lane == 0) w = !*fail && mbar_wait(&sm.raw_empty[slot], ((i / TCM_NR) - 1) & 1, err, 33);
+                    if (!__shfl_sync(~0u, w, 0)) {
                         *fail = 1;
+                        ok = false;
                         break;
                     }
                 }
-                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-                const int meta = my_steps[i].meta, nk = meta & 3, mode = (meta >> 12) & 15;
-                const uint32_t d = tmem + (uint32_t)(buf * 2 * NV);
-                uint64_t ad = smem_desc(smem_u32(sm.a[slot]), LBA, 128), bd = smem_desc(smem_u32(sm.b[slot]), LBB, 128);
-                const uint64_t da = (2 * LBA) >> 4, db = (2 * LBB) >> 4;
-                const uint64_t alo = (16 * 128) >> 4, blo = (NV * 16) >> 4;  // part q: + q alo / q blo
-                for (int k = 0; k < nk; k++) {
-                    const uint32_t acc = k > 0 ? 1u : 0u;
-                    tc_mma(d, ad, bd, tc_idesc<NV>(), acc);
-                    if (mode >= 3) {
-                        tc_mma(d + NV, ad, bd + blo, tc_idesc<NV>(), acc);
-                        tc_mma(d + NV, ad + alo, bd, tc_idesc<NV>(), 1u);
-                    }
-                    if (mode >= 6) {
-                        tc_mma(d + NV, ad, bd + 2 * blo, tc_idesc<NV>(), 1u);
-                        tc_mma(d + NV, ad + 2 * alo, bd, tc_idesc<NV>(), 1u);
-                        tc_mma(d + NV, ad + alo, bd + blo, tc_idesc<NV>(), 1u);
-                    }
-                    ad += da;
-                    bd += db;
+                TcmHdr& H = sm.hdr[slot];
+                if (lane == 0) {
+                    H.kp0 = kp0; H.meta = meta; H.rows = rows; H.cc0 = cc0;
+                    H.t0 = t0; H.t1 = t1; H.t2 = t2;
                 }
-                tc_commit(&sm.empty[slot]);
-                tc_commit(&sm.accf[buf]);
+                unsigned char* dst = sm.raw[slot];
+                if (MODE == 1) {
+                    const char* src = reinterpret_cast<const char*>(rawp);
+                    for (int c = lane; c < n16; c += 32) cpa16(dst + 16 * c, src + 16 * c, 16, pol);
+                } else {
+                    if (lane < 16) cpa16(&H.rtab[8 * lane], &sk->rtab[8 * lane], 16, pol);
+                    // chunk c: V row c / 9, chunk c mod 9, walked without division (32 = 3 * 9 + 5)
+                    const int nch = nq * 9;
+                    int r = lane / 9, kk = lane - 9 * (lane / 9);
+                    for (int c = lane; c < nch; c += 32) {
+                        const int ch = cc0 + kk;
+                        const bool in = ch >= 0 && ch < m2p4;
+                        const char* rp = rowptr[r];
+                        cpa16(dst + r * TCM_RROW + 16 * kk, in ? rp + 16 * ch : rp, in ? 16u : 0u, pol);
+                        r += 3;
+                        kk += 5;
+                        if (kk >= 9) {
+                            kk -= 9;
+                            r += 1;
+                        }
+                    }
+                }
+                cpa_arrive(&sm.raw_full[slot]);
+                __syncwarp();
+                if (lane == 0) mbar_arrive(&sm.raw_full[slot]);
             }
+        }
+        // every copy of this warp has landed before the CTA leaves
+        asm volatile("cp.async.wait_all;" ::: "memory");
+        __syncwarp();
+    } else if (warp == 4) {
+        // ---- B operand of every step: one bulk copy, lane 0 ----
+        int issued = 0;
+        bool ok = true;
+        for (int i0 = 0; i0 < nsteps && ok; i0 += 32) {
+            int mt = 0;
+            long long bk = 0;
+            if (i0 + lane < nsteps) {
+                mt = my_steps[i0 + lane].meta;
+                bk = my_steps[i0 + lane].b_kc;
+            }
+            const int cnt = min(32, nsteps - i0);
+            for (int k = 0; k < cnt; k++) {
+                const int i = i0 + k, slot = i % TCM_NB;
+                const int meta = __shfl_sync(~0u, mt, k);
+                const long long b_kc = __shfl_sync(~0u, bk, k);
+                bool w = true;
+                if (lane == 0) {
+                    if (i >= TCM_NB) w = !*fail && mbar_wait(&sm.b_empty[slot], ((i / TCM_NB) - 1) & 1, err, 34);
+                    if (w) {
+                        const unsigned bytes = (unsigned)(2 * (meta & 3)) * KB;
+                        mbar_arrive_expect_tx(&sm.b_full[slot], bytes);
+                        bulk_g2s(sm.b[slot], Bbuf + b_kc * KB, bytes, &sm.b_full[slot]);
+                        issued++;
+                    }
+                }
+                if (!__shfl_sync(~0u, w, 0)) {
+                    *fail = 1;
+                    ok = false;
+                    break;
+                }
+            }
+        }
+        // the last copy into every stage has landed before the CTA leaves
+        if (lane == 0)
+            for (int s = 0; s < TCM_NB && s < issued; s++)
+                mbar_wait(&sm.b_full[(issued - 1 - s) % TCM_NB], ((issued - 1 - s) / TCM_NB) & 1, err, 35);
+        __syncwarp();
+    } else if (warp == 5) {
+        // ---- MMAs, lane 0: one per part of A, over the B parts side by side along N ----
+        constexpr uint32_t LBA = P * 16 * 128, LBB = KB;  // K-core strides of A and B
+        bool ok = true;
+        for (int i0 = 0; i0 < nsteps && ok; i0 += 32) {
+            const int mt = i0 + lane < nsteps ? my_steps[i0 + lane].meta : 0;
+            const int cnt = min(32, nsteps - i0);
+            for (int k = 0; k < cnt; k++) {
+                const int i = i0 + k, as = i % TCM_NA, bs = i % TCM_NB, buf = i & 1;
+                const int meta = __shfl_sync(~0u, mt, k);
+                bool w = true;
+                if (lane == 0) {
+                    w = !*fail && mbar_wait(&sm.a_full[as], (i / TCM_NA) & 1, err, 36) &&
+                        mbar_wait(&sm.b_full[bs], (i / TCM_NB) & 1, err, 37);
+                    // the epilogue has read this buffer's previous step
+                    if (w && i >= 2) w = mbar_wait(&sm.acce[buf], ((i >> 1) - 1) & 1, err, 38);
+                    if (w) {
+                        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                        const int nk = meta & 3, mode = (meta >> 12) & 15;
+                        const uint32_t d = tmem + (uint32_t)(buf * 3 * NV);  // hi, c1, c2
+                        uint64_t ad = smem_desc(smem_u32(sm.a[as]), LBA, 128), bd = smem_desc(smem_u32(sm.b[bs]), LBB, 128);
+                        const uint64_t da = (2 * LBA) >> 4, db = (2 * LBB) >> 4;
+                        const uint64_t alo = (16 * 128) >> 4;  // part q of A: + q alo
+                        for (int kk = 0; kk < nk; kk++) {
+                            const uint32_t acc = kk > 0 ? 1u : 0u;
+                            if (mode >= 6) {
+                                tc_mma(d, ad, bd, tc_idesc<3 * NV>(), acc);
+                                tc_mma(d + NV, ad + alo, bd, tc_idesc<2 * NV>(), 1u);
+                                tc_mma(d + NV, ad + 2 * alo, bd, tc_idesc<NV>(), 1u);
+                            } else if (mode >= 3) {
+                                tc_mma(d, ad, bd, tc_idesc<2 * NV>(), acc);
+                                tc_mma(d + NV, ad + alo, bd, tc_idesc<NV>(), 1u);
+                            } else {
+                                tc_mma(d, ad, bd, tc_idesc<NV>(), acc);
+                            }
+                            ad += da;
+                            bd += db;
+                        }
+                        tc_commit(&sm.a_empty[as]);
+                        tc_commit(&sm.b_empty[bs]);
+                        tc_commit(&sm.accf[buf]);
+                    }
+                }
+                if (!__shfl_sync(~0u, w, 0)) {
+                    *fail = 1;
+                    ok = false;
+                    break;
+                }
+            }
+        }
+        if (lane == 0) {
             tc_commit(&sm.fin);  // every MMA issued here has completed before tensor memory is freed
-            mbar_wait(&sm.fin, 0, err, 26);
+            mbar_wait(&sm.fin, 0, err, 39);
         }
         __syncwarp();
     } else {
@@ -434,45 +584,55 @@ __global__ void __launch_bounds__(TCM_THREADS, 1)
         float f[NV];
         const int njobs = hi.x - lo.x;
         const TcmJob* my_jobs = jobs + lo.x;
-        int jc = 0, rows = 0, yrow = 0, tdst[4] = {0, 0, 0, 0};
-        float scale = 1.0f;
+        // job jc's rows, first row / term and per-row value (Y row or term scale) are
+        // loaded while job jc - 1 runs; the record of job jc + 1 one job earlier still
+        auto row_value = [&](const TcmJob& jb) -> unsigned {
+            if (row >= jb.rows) return 0u;
+            return MODE == 1 ? (unsigned)map[jb.r0 + row] : __float_as_uint(tscale[jb.r0 + row]);
+        };
+        TcmJob cur = njobs > 0 ? my_jobs[0] : TcmJob{0, 0};
+        unsigned cur_val = njobs > 0 ? row_value(cur) : 0u;
+        TcmJob nxt = njobs > 1 ? my_jobs[1] : TcmJob{0, 0};
+        int jc = 0, rows = 0, r0 = 0;
+        unsigned val = 0u;
         bool ok = true;
+        int mt_next = lane < nsteps ? my_steps[lane].meta : 0;
         for (int i0 = 0; i0 < nsteps && ok; i0 += 32) {
-            const int mt = i0 + lane < nsteps ? my_steps[i0 + lane].meta : 0;
+            const int mt = mt_next;
+            mt_next = i0 + 32 + lane < nsteps ? my_steps[i0 + 32 + lane].meta : 0;
             const int cnt = min(32, nsteps - i0);
             for (int k = 0; k < cnt; k++) {
                 const int i = i0 + k, meta = __shfl_sync(~0u, mt, k), buf = i & 1;
                 const bool first = meta & 256, last = meta & 512;
                 const int mode = (meta >> 12) & 15;
                 if (first) {
-                    const TcmJob jb = jc < njobs ? my_jobs[jc] : TcmJob{0, 0};
-                    rows = jb.rows;
-                    if (MODE == 1) {
-                        yrow = row < rows ? map[jb.r0 + row] : 0;
-                    } else {
-#pragma unroll
-                        for (int q = 0; q < 4; q++)
-                            tdst[q] = (warp * 4 + q < (rows >> 3)) ? map[jb.r0 * 16 + warp * 4 + q] : 0;
-                        scale = row < rows ? stack_scale(stacks[jb.r0], ptrV, rank, tier32, tier16, row) : 1.0f;
-                    }
+                    rows = cur.rows;
+                    r0 = cur.r0;
+                    val = cur_val;
+                    cur = nxt;
+                    cur_val = jc + 1 < njobs ? row_value(cur) : 0u;
+                    nxt = jc + 2 < njobs ? my_jobs[jc + 2] : TcmJob{0, 0};
                 }
-                if (!__all_sync(~0u, !*fail && mbar_wait(&sm.accf[buf], (i >> 1) & 1, err, 27))) {
+                if (!__all_sync(~0u, !*fail && mbar_wait(&sm.accf[buf], (i >> 1) & 1, err, 40))) {
                     ok = false;
                     break;
                 }
                 asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-                const uint32_t taddr = tmem + (uint32_t)(buf * 2 * NV) + ((uint32_t)(warp * 32) << 16);
-                // 16 columns at a time: the running sums f[NV] stay in registers beside them
+                const uint32_t taddr = tmem + (uint32_t)(buf * 3 * NV) + ((uint32_t)(warp * 32) << 16);
+                // 8 columns of each accumulator at a time: the running sums f[NV] stay in
+                // registers beside them
 #pragma unroll
-                for (int h = 0; h < NV / 16; h++) {
-                    uint32_t v[16], c[16];
-                    tc_ld16(taddr + 16 * h, v);
-                    if (mode > 1) tc_ld16(taddr + NV + 16 * h, c);
+                for (int h = 0; h < NV / 8; h++) {
+                    uint32_t v[8], c1[8], c2[8];
+                    tc_ld8(taddr + 8 * h, v);
+                    if (mode > 1) tc_ld8(taddr + NV + 8 * h, c1);
+                    if (mode > 3) tc_ld8(taddr + 2 * NV + 8 * h, c2);
                     asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 #pragma unroll
-                    for (int q = 0; q < 16; q++) {
-                        const float tv = __uint_as_float(v[q]) + (mode > 1 ? __uint_as_float(c[q]) : 0.0f);
-                        f[16 * h + q] = first ? tv : f[16 * h + q] + tv;
+                    for (int q = 0; q < 8; q++) {
+                        const float c = mode > 1 ? __uint_as_float(c1[q]) + (mode > 3 ? __uint_as_float(c2[q]) : 0.0f) : 0.0f;
+                        const float tv = __uint_as_float(v[q]) + c;
+                        f[8 * h + q] = first ? tv : f[8 * h + q] + tv;
                     }
                 }
                 asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -482,46 +642,37 @@ __global__ void __launch_bounds__(TCM_THREADS, 1)
                 jc++;
                 if (MODE == 1) {
                     if (row < rows) {
-                        double* y = Y + yrow;
+                        double* y = Y + (int)val;
 #pragma unroll
                         for (int q = 0; q < NV; q++)
                             if (q < nrhs) y[(size_t)q * ldy] = (double)f[q];
                     }
                 } else {
-                    // term row -> 3-part B cores of pass 2 (see tc.cu's pass-1 epilogue):
-                    // lanes 2p, 2p+1 pair their terms into 32-bit words; staging row u
-                    // (K core u / NV, vector u % NV) at u ^ (2 (u / NV)) spreads the banks
-                    uint32_t* stg = reinterpret_cast<uint32_t*>(sm.stg[warp]);
-                    const bool odd = lane & 1;
+                    // term row -> 3-part B cores of pass 2 through the warp's staging
+                    // array [vector][row] (rows padded to 40: the 16-byte reads of 8
+                    // consecutive vectors hit distinct bank groups)
+                    __nv_bfloat16* stg = sm.stg[warp];
+                    const float scale = __uint_as_float(val);
 #pragma unroll
                     for (int q = 0; q < NV; q++) f[q] *= scale;
-#pragma unroll
+                    // part p: the BF16 rounding of what parts 0..p-1 miss, f keeping the rest
+#pragma unroll 1
                     for (int part = 0; part < P; part++) {
+                        if (part > 0) {
 #pragma unroll
-                        for (int t = 0; t < NV / 2; t++) {
-                            float v0 = f[2 * t], v1 = f[2 * t + 1];
-#pragma unroll
-                            for (int pp = 0; pp < part; pp++) {
-                                v0 -= __bfloat162float(__float2bfloat16_rn(v0));
-                                v1 -= __bfloat162float(__float2bfloat16_rn(v1));
-                            }
-                            const float x = __shfl_xor_sync(~0u, odd ? v0 : v1, 1);
-                            const int q = odd ? 2 * t + 1 : 2 * t;
-                            const uint32_t w = odd ? pack_bf16(x, v1) : pack_bf16(v0, x);
-                            const int u = (lane >> 3) * NV + q;
-                            stg[(u ^ ((lane >> 3) * 2)) * 4 + ((lane & 7) >> 1)] = w;
+                            for (int q = 0; q < NV; q++) f[q] -= __bfloat162float(__float2bfloat16_rn(f[q]));
                         }
+#pragma unroll
+                        for (int q = 0; q < NV; q++) stg[q * TCM_STGR + lane] = __float2bfloat16_rn(f[q]);
                         __syncwarp();
                         uint4* dst = reinterpret_cast<uint4*>(Bbuf);
-                        const uint4* src = reinterpret_cast<const uint4*>(stg);
-#pragma unroll
-                        for (int it = 0; it < NV / 8; it++) {
-                            // staging row u = it * 32 + lane: K core kcl (a constant after unrolling,
-                            // NV being a multiple of 32), vector vq
-                            constexpr int per = NV / 32;
-                            const int kcl = it / per, vq = (it % per) * 32 + lane, u = it * 32 + lane;
+#pragma unroll 1
+                        for (int u = lane; u < 4 * NV; u += 32) {
+                            // K core kcl (rows 8 kcl .. 8 kcl + 7 of the warp) of vector vq
+                            const int kcl = u / NV, vq = u % NV;
                             if (warp * 4 + kcl < (rows >> 3))
-                                dst[((size_t)(tb_kc + tdst[kcl]) * P + part) * NV + vq] = src[u ^ (kcl * 2)];
+                                dst[((size_t)(tb_kc + (r0 >> 3) + warp * 4 + kcl) * P + part) * NV + vq] =
+                                    *reinterpret_cast<const uint4*>(stg + vq * TCM_STGR + 8 * kcl);
                         }
                         __syncwarp();
                     }
@@ -533,8 +684,27 @@ __global__ void __launch_bounds__(TCM_THREADS, 1)
     __syncthreads();
     if (warp == 5) {
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "n"(TMEM_COLS));
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "n"(TCM_TMEM_COLS));
     }
+}
+
+// scale of every t_b term: su_l sv_l for the FP16 / FP8 terms of mixed storage, else 1
+// (padding terms up to the rank rounded to 16 included); one warp per block
+__global__ void k_tcm_scales(const int* __restrict__ far, int nfar, const int* __restrict__ rank,
+                             const int* __restrict__ tier32, const int* __restrict__ tier16,
+                             const int* __restrict__ blk_m2, void* const* ptrV, const long long* __restrict__ tterm,
+                             int mixed, float* __restrict__ tscale)
+{
+    const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    if (w >= nfar) return;
+    const int b = far[w], r = rank[b], r16p = (r + 15) & ~15;
+    const int r32 = tier32[b], r16 = tier16[b];
+    const size_t m2p = (size_t)((blk_m2[b] + 3) & ~3);
+    const float* scal =
+        reinterpret_cast<const float*>(static_cast<const char*>(ptrV[b]) + m2p * (4 * (size_t)r32 + 2 * (size_t)r16 +
+                                                                                  (size_t)(r - r32 - r16)));
+    for (int l = lane; l < r16p; l += 32)
+        tscale[tterm[w] + l] = (mixed && l >= r32 && l < r) ? scal[l] : 1.0f;
 }
 
 // ---------------------------------------------------------------------------
@@ -553,7 +723,7 @@ void free_tcm(hmg_matrix* h)
         dfree(p, s);
         h->tcm_stacks = nullptr;
     }
-    dfree(h->tcm_kmap, s);
+    dfree(h->tcm_tscale, s);
     for (int q = 0; q < 2; q++) {
         dfree(h->tcm_steps[q], s);
         dfree(h->tcm_jobs[q], s);
@@ -578,16 +748,12 @@ struct TcmPlan {
         jobs.push_back(j);
         cost.push_back(0.0);
     }
-    // K positions [0, kw) (a multiple of 16) of one source in steps of 32
-    void add(int src, int kw, long long b_kc, int rows, int mode_of_first, int r32, int r16, bool far, double bytes_per_k)
+    void add(const TcmStep& st, double raw_bytes)
     {
-        for (int kp0 = 0; kp0 < kw; kp0 += 32) {
-            const int nk = std::min(2, (kw - kp0) / 16);
-            int mode = mode_of_first;
-            if (far) mode = kp0 < r32 ? 6 : (kp0 < r32 + r16 ? 3 : 1);
-            steps.push_back(TcmStep{b_kc + kp0 / 8, src, kp0, nk | (mode << 12), rows});
-            cost.back() += bytes_per_k * 16 * nk + 2048.0 * mode * nk;
-        }
+        steps.push_back(st);
+        const int nk = st.meta & 3, mode = (st.meta >> 12) & 15;
+        // copy bytes plus the MMA issue time (~46 cycles a 128 x N x 16 MMA) in bytes
+        cost.back() += raw_bytes + 2048.0 * mode * nk;
     }
     void finish()
     {
@@ -600,15 +766,22 @@ struct TcmPlan {
     }
 };
 
-// longest job first onto the least loaded CTA; steps and jobs CTA by CTA
+// Jobs onto CTAs: the few large ones first, longest first, then the rest in plan order
+// (row tiles / column clusters in Z order), each onto the least loaded CTA, so that the
+// CTAs work through neighbouring tiles at the same time and share X in L2.
 hmg_status upload_plan(hmg_matrix* h, int q, const TcmPlan& L, int grid)
 {
     cudaStream_t s = h->stream;
     const int nj = (int)L.jobs.size();
+    double total = 0.0;
+    for (int j = 0; j < nj; j++) total += L.cost[j];
+    const double big = total / (4.0 * grid);
     std::vector<int> order;
     for (int j = 0; j < nj; j++)
-        if (L.step0[j] < L.step0[j + 1]) order.push_back(j);
+        if (L.step0[j] < L.step0[j + 1] && L.cost[j] > big) order.push_back(j);
     std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return L.cost[a] > L.cost[b]; });
+    for (int j = 0; j < nj; j++)
+        if (L.step0[j] < L.step0[j + 1] && !(L.cost[j] > big)) order.push_back(j);
     using Load = std::pair<double, int>;
     std::priority_queue<Load, std::vector<Load>, std::greater<Load>> heap;
     for (int c = 0; c < grid; c++) heap.push({0.0, c});
@@ -646,6 +819,9 @@ hmg_status upload_plan(hmg_matrix* h, int q, const TcmPlan& L, int grid)
     return HMG_OK;
 }
 
+// chunk column of K position k of a low-rank slice: FP32 terms, then FP16 pairs, then FP8 quads
+inline int far_chunk(int k, int r32, int r16) { return k < r32 ? k : (k < r32 + r16 ? r32 + (k - r32) / 2 : r32 + r16 / 2 + (k - r32 - r16) / 4); }
+
 }  // namespace
 
 hmg_status build_tcm(hmg_matrix* h)
@@ -670,17 +846,22 @@ hmg_status build_tcm(hmg_matrix* h)
     if ((st = ensure_desc(h, 4))) return st;
     const int np = h->npairs, nt = h->ntiles, nb = h->nblocks, grid = h->nsm;
     std::vector<int> tps(nt + 1), pblock(np), ts(nt), tr0(nt);
+    std::vector<PairDesc> desc(np);
+    std::vector<void*> pv(nb, nullptr);
     HMG_CUDA_TRY(cudaMemcpy(tps.data(), h->tile_pair_start, sizeof(int) * (nt + 1), cudaMemcpyDeviceToHost));
     HMG_CUDA_TRY(cudaMemcpy(pblock.data(), h->pair_block, sizeof(int) * np, cudaMemcpyDeviceToHost));
     HMG_CUDA_TRY(cudaMemcpy(ts.data(), h->tile_s, sizeof(int) * nt, cudaMemcpyDeviceToHost));
     HMG_CUDA_TRY(cudaMemcpy(tr0.data(), h->tile_r0, sizeof(int) * nt, cudaMemcpyDeviceToHost));
+    if (np > 0) HMG_CUDA_TRY(cudaMemcpy(desc.data(), h->pair_desc, sizeof(PairDesc) * np, cudaMemcpyDeviceToHost));
+    if (h->naca > 0 && h->ptrV) HMG_CUDA_TRY(cudaMemcpy(pv.data(), h->ptrV, sizeof(void*) * nb, cudaMemcpyDeviceToHost));
     const bool mixed = h->far_prec == HMG_PREC_MIXED;
     const long long xkc = (h->n[1] + 7) / 8 + 4;  // X K cores (8 Z-ordered columns each), with slack
     // pass 1: stacks of blocks with the same columns, ranks rounded to 16, first fit
     std::vector<long long> toff(nb, -1);  // first 16-term group of each block's t_b
     long long tgroups = 0;
     std::vector<TcmStack> stacks;
-    std::vector<int> kmap;
+    std::vector<int> far_blocks;
+    std::vector<long long> far_term;
     TcmPlan p1, p2;
     {
         std::vector<int> far;
@@ -707,31 +888,60 @@ hmg_status build_tcm(hmg_matrix* h)
                 members[k].push_back(b);
                 fill[k] += r16;
             }
-            const int c0 = h->h_c0[far[g0]], m2 = h->h_m2[far[g0]], kw = ((c0 & 7) + m2 + 15) & ~15;
+            const int c0 = h->h_c0[far[g0]], m2 = h->h_m2[far[g0]], a = c0 & 7, kw = (a + m2 + 15) & ~15;
+            const int m2p4 = ((m2 + 3) & ~3) / 4;
             for (size_t k = 0; k < members.size(); k++) {
                 TcmStack sk{};
-                sk.c0 = c0;
-                sk.m2 = m2;
-                sk.rows = fill[k];
                 sk.nmem = (int)members[k].size();
-                const int job = (int)stacks.size();
-                kmap.resize(kmap.size() + 16, 0);
-                int off = 0;
+                sk.m2p4 = m2p4;
+                for (int m = 0; m < 128; m++) sk.rtab[m] = 3u << 8;
+                const long long tg0 = tgroups;
+                int off = 0, q = 0;
                 for (int u = 0; u < sk.nmem; u++) {
-                    const int b = members[k][u], r16 = (h->h_rank[b] + 15) & ~15;
-                    sk.blk[u] = b;
-                    sk.off[u] = off;
+                    const int b = members[k][u], r = h->h_rank[b], r16p = (r + 15) & ~15;
+                    const int r32 = mixed ? h->h_r32[b] : r, r16 = mixed ? h->h_r16[b] : 0, r8 = r - r32 - r16;
+                    sk.vptr[u] = static_cast<const char*>(pv[b]);
+                    sk.qb[u] = q;
+                    for (int l = 0; l < r; l++) {
+                        int qq, tier, sel;
+                        if (l < r32) { qq = q + l; tier = 0; sel = 0; }
+                        else if (l < r32 + r16) { qq = q + r32 + (l - r32) / 2; tier = 1; sel = (l - r32) & 1; }
+                        else { qq = q + r32 + r16 / 2 + (l - r32 - r16) / 4; tier = 2; sel = (l - r32 - r16) & 3; }
+                        sk.rtab[off + l] = (uint16_t)(qq | tier << 8 | sel << 10);
+                    }
                     toff[b] = tgroups;
-                    for (int kc = 0; kc < r16 / 8; kc++) kmap[job * 16 + off / 8 + kc] = (int)(tgroups * 2 + kc);
-                    tgroups += r16 / 16;
-                    off += r16;
+                    far_blocks.push_back(b);
+                    far_term.push_back(tgroups * 16);
+                    tgroups += r16p / 16;
+                    off += r16p;
+                    q += r32 + r16 / 2 + r8 / 4;
                 }
+                sk.nq = q;
+                const int job = (int)stacks.size();
                 stacks.push_back(sk);
-                p1.begin(TcmJob{job, sk.rows});
-                p1.add(job, kw, c0 >> 3, sk.rows, 6, 0, 0, false, 4.0 * sk.rows);
+                p1.begin(TcmJob{(int)(tg0 * 16), off});
+                for (int kp0 = 0; kp0 < kw; kp0 += 32) {
+                    const int nk = std::min(2, (kw - kp0) / 16);
+                    TcmStep stp{};
+                    stp.raw = nullptr;
+                    stp.b_kc = (c0 >> 3) + kp0 / 8;
+                    stp.meta = nk | (6 << 12);
+                    stp.rows = off;
+                    stp.kp0 = kp0;
+                    stp.n16 = job;
+                    stp.cc0 = (kp0 - a) >= 0 ? (kp0 - a) / 4 : -((a - kp0 + 3) / 4);
+                    stp.t0 = a;
+                    stp.t1 = m2p4;
+                    stp.t2 = 0;
+                    p1.add(stp, 144.0 * q);
+                }
             }
             g0 = g1;
         }
+    }
+    if (tgroups * 16 > 0x7fffffffll) {
+        set_error("hmg_build_tensor_core_operands: %lld t_b terms exceed the plan's 32-bit term index", tgroups * 16);
+        return HMG_ERR_UNSUPPORTED;
     }
     // pass 2: per tile, its near pairs (B = X) and low-rank pairs (B = t_b)
     bool all_tiles = true;
@@ -746,34 +956,68 @@ hmg_status build_tcm(hmg_matrix* h)
                 p2.begin(TcmJob{tr0[t], ts[t]});
                 started = true;
             }
+            const PairDesc& d = desc[p];
+            const char* data = static_cast<const char*>(d.data);
             if (dense) {
-                const int a = h->h_c0[b] & 7, kw = (a + h->h_m2[b] + 15) & ~15;
-                p2.add(p, kw, h->h_c0[b] >> 3, ts[t], 6, 0, 0, false, 4.0 * sp);
+                const int a = h->h_c0[b] & 7, m2 = h->h_m2[b], kw = (a + m2 + 15) & ~15;
+                for (int kp0 = 0; kp0 < kw; kp0 += 32) {
+                    const int nk = std::min(2, (kw - kp0) / 16);
+                    const int cc0 = std::max(kp0 - a, 0), ce = std::min(kp0 - a + 32, m2);
+                    TcmStep stp{};
+                    stp.raw = data + (size_t)cc0 * sp * 4;
+                    stp.b_kc = (h->h_c0[b] >> 3) + kp0 / 8;
+                    stp.meta = nk | (6 << 12);
+                    stp.rows = ts[t];
+                    stp.kp0 = kp0;
+                    stp.n16 = (ce - cc0) * sp / 4;
+                    stp.cc0 = cc0;
+                    stp.t0 = a;
+                    stp.t1 = m2;
+                    stp.t2 = -1;
+                    p2.add(stp, 16.0 * stp.n16);
+                }
             } else {
-                const int r = h->h_rank[b], r16 = (r + 15) & ~15;
-                const int r32 = mixed ? h->h_r32[b] : r, rr16 = mixed ? h->h_r16[b] : 0;
-                p2.add(p, r16, xkc + toff[b] * 2, ts[t], 6, r32, rr16, true, 4.0 * sp);
+                const int r = h->h_rank[b], kw = (r + 15) & ~15;
+                const int r32 = mixed ? h->h_r32[b] : r, r16 = mixed ? h->h_r16[b] : 0;
+                for (int kp0 = 0; kp0 < kw; kp0 += 32) {
+                    const int nk = std::min(2, (kw - kp0) / 16);
+                    const int mode = kp0 < r32 ? 6 : (kp0 < r32 + r16 ? 3 : 1);
+                    const int cc0 = far_chunk(kp0, r32, r16), ce = far_chunk(std::min(kp0 + 32, r) - 1, r32, r16) + 1;
+                    TcmStep stp{};
+                    stp.raw = data + (size_t)cc0 * sp * 4;
+                    stp.b_kc = xkc + toff[b] * 2 + kp0 / 8;
+                    stp.meta = nk | (mode << 12);
+                    stp.rows = ts[t];
+                    stp.kp0 = kp0;
+                    stp.n16 = (ce - cc0) * sp / 4;
+                    stp.cc0 = cc0;
+                    stp.t0 = r32;
+                    stp.t1 = r32 + r16;
+                    stp.t2 = r;
+                    p2.add(stp, 16.0 * stp.n16);
+                }
             }
         }
         all_tiles = all_tiles && started;
     }
     p1.finish();
     p2.finish();
-    // every step's B copy inside the operand buffer, every row count within 128 rows
+    // every step's B copy inside the operand buffer, its raw copy inside a raw stage,
+    // every row count within 128 rows, every stack row table inside its rows
     const long long bkc = xkc + tgroups * 2;
     for (const TcmPlan* L : {&p1, &p2})
         for (const TcmStep& sp : L->steps) {
             const int nk = sp.meta & 3;
-            if (nk < 1 || nk > 2 || sp.b_kc < 0 || sp.b_kc + 2 * nk > bkc || sp.rows < 1 || sp.rows > 128 ||
-                sp.src < 0 || sp.src >= (L == &p1 ? (int)stacks.size() : np)) {
+            bool bad = nk < 1 || nk > 2 || sp.b_kc < 0 || sp.b_kc + 2 * nk > bkc || sp.rows < 1 || sp.rows > 128;
+            if (L == &p1)
+                bad = bad || sp.n16 < 0 || sp.n16 >= (int)stacks.size() || stacks[sp.n16].nq > 128;
+            else  // whole slice columns of s_pad rows, at most 32 of them
+                bad = bad || sp.n16 < 1 || (4 * sp.n16) % ((sp.rows + 3) & ~3) != 0 ||
+                      (4 * sp.n16) / ((sp.rows + 3) & ~3) > 32 || sp.raw == nullptr;
+            if (bad) {
                 set_error("hmg_build_tensor_core_operands: internal error: a converted-operand step leaves its buffers");
                 return HMG_ERR_UNSUPPORTED;
             }
-        }
-    for (int v : kmap)
-        if (v < 0 || v >= tgroups * 2) {
-            set_error("hmg_build_tensor_core_operands: internal error: a t_b core lies outside its buffer");
-            return HMG_ERR_UNSUPPORTED;
         }
     // operand buffer of a product: X cores then t_b cores, three parts, 64 vectors
     const size_t bbytes = (size_t)bkc * 16 * TCM_NMAX * TCM_PARTS;
@@ -785,15 +1029,29 @@ hmg_status build_tcm(hmg_matrix* h)
                   cudaGetErrorString(ce));
         return ce == cudaErrorMemoryAllocation ? HMG_ERR_NOMEM : HMG_ERR_CUDA;
     }
+    int* d_far = nullptr;
+    long long* d_term = nullptr;
     if ((st = dalloc(reinterpret_cast<char**>(&h->tcm_stacks), std::max(stacks.size(), (size_t)1) * sizeof(TcmStack), s)) ||
-        (st = dalloc(&h->tcm_kmap, std::max(kmap.size(), (size_t)1), s))) {
+        (st = dalloc(&h->tcm_tscale, (size_t)std::max(tgroups * 16, 1ll), s)) ||
+        (st = dalloc(&d_far, std::max(far_blocks.size(), (size_t)1), s)) ||
+        (st = dalloc(&d_term, std::max(far_term.size(), (size_t)1), s))) {
+        dfree(d_far, s);
+        dfree(d_term, s);
         free_tcm(h);
         return st;
     }
     if (!stacks.empty())
         HMG_CUDA_TRY(cudaMemcpyAsync(h->tcm_stacks, stacks.data(), stacks.size() * sizeof(TcmStack), cudaMemcpyHostToDevice, s));
-    if (!kmap.empty())
-        HMG_CUDA_TRY(cudaMemcpyAsync(h->tcm_kmap, kmap.data(), kmap.size() * sizeof(int), cudaMemcpyHostToDevice, s));
+    if (!far_blocks.empty()) {
+        HMG_CUDA_TRY(cudaMemcpyAsync(d_far, far_blocks.data(), far_blocks.size() * sizeof(int), cudaMemcpyHostToDevice, s));
+        HMG_CUDA_TRY(cudaMemcpyAsync(d_term, far_term.data(), far_term.size() * sizeof(long long), cudaMemcpyHostToDevice, s));
+        const int nf = (int)far_blocks.size();
+        k_tcm_scales<<<ceil_div(nf, 8), 256, 0, s>>>(d_far, nf, h->rank, h->tier32, h->tier16, h->blk_m2, h->ptrV, d_term,
+                                                      mixed ? 1 : 0, h->tcm_tscale);
+        HMG_LAUNCH_CHECK();
+    }
+    dfree(d_far, s);
+    dfree(d_term, s);
     if ((st = upload_plan(h, 0, p1, grid)) || (st = upload_plan(h, 1, p2, grid))) {
         free_tcm(h);
         return st;
@@ -817,13 +1075,12 @@ static hmg_status tcm_product(hmg_matrix* h, int nrhs, const double* X, int ldx,
     const size_t smem = sizeof(TcmSmem);
     HMG_CUDA_TRY(cudaFuncSetAttribute(k_tcm_pass<0, NV>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     HMG_CUDA_TRY(cudaFuncSetAttribute(k_tcm_pass<1, NV>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    const PairDesc* desc = static_cast<const PairDesc*>(h->pair_desc);
     const TcmStack* stacks = static_cast<const TcmStack*>(h->tcm_stacks);
     if (h->tcm_njobs[0] > 0) {
         k_tcm_pass<0, NV><<<h->nsm, TCM_THREADS, smem, s>>>(
             reinterpret_cast<const TcmStep*>(h->tcm_steps[0]), reinterpret_cast<const TcmJob*>(h->tcm_jobs[0]),
-            reinterpret_cast<const int2*>(h->tcm_cta[0]), desc, stacks, h->ptrV, h->rank, h->tier32, h->tier16, bbuf,
-            xkc, h->tcm_kmap, 0, nullptr, 0, h->dev_err);
+            reinterpret_cast<const int2*>(h->tcm_cta[0]), stacks, bbuf, xkc, h->tcm_tscale, nullptr, 0, nullptr, 0,
+            h->dev_err);
         HMG_LAUNCH_CHECK();
     }
     if (!h->tcm_all_tiles)  // rows of tiles without products (all their blocks of rank 0) are zero
@@ -831,8 +1088,8 @@ static hmg_status tcm_product(hmg_matrix* h, int nrhs, const double* X, int ldx,
     if (h->tcm_njobs[1] > 0) {
         k_tcm_pass<1, NV><<<h->nsm, TCM_THREADS, smem, s>>>(
             reinterpret_cast<const TcmStep*>(h->tcm_steps[1]), reinterpret_cast<const TcmJob*>(h->tcm_jobs[1]),
-            reinterpret_cast<const int2*>(h->tcm_cta[1]), desc, stacks, h->ptrV, h->rank, h->tier32, h->tier16, bbuf,
-            0, h->perm[0], nrhs, Y, ldy, h->dev_err);
+            reinterpret_cast<const int2*>(h->tcm_cta[1]), stacks, bbuf, 0, nullptr, h->perm[0], nrhs, Y, ldy,
+            h->dev_err);
         HMG_LAUNCH_CHECK();
     }
     return HMG_OK;
@@ -841,8 +1098,6 @@ static hmg_status tcm_product(hmg_matrix* h, int nrhs, const double* X, int ldx,
 // 2..64 vectors in one pass: MMAs of N = 32 for up to 32 vectors, N = 64 above
 hmg_status matvec_multi_tcm(hmg_matrix* h, int nrhs, const double* X, int ldx, double* Y, int ldy)
 {
-    hmg_status st = ensure_desc(h, 4);  // the pair descriptors the converters read
-    if (st) return st;
     return nrhs > 32 ? tcm_product<64>(h, nrhs, X, ldx, Y, ldy) : tcm_product<32>(h, nrhs, X, ldx, Y, ldy);
 }
 
