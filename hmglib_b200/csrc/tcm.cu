@@ -17,18 +17,19 @@
 //     U_slice t_b (K = terms) and D_slice X_b (K = columns), written to Y rows.
 //
 // A step is 32 K positions (4 K cores) of one pair or stack.  Roles of a CTA (one per
-// SM, persistent, 12 warps), each a ring of stages with its own full / empty barriers:
-//   warp 6, the raw producer: copies the stored bytes of a step (pass 2: one run of
+// SM, persistent, 16 warps), each a ring of stages with its own full / empty barriers:
+//   warp 10, the raw producer: copies the stored bytes of a step (pass 2: one run of
 //     whole slice columns; pass 1: 9 16-byte chunks of every V row of the stack, the
 //     out-of-range ones zero-filled) into one of 5 raw stages with 16-byte cp.async,
 //     L2 evict-first, and writes the step's header (geometry, pass 1's row table);
-//   warps 7-11, the converters: all five share each step, an item being 32 rows x 1
-//     K core (one 16-byte row of each part per lane): they read the raw stage
-//     (conflict-free), decode FP16 / FP8 with warp-uniform branches, split, and store
-//     the parts into one of 3 A stages in shared memory;
-//   warp 4, lane 0: the B operand of each step (3-part X or t_b cores) by one bulk
+//   warps 11-15, the converters: all five share each step, an item being 32 rows x 1
+//     K core (one 16-byte row of each part per lane), two items at a time: they read
+//     the raw stage (conflict-free), decode FP16 / FP8 with warp-uniform branches,
+//     split with integer rounding (no conversion unit), and store the parts into one
+//     of 3 A stages in shared memory;
+//   warp 8, lane 0: the B operand of each step (3-part X or t_b cores) by one bulk
 //     copy into one of 3 B stages;
-//   warp 5, lane 0: the MMAs of a step.  The parts of a B K core lie side by side
+//   warp 9, lane 0: the MMAs of a step.  The parts of a B K core lie side by side
 //     along N, so per K16 one MMA of N = 3 NV gives A0 B0 (hi), A0 B1 and A0 B2, one of
 //     N = 2 NV adds A1 B0 and A1 B1 to the last two, and one of N = NV adds A2 B0 to the
 //     first correction: every part of A is read once, into three accumulators (hi,
@@ -36,7 +37,8 @@
 //     terms (A exact in two parts) runs A0 [B0 B1] and A1 B0; one in the FP8 terms
 //     (exact in one part) A0 B0.  tcgen05.commit then frees the A and B stages and
 //     signals the accumulators;
-//   warps 0-3: drain the accumulators after every step (tcgen05.ld) and keep the sums
+//   warps 0-7: drain the accumulators after every step (tcgen05.ld; warp w reads
+//     lanes 32 (w mod 4) .. + 31, half w / 4 of the vectors) and keep the sums
 //     hi + (c1 + c2) in FP32 registers, so no tensor-core accumulation runs longer than
 //     one step.
 // Every role reads its per-step records 32 at a time (one per lane) and the epilogue
@@ -69,17 +71,48 @@ static constexpr int TCM_RAW = 128 * TCM_RROW;               // a raw stage (>= 
 static constexpr int TCM_AST = TCM_KC * TCM_PARTS * 16 * 128;       // A of a step: 128 rows, 24 KB
 static constexpr int TCM_BST = TCM_KC * TCM_PARTS * TCM_NMAX * 16;  // B of a step at 64 vectors, 12 KB
 static constexpr int TCM_TMEM_COLS = 512;                    // two buffers of 3 NV accumulator columns
-static constexpr int TCM_CONV = 5;                           // converter warps
-static constexpr int TCM_THREADS = (7 + TCM_CONV) * 32;
+static constexpr int TCM_CONV = 5;                           // converter warps (11..15)
+static constexpr int TCM_EPI = 8;                            // epilogue warps (0..7)
+static constexpr int TCM_THREADS = (TCM_EPI + 3 + TCM_CONV) * 32;
 static constexpr int TCM_MAXMEM = 8;                         // blocks of a pass-1 stack (ranks rounded to 16)
 static constexpr int TCM_STGR = 40;                          // pass 1 epilogue staging: row stride (BF16)
 static_assert(2 * 3 * TCM_NMAX <= TCM_TMEM_COLS, "accumulators exceed the tensor memory allocation");
 
+// The K layout of a low-rank block's terms (t_b rows, U slice K positions, stack rows
+// of pass 1): its FP32, FP16 and FP8 terms each start a run of 8 K positions, so that
+// every K core holds terms of one storage tier (the padding positions are zero); the
+// block takes tcm_kw of them, a multiple of 16.  A block whose padded runs would pass
+// 128 positions (ranks near 128) keeps its terms back to back instead ("compact"),
+// and its K cores may then mix tiers.
+struct TcmTerms {
+    int r32, r16, r8;     // terms per tier
+    int r32p, r16p, r8p;  // the positions of each run
+    bool compact;
+};
+__host__ __device__ inline TcmTerms tcm_terms(int r, int r32, int r16)
+{
+    TcmTerms t;
+    t.r32 = r32;
+    t.r16 = r16;
+    t.r8 = r - r32 - r16;
+    t.r32p = (r32 + 7) & ~7;
+    t.r16p = (r16 + 7) & ~7;
+    t.r8p = (t.r8 + 7) & ~7;
+    t.compact = t.r32p + t.r16p + t.r8p > 128;
+    if (t.compact) {
+        t.r32p = t.r32;
+        t.r16p = t.r16;
+        t.r8p = t.r8;
+    }
+    return t;
+}
+__host__ __device__ inline int tcm_kw(const TcmTerms& t) { return (t.r32p + t.r16p + t.r8p + 15) & ~15; }
+
 // One step.  Pass 2 (one pair): raw = first byte of its raw copy, n16 chunks of 16
 // bytes; cc0 = the slice's chunk column there (a column of s_pad FP32 rows, a column of
 // FP16 pairs or of FP8 quads); near pair: t0 = a = c0 mod 8 (K position of column 0),
-// t1 = m2, t2 = -1; low-rank pair: K positions < t0 are FP32 terms, < t1 FP16, < t2
-// FP8.  Pass 1 (one stack): n16 = the stack, cc0 = first 16-byte chunk of the step's
+// t1 = m2, t2 = -1; low-rank pair (the K layout of TcmTerms): t0 = r32 | r32p << 16,
+// t1 = r16 | r16p << 16, t2 = r8 | compact << 16.  Pass 1 (one stack): n16 = the stack, cc0 = first 16-byte chunk of the step's
 // columns in a V row (may be negative), t0 = a, t1 = 16-byte chunks of a V row.
 struct TcmStep {
     const char* raw;
@@ -110,6 +143,11 @@ static_assert(sizeof(TcmStack) == 368, "TcmStack layout");
 struct TcmJob {
     int r0;    // pass 2: first Z row of the tile; pass 1: first t_b term of the stack
     int rows;  // pass 2: rows of the tile; pass 1: stack rows
+};
+
+// a step's geometry as the converters keep it in registers (read once per step)
+struct TcmGeo {
+    int cc0, t0, t1, t2;
 };
 
 // written by the raw producer beside each raw stage
@@ -171,27 +209,30 @@ __device__ __forceinline__ void fp8_run(unsigned w0, unsigned w1, unsigned w2, i
     v[4] = c.x; v[5] = c.y; v[6] = d.x; v[7] = d.y;
 }
 
+// BF16 rounding of x (to nearest, ties away from zero) as the FP32 bit pattern with
+// the low 16 bits clear
+__device__ __forceinline__ uint32_t bf16_rn_bits(float x) { return (__float_as_uint(x) + 0x8000u) & 0xffff0000u; }
+
 // the parts of 8 values of one operand row, one uint4 (8 K positions) each: part 0 is
-// the BF16 rounding, each further part the rounding of what the parts before miss
-// (exact differences in FP32; three parts hold an FP32 value exactly)
+// the BF16 rounding, each further part the rounding of what the parts before miss.
+// Every difference is exact in FP32, and what two parts miss has at most 8 significant
+// bits, so three parts hold an FP32 value exactly.  Integer adds, masks and byte
+// permutes only.
 __device__ __forceinline__ void store_parts(unsigned char* stage, int kc, int m, const float (&v)[8], int nparts)
 {
     uint32_t w0[4], w1[4], w2[4];
 #pragma unroll
     for (int k = 0; k < 4; k++) {
         const float a = v[2 * k], b = v[2 * k + 1];
-        const __nv_bfloat162 h = __floats2bfloat162_rn(a, b);
-        w0[k] = *reinterpret_cast<const uint32_t*>(&h);
+        const uint32_t ha = bf16_rn_bits(a), hb = bf16_rn_bits(b);
+        w0[k] = __byte_perm(ha, hb, 0x7632);
         if (nparts > 1) {
-            const float2 hf = __bfloat1622float2(h);
-            const float ra = a - hf.x, rb = b - hf.y;
-            const __nv_bfloat162 l = __floats2bfloat162_rn(ra, rb);
-            w1[k] = *reinterpret_cast<const uint32_t*>(&l);
-            if (nparts > 2) {
-                const float2 lf = __bfloat1622float2(l);
-                const __nv_bfloat162 l2 = __floats2bfloat162_rn(ra - lf.x, rb - lf.y);
-                w2[k] = *reinterpret_cast<const uint32_t*>(&l2);
-            }
+            const float ra = a - __uint_as_float(ha), rb = b - __uint_as_float(hb);
+            const uint32_t ma = bf16_rn_bits(ra), mb = bf16_rn_bits(rb);
+            w1[k] = __byte_perm(ma, mb, 0x7632);
+            if (nparts > 2)
+                w2[k] = __byte_perm(__float_as_uint(ra - __uint_as_float(ma)), __float_as_uint(rb - __uint_as_float(mb)),
+                                    0x7632);
         }
     }
     // row m of K core kc, part q: ((kc * 3 + q) * 16 + m / 8) * 128 + (m % 8) * 16
@@ -201,9 +242,33 @@ __device__ __forceinline__ void store_parts(unsigned char* stage, int kc, int m,
     if (nparts > 2) *reinterpret_cast<uint4*>(base + 2 * 16 * 128) = make_uint4(w2[0], w2[1], w2[2], w2[3]);
 }
 
+// Pass 2, a K core of a compact low-rank block (TcmTerms), whose tiers may meet inside
+// it: position by position
+__device__ __forceinline__ void load_pass2_compact(const unsigned* rw, int sp, int m, int cc0, int k0, int r32, int r16,
+                                                   int r8, float (&v)[8])
+{
+    auto word = [&](int c) -> unsigned { return rw[(c - cc0) * sp + m]; };
+    const int e16 = r32 + r16, r = e16 + r8, c8 = r32 + (r16 >> 1);
+#pragma unroll
+    for (int e = 0; e < 8; e++) {
+        const int kp = k0 + e;
+        float x = 0.0f;
+        if (kp < r32) {
+            x = __uint_as_float(word(kp));
+        } else if (kp < e16) {
+            const float2 f = h2f2(word(r32 + ((kp - r32) >> 1)));
+            x = ((kp - r32) & 1) ? f.y : f.x;
+        } else if (kp < r) {
+            const float2 f = e4m3x2_f2(word(c8 + ((kp - e16) >> 2)) >> (8 * ((kp - e16) & 2)));
+            x = ((kp - e16) & 1) ? f.y : f.x;
+        }
+        v[e] = x;
+    }
+}
+
 // Pass 2, one item: row m (lane) of K core kc.  Word (c, m) of raw chunk column c is at
 // rw[(c - cc0) * sp + m]: consecutive lanes read consecutive words.
-__device__ __forceinline__ void load_pass2(const TcmHdr& H, const unsigned* rw, int sp, int m, int k0, float (&v)[8])
+__device__ __forceinline__ void load_pass2(const TcmGeo H, const unsigned* rw, int sp, int m, int k0, float (&v)[8])
 {
     const int cc0 = H.cc0;
     auto word = [&](int c) -> unsigned { return rw[(c - cc0) * sp + m]; };
@@ -218,55 +283,38 @@ __device__ __forceinline__ void load_pass2(const TcmHdr& H, const unsigned* rw, 
         }
         return;
     }
-    const int r32 = H.t0, e16 = H.t1, r = H.t2, c8 = r32 + ((e16 - r32) >> 1);  // chunk column of FP8 quad 0
-    if (k0 + 8 <= r32) {
+    // low-rank slice: one tier per K core (TcmTerms); chunk columns r32 FP32 terms, then
+    // r16 / 2 FP16 pairs, then r8 / 4 FP8 quads
+    const int r32 = H.t0 & 0xffff, r32p = H.t0 >> 16, r16 = H.t1 & 0xffff, r16p = H.t1 >> 16, r8 = H.t2 & 0xffff;
+    if (H.t2 >> 16) {
+        load_pass2_compact(rw, sp, m, cc0, k0, r32, r16, r8, v);
+        return;
+    }
+    if (k0 < r32p) {
 #pragma unroll
-        for (int e = 0; e < 8; e++) v[e] = __uint_as_float(word(k0 + e));
-    } else if (k0 >= r32 && k0 + 8 <= e16) {
-        // FP16 pairs: term r32 + 2g + t in half t of word g; p = the first term's half
-        const int g0 = r32 + ((k0 - r32) >> 1), p = (k0 - r32) & 1;
-        unsigned w[5];
-#pragma unroll
-        for (int i = 0; i < 4; i++) w[i] = word(g0 + i);
-        w[4] = p ? word(g0 + 4) : 0u;
+        for (int e = 0; e < 8; e++) v[e] = k0 + e < r32 ? __uint_as_float(word(k0 + e)) : 0.0f;
+    } else if (k0 < r32p + r16p) {
+        // FP16 pairs: term 2g + t of the tier in half t of word g
+        const int g0 = (k0 - r32p) >> 1;
 #pragma unroll
         for (int i = 0; i < 4; i++) {
-            const float2 f = h2f2(p ? __byte_perm(w[i], w[i + 1], 0x5432) : w[i]);
+            const float2 f = 2 * (g0 + i) < r16 ? h2f2(word(r32 + g0 + i)) : make_float2(0.0f, 0.0f);
             v[2 * i] = f.x;
             v[2 * i + 1] = f.y;
         }
-    } else if (k0 >= e16 && k0 + 8 <= r) {
-        // FP8 quads: term e16 + 4g + t in byte t of word g
-        const int g0 = c8 + ((k0 - e16) >> 2), p = (k0 - e16) & 3;
-        fp8_run(word(g0), word(g0 + 1), p ? word(g0 + 2) : 0u, p, v);
     } else {
-#pragma unroll
-        for (int e = 0; e < 8; e++) {
-            const int kp = k0 + e;
-            float x = 0.0f;
-            if (kp < r32) {
-                x = __uint_as_float(word(kp));
-            } else if (kp < e16) {
-                const unsigned w = word(r32 + ((kp - r32) >> 1));
-                const float2 f = h2f2(w);
-                x = ((kp - r32) & 1) ? f.y : f.x;
-            } else if (kp < r) {
-                const unsigned w = word(c8 + ((kp - e16) >> 2));
-                const float2 f = e4m3x2_f2(w >> (8 * ((kp - e16) & 2)));
-                x = ((kp - e16) & 1) ? f.y : f.x;
-            }
-            v[e] = x;
-        }
+        // FP8 quads: term 4g + t of the tier in byte t of word g
+        const int g0 = (k0 - r32p - r16p) >> 2, c8 = r32 + (r16 >> 1);
+        const unsigned w0 = 4 * g0 < r8 ? word(c8 + g0) : 0u, w1 = 4 * (g0 + 1) < r8 ? word(c8 + g0 + 1) : 0u;
+        fp8_run(w0, w1, 0u, 0, v);
     }
 }
 
 // Pass 1, one item: stack row m (lane) of K core kc: the 8 words at sh + 8 kc of its raw
 // row (three 16-byte reads; rows 144 bytes apart, so 8 consecutive rows hit 8 distinct
 // bank groups), decoded by the row's tier.
-__device__ __forceinline__ void load_pass1(const TcmHdr& H, const unsigned char* raw, int sh, int m, int kc,
-                                           float (&v)[8])
+__device__ __forceinline__ void load_pass1(const unsigned ent, const unsigned char* raw, int sh, int kc, float (&v)[8])
 {
-    const unsigned ent = H.rtab[m];
     const int tier = (ent >> 8) & 3, sel = (ent >> 10) & 3;
 #pragma unroll
     for (int e = 0; e < 8; e++) v[e] = 0.0f;
@@ -302,6 +350,30 @@ __device__ __forceinline__ void load_pass1(const TcmHdr& H, const unsigned char*
             const float2 f = e4m3x2_f2(__byte_perm(w[2 * i], w[2 * i + 1], s2));
             v[2 * i] = f.x;
             v[2 * i + 1] = f.y;
+        }
+    }
+}
+
+// A bounded wait whose polls sleep in the barrier (up to 100 us each, or until the
+// phase completes) instead of spinning: most warps of the pass kernel wait most of the
+// time, and spinning ones would take issue slots from the converters.  false (and *err
+// set) after ~2^31 cycles, as mbar_wait.
+__device__ __forceinline__ bool mbar_wait_s(uint64_t* bar, unsigned parity, int* err, int code)
+{
+    const long long t0 = clock64();
+    for (;;) {
+        unsigned ok;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}"
+            : "=r"(ok)
+            : "r"(smem_u32(bar)), "r"(parity), "r"(100000u)
+            : "memory");
+        if (ok) return true;
+        if (clock64() - t0 > (1ll << 31)) {
+            atomicCAS(err, 0, code);
+            return false;
         }
     }
 }
@@ -343,13 +415,13 @@ __global__ void __launch_bounds__(TCM_THREADS, 1)
         }
         for (int b = 0; b < 2; b++) {
             mbar_init(&sm.accf[b], 1);
-            mbar_init(&sm.acce[b], 4);
+            mbar_init(&sm.acce[b], TCM_EPI);
         }
         mbar_init(&sm.fin, 1);
         sm.fail = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
-    if (warp == 5) {
+    if (warp == 9) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&sm.tmem)),
                      "n"(TCM_TMEM_COLS));
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
@@ -358,19 +430,21 @@ __global__ void __launch_bounds__(TCM_THREADS, 1)
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const uint32_t tmem = sm.tmem;
 
-    if (warp >= 7) {
-        // ---- converters: every step, items (32 rows, 1 K core) dealt over the warps ----
-        const int cw = warp - 7;
+    if (warp >= 11) {
+        // ---- converters: every step, items (32 rows, 1 K core) dealt over the warps,
+        // two at a time ----
+        const int cw = warp - 11;
         for (int i = 0; i < nsteps; i++) {
             const int slot = i % TCM_NR, as = i % TCM_NA;
-            bool ok = !*fail && mbar_wait(&sm.raw_full[slot], (i / TCM_NR) & 1, err, 31);
-            if (ok && i >= TCM_NA) ok = mbar_wait(&sm.a_empty[as], ((i / TCM_NA) - 1) & 1, err, 32);
+            bool ok = !*fail && mbar_wait_s(&sm.raw_full[slot], (i / TCM_NR) & 1, err, 31);
+            if (ok && i >= TCM_NA) ok = mbar_wait_s(&sm.a_empty[as], ((i / TCM_NA) - 1) & 1, err, 32);
             if (!__all_sync(~0u, ok)) {
                 *fail = 1;
                 break;
             }
             const TcmHdr& H = sm.hdr[slot];
             const int meta = H.meta, rows = H.rows, kp0 = H.kp0;
+            const TcmGeo G{H.cc0, H.t0, H.t1, H.t2};
             const int lg = (meta & 3) == 2 ? 2 : 1, nkc = 1 << lg;  // K cores of the step
             const int mode = (meta >> 12) & 15, nparts = MODE == 0 ? 3 : (mode >= 6 ? 3 : (mode >= 3 ? 2 : 1));
             const int nitems = ((rows + 31) >> 5) << lg;
@@ -379,20 +453,36 @@ __global__ void __launch_bounds__(TCM_THREADS, 1)
                 const int sp = (rows + 3) & ~3;
                 const unsigned* rw = reinterpret_cast<const unsigned*>(sm.raw[slot]);
 #pragma unroll 1
-                for (int it = cw; it < nitems; it += TCM_CONV) {
+                for (int it = cw; it < nitems; it += 2 * TCM_CONV) {
+                    const int it2 = it + TCM_CONV;
                     const int kc = it & (nkc - 1), m = (it >> lg) * 32 + lane;
-                    float v[8];
-                    load_pass2(H, rw, sp, m, kp0 + 8 * kc, v);
+                    const int kc2 = it2 & (nkc - 1), m2 = (it2 >> lg) * 32 + lane;
+                    float v[8], v2[8];
+                    load_pass2(G, rw, sp, m, kp0 + 8 * kc, v);
+                    if (it2 < nitems) load_pass2(G, rw, sp, m2, kp0 + 8 * kc2, v2);
                     store_parts(stage, kc, m, v, nparts);
+                    if (it2 < nitems) store_parts(stage, kc2, m2, v2, nparts);
                 }
             } else {
-                const int sh = (kp0 - H.t0) & 3;
-#pragma unroll 1
-                for (int it = cw; it < nitems; it += TCM_CONV) {
+                const int sh = (kp0 - G.t0) & 3;
+                // the row-table entries of this warp's items, read before any item is stored
+                unsigned ent[4];
+#pragma unroll
+                for (int j = 0; j < 4; j++) {
+                    const int it = cw + j * TCM_CONV;
+                    ent[j] = it < nitems ? H.rtab[(it >> lg) * 32 + lane] : (3u << 8);
+                }
+#pragma unroll
+                for (int j = 0; j < 4; j += 2) {
+                    const int it = cw + j * TCM_CONV, it2 = it + TCM_CONV;
+                    if (it >= nitems) break;
                     const int kc = it & (nkc - 1), m = (it >> lg) * 32 + lane;
-                    float v[8];
-                    load_pass1(H, sm.raw[slot], sh, m, kc, v);
+                    const int kc2 = it2 & (nkc - 1), m2 = (it2 >> lg) * 32 + lane;
+                    float v[8], v2[8];
+                    load_pass1(ent[j], sm.raw[slot], sh, kc, v);
+                    if (it2 < nitems) load_pass1(ent[j + 1], sm.raw[slot], sh, kc2, v2);
                     store_parts(stage, kc, m, v, 3);
+                    if (it2 < nitems) store_parts(stage, kc2, m2, v2, 3);
                 }
             }
             // the generic-proxy stores become visible to the tensor cores' (async) proxy
@@ -403,7 +493,7 @@ __global__ void __launch_bounds__(TCM_THREADS, 1)
                 mbar_arrive(&sm.raw_empty[slot]);
             }
         }
-    } else if (warp == 6) {
+    } else if (warp == 10) {
         // ---- raw producer: the stored bytes of every step, 16-byte cp.async per lane ----
         uint64_t pol;
         asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(pol));
@@ -443,7 +533,7 @@ __global__ void __launch_bounds__(TCM_THREADS, 1)
                 }
                 if (i >= TCM_NR) {
                     bool w = true;
-                    if (lane == 0) w = !*fail && mbar_wait(&sm.raw_empty[slot], ((i / TCM_NR) - 1) & 1, err, 33);
+                    if (lane == 0) w = !*fail && mbar_wait_s(&sm.raw_empty[slot], ((i / TCM_NR) - 1) & 1, err, 33);
                     if (!__shfl_sync(~0u, w, 0)) {
                         *fail = 1;
                         ok = false;
@@ -485,7 +575,7 @@ __global__ void __launch_bounds__(TCM_THREADS, 1)
         // every copy of this warp has landed before the CTA leaves
         asm volatile("cp.async.wait_all;" ::: "memory");
         __syncwarp();
-    } else if (warp == 4) {
+    } else if (warp == 8) {
         // ---- B operand of every step: one bulk copy, lane 0 ----
         int issued = 0;
         bool ok = true;
@@ -503,7 +593,7 @@ __global__ void __launch_bounds__(TCM_THREADS, 1)
                 const long long b_kc = __shfl_sync(~0u, bk, k);
                 bool w = true;
                 if (lane == 0) {
-                    if (i >= TCM_NB) w = !*fail && mbar_wait(&sm.b_empty[slot], ((i / TCM_NB) - 1) & 1, err, 34);
+                    if (i >= TCM_NB) w = !*fail && mbar_wait_s(&sm.b_empty[slot], ((i / TCM_NB) - 1) & 1, err, 34);
                     if (w) {
                         const unsigned bytes = (unsigned)(2 * (meta & 3)) * KB;
                         mbar_arrive_expect_tx(&sm.b_full[slot], bytes);
@@ -521,9 +611,9 @@ __global__ void __launch_bounds__(TCM_THREADS, 1)
         // the last copy into every stage has landed before the CTA leaves
         if (lane == 0)
             for (int s = 0; s < TCM_NB && s < issued; s++)
-                mbar_wait(&sm.b_full[(issued - 1 - s) % TCM_NB], ((issued - 1 - s) / TCM_NB) & 1, err, 35);
+                mbar_wait_s(&sm.b_full[(issued - 1 - s) % TCM_NB], ((issued - 1 - s) / TCM_NB) & 1, err, 35);
         __syncwarp();
-    } else if (warp == 5) {
+    } else if (warp == 9) {
         // ---- MMAs, lane 0: one per part of A, over the B parts side by side along N ----
         constexpr uint32_t LBA = P * 16 * 128, LBB = KB;  // K-core strides of A and B
         bool ok = true;
@@ -535,10 +625,10 @@ __global__ void __launch_bounds__(TCM_THREADS, 1)
                 const int meta = __shfl_sync(~0u, mt, k);
                 bool w = true;
                 if (lane == 0) {
-                    w = !*fail && mbar_wait(&sm.a_full[as], (i / TCM_NA) & 1, err, 36) &&
-                        mbar_wait(&sm.b_full[bs], (i / TCM_NB) & 1, err, 37);
+                    w = !*fail && mbar_wait_s(&sm.a_full[as], (i / TCM_NA) & 1, err, 36) &&
+                        mbar_wait_s(&sm.b_full[bs], (i / TCM_NB) & 1, err, 37);
                     // the epilogue has read this buffer's previous step
-                    if (w && i >= 2) w = mbar_wait(&sm.acce[buf], ((i >> 1) - 1) & 1, err, 38);
+                    if (w && i >= 2) w = mbar_wait_s(&sm.acce[buf], ((i >> 1) - 1) & 1, err, 38);
                     if (w) {
                         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
                         const int nk = meta & 3, mode = (meta >> 12) & 15;
@@ -575,13 +665,16 @@ __global__ void __launch_bounds__(TCM_THREADS, 1)
         }
         if (lane == 0) {
             tc_commit(&sm.fin);  // every MMA issued here has completed before tensor memory is freed
-            mbar_wait(&sm.fin, 0, err, 39);
+            mbar_wait_s(&sm.fin, 0, err, 39);
         }
         __syncwarp();
     } else {
-        // ---- epilogue: warp w owns accumulator rows 32w..32w+31 ----
-        const int row = warp * 32 + lane;
-        float f[NV];
+        // ---- epilogue: warp w owns accumulator rows 32 (w mod 4) .. + 31 and vectors
+        // HV (w / 4) .. + HV - 1 ----
+        constexpr int HV = NV / 2;
+        const int q4 = warp & 3, hv = warp >> 2;
+        const int row = q4 * 32 + lane;
+        float f[HV];
         const int njobs = hi.x - lo.x;
         const TcmJob* my_jobs = jobs + lo.x;
         // job jc's rows, first row / term and per-row value (Y row or term scale) are
@@ -613,26 +706,26 @@ __global__ void __launch_bounds__(TCM_THREADS, 1)
                     cur_val = jc + 1 < njobs ? row_value(cur) : 0u;
                     nxt = jc + 2 < njobs ? my_jobs[jc + 2] : TcmJob{0, 0};
                 }
-                if (!__all_sync(~0u, !*fail && mbar_wait(&sm.accf[buf], (i >> 1) & 1, err, 40))) {
+                if (!__all_sync(~0u, !*fail && mbar_wait_s(&sm.accf[buf], (i >> 1) & 1, err, 40))) {
                     ok = false;
                     break;
                 }
                 asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-                const uint32_t taddr = tmem + (uint32_t)(buf * 3 * NV) + ((uint32_t)(warp * 32) << 16);
-                // 8 columns of each accumulator at a time: the running sums f[NV] stay in
+                const uint32_t taddr = tmem + (uint32_t)(buf * 3 * NV + hv * HV) + ((uint32_t)(q4 * 32) << 16);
+                // 16 columns of each accumulator at a time: the running sums f[HV] stay in
                 // registers beside them
 #pragma unroll
-                for (int h = 0; h < NV / 8; h++) {
-                    uint32_t v[8], c1[8], c2[8];
-                    tc_ld8(taddr + 8 * h, v);
-                    if (mode > 1) tc_ld8(taddr + NV + 8 * h, c1);
-                    if (mode > 3) tc_ld8(taddr + 2 * NV + 8 * h, c2);
+                for (int h = 0; h < HV / 16; h++) {
+                    uint32_t v[16], c1[16], c2[16];
+                    tc_ld16(taddr + 16 * h, v);
+                    if (mode > 1) tc_ld16(taddr + NV + 16 * h, c1);
+                    if (mode > 3) tc_ld16(taddr + 2 * NV + 16 * h, c2);
                     asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 #pragma unroll
-                    for (int q = 0; q < 8; q++) {
+                    for (int q = 0; q < 16; q++) {
                         const float c = mode > 1 ? __uint_as_float(c1[q]) + (mode > 3 ? __uint_as_float(c2[q]) : 0.0f) : 0.0f;
                         const float tv = __uint_as_float(v[q]) + c;
-                        f[8 * h + q] = first ? tv : f[8 * h + q] + tv;
+                        f[16 * h + q] = first ? tv : f[16 * h + q] + tv;
                     }
                 }
                 asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -642,36 +735,37 @@ __global__ void __launch_bounds__(TCM_THREADS, 1)
                 jc++;
                 if (MODE == 1) {
                     if (row < rows) {
-                        double* y = Y + (int)val;
+                        double* y = Y + (int)val + (size_t)(hv * HV) * ldy;
 #pragma unroll
-                        for (int q = 0; q < NV; q++)
-                            if (q < nrhs) y[(size_t)q * ldy] = (double)f[q];
+                        for (int q = 0; q < HV; q++)
+                            if (hv * HV + q < nrhs) y[(size_t)q * ldy] = (double)f[q];
                     }
                 } else {
-                    // term row -> 3-part B cores of pass 2 through the warp's staging
+                    // term row -> 3-part B cores of pass 2 through the quarter's staging
                     // array [vector][row] (rows padded to 40: the 16-byte reads of 8
-                    // consecutive vectors hit distinct bank groups)
-                    __nv_bfloat16* stg = sm.stg[warp];
+                    // consecutive vectors hit distinct bank groups); the two warps of a
+                    // quarter fill and read disjoint vectors of it
+                    __nv_bfloat16* stg = sm.stg[q4];
                     const float scale = __uint_as_float(val);
 #pragma unroll
-                    for (int q = 0; q < NV; q++) f[q] *= scale;
+                    for (int q = 0; q < HV; q++) f[q] *= scale;
                     // part p: the BF16 rounding of what parts 0..p-1 miss, f keeping the rest
 #pragma unroll 1
                     for (int part = 0; part < P; part++) {
                         if (part > 0) {
 #pragma unroll
-                            for (int q = 0; q < NV; q++) f[q] -= __bfloat162float(__float2bfloat16_rn(f[q]));
+                            for (int q = 0; q < HV; q++) f[q] -= __bfloat162float(__float2bfloat16_rn(f[q]));
                         }
 #pragma unroll
-                        for (int q = 0; q < NV; q++) stg[q * TCM_STGR + lane] = __float2bfloat16_rn(f[q]);
+                        for (int q = 0; q < HV; q++) stg[(hv * HV + q) * TCM_STGR + lane] = __float2bfloat16_rn(f[q]);
                         __syncwarp();
                         uint4* dst = reinterpret_cast<uint4*>(Bbuf);
 #pragma unroll 1
-                        for (int u = lane; u < 4 * NV; u += 32) {
-                            // K core kcl (rows 8 kcl .. 8 kcl + 7 of the warp) of vector vq
-                            const int kcl = u / NV, vq = u % NV;
-                            if (warp * 4 + kcl < (rows >> 3))
-                                dst[((size_t)(tb_kc + (r0 >> 3) + warp * 4 + kcl) * P + part) * NV + vq] =
+                        for (int u = lane; u < 4 * HV; u += 32) {
+                            // K core kcl (rows 8 kcl .. 8 kcl + 7 of the quarter) of vector vq
+                            const int kcl = u / HV, vq = hv * HV + u % HV;
+                            if (q4 * 4 + kcl < (rows >> 3))
+                                dst[((size_t)(tb_kc + (r0 >> 3) + q4 * 4 + kcl) * P + part) * NV + vq] =
                                     *reinterpret_cast<const uint4*>(stg + vq * TCM_STGR + 8 * kcl);
                         }
                         __syncwarp();
@@ -682,14 +776,14 @@ __global__ void __launch_bounds__(TCM_THREADS, 1)
         if (!ok) *fail = 1;
     }
     __syncthreads();
-    if (warp == 5) {
+    if (warp == 9) {
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "n"(TCM_TMEM_COLS));
     }
 }
 
-// scale of every t_b term: su_l sv_l for the FP16 / FP8 terms of mixed storage, else 1
-// (padding terms up to the rank rounded to 16 included); one warp per block
+// scale of every t_b term (K position of TcmTerms): su_l sv_l for the FP16 / FP8 terms
+// of mixed storage, else 1 (padding included); one warp per block
 __global__ void k_tcm_scales(const int* __restrict__ far, int nfar, const int* __restrict__ rank,
                              const int* __restrict__ tier32, const int* __restrict__ tier16,
                              const int* __restrict__ blk_m2, void* const* ptrV, const long long* __restrict__ tterm,
@@ -697,14 +791,17 @@ __global__ void k_tcm_scales(const int* __restrict__ far, int nfar, const int* _
 {
     const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
     if (w >= nfar) return;
-    const int b = far[w], r = rank[b], r16p = (r + 15) & ~15;
-    const int r32 = tier32[b], r16 = tier16[b];
+    const int b = far[w], r = rank[b];
+    const TcmTerms T = tcm_terms(r, tier32[b], tier16[b]);
     const size_t m2p = (size_t)((blk_m2[b] + 3) & ~3);
-    const float* scal =
-        reinterpret_cast<const float*>(static_cast<const char*>(ptrV[b]) + m2p * (4 * (size_t)r32 + 2 * (size_t)r16 +
-                                                                                  (size_t)(r - r32 - r16)));
-    for (int l = lane; l < r16p; l += 32)
-        tscale[tterm[w] + l] = (mixed && l >= r32 && l < r) ? scal[l] : 1.0f;
+    const float* scal = reinterpret_cast<const float*>(static_cast<const char*>(ptrV[b]) +
+                                                       m2p * (4 * (size_t)T.r32 + 2 * (size_t)T.r16 + (size_t)T.r8));
+    for (int k = lane; k < tcm_kw(T); k += 32) {
+        int l = -1;
+        if (k >= T.r32p && k < T.r32p + T.r16) l = T.r32 + (k - T.r32p);
+        else if (k >= T.r32p + T.r16p && k < T.r32p + T.r16p + T.r8) l = T.r32 + T.r16 + (k - T.r32p - T.r16p);
+        tscale[tterm[w] + k] = (mixed && l >= 0) ? scal[l] : 1.0f;
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -819,8 +916,6 @@ hmg_status upload_plan(hmg_matrix* h, int q, const TcmPlan& L, int grid)
     return HMG_OK;
 }
 
-// chunk column of K position k of a low-rank slice: FP32 terms, then FP16 pairs, then FP8 quads
-inline int far_chunk(int k, int r32, int r16) { return k < r32 ? k : (k < r32 + r16 ? r32 + (k - r32) / 2 : r32 + r16 / 2 + (k - r32 - r16) / 4); }
 
 }  // namespace
 
@@ -839,7 +934,9 @@ hmg_status build_tcm(hmg_matrix* h)
         return HMG_ERR_STATE;
     }
     for (int b = h->ndense; b < h->nblocks; b++)
-        if (((h->h_rank[b] + 15) & ~15) > 128) {
+        if (h->h_rank[b] > 0 &&
+            tcm_kw(tcm_terms(h->h_rank[b], h->far_prec == HMG_PREC_MIXED ? h->h_r32[b] : h->h_rank[b],
+                             h->far_prec == HMG_PREC_MIXED ? h->h_r16[b] : 0)) > 128) {
             set_error("hmg_build_tensor_core_operands: block %d has rank %d (> 128)", b, h->h_rank[b]);
             return HMG_ERR_UNSUPPORTED;
         }
@@ -867,6 +964,9 @@ hmg_status build_tcm(hmg_matrix* h)
         std::vector<int> far;
         for (int b = h->ndense; b < nb; b++)
             if (h->h_rank[b] > 0) far.push_back(b);
+        auto terms = [&](int b) {
+            return tcm_terms(h->h_rank[b], mixed ? h->h_r32[b] : h->h_rank[b], mixed ? h->h_r16[b] : 0);
+        };
         std::stable_sort(far.begin(), far.end(), [&](int x, int y) {
             if (h->h_c0[x] != h->h_c0[y]) return h->h_c0[x] < h->h_c0[y];
             if (h->h_m2[x] != h->h_m2[y]) return h->h_m2[x] < h->h_m2[y];
@@ -878,15 +978,15 @@ hmg_status build_tcm(hmg_matrix* h)
             std::vector<std::vector<int>> members;
             std::vector<int> fill;
             for (size_t i = g0; i < g1; i++) {
-                const int b = far[i], r16 = (h->h_rank[b] + 15) & ~15;
+                const int b = far[i], kwb = tcm_kw(terms(b));
                 size_t k = 0;
-                while (k < members.size() && fill[k] + r16 > 128) k++;
+                while (k < members.size() && fill[k] + kwb > 128) k++;
                 if (k == members.size()) {
                     members.emplace_back();
                     fill.push_back(0);
                 }
                 members[k].push_back(b);
-                fill[k] += r16;
+                fill[k] += kwb;
             }
             const int c0 = h->h_c0[far[g0]], m2 = h->h_m2[far[g0]], a = c0 & 7, kw = (a + m2 + 15) & ~15;
             const int m2p4 = ((m2 + 3) & ~3) / 4;
@@ -898,23 +998,25 @@ hmg_status build_tcm(hmg_matrix* h)
                 const long long tg0 = tgroups;
                 int off = 0, q = 0;
                 for (int u = 0; u < sk.nmem; u++) {
-                    const int b = members[k][u], r = h->h_rank[b], r16p = (r + 15) & ~15;
-                    const int r32 = mixed ? h->h_r32[b] : r, r16 = mixed ? h->h_r16[b] : 0, r8 = r - r32 - r16;
+                    const int b = members[k][u];
+                    const TcmTerms T = terms(b);
+                    const int kwb = tcm_kw(T);
                     sk.vptr[u] = static_cast<const char*>(pv[b]);
                     sk.qb[u] = q;
-                    for (int l = 0; l < r; l++) {
-                        int qq, tier, sel;
-                        if (l < r32) { qq = q + l; tier = 0; sel = 0; }
-                        else if (l < r32 + r16) { qq = q + r32 + (l - r32) / 2; tier = 1; sel = (l - r32) & 1; }
-                        else { qq = q + r32 + r16 / 2 + (l - r32 - r16) / 4; tier = 2; sel = (l - r32 - r16) & 3; }
-                        sk.rtab[off + l] = (uint16_t)(qq | tier << 8 | sel << 10);
-                    }
+                    // stack rows in the K layout of TcmTerms: FP32 term rows, FP16 pair rows
+                    // (two terms each), FP8 quad rows (four terms each), padding rows zero
+                    for (int t = 0; t < T.r32; t++) sk.rtab[off + t] = (uint16_t)(q + t);
+                    for (int t = 0; t < T.r16; t++)
+                        sk.rtab[off + T.r32p + t] = (uint16_t)((q + T.r32 + t / 2) | 1 << 8 | (t & 1) << 10);
+                    for (int t = 0; t < T.r8; t++)
+                        sk.rtab[off + T.r32p + T.r16p + t] =
+                            (uint16_t)((q + T.r32 + T.r16 / 2 + t / 4) | 2 << 8 | (t & 3) << 10);
                     toff[b] = tgroups;
                     far_blocks.push_back(b);
                     far_term.push_back(tgroups * 16);
-                    tgroups += r16p / 16;
-                    off += r16p;
-                    q += r32 + r16 / 2 + r8 / 4;
+                    tgroups += kwb / 16;
+                    off += kwb;
+                    q += T.r32 + T.r16 / 2 + T.r8 / 4;
                 }
                 sk.nq = q;
                 const int job = (int)stacks.size();
@@ -977,23 +1079,38 @@ hmg_status build_tcm(hmg_matrix* h)
                     p2.add(stp, 16.0 * stp.n16);
                 }
             } else {
-                const int r = h->h_rank[b], kw = (r + 15) & ~15;
-                const int r32 = mixed ? h->h_r32[b] : r, r16 = mixed ? h->h_r16[b] : 0;
+                const TcmTerms T = tcm_terms(h->h_rank[b], mixed ? h->h_r32[b] : h->h_rank[b], mixed ? h->h_r16[b] : 0);
+                const int kw = tcm_kw(T);
+                // chunk column of K position k, or -1 for a padding position
+                auto chunk = [&](int k) -> int {
+                    if (k < T.r32p) return k < T.r32 ? k : -1;
+                    k -= T.r32p;
+                    if (k < T.r16p) return k < T.r16 ? T.r32 + k / 2 : -1;
+                    k -= T.r16p;
+                    return k < T.r8 ? T.r32 + T.r16 / 2 + k / 4 : -1;
+                };
                 for (int kp0 = 0; kp0 < kw; kp0 += 32) {
                     const int nk = std::min(2, (kw - kp0) / 16);
-                    const int mode = kp0 < r32 ? 6 : (kp0 < r32 + r16 ? 3 : 1);
-                    const int cc0 = far_chunk(kp0, r32, r16), ce = far_chunk(std::min(kp0 + 32, r) - 1, r32, r16) + 1;
+                    const int mode = kp0 < T.r32p ? 6 : (kp0 < T.r32p + T.r16p ? 3 : 1);
+                    int cc0 = 1 << 30, ce = -1;
+                    for (int k = kp0; k < kp0 + 16 * nk; k++) {
+                        const int c = chunk(k);
+                        if (c >= 0) {
+                            cc0 = std::min(cc0, c);
+                            ce = std::max(ce, c + 1);
+                        }
+                    }
                     TcmStep stp{};
-                    stp.raw = data + (size_t)cc0 * sp * 4;
+                    stp.raw = ce > cc0 ? data + (size_t)cc0 * sp * 4 : nullptr;
                     stp.b_kc = xkc + toff[b] * 2 + kp0 / 8;
                     stp.meta = nk | (mode << 12);
                     stp.rows = ts[t];
                     stp.kp0 = kp0;
-                    stp.n16 = (ce - cc0) * sp / 4;
+                    stp.n16 = ce > cc0 ? (ce - cc0) * sp / 4 : 0;
                     stp.cc0 = cc0;
-                    stp.t0 = r32;
-                    stp.t1 = r32 + r16;
-                    stp.t2 = r;
+                    stp.t0 = T.r32 | T.r32p << 16;
+                    stp.t1 = T.r16 | T.r16p << 16;
+                    stp.t2 = T.r8 | (T.compact ? 1 << 16 : 0);
                     p2.add(stp, 16.0 * stp.n16);
                 }
             }
