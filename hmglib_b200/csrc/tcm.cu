@@ -23,10 +23,9 @@
 //     out-of-range ones zero-filled) into one of 5 raw stages with 16-byte cp.async,
 //     L2 evict-first, and writes the step's header (geometry, pass 1's row table);
 //   warps 11-15, the converters: all five share each step, an item being 32 rows x 1
-//     K core (one 16-byte row of each part per lane), two items at a time: they read
-//     the raw stage (conflict-free), decode FP16 / FP8 with warp-uniform branches,
-//     split with integer rounding (no conversion unit), and store the parts into one
-//     of 3 A stages in shared memory;
+//     K core (one 16-byte row of each part per lane): they read the raw stage
+//     (conflict-free), decode FP16 / FP8 with warp-uniform branches, split, and store
+//     the parts into one of 3 A stages in shared memory;
 //   warp 8, lane 0: the B operand of each step (3-part X or t_b cores) by one bulk
 //     copy into one of 3 B stages;
 //   warp 9, lane 0: the MMAs of a step.  The parts of a B K core lie side by side
@@ -71,12 +70,16 @@ static constexpr int TCM_RAW = 128 * TCM_RROW;               // a raw stage (>= 
 static constexpr int TCM_AST = TCM_KC * TCM_PARTS * 16 * 128;       // A of a step: 128 rows, 24 KB
 static constexpr int TCM_BST = TCM_KC * TCM_PARTS * TCM_NMAX * 16;  // B of a step at 64 vectors, 12 KB
 static constexpr int TCM_TMEM_COLS = 512;                    // two buffers of 3 NV accumulator columns
-static constexpr int TCM_CONV = 5;                           // converter warps (11..15)
-static constexpr int TCM_EPI = 8;                            // epilogue warps (0..7)
+static constexpr int TCM_EPI = 8;                            // epilogue warps (4 or 8): 0 .. TCM_EPI - 1
+static constexpr int TCM_WB = TCM_EPI;                       // B producer warp
+static constexpr int TCM_WMMA = TCM_EPI + 1;                 // MMA warp
+static constexpr int TCM_WRAW = TCM_EPI + 2;                 // raw producer warp
+static constexpr int TCM_CONV = 5;                           // converter warps, from TCM_EPI + 3
 static constexpr int TCM_THREADS = (TCM_EPI + 3 + TCM_CONV) * 32;
 static constexpr int TCM_MAXMEM = 8;                         // blocks of a pass-1 stack (ranks rounded to 16)
 static constexpr int TCM_STGR = 40;                          // pass 1 epilogue staging: row stride (BF16)
 static_assert(2 * 3 * TCM_NMAX <= TCM_TMEM_COLS, "accumulators exceed the tensor memory allocation");
+static_assert(TCM_EPI == 4 || TCM_EPI == 8, "4 or 8 epilogue warps");
 
 // The K layout of a low-rank block's terms (t_b rows, U slice K positions, stack rows
 // of pass 1): its FP32, FP16 and FP8 terms each start a run of 8 K positions, so that
@@ -130,15 +133,17 @@ static_assert(sizeof(TcmStep) == 48, "TcmStep layout");
 // pass-1 job: the V^T of blocks with the same columns, one under the other.  A block's
 // V^T is a run of 16-byte-aligned rows of m2p words -- r32 FP32 term rows, r16 / 2 FP16
 // pair rows, r8 / 4 FP8 quad rows -- and raw row q of the stack is row q - qb[k] of
-// member k.  rtab[m] for stack row m: raw row (bits 0-7), tier (bits 8-9: 0 FP32, 1
-// FP16, 2 FP8, 3 none) and the term's place in its pair or quad (bits 10-11).
+// member k.  rtab lists the 128 stack rows sorted by storage tier, so that most 32-row
+// groups of it decode one tier: entry i = stack row m (bits 0-7), its raw row (bits
+// 8-15), tier (bits 16-17: 0 FP32, 1 FP16, 2 FP8, 3 none) and the term's place in its
+// pair or quad (bits 18-19).
 struct TcmStack {
     const char* vptr[TCM_MAXMEM];
     int qb[TCM_MAXMEM];
     int nmem, nq, m2p4, pad;
-    uint16_t rtab[128];
+    uint32_t rtab[128];
 };
-static_assert(sizeof(TcmStack) == 368, "TcmStack layout");
+static_assert(sizeof(TcmStack) == 624, "TcmStack layout");
 
 struct TcmJob {
     int r0;    // pass 2: first Z row of the tile; pass 1: first t_b term of the stack
@@ -153,7 +158,7 @@ struct TcmGeo {
 // written by the raw producer beside each raw stage
 struct TcmHdr {
     int kp0, meta, rows, cc0, t0, t1, t2, pad;
-    uint16_t rtab[128];
+    uint32_t rtab[128];
 };
 
 struct TcmSmem {
@@ -209,30 +214,28 @@ __device__ __forceinline__ void fp8_run(unsigned w0, unsigned w1, unsigned w2, i
     v[4] = c.x; v[5] = c.y; v[6] = d.x; v[7] = d.y;
 }
 
-// BF16 rounding of x (to nearest, ties away from zero) as the FP32 bit pattern with
-// the low 16 bits clear
-__device__ __forceinline__ uint32_t bf16_rn_bits(float x) { return (__float_as_uint(x) + 0x8000u) & 0xffff0000u; }
-
 // the parts of 8 values of one operand row, one uint4 (8 K positions) each: part 0 is
 // the BF16 rounding, each further part the rounding of what the parts before miss.
 // Every difference is exact in FP32, and what two parts miss has at most 8 significant
-// bits, so three parts hold an FP32 value exactly.  Integer adds, masks and byte
-// permutes only.
+// bits, so three parts hold an FP32 value exactly.
 __device__ __forceinline__ void store_parts(unsigned char* stage, int kc, int m, const float (&v)[8], int nparts)
 {
     uint32_t w0[4], w1[4], w2[4];
 #pragma unroll
     for (int k = 0; k < 4; k++) {
         const float a = v[2 * k], b = v[2 * k + 1];
-        const uint32_t ha = bf16_rn_bits(a), hb = bf16_rn_bits(b);
-        w0[k] = __byte_perm(ha, hb, 0x7632);
+        const __nv_bfloat162 h = __floats2bfloat162_rn(a, b);
+        w0[k] = *reinterpret_cast<const uint32_t*>(&h);
         if (nparts > 1) {
-            const float ra = a - __uint_as_float(ha), rb = b - __uint_as_float(hb);
-            const uint32_t ma = bf16_rn_bits(ra), mb = bf16_rn_bits(rb);
-            w1[k] = __byte_perm(ma, mb, 0x7632);
-            if (nparts > 2)
-                w2[k] = __byte_perm(__float_as_uint(ra - __uint_as_float(ma)), __float_as_uint(rb - __uint_as_float(mb)),
-                                    0x7632);
+            const float2 hf = __bfloat1622float2(h);
+            const float ra = a - hf.x, rb = b - hf.y;
+            const __nv_bfloat162 l = __floats2bfloat162_rn(ra, rb);
+            w1[k] = *reinterpret_cast<const uint32_t*>(&l);
+            if (nparts > 2) {
+                const float2 lf = __bfloat1622float2(l);
+                const __nv_bfloat162 l2 = __floats2bfloat162_rn(ra - lf.x, rb - lf.y);
+                w2[k] = *reinterpret_cast<const uint32_t*>(&l2);
+            }
         }
     }
     // row m of K core kc, part q: ((kc * 3 + q) * 16 + m / 8) * 128 + (m % 8) * 16
@@ -315,11 +318,11 @@ __device__ __forceinline__ void load_pass2(const TcmGeo H, const unsigned* rw, i
 // bank groups), decoded by the row's tier.
 __device__ __forceinline__ void load_pass1(const unsigned ent, const unsigned char* raw, int sh, int kc, float (&v)[8])
 {
-    const int tier = (ent >> 8) & 3, sel = (ent >> 10) & 3;
+    const int tier = (ent >> 16) & 3, sel = (ent >> 18) & 3;
 #pragma unroll
     for (int e = 0; e < 8; e++) v[e] = 0.0f;
     if (tier == 3) return;
-    const uint4* rr = reinterpret_cast<const uint4*>(raw + (ent & 255) * TCM_RROW) + 2 * kc;
+    const uint4* rr = reinterpret_cast<const uint4*>(raw + ((ent >> 8) & 255) * TCM_RROW) + 2 * kc;
     const uint4 c0 = rr[0], c1 = rr[1], c2 = rr[2];
     const unsigned words[12] = {c0.x, c0.y, c0.z, c0.w, c1.x, c1.y, c1.z, c1.w, c2.x, c2.y, c2.z, c2.w};
     unsigned w[8];
@@ -350,30 +353,6 @@ __device__ __forceinline__ void load_pass1(const unsigned ent, const unsigned ch
             const float2 f = e4m3x2_f2(__byte_perm(w[2 * i], w[2 * i + 1], s2));
             v[2 * i] = f.x;
             v[2 * i + 1] = f.y;
-        }
-    }
-}
-
-// A bounded wait whose polls sleep in the barrier (up to 100 us each, or until the
-// phase completes) instead of spinning: most warps of the pass kernel wait most of the
-// time, and spinning ones would take issue slots from the converters.  false (and *err
-// set) after ~2^31 cycles, as mbar_wait.
-__device__ __forceinline__ bool mbar_wait_s(uint64_t* bar, unsigned parity, int* err, int code)
-{
-    const long long t0 = clock64();
-    for (;;) {
-        unsigned ok;
-        asm volatile(
-            "{\n\t.reg .pred p;\n\t"
-            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
-            "selp.u32 %0, 1, 0, p;\n\t}"
-            : "=r"(ok)
-            : "r"(smem_u32(bar)), "r"(parity), "r"(100000u)
-            : "memory");
-        if (ok) return true;
-        if (clock64() - t0 > (1ll << 31)) {
-            atomicCAS(err, 0, code);
-            return false;
         }
     }
 }
@@ -421,7 +400,7 @@ __global__ void __launch_bounds__(TCM_THREADS, 1)
         sm.fail = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
-    if (warp == 9) {
+    if (warp == TCM_WMMA) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&sm.tmem)),
                      "n"(TCM_TMEM_COLS));
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
@@ -430,14 +409,13 @@ __global__ void __launch_bounds__(TCM_THREADS, 1)
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const uint32_t tmem = sm.tmem;
 
-    if (warp >= 11) {
-        // ---- converters: every step, items (32 rows, 1 K core) dealt over the warps,
-        // two at a time ----
-        const int cw = warp - 11;
+    if (warp >= TCM_WRAW + 1) {
+        // ---- converters: every step, items (32 rows, 1 K core) dealt over the warps ----
+        const int cw = warp - (TCM_WRAW + 1);
         for (int i = 0; i < nsteps; i++) {
             const int slot = i % TCM_NR, as = i % TCM_NA;
-            bool ok = !*fail && mbar_wait_s(&sm.raw_full[slot], (i / TCM_NR) & 1, err, 31);
-            if (ok && i >= TCM_NA) ok = mbar_wait_s(&sm.a_empty[as], ((i / TCM_NA) - 1) & 1, err, 32);
+            bool ok = !*fail && mbar_wait(&sm.raw_full[slot], (i / TCM_NR) & 1, err, 31);
+            if (ok && i >= TCM_NA) ok = mbar_wait(&sm.a_empty[as], ((i / TCM_NA) - 1) & 1, err, 32);
             if (!__all_sync(~0u, ok)) {
                 *fail = 1;
                 break;
@@ -453,36 +431,30 @@ __global__ void __launch_bounds__(TCM_THREADS, 1)
                 const int sp = (rows + 3) & ~3;
                 const unsigned* rw = reinterpret_cast<const unsigned*>(sm.raw[slot]);
 #pragma unroll 1
-                for (int it = cw; it < nitems; it += 2 * TCM_CONV) {
-                    const int it2 = it + TCM_CONV;
+                for (int it = cw; it < nitems; it += TCM_CONV) {
                     const int kc = it & (nkc - 1), m = (it >> lg) * 32 + lane;
-                    const int kc2 = it2 & (nkc - 1), m2 = (it2 >> lg) * 32 + lane;
-                    float v[8], v2[8];
+                    float v[8];
                     load_pass2(G, rw, sp, m, kp0 + 8 * kc, v);
-                    if (it2 < nitems) load_pass2(G, rw, sp, m2, kp0 + 8 * kc2, v2);
                     store_parts(stage, kc, m, v, nparts);
-                    if (it2 < nitems) store_parts(stage, kc2, m2, v2, nparts);
                 }
             } else {
                 const int sh = (kp0 - G.t0) & 3;
-                // the row-table entries of this warp's items, read before any item is stored
+                // the row-table entries of this warp's items (stack rows in tier order), read
+                // before any item is stored
                 unsigned ent[4];
 #pragma unroll
                 for (int j = 0; j < 4; j++) {
                     const int it = cw + j * TCM_CONV;
-                    ent[j] = it < nitems ? H.rtab[(it >> lg) * 32 + lane] : (3u << 8);
+                    ent[j] = it < nitems ? H.rtab[(it >> lg) * 32 + lane] : (3u << 16);
                 }
 #pragma unroll
-                for (int j = 0; j < 4; j += 2) {
-                    const int it = cw + j * TCM_CONV, it2 = it + TCM_CONV;
+                for (int j = 0; j < 4; j++) {
+                    const int it = cw + j * TCM_CONV;
                     if (it >= nitems) break;
-                    const int kc = it & (nkc - 1), m = (it >> lg) * 32 + lane;
-                    const int kc2 = it2 & (nkc - 1), m2 = (it2 >> lg) * 32 + lane;
-                    float v[8], v2[8];
+                    const int kc = it & (nkc - 1), m = ent[j] & 255;
+                    float v[8];
                     load_pass1(ent[j], sm.raw[slot], sh, kc, v);
-                    if (it2 < nitems) load_pass1(ent[j + 1], sm.raw[slot], sh, kc2, v2);
                     store_parts(stage, kc, m, v, 3);
-                    if (it2 < nitems) store_parts(stage, kc2, m2, v2, 3);
                 }
             }
             // the generic-proxy stores become visible to the tensor cores' (async) proxy
@@ -493,7 +465,7 @@ __global__ void __launch_bounds__(TCM_THREADS, 1)
                 mbar_arrive(&sm.raw_empty[slot]);
             }
         }
-    } else if (warp == 10) {
+    } else if (warp == TCM_WRAW) {
         // ---- raw producer: the stored bytes of every step, 16-byte cp.async per lane ----
         uint64_t pol;
         asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(pol));
@@ -533,7 +505,7 @@ __global__ void __launch_bounds__(TCM_THREADS, 1)
                 }
                 if (i >= TCM_NR) {
                     bool w = true;
-                    if (lane == 0) w = !*fail && mbar_wait_s(&sm.raw_empty[slot], ((i / TCM_NR) - 1) & 1, err, 33);
+                    if (lane == 0) w = !*fail && mbar_wait(&sm.raw_empty[slot], ((i / TCM_NR) - 1) & 1, err, 33);
                     if (!__shfl_sync(~0u, w, 0)) {
                         *fail = 1;
                         ok = false;
@@ -550,20 +522,34 @@ __global__ void __launch_bounds__(TCM_THREADS, 1)
                     const char* src = reinterpret_cast<const char*>(rawp);
                     for (int c = lane; c < n16; c += 32) cpa16(dst + 16 * c, src + 16 * c, 16, pol);
                 } else {
-                    if (lane < 16) cpa16(&H.rtab[8 * lane], &sk->rtab[8 * lane], 16, pol);
-                    // chunk c: V row c / 9, chunk c mod 9, walked without division (32 = 3 * 9 + 5)
+                    cpa16(&H.rtab[4 * lane], &sk->rtab[4 * lane], 16, pol);
+                    // chunk c: V row c / 9, chunk c mod 9, walked without division (32 = 3 * 9 + 5);
+                    // four chunks a round, their row pointers read before any copy is issued
                     const int nch = nq * 9;
                     int r = lane / 9, kk = lane - 9 * (lane / 9);
-                    for (int c = lane; c < nch; c += 32) {
-                        const int ch = cc0 + kk;
-                        const bool in = ch >= 0 && ch < m2p4;
-                        const char* rp = rowptr[r];
-                        cpa16(dst + r * TCM_RROW + 16 * kk, in ? rp + 16 * ch : rp, in ? 16u : 0u, pol);
-                        r += 3;
-                        kk += 5;
-                        if (kk >= 9) {
-                            kk -= 9;
-                            r += 1;
+                    for (int c = lane; c < nch; c += 128) {
+                        int rr[4], kq[4];
+#pragma unroll
+                        for (int u = 0; u < 4; u++) {
+                            rr[u] = r;
+                            kq[u] = kk;
+                            r += 3;
+                            kk += 5;
+                            if (kk >= 9) {
+                                kk -= 9;
+                                r += 1;
+                            }
+                        }
+                        const char* rp[4];
+#pragma unroll
+                        for (int u = 0; u < 4; u++) rp[u] = rowptr[min(rr[u], 127)];
+#pragma unroll
+                        for (int u = 0; u < 4; u++) {
+                            if (c + 32 * u < nch) {
+                                const int ch = cc0 + kq[u];
+                                const bool in = ch >= 0 && ch < m2p4;
+                                cpa16(dst + rr[u] * TCM_RROW + 16 * kq[u], in ? rp[u] + 16 * ch : rp[u], in ? 16u : 0u, pol);
+                            }
                         }
                     }
                 }
@@ -575,7 +561,7 @@ __global__ void __launch_bounds__(TCM_THREADS, 1)
         // every copy of this warp has landed before the CTA leaves
         asm volatile("cp.async.wait_all;" ::: "memory");
         __syncwarp();
-    } else if (warp == 8) {
+    } else if (warp == TCM_WB) {
         // ---- B operand of every step: one bulk copy, lane 0 ----
         int issued = 0;
         bool ok = true;
@@ -593,7 +579,7 @@ __global__ void __launch_bounds__(TCM_THREADS, 1)
                 const long long b_kc = __shfl_sync(~0u, bk, k);
                 bool w = true;
                 if (lane == 0) {
-                    if (i >= TCM_NB) w = !*fail && mbar_wait_s(&sm.b_empty[slot], ((i / TCM_NB) - 1) & 1, err, 34);
+                    if (i >= TCM_NB) w = !*fail && mbar_wait(&sm.b_empty[slot], ((i / TCM_NB) - 1) & 1, err, 34);
                     if (w) {
                         const unsigned bytes = (unsigned)(2 * (meta & 3)) * KB;
                         mbar_arrive_expect_tx(&sm.b_full[slot], bytes);
@@ -611,9 +597,9 @@ __global__ void __launch_bounds__(TCM_THREADS, 1)
         // the last copy into every stage has landed before the CTA leaves
         if (lane == 0)
             for (int s = 0; s < TCM_NB && s < issued; s++)
-                mbar_wait_s(&sm.b_full[(issued - 1 - s) % TCM_NB], ((issued - 1 - s) / TCM_NB) & 1, err, 35);
+                mbar_wait(&sm.b_full[(issued - 1 - s) % TCM_NB], ((issued - 1 - s) / TCM_NB) & 1, err, 35);
         __syncwarp();
-    } else if (warp == 9) {
+    } else if (warp == TCM_WMMA) {
         // ---- MMAs, lane 0: one per part of A, over the B parts side by side along N ----
         constexpr uint32_t LBA = P * 16 * 128, LBB = KB;  // K-core strides of A and B
         bool ok = true;
@@ -625,10 +611,10 @@ __global__ void __launch_bounds__(TCM_THREADS, 1)
                 const int meta = __shfl_sync(~0u, mt, k);
                 bool w = true;
                 if (lane == 0) {
-                    w = !*fail && mbar_wait_s(&sm.a_full[as], (i / TCM_NA) & 1, err, 36) &&
-                        mbar_wait_s(&sm.b_full[bs], (i / TCM_NB) & 1, err, 37);
+                    w = !*fail && mbar_wait(&sm.a_full[as], (i / TCM_NA) & 1, err, 36) &&
+                        mbar_wait(&sm.b_full[bs], (i / TCM_NB) & 1, err, 37);
                     // the epilogue has read this buffer's previous step
-                    if (w && i >= 2) w = mbar_wait_s(&sm.acce[buf], ((i >> 1) - 1) & 1, err, 38);
+                    if (w && i >= 2) w = mbar_wait(&sm.acce[buf], ((i >> 1) - 1) & 1, err, 38);
                     if (w) {
                         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
                         const int nk = meta & 3, mode = (meta >> 12) & 15;
@@ -665,13 +651,13 @@ __global__ void __launch_bounds__(TCM_THREADS, 1)
         }
         if (lane == 0) {
             tc_commit(&sm.fin);  // every MMA issued here has completed before tensor memory is freed
-            mbar_wait_s(&sm.fin, 0, err, 39);
+            mbar_wait(&sm.fin, 0, err, 39);
         }
         __syncwarp();
     } else {
         // ---- epilogue: warp w owns accumulator rows 32 (w mod 4) .. + 31 and vectors
-        // HV (w / 4) .. + HV - 1 ----
-        constexpr int HV = NV / 2;
+        // HV (w / 4) .. + HV - 1 (HV = NV with 4 epilogue warps, NV / 2 with 8) ----
+        constexpr int HV = NV * 4 / TCM_EPI;
         const int q4 = warp & 3, hv = warp >> 2;
         const int row = q4 * 32 + lane;
         float f[HV];
@@ -706,7 +692,7 @@ __global__ void __launch_bounds__(TCM_THREADS, 1)
                     cur_val = jc + 1 < njobs ? row_value(cur) : 0u;
                     nxt = jc + 2 < njobs ? my_jobs[jc + 2] : TcmJob{0, 0};
                 }
-                if (!__all_sync(~0u, !*fail && mbar_wait_s(&sm.accf[buf], (i >> 1) & 1, err, 40))) {
+                if (!__all_sync(~0u, !*fail && mbar_wait(&sm.accf[buf], (i >> 1) & 1, err, 40))) {
                     ok = false;
                     break;
                 }
@@ -776,7 +762,7 @@ __global__ void __launch_bounds__(TCM_THREADS, 1)
         if (!ok) *fail = 1;
     }
     __syncthreads();
-    if (warp == 9) {
+    if (warp == TCM_WMMA) {
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "n"(TCM_TMEM_COLS));
     }
@@ -994,7 +980,8 @@ hmg_status build_tcm(hmg_matrix* h)
                 TcmStack sk{};
                 sk.nmem = (int)members[k].size();
                 sk.m2p4 = m2p4;
-                for (int m = 0; m < 128; m++) sk.rtab[m] = 3u << 8;
+                uint32_t row_ent[128];  // per stack row: raw row | tier | place, as rtab without the row
+                for (int m = 0; m < 128; m++) row_ent[m] = 3u << 16;
                 const long long tg0 = tgroups;
                 int off = 0, q = 0;
                 for (int u = 0; u < sk.nmem; u++) {
@@ -1005,12 +992,12 @@ hmg_status build_tcm(hmg_matrix* h)
                     sk.qb[u] = q;
                     // stack rows in the K layout of TcmTerms: FP32 term rows, FP16 pair rows
                     // (two terms each), FP8 quad rows (four terms each), padding rows zero
-                    for (int t = 0; t < T.r32; t++) sk.rtab[off + t] = (uint16_t)(q + t);
+                    for (int t = 0; t < T.r32; t++) row_ent[off + t] = (uint32_t)(q + t) << 8;
                     for (int t = 0; t < T.r16; t++)
-                        sk.rtab[off + T.r32p + t] = (uint16_t)((q + T.r32 + t / 2) | 1 << 8 | (t & 1) << 10);
+                        row_ent[off + T.r32p + t] = (uint32_t)(q + T.r32 + t / 2) << 8 | 1u << 16 | (uint32_t)(t & 1) << 18;
                     for (int t = 0; t < T.r8; t++)
-                        sk.rtab[off + T.r32p + T.r16p + t] =
-                            (uint16_t)((q + T.r32 + T.r16 / 2 + t / 4) | 2 << 8 | (t & 3) << 10);
+                        row_ent[off + T.r32p + T.r16p + t] =
+                            (uint32_t)(q + T.r32 + T.r16 / 2 + t / 4) << 8 | 2u << 16 | (uint32_t)(t & 3) << 18;
                     toff[b] = tgroups;
                     far_blocks.push_back(b);
                     far_term.push_back(tgroups * 16);
@@ -1019,6 +1006,13 @@ hmg_status build_tcm(hmg_matrix* h)
                     q += T.r32 + T.r16 / 2 + T.r8 / 4;
                 }
                 sk.nq = q;
+                // rows in tier order (FP32, FP16, FP8, none), each carrying its row number
+                {
+                    int i = 0;
+                    for (uint32_t tier = 0; tier < 4; tier++)
+                        for (int m = 0; m < 128; m++)
+                            if (((row_ent[m] >> 16) & 3) == tier) sk.rtab[i++] = row_ent[m] | (uint32_t)m;
+                }
                 const int job = (int)stacks.size();
                 stacks.push_back(sk);
                 p1.begin(TcmJob{(int)(tg0 * 16), off});
