@@ -29,17 +29,16 @@
 //   warp 8, lane 0: the B operand of each step (3-part X or t_b cores) by one bulk
 //     copy into one of 3 B stages;
 //   warp 9, lane 0: the MMAs of a step.  The parts of a B K core lie side by side
-//     along N, so per K16 one MMA of N = 3 NV gives A0 B0 (hi), A0 B1 and A0 B2, one of
-//     N = 2 NV adds A1 B0 and A1 B1 to the last two, and one of N = NV adds A2 B0 to the
-//     first correction: every part of A is read once, into three accumulators (hi,
-//     c1 = A0 B1 + A1 B0 + A2 B0, c2 = A0 B2 + A1 B1).  A step that starts in the FP16
-//     terms (A exact in two parts) runs A0 [B0 B1] and A1 B0; one in the FP8 terms
-//     (exact in one part) A0 B0.  tcgen05.commit then frees the A and B stages and
-//     signals the accumulators;
+//     along N, so per K16 one MMA of N = 2 NV gives A0 B0 (hi) and A0 B1 (the first
+//     correction), and four of N = NV add A1 B0, A0 B2, A2 B0 and A1 B1 to the
+//     correction: two accumulators (hi, c).  A step that starts in the FP16 terms (A
+//     exact in two parts) runs A0 [B0 B1] and A1 B0; one in the FP8 terms (exact in one
+//     part) A0 B0.  tcgen05.commit then frees the A and B stages and signals the
+//     accumulators;
 //   warps 0-7: drain the accumulators after every step (tcgen05.ld; warp w reads
-//     lanes 32 (w mod 4) .. + 31, half w / 4 of the vectors) and keep the sums
-//     hi + (c1 + c2) in FP32 registers, so no tensor-core accumulation runs longer than
-//     one step.
+//     lanes 32 (w mod 4) .. + 31, half w / 4 of the vectors) and keep the sums hi + c
+//     in FP32 registers (packed FP32 adds), so no tensor-core accumulation runs longer
+//     than one step.
 // Every role reads its per-step records 32 at a time (one per lane) and the epilogue
 // prefetches the next job's rows, so no role waits on a global load per step.  Every
 // wait is bounded (pipeline.cuh); on a time-out the CTA records an error code in the
@@ -69,7 +68,7 @@ static constexpr int TCM_RROW = 144;                         // pass 1: bytes of
 static constexpr int TCM_RAW = 128 * TCM_RROW;               // a raw stage (>= 32 columns x 128 rows x 4)
 static constexpr int TCM_AST = TCM_KC * TCM_PARTS * 16 * 128;       // A of a step: 128 rows, 24 KB
 static constexpr int TCM_BST = TCM_KC * TCM_PARTS * TCM_NMAX * 16;  // B of a step at 64 vectors, 12 KB
-static constexpr int TCM_TMEM_COLS = 512;                    // two buffers of 3 NV accumulator columns
+static constexpr int TCM_TMEM_COLS = 256;                    // two buffers of 2 NV accumulator columns (hi, c)
 static constexpr int TCM_EPI = 8;                            // epilogue warps (4 or 8): 0 .. TCM_EPI - 1
 static constexpr int TCM_WB = TCM_EPI;                       // B producer warp
 static constexpr int TCM_WMMA = TCM_EPI + 1;                 // MMA warp
@@ -78,7 +77,7 @@ static constexpr int TCM_CONV = 5;                           // converter warps,
 static constexpr int TCM_THREADS = (TCM_EPI + 3 + TCM_CONV) * 32;
 static constexpr int TCM_MAXMEM = 8;                         // blocks of a pass-1 stack (ranks rounded to 16)
 static constexpr int TCM_STGR = 40;                          // pass 1 epilogue staging: row stride (BF16)
-static_assert(2 * 3 * TCM_NMAX <= TCM_TMEM_COLS, "accumulators exceed the tensor memory allocation");
+static_assert(2 * 2 * TCM_NMAX <= TCM_TMEM_COLS, "accumulators exceed the tensor memory allocation");
 static_assert(TCM_EPI == 4 || TCM_EPI == 8, "4 or 8 epilogue warps");
 
 // The K layout of a low-rank block's terms (t_b rows, U slice K positions, stack rows
@@ -357,6 +356,22 @@ __device__ __forceinline__ void load_pass1(const unsigned ent, const unsigned ch
     }
 }
 
+// (a0, a1) += (b0, b1), one packed FP32 add (each lane rounded as a scalar add)
+__device__ __forceinline__ void add_f32x2(uint32_t& a0, uint32_t& a1, uint32_t b0, uint32_t b1)
+{
+    asm("{\n\t.reg .b64 x, y;\n\tmov.b64 x, {%0, %1};\n\tmov.b64 y, {%2, %3};\n\t"
+        "add.rn.f32x2 x, x, y;\n\tmov.b64 {%0, %1}, x;\n\t}"
+        : "+r"(a0), "+r"(a1)
+        : "r"(b0), "r"(b1));
+}
+__device__ __forceinline__ void add_f32x2(float& a0, float& a1, uint32_t b0, uint32_t b1)
+{
+    asm("{\n\t.reg .b64 x, y;\n\tmov.b64 x, {%0, %1};\n\tmov.b64 y, {%2, %3};\n\t"
+        "add.rn.f32x2 x, x, y;\n\tmov.b64 {%0, %1}, x;\n\t}"
+        : "+f"(a0), "+f"(a1)
+        : "r"(b0), "r"(b1));
+}
+
 // ---------------------------------------------------------------------------
 // the pass kernel
 // ---------------------------------------------------------------------------
@@ -600,7 +615,7 @@ __global__ void __launch_bounds__(TCM_THREADS, 1)
                 mbar_wait(&sm.b_full[(issued - 1 - s) % TCM_NB], ((issued - 1 - s) / TCM_NB) & 1, err, 35);
         __syncwarp();
     } else if (warp == TCM_WMMA) {
-        // ---- MMAs, lane 0: one per part of A, over the B parts side by side along N ----
+        // ---- MMAs, lane 0: A0 over the B parts side by side along N, then the corrections ----
         constexpr uint32_t LBA = P * 16 * 128, LBB = KB;  // K-core strides of A and B
         bool ok = true;
         for (int i0 = 0; i0 < nsteps && ok; i0 += 32) {
@@ -618,16 +633,19 @@ __global__ void __launch_bounds__(TCM_THREADS, 1)
                     if (w) {
                         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
                         const int nk = meta & 3, mode = (meta >> 12) & 15;
-                        const uint32_t d = tmem + (uint32_t)(buf * 3 * NV);  // hi, c1, c2
+                        const uint32_t d = tmem + (uint32_t)(buf * 2 * NV);  // hi, c
                         uint64_t ad = smem_desc(smem_u32(sm.a[as]), LBA, 128), bd = smem_desc(smem_u32(sm.b[bs]), LBB, 128);
                         const uint64_t da = (2 * LBA) >> 4, db = (2 * LBB) >> 4;
                         const uint64_t alo = (16 * 128) >> 4;  // part q of A: + q alo
                         for (int kk = 0; kk < nk; kk++) {
                             const uint32_t acc = kk > 0 ? 1u : 0u;
                             if (mode >= 6) {
-                                tc_mma(d, ad, bd, tc_idesc<3 * NV>(), acc);
-                                tc_mma(d + NV, ad + alo, bd, tc_idesc<2 * NV>(), 1u);
+                                const uint64_t blo = (NV * 16) >> 4;
+                                tc_mma(d, ad, bd, tc_idesc<2 * NV>(), acc);
+                                tc_mma(d + NV, ad + alo, bd, tc_idesc<NV>(), 1u);
+                                tc_mma(d + NV, ad, bd + 2 * blo, tc_idesc<NV>(), 1u);
                                 tc_mma(d + NV, ad + 2 * alo, bd, tc_idesc<NV>(), 1u);
+                                tc_mma(d + NV, ad + alo, bd + blo, tc_idesc<NV>(), 1u);
                             } else if (mode >= 3) {
                                 tc_mma(d, ad, bd, tc_idesc<2 * NV>(), acc);
                                 tc_mma(d + NV, ad + alo, bd, tc_idesc<NV>(), 1u);
@@ -697,21 +715,28 @@ __global__ void __launch_bounds__(TCM_THREADS, 1)
                     break;
                 }
                 asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-                const uint32_t taddr = tmem + (uint32_t)(buf * 3 * NV + hv * HV) + ((uint32_t)(q4 * 32) << 16);
+                const uint32_t taddr = tmem + (uint32_t)(buf * 2 * NV + hv * HV) + ((uint32_t)(q4 * 32) << 16);
                 // 16 columns of each accumulator at a time: the running sums f[HV] stay in
                 // registers beside them
 #pragma unroll
                 for (int h = 0; h < HV / 16; h++) {
-                    uint32_t v[16], c1[16], c2[16];
+                    uint32_t v[16], c1[16];
                     tc_ld16(taddr + 16 * h, v);
                     if (mode > 1) tc_ld16(taddr + NV + 16 * h, c1);
-                    if (mode > 3) tc_ld16(taddr + 2 * NV + 16 * h, c2);
+
                     asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+                    // hi + c, then into the running sums: packed pairs, uniform branches
+
+                    if (mode > 1) {
 #pragma unroll
-                    for (int q = 0; q < 16; q++) {
-                        const float c = mode > 1 ? __uint_as_float(c1[q]) + (mode > 3 ? __uint_as_float(c2[q]) : 0.0f) : 0.0f;
-                        const float tv = __uint_as_float(v[q]) + c;
-                        f[16 * h + q] = first ? tv : f[16 * h + q] + tv;
+                        for (int q = 0; q < 16; q += 2) add_f32x2(v[q], v[q + 1], c1[q], c1[q + 1]);
+                    }
+                    if (first) {
+#pragma unroll
+                        for (int q = 0; q < 16; q++) f[16 * h + q] = __uint_as_float(v[q]);
+                    } else {
+#pragma unroll
+                        for (int q = 0; q < 16; q += 2) add_f32x2(f[16 * h + q], f[16 * h + q + 1], v[q], v[q + 1]);
                     }
                 }
                 asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
