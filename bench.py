@@ -358,6 +358,31 @@ def batched_tensor_cores(steps):
     return out
 
 
+def aca_work(H, seconds):
+    """Algorithmic work of the adaptive ACA (k_aca, k_aca_warp) per block-size class.
+    Rank step l of a block reads its l previous U and V columns twice (the residual
+    row / column, then the Frobenius cross terms): 2 l (m1 + m2) FP64 FMAs and as many
+    8-byte reads, so a block of rank r costs r (r - 1) (m1 + m2) of each; plus
+    (m1 + m2) kernel entries per step."""
+    s1l, s1u, s2l, s2u, typ = H.blocks()
+    ranks = H.ranks()
+    far = typ == 1
+    mm = ((s1u - s1l + 1) + (s2u - s2l + 1))[far].astype(np.float64)
+    r = ranks[far].astype(np.float64)
+    fma = r * (r - 1) * mm
+    classes = {}
+    for lo, hi in ((0, 512), (512, 2048), (2048, 8192), (8192, 32768), (32768, 1 << 30)):
+        sel = (mm >= lo) & (mm < hi)
+        classes[f"m1+m2 in [{lo},{hi})"] = {"blocks": int(sel.sum()), "mean_rank": float(r[sel].mean()) if sel.any() else 0.0,
+                                            "fp64_gflop": float(2 * fma[sel].sum() / 1e9),
+                                            "read_gb": float(8 * fma[sel].sum() / 1e9)}
+    total = float(fma.sum())
+    return {"fp64_gflop": 2 * total / 1e9, "read_gb": 8 * total / 1e9, "kernel_entries": float((r * mm).sum()),
+            "fp64_tflops_achieved": 2 * total / seconds / 1e12 if seconds > 0 else None,
+            "read_gbps_achieved": 8 * total / seconds / 1e9 if seconds > 0 else None,
+            "by_size": classes}
+
+
 def run_engine(a, rank, world):
     import torch
     import torch.distributed as dist
@@ -504,6 +529,7 @@ def run_engine(a, rank, world):
                          "frac": whole_bytes / (ms_step * 1e-3) / 1e9 / peak, "vtx_ms": k1_ms,
                          "tiles_ms": k2_ms},
         "build_s": {"setup": t_setup, "aca": t_aca, "dense": t_dense},
+        "aca_work": aca_work(H, t_aca),
         "hmatrix": {k: info[k] for k in ("block_count", "dense_count", "aca_count", "levels", "tile_count",
                                          "max_rank", "near_entries", "far_entries", "near_bytes", "far_bytes")},
         "clocks": clk.summary(),

@@ -94,17 +94,17 @@ __device__ __forceinline__ void block_argmax(double& a, int& i, bool last, doubl
         if (better(reda[w], redi[w], a, i, last)) { a = reda[w]; i = redi[w]; }
 }
 
-__global__ void __launch_bounds__(ACA_THREADS)
-k_aca(BlockGeom g, KernelSpec K0, PointsView P, AcaBatch B, int k, double eps)
+// four CTAs an SM: the rank steps are latency-bound, so occupancy sets their pace
+__global__ void __launch_bounds__(ACA_THREADS, 4)
+k_aca(BlockGeom g, KernelSpec K0, PointsView P, AcaBatch B, int k, double eps, const int* elist)
 {
     __shared__ double coef[ACA_KMAX];
     __shared__ double red[ACA_WARPS];
     __shared__ double reda[ACA_WARPS];
     __shared__ int redi[ACA_WARPS];
-    __shared__ double dots[2][32];
     extern __shared__ unsigned used[];  // adaptive mode: one bit per row
 
-    const int e = blockIdx.x;
+    const int e = elist ? elist[blockIdx.x] : blockIdx.x;
     const int b = B.blocks[e];
     KernelSpec K = K0;
     if (g.param) K.param = g.param[b];
@@ -227,52 +227,38 @@ k_aca(BlockGeom g, KernelSpec K0, PointsView P, AcaBatch B, int k, double eps)
             double nv2 = block_sum(pv, red);
             double nu2 = block_sum(pu, red);
             block_argmax(bu, bi, false, reda, redi);
-            // cross terms sum_l (u_r . U_l)(v_r . V_l), 32 columns at a time
-            double cross = 0.0;
-            for (int l0 = 0; l0 < r; l0 += 32) {
-                int nc = r - l0 < 32 ? r - l0 : 32;
-                double au[32], av[32];
-#pragma unroll
-                for (int c = 0; c < 32; c++) { au[c] = 0.0; av[c] = 0.0; }
-                for (int i = tid; i < m1; i += ACA_THREADS) {
-                    double u = U[i + (size_t)r * m1];
-#pragma unroll
-                    for (int c = 0; c < 32; c++)
-                        if (c < nc) au[c] = __fma_rn(u, U[i + (size_t)(l0 + c) * m1], au[c]);
-                }
-                for (int j = tid; j < m2; j += ACA_THREADS) {
-                    double v = V[j + (size_t)r * m2];
-#pragma unroll
-                    for (int c = 0; c < 32; c++)
-                        if (c < nc) av[c] = __fma_rn(v, V[j + (size_t)(l0 + c) * m2], av[c]);
-                }
-                __syncthreads();
-#pragma unroll
-                for (int c = 0; c < 32; c++) {
-                    double x = au[c], y = av[c];
+            // cross terms sum_l (u_r . U_l)(v_r . V_l): warp w takes columns l = w mod 8 whole
+            // (coalesced dot products, a fixed-order warp reduction), warp 0 sums the
+            // products over l in order.  Few registers per thread, so several CTAs share an SM.
+            {
+                const int warp = tid >> 5, lane = tid & 31;
+                const double* ur = U + (size_t)r * m1;
+                const double* vr = V + (size_t)r * m2;
+                for (int l = warp; l < r; l += ACA_WARPS) {
+                    const double* ul = U + (size_t)l * m1;
+                    const double* vl = V + (size_t)l * m2;
+                    double a = 0.0, c = 0.0;
+                    for (int i = lane; i < m1; i += 32) a = __fma_rn(ur[i], ul[i], a);
+                    for (int j = lane; j < m2; j += 32) c = __fma_rn(vr[j], vl[j], c);
 #pragma unroll
                     for (int o = 16; o > 0; o >>= 1) {
-                        x += __shfl_xor_sync(0xffffffffu, x, o);
-                        y += __shfl_xor_sync(0xffffffffu, y, o);
+                        a += __shfl_xor_sync(0xffffffffu, a, o);
+                        c += __shfl_xor_sync(0xffffffffu, c, o);
                     }
-                    au[c] = x;
-                    av[c] = y;
+                    if (lane == 0) coef[l] = a * c;
                 }
-                // lane c of each warp holds column c; accumulate warps in order
-                double mu = 0.0, mv = 0.0;
+                __syncthreads();
+                if (warp == 0) {
+                    double p = 0.0;
+                    for (int l = lane; l < r; l += 32) p += coef[l];
 #pragma unroll
-                for (int c = 0; c < 32; c++)
-                    if ((tid & 31) == c) { mu = au[c]; mv = av[c]; }
-                for (int w = 0; w < ACA_WARPS; w++) {
-                    if ((tid >> 5) == w && (tid & 31) < nc) {
-                        if (w == 0) { dots[0][tid & 31] = mu; dots[1][tid & 31] = mv; }
-                        else { dots[0][tid & 31] += mu; dots[1][tid & 31] += mv; }
-                    }
-                    __syncthreads();
+                    for (int o = 16; o > 0; o >>= 1) p += __shfl_xor_sync(0xffffffffu, p, o);
+                    if (lane == 0) red[0] = p;
                 }
-                for (int c = 0; c < nc; c++) cross += dots[0][c] * dots[1][c];
                 __syncthreads();
             }
+            const double cross = red[0];
+            __syncthreads();
             S2 = S2 + 2.0 * cross + nu2 * nv2;
             rank = r + 1;
             if (sqrt(nu2 * nv2) <= eps * sqrt(fabs(S2))) break;
@@ -283,6 +269,144 @@ k_aca(BlockGeom g, KernelSpec K0, PointsView P, AcaBatch B, int k, double eps)
         }
     }
     if (tid == 0) {
+        B.rank_out[e] = rank;
+        if (B.s2_out) B.s2_out[e] = S2;
+    }
+}
+
+
+// ---------------------------------------------------------------------------
+// The adaptive ACA of a small block (m1, m2 <= ACA_WSMALL) by one warp: the steps of
+// k_aca's adaptive mode with warp shuffles in place of CTA reductions and no CTA
+// barriers.  Most admissible blocks are small (at N = 2^20, 925k of 1.16M have
+// m1 + m2 < 512); a CTA of 256 threads per block would leave most lanes idle and
+// synchronise six times a rank step.
+// ---------------------------------------------------------------------------
+static constexpr int ACA_WSMALL = 512;              // largest m1 and m2 of the warp variant
+static constexpr int ACA_WPC = 8;                   // warps (blocks) per CTA
+
+__device__ __forceinline__ double warp_sum(double v)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// (value, index) argmax over the warp; ties go to the smaller index
+__device__ __forceinline__ void warp_argmax_first(double& a, int& i)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        const double b = __shfl_xor_sync(0xffffffffu, a, o);
+        const int j = __shfl_xor_sync(0xffffffffu, i, o);
+        if (better(b, j, a, i, false)) { a = b; i = j; }
+    }
+}
+
+__global__ void __launch_bounds__(ACA_WPC * 32, 4)
+k_aca_warp(BlockGeom g, KernelSpec K0, PointsView P, AcaBatch B, int k, double eps, const int* elist, int nlist)
+{
+    __shared__ double coefs[ACA_WPC][ACA_WSMALL];
+    __shared__ unsigned usedw[ACA_WPC][ACA_WSMALL / 32];
+    const int wi = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int slot = blockIdx.x * ACA_WPC + wi;
+    if (slot >= nlist) return;
+    const int e = elist[slot];
+    const int b = B.blocks[e];
+    KernelSpec K = K0;
+    if (g.param) K.param = g.param[b];
+    const int r0 = g.r0[b], m1 = g.m1[b], c0 = g.c0[b], m2 = g.m2[b];
+    int kb = k < m1 ? k : m1;
+    kb = kb < m2 ? kb : m2;
+    double* U = B.U + B.uoff[e];
+    double* V = B.V + B.voff[e];
+    double* coef = coefs[wi];
+    unsigned* used = usedw[wi];
+    for (int w = lane; w < ACA_WSMALL / 32; w += 32) used[w] = 0u;
+    __syncwarp();
+    int rank = 0, ir = 0, nused = 0;
+    double S2 = 0.0;
+    for (int r = 0; r < kb; r++) {
+        int jr = -1;
+        bool have = false;
+        for (;;) {
+            if (lane == 0) used[ir >> 5] |= 1u << (ir & 31);
+            nused++;
+            for (int l = lane; l < r; l += 32) coef[l] = U[ir + (size_t)l * m1];
+            __syncwarp();
+            double best = -1.0;
+            int bj = 0x7fffffff;
+            for (int j = lane; j < m2; j += 32) {
+                double val = kernel_entry(K, P, r0 + ir, c0 + j);
+                for (int l = 0; l < r; l++) val = __fma_rn(-coef[l], V[j + (size_t)l * m2], val);
+                V[j + (size_t)r * m2] = val;
+                const double a = fabs(val);
+                if (better(a, j, best, bj, false)) { best = a; bj = j; }
+            }
+            warp_argmax_first(best, bj);
+            if (best > 0.0) {
+                jr = bj;
+                have = true;
+                break;
+            }
+            // zero residual row: the next unused row in index order
+            int cand = 0x7fffffff;
+            for (int i = lane; i < m1; i += 32)
+                if (!((used[i >> 5] >> (i & 31)) & 1u)) { cand = i; break; }
+            double dummy = 0.0;
+            warp_argmax_first(dummy, cand);
+            if (cand == 0x7fffffff) break;
+            ir = cand;
+            __syncwarp();
+        }
+        if (!have) break;
+        __syncwarp();  // every lane's V[., r] written
+        const double piv = V[jr + (size_t)r * m2];
+        double pv = 0.0;
+        for (int j = lane; j < m2; j += 32) {
+            const double v = V[j + (size_t)r * m2] / piv;
+            V[j + (size_t)r * m2] = v;
+            pv += v * v;
+        }
+        __syncwarp();
+        for (int l = lane; l < r; l += 32) coef[l] = V[jr + (size_t)l * m2];
+        __syncwarp();
+        double pu = 0.0, bu = -1.0;
+        int bi = 0x7fffffff;
+        for (int i = lane; i < m1; i += 32) {
+            double val = kernel_entry(K, P, r0 + i, c0 + jr);
+            for (int l = 0; l < r; l++) val = __fma_rn(-coef[l], U[i + (size_t)l * m1], val);
+            U[i + (size_t)r * m1] = val;
+            pu += val * val;
+            if (!((used[i >> 5] >> (i & 31)) & 1u)) {
+                const double a = fabs(val);
+                if (better(a, i, bu, bi, false)) { bu = a; bi = i; }
+            }
+        }
+        const double nv2 = warp_sum(pv), nu2 = warp_sum(pu);
+        warp_argmax_first(bu, bi);
+        __syncwarp();  // every lane's U[., r] written
+        // cross terms sum_l (u_r . U_l)(v_r . V_l), in l order
+        double cross = 0.0;
+        const double* ur = U + (size_t)r * m1;
+        const double* vr = V + (size_t)r * m2;
+        for (int l = 0; l < r; l++) {
+            const double* ul = U + (size_t)l * m1;
+            const double* vl = V + (size_t)l * m2;
+            double a = 0.0, c = 0.0;
+            for (int i = lane; i < m1; i += 32) a = __fma_rn(ur[i], ul[i], a);
+            for (int j = lane; j < m2; j += 32) c = __fma_rn(vr[j], vl[j], c);
+            cross += warp_sum(a) * warp_sum(c);
+        }
+        S2 = S2 + 2.0 * cross + nu2 * nv2;
+        rank = r + 1;
+        if (sqrt(nu2 * nv2) <= eps * sqrt(fabs(S2))) break;
+        if (nused >= m1) break;
+        if (bi == 0x7fffffff) break;
+        ir = bi;
+        __syncwarp();
+    }
+    if (lane == 0) {
         B.rank_out[e] = rank;
         if (B.s2_out) B.s2_out[e] = S2;
     }
@@ -545,7 +669,7 @@ hmg_status run_aca(hmg_matrix* h, int k, double eps, int precision)
     size_t free_b = 0, total_b = 0;
     HMG_CUDA_TRY(cudaMemGetInfo(&free_b, &total_b));
     size_t budget = free_b / 4;
-    if (budget > ((size_t)8 << 30)) budget = (size_t)8 << 30;
+    if (budget > ((size_t)16 << 30)) budget = (size_t)16 << 30;
     if (budget < ((size_t)64 << 20)) budget = (size_t)64 << 20;
 
     BlockGeom g{h->blk_r0, h->blk_m1, h->blk_c0, h->blk_m2, h->blk_param};
@@ -557,6 +681,21 @@ hmg_status run_aca(hmg_matrix* h, int k, double eps, int precision)
     P.n1 = h->n[0];
     P.n2 = h->n[1];
 
+    // Scratch of the batches, grown to the largest batch and reused across batches: the
+    // stream-ordered pool hands freed memory back at every synchronisation, so
+    // allocating it per batch would map gigabytes afresh for each one.
+    int* d_idx = nullptr;
+    long long *d_uo = nullptr, *d_vo = nullptr, *d_so = nullptr;
+    double *dU = nullptr, *dV = nullptr, *d_s2 = nullptr;
+    int *d_rank = nullptr, *d_r32 = nullptr, *d_r16 = nullptr, *d_list = nullptr;
+    float *d_su = nullptr, *d_sv = nullptr;
+    size_t cap_ne = 0, cap_u = 0, cap_v = 0, cap_sc = 0;
+    auto free_batch = [&]() {
+        dfree(d_idx, s); dfree(d_uo, s); dfree(d_vo, s); dfree(dU, s); dfree(dV, s);
+        dfree(d_rank, s); dfree(d_s2, s); dfree(d_so, s); dfree(d_r32, s); dfree(d_r16, s);
+        dfree(d_su, s); dfree(d_sv, s); dfree(d_list, s);
+        cap_ne = cap_u = cap_v = cap_sc = 0;
+    };
     int bstart = h->ndense;
     while (bstart < nb) {
         std::vector<int> idx;
@@ -578,29 +717,48 @@ hmg_status run_aca(hmg_matrix* h, int k, double eps, int precision)
         }
         bstart = b;
         int ne = (int)idx.size();
-        int* d_idx = nullptr;
-        long long *d_uo = nullptr, *d_vo = nullptr, *d_so = nullptr;
-        double *dU = nullptr, *dV = nullptr, *d_s2 = nullptr;
-        int *d_rank = nullptr, *d_r32 = nullptr, *d_r16 = nullptr;
-        float *d_su = nullptr, *d_sv = nullptr;
         std::vector<long long> so(ne);
         long long nscale = 0;
         for (int e = 0; e < ne; e++) {
             so[e] = nscale;
             nscale += std::min(k, std::min(h->h_m1[idx[e]], h->h_m2[idx[e]]));
         }
-        auto free_batch = [&]() {
-            dfree(d_idx, s); dfree(d_uo, s); dfree(d_vo, s); dfree(dU, s); dfree(dV, s);
-            dfree(d_rank, s); dfree(d_s2, s); dfree(d_so, s); dfree(d_r32, s); dfree(d_r16, s);
-            dfree(d_su, s); dfree(d_sv, s);
-        };
-        if ((st = dalloc(&d_idx, ne, s)) || (st = dalloc(&d_uo, ne, s)) || (st = dalloc(&d_vo, ne, s)) ||
-            (st = dalloc(&dU, (size_t)us, s)) || (st = dalloc(&dV, (size_t)vs, s)) ||
-            (st = dalloc(&d_rank, ne, s)) || (st = dalloc(&d_s2, ne, s)) ||
-            (mixed && ((st = dalloc(&d_so, ne, s)) || (st = dalloc(&d_r32, ne, s)) || (st = dalloc(&d_r16, ne, s)) ||
-                       (st = dalloc(&d_su, (size_t)nscale, s)) || (st = dalloc(&d_sv, (size_t)nscale, s))))) {
-            free_batch();
-            return st;
+        if ((size_t)ne > cap_ne) {
+            dfree(d_idx, s); dfree(d_uo, s); dfree(d_vo, s); dfree(d_rank, s); dfree(d_s2, s);
+            dfree(d_so, s); dfree(d_r32, s); dfree(d_r16, s); dfree(d_list, s);
+            cap_ne = (size_t)ne;
+            if ((st = dalloc(&d_idx, cap_ne, s)) || (st = dalloc(&d_uo, cap_ne, s)) || (st = dalloc(&d_vo, cap_ne, s)) ||
+                (st = dalloc(&d_rank, cap_ne, s)) || (st = dalloc(&d_s2, cap_ne, s)) || (st = dalloc(&d_list, cap_ne, s)) ||
+                (mixed && ((st = dalloc(&d_so, cap_ne, s)) || (st = dalloc(&d_r32, cap_ne, s)) ||
+                           (st = dalloc(&d_r16, cap_ne, s))))) {
+                free_batch();
+                return st;
+            }
+        }
+        if ((size_t)us > cap_u) {
+            dfree(dU, s);
+            cap_u = (size_t)us;
+            if ((st = dalloc(&dU, cap_u, s))) {
+                free_batch();
+                return st;
+            }
+        }
+        if ((size_t)vs > cap_v) {
+            dfree(dV, s);
+            cap_v = (size_t)vs;
+            if ((st = dalloc(&dV, cap_v, s))) {
+                free_batch();
+                return st;
+            }
+        }
+        if (mixed && (size_t)nscale > cap_sc) {
+            dfree(d_su, s);
+            dfree(d_sv, s);
+            cap_sc = (size_t)nscale;
+            if ((st = dalloc(&d_su, cap_sc, s)) || (st = dalloc(&d_sv, cap_sc, s))) {
+                free_batch();
+                return st;
+            }
         }
         HMG_CUDA_TRY(cudaMemcpyAsync(d_idx, idx.data(), sizeof(int) * ne, cudaMemcpyHostToDevice, s));
         HMG_CUDA_TRY(cudaMemcpyAsync(d_uo, uo.data(), sizeof(long long) * ne, cudaMemcpyHostToDevice, s));
@@ -611,13 +769,38 @@ hmg_status run_aca(hmg_matrix* h, int k, double eps, int precision)
         size_t dyn = eps > 0.0 ? (size_t)((maxm1 + 31) / 32) * 4 : 0;
         if (dyn > 200 * 1024) {
             set_error("block with %d rows exceeds the adaptive ACA's row-mask capacity", maxm1);
+            free_batch();
             return HMG_ERR_UNSUPPORTED;
         }
         if (dyn > 48 * 1024)
             HMG_CUDA_TRY(cudaFuncSetAttribute(k_aca, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                               (int)dyn));
-        k_aca<<<ne, ACA_THREADS, dyn, s>>>(g, h->kspec, P, B, k, eps);
-        HMG_LAUNCH_CHECK();
+        if (eps > 0.0) {
+            // adaptive mode: small blocks one warp each, the others one CTA each
+            std::vector<int> small, large;
+            for (int e = 0; e < ne; e++) {
+                const int bb = idx[e];
+                ((h->h_m1[bb] <= ACA_WSMALL && h->h_m2[bb] <= ACA_WSMALL) ? small : large).push_back(e);
+            }
+            if (!small.empty())
+                HMG_CUDA_TRY(cudaMemcpyAsync(d_list, small.data(), sizeof(int) * small.size(), cudaMemcpyHostToDevice, s));
+            if (!large.empty())
+                HMG_CUDA_TRY(cudaMemcpyAsync(d_list + small.size(), large.data(), sizeof(int) * large.size(),
+                                             cudaMemcpyHostToDevice, s));
+            if (!small.empty()) {
+                const int ns = (int)small.size();
+                k_aca_warp<<<ceil_div(ns, ACA_WPC), ACA_WPC * 32, 0, s>>>(g, h->kspec, P, B, k, eps, d_list, ns);
+                HMG_LAUNCH_CHECK();
+            }
+            if (!large.empty()) {
+                k_aca<<<(unsigned)large.size(), ACA_THREADS, dyn, s>>>(g, h->kspec, P, B, k, eps, d_list + small.size());
+                HMG_LAUNCH_CHECK();
+            }
+            HMG_CUDA_TRY(cudaStreamSynchronize(s));  // the host vectors go out of scope
+        } else {
+            k_aca<<<ne, ACA_THREADS, dyn, s>>>(g, h->kspec, P, B, k, eps, nullptr);
+            HMG_LAUNCH_CHECK();
+        }
         if (mixed) {
             k_aca_tiers<<<ne, 256, 0, s>>>(g, B, T);
             HMG_LAUNCH_CHECK();
@@ -696,8 +879,8 @@ hmg_status run_aca(hmg_matrix* h, int k, double eps, int precision)
             HMG_LAUNCH_CHECK();
         }
         HMG_CUDA_TRY(cudaStreamSynchronize(s));
-        free_batch();
     }
+    free_batch();
 
     // ranks and their offsets
     std::vector<long long> roff(nb + 1, 0);
