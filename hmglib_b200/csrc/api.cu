@@ -450,6 +450,13 @@ hmg_status hmg_destroy(hmg_matrix* h)
     cudaStreamSynchronize(h->stream);
     for (int i = 0; i < 4; i++)
         if (h->ev[i]) cudaEventDestroy(h->ev[i]);
+    for (int i = 0; i < 2; i++)
+        if (h->k1_aux[i]) {
+            cudaStreamSynchronize(h->k1_aux[i]);
+            cudaStreamDestroy(h->k1_aux[i]);
+        }
+    for (int i = 0; i < 3; i++)
+        if (h->k1_ev[i]) cudaEventDestroy(h->k1_ev[i]);
     free_matrix_buffers(h);
     cudaStreamSynchronize(h->stream);
     delete h;

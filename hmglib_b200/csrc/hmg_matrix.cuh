@@ -143,6 +143,8 @@ struct hmg_matrix {
     int k1_grid = 0, k2_grid = 0;
     bool profiling = false;
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+    cudaStream_t k1_aux[2] = {nullptr, nullptr};  // side streams of the FP16 / FP8 V^T x tiers (matvec.cu)
+    cudaEvent_t k1_ev[3] = {nullptr, nullptr, nullptr};  // their fork and joins
 };
 
 namespace hmg {

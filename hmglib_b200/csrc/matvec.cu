@@ -849,7 +849,21 @@ static hmg_status launch_product(hmg_matrix* h, const double* x, double* y, bool
         const K1Desc* dd = static_cast<const K1Desc*>(h->k1_units);
         double* t64 = static_cast<double*>(h->tbuf);
         float* t32 = static_cast<float*>(h->tbuf);
+        // The tiers write disjoint t_b entries: the FP16 and FP8 tiers run on two side
+        // streams beside the FP32 one (forked from and joined back into the handle's
+        // stream), so the FP8 tier's conversion-bound warps share the SMs with the FP32
+        // tier's load-bound ones and the three launches' tails overlap.
+        const bool fork = h->k1_task_start[1][4] > 0 || h->k1_task_start[2][4] > 0;
+        if (fork) {
+            for (int i = 0; i < 2; i++)
+                if (!h->k1_aux[i]) HMG_CUDA_TRY(cudaStreamCreateWithFlags(&h->k1_aux[i], cudaStreamNonBlocking));
+            for (int i = 0; i < 3; i++)
+                if (!h->k1_ev[i]) HMG_CUDA_TRY(cudaEventCreateWithFlags(&h->k1_ev[i], cudaEventDisableTiming));
+            HMG_CUDA_TRY(cudaEventRecord(h->k1_ev[0], s));
+            for (int i = 0; i < 2; i++) HMG_CUDA_TRY(cudaStreamWaitEvent(h->k1_aux[i], h->k1_ev[0], 0));
+        }
         for (int tier = 0; tier < 3; tier++) {
+            const cudaStream_t ts = (fork && tier > 0) ? h->k1_aux[tier - 1] : s;
             K1Classes cls;
             for (int c = 0; c < 5; c++) {
                 cls.piece_start[c] = h->k1_piece_start[tier][c];
@@ -860,24 +874,29 @@ static hmg_status launch_product(hmg_matrix* h, const double* x, double* y, bool
             const int grid = std::min(ceil_div(ntasks, 8), h->nsm * h->k1_ctas_per_sm);
             if (tier == 0) {
                 if (fp64)
-                    k_vtx<double, double, 0><<<grid, 256, 0, s>>>(dd, cls, h->xs64, t64);
+                    k_vtx<double, double, 0><<<grid, 256, 0, ts>>>(dd, cls, h->xs64, t64);
                 else if (arith64)
-                    k_vtx<float, double, 0><<<grid, 256, 0, s>>>(dd, cls, h->xs64, t64);
+                    k_vtx<float, double, 0><<<grid, 256, 0, ts>>>(dd, cls, h->xs64, t64);
                 else
-                    k_vtx<float, float, 0><<<grid, 256, 0, s>>>(dd, cls, h->xs32, t32);
+                    k_vtx<float, float, 0><<<grid, 256, 0, ts>>>(dd, cls, h->xs32, t32);
             } else if (tier == 1) {
                 if (arith64)
-                    k_vtx<float, double, 1><<<grid, 256, 0, s>>>(dd, cls, h->xs64, t64);
+                    k_vtx<float, double, 1><<<grid, 256, 0, ts>>>(dd, cls, h->xs64, t64);
                 else
-                    k_vtx<float, float, 1><<<grid, 256, 0, s>>>(dd, cls, h->xs32, t32);
+                    k_vtx<float, float, 1><<<grid, 256, 0, ts>>>(dd, cls, h->xs32, t32);
             } else {
                 if (arith64)
-                    k_vtx<float, double, 2><<<grid, 256, 0, s>>>(dd, cls, h->xs64, t64);
+                    k_vtx<float, double, 2><<<grid, 256, 0, ts>>>(dd, cls, h->xs64, t64);
                 else
-                    k_vtx<float, float, 2><<<grid, 256, 0, s>>>(dd, cls, h->xs32, t32);
+                    k_vtx<float, float, 2><<<grid, 256, 0, ts>>>(dd, cls, h->xs32, t32);
             }
             HMG_LAUNCH_CHECK();
         }
+        if (fork)
+            for (int i = 0; i < 2; i++) {
+                HMG_CUDA_TRY(cudaEventRecord(h->k1_ev[1 + i], h->k1_aux[i]));
+                HMG_CUDA_TRY(cudaStreamWaitEvent(s, h->k1_ev[1 + i], 0));
+            }
     }
     if (h->profiling) HMG_CUDA_TRY(cudaEventRecord(h->ev[2], s));
     if (h->ntiles > 0 && bulk_k2) {
