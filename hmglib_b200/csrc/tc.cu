@@ -370,17 +370,20 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                 uint32_t acc = (SPLIT || first) ? 0u : 1u;
 #pragma unroll 4
                 for (int q = 0; q < ks_all; q++) {
-                    tc_mma(d, ad, bd, tc_idesc<NV>(), acc);
                     if (SPLIT) {
-                        // the correction terms in their own accumulator: added to hi*hi they
-                        // would each be truncated at the scale of the (256x larger) sum
-                        tc_mma(d + NV, ad, bd + blo, tc_idesc<NV>(), acc);
+                        // the correction terms in their own accumulator (added to hi*hi they
+                        // would each be truncated at the scale of the 256x larger sum).  The
+                        // parts of a B K core lie side by side along N, so one MMA of N = 2 NV
+                        // gives hi = A0 B0 and the correction's A0 B1.
+                        tc_mma(d, ad, bd, tc_idesc<2 * NV>(), acc);
                         tc_mma(d + NV, ad + alo, bd, tc_idesc<NV>(), 1u);
-                    }
-                    if (PARTS == 3) {
-                        tc_mma(d + NV, ad, bd + 2 * blo, tc_idesc<NV>(), 1u);
-                        tc_mma(d + NV, ad + 2 * alo, bd, tc_idesc<NV>(), 1u);
-                        tc_mma(d + NV, ad + alo, bd + blo, tc_idesc<NV>(), 1u);
+                        if (PARTS == 3) {
+                            tc_mma(d + NV, ad, bd + 2 * blo, tc_idesc<NV>(), 1u);
+                            tc_mma(d + NV, ad + 2 * alo, bd, tc_idesc<NV>(), 1u);
+                            tc_mma(d + NV, ad + alo, bd + blo, tc_idesc<NV>(), 1u);
+                        }
+                    } else {
+                        tc_mma(d, ad, bd, tc_idesc<NV>(), acc);
                     }
                     acc = 1u;
                     ad += da;
@@ -463,10 +466,17 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                 tc_ld32(taddr + 32 * h, v);
                 if (SPLIT) tc_ld32(taddr + NV + 32 * h, c);
                 asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+                // hi + c, then into the running sums: packed pairs, uniform branches
+                if (SPLIT) {
 #pragma unroll
-                for (int q = 0; q < 32; q++) {
-                    const float t = SPLIT ? __uint_as_float(v[q]) + __uint_as_float(c[q]) : __uint_as_float(v[q]);
-                    f[32 * h + q] = fresh ? t : f[32 * h + q] + t;
+                    for (int q = 0; q < 32; q += 2) add_f32x2(v[q], v[q + 1], c[q], c[q + 1]);
+                }
+                if (fresh) {
+#pragma unroll
+                    for (int q = 0; q < 32; q++) f[32 * h + q] = __uint_as_float(v[q]);
+                } else {
+#pragma unroll
+                    for (int q = 0; q < 32; q += 2) add_f32x2(f[32 * h + q], f[32 * h + q + 1], v[q], v[q + 1]);
                 }
             }
             asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");

@@ -356,22 +356,6 @@ __device__ __forceinline__ void load_pass1(const unsigned ent, const unsigned ch
     }
 }
 
-// (a0, a1) += (b0, b1), one packed FP32 add (each lane rounded as a scalar add)
-__device__ __forceinline__ void add_f32x2(uint32_t& a0, uint32_t& a1, uint32_t b0, uint32_t b1)
-{
-    asm("{\n\t.reg .b64 x, y;\n\tmov.b64 x, {%0, %1};\n\tmov.b64 y, {%2, %3};\n\t"
-        "add.rn.f32x2 x, x, y;\n\tmov.b64 {%0, %1}, x;\n\t}"
-        : "+r"(a0), "+r"(a1)
-        : "r"(b0), "r"(b1));
-}
-__device__ __forceinline__ void add_f32x2(float& a0, float& a1, uint32_t b0, uint32_t b1)
-{
-    asm("{\n\t.reg .b64 x, y;\n\tmov.b64 x, {%0, %1};\n\tmov.b64 y, {%2, %3};\n\t"
-        "add.rn.f32x2 x, x, y;\n\tmov.b64 {%0, %1}, x;\n\t}"
-        : "+f"(a0), "+f"(a1)
-        : "r"(b0), "r"(b1));
-}
-
 // ---------------------------------------------------------------------------
 // the pass kernel
 // ---------------------------------------------------------------------------
