@@ -73,7 +73,7 @@ static constexpr int TCM_EPI = 8;                            // epilogue warps (
 static constexpr int TCM_WB = TCM_EPI;                       // B producer warp
 static constexpr int TCM_WMMA = TCM_EPI + 1;                 // MMA warp
 static constexpr int TCM_WRAW = TCM_EPI + 2;                 // raw producer warp
-static constexpr int TCM_CONV = 5;                           // converter warps, from TCM_EPI + 3
+static constexpr int TCM_CONV = 8;                           // converter warps, from TCM_EPI + 3
 static constexpr int TCM_THREADS = (TCM_EPI + 3 + TCM_CONV) * 32;
 static constexpr int TCM_MAXMEM = 8;                         // blocks of a pass-1 stack (ranks rounded to 16)
 static constexpr int TCM_STGR = 40;                          // pass 1 epilogue staging: row stride (BF16)
