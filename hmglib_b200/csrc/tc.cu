@@ -401,7 +401,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
         // ---- epilogue: warp w owns accumulator rows 32w..32w+31 ----
         const int row = warp * 32 + lane;
         // a finished job's sums f (row `row`, vectors 0..NV-1) to their destination
-        auto emit = [&](const float (&f)[NV], int rows, int yrow, const int (&tdst)[4]) {
+        auto emit = [&](float (&f)[NV], int rows, int yrow, const int (&tdst)[4]) {
             if (MODE == 1) {
                 if (row < rows) {
                     double* y = Y + yrow;
@@ -420,18 +420,20 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                 const bool odd = lane & 1;
 #pragma unroll
                 for (int part = 0; part < PARTS; part++) {
-                    // part 0: BF16 of t; part p: BF16 of what parts 0..p-1 miss
+                    // part 0: BF16 of t; part p: BF16 of what parts 0..p-1 miss.  Each lane
+                    // rounds its own pair once (one packed conversion), keeps the residual
+                    // in f for the next part, and swaps halves with its neighbour: the even
+                    // lane keeps the low halves (vector 2t), the odd lane the high ones.
 #pragma unroll
                     for (int t = 0; t < NV / 2; t++) {
-                        float v0 = f[2 * t], v1 = f[2 * t + 1];
-#pragma unroll
-                        for (int pp = 0; pp < part; pp++) {
-                            v0 -= __bfloat162float(__float2bfloat16_rn(v0));
-                            v1 -= __bfloat162float(__float2bfloat16_rn(v1));
+                        const uint32_t own = pack_bf16(f[2 * t], f[2 * t + 1]);
+                        if (part + 1 < PARTS) {
+                            f[2 * t] -= __uint_as_float(own << 16);
+                            f[2 * t + 1] -= __uint_as_float(own & 0xffff0000u);
                         }
-                        const float x = __shfl_xor_sync(~0u, odd ? v0 : v1, 1);
+                        const uint32_t other = __shfl_xor_sync(~0u, own, 1);
                         const int q = odd ? 2 * t + 1 : 2 * t;
-                        const uint32_t w = odd ? pack_bf16(x, v1) : pack_bf16(v0, x);
+                        const uint32_t w = odd ? __byte_perm(own, other, 0x3276) : __byte_perm(own, other, 0x5410);
                         const int u = (lane >> 3) * NV + q;
                         stg[(u ^ ((lane >> 3) * 2)) * 4 + ((lane & 7) >> 1)] = w;
                     }

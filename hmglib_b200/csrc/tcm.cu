@@ -660,6 +660,7 @@ __global__ void __launch_bounds__(TCM_THREADS, 1)
         // ---- epilogue: warp w owns accumulator rows 32 (w mod 4) .. + 31 and vectors
         // HV (w / 4) .. + HV - 1 (HV = NV with 4 epilogue warps, NV / 2 with 8) ----
         constexpr int HV = NV * 4 / TCM_EPI;
+        static_assert(HV % 2 == 0, "pairs of vectors per epilogue thread");
         const int q4 = warp & 3, hv = warp >> 2;
         const int row = q4 * 32 + lane;
         float f[HV];
@@ -745,14 +746,20 @@ __global__ void __launch_bounds__(TCM_THREADS, 1)
 #pragma unroll
                     for (int q = 0; q < HV; q++) f[q] *= scale;
                     // part p: the BF16 rounding of what parts 0..p-1 miss, f keeping the rest
+                    // (one packed rounding per pair of vectors, reused for the residual)
+                    unsigned short* stg16 = reinterpret_cast<unsigned short*>(stg);
 #pragma unroll 1
                     for (int part = 0; part < P; part++) {
-                        if (part > 0) {
 #pragma unroll
-                            for (int q = 0; q < HV; q++) f[q] -= __bfloat162float(__float2bfloat16_rn(f[q]));
+                        for (int q = 0; q < HV; q += 2) {
+                            const uint32_t h = pack_bf16(f[q], f[q + 1]);
+                            if (part + 1 < P) {
+                                f[q] -= __uint_as_float(h << 16);
+                                f[q + 1] -= __uint_as_float(h & 0xffff0000u);
+                            }
+                            stg16[(hv * HV + q) * TCM_STGR + lane] = (unsigned short)(h & 0xffffu);
+                            stg16[(hv * HV + q + 1) * TCM_STGR + lane] = (unsigned short)(h >> 16);
                         }
-#pragma unroll
-                        for (int q = 0; q < HV; q++) stg[(hv * HV + q) * TCM_STGR + lane] = __float2bfloat16_rn(f[q]);
                         __syncwarp();
                         uint4* dst = reinterpret_cast<uint4*>(Bbuf);
 #pragma unroll 1
