@@ -12,7 +12,8 @@ over 4,096 rows is reported beside every number (err_vs_fp64).
 
   value  H-matvecs/s with x and y resident in HBM (device-timed with CUDA events);
   e2e    the same through the host-buffer C-ABI call hmg_matvec_host: x copied
-         in from pinned memory and y copied out, every step, inside the timing.
+         in from the caller's pageable host memory and y copied out to it, every
+         step, inside the timing.
   multi_rhs  products of 32 vectors a pass on the same H-matrix (hmg_matvec_multi,
          CUDA cores), vectors per second.
   batched_tensor_cores  64 vectors a pass on the tensor cores with three-part BF16

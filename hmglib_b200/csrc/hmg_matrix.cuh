@@ -136,8 +136,6 @@ struct hmg_matrix {
     void* capture_stream = nullptr;  // cudaStream_t the graph is captured on
     int arith_prec = HMG_PREC_FP32;  // products over FP32 / mixed storage: FP32 or FP64 arithmetic
     int last_variant_k1 = -1, last_variant_k2 = -1;
-    double* host_x = nullptr; // pinned staging
-    double* host_y = nullptr;
     double* dev_x = nullptr;
     double* dev_y = nullptr;
     int k1_grid = 0, k2_grid = 0;

@@ -144,7 +144,9 @@ hmg_status hmg_matvec(hmg_matrix* h, const double* x, double* y);
 hmg_status hmg_matvec_unbatched(hmg_matrix* h, const double* x, double* y);
 
 /* Same product with host vectors: copies x in, multiplies, copies y out, returns
- * when y is written.  The copies use a pinned staging buffer of the handle. */
+ * when y is written.  x and y may be pageable or pinned memory; they are copied
+ * directly between the caller's memory and the device (the driver stages pageable
+ * memory itself). */
 hmg_status hmg_matvec_host(hmg_matrix* h, const double* x_host, double* y_host);
 
 /* y = K x in FP64 by direct summation on the GPU (no N^2 storage).  Replaces
