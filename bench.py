@@ -742,7 +742,9 @@ def run_group(a, rank, world):
     """Many independent H-matrices (512 sets, sizes log-uniform in [2^10, 2^16], half 2D
     and half 3D, Gaussian length^2 U[0.01, 0.2], FP32 factors, ACA eps 1e-5): one
     grouped H-matrix multiplied in one set of launches, against the same sets
-    compressed and multiplied one handle at a time.  One step = every set once."""
+    compressed and multiplied one handle at a time.  One step = every set once.
+    Clustering is timed both ways: hmg_setup per set then hmg_group_create, and
+    hmg_group_setup (every set ordered and clustered in the same launches)."""
     import torch
 
     import hmglib_b200 as hmg
@@ -751,20 +753,39 @@ def run_group(a, rank, world):
     torch.cuda.set_device(local)
     count = a.group_count
     sets = synth.group_sets(count, 3)
+    leaf = [64 if p.shape[0] == 2 else 128 for p, _ in sets]
+
+    def handles():
+        out = []
+        for p, l2 in sets:
+            dim, n = p.shape
+            H = hmg.HMatrix(n, n, dim)
+            H.set_points(0, p)
+            H.set_points(1, p)
+            H.set_kernel(hmg.KERNEL_GAUSSIAN, l2, 0.0)
+            out.append(H)
+        return out
     t0 = time.perf_counter()
-    hs = []
-    for p, l2 in sets:
-        dim, n = p.shape
-        H = hmg.HMatrix(n, n, dim)
-        H.set_points(0, p)
-        H.set_points(1, p)
-        H.setup(1.5, 64 if dim == 2 else 128, rule=hmg.ADMISSIBLE_MIN)
-        H.set_kernel(hmg.KERNEL_GAUSSIAN, l2, 0.0)
-        hs.append(H)
+    hs = handles()
+    t_handles = time.perf_counter() - t0
+    # clustering one set at a time (hmg_setup per set, then hmg_group_create) ...
+    t0 = time.perf_counter()
+    for H, c in zip(hs, leaf):
+        H.setup(1.5, c, rule=hmg.ADMISSIBLE_MIN)
     t_setup = time.perf_counter() - t0
     t0 = time.perf_counter()
     G = hmg.group(hs)
     t_group = time.perf_counter() - t0
+    # ... and every set in the same launches (hmg_group_setup): the same handle
+    raw = handles()
+    t0 = time.perf_counter()
+    G1 = hmg.group_setup(raw, 1.5, leaf, rule=hmg.ADMISSIBLE_MIN)
+    t_group_setup = time.perf_counter() - t0
+    same_tree = all(bool(np.array_equal(u, v)) for u, v in zip(G.blocks(), G1.blocks())) and \
+        all(bool(np.array_equal(G.order(w), G1.order(w))) for w in (0, 1))
+    G1.close()
+    for H in raw:
+        H.close()
     off = G.offsets(0)
     n = int(off[-1])
     x = synth.rhs_vector(n, 3)
@@ -853,7 +874,9 @@ def run_group(a, rank, world):
         "roofline": {"bound": "hbm", "kernel": "whole product", "achieved": bytes_ / (ms * 1e-3) / 1e9,
                      "peak": peak, "unit": "GB/s", "frac": bytes_ / (ms * 1e-3) / 1e9 / peak, "traffic": None,
                      "peak_kind": peak_kind, "bytes_per_launch": bytes_},
-        "build_s": {"setup_sets": t_setup, "group_create": t_group, "aca_dense_group": t_build_group},
+        "build_s": {"handles": t_handles, "setup_sets": t_setup, "group_create": t_group,
+                    "group_setup": t_group_setup, "group_setup_equals_setup_sets": same_tree,
+                    "aca_dense_group": t_build_group},
         "hmatrix": {k: info[k] for k in ("block_count", "dense_count", "aca_count", "tile_count", "max_rank",
                                          "near_bytes", "far_bytes")},
         "clocks": clk.summary(),

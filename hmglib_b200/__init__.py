@@ -9,4 +9,4 @@ from ._lib import (ADMISSIBLE_MAX, ADMISSIBLE_MIN, KERNEL_GAUSSIAN, KERNEL_GAUSS
                    KERNEL_MATERN32, KERNEL_MATERN_REF, NEAR_ONTHEFLY, NEAR_STORED, PREC_FP32,
                    PREC_BF16, PREC_BF16X3, PREC_BF16X6, PREC_BF16X6_ONCHIP, PREC_FP64, PREC_MIXED,
                    HmgError, lib)
-from .hmatrix import CgMulti, HMatrix, group, load, morton_codes, radix_sort_u64  # noqa: F401
+from .hmatrix import CgMulti, HMatrix, group, group_setup, load, morton_codes, radix_sort_u64  # noqa: F401

@@ -71,6 +71,8 @@ _PROTOS = {
     "hmg_matvec_unbatched": (C.c_int, [_vp, _vp, _vp]),
     "hmg_matvec_multi": (C.c_int, [_vp, C.c_int, _vp, C.c_int, _vp, C.c_int]),
     "hmg_group_create": (C.c_int, [C.POINTER(_vp), C.POINTER(_vp), C.c_int, _vp]),
+    "hmg_group_setup": (C.c_int, [C.POINTER(_vp), C.POINTER(_vp), C.c_int, C.c_double, C.POINTER(C.c_int),
+                                  C.c_int, C.c_int, _vp]),
     "hmg_group_offsets": (C.c_int, [_vp, C.c_int, _vp]),
     "hmg_save": (C.c_int, [_vp, C.c_char_p]),
     "hmg_build_bf16_factors": (C.c_int, [_vp]),

@@ -276,6 +276,19 @@ hmg_status hmg_group_create(hmg_matrix** out, hmg_matrix* const* sets, int count
     return group_create(out, sets, count, (cudaStream_t)stream);
 }
 
+hmg_status hmg_group_setup(hmg_matrix** out, hmg_matrix* const* sets, int count, double eta, const int* c_leaf,
+                           int max_level, int rule, void* stream)
+{
+    HMG_REQUIRE(out && sets && c_leaf, HMG_ERR_INVALID, "hmg_group_setup: NULL argument");
+    *out = nullptr;
+    HMG_REQUIRE(count >= 1, HMG_ERR_INVALID, "hmg_group_setup: count must be >= 1 (got %d)", count);
+    HMG_REQUIRE(eta >= 0.0 && std::isfinite(eta), HMG_ERR_INVALID, "hmg_group_setup: eta must be finite and >= 0");
+    HMG_REQUIRE(max_level >= 1, HMG_ERR_INVALID, "hmg_group_setup: max_level must be >= 1");
+    HMG_REQUIRE(rule == HMG_ADMISSIBLE_MAX || rule == HMG_ADMISSIBLE_MIN, HMG_ERR_INVALID,
+                "hmg_group_setup: unknown admissibility rule %d", rule);
+    return group_setup(out, sets, count, eta, c_leaf, max_level, rule, (cudaStream_t)stream);
+}
+
 hmg_status hmg_group_offsets(hmg_matrix* h, int set, int64_t* offsets)
 {
     HMG_REQUIRE(h && offsets, HMG_ERR_INVALID, "hmg_group_offsets: NULL argument");

@@ -146,4 +146,102 @@ hmg_status group_create(hmg_matrix** out, hmg_matrix* const* sets, int count, cu
     return HMG_OK;
 }
 
+// The sets' points and kernels, clustered together (hmg_group_setup): the union of
+// their points is ordered and its block-cluster tree built in the same launches for
+// every set (one Morton pass, one stable sort pair, one level loop from one root pair
+// per set), instead of one hmg_setup per set followed by hmg_group_create.  The result
+// is the handle hmg_group_create makes from the sets after hmg_setup with these
+// parameters: the same permutation, blocks, block order and kernel parameters.
+hmg_status group_setup(hmg_matrix** out, hmg_matrix* const* sets, int count, double eta, const int* c_leaf,
+                       int max_level, int rule, cudaStream_t s)
+{
+    hmg_status st;
+    int n1 = 0, n2 = 0, dim = 2;
+    const hmg_matrix* s0 = sets[0];
+    std::vector<int> sdim(count), sbits(count), sleaf(count);
+    for (int i = 0; i < count; i++) {
+        const hmg_matrix* h = sets[i];
+        if (!h || !h->points_set[0] || !h->points_set[1] || !h->kernel_set) {
+            set_error("hmg_group_setup: set %d needs its points (both sides) and a kernel", i);
+            return HMG_ERR_STATE;
+        }
+        if (h->group_count) {
+            set_error("hmg_group_setup: set %d is itself a group", i);
+            return HMG_ERR_INVALID;
+        }
+        if (h->dim != 2 && h->dim != 3) {
+            set_error("hmg_group_setup: set %d has dimension %d (2 or 3 are grouped)", i, h->dim);
+            return HMG_ERR_UNSUPPORTED;
+        }
+        if (h->kspec.kind != s0->kspec.kind || h->kspec.reg != s0->kspec.reg ||
+            (h->kspec.kind == HMG_KERNEL_MATERN_REF && h->kspec.matern_ref_denom != s0->kspec.matern_ref_denom)) {
+            set_error("hmg_group_setup: set %d has another kernel kind or regularization than set 0", i);
+            return HMG_ERR_INVALID;
+        }
+        if (c_leaf[i] < 1) {
+            set_error("hmg_group_setup: c_leaf[%d] must be >= 1 (got %d)", i, c_leaf[i]);
+            return HMG_ERR_INVALID;
+        }
+        if ((long long)n1 + h->n[0] > 0x7fffffff || (long long)n2 + h->n[1] > 0x7fffffff) {
+            set_error("hmg_group_setup: more than 2^31 - 1 points in the group");
+            return HMG_ERR_INVALID;
+        }
+        n1 += h->n[0];
+        n2 += h->n[1];
+        dim = std::max(dim, h->dim);
+        sdim[i] = h->dim;
+        // (dim, bits) pairs with Morton codes (morton.cu:65); others get code 0
+        const bool coded = (h->dim == 2 && h->bits == 32) || (h->dim == 3 && h->bits == 20);
+        sbits[i] = coded ? h->bits : 0;
+        sleaf[i] = c_leaf[i];
+    }
+    hmg_matrix* g = nullptr;
+    if ((st = hmg_create(&g, n1, n2, dim, dim == 2 ? 32 : 20, (void*)s))) return st;
+    g->group_count = count;
+    for (int w = 0; w < 2; w++) {
+        g->group_off[w].assign(1, 0);
+        for (int i = 0; i < count; i++) {
+            const hmg_matrix* h = sets[i];
+            const int off = g->group_off[w].back(), n = h->n[w];
+            k_copy_points<<<ceil_div(n, 256), 256, 0, s>>>(h->pts[w], n, h->dim, g->pts[w], g->n[w], off, dim);
+            HMG_LAUNCH_CHECK();
+            g->group_off[w].push_back(off + n);
+        }
+    }
+    g->points_set[0] = g->points_set[1] = true;
+    g->eta = eta;
+    g->c_leaf = *std::max_element(sleaf.begin(), sleaf.end());
+    g->max_level = max_level;
+    g->rule = rule;
+    const int* offp[2] = {g->group_off[0].data(), g->group_off[1].data()};
+    if ((st = group_setup_tree(g, count, offp, sdim.data(), sbits.data(), sleaf.data()))) {
+        hmg_destroy(g);
+        return st;
+    }
+    // each block's kernel parameter: that of the set holding its rows
+    const int nb = g->nblocks;
+    std::vector<double> param(nb);
+    for (int q = 0; q < nb; q++) {
+        const int set = (int)(std::upper_bound(g->group_off[0].begin(), g->group_off[0].end(), g->h_r0[q]) -
+                              g->group_off[0].begin()) - 1;
+        param[q] = sets[set]->kspec.param;
+    }
+    if ((st = dalloc(&g->blk_param, (size_t)(nb > 0 ? nb : 1), s))) {
+        hmg_destroy(g);
+        return st;
+    }
+    if (nb > 0) HMG_CUDA_TRY(cudaMemcpyAsync(g->blk_param, param.data(), sizeof(double) * nb, cudaMemcpyHostToDevice, s));
+    if ((st = build_tiles(g))) {
+        hmg_destroy(g);
+        return st;
+    }
+    g->kspec = s0->kspec;
+    g->kspec.dim = dim;
+    g->kernel_set = true;
+    g->setup_done = true;
+    HMG_CUDA_TRY(cudaStreamSynchronize(s));
+    *out = g;
+    return HMG_OK;
+}
+
 }  // namespace hmg

@@ -147,8 +147,12 @@ struct hmg_matrix {
 
 namespace hmg {
 hmg_status setup_tree(hmg_matrix* h);
+hmg_status group_setup_tree(hmg_matrix* g, int nsets, const int* const* off, const int* sdim,
+                            const int* sbits, const int* sleaf);
 hmg_status build_tiles(hmg_matrix* h);
 hmg_status group_create(hmg_matrix** out, hmg_matrix* const* sets, int count, cudaStream_t s);
+hmg_status group_setup(hmg_matrix** out, hmg_matrix* const* sets, int count, double eta, const int* c_leaf,
+                       int max_level, int rule, cudaStream_t s);
 hmg_status save(hmg_matrix* h, const char* path);
 hmg_status load(hmg_matrix** out, const char* path, cudaStream_t s);
 hmg_status run_aca(hmg_matrix* h, int k, double eps, int precision);

@@ -14,6 +14,9 @@
 //     are emitted at offsets from one packed (leaf, child) exclusive scan.
 //   * organize_mat_vec_data (linear_algebra.cu:4037-4051): stable DENSE-first
 //     partition by one scan.
+#include <algorithm>
+#include <vector>
+
 #include "hmg_matrix.cuh"
 
 namespace hmg {
@@ -185,9 +188,10 @@ __device__ int split_index(const uint64_t* codes, int first, int last)
 }
 
 // One CTA per cluster [l,u]: exact bounding box into the per-level maps (indexed by
-// l), and the split point for clusters that may be subdivided.
+// l), and the split point for clusters that may be subdivided.  leaf_at (grouped
+// point sets, else null) gives the leaf size of the set that holds each point.
 __global__ void k_cluster_bbox(const int* cl_l, const int* cl_u, int ncl, const double* z,
-                               int n, int dim, const uint64_t* codes, int c_leaf,
+                               int n, int dim, const uint64_t* codes, int c_leaf, const int* leaf_at,
                                double* bb_lo, double* bb_hi, int* split_of)
 {
     __shared__ double red[2][3][8];
@@ -225,7 +229,7 @@ __global__ void k_cluster_bbox(const int* cl_l, const int* cl_u, int ncl, const 
             bb_lo[(size_t)d * n + l] = lo;
             bb_hi[(size_t)d * n + l] = hi;
         }
-        if (u - l + 1 > c_leaf) split_of[l] = split_index(codes, l, u);
+        if (u - l + 1 > (leaf_at ? leaf_at[l] : c_leaf)) split_of[l] = split_index(codes, l, u);
     }
 }
 
@@ -258,12 +262,14 @@ struct NodeArrays {
 __global__ void k_node_classify(NodeArrays nd, int nn, int n1, int n2, int dim,
                                 const double* bb1_lo, const double* bb1_hi,
                                 const double* bb2_lo, const double* bb2_hi, double eta,
-                                int rule, int c_leaf, int last_level, long long* packed,
+                                int rule, int c_leaf, const int* leaf_at, int last_level, long long* packed,
                                 signed char* leaf_type)
 {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= nn) return;
     int l1 = nd.l1[i], u1 = nd.u1[i], l2 = nd.l2[i], u2 = nd.u2[i];
+    // both clusters of a node belong to one set: its leaf size
+    if (leaf_at) c_leaf = leaf_at[l1];
     double lo1[3], hi1[3], lo2[3], hi2[3];
     for (int d = 0; d < dim; d++) {
         lo1[d] = bb1_lo[(size_t)d * n1 + l1];
@@ -320,20 +326,20 @@ __global__ void k_node_emit(NodeArrays nd, int nn, const long long* offs,
 
 // clusters of the next level: both children of every cluster larger than c_leaf
 __global__ void k_cluster_count(const int* cl_l, const int* cl_u, int ncl, int c_leaf,
-                                int* cnt)
+                                const int* leaf_at, int* cnt)
 {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= ncl) return;
-    cnt[i] = (cl_u[i] - cl_l[i] + 1 > c_leaf) ? 2 : 0;
+    cnt[i] = (cl_u[i] - cl_l[i] + 1 > (leaf_at ? leaf_at[cl_l[i]] : c_leaf)) ? 2 : 0;
 }
 
 __global__ void k_cluster_emit(const int* cl_l, const int* cl_u, int ncl, const int* off,
-                               int c_leaf, const int* split_of, int* nl, int* nu)
+                               int c_leaf, const int* leaf_at, const int* split_of, int* nl, int* nu)
 {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= ncl) return;
     int l = cl_l[i], u = cl_u[i];
-    if (u - l + 1 <= c_leaf) return;
+    if (u - l + 1 <= (leaf_at ? leaf_at[l] : c_leaf)) return;
     int s = split_of[l];
     int o = off[i];
     nl[o] = l; nu[o] = s;
@@ -426,65 +432,47 @@ static void free_cluster_set(ClusterSet& c, cudaStream_t s)
     dfree(c.split_of, s);
 }
 
-hmg_status setup_tree(hmg_matrix* h)
+// Level-synchronous traversal (tree.cu:1429-1557) from nroots root pairs: root i pairs
+// the row cluster [rl1[i], ru1[i]] with the column cluster [rl2[i], ru2[i]], and each
+// side's cluster list starts from its roots' ranges.  Leaves are appended in the order
+// the levels emit them; leaf_at[side] (grouped point sets, else null) gives the leaf
+// size of the set that holds each point.
+static hmg_status traverse(hmg_matrix* h, int nroots, const int* rl1, const int* ru1, const int* rl2,
+                           const int* ru2, const int* const* leaf_at, LeafArrays& leaves, int& nleaves,
+                           int& levels)
 {
     cudaStream_t s = h->stream;
     hmg_status st = HMG_OK;
     const int dim = h->dim;
-
-    // ---- Morton codes, sort, gather (hmglib.cu:128-162) ------------------------
-    for (int set = 0; set < 2; set++) {
-        int n = h->n[set];
-        uint32_t* order = nullptr;
-        if ((st = morton_codes(h->pts[set], n, dim, h->bits, h->codes[set], s))) return st;
-        if ((st = dalloc(&order, (size_t)n, s))) return st;
-        k_iota<<<ceil_div(n, 256), 256, 0, s>>>(order, n);
-        HMG_LAUNCH_CHECK();
-        int key_bits = dim * h->bits;
-        if (key_bits > 64) key_bits = 64;
-        if ((st = radix_sort_pairs(h->codes[set], order, n, key_bits, s))) {
-            dfree(order, s);
-            return st;
-        }
-        k_gather_points<<<ceil_div(n, 256), 256, 0, s>>>(h->pts[set], h->zpts[set], order, n,
-                                                         dim, h->perm[set], h->iperm[set]);
-        HMG_LAUNCH_CHECK();
-        dfree(order, s);
-    }
-
-    // ---- level-synchronous traversal (tree.cu:1429-1557) -----------------------
     ClusterSet cs[2];
     NodeArrays cur{}, nxt{};
-    LeafArrays leaves{};
-    int leaf_cap = 0, nleaves = 0;
+    int leaf_cap = 0;
     long long* packed = nullptr;
     signed char* ltype = nullptr;
     int* ccnt = nullptr;
     long long* ptot = nullptr;
-    int nn = 1;
-    int levels = 0;
+    int nn = nroots;
+    nleaves = 0;
+    levels = 0;
+    leaves = LeafArrays{};
 
     for (int set = 0; set < 2; set++) {
         ClusterSet& c = cs[set];
         c.n = h->n[set];
-        c.ncl = 1;
-        if ((st = dalloc(&c.cl_l, 1, s)) || (st = dalloc(&c.cl_u, 1, s)) ||
+        c.ncl = nroots;
+        if ((st = dalloc(&c.cl_l, (size_t)nroots, s)) || (st = dalloc(&c.cl_u, (size_t)nroots, s)) ||
             (st = dalloc(&c.bb_lo, (size_t)dim * c.n, s)) ||
             (st = dalloc(&c.bb_hi, (size_t)dim * c.n, s)) ||
             (st = dalloc(&c.split_of, (size_t)c.n, s)))
             goto done;
-        int root[2] = {0, c.n - 1};
-        HMG_CUDA_TRY(cudaMemcpyAsync(c.cl_l, &root[0], sizeof(int), cudaMemcpyHostToDevice, s));
-        HMG_CUDA_TRY(cudaMemcpyAsync(c.cl_u, &root[1], sizeof(int), cudaMemcpyHostToDevice, s));
+        HMG_CUDA_TRY(cudaMemcpyAsync(c.cl_l, set ? rl2 : rl1, sizeof(int) * nroots, cudaMemcpyHostToDevice, s));
+        HMG_CUDA_TRY(cudaMemcpyAsync(c.cl_u, set ? ru2 : ru1, sizeof(int) * nroots, cudaMemcpyHostToDevice, s));
     }
-    if ((st = alloc_nodes(cur, 1, s))) goto done;
-    {
-        int root[4] = {0, h->n[0] - 1, 0, h->n[1] - 1};
-        HMG_CUDA_TRY(cudaMemcpyAsync(cur.l1, &root[0], sizeof(int), cudaMemcpyHostToDevice, s));
-        HMG_CUDA_TRY(cudaMemcpyAsync(cur.u1, &root[1], sizeof(int), cudaMemcpyHostToDevice, s));
-        HMG_CUDA_TRY(cudaMemcpyAsync(cur.l2, &root[2], sizeof(int), cudaMemcpyHostToDevice, s));
-        HMG_CUDA_TRY(cudaMemcpyAsync(cur.u2, &root[3], sizeof(int), cudaMemcpyHostToDevice, s));
-    }
+    if ((st = alloc_nodes(cur, (size_t)nroots, s))) goto done;
+    HMG_CUDA_TRY(cudaMemcpyAsync(cur.l1, rl1, sizeof(int) * nroots, cudaMemcpyHostToDevice, s));
+    HMG_CUDA_TRY(cudaMemcpyAsync(cur.u1, ru1, sizeof(int) * nroots, cudaMemcpyHostToDevice, s));
+    HMG_CUDA_TRY(cudaMemcpyAsync(cur.l2, rl2, sizeof(int) * nroots, cudaMemcpyHostToDevice, s));
+    HMG_CUDA_TRY(cudaMemcpyAsync(cur.u2, ru2, sizeof(int) * nroots, cudaMemcpyHostToDevice, s));
     if ((st = dalloc(&ptot, 3, s))) goto done;
 
     for (int it = 0; it < h->max_level && nn > 0; it++) {
@@ -495,8 +483,8 @@ hmg_status setup_tree(hmg_matrix* h)
             ClusterSet& c = cs[set];
             if (c.ncl > 0) {
                 k_cluster_bbox<<<c.ncl, 256, 0, s>>>(c.cl_l, c.cl_u, c.ncl, h->zpts[set], c.n, dim,
-                                                     h->codes[set], h->c_leaf, c.bb_lo, c.bb_hi,
-                                                     c.split_of);
+                                                     h->codes[set], h->c_leaf, leaf_at[set], c.bb_lo,
+                                                     c.bb_hi, c.split_of);
                 HMG_LAUNCH_CHECK();
             }
         }
@@ -504,7 +492,7 @@ hmg_status setup_tree(hmg_matrix* h)
             goto done;
         k_node_classify<<<ceil_div(nn, 256), 256, 0, s>>>(
             cur, nn, h->n[0], h->n[1], dim, cs[0].bb_lo, cs[0].bb_hi, cs[1].bb_lo, cs[1].bb_hi,
-            h->eta, h->rule, h->c_leaf, last_level ? 1 : 0, packed, ltype);
+            h->eta, h->rule, h->c_leaf, leaf_at[0], last_level ? 1 : 0, packed, ltype);
         HMG_LAUNCH_CHECK();
         if ((st = scan_exclusive<long long>(packed, packed, nn, ptot, s))) goto done;
         long long tot = 0;
@@ -548,7 +536,7 @@ hmg_status setup_tree(hmg_matrix* h)
                 int ntot = 0;
                 if ((st = dalloc(&ccnt, (size_t)c.ncl, s))) goto done;
                 k_cluster_count<<<ceil_div(c.ncl, 256), 256, 0, s>>>(c.cl_l, c.cl_u, c.ncl,
-                                                                     h->c_leaf, ccnt);
+                                                                     h->c_leaf, leaf_at[set], ccnt);
                 HMG_LAUNCH_CHECK();
                 if ((st = scan_exclusive<int>(ccnt, ccnt, c.ncl, (int*)ptot, s))) goto done;
                 HMG_CUDA_TRY(cudaMemcpyAsync(&ntot, ptot, sizeof(int), cudaMemcpyDeviceToHost, s));
@@ -557,7 +545,8 @@ hmg_status setup_tree(hmg_matrix* h)
                     (st = dalloc(&nu, (size_t)(ntot > 0 ? ntot : 1), s)))
                     goto done;
                 k_cluster_emit<<<ceil_div(c.ncl, 256), 256, 0, s>>>(c.cl_l, c.cl_u, c.ncl, ccnt,
-                                                                    h->c_leaf, c.split_of, nl, nu);
+                                                                    h->c_leaf, leaf_at[set], c.split_of,
+                                                                    nl, nu);
                 HMG_LAUNCH_CHECK();
                 dfree(ccnt, s);
                 dfree(c.cl_l, s);
@@ -569,52 +558,326 @@ hmg_status setup_tree(hmg_matrix* h)
         }
     }
 
-    // ---- DENSE-first partition into the handle's block arrays -------------------
-    {
-        int nb = nleaves;
-        int* f = nullptr;
-        int nd = 0;
-        h->nblocks = nb;
-        if ((st = dalloc(&h->blk_r0, (size_t)nb, s)) || (st = dalloc(&h->blk_m1, (size_t)nb, s)) ||
-            (st = dalloc(&h->blk_c0, (size_t)nb, s)) || (st = dalloc(&h->blk_m2, (size_t)nb, s)) ||
-            (st = dalloc(&h->blk_type, (size_t)nb, s)) || (st = dalloc(&f, (size_t)nb, s)))
-            goto done;
-        if (nb > 0) {
-            k_dense_flags<<<ceil_div(nb, 256), 256, 0, s>>>(leaves.type, nb, f);
-            HMG_LAUNCH_CHECK();
-            if ((st = scan_exclusive<int>(f, f, nb, (int*)ptot, s))) { dfree(f, s); goto done; }
-            HMG_CUDA_TRY(cudaMemcpyAsync(&nd, ptot, sizeof(int), cudaMemcpyDeviceToHost, s));
-            HMG_CUDA_TRY(cudaStreamSynchronize(s));
-            k_partition<<<ceil_div(nb, 256), 256, 0, s>>>(leaves, nb, f, nd, h->blk_r0, h->blk_m1,
-                                                          h->blk_c0, h->blk_m2, h->blk_type);
-            HMG_LAUNCH_CHECK();
-        }
-        dfree(f, s);
-        h->ndense = nd;
-        h->naca = nb - nd;
-        h->levels = levels;
-        h->h_r0.resize(nb); h->h_m1.resize(nb); h->h_c0.resize(nb); h->h_m2.resize(nb);
-        h->h_type.resize(nb);
-        if (nb > 0) {
-            HMG_CUDA_TRY(cudaMemcpyAsync(h->h_r0.data(), h->blk_r0, sizeof(int) * nb, cudaMemcpyDeviceToHost, s));
-            HMG_CUDA_TRY(cudaMemcpyAsync(h->h_m1.data(), h->blk_m1, sizeof(int) * nb, cudaMemcpyDeviceToHost, s));
-            HMG_CUDA_TRY(cudaMemcpyAsync(h->h_c0.data(), h->blk_c0, sizeof(int) * nb, cudaMemcpyDeviceToHost, s));
-            HMG_CUDA_TRY(cudaMemcpyAsync(h->h_m2.data(), h->blk_m2, sizeof(int) * nb, cudaMemcpyDeviceToHost, s));
-            HMG_CUDA_TRY(cudaMemcpyAsync(h->h_type.data(), h->blk_type, sizeof(int) * nb, cudaMemcpyDeviceToHost, s));
-        }
-        HMG_CUDA_TRY(cudaStreamSynchronize(s));
-    }
-
 done:
     free_nodes(cur, s);
     free_nodes(nxt, s);
-    free_leaves(leaves, s);
     dfree(packed, s);
     dfree(ltype, s);
     dfree(ccnt, s);
     dfree(ptot, s);
     free_cluster_set(cs[0], s);
     free_cluster_set(cs[1], s);
+    return st;
+}
+
+// sort key of a leaf for the grouped order: DENSE first, then the set of its rows
+// (set_off: the first row of every set and the total, nsets + 1 entries)
+__global__ void k_leaf_keys(LeafArrays in, int n, const int* set_off, int nsets, int set_bits,
+                            uint64_t* keys, uint32_t* idx)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int r = in.l1[i];
+    int lo = 0, hi = nsets;  // set_off[lo] <= r < set_off[hi]
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (set_off[mid] <= r) lo = mid; else hi = mid;
+    }
+    keys[i] = ((uint64_t)(in.type[i] == HMG_WT_DENSE ? 0 : 1) << set_bits) | (uint64_t)lo;
+    idx[i] = (uint32_t)i;
+}
+
+__global__ void k_gather_leaves(LeafArrays in, int n, const uint32_t* idx, int* r0, int* m1, int* c0,
+                                int* m2, int* type)
+{
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    const int i = (int)idx[k];
+    r0[k] = in.l1[i];
+    m1[k] = in.u1[i] - in.l1[i] + 1;
+    c0[k] = in.l2[i];
+    m2[k] = in.u2[i] - in.l2[i] + 1;
+    type[k] = in.type[i];
+}
+
+// The leaves as the handle's block arrays, DENSE first (linear_algebra.cu:63-86,
+// a stable partition), and their host copies.  With set_off (grouped point sets: the
+// first row of every set and the total, on the device) the order is DENSE first, then
+// by set, each set's blocks in the order they were emitted.
+static hmg_status partition_blocks(hmg_matrix* h, const LeafArrays& leaves, int nb, int levels,
+                                   const int* set_off, int nsets)
+{
+    cudaStream_t s = h->stream;
+    hmg_status st = HMG_OK;
+    int* f = nullptr;
+    int* tot = nullptr;
+    uint64_t* keys = nullptr;
+    uint32_t* idx = nullptr;
+    int nd = 0;
+    h->nblocks = nb;
+    if ((st = dalloc(&h->blk_r0, (size_t)nb, s)) || (st = dalloc(&h->blk_m1, (size_t)nb, s)) ||
+        (st = dalloc(&h->blk_c0, (size_t)nb, s)) || (st = dalloc(&h->blk_m2, (size_t)nb, s)) ||
+        (st = dalloc(&h->blk_type, (size_t)nb, s)))
+        goto done;
+    if (nb > 0 && !set_off) {
+        if ((st = dalloc(&f, (size_t)nb, s)) || (st = dalloc(&tot, 1, s))) goto done;
+        k_dense_flags<<<ceil_div(nb, 256), 256, 0, s>>>(leaves.type, nb, f);
+        HMG_LAUNCH_CHECK();
+        if ((st = scan_exclusive<int>(f, f, nb, tot, s))) goto done;
+        HMG_CUDA_TRY(cudaMemcpyAsync(&nd, tot, sizeof(int), cudaMemcpyDeviceToHost, s));
+        HMG_CUDA_TRY(cudaStreamSynchronize(s));
+        k_partition<<<ceil_div(nb, 256), 256, 0, s>>>(leaves, nb, f, nd, h->blk_r0, h->blk_m1,
+                                                      h->blk_c0, h->blk_m2, h->blk_type);
+        HMG_LAUNCH_CHECK();
+    } else if (nb > 0) {
+        int set_bits = 1;
+        while ((1 << set_bits) < nsets) set_bits++;
+        if ((st = dalloc(&keys, (size_t)nb, s)) || (st = dalloc(&idx, (size_t)nb, s))) goto done;
+        k_leaf_keys<<<ceil_div(nb, 256), 256, 0, s>>>(leaves, nb, set_off, nsets, set_bits, keys, idx);
+        HMG_LAUNCH_CHECK();
+        if ((st = radix_sort_pairs(keys, idx, nb, set_bits + 1, s))) goto done;
+        k_gather_leaves<<<ceil_div(nb, 256), 256, 0, s>>>(leaves, nb, idx, h->blk_r0, h->blk_m1, h->blk_c0,
+                                                          h->blk_m2, h->blk_type);
+        HMG_LAUNCH_CHECK();
+    }
+    h->levels = levels;
+    h->h_r0.resize(nb); h->h_m1.resize(nb); h->h_c0.resize(nb); h->h_m2.resize(nb);
+    h->h_type.resize(nb);
+    if (nb > 0) {
+        HMG_CUDA_TRY(cudaMemcpyAsync(h->h_r0.data(), h->blk_r0, sizeof(int) * nb, cudaMemcpyDeviceToHost, s));
+        HMG_CUDA_TRY(cudaMemcpyAsync(h->h_m1.data(), h->blk_m1, sizeof(int) * nb, cudaMemcpyDeviceToHost, s));
+        HMG_CUDA_TRY(cudaMemcpyAsync(h->h_c0.data(), h->blk_c0, sizeof(int) * nb, cudaMemcpyDeviceToHost, s));
+        HMG_CUDA_TRY(cudaMemcpyAsync(h->h_m2.data(), h->blk_m2, sizeof(int) * nb, cudaMemcpyDeviceToHost, s));
+        HMG_CUDA_TRY(cudaMemcpyAsync(h->h_type.data(), h->blk_type, sizeof(int) * nb, cudaMemcpyDeviceToHost, s));
+    }
+    HMG_CUDA_TRY(cudaStreamSynchronize(s));
+    if (set_off) nd = (int)std::count(h->h_type.begin(), h->h_type.end(), (int)HMG_WT_DENSE);
+    h->ndense = nd;
+    h->naca = nb - nd;
+
+done:
+    dfree(f, s);
+    dfree(tot, s);
+    dfree(keys, s);
+    dfree(idx, s);
+    return st;
+}
+
+hmg_status setup_tree(hmg_matrix* h)
+{
+    cudaStream_t s = h->stream;
+    hmg_status st = HMG_OK;
+    const int dim = h->dim;
+
+    // ---- Morton codes, sort, gather (hmglib.cu:128-162) ------------------------
+    for (int set = 0; set < 2; set++) {
+        int n = h->n[set];
+        uint32_t* order = nullptr;
+        if ((st = morton_codes(h->pts[set], n, dim, h->bits, h->codes[set], s))) return st;
+        if ((st = dalloc(&order, (size_t)n, s))) return st;
+        k_iota<<<ceil_div(n, 256), 256, 0, s>>>(order, n);
+        HMG_LAUNCH_CHECK();
+        int key_bits = dim * h->bits;
+        if (key_bits > 64) key_bits = 64;
+        if ((st = radix_sort_pairs(h->codes[set], order, n, key_bits, s))) {
+            dfree(order, s);
+            return st;
+        }
+        k_gather_points<<<ceil_div(n, 256), 256, 0, s>>>(h->pts[set], h->zpts[set], order, n,
+                                                         dim, h->perm[set], h->iperm[set]);
+        HMG_LAUNCH_CHECK();
+        dfree(order, s);
+    }
+
+    // ---- block-cluster tree from the root pair, then the DENSE-first block list ----
+    const int root[4] = {0, h->n[0] - 1, 0, h->n[1] - 1};
+    const int* no_leaf_at[2] = {nullptr, nullptr};
+    LeafArrays leaves{};
+    int nleaves = 0, levels = 0;
+    st = traverse(h, 1, &root[0], &root[1], &root[2], &root[3], no_leaf_at, leaves, nleaves, levels);
+    if (!st) st = partition_blocks(h, leaves, nleaves, levels, nullptr, 0);
+    free_leaves(leaves, s);
+    return st;
+}
+
+// ---------------------------------------------------------------------------
+// many point sets clustered in the same launches (hmg_group_setup)
+// ---------------------------------------------------------------------------
+
+// set of union index i: off[set] <= i < off[set + 1]
+__device__ __forceinline__ int set_of_index(const int* off, int nsets, int i)
+{
+    int lo = 0, hi = nsets;
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (off[mid] <= i) lo = mid; else hi = mid;
+    }
+    return lo;
+}
+
+// One CTA per set: order keys of its per-dimension minimum and maximum into
+// mm[(set * 3 + d) * 2 + {0, 1}] (exact, as k_minmax).
+__global__ void k_minmax_sets(const double* coords, int n, const int* off, const int* sdim,
+                              unsigned long long* mm)
+{
+    __shared__ unsigned long long red[2][32];
+    const int set = blockIdx.x, a = off[set], b = off[set + 1], dim = sdim[set];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    for (int d = 0; d < dim; d++) {
+        const double* c = coords + (size_t)d * n;
+        unsigned long long lo = ~0ull, hi = 0ull;
+        for (int i = a + threadIdx.x; i < b; i += blockDim.x) {
+            const unsigned long long k = order_key(c[i]);
+            lo = k < lo ? k : lo;
+            hi = k > hi ? k : hi;
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            const unsigned long long x = __shfl_xor_sync(0xffffffffu, lo, o);
+            const unsigned long long y = __shfl_xor_sync(0xffffffffu, hi, o);
+            lo = x < lo ? x : lo;
+            hi = y > hi ? y : hi;
+        }
+        if (lane == 0) {
+            red[0][warp] = lo;
+            red[1][warp] = hi;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            for (int w = 1; w < nw; w++) {
+                lo = red[0][w] < lo ? red[0][w] : lo;
+                hi = red[1][w] > hi ? red[1][w] : hi;
+            }
+            mm[((size_t)set * 3 + d) * 2] = lo;
+            mm[((size_t)set * 3 + d) * 2 + 1] = hi;
+        }
+        __syncthreads();
+    }
+}
+
+// k_morton for every set at once: point i of the union (stride n) takes its set's
+// dimension, bits and extremes; sbits 0 marks a (dim, bits) without Morton codes
+// (code 0, as morton.cu:65).  set_of[i] receives the point's set.
+__global__ void k_morton_sets(const double* coords, int n, const int* off, int nsets, const int* sdim,
+                              const int* sbits, const unsigned long long* mm, uint64_t* codes,
+                              uint64_t* set_of)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int set = set_of_index(off, nsets, i);
+    const int dim = sdim[set], bits = sbits[set];
+    uint64_t code = 0;
+    if (bits > 0) {
+        const double scale = (double)(1ull << bits);
+        const uint64_t cap = (1ull << bits) - 1ull;
+        for (int d = 0; d < dim; d++) {
+            double lo = order_key_inv(mm[((size_t)set * 3 + d) * 2]);
+            double hi = order_key_inv(mm[((size_t)set * 3 + d) * 2 + 1]);
+            double range = hi - lo;
+            double t = (coords[(size_t)d * n + i] - lo) / range;
+            uint64_t q = (uint64_t)floor(t * scale);
+            q = q < cap ? q : cap;
+            for (int b = 0; b < bits; b++) code |= ((q >> b) & 1ull) << (b * dim + d);
+        }
+    }
+    codes[i] = code;
+    set_of[i] = (uint64_t)set;
+}
+
+__global__ void k_gather_u64(const uint64_t* in, const uint32_t* idx, int n, uint64_t* out)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) out[i] = in[idx[i]];
+}
+
+__global__ void k_leaf_at(const int* off, int nsets, const int* sleaf, int n, int* leaf_at)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) leaf_at[i] = sleaf[set_of_index(off, nsets, i)];
+}
+
+// The tree of a group handle whose union points (g->pts, sets contiguous at off[w],
+// 2D sets padded with a zero third coordinate) are in place: every set ordered by its
+// own Morton codes, then one level-synchronous traversal from one root pair per set.
+// Per set: sdim, sbits (0: no Morton codes), sleaf (leaf size).  Each set's
+// permutation, tree and blocks are those hmg_setup gives the set alone; the blocks are
+// ordered DENSE first, then by set.
+hmg_status group_setup_tree(hmg_matrix* g, int nsets, const int* const* off, const int* sdim,
+                            const int* sbits, const int* sleaf)
+{
+    cudaStream_t s = g->stream;
+    hmg_status st = HMG_OK;
+    int* doff[2] = {nullptr, nullptr};
+    int *dsdim = nullptr, *dsbits = nullptr, *dsleaf = nullptr;
+    int* leaf_at[2] = {nullptr, nullptr};
+    unsigned long long* mm = nullptr;
+    uint64_t *keys = nullptr, *set_of = nullptr;
+    uint32_t* order = nullptr;
+    LeafArrays leaves{};
+    int nleaves = 0, levels = 0, code_bits = 1, set_bits = 1;
+    std::vector<int> rl[2], ru[2];
+    for (int i = 0; i < nsets; i++) code_bits = std::max(code_bits, std::min(64, sdim[i] * sbits[i]));
+    while ((1 << set_bits) < nsets) set_bits++;
+    if ((st = dalloc(&dsdim, (size_t)nsets, s)) || (st = dalloc(&dsbits, (size_t)nsets, s)) ||
+        (st = dalloc(&dsleaf, (size_t)nsets, s)) || (st = dalloc(&mm, (size_t)nsets * 6, s)))
+        goto done;
+    HMG_CUDA_TRY(cudaMemcpyAsync(dsdim, sdim, sizeof(int) * nsets, cudaMemcpyHostToDevice, s));
+    HMG_CUDA_TRY(cudaMemcpyAsync(dsbits, sbits, sizeof(int) * nsets, cudaMemcpyHostToDevice, s));
+    HMG_CUDA_TRY(cudaMemcpyAsync(dsleaf, sleaf, sizeof(int) * nsets, cudaMemcpyHostToDevice, s));
+    for (int w = 0; w < 2; w++) {
+        const int n = g->n[w];
+        if ((st = dalloc(&doff[w], (size_t)nsets + 1, s)) || (st = dalloc(&leaf_at[w], (size_t)n, s)) ||
+            (st = dalloc(&keys, (size_t)n, s)) || (st = dalloc(&set_of, (size_t)n, s)) ||
+            (st = dalloc(&order, (size_t)n, s)))
+            goto done;
+        HMG_CUDA_TRY(cudaMemcpyAsync(doff[w], off[w], sizeof(int) * (nsets + 1), cudaMemcpyHostToDevice, s));
+        // ---- every set's Morton codes, then its points in code order (hmglib.cu:128-162) ----
+        k_minmax_sets<<<nsets, 256, 0, s>>>(g->pts[w], n, doff[w], dsdim, mm);
+        HMG_LAUNCH_CHECK();
+        k_morton_sets<<<ceil_div(n, 256), 256, 0, s>>>(g->pts[w], n, doff[w], nsets, dsdim, dsbits, mm,
+                                                       g->codes[w], set_of);
+        HMG_LAUNCH_CHECK();
+        // stable by code, then stable by set: each set in its own stable code order
+        HMG_CUDA_TRY(cudaMemcpyAsync(keys, g->codes[w], sizeof(uint64_t) * n, cudaMemcpyDeviceToDevice, s));
+        k_iota<<<ceil_div(n, 256), 256, 0, s>>>(order, n);
+        HMG_LAUNCH_CHECK();
+        if ((st = radix_sort_pairs(keys, order, n, code_bits, s))) goto done;
+        k_gather_u64<<<ceil_div(n, 256), 256, 0, s>>>(set_of, order, n, keys);
+        HMG_LAUNCH_CHECK();
+        if ((st = radix_sort_pairs(keys, order, n, set_bits, s))) goto done;
+        k_gather_u64<<<ceil_div(n, 256), 256, 0, s>>>(g->codes[w], order, n, keys);
+        HMG_LAUNCH_CHECK();
+        HMG_CUDA_TRY(cudaMemcpyAsync(g->codes[w], keys, sizeof(uint64_t) * n, cudaMemcpyDeviceToDevice, s));
+        k_gather_points<<<ceil_div(n, 256), 256, 0, s>>>(g->pts[w], g->zpts[w], order, n, g->dim,
+                                                         g->perm[w], g->iperm[w]);
+        HMG_LAUNCH_CHECK();
+        k_leaf_at<<<ceil_div(n, 256), 256, 0, s>>>(doff[w], nsets, dsleaf, n, leaf_at[w]);
+        HMG_LAUNCH_CHECK();
+        dfree(keys, s);
+        dfree(set_of, s);
+        dfree(order, s);
+        rl[w].resize(nsets);
+        ru[w].resize(nsets);
+        for (int i = 0; i < nsets; i++) {
+            rl[w][i] = off[w][i];
+            ru[w][i] = off[w][i + 1] - 1;
+        }
+    }
+    // ---- one traversal from every set's root pair, then the blocks -----------------
+    {
+        const int* la[2] = {leaf_at[0], leaf_at[1]};
+        st = traverse(g, nsets, rl[0].data(), ru[0].data(), rl[1].data(), ru[1].data(), la, leaves, nleaves,
+                      levels);
+    }
+    if (!st) st = partition_blocks(g, leaves, nleaves, levels, doff[0], nsets);
+
+done:
+    free_leaves(leaves, s);
+    dfree(doff[0], s); dfree(doff[1], s);
+    dfree(dsdim, s); dfree(dsbits, s); dfree(dsleaf, s);
+    dfree(leaf_at[0], s); dfree(leaf_at[1], s);
+    dfree(mm, s);
+    dfree(keys, s); dfree(set_of, s); dfree(order, s);
     return st;
 }
 

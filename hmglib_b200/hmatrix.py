@@ -316,6 +316,31 @@ def group(sets, stream: int | None = None) -> "HMatrix":
     return g
 
 
+def group_setup(sets, eta: float, c_leaf, max_level: int = 50, rule: int = L.ADMISSIBLE_MAX,
+                stream: int | None = None) -> "HMatrix":
+    """The block-diagonal union of HMatrix objects that have points and a kernel but
+    need not be set up (hmg_group_setup): every set is ordered and clustered in the same
+    kernel launches.  `c_leaf` is one leaf size for all sets or one per set.  Equal, bit
+    for bit, to `group` over the sets after `setup(eta, c_leaf[i], max_level,
+    rule=rule)` on each."""
+    lib = L.lib()
+    leaf = [int(c_leaf)] * len(sets) if np.isscalar(c_leaf) else [int(c) for c in c_leaf]
+    if len(leaf) != len(sets):
+        raise ValueError("c_leaf: one value, or one per set")
+    arr = (C.c_void_p * len(sets))(*[hm._h.value for hm in sets])
+    lv = (C.c_int * len(sets))(*leaf)
+    h = C.c_void_p()
+    L.check(lib.hmg_group_setup(C.byref(h), arr, len(sets), float(eta), lv, int(max_level), int(rule),
+                                C.c_void_p(stream or 0)), "hmg_group_setup")
+    g = HMatrix.__new__(HMatrix)
+    g._lib = lib
+    g._h = h
+    g.n1 = sum(hm.n1 for hm in sets)
+    g.n2 = sum(hm.n2 for hm in sets)
+    g.dim = max(hm.dim for hm in sets)
+    return g
+
+
 def radix_sort_u64(keys_ptr: int, vals_ptr: int, n: int, key_bits: int = 64, stream: int = 0):
     L.check(L.lib().hmg_radix_sort_u64(C.c_void_p(keys_ptr), C.c_void_p(vals_ptr), int(n),
                                        int(key_bits), C.c_void_p(stream)), "hmg_radix_sort_u64")

@@ -206,6 +206,18 @@ hmg_status hmg_load(hmg_matrix** out, const char* path, void* stream);
  * vectors are the concatenation of the sets' vectors.  Each set's result equals its
  * own handle's bit for bit.  The set handles stay valid and independent. */
 hmg_status hmg_group_create(hmg_matrix** out, hmg_matrix* const* sets, int count, void* stream);
+/* The same group built without setting the sets up one by one: `sets` need only
+ * hmg_set_points (both sides) and hmg_set_kernel (same kernel kind and regularization,
+ * 2D and 3D mixed).  Every set's points are ordered by its own Morton codes and every
+ * set's block-cluster tree is built in the same kernel launches (one level loop from
+ * one root pair per set), with admissibility parameter eta, rule and max_level shared
+ * and the leaf size c_leaf[i] of set i.  The result equals hmg_setup(sets[i], eta,
+ * c_leaf[i], max_level, ..., rule) on every set followed by hmg_group_create, bit for
+ * bit: the same permutations, blocks, block order and products.  The set handles are
+ * not modified.  No reference counterpart (the reference builds one tree per call,
+ * hmglib.cu:125-225). */
+hmg_status hmg_group_setup(hmg_matrix** out, hmg_matrix* const* sets, int count, double eta, const int* c_leaf,
+                           int max_level, int rule, void* stream);
 /* offsets[0..count] of a group's rows (set 0) or columns (set 1); offsets[count] = n */
 hmg_status hmg_group_offsets(hmg_matrix* h, int set, int64_t* offsets);
 

@@ -97,3 +97,124 @@ def test_group_solve_and_errors(hmg, cuda):
     for H in sets + [other]:
         H.close()
     G.close()
+
+
+def _raw_sets(hmg, sizes, seed=3):
+    """The sets of _sets (same points and kernel parameters) with points and kernel
+    only: no hmg_setup."""
+    rng = np.random.default_rng(seed)
+    out, leaf = [], []
+    for i, n in enumerate(sizes):
+        dim = 2 if i % 2 == 0 else 3
+        p = make_points("uniform", n, dim, seed * 1000 + i)
+        H = hmg.HMatrix(n, n, dim)
+        H.set_points(0, p)
+        H.set_points(1, p)
+        H.set_kernel(hmg.KERNEL_GAUSSIAN, float(rng.uniform(0.01, 0.2)), 0.0)
+        out.append(H)
+        leaf.append(64 if dim == 2 else 128)
+    return out, leaf
+
+
+@pytest.mark.parametrize("rule", [1, 0], ids=["min", "max"])
+def test_group_setup_equals_per_set_setup(hmg, cuda, rule):
+    """hmg_group_setup orders and clusters every set in the same launches; the handle
+    must equal the one hmg_group_create makes from sets set up one by one: offsets,
+    Z-ordered points, permutations, every set's Morton codes, the block list in
+    order, the ranks and the products, bit for bit."""
+    sizes = [1024, 3000, 700, 5000, 64, 2500, 9000, 1500, 65, 4097]
+    ref = []
+    rng = np.random.default_rng(3)
+    for i, n in enumerate(sizes):
+        dim = 2 if i % 2 == 0 else 3
+        p = make_points("uniform", n, dim, 3 * 1000 + i)
+        H = engine(hmg, p, p, 1.5, 64 if dim == 2 else 128, rule=rule)
+        H.set_kernel(hmg.KERNEL_GAUSSIAN, float(rng.uniform(0.01, 0.2)), 0.0)
+        ref.append(H)
+    G0 = hmg.group(ref)
+    raw, leaf = _raw_sets(hmg, sizes)
+    G1 = hmg.group_setup(raw, 1.5, leaf, rule=rule)
+    off = G1.offsets(0)
+    np.testing.assert_array_equal(off, G0.offsets(0))
+    np.testing.assert_array_equal(G1.offsets(1), G0.offsets(1))
+    i0, i1 = G0.info(), G1.info()
+    for k in ("block_count", "dense_count", "aca_count", "tile_count", "group_count", "levels"):
+        assert i1[k] == i0[k], k
+    for a, b in zip(G1.blocks(), G0.blocks()):
+        np.testing.assert_array_equal(a, b)
+    for w in (0, 1):
+        np.testing.assert_array_equal(G1.order(w), G0.order(w))
+        np.testing.assert_array_equal(G1.points(w), G0.points(w))
+        c = G1.codes(w)
+        for i, H in enumerate(ref):
+            np.testing.assert_array_equal(c[off[i]:off[i + 1]], H.codes(w))
+    for G in (G0, G1):
+        G.precompute_aca(64, 1e-5, 1)
+        G.precompute_dense(1)
+    np.testing.assert_array_equal(G1.ranks(), G0.ranks())
+    x = np.random.default_rng(7).uniform(-1, 1, int(off[-1]))
+    np.testing.assert_array_equal(G1.matvec(x), G0.matvec(x))
+    # the sets themselves are untouched: still without a tree
+    with pytest.raises(hmg.HmgError):
+        raw[0].blocks()
+    for H in ref + raw:
+        H.close()
+    G0.close()
+    G1.close()
+
+
+def test_group_setup_many_sets(hmg, cuda):
+    """512 sets of 2^8 .. 2^11 points, 2D and 3D: one grouped setup against per-set
+    setups, compared on the block list and one product."""
+    from hmglib_b200 import synth
+    sets = synth.group_sets(512, 5, 8.0, 11.0)
+    ref, raw, leaf = [], [], []
+    for p, l2 in sets:
+        dim, n = p.shape
+        c = 64 if dim == 2 else 128
+        H = engine(hmg, p, p, 1.5, c, rule=1)
+        H.set_kernel(hmg.KERNEL_GAUSSIAN, l2, 0.0)
+        ref.append(H)
+        R = hmg.HMatrix(n, n, dim)
+        R.set_points(0, p)
+        R.set_points(1, p)
+        R.set_kernel(hmg.KERNEL_GAUSSIAN, l2, 0.0)
+        raw.append(R)
+        leaf.append(c)
+    G0 = hmg.group(ref)
+    G1 = hmg.group_setup(raw, 1.5, leaf, rule=1)
+    for a, b in zip(G1.blocks(), G0.blocks()):
+        np.testing.assert_array_equal(a, b)
+    for w in (0, 1):
+        np.testing.assert_array_equal(G1.order(w), G0.order(w))
+    for G in (G0, G1):
+        G.precompute_aca(32, 1e-5, 1)
+        G.precompute_dense(1)
+    x = np.random.default_rng(8).uniform(-1, 1, G0.n2)
+    np.testing.assert_array_equal(G1.matvec(x), G0.matvec(x))
+    for H in ref + raw:
+        H.close()
+    G0.close()
+    G1.close()
+
+
+def test_group_setup_errors(hmg, cuda):
+    raw, leaf = _raw_sets(hmg, [500, 800])
+    with pytest.raises(ValueError):
+        hmg.group_setup(raw, 1.5, [64])
+    with pytest.raises(hmg.HmgError):
+        hmg.group_setup(raw, 1.5, [64, 0])
+    with pytest.raises(hmg.HmgError):
+        hmg.group_setup(raw, -1.0, leaf)
+    bare = hmg.HMatrix(300, 300, 3)  # no points, no kernel
+    with pytest.raises(hmg.HmgError):
+        hmg.group_setup(raw + [bare], 1.5, leaf + [128])
+    other = hmg.HMatrix(300, 300, 3)
+    p = make_points("uniform", 300, 3, 9)
+    other.set_points(0, p)
+    other.set_points(1, p)
+    other.set_kernel(hmg.KERNEL_MATERN32, 0.2, 0.0)  # another kernel kind
+    with pytest.raises(hmg.HmgError):
+        hmg.group_setup(raw + [other], 1.5, leaf + [128])
+    for H in raw + [bare, other]:
+        H.close()
