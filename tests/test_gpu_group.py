@@ -218,3 +218,19 @@ def test_group_setup_errors(hmg, cuda):
         hmg.group_setup(raw + [other], 1.5, leaf + [128])
     for H in raw + [bare, other]:
         H.close()
+
+
+def test_group_setup_one_set(hmg, cuda):
+    """A group of one set: the same tree as hmg_setup on that set alone."""
+    raw, leaf = _raw_sets(hmg, [6000])
+    G = hmg.group_setup(raw, 1.5, leaf, rule=1)
+    ref = _sets(hmg, [6000])[0]
+    for a, b in zip(G.blocks(), ref.blocks()):
+        np.testing.assert_array_equal(a, b)
+    for w in (0, 1):
+        np.testing.assert_array_equal(G.order(w), ref.order(w))
+        np.testing.assert_array_equal(G.codes(w), ref.codes(w))
+    assert G.info()["levels"] == ref.info()["levels"]
+    for H in raw + [ref]:
+        H.close()
+    G.close()
