@@ -234,3 +234,45 @@ def test_group_setup_one_set(hmg, cuda):
     for H in raw + [ref]:
         H.close()
     G.close()
+
+
+def test_group_setup_rectangular(hmg, cuda):
+    """Sets whose rows and columns are different point clouds (n1 != n2), one of them
+    on a line: grouped setup against per-set setup, on the blocks, both orders and one
+    product."""
+    shapes = [(3000, 1200), (700, 2500), (4096, 4000), (90, 300)]
+    rng = np.random.default_rng(11)
+    ref, raw, leaf = [], [], []
+    for i, (n1, n2) in enumerate(shapes):
+        dim = 3 if i % 2 == 0 else 2
+        # the last set lies on a line: max == min in every dimension but the first
+        gen = "line" if i == len(shapes) - 1 else "uniform"
+        p1 = make_points(gen, n1, dim, 500 + i)
+        p2 = make_points(gen, n2, dim, 600 + i)
+        l2 = float(rng.uniform(0.01, 0.2))
+        c = 64 if dim == 2 else 128
+        H = engine(hmg, p1, p2, 1.5, c, rule=1)
+        H.set_kernel(hmg.KERNEL_GAUSSIAN, l2, 0.0)
+        ref.append(H)
+        R = hmg.HMatrix(n1, n2, dim)
+        R.set_points(0, p1)
+        R.set_points(1, p2)
+        R.set_kernel(hmg.KERNEL_GAUSSIAN, l2, 0.0)
+        raw.append(R)
+        leaf.append(c)
+    G0 = hmg.group(ref)
+    G1 = hmg.group_setup(raw, 1.5, leaf, rule=1)
+    np.testing.assert_array_equal(G1.offsets(1), G0.offsets(1))
+    for a, b in zip(G1.blocks(), G0.blocks()):
+        np.testing.assert_array_equal(a, b)
+    for w in (0, 1):
+        np.testing.assert_array_equal(G1.order(w), G0.order(w))
+    for G in (G0, G1):
+        G.precompute_aca(64, 1e-6, 1)
+        G.precompute_dense(1)
+    x = np.random.default_rng(12).uniform(-1, 1, G0.n2)
+    np.testing.assert_array_equal(G1.matvec(x), G0.matvec(x))
+    for H in ref + raw:
+        H.close()
+    G0.close()
+    G1.close()
