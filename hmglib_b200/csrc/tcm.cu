@@ -48,7 +48,10 @@
 #include <cuda_fp8.h>
 
 #include <algorithm>
+#include <functional>
+#include <memory>
 #include <queue>
+#include <thread>
 #include <vector>
 
 #include "hmg_matrix.cuh"
@@ -854,6 +857,15 @@ struct TcmPlan {
         // copy bytes plus the MMA issue time (~46 cycles a 128 x N x 16 MMA) in bytes
         cost.back() += raw_bytes + 2048.0 * mode * nk;
     }
+    // src's jobs after this plan's (before finish)
+    void append(const TcmPlan& src)
+    {
+        const int base = (int)steps.size();
+        for (int x : src.step0) step0.push_back(base + x);
+        steps.insert(steps.end(), src.steps.begin(), src.steps.end());
+        jobs.insert(jobs.end(), src.jobs.begin(), src.jobs.end());
+        cost.insert(cost.end(), src.cost.begin(), src.cost.end());
+    }
     void finish()
     {
         step0.push_back((int)steps.size());
@@ -864,6 +876,12 @@ struct TcmPlan {
         }
     }
 };
+
+// host threads for building a plan
+int plan_threads()
+{
+    return (int)std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+}
 
 // Jobs onto CTAs: the few large ones first, longest first, then the rest in plan order
 // (row tiles / column clusters in Z order), each onto the least loaded CTA, so that the
@@ -891,25 +909,43 @@ hmg_status upload_plan(hmg_matrix* h, int q, const TcmPlan& L, int grid)
         mine[l.second].push_back(j);
         heap.push({l.first + L.cost[j] + 4096.0, l.second});
     }
-    std::vector<TcmStep> steps;
     std::vector<TcmJob> jobs;
     std::vector<int2> cta(grid + 1);
-    steps.reserve(L.steps.size());
+    size_t nsteps = 0;
     for (int c = 0; c < grid; c++) {
-        cta[c] = make_int2((int)jobs.size(), (int)steps.size());
+        cta[c] = make_int2((int)jobs.size(), (int)nsteps);
         for (int j : mine[c]) {
             jobs.push_back(L.jobs[j]);
-            for (int i = L.step0[j]; i < L.step0[j + 1]; i++) steps.push_back(L.steps[i]);
+            nsteps += (size_t)(L.step0[j + 1] - L.step0[j]);
         }
     }
-    cta[grid] = make_int2((int)jobs.size(), (int)steps.size());
+    cta[grid] = make_int2((int)jobs.size(), (int)nsteps);
+    // the steps in CTA order, each CTA's range copied on one of a few host threads
+    std::unique_ptr<TcmStep[]> steps(new TcmStep[std::max(nsteps, (size_t)1)]);
+    {
+        auto copy = [&](int c0, int c1) {
+            for (int c = c0; c < c1; c++) {
+                size_t o = (size_t)cta[c].y;
+                for (int j : mine[c]) {
+                    const size_t k = (size_t)(L.step0[j + 1] - L.step0[j]);
+                    std::copy(L.steps.begin() + L.step0[j], L.steps.begin() + L.step0[j + 1], steps.get() + o);
+                    o += k;
+                }
+            }
+        };
+        const int nth = std::min(8, plan_threads());
+        std::vector<std::thread> th;
+        for (int k = 1; k < nth; k++) th.emplace_back(copy, grid * k / nth, grid * (k + 1) / nth);
+        copy(0, grid / nth);
+        for (std::thread& x : th) x.join();
+    }
     hmg_status st;
-    if ((st = dalloc(&h->tcm_steps[q], std::max(steps.size(), (size_t)1) * sizeof(TcmStep), s)) ||
+    if ((st = dalloc(&h->tcm_steps[q], std::max(nsteps, (size_t)1) * sizeof(TcmStep), s)) ||
         (st = dalloc(&h->tcm_jobs[q], std::max(jobs.size(), (size_t)1) * sizeof(TcmJob), s)) ||
         (st = dalloc(&h->tcm_cta[q], (size_t)(grid + 1) * sizeof(int2), s)))
         return st;
-    if (!steps.empty())
-        HMG_CUDA_TRY(cudaMemcpyAsync(h->tcm_steps[q], steps.data(), steps.size() * sizeof(TcmStep), cudaMemcpyHostToDevice, s));
+    if (nsteps > 0)
+        HMG_CUDA_TRY(cudaMemcpyAsync(h->tcm_steps[q], steps.get(), nsteps * sizeof(TcmStep), cudaMemcpyHostToDevice, s));
     if (!jobs.empty())
         HMG_CUDA_TRY(cudaMemcpyAsync(h->tcm_jobs[q], jobs.data(), jobs.size() * sizeof(TcmJob), cudaMemcpyHostToDevice, s));
     HMG_CUDA_TRY(cudaMemcpyAsync(h->tcm_cta[q], cta.data(), cta.size() * sizeof(int2), cudaMemcpyHostToDevice, s));
@@ -974,90 +1010,147 @@ hmg_status build_tcm(hmg_matrix* h)
             if (h->h_m2[x] != h->h_m2[y]) return h->h_m2[x] < h->h_m2[y];
             return h->h_rank[x] > h->h_rank[y];
         });
-        for (size_t g0 = 0; g0 < far.size();) {
-            size_t g1 = g0;
-            while (g1 < far.size() && h->h_c0[far[g1]] == h->h_c0[far[g0]] && h->h_m2[far[g1]] == h->h_m2[far[g0]]) g1++;
-            std::vector<std::vector<int>> members;
+        // the column clusters (runs of equal c0 and m2 in `far`) are planned in contiguous
+        // ranges on several host threads with range-local stack and t_b numbering, and
+        // joined in order with those numbers shifted: the plan does not depend on the split
+        std::vector<size_t> gs;  // first entry of every column cluster, then far.size()
+        for (size_t g = 0; g < far.size(); g++)
+            if (g == 0 || h->h_c0[far[g]] != h->h_c0[far[g - 1]] || h->h_m2[far[g]] != h->h_m2[far[g - 1]])
+                gs.push_back(g);
+        gs.push_back(far.size());
+        const int ncl = (int)gs.size() - 1;
+        struct Part {
+            std::vector<TcmStack> stacks;
+            std::vector<int> far_blocks;
+            std::vector<long long> far_term;
+            TcmPlan plan;
+            long long tgroups = 0;
+        };
+        auto plan_clusters = [&](int k0, int k1, Part& P) {
+            std::vector<std::vector<int>> members;  // the stacks of one cluster (first fit)
             std::vector<int> fill;
-            for (size_t i = g0; i < g1; i++) {
-                const int b = far[i], kwb = tcm_kw(terms(b));
-                size_t k = 0;
-                while (k < members.size() && fill[k] + kwb > 128) k++;
-                if (k == members.size()) {
-                    members.emplace_back();
-                    fill.push_back(0);
+            for (int gk = k0; gk < k1; gk++) {
+                const size_t g0 = gs[gk], g1 = gs[gk + 1];
+                size_t nstk = 0;
+                for (size_t i = g0; i < g1; i++) {
+                    const int b = far[i], kwb = tcm_kw(terms(b));
+                    size_t k = 0;
+                    while (k < nstk && fill[k] + kwb > 128) k++;
+                    if (k == nstk) {
+                        if (nstk == members.size()) {
+                            members.emplace_back();
+                            fill.push_back(0);
+                        }
+                        members[nstk].clear();
+                        fill[nstk] = 0;
+                        nstk++;
+                    }
+                    members[k].push_back(b);
+                    fill[k] += kwb;
                 }
-                members[k].push_back(b);
-                fill[k] += kwb;
+                const int c0 = h->h_c0[far[g0]], m2 = h->h_m2[far[g0]], a = c0 & 7, kw = (a + m2 + 15) & ~15;
+                const int m2p4 = ((m2 + 3) & ~3) / 4;
+                for (size_t k = 0; k < nstk; k++) {
+                    TcmStack sk{};
+                    sk.nmem = (int)members[k].size();
+                    sk.m2p4 = m2p4;
+                    uint32_t row_ent[128];  // per stack row: raw row | tier | place, as rtab without the row
+                    for (int m = 0; m < 128; m++) row_ent[m] = 3u << 16;
+                    const long long tg0 = P.tgroups;
+                    int off = 0, q = 0;
+                    for (int u = 0; u < sk.nmem; u++) {
+                        const int b = members[k][u];
+                        const TcmTerms T = terms(b);
+                        const int kwb = tcm_kw(T);
+                        sk.vptr[u] = static_cast<const char*>(pv[b]);
+                        sk.qb[u] = q;
+                        // stack rows in the K layout of TcmTerms: FP32 term rows, FP16 pair rows
+                        // (two terms each), FP8 quad rows (four terms each), padding rows zero
+                        for (int t = 0; t < T.r32; t++) row_ent[off + t] = (uint32_t)(q + t) << 8;
+                        for (int t = 0; t < T.r16; t++)
+                            row_ent[off + T.r32p + t] = (uint32_t)(q + T.r32 + t / 2) << 8 | 1u << 16 | (uint32_t)(t & 1) << 18;
+                        for (int t = 0; t < T.r8; t++)
+                            row_ent[off + T.r32p + T.r16p + t] =
+                                (uint32_t)(q + T.r32 + T.r16 / 2 + t / 4) << 8 | 2u << 16 | (uint32_t)(t & 3) << 18;
+                        toff[b] = P.tgroups;
+                        P.far_blocks.push_back(b);
+                        P.far_term.push_back(P.tgroups * 16);
+                        P.tgroups += kwb / 16;
+                        off += kwb;
+                        q += T.r32 + T.r16 / 2 + T.r8 / 4;
+                    }
+                    sk.nq = q;
+                    // rows in tier order (FP32, FP16, FP8, none), each carrying its row number
+                    // (a counting sort: row order kept within a tier)
+                    {
+                        int start[4] = {0, 0, 0, 0};
+                        for (int m = 0; m < 128; m++) start[(row_ent[m] >> 16) & 3]++;
+                        for (int t = 3, acc = 128; t >= 0; t--) {
+                            acc -= start[t];
+                            start[t] = acc;
+                        }
+                        for (int m = 0; m < 128; m++) sk.rtab[start[(row_ent[m] >> 16) & 3]++] = row_ent[m] | (uint32_t)m;
+                    }
+                    const int job = (int)P.stacks.size();
+                    P.stacks.push_back(sk);
+                    P.plan.begin(TcmJob{(int)(tg0 * 16), off});
+                    for (int kp0 = 0; kp0 < kw; kp0 += 32) {
+                        const int nk = std::min(2, (kw - kp0) / 16);
+                        TcmStep stp{};
+                        stp.raw = nullptr;
+                        stp.b_kc = (c0 >> 3) + kp0 / 8;
+                        stp.meta = nk | (6 << 12);
+                        stp.rows = off;
+                        stp.kp0 = kp0;
+                        stp.n16 = job;
+                        stp.cc0 = (kp0 - a) >= 0 ? (kp0 - a) / 4 : -((a - kp0 + 3) / 4);
+                        stp.t0 = a;
+                        stp.t1 = m2p4;
+                        stp.t2 = 0;
+                        P.plan.add(stp, 144.0 * q);
+                    }
+                }
             }
-            const int c0 = h->h_c0[far[g0]], m2 = h->h_m2[far[g0]], a = c0 & 7, kw = (a + m2 + 15) & ~15;
-            const int m2p4 = ((m2 + 3) & ~3) / 4;
-            for (size_t k = 0; k < members.size(); k++) {
-                TcmStack sk{};
-                sk.nmem = (int)members[k].size();
-                sk.m2p4 = m2p4;
-                uint32_t row_ent[128];  // per stack row: raw row | tier | place, as rtab without the row
-                for (int m = 0; m < 128; m++) row_ent[m] = 3u << 16;
-                const long long tg0 = tgroups;
-                int off = 0, q = 0;
-                for (int u = 0; u < sk.nmem; u++) {
-                    const int b = members[k][u];
-                    const TcmTerms T = terms(b);
-                    const int kwb = tcm_kw(T);
-                    sk.vptr[u] = static_cast<const char*>(pv[b]);
-                    sk.qb[u] = q;
-                    // stack rows in the K layout of TcmTerms: FP32 term rows, FP16 pair rows
-                    // (two terms each), FP8 quad rows (four terms each), padding rows zero
-                    for (int t = 0; t < T.r32; t++) row_ent[off + t] = (uint32_t)(q + t) << 8;
-                    for (int t = 0; t < T.r16; t++)
-                        row_ent[off + T.r32p + t] = (uint32_t)(q + T.r32 + t / 2) << 8 | 1u << 16 | (uint32_t)(t & 1) << 18;
-                    for (int t = 0; t < T.r8; t++)
-                        row_ent[off + T.r32p + T.r16p + t] =
-                            (uint32_t)(q + T.r32 + T.r16 / 2 + t / 4) << 8 | 2u << 16 | (uint32_t)(t & 3) << 18;
-                    toff[b] = tgroups;
-                    far_blocks.push_back(b);
-                    far_term.push_back(tgroups * 16);
-                    tgroups += kwb / 16;
-                    off += kwb;
-                    q += T.r32 + T.r16 / 2 + T.r8 / 4;
-                }
-                sk.nq = q;
-                // rows in tier order (FP32, FP16, FP8, none), each carrying its row number
-                {
-                    int i = 0;
-                    for (uint32_t tier = 0; tier < 4; tier++)
-                        for (int m = 0; m < 128; m++)
-                            if (((row_ent[m] >> 16) & 3) == tier) sk.rtab[i++] = row_ent[m] | (uint32_t)m;
-                }
-                const int job = (int)stacks.size();
-                stacks.push_back(sk);
-                p1.begin(TcmJob{(int)(tg0 * 16), off});
-                for (int kp0 = 0; kp0 < kw; kp0 += 32) {
-                    const int nk = std::min(2, (kw - kp0) / 16);
-                    TcmStep stp{};
-                    stp.raw = nullptr;
-                    stp.b_kc = (c0 >> 3) + kp0 / 8;
-                    stp.meta = nk | (6 << 12);
-                    stp.rows = off;
-                    stp.kp0 = kp0;
-                    stp.n16 = job;
-                    stp.cc0 = (kp0 - a) >= 0 ? (kp0 - a) / 4 : -((a - kp0 + 3) / 4);
-                    stp.t0 = a;
-                    stp.t1 = m2p4;
-                    stp.t2 = 0;
-                    p1.add(stp, 144.0 * q);
-                }
+        };
+        const int parts = std::max(1, std::min(plan_threads(), ncl / 256));
+        std::vector<int> cut(parts + 1, ncl);
+        cut[0] = 0;
+        for (int k = 1, g = 0; k < parts; k++) {  // about far.size() / parts blocks a range
+            const size_t goal = far.size() * k / parts;
+            while (g < ncl && gs[g] < goal) g++;
+            cut[k] = std::max(g, cut[k - 1]);
+        }
+        std::vector<Part> part(parts);
+        std::vector<std::thread> th;
+        for (int k = 1; k < parts; k++) th.emplace_back(plan_clusters, cut[k], cut[k + 1], std::ref(part[k]));
+        plan_clusters(cut[0], cut[1], part[0]);
+        for (std::thread& x : th) x.join();
+        for (int k = 0; k < parts; k++) {
+            Part& P = part[k];
+            const int base_stack = (int)stacks.size();
+            const long long base_tg = tgroups;
+            for (TcmStep& stp : P.plan.steps) stp.n16 += base_stack;
+            for (TcmJob& j : P.plan.jobs) j.r0 = (int)((long long)j.r0 + base_tg * 16);
+            for (size_t i = 0; i < P.far_blocks.size(); i++) {
+                toff[P.far_blocks[i]] += base_tg;
+                P.far_term[i] += base_tg * 16;
             }
-            g0 = g1;
+            stacks.insert(stacks.end(), P.stacks.begin(), P.stacks.end());
+            far_blocks.insert(far_blocks.end(), P.far_blocks.begin(), P.far_blocks.end());
+            far_term.insert(far_term.end(), P.far_term.begin(), P.far_term.end());
+            p1.append(P.plan);
+            tgroups += P.tgroups;
+            P = Part();
         }
     }
     if (tgroups * 16 > 0x7fffffffll) {
         set_error("hmg_build_tensor_core_operands: %lld t_b terms exceed the plan's 32-bit term index", tgroups * 16);
         return HMG_ERR_UNSUPPORTED;
     }
-    // pass 2: per tile, its near pairs (B = X) and low-rank pairs (B = t_b)
-    bool all_tiles = true;
-    for (int t = 0; t < nt; t++) {
+    // pass 2: per tile, its near pairs (B = X) and low-rank pairs (B = t_b); tiles are
+    // independent, so contiguous ranges of them are planned on several host threads and
+    // the parts joined in tile order (the plan does not depend on the split)
+    auto plan_tile = [&](int t, TcmPlan& P) -> bool {
         bool started = false;
         const int sp = (ts[t] + 3) & ~3;
         for (int p = tps[t]; p < tps[t + 1]; p++) {
@@ -1065,7 +1158,7 @@ hmg_status build_tcm(hmg_matrix* h)
             const bool dense = b < h->ndense;
             if (!dense && h->h_rank[b] == 0) continue;
             if (!started) {
-                p2.begin(TcmJob{tr0[t], ts[t]});
+                P.begin(TcmJob{tr0[t], ts[t]});
                 started = true;
             }
             const PairDesc& d = desc[p];
@@ -1086,7 +1179,7 @@ hmg_status build_tcm(hmg_matrix* h)
                     stp.t0 = a;
                     stp.t1 = m2;
                     stp.t2 = -1;
-                    p2.add(stp, 16.0 * stp.n16);
+                    P.add(stp, 16.0 * stp.n16);
                 }
             } else {
                 const TcmTerms T = tcm_terms(h->h_rank[b], mixed ? h->h_r32[b] : h->h_rank[b], mixed ? h->h_r16[b] : 0);
@@ -1121,11 +1214,37 @@ hmg_status build_tcm(hmg_matrix* h)
                     stp.t0 = T.r32 | T.r32p << 16;
                     stp.t1 = T.r16 | T.r16p << 16;
                     stp.t2 = T.r8 | (T.compact ? 1 << 16 : 0);
-                    p2.add(stp, 16.0 * stp.n16);
+                    P.add(stp, 16.0 * stp.n16);
                 }
             }
         }
-        all_tiles = all_tiles && started;
+        return started;
+    };
+    bool all_tiles = true;
+    {
+        const int parts = std::max(1, std::min(plan_threads(), nt / 64));
+        std::vector<int> cut(parts + 1, nt);
+        cut[0] = 0;
+        for (int k = 1, t = 0; k < parts; k++) {  // about np / parts pairs a range
+            const long long goal = (long long)np * k / parts;
+            while (t < nt && tps[t] < goal) t++;
+            cut[k] = std::max(t, cut[k - 1]);
+        }
+        std::vector<TcmPlan> part(parts);
+        std::vector<char> all(parts, 1);
+        auto run = [&](int k) {
+            for (int t = cut[k]; t < cut[k + 1]; t++)
+                if (!plan_tile(t, part[k])) all[k] = 0;
+        };
+        std::vector<std::thread> th;
+        for (int k = 1; k < parts; k++) th.emplace_back(run, k);
+        run(0);
+        for (std::thread& x : th) x.join();
+        for (int k = 0; k < parts; k++) {
+            p2.append(part[k]);
+            all_tiles = all_tiles && all[k];
+            part[k] = TcmPlan();
+        }
     }
     p1.finish();
     p2.finish();
