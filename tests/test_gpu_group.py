@@ -276,3 +276,28 @@ def test_group_setup_rectangular(hmg, cuda):
         H.close()
     G0.close()
     G1.close()
+
+
+@pytest.mark.parametrize("max_level", [1, 3, 6])
+def test_group_setup_max_level(hmg, cuda, max_level):
+    """A level cap: the traversal's last level turns every remaining node into a leaf,
+    for all sets at once; the trees equal those of per-set setups with the same cap."""
+    sizes = [3000, 5000, 800]
+    ref = []
+    rng = np.random.default_rng(3)
+    for i, n in enumerate(sizes):
+        dim = 2 if i % 2 == 0 else 3
+        p = make_points("uniform", n, dim, 3 * 1000 + i)
+        H = engine(hmg, p, p, 1.5, 64 if dim == 2 else 128, rule=1, max_level=max_level)
+        H.set_kernel(hmg.KERNEL_GAUSSIAN, float(rng.uniform(0.01, 0.2)), 0.0)
+        ref.append(H)
+    G0 = hmg.group(ref)
+    raw, leaf = _raw_sets(hmg, sizes)
+    G1 = hmg.group_setup(raw, 1.5, leaf, max_level=max_level, rule=1)
+    for a, b in zip(G1.blocks(), G0.blocks()):
+        np.testing.assert_array_equal(a, b)
+    assert G1.info()["levels"] == G0.info()["levels"] <= max_level
+    for H in ref + raw:
+        H.close()
+    G0.close()
+    G1.close()
