@@ -151,3 +151,30 @@ def test_onchip_group_vs_fp64(hmg, cuda):
     for Hs in sets:
         Hs.close()
     G.close()
+
+
+def test_onchip_rectangular_and_plan_rebuild(hmg, cuda):
+    """Rows and columns from different point clouds (n1 != n2), mixed storage: on-chip
+    products within 1e-6 of FP64; the plan, built on several host threads, gives
+    bit-identical products when it is built again."""
+    torch = cuda
+    n1, n2 = 21000, 14000
+    p1 = make_points("uniform", n1, 3, 71)
+    p2 = make_points("uniform", n2, 3, 72)
+    H = engine(hmg, p1, p2, 1.5, 128, rule=1)
+    H.set_kernel(MATERN, 0.2, 0.0)
+    H.precompute_aca(96, 1e-8, hmg.PREC_MIXED)
+    H.precompute_dense(hmg.PREC_FP32)
+    X = torch.from_numpy(np.random.default_rng(5).uniform(-1, 1, (24, n2))).cuda()
+    Y = torch.empty(24, n1, dtype=torch.float64, device="cuda")
+    H.build_bf16_factors(near=hmg.PREC_BF16X6_ONCHIP)
+    H.matvec_multi(X, Y)
+    torch.cuda.synchronize()
+    errs = _errors_vs_fp64(torch, H, X, Y, seed=3)
+    assert max(errs) <= 1e-6, errs
+    H.build_bf16_factors(near=hmg.PREC_BF16X6_ONCHIP)
+    Y2 = torch.empty_like(Y)
+    H.matvec_multi(X, Y2)
+    torch.cuda.synchronize()
+    assert torch.equal(Y2, Y)
+    H.close()
