@@ -301,3 +301,32 @@ def test_fp64_arithmetic_products(hmg, cuda, prec):
     with pytest.raises(hmg.HmgError):
         H.set_product_precision(hmg.PREC_MIXED)
     H.close()
+
+
+def test_host_buffer_products(hmg, cuda):
+    """hmg_matvec_host copies x and y directly between the caller's memory and the
+    device: pageable and pinned host vectors give the device product bit for bit, and
+    the input vector is left unchanged."""
+    torch = cuda
+    n = 30000
+    p = make_points("uniform", n, 3, 41)
+    H = engine(hmg, p, p, 1.5, 128, rule=1)
+    H.set_kernel(hmg.KERNEL_MATERN32, 0.2, 0.0)
+    H.precompute_aca(96, 1e-8, hmg.PREC_MIXED)
+    H.precompute_dense(hmg.PREC_FP32)
+    x = np.random.default_rng(9).uniform(-1, 1, n)
+    dx = torch.from_numpy(x).cuda()
+    dy = torch.empty_like(dx)
+    H.matvec(dx, dy)
+    torch.cuda.synchronize()
+    ref = dy.cpu().numpy()
+    x_keep = x.copy()
+    np.testing.assert_array_equal(H.matvec(x), ref)  # pageable in, pageable out
+    np.testing.assert_array_equal(x, x_keep)
+    xp = torch.from_numpy(x).pin_memory()
+    yp = torch.empty(n, dtype=torch.float64).pin_memory()
+    H.matvec(xp.numpy(), yp.numpy())  # pinned in, pinned out
+    np.testing.assert_array_equal(yp.numpy(), ref)
+    for _ in range(3):  # repeated calls reuse the handle's device vectors
+        np.testing.assert_array_equal(H.matvec(x), ref)
+    H.close()
