@@ -97,6 +97,7 @@ _PROTOS = {
     "hmg_get_profile": (C.c_int, [_vp, _vp]),
     "hmg_set_matvec_variant": (C.c_int, [_vp, C.c_int]),
     "hmg_set_product_precision": (C.c_int, [_vp, C.c_int]),
+    "hmg_set_tensor_core_min_vectors": (C.c_int, [_vp, C.c_int]),
     "hmg_destroy": (C.c_int, [_vp]),
     "hmg_get_info": (C.c_int, [_vp, C.POINTER(Info)]),
     "hmg_get_codes": (C.c_int, [_vp, C.c_int, _vp]),

@@ -418,6 +418,14 @@ hmg_status hmg_set_graphs(hmg_matrix* h, int on)
     return HMG_OK;
 }
 
+hmg_status hmg_set_tensor_core_min_vectors(hmg_matrix* h, int nrhs)
+{
+    HMG_REQUIRE(h, HMG_ERR_INVALID, "hmg_set_tensor_core_min_vectors: NULL handle");
+    HMG_REQUIRE(nrhs >= 2, HMG_ERR_INVALID, "hmg_set_tensor_core_min_vectors: nrhs must be >= 2 (got %d)", nrhs);
+    h->tcm_min_nrhs = nrhs;
+    return HMG_OK;
+}
+
 hmg_status hmg_set_product_precision(hmg_matrix* h, int precision)
 {
     HMG_REQUIRE(h, HMG_ERR_INVALID, "hmg_set_product_precision: NULL handle");

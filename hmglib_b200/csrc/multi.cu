@@ -751,8 +751,10 @@ void launch_gather_multi32(hmg_matrix* h, const double* X, int ldx, int nrhs, fl
 
 hmg_status matvec_multi(hmg_matrix* h, int nrhs, const double* X, int ldx, double* Y, int ldy)
 {
-    // tensor cores, operands converted on chip from the stored factors and near field
-    if (h->tcm_ready && nrhs >= 2 && h->arith_prec == HMG_PREC_FP32 &&
+    // tensor cores, operands converted on chip from the stored factors and near field;
+    // a pass costs about the same for 2 to 32 vectors, so fewer than tcm_min_nrhs
+    // (hmg_set_tensor_core_min_vectors) run on the CUDA cores below
+    if (h->tcm_ready && nrhs >= 2 && nrhs >= h->tcm_min_nrhs && h->arith_prec == HMG_PREC_FP32 &&
         (h->ndense == 0 || (h->near_mode == HMG_NEAR_STORED && h->near_prec == HMG_PREC_FP32)))
         return matvec_multi_tcm(h, nrhs, X, ldx, Y, ldy);
     // tensor cores: a BF16 copy of the FP32 factors and an FP32 stored near field (up to 64 vectors a pass)

@@ -188,6 +188,11 @@ class HMatrix:
         self._call("hmg_group_offsets", int(which), _ptr(out))
         return out
 
+    def set_tensor_core_min_vectors(self, nrhs: int):
+        """With on-chip tensor-core operands, multi-vector products of fewer than nrhs
+        vectors (default 16) run on the CUDA cores (hmg_set_tensor_core_min_vectors)."""
+        self._call("hmg_set_tensor_core_min_vectors", int(nrhs))
+
     def set_product_precision(self, precision: int):
         """Arithmetic of products over FP32/mixed storage: PREC_FP32 (default) or PREC_FP64."""
         self._call("hmg_set_product_precision", int(precision))

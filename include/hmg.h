@@ -313,6 +313,14 @@ hmg_status hmg_autotune(hmg_matrix* h, int reps, int* piece_bytes, int* ctas_per
  * Results are bit-identical to direct launches.  Default off. */
 hmg_status hmg_set_graphs(hmg_matrix* h, int on);
 
+/* Multi-vector products on a handle with operands converted on chip
+ * (hmg_build_tensor_core_operands with HMG_PREC_BF16X6_ONCHIP) run on the tensor
+ * cores from nrhs vectors a pass (default 16); smaller batches run on the CUDA
+ * cores, which are faster there: a tensor-core pass costs about the same for 2 to
+ * 32 vectors.  nrhs >= 2; 2 sends every multi-vector product to the tensor cores.
+ * No reference counterpart (the reference multiplies one vector per call). */
+hmg_status hmg_set_tensor_core_min_vectors(hmg_matrix* h, int nrhs);
+
 /* Arithmetic of the products over FP32 or mixed storage (no reference counterpart):
  * HMG_PREC_FP32 (default) multiplies each slice in FP32 and sums the slices in FP64;
  * HMG_PREC_FP64 converts every stored value and multiplies in FP64, so the stored

@@ -53,6 +53,7 @@ def test_onchip_products_vs_fp64(hmg, cuda, case):
     Ycc = torch.empty_like(X)
     H.matvec_multi(X, Ycc)  # CUDA cores, before the plan exists
     H.build_bf16_factors(near=hmg.PREC_BF16X6_ONCHIP)
+    H.set_tensor_core_min_vectors(2)  # every multi-vector product on the tensor cores
     info = H.info()
     assert info["tc_onchip"] == 1 and info["tc_parts"] == 3 and info["tc_bytes"] == 0
     Y = torch.full_like(X, float("nan"))
@@ -99,6 +100,7 @@ def test_onchip_leading_dimensions_and_refusals(hmg, cuda):
     n = 9000
     H = _build(hmg, "uniform", n, 2, 64, GAUSS, 0.1, 32, 1e-6, hmg.PREC_MIXED, seed=3)
     H.build_bf16_factors(near=hmg.PREC_BF16X6_ONCHIP)
+    H.set_tensor_core_min_vectors(2)
     nrhs, ld = 5, n + 17
     Xb = torch.from_numpy(np.random.default_rng(1).uniform(-1, 1, (nrhs, ld))).cuda()
     Yb = torch.zeros(nrhs, ld + 5, dtype=torch.float64, device="cuda")
@@ -135,6 +137,7 @@ def test_onchip_group_vs_fp64(hmg, cuda):
     G.precompute_aca(64, 1e-8, hmg.PREC_MIXED)
     G.precompute_dense(hmg.PREC_FP32)
     G.build_bf16_factors(near=hmg.PREC_BF16X6_ONCHIP)
+    G.set_tensor_core_min_vectors(2)
     off = G.offsets(0)
     X = torch.from_numpy(np.random.default_rng(24).uniform(-1, 1, (8, int(off[-1])))).cuda()
     Y = torch.empty_like(X)
@@ -177,4 +180,28 @@ def test_onchip_rectangular_and_plan_rebuild(hmg, cuda):
     H.matvec_multi(X, Y2)
     torch.cuda.synchronize()
     assert torch.equal(Y2, Y)
+    H.close()
+
+
+def test_onchip_min_vectors_dispatch(hmg, cuda):
+    """Below the threshold (default 16 vectors) a handle with on-chip operands
+    multiplies on the CUDA cores: the same bits as before the plan existed; at or above
+    it, on the tensor cores (other rounding, same accuracy)."""
+    torch = cuda
+    n = 20000
+    H = _build(hmg, "uniform", n, 3, 128, MATERN, 0.2, 96, 1e-8, hmg.PREC_MIXED, seed=51)
+    X = torch.from_numpy(np.random.default_rng(52).uniform(-1, 1, (8, n))).cuda()
+    Ycc, Y = torch.empty_like(X), torch.empty_like(X)
+    H.matvec_multi(X, Ycc)
+    H.build_bf16_factors(near=hmg.PREC_BF16X6_ONCHIP)
+    H.matvec_multi(X, Y)  # 8 < 16: CUDA cores
+    torch.cuda.synchronize()
+    assert torch.equal(Y, Ycc)
+    H.set_tensor_core_min_vectors(8)
+    H.matvec_multi(X, Y)  # tensor cores
+    torch.cuda.synchronize()
+    assert not torch.equal(Y, Ycc)
+    assert max(_errors_vs_fp64(torch, H, X, Y, nrows=1024, seed=4)) <= 1e-6
+    with pytest.raises(hmg.HmgError):
+        H.set_tensor_core_min_vectors(1)
     H.close()
