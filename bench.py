@@ -635,7 +635,9 @@ def run_precision(a, rank, world):
     """The precision workload: N = 2^21 points in 2D from a 16-component Gaussian
     mixture (seed 2), Gaussian kernel length^2 0.05, ACA eps 1e-6.  Products of 32
     vectors per pass with FP32 factors and with mixed (FP32/FP16/FP8) factors, FP32
-    near field, FP32 products summed in FP64, and a kernel-ridge CG solve of
+    near field, FP32 products summed in FP64 (and on the tensor cores: BF16 copies of the
+    FP32 factors; three BF16 parts split on chip from the mixed storage), and a
+    kernel-ridge CG solve of
     (K + 1e-3 I) x = b to relative residual 1e-8 with refinement (FP64 residuals,
     relaxed-precision inner products).  Each result's error against FP64 direct sums
     over 2,048 sampled rows is reported."""
@@ -709,6 +711,30 @@ def run_precision(a, rank, world):
                "max_rank": info["max_rank"]}
         if prec == hmg.PREC_FP32:
             res["bf16_tensor_cores"] = tc
+        if prec == hmg.PREC_MIXED:
+            # tensor cores over the same mixed storage, every operand split into three
+            # BF16 parts on chip (no copy; error <= 1e-6 territory)
+            t0 = time.perf_counter()
+            H.build_bf16_factors(near=hmg.PREC_BF16X6_ONCHIP)
+            t_plan = time.perf_counter() - t0
+            Yt = torch.empty_like(X)
+            for _ in range(2):
+                H.matvec_multi(X, Yt)
+            torch.cuda.synchronize()
+            e0.record(stream)
+            for _ in range(a.steps):
+                H.matvec_multi(X, Yt)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            ms_oc = e0.elapsed_time(e1) / a.steps
+            errs_oc = []
+            for j in range(0, nrhs, 8):
+                yd = torch.empty(rows.shape[0], dtype=torch.float64, device="cuda")
+                H.full_matvec_rows(X[j], rows, yd)
+                torch.cuda.synchronize()
+                errs_oc.append(float(torch.linalg.norm(Yt[j][rows.long()] - yd) / torch.linalg.norm(yd)))
+            res["onchip_tensor_cores"] = {"ms_per_32_vectors": ms_oc, "vectors_per_s": nrhs * 1000.0 / ms_oc,
+                                          "err_vs_fp64_max": max(errs_oc), "plan_s": t_plan}
         if name == "fp32" and not a.no_feasibility:
             res["ridge_feasibility"] = ridge_feasibility(torch, hmg, H, n, [1e-3, 1e-2, 1e-1, 1.0],
                                                          cg_maxit=a.cg_maxit)
