@@ -181,7 +181,9 @@ hmg_status hmg_full_matvec_rows(hmg_matrix* h, const double* x, const int* rows,
  * they stream it (FP16 / FP8 terms into the parts that hold them exactly, with fewer
  * MMAs).  Products agree with FP64 to ~4e-7 like HMG_PREC_BF16X6, and the only memory
  * added is the X and t_b operand buffer (3 x 2 bytes x 64 vectors per column and per
- * term): this is the form that fits at N = 2^20.
+ * term): this is the form that fits at N = 2^20.  Its products of fewer than 16
+ * vectors a pass run on the CUDA cores (hmg_set_tensor_core_min_vectors).  The plan
+ * is built on the host once, on several threads.
  * hmg_build_bf16_factors(h) is hmg_build_tensor_core_operands(h, HMG_PREC_BF16). */
 hmg_status hmg_build_tensor_core_operands(hmg_matrix* h, int near_precision);
 hmg_status hmg_build_bf16_factors(hmg_matrix* h);
