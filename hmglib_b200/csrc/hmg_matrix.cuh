@@ -103,7 +103,7 @@ struct hmg_matrix {
 
     // ---- tensor-core products with operands converted on chip (tcm.cu) ------------
     bool tcm_ready = false;
-    int tcm_min_nrhs = 16;    // on-chip tensor-core products from this many vectors a pass
+    int tcm_min_nrhs = 17;    // on-chip tensor-core products from this many vectors a pass
     char* tcm_steps[2] = {nullptr, nullptr};  // per pass: steps, CTA by CTA
     char* tcm_jobs[2] = {nullptr, nullptr};   // per pass: jobs, CTA by CTA
     char* tcm_cta[2] = {nullptr, nullptr};    // per CTA: first job and step (int2), then the ends

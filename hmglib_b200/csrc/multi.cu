@@ -120,6 +120,18 @@ static constexpr size_t K1M_SMEM = 8 * K1M_STAGES * 4 * 128 * sizeof(float);  //
 // computes 4 rows x 4 vectors over every CGN-th group of 4 columns of a stage (V
 // from shared memory, X from global/L1), and the CGN column groups are summed by a
 // fixed xor butterfly at the end of each 4-row block.
+// {a0, a1} += s * {b0, b1}: one packed FP32 multiply-add (two vectors of one stored
+// value), each lane rounded as fmaf would round it
+__device__ __forceinline__ void fma2s(float& a0, float& a1, float s, float b0, float b1)
+{
+    uint32_t x0 = __float_as_uint(a0), x1 = __float_as_uint(a1);
+    asm("{\n\t.reg .b64 a, b, d;\n\tmov.b64 a, {%2, %2};\n\tmov.b64 b, {%3, %4};\n\tmov.b64 d, {%0, %1};\n\t"
+        "fma.rn.f32x2 d, a, b, d;\n\tmov.b64 {%0, %1}, d;\n\t}"
+        : "+r"(x0), "+r"(x1) : "r"(__float_as_uint(s)), "r"(__float_as_uint(b0)), "r"(__float_as_uint(b1)));
+    a0 = __uint_as_float(x0);
+    a1 = __uint_as_float(x1);
+}
+
 // 16 bytes of a K1 piece row of tier TIER as [column q][term t] floats: 4 columns of
 // TG = 1 (FP32), 2 (FP16 pairs) or 4 (FP8 quads) terms
 template <int TIER>
@@ -212,10 +224,8 @@ __global__ void __launch_bounds__(256) k_vtx_multi_smem(const K1Desc* __restrict
                         for (int tt = 0; tt < TG; tt++) {
                             const float vv = f[q * TG + tt];
                             float* ac = acc[k * TG + tt];
-                            ac[0] = fmaf(vv, xv[q].x, ac[0]);
-                            ac[1] = fmaf(vv, xv[q].y, ac[1]);
-                            ac[2] = fmaf(vv, xv[q].z, ac[2]);
-                            ac[3] = fmaf(vv, xv[q].w, ac[3]);
+                            fma2s(ac[0], ac[1], vv, xv[q].x, xv[q].y);
+                            fma2s(ac[2], ac[3], vv, xv[q].z, xv[q].w);
                         }
                 }
             }
@@ -404,10 +414,8 @@ __global__ void __launch_bounds__(256) k_tile_multi_smem(const PairDesc* __restr
             const float4 w = *reinterpret_cast<const float4*>(&Ts[buf][k][cg * 4]);
 #pragma unroll
             for (int i = 0; i < TR; i++) {
-                acc[i][0] = fmaf(u[i], w.x, acc[i][0]);
-                acc[i][1] = fmaf(u[i], w.y, acc[i][1]);
-                acc[i][2] = fmaf(u[i], w.z, acc[i][2]);
-                acc[i][3] = fmaf(u[i], w.w, acc[i][3]);
+                fma2s(acc[i][0], acc[i][1], u[i], w.x, w.y);
+                fma2s(acc[i][2], acc[i][3], u[i], w.z, w.w);
             }
         }
         int pn = p, kn = k0;
@@ -544,10 +552,8 @@ __global__ void __launch_bounds__(256) k_tile_multi_mixed(const PairDesc* __rest
 #pragma unroll
                 for (int i = 0; i < TR; i++) {
                     const float u = __uint_as_float(w[i]);
-                    acc[i][0] = fmaf(u, x.x, acc[i][0]);
-                    acc[i][1] = fmaf(u, x.y, acc[i][1]);
-                    acc[i][2] = fmaf(u, x.z, acc[i][2]);
-                    acc[i][3] = fmaf(u, x.w, acc[i][3]);
+                    fma2s(acc[i][0], acc[i][1], u, x.x, x.y);
+                    fma2s(acc[i][2], acc[i][3], u, x.z, x.w);
                 }
             } else if (tg == 2) {
                 const float4 x0 = *reinterpret_cast<const float4*>(&Ts[buf][k][0][cg * 4]);
@@ -555,10 +561,10 @@ __global__ void __launch_bounds__(256) k_tile_multi_mixed(const PairDesc* __rest
 #pragma unroll
                 for (int i = 0; i < TR; i++) {
                     const float2 f = __half22float2(*reinterpret_cast<const __half2*>(&w[i]));
-                    acc[i][0] = fmaf(f.y, x1.x, fmaf(f.x, x0.x, acc[i][0]));
-                    acc[i][1] = fmaf(f.y, x1.y, fmaf(f.x, x0.y, acc[i][1]));
-                    acc[i][2] = fmaf(f.y, x1.z, fmaf(f.x, x0.z, acc[i][2]));
-                    acc[i][3] = fmaf(f.y, x1.w, fmaf(f.x, x0.w, acc[i][3]));
+                    fma2s(acc[i][0], acc[i][1], f.x, x0.x, x0.y);
+                    fma2s(acc[i][2], acc[i][3], f.x, x0.z, x0.w);
+                    fma2s(acc[i][0], acc[i][1], f.y, x1.x, x1.y);
+                    fma2s(acc[i][2], acc[i][3], f.y, x1.z, x1.w);
                 }
             } else {
                 float4 x[4];
@@ -573,10 +579,8 @@ __global__ void __launch_bounds__(256) k_tile_multi_mixed(const PairDesc* __rest
                     const float f[4] = {a.x, a.y, c.x, c.y};
 #pragma unroll
                     for (int tt = 0; tt < 4; tt++) {
-                        acc[i][0] = fmaf(f[tt], x[tt].x, acc[i][0]);
-                        acc[i][1] = fmaf(f[tt], x[tt].y, acc[i][1]);
-                        acc[i][2] = fmaf(f[tt], x[tt].z, acc[i][2]);
-                        acc[i][3] = fmaf(f[tt], x[tt].w, acc[i][3]);
+                        fma2s(acc[i][0], acc[i][1], f[tt], x[tt].x, x[tt].y);
+                        fma2s(acc[i][2], acc[i][3], f[tt], x[tt].z, x[tt].w);
                     }
                 }
             }
@@ -753,7 +757,8 @@ hmg_status matvec_multi(hmg_matrix* h, int nrhs, const double* X, int ldx, doubl
 {
     // tensor cores, operands converted on chip from the stored factors and near field;
     // a pass costs about the same for 2 to 32 vectors, so fewer than tcm_min_nrhs
-    // (hmg_set_tensor_core_min_vectors) run on the CUDA cores below
+    // (hmg_set_tensor_core_min_vectors; 17: the CUDA-core kernels below take up to 16
+    // vectors a pass faster, and 17 to 32 at the cost of 32) run on the CUDA cores
     if (h->tcm_ready && nrhs >= 2 && nrhs >= h->tcm_min_nrhs && h->arith_prec == HMG_PREC_FP32 &&
         (h->ndense == 0 || (h->near_mode == HMG_NEAR_STORED && h->near_prec == HMG_PREC_FP32)))
         return matvec_multi_tcm(h, nrhs, X, ldx, Y, ldy);

@@ -190,7 +190,7 @@ class HMatrix:
 
     def set_tensor_core_min_vectors(self, nrhs: int):
         """With on-chip tensor-core operands, multi-vector products of fewer than nrhs
-        vectors (default 16) run on the CUDA cores (hmg_set_tensor_core_min_vectors)."""
+        vectors (default 17) run on the CUDA cores (hmg_set_tensor_core_min_vectors)."""
         self._call("hmg_set_tensor_core_min_vectors", int(nrhs))
 
     def set_product_precision(self, precision: int):

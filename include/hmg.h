@@ -181,7 +181,7 @@ hmg_status hmg_full_matvec_rows(hmg_matrix* h, const double* x, const int* rows,
  * they stream it (FP16 / FP8 terms into the parts that hold them exactly, with fewer
  * MMAs).  Products agree with FP64 to ~4e-7 like HMG_PREC_BF16X6, and the only memory
  * added is the X and t_b operand buffer (3 x 2 bytes x 64 vectors per column and per
- * term): this is the form that fits at N = 2^20.  Its products of fewer than 16
+ * term): this is the form that fits at N = 2^20.  Its products of fewer than 17
  * vectors a pass run on the CUDA cores (hmg_set_tensor_core_min_vectors).  The plan
  * is built on the host once, on several threads.
  * hmg_build_bf16_factors(h) is hmg_build_tensor_core_operands(h, HMG_PREC_BF16). */
@@ -317,7 +317,7 @@ hmg_status hmg_set_graphs(hmg_matrix* h, int on);
 
 /* Multi-vector products on a handle with operands converted on chip
  * (hmg_build_tensor_core_operands with HMG_PREC_BF16X6_ONCHIP) run on the tensor
- * cores from nrhs vectors a pass (default 16); smaller batches run on the CUDA
+ * cores from nrhs vectors a pass (default 17); smaller batches run on the CUDA
  * cores, which are faster there: a tensor-core pass costs about the same for 2 to
  * 32 vectors.  nrhs >= 2; 2 sends every multi-vector product to the tensor cores.
  * No reference counterpart (the reference multiplies one vector per call). */

@@ -184,7 +184,7 @@ def test_onchip_rectangular_and_plan_rebuild(hmg, cuda):
 
 
 def test_onchip_min_vectors_dispatch(hmg, cuda):
-    """Below the threshold (default 16 vectors) a handle with on-chip operands
+    """Below the threshold (default 17 vectors) a handle with on-chip operands
     multiplies on the CUDA cores: the same bits as before the plan existed; at or above
     it, on the tensor cores (other rounding, same accuracy)."""
     torch = cuda
@@ -194,7 +194,7 @@ def test_onchip_min_vectors_dispatch(hmg, cuda):
     Ycc, Y = torch.empty_like(X), torch.empty_like(X)
     H.matvec_multi(X, Ycc)
     H.build_bf16_factors(near=hmg.PREC_BF16X6_ONCHIP)
-    H.matvec_multi(X, Y)  # 8 < 16: CUDA cores
+    H.matvec_multi(X, Y)  # 8 < 17: CUDA cores
     torch.cuda.synchronize()
     assert torch.equal(Y, Ycc)
     H.set_tensor_core_min_vectors(8)
