@@ -446,21 +446,23 @@ __global__ void __launch_bounds__(256) k_tile_multi_smem(const PairDesc* __restr
 // Mixed storage (FP32 / FP16-pair / FP8-quad chunk columns), R = 8, 16 or 32
 // vectors: the tile kernel above with each chunk column decoded at use.  A chunk
 // column holds TG = 1, 2 or 4 terms for 4 rows per 16 bytes; the stage carries the TG
-// vector rows (t_b, already scaled) that multiply it.
+// vector rows (t_b, already scaled) that multiply it.  A thread keeps VT vectors of its
+// rows (8 for R = 8, in blocks of 128 threads, so that each decoded value feeds four
+// packed multiply-adds; else 4, in blocks of 256).
 template <int R>
 constexpr size_t mixed_tile_smem()
 {
     return (size_t)4 * 16 * (HMG_TILE_ROWS + 4 * R) * sizeof(float) + 4 * 16 * sizeof(int);
 }
 
-template <int R>
+template <int R, int VT>
 __global__ void __launch_bounds__(256) k_tile_multi_mixed(const PairDesc* __restrict__ desc,
                                                           const int* tile_pair_start, const int* tile_r0,
                                                           const int* tile_s, const int* perm1,
                                                           const float* __restrict__ xm, const float* __restrict__ tm,
                                                           const char* tbase, int nrhs, double* Y, int ldy)
 {
-    constexpr int KC = 16, NS = 4, CG = R / 4, TR = R / 8;
+    constexpr int KC = 16, NS = 4, CG = R / VT, TR = R / 8, NT = 1024 / VT;  // VT vectors a thread
     extern __shared__ __align__(16) float mx_smem[];
     float (*Us)[KC][HMG_TILE_ROWS] = reinterpret_cast<float (*)[KC][HMG_TILE_ROWS]>(mx_smem);
     float (*Ts)[KC][4][R] = reinterpret_cast<float (*)[KC][4][R]>(mx_smem + NS * KC * HMG_TILE_ROWS);
@@ -478,7 +480,7 @@ __global__ void __launch_bounds__(256) k_tile_multi_mixed(const PairDesc* __rest
         const PairDesc d = desc[p];
         const int nc = cols(d);
         const char* data = static_cast<const char*>(d.data);
-        for (int idx = tid; idx < KC * sp4; idx += 256) {
+        for (int idx = tid; idx < KC * sp4; idx += NT) {
             const int kk = idx / sp4, r4 = idx - kk * sp4;
             const bool v = k0 + kk < nc;
             cp_async16(&Us[b][kk][r4 * 4], v ? data + ((size_t)(k0 + kk) * sp + r4 * 4) * 4 : data, v);
@@ -486,7 +488,7 @@ __global__ void __launch_bounds__(256) k_tile_multi_mixed(const PairDesc* __rest
         const bool far = d.kind == PAIR_FAR_MIXED;
         const float* tb = far ? tm + (size_t)((static_cast<const char*>(d.w) - tbase) / 4) * R : xm + (size_t)d.c0 * R;
         const int n32 = d.ncol, n16 = d.c0 >> 1;
-        for (int idx = tid; idx < KC * 4 * (R / 4); idx += 256) {
+        for (int idx = tid; idx < KC * 4 * (R / 4); idx += NT) {
             const int kk = idx / (4 * (R / 4)), rem = idx - kk * (4 * (R / 4));
             const int tt = rem / (R / 4), c4 = rem - tt * (R / 4);
             const int k = k0 + kk;
@@ -519,12 +521,12 @@ __global__ void __launch_bounds__(256) k_tile_multi_mixed(const PairDesc* __rest
         }
         asm volatile("cp.async.commit_group;" ::: "memory");
     }
-    double acc64[TR][4];
-    float acc[TR][4];
+    double acc64[TR][VT];
+    float acc[TR][VT];
 #pragma unroll
     for (int i = 0; i < TR; i++)
 #pragma unroll
-        for (int c = 0; c < 4; c++) acc64[i][c] = 0.0, acc[i][c] = 0.0f;
+        for (int c = 0; c < VT; c++) acc64[i][c] = 0.0, acc[i][c] = 0.0f;
     for (int it = 0; p < pend; it++) {
         if (pp < pend) {
             issue((it + NS - 1) % NS, pp, kp);
@@ -548,28 +550,41 @@ __global__ void __launch_bounds__(256) k_tile_multi_mixed(const PairDesc* __rest
             }
             const int tg = Tg[buf][k];
             if (tg == 1) {
-                const float4 x = *reinterpret_cast<const float4*>(&Ts[buf][k][0][cg * 4]);
 #pragma unroll
-                for (int i = 0; i < TR; i++) {
-                    const float u = __uint_as_float(w[i]);
-                    fma2s(acc[i][0], acc[i][1], u, x.x, x.y);
-                    fma2s(acc[i][2], acc[i][3], u, x.z, x.w);
+                for (int hh = 0; hh < VT / 4; hh++) {
+                    const float4 x = *reinterpret_cast<const float4*>(&Ts[buf][k][0][cg * VT + 4 * hh]);
+#pragma unroll
+                    for (int i = 0; i < TR; i++) {
+                        const float u = __uint_as_float(w[i]);
+                        fma2s(acc[i][4 * hh], acc[i][4 * hh + 1], u, x.x, x.y);
+                        fma2s(acc[i][4 * hh + 2], acc[i][4 * hh + 3], u, x.z, x.w);
+                    }
                 }
             } else if (tg == 2) {
-                const float4 x0 = *reinterpret_cast<const float4*>(&Ts[buf][k][0][cg * 4]);
-                const float4 x1 = *reinterpret_cast<const float4*>(&Ts[buf][k][1][cg * 4]);
+                float4 x0[VT / 4], x1[VT / 4];
+#pragma unroll
+                for (int hh = 0; hh < VT / 4; hh++) {
+                    x0[hh] = *reinterpret_cast<const float4*>(&Ts[buf][k][0][cg * VT + 4 * hh]);
+                    x1[hh] = *reinterpret_cast<const float4*>(&Ts[buf][k][1][cg * VT + 4 * hh]);
+                }
 #pragma unroll
                 for (int i = 0; i < TR; i++) {
                     const float2 f = __half22float2(*reinterpret_cast<const __half2*>(&w[i]));
-                    fma2s(acc[i][0], acc[i][1], f.x, x0.x, x0.y);
-                    fma2s(acc[i][2], acc[i][3], f.x, x0.z, x0.w);
-                    fma2s(acc[i][0], acc[i][1], f.y, x1.x, x1.y);
-                    fma2s(acc[i][2], acc[i][3], f.y, x1.z, x1.w);
+#pragma unroll
+                    for (int hh = 0; hh < VT / 4; hh++) {
+                        fma2s(acc[i][4 * hh], acc[i][4 * hh + 1], f.x, x0[hh].x, x0[hh].y);
+                        fma2s(acc[i][4 * hh + 2], acc[i][4 * hh + 3], f.x, x0[hh].z, x0[hh].w);
+                        fma2s(acc[i][4 * hh], acc[i][4 * hh + 1], f.y, x1[hh].x, x1[hh].y);
+                        fma2s(acc[i][4 * hh + 2], acc[i][4 * hh + 3], f.y, x1[hh].z, x1[hh].w);
+                    }
                 }
             } else {
-                float4 x[4];
+                float4 x[4][VT / 4];
 #pragma unroll
-                for (int tt = 0; tt < 4; tt++) x[tt] = *reinterpret_cast<const float4*>(&Ts[buf][k][tt][cg * 4]);
+                for (int tt = 0; tt < 4; tt++)
+#pragma unroll
+                    for (int hh = 0; hh < VT / 4; hh++)
+                        x[tt][hh] = *reinterpret_cast<const float4*>(&Ts[buf][k][tt][cg * VT + 4 * hh]);
 #pragma unroll
                 for (int i = 0; i < TR; i++) {
                     __half2_raw lo = __nv_cvt_fp8x2_to_halfraw2((__nv_fp8x2_storage_t)(w[i] & 0xffffu), __NV_E4M3);
@@ -578,10 +593,12 @@ __global__ void __launch_bounds__(256) k_tile_multi_mixed(const PairDesc* __rest
                     const float2 c = __half22float2(*reinterpret_cast<const __half2*>(&hi));
                     const float f[4] = {a.x, a.y, c.x, c.y};
 #pragma unroll
-                    for (int tt = 0; tt < 4; tt++) {
-                        fma2s(acc[i][0], acc[i][1], f[tt], x[tt].x, x[tt].y);
-                        fma2s(acc[i][2], acc[i][3], f[tt], x[tt].z, x[tt].w);
-                    }
+                    for (int tt = 0; tt < 4; tt++)
+#pragma unroll
+                        for (int hh = 0; hh < VT / 4; hh++) {
+                            fma2s(acc[i][4 * hh], acc[i][4 * hh + 1], f[tt], x[tt][hh].x, x[tt][hh].y);
+                            fma2s(acc[i][4 * hh + 2], acc[i][4 * hh + 3], f[tt], x[tt][hh].z, x[tt][hh].w);
+                        }
                 }
             }
         }
@@ -591,7 +608,7 @@ __global__ void __launch_bounds__(256) k_tile_multi_mixed(const PairDesc* __rest
 #pragma unroll
             for (int i = 0; i < TR; i++)
 #pragma unroll
-                for (int c = 0; c < 4; c++) acc64[i][c] += (double)acc[i][c], acc[i][c] = 0.0f;
+                for (int c = 0; c < VT; c++) acc64[i][c] += (double)acc[i][c], acc[i][c] = 0.0f;
         }
         __syncthreads();  // this buffer is refilled NS - 1 stages on
         p = pn;
@@ -603,8 +620,8 @@ __global__ void __launch_bounds__(256) k_tile_multi_mixed(const PairDesc* __rest
         const int row = rg * TR + i;
         if (row < s)
 #pragma unroll
-            for (int c = 0; c < 4; c++) {
-                const int j = cg * 4 + c;
+            for (int c = 0; c < VT; c++) {
+                const int j = cg * VT + c;
                 if (j < nrhs) Y[perm1[tr0 + row] + (size_t)j * ldy] = acc64[i][c];
             }
     }
@@ -641,9 +658,10 @@ static hmg_status launch_multi_mixed(hmg_matrix* h, int nrhs, const double* X, i
         first += cnt[tier];
     }
     if (h->ntiles > 0) {
-        HMG_CUDA_TRY(cudaFuncSetAttribute(k_tile_multi_mixed<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        constexpr int VT = R == 8 ? 8 : 4;
+        HMG_CUDA_TRY(cudaFuncSetAttribute(k_tile_multi_mixed<R, VT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                           (int)mixed_tile_smem<R>()));
-        k_tile_multi_mixed<R><<<h->ntiles, 256, mixed_tile_smem<R>(), s>>>(
+        k_tile_multi_mixed<R, VT><<<h->ntiles, 1024 / VT, mixed_tile_smem<R>(), s>>>(
             static_cast<const PairDesc*>(h->pair_desc), h->tile_pair_start, h->tile_r0, h->tile_s, h->perm[0], xm, tm,
             static_cast<const char*>(h->tbuf), nrhs, Y, ldy);
         HMG_LAUNCH_CHECK();
